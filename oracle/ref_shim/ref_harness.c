@@ -1,0 +1,643 @@
+/*
+ * Harness around the unmodified SSENSS sources (test infrastructure, built
+ * into oracle/_ref/libssenss_ref.so).  It sets the solver up the way
+ * src/main.c:36-90 does, but from an in-memory mesh, and exposes flat-array
+ * entry points for Python (ctypes) to call: operator apply, DSS, weighted dot,
+ * the Poisson/Helmholtz solves with their residual histories, one p-multigrid
+ * application, dealiased convection, particle advance and the Navier-Stokes
+ * step.  The reference is not re-entrant (src/precon.c:273-281), so all state
+ * lives in file-scope variables and one mesh is set up at a time.
+ *
+ * Residual histories: the build renames global_dot_product in src/global.c to
+ * ssgref_dot_impl and every caller's reference to ssgref_dot_hook; likewise
+ * multigrid_preconditioner (src/precon.c) becomes ssgref_mg_impl behind
+ * ssgref_mg_hook.  The hook records sqrt(x.x) for calls with x == y made
+ * outside the preconditioner, which in conjugate_gradient and
+ * flexible_conjugate_gradient (src/solver.c:72-73,151-152) is exactly the
+ * residual check; the nullspace norm (x == y == ones, src/solver.c:207) is
+ * filtered out.
+ */
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include "structs.h"
+#include "utils.h"
+#include "linalg.h"
+#include "tripalg.h"
+#include "basis.h"
+#include "geometry.h"
+#include "interpolation.h"
+#include "deriv.h"
+#include "init.h"
+#include "final.h"
+#include "poisson.h"
+#include "helmholtz.h"
+#include "global.h"
+#include "solver.h"
+#include "precon.h"
+#include "convection.h"
+#include "navier_stokes.h"
+#include "particles.h"
+#include "stokes.h"
+#include "time.h"
+#include "test.h"
+#include "synth_dataio.h"
+
+double ssgref_dot_impl(struct element **sel, double ****x, double ****y);
+void ssgref_mg_impl(struct element **sel, double ****x, double ****px,
+		int var, double eps, void (*opeval) ());
+
+static struct parameters *H_params;
+static struct communicator *H_comm;
+static struct basis *H_gll;
+static struct basis *H_conv;
+static struct geometry **H_geom;
+static struct geometry **H_cgeom;
+static struct element **H_sel;
+static int H_nel;
+static int H_n;
+
+static int H_recording;
+static int H_precon_depth;
+static double *H_hist;
+static int H_hist_cap;
+static int H_hist_len;
+
+static int all_ones(double ****x, size_t len)
+{
+	const double *p = ***x;
+	return p[0] == 1.0 && p[len / 2] == 1.0 && p[len - 1] == 1.0;
+}
+
+double ssgref_dot_hook(struct element **sel, double ****x, double ****y)
+{
+	const double v = ssgref_dot_impl(sel, x, y);
+	const size_t len = (size_t) (*sel)->basis->ntot * (size_t) (*sel)->nel;
+	if (H_recording && H_precon_depth == 0 && x == y && !all_ones(x, len)) {
+		if (H_hist_len < H_hist_cap)
+			H_hist[H_hist_len] = sqrt(v);
+		++H_hist_len;
+	}
+	return v;
+}
+
+void ssgref_mg_hook(struct element **sel, double ****x, double ****px,
+		int var, double eps, void (*opeval) ())
+{
+	++H_precon_depth;
+	ssgref_mg_impl(sel, x, px, var, eps, opeval);
+	--H_precon_depth;
+}
+
+static size_t npts(void)
+{
+	return (size_t) H_nel * (size_t) H_n * H_n * H_n;
+}
+
+/* Copy a flat L-vector into a fresh 4-D array (src/utils.c:64-81 layout). */
+static double ****from_flat(const double *src)
+{
+	double ****a = new_4d_array(H_n, H_n, H_n, H_nel);
+	memcpy(***a, src, npts() * sizeof(double));
+	return a;
+}
+
+void ssgref_teardown(void)
+{
+	if (!H_sel)
+		return;
+	free_basis(H_gll);
+	free_basis(H_conv);
+	disconnect_elements(H_sel);
+	free_elements(H_sel);
+	free_communicator(H_comm);
+	free_geometries(H_geom);
+	free_geometries(H_cgeom);
+	free_parameters(H_params);
+	H_sel = NULL;
+}
+
+/* Set the solver up as src/main.c:36-90 does (minus files and particles). */
+int ssgref_setup(int n, int nel, const double *vertices, const int *neigh,
+		double dt, double visc, double dens)
+{
+	ssgref_teardown();
+	ssgref_mesh.nel = nel;
+	ssgref_mesh.vertices = vertices;
+	ssgref_mesh.neigh = neigh;
+	ssgref_mesh.init_velocity = NULL;
+
+	H_comm = new_communicator(0, 1, MPI_COMM_WORLD, MPI_INFO_NULL);
+	H_params = new_parameters(0, 1);
+	H_params->n = n;
+	H_params->dt = dt;
+	H_params->visc = visc;
+	H_params->dens = dens;
+	H_params->nconv = (3 * n) / 2;
+	H_params->svvn = 2 * n / 3;
+	H_params->svva = 0.0;
+	get_grid_size(H_params, H_comm, "");
+
+	H_gll = new_gll_basis(n);
+	H_conv = new_gll_basis(H_params->nconv);
+	create_interpolation_matrices(H_gll, H_conv);
+	compute_svv_derivative_matrix(H_gll, H_params->svvn, H_params->svva);
+
+	H_geom = new_geometries(H_gll, H_params->nel, H_params->neltot);
+	H_cgeom = new_geometries(H_conv, H_params->nel, H_params->neltot);
+	read_grid(H_geom, H_comm, H_gll, "");
+	read_grid(H_cgeom, H_comm, H_conv, "");
+
+	H_sel = new_elements(H_geom, H_cgeom, H_gll, H_conv, H_params, H_comm);
+	connect_elements(H_sel);
+	initialise_preconditioners(H_sel);
+	H_nel = nel;
+	H_n = n;
+	return (*H_sel)->precon->nlevels;
+}
+
+void ssgref_set_time(double t, double dt, double visc)
+{
+	H_params->t = t;
+	H_params->dt = dt;
+	H_params->visc = visc;
+}
+
+/* ---- discretisation data, exported for the oracle and for parity ---- */
+
+int ssgref_level_order(int level)
+{
+	return (*H_sel)->precon->nmg[level];
+}
+
+int ssgref_conv_order(void)
+{
+	return H_params->nconv;
+}
+
+/* GLL points, weights and the stored derivative matrices d[j][i] = D_ij
+ * of level `level` (src/basis.c:160-177, src/deriv.c:81-104). */
+void ssgref_level_basis(int level, double *points, double *weights,
+		double *deriv, double *svv_deriv)
+{
+	struct basis *b = (*H_sel)->precon->basis[2 * level];
+	const int m = b->n;
+	memcpy(points, b->points, m * sizeof(double));
+	memcpy(weights, b->weights, m * sizeof(double));
+	memcpy(deriv, *b->deriv_matrix, (size_t) m * m * sizeof(double));
+	memcpy(svv_deriv, *b->svv_deriv_matrix, (size_t) m * m * sizeof(double));
+}
+
+/* Interpolation matrix between levels level-1 (fine) and level (coarse):
+ * interp[p][i] = l_p^coarse(xi_i^fine), stored on the fine duplicate basis
+ * (src/precon.c:130-137, src/interpolation.c:115-134). */
+void ssgref_level_interp(int level, double *interp)
+{
+	struct basis *b = (*H_sel)->precon->basis[2 * level - 1];
+	const int nf = b->n;
+	const int nc = (*H_sel)->precon->nmg[level];
+	memcpy(interp, *b->interp_matrix, (size_t) nf * nc * sizeof(double));
+}
+
+static void put_field(double *dst, double ***(*get)(struct element *, int),
+		int level, int which)
+{
+	(void) level;
+	const int m = (*H_sel)->basis->n;
+	const size_t nt = (size_t) m * m * m;
+	for (int e = 0; e < H_nel; ++e)
+		memcpy(dst + e * nt, **get(H_sel[e], which), nt * sizeof(double));
+}
+
+static double ***geom_component(struct element *s, int which)
+{
+	struct geometry *g = s->geom;
+	switch (which) {
+	case 0: return g->geom_mat->x.x;
+	case 1: return g->geom_mat->x.y;
+	case 2: return g->geom_mat->x.z;
+	case 3: return g->geom_mat->y.y;
+	case 4: return g->geom_mat->y.z;
+	case 5: return g->geom_mat->z.z;
+	case 6: return g->jac_det;
+	case 7: return g->grid->x;
+	case 8: return g->grid->y;
+	case 9: return g->grid->z;
+	default: return (double ***) NULL;
+	}
+}
+
+static void switch_level(int level)
+{
+	for (int e = 0; e < H_nel; ++e) {
+		H_sel[e]->precon->level = level;
+		H_sel[e]->basis = H_sel[e]->precon->basis[2 * level];
+		H_sel[e]->geom = H_sel[e]->precon->geom[level];
+	}
+}
+
+/* Geometric factors of a level: comp 0..5 = G11,G12,G13,G22,G23,G33,
+ * 6 = det J, 7..9 = x,y,z of the GLL grid. */
+void ssgref_level_geometry(int level, int comp, double *dst)
+{
+	switch_level(level);
+	put_field(dst, geom_component, level, comp);
+	switch_level(0);
+}
+
+/* Per-level preconditioner arrays, contiguous over elements:
+ * which 0 = Poisson diagonal inverse, 1 = Helmholtz diagonal inverse,
+ * 2 = stiffness-summation scale 1/multiplicity, 3 = Dirichlet mask,
+ * 4 = inverse assembled mass (level 0 only). */
+void ssgref_level_precon(int level, int which, double *dst)
+{
+	struct preconditioner *pc = (*H_sel)->precon;
+	const int m = pc->nmg[level];
+	const size_t len = (size_t) H_nel * m * m * m;
+	const double *src = NULL;
+	switch (which) {
+	case 0: src = **pc->poisson_diag[level]; break;
+	case 1: src = **pc->helmholtz_diag[level]; break;
+	case 2: src = **pc->stiffsum_scale[level]; break;
+	case 3: src = **pc->dirichlet_mask[level]; break;
+	case 4: src = **pc->inverse_mass; break;
+	}
+	memcpy(dst, src, len * sizeof(double));
+}
+
+/* Conversion-grid (dealiasing) factors: comp 0..8 = tinv_jac row-major
+ * [a][b] after the final transpose (src/geometry.c:102-113), 9 = det J. */
+void ssgref_conv_geometry(int comp, double *dst)
+{
+	const int m = H_params->nconv;
+	const size_t nt = (size_t) m * m * m;
+	for (int e = 0; e < H_nel; ++e) {
+		struct geometry *g = H_sel[e]->conv_geom;
+		double ***src = comp < 9 ? *g->tinv_jac->ind[comp / 3][comp % 3]
+				: g->jac_det;
+		memcpy(dst + e * nt, **src, nt * sizeof(double));
+	}
+}
+
+void ssgref_conv_basis(double *points, double *weights, double *interp)
+{
+	const int m = H_conv->n;
+	memcpy(points, H_conv->points, m * sizeof(double));
+	memcpy(weights, H_conv->weights, m * sizeof(double));
+	memcpy(interp, *H_conv->interp_matrix, (size_t) m * H_n * sizeof(double));
+}
+
+/* ---- operators ---- */
+
+void ssgref_global_opeval(int var, const double *p, double *ap)
+{
+	double ****P = from_flat(p);
+	double ****AP = new_4d_array(H_n, H_n, H_n, H_nel);
+	void (*op)() = var == PRESSURE ? (void (*)()) discrete_laplace_operator
+			: (void (*)()) discrete_helmholtz_operator;
+	global_opeval(H_sel, P, AP, var, op);
+	memcpy(ap, ***AP, npts() * sizeof(double));
+	free_4d_array(P);
+	free_4d_array(AP);
+}
+
+/* Element-local operator only (no mask, no DSS). */
+void ssgref_local_opeval(int var, const double *p, double *ap)
+{
+	double ****P = from_flat(p);
+	double ****AP = new_4d_array(H_n, H_n, H_n, H_nel);
+	for (int e = 0; e < H_nel; ++e) {
+		if (var == PRESSURE)
+			discrete_laplace_operator(H_sel[e], P[e], AP[e]);
+		else
+			discrete_helmholtz_operator(H_sel[e], P[e], AP[e]);
+	}
+	memcpy(ap, ***AP, npts() * sizeof(double));
+	free_4d_array(P);
+	free_4d_array(AP);
+}
+
+void ssgref_dss(double *u)
+{
+	double ****U = from_flat(u);
+	direct_stiffness_summation(H_sel, U);
+	memcpy(u, ***U, npts() * sizeof(double));
+	free_4d_array(U);
+}
+
+/* DSS at a coarser level (order of that level, nel * m^3 values). */
+void ssgref_dss_level(int level, double *u)
+{
+	const int m = (*H_sel)->precon->nmg[level];
+	switch_level(level);
+	double ****U = new_4d_array(m, m, m, H_nel);
+	memcpy(***U, u, (size_t) H_nel * m * m * m * sizeof(double));
+	direct_stiffness_summation(H_sel, U);
+	memcpy(u, ***U, (size_t) H_nel * m * m * m * sizeof(double));
+	free_4d_array(U);
+	switch_level(0);
+}
+
+double ssgref_dot(const double *x, const double *y)
+{
+	double ****X = from_flat(x);
+	double ****Y = from_flat(y);
+	double v = ssgref_dot_impl(H_sel, X, Y);
+	free_4d_array(X);
+	free_4d_array(Y);
+	return v;
+}
+
+/* ---- solves (src/solver.c:159-189) ---- */
+
+static void begin_record(double *hist, int cap)
+{
+	H_hist = hist;
+	H_hist_cap = cap;
+	H_hist_len = 0;
+	H_recording = 1;
+}
+
+static int end_record(void)
+{
+	H_recording = 0;
+	return H_hist_len;
+}
+
+/* Poisson: var = PRESSURE, initial guess in u (overwritten by the result). */
+int ssgref_solve_poisson(const double *f, double *u, double eps,
+		double *hist, int cap)
+{
+	double ****F = from_flat(f);
+	for (int e = 0; e < H_nel; ++e)
+		memcpy(**H_sel[e]->p, u + e * (size_t) H_n * H_n * H_n,
+				(size_t) H_n * H_n * H_n * sizeof(double));
+	begin_record(hist, cap);
+	solve_poisson_cg(H_sel, F, PRESSURE, eps);
+	const int it = end_record();
+	for (int e = 0; e < H_nel; ++e)
+		memcpy(u + e * (size_t) H_n * H_n * H_n, **H_sel[e]->p,
+				(size_t) H_n * H_n * H_n * sizeof(double));
+	free_4d_array(F);
+	return it;
+}
+
+/* Helmholtz: var = X/Y/Z_VELOCITY (mask applies on walls). */
+int ssgref_solve_helmholtz(int var, const double *f, double *u, double eps,
+		double *hist, int cap)
+{
+	double ****F = from_flat(f);
+	const size_t nt = (size_t) H_n * H_n * H_n;
+	for (int e = 0; e < H_nel; ++e)
+		memcpy(**variable_array(H_sel[e], var), u + e * nt,
+				nt * sizeof(double));
+	begin_record(hist, cap);
+	solve_helmholtz_cg(H_sel, F, var, eps);
+	const int it = end_record();
+	for (int e = 0; e < H_nel; ++e)
+		memcpy(u + e * nt, **variable_array(H_sel[e], var),
+				nt * sizeof(double));
+	free_4d_array(F);
+	return it;
+}
+
+/* Raw Krylov calls with an iteration cap (returns the final residual). */
+double ssgref_fcg_mg(const double *f, double *u, double eps, int max_iter)
+{
+	double ****F = from_flat(f);
+	double ****U = from_flat(u);
+	double err = flexible_conjugate_gradient(H_sel, F, U, PRESSURE,
+			discrete_laplace_operator, ssgref_mg_hook, eps,
+			max_iter);
+	memcpy(u, ***U, npts() * sizeof(double));
+	free_4d_array(F);
+	free_4d_array(U);
+	return err;
+}
+
+double ssgref_cg_jacobi(int var, const double *f, double *u, double eps,
+		int max_iter)
+{
+	double ****F = from_flat(f);
+	double ****U = from_flat(u);
+	void (*op)() = var == PRESSURE ? (void (*)()) discrete_laplace_operator
+			: (void (*)()) discrete_helmholtz_operator;
+	double err = conjugate_gradient(H_sel, F, U, var, op,
+			jacobi_preconditioner, eps, max_iter);
+	memcpy(u, ***U, npts() * sizeof(double));
+	free_4d_array(F);
+	free_4d_array(U);
+	return err;
+}
+
+/* One application of the p-multigrid preconditioner z = M^-1 r
+ * (src/precon.c:227-236). */
+void ssgref_mg_precon(const double *r, double *z, double eps)
+{
+	double ****R = from_flat(r);
+	double ****Z = new_4d_array(H_n, H_n, H_n, H_nel);
+	ssgref_mg_hook(H_sel, R, Z, PRESSURE, eps,
+			(void (*)()) discrete_laplace_operator);
+	memcpy(z, ***Z, npts() * sizeof(double));
+	free_4d_array(R);
+	free_4d_array(Z);
+}
+
+/* ---- dealiased convection (src/convection.c:31-69) ---- */
+
+static void trivec_in(struct trivec *t, const double *src, int e)
+{
+	const size_t nt = (size_t) H_n * H_n * H_n;
+	for (int c = 0; c < 3; ++c)
+		memcpy(***t->ind[c], src + ((size_t) c * H_nel + e) * nt,
+				nt * sizeof(double));
+}
+
+static void trivec_out(struct trivec *t, double *dst, int e)
+{
+	const size_t nt = (size_t) H_n * H_n * H_n;
+	for (int c = 0; c < 3; ++c)
+		memcpy(dst + ((size_t) c * H_nel + e) * nt, ***t->ind[c],
+				nt * sizeof(double));
+}
+
+/* u, v, out: 3 x nel x n^3 (component-major). */
+void ssgref_convection(const double *u, const double *v, double *out)
+{
+	struct trivec *tu = new_trivec(H_n);
+	struct trivec *tv = new_trivec(H_n);
+	struct trivec *to = new_trivec(H_n);
+	for (int e = 0; e < H_nel; ++e) {
+		trivec_in(tu, u, e);
+		trivec_in(tv, v, e);
+		convection_operator(H_sel[e], tu, tv, to);
+		trivec_out(to, out, e);
+	}
+	free_trivec(tu);
+	free_trivec(tv);
+	free_trivec(to);
+}
+
+/* ---- Navier-Stokes step on the Taylor-Green vortex ---- */
+
+static double tgv_u(double x, double y, double z, double t)
+{
+	(void) t;
+	return sin(x) * cos(y) * cos(z);
+}
+
+static double tgv_v(double x, double y, double z, double t)
+{
+	(void) t;
+	return -cos(x) * sin(y) * cos(z);
+}
+
+static double tgv_w(double x, double y, double z, double t)
+{
+	(void) x;
+	(void) y;
+	(void) z;
+	(void) t;
+	return 0.0;
+}
+
+static double tgv_p(double x, double y, double z)
+{
+	return (cos(2.0 * x) + cos(2.0 * y)) * (cos(2.0 * z) + 2.0) / 16.0;
+}
+
+/* Initial condition as src/poisson.c:245-273 sets it from functions, pressure
+ * in all three history levels, then the reference-domain velocity
+ * (src/main.c:84). */
+void ssgref_init_tgv(void)
+{
+	initialise_from_function(H_sel, tgv_u, tgv_v, tgv_w);
+	const size_t nt = (size_t) H_n * H_n * H_n;
+	for (int e = 0; e < H_nel; ++e) {
+		struct element *s = H_sel[e];
+		const double *x = **s->geom->grid->x;
+		const double *y = **s->geom->grid->y;
+		const double *z = **s->geom->grid->z;
+		for (size_t q = 0; q < nt; ++q) {
+			const double p = tgv_p(x[q], y[q], z[q]);
+			(**s->p)[q] = p;
+			(**s->old->p)[q] = p;
+			(**s->old->old->p)[q] = p;
+		}
+	}
+	compute_reference_domain_velocity(H_sel);
+}
+
+/* One step of src/main.c:101-111 without particles and logging. */
+void ssgref_ns_step(void)
+{
+	set_source_term(H_sel, X_SOURCE, one_func, H_params->gx);
+	set_source_term(H_sel, Y_SOURCE, one_func, H_params->gy);
+	set_source_term(H_sel, Z_SOURCE, one_func, H_params->gz);
+	integrate_navier_stokes(H_sel);
+}
+
+double ssgref_time(void)
+{
+	return H_params->t;
+}
+
+/* which: 0..2 = u,v,w; 3 = p; 4..6 = reference-domain velocity ur. */
+void ssgref_get_field(int which, int hist_level, double *dst)
+{
+	const size_t nt = (size_t) H_n * H_n * H_n;
+	for (int e = 0; e < H_nel; ++e) {
+		struct element *s = H_sel[e];
+		double ***src;
+		struct trivec *u = s->u, *ur = s->ur;
+		double ***p = s->p;
+		if (hist_level >= 1) {
+			u = s->old->u; ur = s->old->ur; p = s->old->p;
+		}
+		if (hist_level >= 2) {
+			u = s->old->old->u; ur = s->old->old->ur;
+			p = s->old->old->p;
+		}
+		if (which < 3)
+			src = *u->ind[which];
+		else if (which == 3)
+			src = p;
+		else
+			src = *ur->ind[which - 4];
+		memcpy(dst + e * nt, **src, nt * sizeof(double));
+	}
+}
+
+void ssgref_set_field(int which, int hist_level, const double *src)
+{
+	const size_t nt = (size_t) H_n * H_n * H_n;
+	for (int e = 0; e < H_nel; ++e) {
+		struct element *s = H_sel[e];
+		double ***dst;
+		struct trivec *u = s->u, *ur = s->ur;
+		double ***p = s->p;
+		if (hist_level >= 1) {
+			u = s->old->u; ur = s->old->ur; p = s->old->p;
+		}
+		if (hist_level >= 2) {
+			u = s->old->old->u; ur = s->old->old->ur;
+			p = s->old->old->p;
+		}
+		if (which < 3)
+			dst = *u->ind[which];
+		else if (which == 3)
+			dst = p;
+		else
+			dst = *ur->ind[which - 4];
+		memcpy(**dst, src + e * nt, nt * sizeof(double));
+	}
+}
+
+/* ---- particles (src/particles.c:182-218) ---- */
+
+/* Flat particle record exchanged with the caller:
+ * x,y,z,u,v,w,t,tau as doubles and el, old_el, status as ints. */
+int ssgref_particles_advance(size_t np, double *state /* np x 8 */,
+		int *ints /* np x 3 */)
+{
+	struct plist pl;
+	pl.n = np;
+	pl.ntot = np;
+	pl.nbuff = np + 1;
+	pl.ntypes = 1;
+	pl.tau = NULL;
+	pl.nproc = 1;
+	pl.mpi_comm = MPI_COMM_WORLD;
+	pl.list = ec_malloc(sizeof(*pl.list) * pl.nbuff);
+	for (size_t i = 0; i < np; ++i) {
+		struct particle *q = &pl.list[i];
+		const double *s = state + 8 * i;
+		q->id = i;
+		q->type = 0;
+		q->x = s[0]; q->y = s[1]; q->z = s[2];
+		q->u = s[3]; q->v = s[4]; q->w = s[5];
+		q->t = s[6]; q->tau = s[7];
+		q->el = ints[3 * i];
+		q->old_el = ints[3 * i + 1];
+		q->proc = 0;
+		q->old_proc = 0;
+		q->status = 0; /* P_NORMAL */
+	}
+	pl.list[np].status = 4; /* P_BUFFER */
+	integrate_particle_equations(&pl, H_sel);
+	/* particles are re-sorted by status (stable qsort is not guaranteed),
+	 * so the id carries each particle back to its slot */
+	for (size_t i = 0; i < np; ++i) {
+		const struct particle *q = &pl.list[i];
+		double *s = state + 8 * q->id;
+		s[0] = q->x; s[1] = q->y; s[2] = q->z;
+		s[3] = q->u; s[4] = q->v; s[5] = q->w;
+		s[6] = q->t; s[7] = q->tau;
+		ints[3 * q->id] = q->el;
+		ints[3 * q->id + 1] = q->old_el;
+		ints[3 * q->id + 2] = q->status;
+	}
+	free(pl.list);
+	return 0;
+}
