@@ -1,0 +1,236 @@
+/*
+ * ssenss_b200 -- B200 (sm_100a) implementation of the SSENSS per-timestep
+ * solve path behind a plain C ABI.
+ *
+ * The host (the SSENSS C driver: src/main.c, src/navier_stokes.c,
+ * src/stokes.c, src/time.c) keeps its own call surface; a thin binding maps
+ * each of the reference functions named below onto one of these entry
+ * points.  All compute runs as hand-written CUDA kernels on one GPU; there is
+ * no CPU fallback: every entry point fails with SSG_ERR_CUDA when no device
+ * is usable.
+ *
+ * Conventions
+ *  - A field is an element-local L-vector u[e][k][j][i], i fastest, nel * n^3
+ *    doubles, n = GLL points per direction (N+1), exactly the contiguous
+ *    block new_4d_array allocates (src/utils.c:64-81).  Vector fields are
+ *    three such blocks, x then y then z.
+ *  - Every field argument may be a host pointer or a device pointer (CUDA
+ *    global memory); the library tells them apart with
+ *    cudaPointerGetAttributes.  Host arguments are copied through pinned
+ *    staging on the context's stream.
+ *  - Every entry point returns an ssg_status; SSG_OK is 0.  Nothing exits
+ *    the process (the reference's fatal_error, src/utils.c:162-174, does).
+ *  - A context is re-entrant with respect to other contexts; calls on one
+ *    context must not overlap.  All work of a context is ordered on its
+ *    CUDA stream; calls return after that work has completed unless stated.
+ *  - var follows src/poisson.h:33: SSG_PRESSURE selects the Laplacian
+ *    (Poisson, nullspace removed, no Dirichlet mask), the velocities select
+ *    the Helmholtz operator with lambda = (11/6) / (dt * visc)
+ *    (src/helmholtz.c:37-38) and the Dirichlet mask.
+ */
+#ifndef SSENSS_B200_H
+#define SSENSS_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+	SSG_OK = 0,
+	SSG_ERR_ARG = 1,        /* invalid argument or unsupported order */
+	SSG_ERR_CUDA = 2,       /* CUDA runtime failure / no device */
+	SSG_ERR_NOMEM = 3,      /* device allocation failed */
+	SSG_ERR_BUDGET = 4,     /* request exceeds the HBM budget */
+	SSG_MAXITER = 5,        /* iteration cap reached before eps */
+	SSG_NONFINITE = 6,      /* NaN/Inf residual or breakdown */
+	SSG_ERR_MESH = 7,       /* inconsistent connectivity */
+	SSG_ERR_STATE = 8,      /* call out of order (no mesh yet, ...) */
+	SSG_ERR_TIMEOUT = 9,    /* deadline or bounded device wait expired */
+	SSG_ERR_CANCELLED = 10  /* request cancelled */
+} ssg_status;
+
+enum {
+	SSG_PRESSURE = 0,
+	SSG_X_VELOCITY = 1,
+	SSG_Y_VELOCITY = 2,
+	SSG_Z_VELOCITY = 3
+};
+
+/* arithmetic of the preconditioner (the outer Krylov loop, its residual and
+ * inner products, DSS accumulation and the coarse solve stay FP64) */
+enum {
+	SSG_PRECISION_FP64 = 0,
+	SSG_PRECISION_MIXED = 1  /* FP32 smoothers, transfers and local
+	                            operator inside the p-multigrid V-cycle */
+};
+
+typedef struct ssg_context ssg_context;
+
+/* Outcome of one solve.  history, when non-NULL, receives sqrt((r.r)_w)
+ * after each outer iteration (the reference's residual check,
+ * src/solver.c:72-73 and 151-152), at most history_cap values. */
+typedef struct {
+	int iterations;          /* outer iterations run */
+	double residual;         /* final sqrt((r.r)_w) */
+	double initial_residual; /* sqrt((r.r)_w) before the first iteration */
+	double solve_ms;         /* device time of the solve (CUDA events) */
+	double *history;
+	int history_cap;
+	int history_len;
+} ssg_solve_info;
+
+/* ---- context ---------------------------------------------------------- */
+
+/* Create a context on CUDA device `device` with its own stream.  Replaces
+ * the process-wide state main.c builds (src/main.c:36-90). */
+ssg_status ssg_create(int device, ssg_context **out);
+/* Same, ordering all work on the caller's stream (a cudaStream_t). */
+ssg_status ssg_create_on_stream(int device, void *cuda_stream,
+		ssg_context **out);
+void ssg_destroy(ssg_context *ctx);
+const char *ssg_status_string(ssg_status s);
+/* Detail of the last failure on this context (never NULL). */
+const char *ssg_last_error(const ssg_context *ctx);
+/* The context's cudaStream_t. */
+void *ssg_stream(const ssg_context *ctx);
+
+/* struct parameters fields used by the solve path (src/structs.h:56-79). */
+ssg_status ssg_set_parameters(ssg_context *ctx, double dt, double visc,
+		double dens);
+ssg_status ssg_set_precision(ssg_context *ctx, int precision);
+/* Use CUDA graphs for the Krylov iterations (default on). */
+ssg_status ssg_set_graphs(ssg_context *ctx, int enable);
+
+/* ---- discretisation set-up ------------------------------------------- */
+
+/* Build the whole discretisation from grid records, as read_grid +
+ * connect_elements + initialise_preconditioners do (src/dataio.c:197-227,
+ * src/init.c:38-50, src/precon.c:196-205): GLL bases of all p-multigrid
+ * levels (src/precon.c:58-83), geometric factors, the dealiasing grid
+ * (m = 3n/2, src/main.c:53), Jacobi diagonals, DSS pairing.
+ *   vertices: nel x {x[8], y[8], z[8]} (trilinear n=2 element, x fastest)
+ *   neigh:    nel x {face[6], edge[12], corner[8]} neighbour element ids,
+ *             negative = wall code (-1 = no-slip / Dirichlet). */
+ssg_status ssg_setup_mesh(ssg_context *ctx, int n, int nel,
+		const double *vertices, const int *neigh);
+
+/* Drop-in set-up from the host's own discretisation (what the reference
+ * already holds in sel[i]->precon after initialise_preconditioners).
+ * Call ssg_setup_connectivity, then ssg_setup_level for every level
+ * 0..nlevels-1 (orders as new_preconditioner gives, src/precon.c:62-69),
+ * then ssg_setup_finish.
+ *   deriv, svv_deriv: n*n, the stored basis->deriv_matrix / svv_deriv_matrix
+ *                     (d[j][i] = D_ij, src/basis.c:160-177)
+ *   weights:          n GLL weights
+ *   geom:             6 x nel x n^3: G11, G12, G13, G22, G23, G33
+ *                     (geom_mat, src/geometry.c:130-135)
+ *   jac_det:          nel x n^3
+ *   interp:           level >= 1: the fine-duplicate basis interp_matrix,
+ *                     n_coarse x n_fine doubles (src/precon.c:130-137);
+ *                     NULL at level 0. */
+ssg_status ssg_setup_connectivity(ssg_context *ctx, int nel,
+		const int *neigh);
+ssg_status ssg_setup_level(ssg_context *ctx, int level, int n,
+		const double *deriv, const double *svv_deriv,
+		const double *weights, const double *geom,
+		const double *jac_det, const double *interp);
+ssg_status ssg_setup_finish(ssg_context *ctx);
+
+/* Dealiasing grid for convection_operator: conv_basis order m and its
+ * factors (tinv_jac 9 x nel x m^3 row-major [a][b] after the transpose of
+ * src/geometry.c:112, jac_det nel x m^3, weights m, deriv m*m stored as
+ * d[j][i], interp = conv_basis->interp_matrix n x m). Drop-in path only;
+ * ssg_setup_mesh builds it itself. */
+ssg_status ssg_setup_dealias(ssg_context *ctx, int m, const double *deriv,
+		const double *weights, const double *tinv_jac,
+		const double *jac_det, const double *interp);
+
+/* Geometry of level 0 for particles: jac (9 x nel x n^3, J[a][b] =
+ * dx_a/dr_b) and tinv_jac (9 x nel x n^3) as the reference stores them.
+ * Drop-in path only; ssg_setup_mesh builds them itself. */
+ssg_status ssg_setup_particle_geometry(ssg_context *ctx, const double *jac,
+		const double *tinv_jac);
+
+ssg_status ssg_mesh_info(const ssg_context *ctx, int *n, int *nel,
+		int *nlevels, int *orders /* >= 8 entries or NULL */);
+/* Read back level data: which 0..5 = G * rho * J (the factors the
+ * operator streams), 6 = rho * J, 7 = Poisson diagonal inverse,
+ * 8 = Helmholtz diagonal inverse, 9 = 1/multiplicity, 10 = Dirichlet mask,
+ * 11 = inverse assembled mass (level 0), 12..14 = GLL grid x, y, z. */
+ssg_status ssg_level_data(ssg_context *ctx, int level, int which,
+		double *dst);
+
+/* ---- operators ---------------------------------------------------------- */
+
+/* ap = DSS(mask(A_e p)) -- global_opeval (src/solver.c:191-198) with
+ * discrete_laplace_operator (var = SSG_PRESSURE, src/poisson.c:34-56) or
+ * discrete_helmholtz_operator (src/helmholtz.c:33-49). */
+ssg_status ssg_global_opeval(ssg_context *ctx, int var, const double *p,
+		double *ap);
+/* Element-local operator only, no mask or DSS (parity tests). */
+ssg_status ssg_local_opeval(ssg_context *ctx, int var, const double *p,
+		double *ap);
+/* In-place DSS -- direct_stiffness_summation (src/global.c:241-257);
+ * integer pairing and addition order as the reference's, so the result
+ * is bitwise equal. */
+ssg_status ssg_direct_stiffness_summation(ssg_context *ctx, double *u);
+/* sum (x * w) * y, w = 1/multiplicity -- global_dot_product
+ * (src/global.c:270-282). */
+ssg_status ssg_global_dot_product(ssg_context *ctx, const double *x,
+		const double *y, double *out);
+/* u *= inverse assembled mass -- global_inverse_mass_matrix_operator
+ * (src/poisson.c:77-87). */
+ssg_status ssg_inverse_mass(ssg_context *ctx, double *u);
+
+/* ---- solves ------------------------------------------------------------- */
+
+/* solve_poisson_cg (src/solver.c:159-173): flexible CG with the
+ * p-multigrid preconditioner to sqrt((r.r)_w) <= eps, at most max_iter
+ * (the reference uses 5000).  u holds the initial guess and receives the
+ * solution.  Returns SSG_MAXITER when the cap is hit (u still written). */
+ssg_status ssg_solve_poisson_cg(ssg_context *ctx, const double *f, double *u,
+		double eps, int max_iter, ssg_solve_info *info);
+/* solve_helmholtz_cg (src/solver.c:175-189): CG with the Jacobi
+ * preconditioner on the Helmholtz operator. */
+ssg_status ssg_solve_helmholtz_cg(ssg_context *ctx, int var, const double *f,
+		double *u, double eps, int max_iter, ssg_solve_info *info);
+/* conjugate_gradient with jacobi_preconditioner on either operator
+ * (src/solver.c:33-81). */
+ssg_status ssg_conjugate_gradient(ssg_context *ctx, int var, const double *f,
+		double *u, double eps, int max_iter, ssg_solve_info *info);
+/* One application z = M^-1 r of multigrid_preconditioner
+ * (src/precon.c:227-236). */
+ssg_status ssg_multigrid_preconditioner(ssg_context *ctx, const double *r,
+		double *z, double eps);
+
+/* ---- convection ----------------------------------------------------------- */
+
+/* Dealiased skew-symmetric convection of the whole mesh --
+ * convection_operator for every element (src/convection.c:31-69).
+ * u (advecting), v (advected), udv: 3 x nel x n^3. */
+ssg_status ssg_convection_operator(ssg_context *ctx, const double *u,
+		const double *v, double *udv);
+
+/* ---- particles -------------------------------------------------------------- */
+
+/* Reference-domain velocity snapshots the particles see (sel->ur and its two
+ * older levels, src/structs.h:96,116): ur is 3 levels (t-2dt, t-dt, t) x 3
+ * components x nel x n^3. */
+ssg_status ssg_set_particle_velocity(ssg_context *ctx, const double *ur);
+/* integrate_particle_equations at one rank (src/particles.c:182-218):
+ * advance every particle to time t, walking across element faces.
+ *   state: np x {x, y, z, u, v, w, t, tau} (reference coordinates and
+ *          reference-domain velocity, particle time, response time)
+ *   ints:  np x {el, old_el, status}; on return status 0 = done,
+ *          5 = needs a reseed (the reference draws a random position).
+ * dt is the flow time step (struct parameters dt). */
+ssg_status ssg_integrate_particle_equations(ssg_context *ctx, size_t np,
+		double *state, int *ints, double t, double dt, int *passes);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,226 @@
+"""B200 (sm_100a) implementation of the SSENSS per-timestep solve path.
+
+Python mirror of the reference's solver call surface (src/solver.h,
+src/global.h, src/convection.h, src/particles.h) over the C ABI in
+include/ssenss_b200.h.  Fields are numpy arrays (host memory; copied through
+the library's staging) or CUDA tensors (device memory, used in place) in the
+reference's L-vector layout u[e][k][j][i].
+
+    ctx = Context(device=0)
+    ctx.setup_mesh(mesh, n=8)          # ssenss_b200.mesh.box_mesh(...)
+    ap = ctx.global_opeval(PRESSURE, p)
+    u, info = ctx.solve_poisson_cg(f, u0, eps=1e-10)
+
+Every compute call runs CUDA kernels; without a usable GPU the context
+cannot be created (SsgError with SSG_ERR_CUDA).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import SolveInfo
+
+PRESSURE, X_VELOCITY, Y_VELOCITY, Z_VELOCITY = 0, 1, 2, 3
+FP64, MIXED = 0, 1
+
+STATUS = {
+    0: "SSG_OK", 1: "SSG_ERR_ARG", 2: "SSG_ERR_CUDA", 3: "SSG_ERR_NOMEM",
+    4: "SSG_ERR_BUDGET", 5: "SSG_MAXITER", 6: "SSG_NONFINITE", 7: "SSG_ERR_MESH",
+    8: "SSG_ERR_STATE", 9: "SSG_ERR_TIMEOUT", 10: "SSG_ERR_CANCELLED",
+}
+
+
+class SsgError(RuntimeError):
+    def __init__(self, status, detail=""):
+        self.status = status
+        super().__init__(f"{STATUS.get(status, status)}: {detail}")
+
+
+def _ptr(a):
+    """Pointer to a numpy array's data or a CUDA tensor's storage."""
+    if isinstance(a, np.ndarray):
+        if not a.flags.c_contiguous:
+            raise ValueError("array must be C-contiguous")
+        return C.c_void_p(a.ctypes.data)
+    if hasattr(a, "data_ptr"):
+        if not a.is_contiguous():
+            raise ValueError("tensor must be contiguous")
+        return C.c_void_p(a.data_ptr())
+    raise TypeError(f"unsupported field type {type(a)}")
+
+
+class Context:
+    """One GPU context (ssg_context): mesh, factors, workspace, stream."""
+
+    def __init__(self, device: int = 0, stream=None):
+        self.lib = _lib.load()
+        h = C.c_void_p()
+        if stream is None:
+            st = self.lib.ssg_create(device, C.byref(h))
+        else:
+            st = self.lib.ssg_create_on_stream(device, C.c_void_p(stream), C.byref(h))
+        if st != 0:
+            raise SsgError(st, "ssg_create")
+        self.h = h
+        self.n = self.nel = self.nlevels = 0
+        self.orders = []
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.ssg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st, what, ok=(0,)):
+        if st not in ok:
+            raise SsgError(st, f"{what}: {self.lib.ssg_last_error(self.h).decode()}")
+        return st
+
+    @property
+    def stream(self) -> int:
+        return self.lib.ssg_stream(self.h) or 0
+
+    # -- set-up ---------------------------------------------------------------
+    def set_parameters(self, dt, visc, dens=1.0):
+        self._check(self.lib.ssg_set_parameters(self.h, dt, visc, dens), "set_parameters")
+
+    def set_precision(self, precision):
+        p = {"fp64": FP64, "mixed": MIXED}.get(precision, precision)
+        self._check(self.lib.ssg_set_precision(self.h, int(p)), "set_precision")
+
+    def set_graphs(self, enable: bool):
+        self._check(self.lib.ssg_set_graphs(self.h, int(bool(enable))), "set_graphs")
+
+    def setup_mesh(self, mesh, n: int):
+        vert = np.ascontiguousarray(mesh.vertices, dtype=np.float64)
+        neigh = np.ascontiguousarray(mesh.neigh, dtype=np.int32)
+        self._check(self.lib.ssg_setup_mesh(
+            self.h, int(n), int(mesh.nel), vert.ctypes.data_as(_lib._dp),
+            neigh.ctypes.data_as(_lib._ip)), "setup_mesh")
+        self._info()
+
+    def _info(self):
+        n, nel, nl = C.c_int(), C.c_int(), C.c_int()
+        orders = (C.c_int * 8)()
+        self._check(self.lib.ssg_mesh_info(self.h, C.byref(n), C.byref(nel), C.byref(nl),
+                                           orders), "mesh_info")
+        self.n, self.nel, self.nlevels = n.value, nel.value, nl.value
+        self.orders = [orders[i] for i in range(nl.value)]
+
+    def level_data(self, level, which):
+        m = self.orders[level]
+        out = np.empty((self.nel, m, m, m))
+        self._check(self.lib.ssg_level_data(self.h, level, which,
+                                            out.ctypes.data_as(_lib._dp)), "level_data")
+        return out
+
+    def shape(self):
+        return (self.nel, self.n, self.n, self.n)
+
+    # -- operators (src/solver.c:191-198, src/global.c) ---------------------
+    def _out_like(self, a, out):
+        if out is not None:
+            return out
+        if isinstance(a, np.ndarray):
+            return np.empty_like(a, dtype=np.float64)
+        return a.new_empty(a.shape)
+
+    def global_opeval(self, var, p, out=None):
+        out = self._out_like(p, out)
+        self._check(self.lib.ssg_global_opeval(self.h, var, _ptr(p), _ptr(out)),
+                    "global_opeval")
+        return out
+
+    def local_opeval(self, var, p, out=None):
+        out = self._out_like(p, out)
+        self._check(self.lib.ssg_local_opeval(self.h, var, _ptr(p), _ptr(out)),
+                    "local_opeval")
+        return out
+
+    def direct_stiffness_summation(self, u):
+        """In place, like the reference."""
+        self._check(self.lib.ssg_direct_stiffness_summation(self.h, _ptr(u)), "dss")
+        return u
+
+    def global_dot_product(self, x, y):
+        r = C.c_double()
+        self._check(self.lib.ssg_global_dot_product(self.h, _ptr(x), _ptr(y), C.byref(r)),
+                    "global_dot_product")
+        return r.value
+
+    def inverse_mass(self, u):
+        self._check(self.lib.ssg_inverse_mass(self.h, _ptr(u)), "inverse_mass")
+        return u
+
+    # -- solves (src/solver.c:33-189) ---------------------------------------
+    def _solve(self, fn, args, what, history, max_iter):
+        info = SolveInfo()
+        hist = None
+        if history:
+            hist = np.zeros(min(max_iter, 8192))
+            info.history = hist.ctypes.data_as(_lib._dp)
+            info.history_cap = len(hist)
+        st = fn(*args, C.byref(info))
+        self._check(st, what, ok=(0, 5))
+        res = {
+            "status": STATUS[st],
+            "iterations": info.iterations,
+            "residual": info.residual,
+            "initial_residual": info.initial_residual,
+            "solve_ms": info.solve_ms,
+        }
+        if hist is not None:
+            res["history"] = hist[:info.history_len].copy()
+        return res
+
+    def solve_poisson_cg(self, f, u, eps=1e-10, max_iter=5000, history=True):
+        """u: initial guess, overwritten with the solution (as the reference
+        overwrites sel->p)."""
+        info = self._solve(self.lib.ssg_solve_poisson_cg,
+                           (self.h, _ptr(f), _ptr(u), eps, max_iter),
+                           "solve_poisson_cg", history, max_iter)
+        return u, info
+
+    def solve_helmholtz_cg(self, var, f, u, eps=1e-10, max_iter=5000, history=True):
+        info = self._solve(self.lib.ssg_solve_helmholtz_cg,
+                           (self.h, var, _ptr(f), _ptr(u), eps, max_iter),
+                           "solve_helmholtz_cg", history, max_iter)
+        return u, info
+
+    def conjugate_gradient(self, var, f, u, eps=1e-10, max_iter=5000, history=True):
+        info = self._solve(self.lib.ssg_conjugate_gradient,
+                           (self.h, var, _ptr(f), _ptr(u), eps, max_iter),
+                           "conjugate_gradient", history, max_iter)
+        return u, info
+
+    def multigrid_preconditioner(self, r, z=None, eps=1e-10):
+        z = self._out_like(r, z)
+        self._check(self.lib.ssg_multigrid_preconditioner(self.h, _ptr(r), _ptr(z), eps),
+                    "multigrid_preconditioner")
+        return z
+
+    # -- convection, particles ------------------------------------------------
+    def convection_operator(self, u, v, out=None):
+        out = self._out_like(u, out)
+        self._check(self.lib.ssg_convection_operator(self.h, _ptr(u), _ptr(v), _ptr(out)),
+                    "convection_operator")
+        return out
+
+    def set_particle_velocity(self, ur):
+        self._check(self.lib.ssg_set_particle_velocity(self.h, _ptr(ur)),
+                    "set_particle_velocity")
+
+    def integrate_particle_equations(self, state, ints, t, dt):
+        passes = C.c_int()
+        self._check(self.lib.ssg_integrate_particle_equations(
+            self.h, state.shape[0], _ptr(state), _ptr(ints), t, dt, C.byref(passes)),
+            "integrate_particle_equations")
+        return state, ints, passes.value

@@ -1,0 +1,88 @@
+"""ctypes binding of libssenss_b200.so (the C ABI of include/ssenss_b200.h).
+
+The shared library is built in place by ssenss_b200/csrc/Makefile.  There is
+no fallback: importing a compute entry point without the library raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libssenss_b200.so")
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+
+
+class SolveInfo(C.Structure):
+    _fields_ = [
+        ("iterations", C.c_int),
+        ("residual", C.c_double),
+        ("initial_residual", C.c_double),
+        ("solve_ms", C.c_double),
+        ("history", _dp),
+        ("history_cap", C.c_int),
+        ("history_len", C.c_int),
+    ]
+
+
+# (name, restype, argtypes) of every symbol include/ssenss_b200.h declares
+SIGNATURES = [
+    ("ssg_create", C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
+    ("ssg_create_on_stream", C.c_int, [C.c_int, C.c_void_p, C.POINTER(C.c_void_p)]),
+    ("ssg_destroy", None, [C.c_void_p]),
+    ("ssg_status_string", C.c_char_p, [C.c_int]),
+    ("ssg_last_error", C.c_char_p, [C.c_void_p]),
+    ("ssg_stream", C.c_void_p, [C.c_void_p]),
+    ("ssg_set_parameters", C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double]),
+    ("ssg_set_precision", C.c_int, [C.c_void_p, C.c_int]),
+    ("ssg_set_graphs", C.c_int, [C.c_void_p, C.c_int]),
+    ("ssg_setup_mesh", C.c_int, [C.c_void_p, C.c_int, C.c_int, _dp, _ip]),
+    ("ssg_setup_connectivity", C.c_int, [C.c_void_p, C.c_int, _ip]),
+    ("ssg_setup_level", C.c_int, [C.c_void_p, C.c_int, C.c_int, _dp, _dp, _dp, _dp,
+                                  _dp, _dp]),
+    ("ssg_setup_finish", C.c_int, [C.c_void_p]),
+    ("ssg_setup_dealias", C.c_int, [C.c_void_p, C.c_int, _dp, _dp, _dp, _dp, _dp]),
+    ("ssg_setup_particle_geometry", C.c_int, [C.c_void_p, _dp, _dp]),
+    ("ssg_mesh_info", C.c_int, [C.c_void_p, _ip, _ip, _ip, _ip]),
+    ("ssg_level_data", C.c_int, [C.c_void_p, C.c_int, C.c_int, _dp]),
+    ("ssg_global_opeval", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    ("ssg_local_opeval", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    ("ssg_direct_stiffness_summation", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("ssg_global_dot_product", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, _dp]),
+    ("ssg_inverse_mass", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("ssg_solve_poisson_cg", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
+                                       C.c_int, C.POINTER(SolveInfo)]),
+    ("ssg_solve_helmholtz_cg", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+                                         C.c_double, C.c_int, C.POINTER(SolveInfo)]),
+    ("ssg_conjugate_gradient", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+                                         C.c_double, C.c_int, C.POINTER(SolveInfo)]),
+    ("ssg_multigrid_preconditioner", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p,
+                                               C.c_double]),
+    ("ssg_convection_operator", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p,
+                                          C.c_void_p]),
+    ("ssg_set_particle_velocity", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("ssg_integrate_particle_equations", C.c_int, [C.c_void_p, C.c_size_t, C.c_void_p,
+                                                   C.c_void_p, C.c_double, C.c_double,
+                                                   _ip]),
+]
+
+_LIB = None
+
+
+def load():
+    """Load libssenss_b200.so; raises when it has not been built."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with `make -C ssenss_b200/csrc` "
+                "(there is no CPU fallback)")
+        lib = C.CDLL(LIB_PATH)
+        for name, res, args in SIGNATURES:
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _LIB = lib
+    return _LIB

@@ -1,0 +1,681 @@
+// C-ABI entry points: context, set-up/upload, operators.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "ssg_internal.h"
+#include "ssg_kernels.h"
+
+namespace ssg {
+
+ssg_status fail(ssg_context* c, ssg_status s, const std::string& msg) {
+  if (c) c->err = msg;
+  return s;
+}
+
+ssg_status cuda_fail(ssg_context* c, cudaError_t e, const char* what) {
+  std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+  if (e == cudaErrorMemoryAllocation) return fail(c, SSG_ERR_NOMEM, m);
+  return fail(c, SSG_ERR_CUDA, m);
+}
+
+bool is_device_ptr(const void* p) {
+  if (!p) return false;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+template <typename T>
+static ssg_status dalloc(ssg_context* c, T** p, size_t count) {
+  *p = nullptr;
+  if (count == 0) return SSG_OK;
+  SSG_CUDA(c, cudaMalloc((void**)p, count * sizeof(T)));
+  return SSG_OK;
+}
+
+template <typename T>
+static ssg_status dupload(ssg_context* c, T** p, const T* src, size_t count) {
+  SSG_TRY(dalloc(c, p, count));
+  if (count) SSG_CUDA(c, cudaMemcpy(*p, src, count * sizeof(T), cudaMemcpyHostToDevice));
+  return SSG_OK;
+}
+
+static ssg_status upload_f32(ssg_context* c, float** p, const double* src, size_t count) {
+  std::vector<float> t(src, src + count);
+  return dupload(c, p, t.data(), count);
+}
+
+static void dfree(void* p) {
+  if (p) cudaFree(p);
+}
+
+static void free_level(ssg::DevLevel& d) {
+  dfree(d.gf); dfree(d.bj); dfree(d.kdiag); dfree(d.dinv_p); dfree(d.dinv_h);
+  dfree(d.scale); dfree(d.mask); dfree(d.D); dfree(d.S); dfree(d.Ar); dfree(d.Ap);
+  dfree(d.gf32); dfree(d.dinv_p32); dfree(d.scale32); dfree(d.D32); dfree(d.Ar32);
+  dfree(d.Ap32);
+  d = ssg::DevLevel();
+}
+
+static void free_mesh(ssg_context* c) {
+  if (c->ws) {
+    free_workspace(c->ws);
+    c->ws = nullptr;
+  }
+  for (auto& l : c->lev) free_level(l);
+  dfree(c->d_pairs); c->d_pairs = nullptr;
+  dfree(c->inv_mass); c->inv_mass = nullptr;
+  dfree(c->conv_tinv); dfree(c->conv_bj); dfree(c->conv_D); dfree(c->conv_J);
+  c->conv_tinv = c->conv_bj = c->conv_D = c->conv_J = nullptr;
+  dfree(c->p_jac); dfree(c->p_tinv); dfree(c->p_ur); dfree(c->p_x);
+  c->p_jac = c->p_tinv = c->p_ur = c->p_x = nullptr;
+  dfree(c->d_part); c->d_part = nullptr;
+  for (auto& s : c->d_stage) { dfree(s); s = nullptr; }
+  c->stage_cap = 0;
+  c->ready = false;
+}
+
+// rho_ijk = (w_i w_j) w_k (gll_weights_array, src/basis.c:179-188)
+static std::vector<double> rho3(const std::vector<double>& w) {
+  const int n = (int)w.size();
+  std::vector<double> r((size_t)n * n * n);
+  for (int k = 0; k < n; ++k)
+    for (int j = 0; j < n; ++j)
+      for (int i = 0; i < n; ++i) r[(k * n + j) * n + i] = (w[i] * w[j]) * w[k];
+  return r;
+}
+
+// Upload every level (and the optional dealiasing / particle data) from
+// c->host; the diagonals, multiplicities and masks are derived here as
+// initialise_preconditioners does (src/precon.c:336-413).
+static ssg_status upload_all(ssg_context* c) {
+  ssg::HostMesh& H = c->host;
+  const int nel = H.nel;
+  c->n = H.n;
+  c->nel = nel;
+  c->nlev = H.nlev;
+  c->has_walls = false;
+  for (int e = 0; e < nel; ++e)
+    if (H.bc[e]) c->has_walls = true;
+  SSG_TRY(dupload(c, &c->d_pairs, H.pairs.data(), H.pairs.size()));
+  for (int l = 0; l < H.nlev; ++l) {
+    const ssg::HostLevel& h = H.lev[l];
+    ssg::DevLevel& d = c->lev[l];
+    c->orders[l] = h.n;
+    d.n = h.n;
+    d.nt = h.nt;
+    d.npts = h.nt * nel;
+    const size_t np = d.npts;
+    const std::vector<double> rho = rho3(h.w);
+    std::vector<double> bj(np), gf(6 * np);
+    for (int e = 0; e < nel; ++e)
+      for (size_t q = 0; q < h.nt; ++q) bj[e * h.nt + q] = rho[q] * h.det[e * h.nt + q];
+    for (int a = 0; a < 6; ++a)
+      for (size_t q = 0; q < np; ++q) gf[a * np + q] = h.g[a][q] * bj[q];
+    std::vector<double> kd(np);
+    stiffness_diagonal(h, nel, kd.data());
+    std::vector<double> dp(kd);
+    host_dss(H, h.n, dp.data());
+    for (auto& v : dp) v = 1.0 / v;
+    std::vector<double> sc(np, 1.0);
+    host_dss(H, h.n, sc.data());
+    for (auto& v : sc) v = 1.0 / v;
+    double nun = 0.0;
+    for (double v : sc) nun += v;
+    d.nunique = nun;
+    SSG_TRY(dupload(c, &d.gf, gf.data(), gf.size()));
+    SSG_TRY(dupload(c, &d.bj, bj.data(), np));
+    SSG_TRY(dupload(c, &d.kdiag, kd.data(), np));
+    SSG_TRY(dupload(c, &d.dinv_p, dp.data(), np));
+    SSG_TRY(dalloc(c, &d.dinv_h, np));
+    d.lambda_h = -1.0;
+    SSG_TRY(dupload(c, &d.scale, sc.data(), np));
+    if (c->has_walls) {
+      std::vector<double> mk(np, 1.0);
+      const int n = h.n;
+      for (int e = 0; e < nel; ++e)
+        for (int f = 0; f < 6; ++f)
+          if (H.bc[e] & (1 << f))
+            for (int k = 0; k < n; ++k)
+              for (int j = 0; j < n; ++j)
+                for (int i = 0; i < n; ++i) {
+                  const bool on = (f == 0 && i == 0) || (f == 1 && i == n - 1) ||
+                                  (f == 2 && j == 0) || (f == 3 && j == n - 1) ||
+                                  (f == 4 && k == 0) || (f == 5 && k == n - 1);
+                  if (on) mk[e * h.nt + (k * n + j) * n + i] = 0.0;
+                }
+      SSG_TRY(dupload(c, &d.mask, mk.data(), np));
+    }
+    SSG_TRY(dupload(c, &d.D, h.D.data(), h.D.size()));
+    SSG_TRY(dupload(c, &d.S, h.S.data(), h.S.size()));
+    SSG_TRY(upload_f32(c, &d.gf32, gf.data(), gf.size()));
+    SSG_TRY(upload_f32(c, &d.dinv_p32, dp.data(), np));
+    SSG_TRY(upload_f32(c, &d.scale32, sc.data(), np));
+    SSG_TRY(upload_f32(c, &d.D32, h.D.data(), h.D.size()));
+    if (l >= 1) {
+      const int nf = H.lev[l - 1].n, nc = h.n;
+      std::vector<double> Ar((size_t)nc * nf);
+      for (int i = 0; i < nf; ++i)
+        for (int p = 0; p < nc; ++p) Ar[p * nf + i] = h.jf[i * nc + p];
+      SSG_TRY(dupload(c, &d.Ar, Ar.data(), Ar.size()));
+      SSG_TRY(dupload(c, &d.Ap, h.jf.data(), h.jf.size()));
+      SSG_TRY(upload_f32(c, &d.Ar32, Ar.data(), Ar.size()));
+      SSG_TRY(upload_f32(c, &d.Ap32, h.jf.data(), h.jf.size()));
+    }
+    if (l == 0) {
+      std::vector<double> im(bj);
+      host_dss(H, h.n, im.data());
+      for (auto& v : im) v = 1.0 / v;
+      SSG_TRY(dupload(c, &c->inv_mass, im.data(), np));
+    }
+  }
+  const size_t np0 = c->lev[0].npts;
+  if (H.has_conv) {
+    const ssg::HostLevel& m = H.conv;
+    c->m = m.n;
+    const size_t mp = m.nt * nel;
+    std::vector<double> tv(9 * mp), cb(mp);
+    for (int a = 0; a < 9; ++a) std::copy(m.tinv[a].begin(), m.tinv[a].end(), tv.begin() + a * mp);
+    const std::vector<double> rho = rho3(m.w);
+    for (int e = 0; e < nel; ++e)
+      for (size_t q = 0; q < m.nt; ++q) cb[e * m.nt + q] = rho[q] * m.det[e * m.nt + q];
+    SSG_TRY(dupload(c, &c->conv_tinv, tv.data(), tv.size()));
+    SSG_TRY(dupload(c, &c->conv_bj, cb.data(), cb.size()));
+    SSG_TRY(dupload(c, &c->conv_D, m.D.data(), m.D.size()));
+    SSG_TRY(dupload(c, &c->conv_J, H.jconv.data(), H.jconv.size()));
+  }
+  if (H.has_particle_geom) {
+    const ssg::HostLevel& h = H.lev[0];
+    std::vector<double> ja(9 * np0), ti(9 * np0);
+    for (int a = 0; a < 9; ++a) {
+      std::copy(h.jac[a].begin(), h.jac[a].end(), ja.begin() + a * np0);
+      std::copy(h.tinv[a].begin(), h.tinv[a].end(), ti.begin() + a * np0);
+    }
+    SSG_TRY(dupload(c, &c->p_jac, ja.data(), ja.size()));
+    SSG_TRY(dupload(c, &c->p_tinv, ti.data(), ti.size()));
+    SSG_TRY(dalloc(c, &c->p_ur, 9 * np0));
+    SSG_CUDA(c, cudaMemset(c->p_ur, 0, 9 * np0 * sizeof(double)));
+  }
+  SSG_TRY(dupload(c, &c->p_x, H.lev[0].x.data(), H.lev[0].x.size()));
+  // reduction partials: enough for 10 dot products over the largest grid
+  const size_t vb = (size_t)vec_blocks(np0);
+  const size_t db = (size_t)dss_grid(c->n, nel);
+  c->part_cap = std::max(16 * vb, 2 * db) + 64;
+  SSG_TRY(dalloc(c, &c->d_part, c->part_cap));
+  // staging for host arguments: up to three vector fields
+  c->stage_cap = 3 * std::max(np0, (size_t)nel * c->m * c->m * c->m);
+  for (auto& s : c->d_stage) SSG_TRY(dalloc(c, &s, c->stage_cap));
+  SSG_CUDA(c, cudaDeviceSynchronize());
+  c->ready = true;
+  return SSG_OK;
+}
+
+// Helmholtz Jacobi inverse for lambda = (11/6)/(dt visc) at level 0
+// (initialise_diagonal_precon, src/precon.c:336-359): DSS(kdiag +
+// (lambda rho) J), reciprocal.
+ssg_status helmholtz_diag_update(ssg_context* c) {
+  const double lam = (11.0 / 6.0) * 1.0 / (c->dt * c->visc);
+  ssg::DevLevel& d = c->lev[0];
+  if (d.lambda_h == lam) return SSG_OK;
+  const ssg::HostLevel& h = c->host.lev[0];
+  const size_t np = d.npts;
+  std::vector<double> kd(np), hd(np);
+  stiffness_diagonal(h, c->nel, kd.data());
+  const std::vector<double> rho = rho3(h.w);
+  for (int e = 0; e < c->nel; ++e)
+    for (size_t q = 0; q < h.nt; ++q)
+      hd[e * h.nt + q] = kd[e * h.nt + q] + lam * rho[q] * h.det[e * h.nt + q];
+  host_dss(c->host, h.n, hd.data());
+  for (auto& v : hd) v = 1.0 / v;
+  SSG_CUDA(c, cudaMemcpy(d.dinv_h, hd.data(), np * sizeof(double), cudaMemcpyHostToDevice));
+  d.lambda_h = lam;
+  return SSG_OK;
+}
+
+// ---- staging ------------------------------------------------------------
+
+// Device view of a caller field: the pointer itself when it is device
+// memory, else a staging slot filled from the host.
+static ssg_status stage_in(ssg_context* c, int slot, const double* p, size_t count,
+                           const double** out) {
+  if (!p) return fail(c, SSG_ERR_ARG, "null field pointer");
+  if (is_device_ptr(p)) {
+    *out = p;
+    return SSG_OK;
+  }
+  if (count > c->stage_cap) return fail(c, SSG_ERR_ARG, "field larger than staging");
+  SSG_CUDA(c, cudaMemcpyAsync(c->d_stage[slot], p, count * sizeof(double),
+                              cudaMemcpyHostToDevice, c->stream));
+  *out = c->d_stage[slot];
+  return SSG_OK;
+}
+
+static ssg_status stage_out(ssg_context* c, int slot, double* p, size_t count,
+                            double** out) {
+  if (!p) return fail(c, SSG_ERR_ARG, "null field pointer");
+  if (is_device_ptr(p)) {
+    *out = p;
+    return SSG_OK;
+  }
+  if (count > c->stage_cap) return fail(c, SSG_ERR_ARG, "field larger than staging");
+  *out = c->d_stage[slot];
+  return SSG_OK;
+}
+
+static ssg_status stage_back(ssg_context* c, double* host, const double* dev, size_t count) {
+  if (host != dev)
+    SSG_CUDA(c, cudaMemcpyAsync(host, dev, count * sizeof(double), cudaMemcpyDeviceToHost,
+                                c->stream));
+  SSG_CUDA(c, cudaStreamSynchronize(c->stream));
+  return SSG_OK;
+}
+
+static ssg_status need_ready(ssg_context* c) {
+  if (!c) return SSG_ERR_ARG;
+  if (!c->ready) return fail(c, SSG_ERR_STATE, "no mesh set up on this context");
+  SSG_CUDA(c, cudaSetDevice(c->device));
+  return SSG_OK;
+}
+
+}  // namespace ssg
+
+using namespace ssg;
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+static ssg_status create_impl(int device, void* stream, ssg_context** out) {
+  if (!out) return SSG_ERR_ARG;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return SSG_ERR_CUDA;
+  }
+  if (device < 0 || device >= ndev) return SSG_ERR_ARG;
+  ssg_context* c = new ssg_context();
+  c->device = device;
+  if (cudaSetDevice(device) != cudaSuccess) {
+    delete c;
+    return SSG_ERR_CUDA;
+  }
+  if (stream) {
+    c->stream = (cudaStream_t)stream;
+    c->own_stream = false;
+  } else {
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      delete c;
+      return SSG_ERR_CUDA;
+    }
+    c->own_stream = true;
+  }
+  if (cudaMalloc(&c->d_sums, 16 * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&c->d_sc, FR_COUNT * F_SIZE * sizeof(double)) != cudaSuccess ||
+      cudaMallocHost(&c->h_pin, 64 * sizeof(double)) != cudaSuccess ||
+      cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
+    ssg_destroy(c);
+    return SSG_ERR_CUDA;
+  }
+  cudaMemset(c->d_sc, 0, FR_COUNT * F_SIZE * sizeof(double));
+  *out = c;
+  return SSG_OK;
+}
+
+ssg_status ssg_create(int device, ssg_context** out) { return create_impl(device, nullptr, out); }
+
+ssg_status ssg_create_on_stream(int device, void* cuda_stream, ssg_context** out) {
+  return create_impl(device, cuda_stream, out);
+}
+
+void ssg_destroy(ssg_context* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  free_mesh(c);
+  dfree(c->d_sums);
+  dfree(c->d_sc);
+  if (c->h_pin) cudaFreeHost(c->h_pin);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+const char* ssg_status_string(ssg_status s) {
+  switch (s) {
+    case SSG_OK: return "ok";
+    case SSG_ERR_ARG: return "invalid argument";
+    case SSG_ERR_CUDA: return "CUDA failure or no device";
+    case SSG_ERR_NOMEM: return "device allocation failed";
+    case SSG_ERR_BUDGET: return "request exceeds the HBM budget";
+    case SSG_MAXITER: return "iteration cap reached";
+    case SSG_NONFINITE: return "non-finite residual";
+    case SSG_ERR_MESH: return "inconsistent mesh connectivity";
+    case SSG_ERR_STATE: return "call out of order";
+    case SSG_ERR_TIMEOUT: return "deadline expired";
+    case SSG_ERR_CANCELLED: return "cancelled";
+  }
+  return "unknown status";
+}
+
+const char* ssg_last_error(const ssg_context* c) { return c ? c->err.c_str() : ""; }
+
+void* ssg_stream(const ssg_context* c) { return c ? (void*)c->stream : nullptr; }
+
+ssg_status ssg_set_parameters(ssg_context* c, double dt, double visc, double dens) {
+  if (!c) return SSG_ERR_ARG;
+  if (!(dt > 0.0) || !(visc > 0.0)) return fail(c, SSG_ERR_ARG, "dt and visc must be > 0");
+  c->dt = dt;
+  c->visc = visc;
+  c->dens = dens;
+  return SSG_OK;
+}
+
+ssg_status ssg_set_precision(ssg_context* c, int precision) {
+  if (!c) return SSG_ERR_ARG;
+  if (precision != SSG_PRECISION_FP64 && precision != SSG_PRECISION_MIXED)
+    return fail(c, SSG_ERR_ARG, "unknown precision");
+  c->precision = precision;
+  return SSG_OK;
+}
+
+ssg_status ssg_set_graphs(ssg_context* c, int enable) {
+  if (!c) return SSG_ERR_ARG;
+  c->graphs = enable != 0;
+  return SSG_OK;
+}
+
+ssg_status ssg_setup_mesh(ssg_context* c, int n, int nel, const double* vertices,
+                          const int* neigh) {
+  if (!c || !vertices || !neigh) return SSG_ERR_ARG;
+  SSG_CUDA(c, cudaSetDevice(c->device));
+  free_mesh(c);
+  c->host = ssg::HostMesh();
+  ssg_status st = build_mesh(c->host, n, nel, vertices, neigh, c->err);
+  if (st != SSG_OK) return st;
+  return upload_all(c);
+}
+
+ssg_status ssg_setup_connectivity(ssg_context* c, int nel, const int* neigh) {
+  if (!c || !neigh || nel <= 0) return SSG_ERR_ARG;
+  SSG_CUDA(c, cudaSetDevice(c->device));
+  free_mesh(c);
+  c->host = ssg::HostMesh();
+  c->host.nel = nel;
+  c->host.neigh.assign(neigh, neigh + 26 * (size_t)nel);
+  return build_pairs(c->host, c->err);
+}
+
+ssg_status ssg_setup_level(ssg_context* c, int level, int n, const double* deriv,
+                           const double* svv_deriv, const double* weights,
+                           const double* geom, const double* jac_det,
+                           const double* interp) {
+  if (!c || !deriv || !weights || !geom || !jac_det) return SSG_ERR_ARG;
+  ssg::HostMesh& H = c->host;
+  if (H.nel <= 0) return fail(c, SSG_ERR_STATE, "ssg_setup_connectivity first");
+  if (level < 0 || level >= SSG_MAXLEV || n < 2 || n > 12)
+    return fail(c, SSG_ERR_ARG, "bad level or order");
+  if (level > 0 && (!interp || H.lev[level - 1].n == 0))
+    return fail(c, SSG_ERR_STATE, "levels must be set in order, with interp");
+  ssg::HostLevel& L = H.lev[level];
+  L = ssg::HostLevel();
+  L.n = n;
+  L.nt = (size_t)n * n * n;
+  const size_t np = L.nt * H.nel;
+  L.x.resize(n);
+  L.w.assign(weights, weights + n);
+  gll_basis(n, L.x.data(), std::vector<double>(n).data());
+  L.D.resize(n * n);
+  L.S.resize(n * n);
+  // stored d[j][i] = D_ij  ->  D[i*n+j]
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j) {
+      L.D[i * n + j] = deriv[j * n + i];
+      L.S[i * n + j] = (svv_deriv ? svv_deriv : deriv)[j * n + i];
+    }
+  for (int a = 0; a < 6; ++a) L.g[a].assign(geom + a * np, geom + (a + 1) * np);
+  L.det.assign(jac_det, jac_det + np);
+  if (level > 0) {
+    const int nf = H.lev[level - 1].n;
+    L.jf.resize((size_t)nf * n);
+    // stored interp[p][i] (p coarse, i fine) -> jf[i*n+p]
+    for (int p = 0; p < n; ++p)
+      for (int i = 0; i < nf; ++i) L.jf[i * n + p] = interp[p * nf + i];
+  }
+  if (level == 0) H.n = n;
+  if (level + 1 > H.nlev) H.nlev = level + 1;
+  return SSG_OK;
+}
+
+ssg_status ssg_setup_finish(ssg_context* c) {
+  if (!c) return SSG_ERR_ARG;
+  if (c->host.nlev < 1) return fail(c, SSG_ERR_STATE, "no levels set");
+  if (c->host.lev[c->host.nlev - 1].n != 2)
+    return fail(c, SSG_ERR_STATE, "the coarsest level must have order 2");
+  SSG_CUDA(c, cudaSetDevice(c->device));
+  return upload_all(c);
+}
+
+ssg_status ssg_mesh_info(const ssg_context* c, int* n, int* nel, int* nlevels, int* orders) {
+  if (!c) return SSG_ERR_ARG;
+  if (n) *n = c->n;
+  if (nel) *nel = c->nel;
+  if (nlevels) *nlevels = c->nlev;
+  if (orders)
+    for (int l = 0; l < c->nlev; ++l) orders[l] = c->orders[l];
+  return c->ready ? SSG_OK : SSG_ERR_STATE;
+}
+
+ssg_status ssg_level_data(ssg_context* c, int level, int which, double* dst) {
+  SSG_TRY(need_ready(c));
+  if (level < 0 || level >= c->nlev || !dst) return fail(c, SSG_ERR_ARG, "bad level");
+  const ssg::DevLevel& d = c->lev[level];
+  const size_t np = d.npts;
+  const double* src = nullptr;
+  std::vector<double> tmp;
+  if (which >= 0 && which < 6)
+    src = d.gf + which * np;
+  else if (which == 6)
+    src = d.bj;
+  else if (which == 7)
+    src = d.dinv_p;
+  else if (which == 8) {
+    SSG_TRY(helmholtz_diag_update(c));
+    src = d.dinv_h;
+  } else if (which == 9)
+    src = d.scale;
+  else if (which == 10) {
+    if (d.mask)
+      src = d.mask;
+    else {
+      std::fill(dst, dst + np, 1.0);
+      return SSG_OK;
+    }
+  } else if (which == 11 && level == 0)
+    src = c->inv_mass;
+  else if (which >= 12 && which <= 14) {
+    const auto& g = c->host.lev[level].grid[which - 12];
+    if (g.size() != np) return fail(c, SSG_ERR_STATE, "grid not available");
+    std::copy(g.begin(), g.end(), dst);
+    return SSG_OK;
+  } else
+    return fail(c, SSG_ERR_ARG, "bad selector");
+  SSG_CUDA(c, cudaMemcpy(dst, src, np * sizeof(double), cudaMemcpyDeviceToHost));
+  return SSG_OK;
+}
+
+ssg_status ssg_global_opeval(ssg_context* c, int var, const double* p, double* ap) {
+  SSG_TRY(need_ready(c));
+  const size_t np = c->lev[0].npts;
+  const double* dp;
+  double* dap;
+  SSG_TRY(stage_in(c, 0, p, np, &dp));
+  SSG_TRY(stage_out(c, 1, ap, np, &dap));
+  SSG_TRY(op_apply(c, 0, var, false, dp, dap, true));
+  return stage_back(c, ap, dap, np);
+}
+
+ssg_status ssg_local_opeval(ssg_context* c, int var, const double* p, double* ap) {
+  SSG_TRY(need_ready(c));
+  const size_t np = c->lev[0].npts;
+  const double* dp;
+  double* dap;
+  SSG_TRY(stage_in(c, 0, p, np, &dp));
+  SSG_TRY(stage_out(c, 1, ap, np, &dap));
+  SSG_TRY(op_apply(c, 0, var, false, dp, dap, false));
+  return stage_back(c, ap, dap, np);
+}
+
+ssg_status ssg_direct_stiffness_summation(ssg_context* c, double* u) {
+  SSG_TRY(need_ready(c));
+  const size_t np = c->lev[0].npts;
+  const double* du;
+  SSG_TRY(stage_in(c, 0, u, np, &du));
+  // DSS is out of place: gather from a copy
+  double* tmp = c->d_stage[1];
+  SSG_CUDA(c, cudaMemcpyAsync(tmp, du, np * sizeof(double), cudaMemcpyDeviceToDevice,
+                              c->stream));
+  double* dout = (double*)du;
+  if (!is_device_ptr(u)) dout = c->d_stage[0];
+  SSG_CUDA(c, run_dss(c->stream, DSS_PLAIN, false, c->n, c->nel, tmp, dout, c->d_pairs,
+                      nullptr, nullptr, nullptr, nullptr));
+  return stage_back(c, u, dout, np);
+}
+
+ssg_status ssg_global_dot_product(ssg_context* c, const double* x, const double* y,
+                                  double* out) {
+  SSG_TRY(need_ready(c));
+  if (!out) return SSG_ERR_ARG;
+  const size_t np = c->lev[0].npts;
+  const double *dx, *dy;
+  SSG_TRY(stage_in(c, 0, x, np, &dx));
+  SSG_TRY(stage_in(c, 1, y, np, &dy));
+  const int nb = vec_blocks(np);
+  PtrList pl;
+  pl.p[0] = dy;
+  SSG_CUDA(c, run_dots(c->stream, false, np, dx, pl, 1, c->lev[0].scale, c->d_part, nb));
+  ScalarOp op;
+  SSG_CUDA(c, run_reduce(c->stream, c->d_part, nb, 1, c->d_sums, op));
+  SSG_CUDA(c, cudaMemcpyAsync(c->h_pin, c->d_sums, sizeof(double), cudaMemcpyDeviceToHost,
+                              c->stream));
+  SSG_CUDA(c, cudaStreamSynchronize(c->stream));
+  *out = c->h_pin[0];
+  return SSG_OK;
+}
+
+ssg_status ssg_inverse_mass(ssg_context* c, double* u) {
+  SSG_TRY(need_ready(c));
+  const size_t np = c->lev[0].npts;
+  const double* du;
+  SSG_TRY(stage_in(c, 0, u, np, &du));
+  SSG_CUDA(c, run_mul(c->stream, false, np, (void*)du, c->inv_mass));
+  return stage_back(c, u, du, np);
+}
+
+static void timing_begin(ssg_context* c) { cudaEventRecord(c->ev0, c->stream); }
+
+static double timing_end(ssg_context* c) {
+  cudaEventRecord(c->ev1, c->stream);
+  cudaEventSynchronize(c->ev1);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+  return ms;
+}
+
+ssg_status ssg_solve_poisson_cg(ssg_context* c, const double* f, double* u, double eps,
+                                int max_iter, ssg_solve_info* info) {
+  SSG_TRY(need_ready(c));
+  if (max_iter <= 0) return fail(c, SSG_ERR_ARG, "max_iter must be positive");
+  const size_t np = c->lev[0].npts;
+  const double* df;
+  const double* du0;
+  SSG_TRY(stage_in(c, 0, f, np, &df));
+  SSG_TRY(stage_in(c, 1, u, np, &du0));
+  SSG_TRY(ensure_workspace(c));
+  timing_begin(c);
+  ssg_status st = fcg_solve(c, df, (double*)du0, eps, max_iter, info);
+  const double ms = timing_end(c);
+  if (info) info->solve_ms = ms;
+  if (st != SSG_OK && st != SSG_MAXITER) return st;
+  ssg_status st2 = stage_back(c, u, du0, np);
+  return st2 != SSG_OK ? st2 : st;
+}
+
+ssg_status ssg_conjugate_gradient(ssg_context* c, int var, const double* f, double* u,
+                                  double eps, int max_iter, ssg_solve_info* info) {
+  SSG_TRY(need_ready(c));
+  if (max_iter <= 0) return fail(c, SSG_ERR_ARG, "max_iter must be positive");
+  if (var < SSG_PRESSURE || var > SSG_Z_VELOCITY) return fail(c, SSG_ERR_ARG, "bad var");
+  const size_t np = c->lev[0].npts;
+  const double* df;
+  const double* du0;
+  SSG_TRY(stage_in(c, 0, f, np, &df));
+  SSG_TRY(stage_in(c, 1, u, np, &du0));
+  SSG_TRY(ensure_workspace(c));
+  // the reference masks f in place; work on a copy so the caller's f stays
+  double* fc = c->d_stage[2];
+  SSG_CUDA(c, cudaMemcpyAsync(fc, df, np * sizeof(double), cudaMemcpyDeviceToDevice,
+                              c->stream));
+  if (var != SSG_PRESSURE) SSG_TRY(helmholtz_diag_update(c));
+  double* hist_d = nullptr;
+  int cap = 0;
+  if (info && info->history && info->history_cap > 0) {
+    cap = std::min(info->history_cap, max_iter);
+    SSG_CUDA(c, cudaMalloc(&hist_d, cap * sizeof(double)));
+  }
+  timing_begin(c);
+  ssg_status st = cg_solve(c, 0, var, false, fc, (double*)du0, eps, max_iter, FR_HELM,
+                           hist_d, cap, true);
+  const double ms = timing_end(c);
+  if (info) {
+    double* fr = c->d_sc + FR_HELM * F_SIZE;
+    double h[F_SIZE];
+    cudaMemcpy(h, fr, sizeof(h), cudaMemcpyDeviceToHost);
+    info->iterations = (int)h[F_ITER];
+    info->residual = h[F_ERR];
+    info->initial_residual = h[F_ERR0];
+    info->solve_ms = ms;
+    info->history_len = std::min((int)h[F_ITER], cap);
+    if (hist_d) {
+      cudaMemcpy(info->history, hist_d, info->history_len * sizeof(double),
+                 cudaMemcpyDeviceToHost);
+    }
+  }
+  if (hist_d) cudaFree(hist_d);
+  if (st != SSG_OK && st != SSG_MAXITER) return st;
+  ssg_status st2 = stage_back(c, u, du0, np);
+  return st2 != SSG_OK ? st2 : st;
+}
+
+ssg_status ssg_solve_helmholtz_cg(ssg_context* c, int var, const double* f, double* u,
+                                  double eps, int max_iter, ssg_solve_info* info) {
+  if (var < SSG_X_VELOCITY || var > SSG_Z_VELOCITY)
+    return ssg::fail(c, SSG_ERR_ARG, "Helmholtz var must be a velocity component");
+  return ssg_conjugate_gradient(c, var, f, u, eps, max_iter, info);
+}
+
+ssg_status ssg_multigrid_preconditioner(ssg_context* c, const double* r, double* z,
+                                        double eps) {
+  SSG_TRY(need_ready(c));
+  const size_t np = c->lev[0].npts;
+  const double* dr;
+  double* dz;
+  SSG_TRY(stage_in(c, 0, r, np, &dr));
+  SSG_TRY(stage_out(c, 1, z, np, &dz));
+  SSG_TRY(ensure_workspace(c));
+  SSG_TRY(mg_apply(c, dr, dz, eps));
+  return stage_back(c, z, dz, np);
+}
+
+}  // extern "C"

@@ -1,0 +1,783 @@
+// Element operators, direct stiffness summation, transfers and fused vector
+// kernels of the SSENSS solve path, for sm_100a.
+//
+// Local operator (discrete_laplace_operator / discrete_helmholtz_operator,
+// src/poisson.c:34-56, src/helmholtz.c:33-49):
+//   A_e u = D^T (rho J G . D u)  [+ lambda rho J u]
+// streamed once per point: u, the six G_ab * rho * J factors, (rho J), out.
+// Each element block and the 1-D derivative matrices sit in shared memory;
+// thread (i, j) keeps its k-column of u and of the t-flux in registers.
+//
+// DSS (direct_stiffness_summation, src/global.c:241-257): each local node
+// adds its neighbours' pre-sum copies in the reference's order (faces w, e,
+// s, n, b, t; edges sw..tn; corners 0..7) from the pairing built on the host
+// (src/init.c:68-130), accumulating in FP64: the result is bitwise equal to
+// the reference's for FP64 data.
+#include <cuda_runtime.h>
+#include <cstdio>
+
+#include "kernels.cuh"
+#include "ssg_internal.h"
+#include "ssg_kernels.h"
+
+namespace ssg {
+namespace dev {
+
+// ---------------------------------------------------------------------------
+// local operator
+// ---------------------------------------------------------------------------
+template <int N, typename T, bool HELM>
+__global__ void __launch_bounds__(256, 2) k_ax(int nel, const T* __restrict__ u,
+                                             T* __restrict__ au,
+                                             const T* __restrict__ gf,
+                                             size_t npts,
+                                             const T* __restrict__ bj,
+                                             const T* __restrict__ Dg,
+                                             const T* __restrict__ Sg,
+                                             T lambda) {
+  constexpr int NN = N * N, NNN = N * N * N, P = N + 1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* sD = reinterpret_cast<T*>(smem_raw);
+  T* sS = sD + N * P;
+  T* su = sS + N * P + threadIdx.z * 3 * NNN;
+  T* sw0 = su + NNN;
+  T* sw1 = sw0 + NNN;
+  const int i = threadIdx.x, j = threadIdx.y;
+  const int tid = i + N * (j + N * threadIdx.z);
+  const int nthr = NN * blockDim.z;
+  for (int q = tid; q < NN; q += nthr) {
+    sD[(q / N) * P + q % N] = Dg[q];
+    sS[(q / N) * P + q % N] = HELM ? Sg[q] : Dg[q];
+  }
+  const int e = blockIdx.x * blockDim.z + threadIdx.z;
+  const bool active = e < nel;
+  const size_t off = (size_t)(active ? e : 0) * NNN + j * N + i;
+  T ru[N], rw2[N];
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+    ru[k] = active ? u[off + k * NN] : T(0);
+    su[k * NN + j * N + i] = ru[k];
+  }
+  __syncthreads();
+  const T* Dx = sS;   // r-derivative: S for Helmholtz, D otherwise
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+    T ur = 0, us = 0, ut = 0;
+#pragma unroll
+    for (int m = 0; m < N; ++m) {
+      ur += Dx[i * P + m] * su[k * NN + j * N + m];
+      us += sD[j * P + m] * su[k * NN + m * N + i];
+      ut += sD[k * P + m] * ru[m];
+    }
+    const size_t o = off + (size_t)k * NN;
+    T g0 = 0, g1 = 0, g2 = 0, g3 = 0, g4 = 0, g5 = 0;
+    if (active) {
+      g0 = __ldg(gf + o);
+      g1 = __ldg(gf + npts + o);
+      g2 = __ldg(gf + 2 * npts + o);
+      g3 = __ldg(gf + 3 * npts + o);
+      g4 = __ldg(gf + 4 * npts + o);
+      g5 = __ldg(gf + 5 * npts + o);
+    }
+    sw0[k * NN + j * N + i] = g0 * ur + g1 * us + g2 * ut;
+    sw1[k * NN + j * N + i] = g1 * ur + g3 * us + g4 * ut;
+    rw2[k] = g2 * ur + g4 * us + g5 * ut;
+  }
+  __syncthreads();
+  // transposed derivatives: r with D, s and t with S (= D for Poisson)
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+    T acc = 0, acs = 0, act = 0;
+#pragma unroll
+    for (int m = 0; m < N; ++m) {
+      acc += sD[m * P + i] * sw0[k * NN + j * N + m];
+      acs += sS[m * P + j] * sw1[k * NN + m * N + i];
+      act += sS[m * P + k] * rw2[m];
+    }
+    T out = (acc + acs) + act;
+    if (HELM && active) out += lambda * (__ldg(bj + off + (size_t)k * NN) * ru[k]);
+    if (active) au[off + (size_t)k * NN] = out;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// DSS gather with fused epilogues
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ double ld_masked(const T* in, const double* mask,
+                                            size_t idx) {
+  double v = (double)in[idx];
+  if (mask) v = v * mask[idx];
+  return v;
+}
+
+// out = DSS(mask .* in) then, by MODE:
+//   DSS_PLAIN: store
+//   DSS_DOT:   store; partial sum (y w) out                       [1]
+//   DSS_DOT2:  store; partial sums (y w) out, (y w) y2            [2]
+//   DSS_RESID: out = y - DSS; partial sum w out                   [1]
+//   DSS_AVG:   out = DSS * w (direct_stiffness_averaging)
+// w = 1 / multiplicity = 1 / (1 + number of contributions).
+template <typename T, int MODE>
+__global__ void __launch_bounds__(256) k_dss(int n, int nel, int epb,
+                                             const T* __restrict__ in,
+                                             T* __restrict__ out,
+                                             const int2* __restrict__ pairs,
+                                             const double* __restrict__ mask,
+                                             const T* __restrict__ y,
+                                             const T* __restrict__ y2,
+                                             double* __restrict__ part) {
+  __shared__ int2 sp[64 * 26];
+  __shared__ double sred[2 * 32];
+  const int nt = n * n * n;
+  const int e0 = blockIdx.x * epb;
+  const int ne = min(epb, nel - e0);
+  for (int q = threadIdx.x; q < ne * 26; q += blockDim.x)
+    sp[q] = pairs[(size_t)e0 * 26 + q];
+  __syncthreads();
+  double s0 = 0.0, s1 = 0.0;
+  const int m = n - 1;
+  for (int q = threadIdx.x; q < ne * nt; q += blockDim.x) {
+    const int z = q / nt, loc = q - z * nt;
+    const int i = loc % n, j = (loc / n) % n, k = loc / (n * n);
+    const size_t gi = (size_t)(e0 + z) * nt + loc;
+    const int2* pr = sp + z * 26;
+    double acc = ld_masked(in, mask, gi);
+    int cnt = 0;
+#define SSG_ADD(PR, NODE)                                              \
+  {                                                                     \
+    const int2 p_ = (PR);                                               \
+    if (p_.x >= 0) {                                                    \
+      acc += ld_masked(in, mask, (size_t)p_.x * nt + (NODE));           \
+      ++cnt;                                                            \
+    }                                                                   \
+  }
+    if (i == 0) SSG_ADD(pr[0], face_node(n, pr[0].y, k, j));
+    if (i == m) SSG_ADD(pr[1], face_node(n, pr[1].y, k, j));
+    if (j == 0) SSG_ADD(pr[2], face_node(n, pr[2].y, k, i));
+    if (j == m) SSG_ADD(pr[3], face_node(n, pr[3].y, k, i));
+    if (k == 0) SSG_ADD(pr[4], face_node(n, pr[4].y, j, i));
+    if (k == m) SSG_ADD(pr[5], face_node(n, pr[5].y, j, i));
+    if (i == 0 && j == 0) SSG_ADD(pr[6], edge_node(n, pr[6].y, k));
+    if (i == m && j == 0) SSG_ADD(pr[7], edge_node(n, pr[7].y, k));
+    if (i == 0 && j == m) SSG_ADD(pr[8], edge_node(n, pr[8].y, k));
+    if (i == m && j == m) SSG_ADD(pr[9], edge_node(n, pr[9].y, k));
+    if (k == 0 && i == 0) SSG_ADD(pr[10], edge_node(n, pr[10].y, j));
+    if (k == 0 && i == m) SSG_ADD(pr[11], edge_node(n, pr[11].y, j));
+    if (k == m && i == 0) SSG_ADD(pr[12], edge_node(n, pr[12].y, j));
+    if (k == m && i == m) SSG_ADD(pr[13], edge_node(n, pr[13].y, j));
+    if (k == 0 && j == 0) SSG_ADD(pr[14], edge_node(n, pr[14].y, i));
+    if (k == 0 && j == m) SSG_ADD(pr[15], edge_node(n, pr[15].y, i));
+    if (k == m && j == 0) SSG_ADD(pr[16], edge_node(n, pr[16].y, i));
+    if (k == m && j == m) SSG_ADD(pr[17], edge_node(n, pr[17].y, i));
+    if ((i == 0 || i == m) && (j == 0 || j == m) && (k == 0 || k == m)) {
+      const int c = (i == m) | ((j == m) << 1) | ((k == m) << 2);
+      SSG_ADD(pr[18 + c], corner_node(n, pr[18 + c].y));
+    }
+#undef SSG_ADD
+    const double w = 1.0 / (1.0 + (double)cnt);
+    if (MODE == DSS_RESID) {
+      const double r = (double)y[gi] + -acc;
+      out[gi] = (T)r;
+      s0 += (double)(T)r * w;
+    } else if (MODE == DSS_AVG) {
+      out[gi] = (T)(acc * w);
+    } else {
+      out[gi] = (T)acc;
+      if (MODE == DSS_DOT || MODE == DSS_DOT2) {
+        const double yw = (double)y[gi] * w;
+        s0 += yw * (double)(T)acc;
+        if (MODE == DSS_DOT2) s1 += yw * (double)y2[gi];
+      }
+    }
+  }
+  if (MODE == DSS_DOT || MODE == DSS_RESID || MODE == DSS_DOT2) {
+    double v[2] = {s0, s1};
+    block_reduce<2>(v, sred);
+    if (threadIdx.x == 0) {
+      part[blockIdx.x] = v[0];
+      if (MODE == DSS_DOT2) part[gridDim.x + blockIdx.x] = v[1];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// tensor-product transfer between orders, stages in x, y, z order
+// (interpolate_to_grid / integrate_to_grid, src/interpolation.c:136-176):
+// out (no^3) [+]= (A x A x A) in (ni^3), A[o*ni + q]
+// ---------------------------------------------------------------------------
+template <typename T, bool ADD>
+__global__ void __launch_bounds__(256) k_tensor3(int nel, int ni, int no,
+                                                 const T* __restrict__ A,
+                                                 const T* __restrict__ in,
+                                                 T* __restrict__ out) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* sA = reinterpret_cast<T*>(smem_raw);
+  T* sin = sA + no * ni;
+  T* t1 = sin + ni * ni * ni;
+  T* t2 = t1 + no * ni * ni;
+  const int e = blockIdx.x;
+  const int nti = ni * ni * ni, nto = no * no * no;
+  for (int q = threadIdx.x; q < no * ni; q += blockDim.x) sA[q] = A[q];
+  for (int q = threadIdx.x; q < nti; q += blockDim.x) sin[q] = in[(size_t)e * nti + q];
+  __syncthreads();
+  for (int q = threadIdx.x; q < no * ni * ni; q += blockDim.x) {
+    const int o = q % no, kj = q / no;
+    T s = 0;
+    for (int r = 0; r < ni; ++r) s += sA[o * ni + r] * sin[kj * ni + r];
+    t1[q] = s;
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < no * no * ni; q += blockDim.x) {
+    const int o1 = q % no, o2 = (q / no) % no, k = q / (no * no);
+    T s = 0;
+    for (int r = 0; r < ni; ++r) s += sA[o2 * ni + r] * t1[(k * ni + r) * no + o1];
+    t2[q] = s;
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < nto; q += blockDim.x) {
+    const int o12 = q % (no * no), o3 = q / (no * no);
+    T s = 0;
+    for (int r = 0; r < ni; ++r) s += sA[o3 * ni + r] * t2[r * no * no + o12];
+    if (ADD)
+      out[(size_t)e * nto + q] += s;
+    else
+      out[(size_t)e * nto + q] = s;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// fused vector kernels (grid-stride, 256 threads, one partial per block)
+// ---------------------------------------------------------------------------
+
+// CG step after ap is known (src/solver.c:66-71):
+//   x += alpha p; r -= alpha ap; z = dinv .* r
+// partials: (r w).z, (r w).r, w.z, w.r
+template <typename T>
+__global__ void __launch_bounds__(256) k_cg_update(size_t npts,
+                                                   const double* __restrict__ alpha_p,
+                                                   T* __restrict__ x,
+                                                   const T* __restrict__ p,
+                                                   T* __restrict__ r,
+                                                   const T* __restrict__ ap,
+                                                   const T* __restrict__ dinv,
+                                                   const T* __restrict__ scale,
+                                                   T* __restrict__ z,
+                                                   double* __restrict__ part) {
+  __shared__ double sred[4 * 32];
+  const T alpha = (T)*alpha_p;
+  double v[4] = {0.0, 0.0, 0.0, 0.0};
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < npts;
+       q += (size_t)gridDim.x * blockDim.x) {
+    x[q] = x[q] + alpha * p[q];
+    const T rq = r[q] + -alpha * ap[q];
+    r[q] = rq;
+    const T zq = rq * dinv[q];
+    z[q] = zq;
+    const double w = (double)scale[q];
+    const double rw = (double)rq * w;
+    v[0] += rw * (double)zq;
+    v[1] += rw * (double)rq;
+    v[2] += w * (double)zq;
+    v[3] += rw;
+  }
+  block_reduce<4>(v, sred);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) part[k * gridDim.x + blockIdx.x] = v[k];
+  }
+}
+
+// p = (beta p + (z - c)) .* mask; first iteration p = z - c
+// (src/solver.c:59-60,75-77 with subtract_nullspace folded in)
+template <typename T>
+__global__ void __launch_bounds__(256) k_p_update(size_t npts, const double* __restrict__ beta_p,
+                                                  const double* __restrict__ c_p,
+                                                  T* __restrict__ p,
+                                                  const T* __restrict__ z,
+                                                  const double* __restrict__ mask,
+                                                  int first) {
+  const T beta = first ? T(0) : (T)*beta_p;
+  const T c = c_p ? (T)*c_p : T(0);
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < npts;
+       q += (size_t)gridDim.x * blockDim.x) {
+    const T zc = z[q] - c;
+    T v = first ? zc : beta * p[q] + zc;
+    if (mask) v = v * (T)mask[q];
+    p[q] = v;
+  }
+}
+
+// z = dinv .* r; partial w.z (Jacobi preconditioner, src/precon.c:311-324)
+template <typename T>
+__global__ void __launch_bounds__(256) k_jacobi(size_t npts, const T* __restrict__ r,
+                                                const T* __restrict__ dinv,
+                                                const T* __restrict__ scale,
+                                                T* __restrict__ z,
+                                                double* __restrict__ part) {
+  __shared__ double sred[32];
+  double v[1] = {0.0};
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < npts;
+       q += (size_t)gridDim.x * blockDim.x) {
+    const T zq = r[q] * dinv[q];
+    z[q] = zq;
+    v[0] += (double)scale[q] * (double)zq;
+  }
+  block_reduce<1>(v, sred);
+  if (threadIdx.x == 0) part[blockIdx.x] = v[0];
+}
+
+// partial sums of (x w) y_k, k < K (up to 10 vectors)
+template <typename T, int K>
+__global__ void __launch_bounds__(256) k_dots(size_t npts, const T* __restrict__ x,
+                                              PtrList ys, const T* __restrict__ scale,
+                                              double* __restrict__ part) {
+  __shared__ double sred[K * 32];
+  double v[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) v[k] = 0.0;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < npts;
+       q += (size_t)gridDim.x * blockDim.x) {
+    const double xw = (double)x[q] * (double)scale[q];
+#pragma unroll
+    for (int k = 0; k < K; ++k) v[k] += xw * (double)((const T*)ys.p[k])[q];
+  }
+  block_reduce<K>(v, sred);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) part[k * gridDim.x + blockIdx.x] = v[k];
+  }
+}
+
+// partial sums of w x (the nullspace component, src/solver.c:200-213)
+template <typename T>
+__global__ void __launch_bounds__(256) k_wsum(size_t npts, const T* __restrict__ x,
+                                              const T* __restrict__ scale,
+                                              double* __restrict__ part) {
+  __shared__ double sred[32];
+  double v[1] = {0.0};
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < npts;
+       q += (size_t)gridDim.x * blockDim.x)
+    v[0] += (double)x[q] * (double)scale[q];
+  block_reduce<1>(v, sred);
+  if (threadIdx.x == 0) part[blockIdx.x] = v[0];
+}
+
+// x += a_k y_k for k < K with a_k = sign * coef[k] read on the device;
+// optional subtraction of a device constant c first: x = (x - c) + ...
+template <typename T>
+__global__ void __launch_bounds__(256) k_combine(size_t npts, T* __restrict__ x,
+                                                 PtrList ys,
+                                                 const double* __restrict__ coef,
+                                                 int K, double sign,
+                                                 const double* __restrict__ c_p,
+                                                 const double* __restrict__ mask) {
+  const double c = c_p ? *c_p : 0.0;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < npts;
+       q += (size_t)gridDim.x * blockDim.x) {
+    T v = x[q];
+    if (c_p) v = v - (T)c;
+    for (int k = 0; k < K; ++k) v = v + (T)(sign * coef[k]) * ((const T*)ys.p[k])[q];
+    if (mask) v = v * (T)mask[q];
+    x[q] = v;
+  }
+}
+
+// u += alpha p; r -= alpha ap; partial (r w).r   (src/solver.c:148-152)
+__global__ void __launch_bounds__(256) k_fcg_update(size_t npts,
+                                                    const double* __restrict__ alpha_p,
+                                                    double* __restrict__ u,
+                                                    const double* __restrict__ p,
+                                                    double* __restrict__ r,
+                                                    const double* __restrict__ ap,
+                                                    const double* __restrict__ scale,
+                                                    double* __restrict__ part) {
+  __shared__ double sred[32];
+  const double alpha = *alpha_p;
+  double v[1] = {0.0};
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < npts;
+       q += (size_t)gridDim.x * blockDim.x) {
+    u[q] = u[q] + alpha * p[q];
+    const double rq = r[q] + -alpha * ap[q];
+    r[q] = rq;
+    v[0] += (rq * scale[q]) * rq;
+  }
+  block_reduce<1>(v, sred);
+  if (threadIdx.x == 0) part[blockIdx.x] = v[0];
+}
+
+// y = x + a (a device constant, negated when neg)
+template <typename T>
+__global__ void __launch_bounds__(256) k_add_const(size_t npts, T* __restrict__ x,
+                                                   const double* __restrict__ a_p,
+                                                   int neg) {
+  const T a = (T)(neg ? -*a_p : *a_p);
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < npts;
+       q += (size_t)gridDim.x * blockDim.x)
+    x[q] = x[q] + a;
+}
+
+template <typename TI, typename TO>
+__global__ void __launch_bounds__(256) k_convert(size_t npts, const TI* __restrict__ in,
+                                                 TO* __restrict__ out) {
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < npts;
+       q += (size_t)gridDim.x * blockDim.x)
+    out[q] = (TO)in[q];
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_mul(size_t npts, T* __restrict__ x,
+                                             const double* __restrict__ y) {
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < npts;
+       q += (size_t)gridDim.x * blockDim.x)
+    x[q] = x[q] * (T)y[q];
+}
+
+// ---------------------------------------------------------------------------
+// deterministic reduction of block partials + solver scalar algebra
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_reduce(const double* __restrict__ part,
+                                                int nblk, int nq,
+                                                double* __restrict__ sums,
+                                                ScalarOp op) {
+  __shared__ double sred[32];
+  for (int q = 0; q < nq; ++q) {
+    double v[1] = {0.0};
+    for (int b = threadIdx.x; b < nblk; b += blockDim.x) v[0] += part[(size_t)q * nblk + b];
+    block_reduce<1>(v, sred);
+    if (threadIdx.x == 0) sums[q] = v[0];
+  }
+  if (threadIdx.x != 0) return;
+  double* f = op.frame;
+  switch (op.code) {
+    case OP_NONE:
+      break;
+    case OP_CG_INIT_C:   // c = (w.z)/nunique (pressure)
+      f[F_C] = op.pressure ? sums[0] / op.nunique : 0.0;
+      break;
+    case OP_CG_INIT_RDZ:  // rdz = (r w).p, |r|_w ; reset counters
+      f[F_RDZ] = sums[0];
+      f[F_ERR0] = sqrt(sums[1]);
+      f[F_ITER] = 0.0;
+      f[F_DONE] = 0.0;
+      f[F_ERR] = sqrt(sums[1]);
+      break;
+    case OP_CG_ALPHA:     // alpha = rdz / (p w).ap
+      f[F_PAP] = sums[0];
+      f[F_ALPHA] = f[F_RDZ] / sums[0];
+      break;
+    case OP_CG_BETA: {    // sums: (r w).z, (r w).r, w.z, w.r
+      const double c = op.pressure ? sums[2] / op.nunique : 0.0;
+      const double rdz = sums[0] - c * sums[3];
+      f[F_C] = c;
+      f[F_BETA] = rdz / f[F_RDZ];
+      f[F_RDZ] = rdz;
+      const double err = sqrt(sums[1]);
+      f[F_ERR] = err;
+      f[F_ITER] += 1.0;
+      const bool go = (err > op.eps) && (f[F_ITER] < (double)op.max_iter);
+      f[F_DONE] = go ? 0.0 : 1.0;
+      if (op.hist && (int)f[F_ITER] <= op.hist_cap) op.hist[(int)f[F_ITER] - 1] = err;
+      break;
+    }
+    case OP_NULL_C:       // c = (w.x)/nunique into frame slot
+      f[F_C] = sums[0] / op.nunique;
+      break;
+    case OP_FCG_BETA:     // beta_k = sums[k] / pap[k]
+      for (int k = 0; k < op.m; ++k) f[F_FBETA + k] = sums[k] / f[F_FPAP + op.pap_idx[k]];
+      break;
+    case OP_FCG_ALPHA:    // pap0 and alpha = (p0 w).r / pap0
+      f[F_FPAP + op.pap_idx[0]] = sums[0];
+      f[F_ALPHA] = sums[1] / sums[0];
+      break;
+    case OP_FCG_ERR: {
+      const double err = sqrt(sums[0]);
+      f[F_ERR] = err;
+      f[F_ITER] += 1.0;
+      const bool go = (err > op.eps) && (f[F_ITER] < (double)op.max_iter);
+      f[F_DONE] = go ? 0.0 : 1.0;
+      if (op.hist && (int)f[F_ITER] <= op.hist_cap) op.hist[(int)f[F_ITER] - 1] = err;
+      break;
+    }
+    case OP_ERR0:
+      f[F_ERR0] = sqrt(sums[0]);
+      f[F_ITER] = 0.0;
+      f[F_DONE] = 0.0;
+      f[F_ERR] = sqrt(sums[0]);
+      break;
+  }
+}
+
+}  // namespace dev
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+using namespace dev;
+
+int vec_blocks(size_t npts) {
+  size_t b = (npts + 255) / 256;
+  const size_t cap = 148 * 8;
+  return (int)(b < cap ? (b ? b : 1) : cap);
+}
+
+int ax_epb(int n, bool fp32) {
+  // elements per block: at least 64 threads, at most 1024, <= 96 KB smem
+  const size_t bytes = fp32 ? 4 : 8;
+  int epb = 1;
+  while (epb * 2 * n * n <= 256 && (size_t)(epb * 2) * 3 * n * n * n * bytes <= 96 * 1024)
+    epb *= 2;
+  return epb;
+}
+
+template <int N, typename T, bool HELM>
+static cudaError_t launch_ax_t(cudaStream_t s, int nel, int epb, const T* u, T* au,
+                               const T* gf, size_t npts, const T* bj, const T* D,
+                               const T* S, T lambda) {
+  const size_t smem = (2 * N * (N + 1) + (size_t)epb * 3 * N * N * N) * sizeof(T);
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(k_ax<N, T, HELM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         200 * 1024);
+    attr_set = true;
+  }
+  dim3 blk(N, N, epb);
+  dim3 grd((nel + epb - 1) / epb);
+  k_ax<N, T, HELM><<<grd, blk, smem, s>>>(nel, u, au, gf, npts, bj, D, S, lambda);
+  return cudaGetLastError();
+}
+
+template <typename T, bool HELM>
+static cudaError_t ax_dispatch(int n, cudaStream_t s, int nel, int epb, const T* u, T* au,
+                               const T* gf, size_t npts, const T* bj, const T* D,
+                               const T* S, T lambda) {
+  switch (n) {
+#define SSG_AXN(NV) \
+  case NV: return launch_ax_t<NV, T, HELM>(s, nel, epb, u, au, gf, npts, bj, D, S, lambda);
+    SSG_AXN(2) SSG_AXN(3) SSG_AXN(4) SSG_AXN(5) SSG_AXN(6) SSG_AXN(7)
+    SSG_AXN(8) SSG_AXN(9) SSG_AXN(10) SSG_AXN(11) SSG_AXN(12)
+#undef SSG_AXN
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t run_ax(cudaStream_t s, int n, int nel, int epb, bool helm, bool fp32,
+                   const void* in, void* out, const void* gf, size_t npts,
+                   const double* bj, const void* D, const void* S, double lambda) {
+  if (epb <= 0) epb = ax_epb(n, fp32);
+  if (fp32) {
+    return ax_dispatch<float, false>(n, s, nel, epb, (const float*)in, (float*)out,
+                                     (const float*)gf, npts, nullptr, (const float*)D,
+                                     (const float*)D, 0.0f);
+  }
+  if (helm)
+    return ax_dispatch<double, true>(n, s, nel, epb, (const double*)in, (double*)out,
+                                     (const double*)gf, npts, bj, (const double*)D,
+                                     (const double*)S, lambda);
+  return ax_dispatch<double, false>(n, s, nel, epb, (const double*)in, (double*)out,
+                                    (const double*)gf, npts, nullptr, (const double*)D,
+                                    (const double*)D, 0.0);
+}
+
+int dss_epb(int n) {
+  const int nt = n * n * n;
+  int epb = 1;
+  while (epb * 2 <= 64 && epb * 2 * nt <= 1024) epb *= 2;
+  return epb;
+}
+
+int dss_grid(int n, int nel) {
+  const int epb = dss_epb(n);
+  return (nel + epb - 1) / epb;
+}
+
+template <typename T>
+static cudaError_t run_dss_t(cudaStream_t s, int mode, int n, int nel, const T* in, T* out,
+                             const int* pairs, const double* mask, const T* y,
+                             const T* y2, double* part) {
+  const int epb = dss_epb(n);
+  const int grd = (nel + epb - 1) / epb;
+  const int2* pr = reinterpret_cast<const int2*>(pairs);
+  switch (mode) {
+    case DSS_PLAIN:
+      k_dss<T, DSS_PLAIN><<<grd, 256, 0, s>>>(n, nel, epb, in, out, pr, mask, y, y2, part);
+      break;
+    case DSS_DOT:
+      k_dss<T, DSS_DOT><<<grd, 256, 0, s>>>(n, nel, epb, in, out, pr, mask, y, y2, part);
+      break;
+    case DSS_DOT2:
+      k_dss<T, DSS_DOT2><<<grd, 256, 0, s>>>(n, nel, epb, in, out, pr, mask, y, y2, part);
+      break;
+    case DSS_RESID:
+      k_dss<T, DSS_RESID><<<grd, 256, 0, s>>>(n, nel, epb, in, out, pr, mask, y, y2, part);
+      break;
+    case DSS_AVG:
+      k_dss<T, DSS_AVG><<<grd, 256, 0, s>>>(n, nel, epb, in, out, pr, mask, y, y2, part);
+      break;
+    default:
+      return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t run_dss(cudaStream_t s, int mode, bool fp32, int n, int nel, const void* in,
+                    void* out, const int* pairs, const double* mask, const void* y,
+                    const void* y2, double* part) {
+  if (fp32)
+    return run_dss_t<float>(s, mode, n, nel, (const float*)in, (float*)out, pairs, mask,
+                            (const float*)y, (const float*)y2, part);
+  return run_dss_t<double>(s, mode, n, nel, (const double*)in, (double*)out, pairs, mask,
+                           (const double*)y, (const double*)y2, part);
+}
+
+cudaError_t run_tensor3(cudaStream_t s, bool fp32, bool add, int nel, int ni, int no,
+                        const void* A, const void* in, void* out) {
+  const size_t bytes = fp32 ? 4 : 8;
+  const size_t smem = ((size_t)no * ni + (size_t)ni * ni * ni + (size_t)no * ni * ni +
+                       (size_t)no * no * ni) * bytes;
+  if (fp32) {
+    if (add)
+      k_tensor3<float, true><<<nel, 256, smem, s>>>(nel, ni, no, (const float*)A,
+                                                    (const float*)in, (float*)out);
+    else
+      k_tensor3<float, false><<<nel, 256, smem, s>>>(nel, ni, no, (const float*)A,
+                                                     (const float*)in, (float*)out);
+  } else {
+    if (add)
+      k_tensor3<double, true><<<nel, 256, smem, s>>>(nel, ni, no, (const double*)A,
+                                                     (const double*)in, (double*)out);
+    else
+      k_tensor3<double, false><<<nel, 256, smem, s>>>(nel, ni, no, (const double*)A,
+                                                      (const double*)in, (double*)out);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t run_cg_update(cudaStream_t s, bool fp32, size_t npts, const double* alpha,
+                          void* x, const void* p, void* r, const void* ap,
+                          const void* dinv, const void* scale, void* z, double* part,
+                          int nblk) {
+  if (fp32)
+    k_cg_update<float><<<nblk, 256, 0, s>>>(npts, alpha, (float*)x, (const float*)p,
+                                            (float*)r, (const float*)ap,
+                                            (const float*)dinv, (const float*)scale,
+                                            (float*)z, part);
+  else
+    k_cg_update<double><<<nblk, 256, 0, s>>>(npts, alpha, (double*)x, (const double*)p,
+                                             (double*)r, (const double*)ap,
+                                             (const double*)dinv, (const double*)scale,
+                                             (double*)z, part);
+  return cudaGetLastError();
+}
+
+cudaError_t run_p_update(cudaStream_t s, bool fp32, size_t npts, const double* beta,
+                         const double* c, void* p, const void* z, const double* mask,
+                         int first) {
+  const int nblk = vec_blocks(npts);
+  if (fp32)
+    k_p_update<float><<<nblk, 256, 0, s>>>(npts, beta, c, (float*)p, (const float*)z, mask,
+                                           first);
+  else
+    k_p_update<double><<<nblk, 256, 0, s>>>(npts, beta, c, (double*)p, (const double*)z,
+                                            mask, first);
+  return cudaGetLastError();
+}
+
+cudaError_t run_jacobi(cudaStream_t s, bool fp32, size_t npts, const void* r,
+                       const void* dinv, const void* scale, void* z, double* part,
+                       int nblk) {
+  if (fp32)
+    k_jacobi<float><<<nblk, 256, 0, s>>>(npts, (const float*)r, (const float*)dinv,
+                                         (const float*)scale, (float*)z, part);
+  else
+    k_jacobi<double><<<nblk, 256, 0, s>>>(npts, (const double*)r, (const double*)dinv,
+                                          (const double*)scale, (double*)z, part);
+  return cudaGetLastError();
+}
+
+template <typename T>
+static cudaError_t run_dots_t(cudaStream_t s, size_t npts, const T* x, const PtrList& ys,
+                              int K, const T* scale, double* part, int nblk) {
+  switch (K) {
+#define SSG_DOTK(KV)                                                        \
+  case KV:                                                                  \
+    k_dots<T, KV><<<nblk, 256, 0, s>>>(npts, x, ys, scale, part);           \
+    break;
+    SSG_DOTK(1) SSG_DOTK(2) SSG_DOTK(3) SSG_DOTK(4) SSG_DOTK(5)
+    SSG_DOTK(6) SSG_DOTK(7) SSG_DOTK(8) SSG_DOTK(9) SSG_DOTK(10)
+#undef SSG_DOTK
+    default:
+      return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t run_dots(cudaStream_t s, bool fp32, size_t npts, const void* x,
+                     const PtrList& ys, int K, const void* scale, double* part, int nblk) {
+  if (fp32)
+    return run_dots_t<float>(s, npts, (const float*)x, ys, K, (const float*)scale, part, nblk);
+  return run_dots_t<double>(s, npts, (const double*)x, ys, K, (const double*)scale, part,
+                            nblk);
+}
+
+cudaError_t run_wsum(cudaStream_t s, bool fp32, size_t npts, const void* x,
+                     const void* scale, double* part, int nblk) {
+  if (fp32)
+    k_wsum<float><<<nblk, 256, 0, s>>>(npts, (const float*)x, (const float*)scale, part);
+  else
+    k_wsum<double><<<nblk, 256, 0, s>>>(npts, (const double*)x, (const double*)scale, part);
+  return cudaGetLastError();
+}
+
+cudaError_t run_combine(cudaStream_t s, size_t npts, double* x, const PtrList& ys,
+                        const double* coef, int K, double sign, const double* c,
+                        const double* mask) {
+  k_combine<double><<<vec_blocks(npts), 256, 0, s>>>(npts, x, ys, coef, K, sign, c, mask);
+  return cudaGetLastError();
+}
+
+cudaError_t run_fcg_update(cudaStream_t s, size_t npts, const double* alpha, double* u,
+                           const double* p, double* r, const double* ap,
+                           const double* scale, double* part, int nblk) {
+  k_fcg_update<<<nblk, 256, 0, s>>>(npts, alpha, u, p, r, ap, scale, part);
+  return cudaGetLastError();
+}
+
+cudaError_t run_add_const(cudaStream_t s, bool fp32, size_t npts, void* x,
+                          const double* a, int neg) {
+  if (fp32)
+    k_add_const<float><<<vec_blocks(npts), 256, 0, s>>>(npts, (float*)x, a, neg);
+  else
+    k_add_const<double><<<vec_blocks(npts), 256, 0, s>>>(npts, (double*)x, a, neg);
+  return cudaGetLastError();
+}
+
+cudaError_t run_convert(cudaStream_t s, size_t npts, const void* in, bool in32, void* out,
+                        bool out32) {
+  const int nb = vec_blocks(npts);
+  if (in32 && !out32)
+    k_convert<float, double><<<nb, 256, 0, s>>>(npts, (const float*)in, (double*)out);
+  else if (!in32 && out32)
+    k_convert<double, float><<<nb, 256, 0, s>>>(npts, (const double*)in, (float*)out);
+  else if (in32)
+    k_convert<float, float><<<nb, 256, 0, s>>>(npts, (const float*)in, (float*)out);
+  else
+    k_convert<double, double><<<nb, 256, 0, s>>>(npts, (const double*)in, (double*)out);
+  return cudaGetLastError();
+}
+
+cudaError_t run_mul(cudaStream_t s, bool fp32, size_t npts, void* x, const double* y) {
+  if (fp32)
+    k_mul<float><<<vec_blocks(npts), 256, 0, s>>>(npts, (float*)x, y);
+  else
+    k_mul<double><<<vec_blocks(npts), 256, 0, s>>>(npts, (double*)x, y);
+  return cudaGetLastError();
+}
+
+cudaError_t run_reduce(cudaStream_t s, const double* part, int nblk, int nq, double* sums,
+                       const ScalarOp& op) {
+  k_reduce<<<1, 256, 0, s>>>(part, nblk, nq, sums, op);
+  return cudaGetLastError();
+}
+
+}  // namespace ssg

@@ -1,0 +1,386 @@
+// Krylov solvers and the p-multigrid V-cycle on the device.
+//
+//   cg_solve   conjugate_gradient with jacobi_preconditioner
+//              (src/solver.c:33-81, src/precon.c:311-324)
+//   mg_apply   multigrid_preconditioner / multigrid_recurse
+//              (src/precon.c:227-300)
+//   fcg_solve  flexible_conjugate_gradient with the window
+//              m = min(j, max(1, j mod 11)) (src/solver.c:83-157)
+//
+// All vectors and scalars stay on the device; the scalar algebra (alpha,
+// beta, nullspace constant, residual norm, stop flag) runs in the
+// reduction kernel, so the host only reads the stop flag.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "ssg_internal.h"
+#include "ssg_kernels.h"
+
+namespace ssg {
+
+struct LevelWork {
+  void *f = nullptr, *x = nullptr, *rr = nullptr, *r = nullptr, *z = nullptr;
+  void *p = nullptr, *ap = nullptr, *aploc = nullptr, *tc = nullptr;
+};
+
+struct Workspace {
+  LevelWork w64[SSG_MAXLEV];
+  LevelWork w32[SSG_MAXLEV];
+  bool have32 = false;
+  double *r = nullptr, *z = nullptr, *aploc = nullptr;
+  double* P[11] = {};
+  double* AP[10] = {};
+  double* hist = nullptr;
+  int hist_cap = 0;
+  std::vector<void*> blocks;
+};
+
+void free_workspace(Workspace* w) {
+  if (!w) return;
+  for (void* p : w->blocks) cudaFree(p);
+  delete w;
+}
+
+static ssg_status wsalloc(ssg_context* c, Workspace* w, void** p, size_t bytes) {
+  SSG_CUDA(c, cudaMalloc(p, bytes));
+  w->blocks.push_back(*p);
+  return SSG_OK;
+}
+
+static ssg_status alloc_level_work(ssg_context* c, Workspace* w, LevelWork& L, size_t np,
+                                   size_t bytes) {
+  void** v[] = {&L.f, &L.x, &L.rr, &L.r, &L.z, &L.p, &L.ap, &L.aploc, &L.tc};
+  for (void** p : v) SSG_TRY(wsalloc(c, w, p, np * bytes));
+  return SSG_OK;
+}
+
+ssg_status ensure_workspace(ssg_context* c) {
+  if (!c->ws) {
+    Workspace* w = new Workspace();
+    c->ws = w;
+    for (int l = 0; l < c->nlev; ++l)
+      SSG_TRY(alloc_level_work(c, w, w->w64[l], c->lev[l].npts, sizeof(double)));
+    const size_t np = c->lev[0].npts * sizeof(double);
+    SSG_TRY(wsalloc(c, w, (void**)&w->r, np));
+    SSG_TRY(wsalloc(c, w, (void**)&w->z, np));
+    SSG_TRY(wsalloc(c, w, (void**)&w->aploc, np));
+    for (auto& p : w->P) SSG_TRY(wsalloc(c, w, (void**)&p, np));
+    for (auto& p : w->AP) SSG_TRY(wsalloc(c, w, (void**)&p, np));
+    w->hist_cap = 8192;
+    SSG_TRY(wsalloc(c, w, (void**)&w->hist, w->hist_cap * sizeof(double)));
+  }
+  if (c->precision == SSG_PRECISION_MIXED && !c->ws->have32) {
+    for (int l = 0; l < c->nlev; ++l)
+      SSG_TRY(alloc_level_work(c, c->ws, c->ws->w32[l], c->lev[l].npts, sizeof(float)));
+    c->ws->have32 = true;
+  }
+  return SSG_OK;
+}
+
+static inline double lambda_of(const ssg_context* c) {
+  return (11.0 / 6.0) / (c->dt * c->visc);
+}
+
+// out = A_e in (global: then mask and DSS), at one level
+ssg_status op_apply(ssg_context* c, int level, int var, bool fp32, const void* in,
+                    void* out, bool global) {
+  SSG_TRY(ensure_workspace(c));
+  const DevLevel& L = c->lev[level];
+  const bool helm = var != SSG_PRESSURE;
+  if (helm && (fp32 || level != 0))
+    return fail(c, SSG_ERR_ARG, "the Helmholtz operator is FP64 at level 0 only");
+  void* loc = global ? (fp32 ? c->ws->w32[level].aploc : c->ws->w64[level].aploc) : out;
+  SSG_CUDA(c, run_ax(c->stream, L.n, c->nel, 0, helm, fp32, in, loc,
+                     fp32 ? (const void*)L.gf32 : (const void*)L.gf, L.npts, L.bj,
+                     fp32 ? (const void*)L.D32 : (const void*)L.D, L.S, lambda_of(c)));
+  if (global)
+    SSG_CUDA(c, run_dss(c->stream, DSS_PLAIN, fp32, L.n, c->nel, loc, out, c->d_pairs,
+                        helm ? L.mask : nullptr, nullptr, nullptr, nullptr));
+  return SSG_OK;
+}
+
+static ssg_status read_flag(ssg_context* c, const double* dptr, double* v) {
+  SSG_CUDA(c, cudaMemcpyAsync(c->h_pin, dptr, sizeof(double), cudaMemcpyDeviceToHost,
+                              c->stream));
+  SSG_CUDA(c, cudaStreamSynchronize(c->stream));
+  *v = c->h_pin[0];
+  return SSG_OK;
+}
+
+ssg_status cg_solve(ssg_context* c, int level, int var, bool fp32, void* f, void* x,
+                    double eps, int max_iter, int frame, double* hist, int hist_cap,
+                    bool sync_each) {
+  const DevLevel& L = c->lev[level];
+  LevelWork& W = fp32 ? c->ws->w32[level] : c->ws->w64[level];
+  const size_t np = L.npts;
+  const int nb = vec_blocks(np);
+  const int nbd = dss_grid(L.n, c->nel);
+  const bool helm = var != SSG_PRESSURE;
+  const bool pres = !helm;
+  if (helm && (fp32 || level != 0))
+    return fail(c, SSG_ERR_ARG, "the Helmholtz operator is FP64 at level 0 only");
+  const double* mask = helm && c->has_walls ? L.mask : nullptr;
+  double* fr = c->d_sc + frame * F_SIZE;
+  const void* dinv = helm ? (const void*)L.dinv_h
+                          : (fp32 ? (const void*)L.dinv_p32 : (const void*)L.dinv_p);
+  const void* scale = fp32 ? (const void*)L.scale32 : (const void*)L.scale;
+  const void* gf = fp32 ? (const void*)L.gf32 : (const void*)L.gf;
+  const void* D = fp32 ? (const void*)L.D32 : (const void*)L.D;
+  const double lam = lambda_of(c);
+  cudaStream_t s = c->stream;
+  ScalarOp op;
+  op.frame = fr;
+  op.pressure = pres;
+  op.nunique = L.nunique;
+  op.eps = eps;
+  op.max_iter = max_iter;
+  op.hist = hist;
+  op.hist_cap = hist_cap;
+
+  // mask f; r = f - A x; subtract_nullspace(r)
+  if (mask) SSG_CUDA(c, run_mul(s, fp32, np, f, mask));
+  SSG_CUDA(c, run_ax(s, L.n, c->nel, 0, helm, fp32, x, W.aploc, gf, np, L.bj, D, L.S, lam));
+  SSG_CUDA(c, run_dss(s, DSS_RESID, fp32, L.n, c->nel, W.aploc, W.r, c->d_pairs, mask, f,
+                      nullptr, c->d_part));
+  if (pres) {
+    op.code = OP_NULL_C;
+    SSG_CUDA(c, run_reduce(s, c->d_part, nbd, 1, c->d_sums, op));
+    SSG_CUDA(c, run_add_const(s, fp32, np, W.r, fr + F_C, 1));
+  }
+  // z = M^-1 r; subtract_nullspace(z); p = z; rdz = (r w).z
+  SSG_CUDA(c, run_jacobi(s, fp32, np, W.r, dinv, scale, W.z, c->d_part, nb));
+  op.code = OP_CG_INIT_C;
+  SSG_CUDA(c, run_reduce(s, c->d_part, nb, 1, c->d_sums, op));
+  SSG_CUDA(c, run_p_update(s, fp32, np, nullptr, pres ? fr + F_C : nullptr, W.p, W.z,
+                           mask, 1));
+  PtrList ys;
+  ys.p[0] = W.p;
+  ys.p[1] = W.r;
+  SSG_CUDA(c, run_dots(s, fp32, np, W.r, ys, 2, scale, c->d_part, nb));
+  op.code = OP_CG_INIT_RDZ;
+  SSG_CUDA(c, run_reduce(s, c->d_part, nb, 2, c->d_sums, op));
+
+  for (int it = 0; it < max_iter; ++it) {
+    // ap = DSS(mask A p); alpha = rdz / (p w).ap
+    SSG_CUDA(c, run_ax(s, L.n, c->nel, 0, helm, fp32, W.p, W.aploc, gf, np, L.bj, D, L.S,
+                       lam));
+    SSG_CUDA(c, run_dss(s, DSS_DOT, fp32, L.n, c->nel, W.aploc, W.ap, c->d_pairs, mask,
+                        W.p, nullptr, c->d_part));
+    op.code = OP_CG_ALPHA;
+    SSG_CUDA(c, run_reduce(s, c->d_part, nbd, 1, c->d_sums, op));
+    // x += alpha p; r -= alpha ap; z = M^-1 r; beta; err
+    SSG_CUDA(c, run_cg_update(s, fp32, np, fr + F_ALPHA, x, W.p, W.r, W.ap, dinv, scale,
+                              W.z, c->d_part, nb));
+    op.code = OP_CG_BETA;
+    SSG_CUDA(c, run_reduce(s, c->d_part, nb, 4, c->d_sums, op));
+    // p = beta p + (z - c); mask
+    SSG_CUDA(c, run_p_update(s, fp32, np, fr + F_BETA, pres ? fr + F_C : nullptr, W.p, W.z,
+                             mask, 0));
+    if (sync_each) {
+      double done;
+      SSG_TRY(read_flag(c, fr + F_DONE, &done));
+      if (done != 0.0) break;
+    }
+  }
+  double err, iters;
+  SSG_TRY(read_flag(c, fr + F_ERR, &err));
+  SSG_TRY(read_flag(c, fr + F_ITER, &iters));
+  if (!std::isfinite(err)) return fail(c, SSG_NONFINITE, "non-finite CG residual");
+  if (!(err <= eps) && iters >= max_iter) return SSG_MAXITER;
+  return SSG_OK;
+}
+
+// V-cycle from level L (multigrid_recurse, src/precon.c:238-271)
+static ssg_status mg_recurse(ssg_context* c, int L, void* f, void* x, double eps,
+                             bool fp32) {
+  const int last = c->nlev - 1;
+  cudaStream_t s = c->stream;
+  if (L == last) {
+    // coarsest level: CG-Jacobi to eps, 500 iterations, always FP64
+    if (fp32) {
+      LevelWork& W64 = c->ws->w64[L];
+      const size_t np = c->lev[L].npts;
+      SSG_CUDA(c, run_convert(s, np, f, true, W64.f, false));
+      SSG_CUDA(c, cudaMemsetAsync(W64.x, 0, np * sizeof(double), s));
+      ssg_status st = cg_solve(c, L, SSG_PRESSURE, false, W64.f, W64.x, eps, 500,
+                               FR_LEVEL0 + L, nullptr, 0, true);
+      if (st != SSG_OK && st != SSG_MAXITER) return st;
+      SSG_CUDA(c, run_convert(s, np, W64.x, false, x, true));
+      return SSG_OK;
+    }
+    ssg_status st = cg_solve(c, L, SSG_PRESSURE, false, f, x, eps, 500, FR_LEVEL0 + L,
+                             nullptr, 0, true);
+    return st == SSG_MAXITER ? SSG_OK : st;
+  }
+  const DevLevel& F = c->lev[L];
+  const DevLevel& C = c->lev[L + 1];
+  LevelWork& W = fp32 ? c->ws->w32[L] : c->ws->w64[L];
+  LevelWork& Wc = fp32 ? c->ws->w32[L + 1] : c->ws->w64[L + 1];
+  const void* rin = f;
+  if (L == 0) {
+    // r = f - A x (compute_residual, src/precon.c:302-309)
+    SSG_CUDA(c, run_ax(s, F.n, c->nel, 0, false, fp32, x, W.aploc,
+                       fp32 ? (const void*)F.gf32 : (const void*)F.gf, F.npts, nullptr,
+                       fp32 ? (const void*)F.D32 : (const void*)F.D, nullptr, 0.0));
+    SSG_CUDA(c, run_dss(s, DSS_RESID, fp32, F.n, c->nel, W.aploc, W.rr, c->d_pairs, nullptr,
+                        f, nullptr, c->d_part));
+    rin = W.rr;
+  }
+  // restriction: (J^T)^3 then DSS-average at the coarse level
+  SSG_CUDA(c, run_tensor3(s, fp32, false, c->nel, F.n, C.n,
+                          fp32 ? (const void*)C.Ar32 : (const void*)C.Ar, rin, Wc.tc));
+  SSG_CUDA(c, run_dss(s, DSS_AVG, fp32, C.n, c->nel, Wc.tc, Wc.f, c->d_pairs, nullptr,
+                      nullptr, nullptr, nullptr));
+  SSG_CUDA(c, cudaMemsetAsync(Wc.x, 0, C.npts * (fp32 ? sizeof(float) : sizeof(double)), s));
+  SSG_TRY(mg_recurse(c, L + 1, Wc.f, Wc.x, eps, fp32));
+  // prolongation J^3 and x += e
+  SSG_CUDA(c, run_tensor3(s, fp32, true, c->nel, C.n, F.n,
+                          fp32 ? (const void*)C.Ap32 : (const void*)C.Ap, Wc.x, x));
+  // post-smoothing: CG-Jacobi, 15 iterations, stop at eps
+  ssg_status st = cg_solve(c, L, SSG_PRESSURE, fp32, f, x, eps, 15, FR_LEVEL0 + L, nullptr,
+                           0, true);
+  return st == SSG_MAXITER ? SSG_OK : st;
+}
+
+// z = M^-1 r: Jacobi then one V-cycle (multigrid_preconditioner,
+// src/precon.c:227-236)
+ssg_status mg_apply(ssg_context* c, const double* r, double* z, double eps) {
+  SSG_TRY(ensure_workspace(c));
+  const bool fp32 = c->precision == SSG_PRECISION_MIXED;
+  const DevLevel& L = c->lev[0];
+  const size_t np = L.npts;
+  const int nb = vec_blocks(np);
+  cudaStream_t s = c->stream;
+  void* f0 = (void*)r;
+  void* x0 = z;
+  if (fp32) {
+    f0 = c->ws->w32[0].f;
+    x0 = c->ws->w32[0].x;
+    SSG_CUDA(c, run_convert(s, np, r, false, f0, true));
+  }
+  SSG_CUDA(c, run_jacobi(s, fp32, np, f0, fp32 ? (const void*)L.dinv_p32 : (const void*)L.dinv_p,
+                         fp32 ? (const void*)L.scale32 : (const void*)L.scale, x0, c->d_part,
+                         nb));
+  if (c->nlev > 1) SSG_TRY(mg_recurse(c, 0, f0, x0, eps, fp32));
+  if (fp32) SSG_CUDA(c, run_convert(s, np, x0, true, z, false));
+  return SSG_OK;
+}
+
+ssg_status fcg_solve(ssg_context* c, const double* f, double* u, double eps, int max_iter,
+                     ssg_solve_info* info) {
+  SSG_TRY(ensure_workspace(c));
+  Workspace* w = c->ws;
+  const DevLevel& L = c->lev[0];
+  const size_t np = L.npts;
+  const int nb = vec_blocks(np);
+  const int nbd = dss_grid(L.n, c->nel);
+  cudaStream_t s = c->stream;
+  double* fr = c->d_sc + FR_FCG * F_SIZE;
+  const int hcap = info && info->history && info->history_cap > 0
+                       ? std::min(std::min(info->history_cap, max_iter), w->hist_cap)
+                       : 0;
+  ScalarOp op;
+  op.frame = fr;
+  op.pressure = 1;
+  op.nunique = L.nunique;
+  op.eps = eps;
+  op.max_iter = max_iter;
+  op.hist = hcap ? w->hist : nullptr;
+  op.hist_cap = hcap;
+
+  // r = f - A u; subtract_nullspace(r)
+  SSG_CUDA(c, run_ax(s, L.n, c->nel, 0, false, false, u, w->aploc, L.gf, np, nullptr, L.D,
+                     nullptr, 0.0));
+  SSG_CUDA(c, run_dss(s, DSS_RESID, false, L.n, c->nel, w->aploc, w->r, c->d_pairs, nullptr,
+                      f, nullptr, c->d_part));
+  op.code = OP_NULL_C;
+  SSG_CUDA(c, run_reduce(s, c->d_part, nbd, 1, c->d_sums, op));
+  SSG_CUDA(c, run_add_const(s, false, np, w->r, fr + F_C, 1));
+  PtrList ys;
+  ys.p[0] = w->r;
+  SSG_CUDA(c, run_dots(s, false, np, w->r, ys, 1, L.scale, c->d_part, nb));
+  op.code = OP_ERR0;
+  SSG_CUDA(c, run_reduce(s, c->d_part, nb, 1, c->d_sums, op));
+
+  int pslot[11], aslot[10];
+  for (int k = 0; k < 11; ++k) pslot[k] = k;
+  for (int k = 0; k < 10; ++k) aslot[k] = k;
+  const int mmax = 10;
+  for (int j = 0; j < max_iter; ++j) {
+    int m = std::max(1, j % (mmax + 1));
+    m = std::min(m, j);
+    SSG_TRY(mg_apply(c, w->r, w->z, eps));
+    // subtract_nullspace(z)
+    SSG_CUDA(c, run_wsum(s, false, np, w->z, L.scale, c->d_part, nb));
+    op.code = OP_NULL_C;
+    SSG_CUDA(c, run_reduce(s, c->d_part, nb, 1, c->d_sums, op));
+    SSG_CUDA(c, run_add_const(s, false, np, w->z, fr + F_C, 1));
+    // beta_k = (z w).ap_k / pap_k
+    if (m > 0) {
+      PtrList yb;
+      for (int k = 0; k < m; ++k) {
+        yb.p[k] = w->AP[aslot[k]];
+        op.pap_idx[k] = aslot[k];
+      }
+      op.m = m;
+      SSG_CUDA(c, run_dots(s, false, np, w->z, yb, m, L.scale, c->d_part, nb));
+      op.code = OP_FCG_BETA;
+      SSG_CUDA(c, run_reduce(s, c->d_part, nb, m, c->d_sums, op));
+    }
+    // shift the directions and form p0 = z - sum beta_k p_k
+    const int tail = pslot[m];
+    for (int k = m; k > 0; --k) pslot[k] = pslot[k - 1];
+    pslot[0] = tail;
+    double* p0 = w->P[pslot[0]];
+    SSG_CUDA(c, cudaMemcpyAsync(p0, w->z, np * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    if (m > 0) {
+      PtrList yp;
+      for (int k = 0; k < m; ++k) yp.p[k] = w->P[pslot[k + 1]];
+      SSG_CUDA(c, run_combine(s, np, p0, yp, fr + F_FBETA, m, -1.0, nullptr, nullptr));
+    }
+    // shift the ap history
+    int m2 = std::max(1, (j + 1) % (mmax + 1));
+    m2 = std::min(m2, j + 1);
+    const int atail = aslot[m2 - 1];
+    for (int k = m2 - 1; k > 0; --k) aslot[k] = aslot[k - 1];
+    aslot[0] = atail;
+    double* ap0 = w->AP[aslot[0]];
+    // ap0 = A p0; pap0 and alpha = (p0 w).r / pap0
+    SSG_CUDA(c, run_ax(s, L.n, c->nel, 0, false, false, p0, w->aploc, L.gf, np, nullptr, L.D,
+                       nullptr, 0.0));
+    SSG_CUDA(c, run_dss(s, DSS_DOT2, false, L.n, c->nel, w->aploc, ap0, c->d_pairs, nullptr,
+                        p0, w->r, c->d_part));
+    op.pap_idx[0] = aslot[0];
+    op.code = OP_FCG_ALPHA;
+    SSG_CUDA(c, run_reduce(s, c->d_part, nbd, 2, c->d_sums, op));
+    // u += alpha p0; r -= alpha ap0; err
+    SSG_CUDA(c, run_fcg_update(s, np, fr + F_ALPHA, u, p0, w->r, ap0, L.scale, c->d_part, nb));
+    op.code = OP_FCG_ERR;
+    SSG_CUDA(c, run_reduce(s, c->d_part, nb, 1, c->d_sums, op));
+    double done;
+    SSG_TRY(read_flag(c, fr + F_DONE, &done));
+    if (done != 0.0) break;
+  }
+  double h[F_SIZE];
+  SSG_CUDA(c, cudaMemcpyAsync(c->h_pin, fr, F_SIZE * sizeof(double), cudaMemcpyDeviceToHost,
+                              s));
+  SSG_CUDA(c, cudaStreamSynchronize(s));
+  std::memcpy(h, c->h_pin, sizeof(h));
+  if (info) {
+    info->iterations = (int)h[F_ITER];
+    info->residual = h[F_ERR];
+    info->initial_residual = h[F_ERR0];
+    info->history_len = std::min((int)h[F_ITER], hcap);
+    if (hcap)
+      SSG_CUDA(c, cudaMemcpy(info->history, w->hist, info->history_len * sizeof(double),
+                             cudaMemcpyDeviceToHost));
+  }
+  if (!std::isfinite(h[F_ERR])) return fail(c, SSG_NONFINITE, "non-finite FCG residual");
+  if (!(h[F_ERR] <= eps)) return SSG_MAXITER;
+  return SSG_OK;
+}
+
+}  // namespace ssg

@@ -1,0 +1,161 @@
+// Internal declarations of libssenss_b200 (not installed).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstddef>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "ssenss_b200.h"
+
+#define SSG_MAXLEV 8
+#define SSG_MAXN 18
+
+namespace ssg {
+
+// ---------------------------------------------------------------------------
+// host-side discretisation (setup.cpp)
+// ---------------------------------------------------------------------------
+struct HostLevel {
+  int n = 0;
+  size_t nt = 0;                        // n^3
+  std::vector<double> x, w;             // GLL points, weights
+  std::vector<double> D, S;             // D[i*n+m] = l_m'(x_i); S = SVV variant
+  std::vector<double> jf;               // from the finer level: jf[i*n+p] = l_p(x_i^fine)
+  std::vector<double> g[6];             // G11 G12 G13 G22 G23 G33 (unscaled)
+  std::vector<double> det;              // det J
+  std::vector<double> grid[3];
+  std::vector<double> jac[9];           // J[a][b] = dx_a/dr_b (level 0, conv)
+  std::vector<double> tinv[9];          // tinv[a][b] = dr_b/dx_a
+};
+
+struct HostMesh {
+  int n = 0, nel = 0, nlev = 0;
+  std::vector<int> neigh;               // nel x 26
+  std::vector<int> pairs;               // nel x 26 x 2: (element, matched index)
+  std::vector<int> bc;                  // Dirichlet face bits per element
+  HostLevel lev[SSG_MAXLEV];
+  HostLevel conv;                       // dealiasing grid (m = 3n/2)
+  std::vector<double> jconv;            // jconv[i*n+p] = l_p^n(x_i^m)
+  bool has_conv = false;
+  bool has_particle_geom = false;
+};
+
+int level_orders(int n, int* orders);
+void gll_basis(int n, double* x, double* w);
+void deriv_matrix(int n, const double* x, double* D);
+void svv_deriv_matrix(int n, const double* x, const double* w, int msvv, double c,
+                      double* S);
+void interp_matrix(int nto, const double* xto, int nfrom, const double* xfrom, double* J);
+ssg_status build_mesh(HostMesh& m, int n, int nel, const double* vertices,
+                      const int* neigh, std::string& err);
+ssg_status build_pairs(HostMesh& m, std::string& err);
+void stiffness_diagonal(const HostLevel& L, int nel, double* out);
+void host_dss(const HostMesh& m, int n, double* u);
+
+// ---------------------------------------------------------------------------
+// device-side level
+// ---------------------------------------------------------------------------
+struct DevLevel {
+  int n = 0;
+  size_t nt = 0, npts = 0;
+  double* gf = nullptr;        // 6 x npts: G_ab * rho * J
+  double* bj = nullptr;        // rho * J
+  double* kdiag = nullptr;     // element-local stiffness diagonal
+  double* dinv_p = nullptr;    // Poisson Jacobi inverse
+  double* dinv_h = nullptr;    // Helmholtz Jacobi inverse (for lambda_h)
+  double* scale = nullptr;     // 1 / multiplicity
+  double* mask = nullptr;      // Dirichlet mask (null without walls)
+  double* D = nullptr;         // n*n
+  double* S = nullptr;         // n*n
+  double* Ar = nullptr;        // restriction into this level: n x n_finer
+  double* Ap = nullptr;        // prolongation from this level: n_finer x n
+  float* gf32 = nullptr;       // FP32 copies for the mixed-precision V-cycle
+  float* dinv_p32 = nullptr;
+  float* scale32 = nullptr;
+  float* D32 = nullptr;
+  float* Ar32 = nullptr;
+  float* Ap32 = nullptr;
+  double nunique = 0.0;        // sum of 1/multiplicity
+  double lambda_h = -1.0;      // lambda the Helmholtz diagonal holds
+};
+
+struct Workspace;
+
+void free_workspace(Workspace* w);
+
+}  // namespace ssg
+
+struct ssg_context {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::string err;
+  double dt = 1.0, visc = 1.0, dens = 1.0;
+  int precision = SSG_PRECISION_FP64;
+  bool graphs = true;
+  bool ready = false;
+  int n = 0, nel = 0, nlev = 0;
+  int orders[SSG_MAXLEV] = {0};
+  ssg::HostMesh host;
+  int* d_pairs = nullptr;       // nel x 26 x int2
+  bool has_walls = false;
+  ssg::DevLevel lev[SSG_MAXLEV];
+  double* inv_mass = nullptr;   // level 0
+  // dealiasing grid
+  int m = 0;
+  double* conv_tinv = nullptr;  // 9 x nel x m^3
+  double* conv_bj = nullptr;    // rho * J at m
+  double* conv_D = nullptr;     // m*m
+  double* conv_J = nullptr;     // m*n, jconv[i*n+p]
+  // particles
+  double* p_jac = nullptr;      // 9 x npts (level 0)
+  double* p_tinv = nullptr;     // 9 x npts
+  double* p_ur = nullptr;       // 3 x 3 x npts
+  double* p_x = nullptr;        // GLL points of level 0
+  // reductions / scalars
+  double* d_part = nullptr;     // block partial sums
+  size_t part_cap = 0;
+  double* d_sums = nullptr;     // 16 raw sums
+  double* d_sc = nullptr;       // solver frames
+  double* h_pin = nullptr;      // pinned host scalars
+  // staging for host arguments
+  double* d_stage[4] = {nullptr, nullptr, nullptr, nullptr};
+  size_t stage_cap = 0;
+  ssg::Workspace* ws = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace ssg {
+
+ssg_status fail(ssg_context* c, ssg_status s, const std::string& msg);
+ssg_status cuda_fail(ssg_context* c, cudaError_t e, const char* what);
+#define SSG_CUDA(c, call)                                           \
+  do {                                                              \
+    cudaError_t _e = (call);                                        \
+    if (_e != cudaSuccess) return ::ssg::cuda_fail((c), _e, #call); \
+  } while (0)
+#define SSG_TRY(call)                    \
+  do {                                   \
+    ssg_status _s = (call);              \
+    if (_s != SSG_OK) return _s;         \
+  } while (0)
+
+bool is_device_ptr(const void* p);
+
+enum Frame { FR_LEVEL0 = 0, FR_HELM = 8, FR_FCG = 9, FR_MISC = 10, FR_COUNT = 12 };
+
+// solver.cu
+ssg_status ensure_workspace(ssg_context* c);
+ssg_status op_apply(ssg_context* c, int level, int var, bool fp32, const void* in,
+                    void* out, bool global);
+ssg_status cg_solve(ssg_context* c, int level, int var, bool fp32, void* f, void* x,
+                    double eps, int max_iter, int frame, double* hist, int hist_cap,
+                    bool sync_each);
+ssg_status mg_apply(ssg_context* c, const double* r, double* z, double eps);
+ssg_status fcg_solve(ssg_context* c, const double* f, double* u, double eps, int max_iter,
+                     ssg_solve_info* info);
+ssg_status helmholtz_diag_update(ssg_context* c);
+
+}  // namespace ssg

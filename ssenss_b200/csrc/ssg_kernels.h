@@ -1,0 +1,93 @@
+// Launch interface of the device kernels (kernels.cu) used by the solver.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstddef>
+
+namespace ssg {
+
+enum OpCode {
+  OP_NONE = 0,
+  OP_CG_INIT_C,     // c = (w.z)/nunique (pressure) else 0
+  OP_CG_INIT_RDZ,   // rdz = (r w).p, reset iteration counters
+  OP_CG_ALPHA,      // alpha = rdz / (p w).ap
+  OP_CG_BETA,       // nullspace constant, beta, err, done flag
+  OP_NULL_C,        // c = (w.x)/nunique
+  OP_FCG_BETA,      // beta_k = (z w).ap_k / pap_k
+  OP_FCG_ALPHA,     // pap_0, alpha = (p0 w).r / pap_0
+  OP_FCG_ERR,       // err, iteration count, done flag
+  OP_ERR0           // initial residual norm
+};
+
+// slots of one solver frame (doubles)
+enum {
+  F_RDZ = 0, F_ALPHA = 1, F_BETA = 2, F_C = 3, F_ERR = 4, F_ITER = 5,
+  F_DONE = 6, F_PAP = 7, F_ERR0 = 8,
+  F_FBETA = 16,     // 10 slots
+  F_FPAP = 32,      // 10 slots
+  F_SIZE = 48
+};
+
+struct ScalarOp {
+  int code = OP_NONE;
+  int pressure = 0;
+  double nunique = 1.0;
+  double eps = 0.0;
+  int max_iter = 0;
+  double* frame = nullptr;
+  double* hist = nullptr;   // device history buffer (optional)
+  int hist_cap = 0;
+  int m = 0;
+  int pap_idx[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+};
+
+// up to 10 vectors passed by value to a kernel (capturable: no upload)
+struct PtrList {
+  const void* p[10] = {nullptr, nullptr, nullptr, nullptr, nullptr,
+                       nullptr, nullptr, nullptr, nullptr, nullptr};
+};
+
+// DSS epilogue modes (kernels.cu)
+enum { DSS_PLAIN = 0, DSS_DOT = 1, DSS_RESID = 2, DSS_AVG = 3, DSS_DOT2 = 4 };
+
+int vec_blocks(size_t npts);
+int ax_epb(int n, bool fp32);
+int dss_grid(int n, int nel);
+
+cudaError_t run_ax(cudaStream_t s, int n, int nel, int epb, bool helm, bool fp32,
+                   const void* in, void* out, const void* gf, size_t npts,
+                   const double* bj, const void* D, const void* S, double lambda);
+cudaError_t run_dss(cudaStream_t s, int mode, bool fp32, int n, int nel, const void* in,
+                    void* out, const int* pairs, const double* mask, const void* y,
+                    const void* y2, double* part);
+cudaError_t run_tensor3(cudaStream_t s, bool fp32, bool add, int nel, int ni, int no,
+                        const void* A, const void* in, void* out);
+cudaError_t run_cg_update(cudaStream_t s, bool fp32, size_t npts, const double* alpha,
+                          void* x, const void* p, void* r, const void* ap,
+                          const void* dinv, const void* scale, void* z, double* part,
+                          int nblk);
+cudaError_t run_p_update(cudaStream_t s, bool fp32, size_t npts, const double* beta,
+                         const double* c, void* p, const void* z, const double* mask,
+                         int first);
+cudaError_t run_jacobi(cudaStream_t s, bool fp32, size_t npts, const void* r,
+                       const void* dinv, const void* scale, void* z, double* part,
+                       int nblk);
+cudaError_t run_dots(cudaStream_t s, bool fp32, size_t npts, const void* x,
+                     const PtrList& ys, int K, const void* scale, double* part, int nblk);
+cudaError_t run_wsum(cudaStream_t s, bool fp32, size_t npts, const void* x,
+                     const void* scale, double* part, int nblk);
+cudaError_t run_combine(cudaStream_t s, size_t npts, double* x, const PtrList& ys,
+                        const double* coef, int K, double sign, const double* c,
+                        const double* mask);
+cudaError_t run_fcg_update(cudaStream_t s, size_t npts, const double* alpha, double* u,
+                           const double* p, double* r, const double* ap,
+                           const double* scale, double* part, int nblk);
+cudaError_t run_add_const(cudaStream_t s, bool fp32, size_t npts, void* x,
+                          const double* a, int neg);
+cudaError_t run_convert(cudaStream_t s, size_t npts, const void* in, bool in32, void* out,
+                        bool out32);
+cudaError_t run_mul(cudaStream_t s, bool fp32, size_t npts, void* x, const double* y);
+cudaError_t run_reduce(cudaStream_t s, const double* part, int nblk, int nq, double* sums,
+                       const ScalarOp& op);
+
+}  // namespace ssg

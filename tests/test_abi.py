@@ -1,0 +1,50 @@
+"""The C-ABI library loads and exports every entry point include/ssenss_b200.h
+declares (no GPU needed)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from conftest import ROOT
+
+
+def header_symbols():
+    src = open(os.path.join(ROOT, "include", "ssenss_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(ssg_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_header_declares_entry_points():
+    syms = header_symbols()
+    for s in ("ssg_global_opeval", "ssg_solve_poisson_cg", "ssg_solve_helmholtz_cg",
+              "ssg_direct_stiffness_summation", "ssg_convection_operator",
+              "ssg_integrate_particle_equations"):
+        assert s in syms
+
+
+def test_library_exports_every_declared_symbol():
+    from ssenss_b200 import _lib
+    lib = ctypes.CDLL(_lib.LIB_PATH)
+    missing = [s for s in header_symbols() if not hasattr(lib, s)]
+    assert not missing, missing
+    bound = {name for name, _, _ in _lib.SIGNATURES}
+    assert set(header_symbols()) <= bound
+
+
+def test_status_strings():
+    from ssenss_b200 import _lib
+    lib = _lib.load()
+    for s in range(11):
+        assert lib.ssg_status_string(s)
+
+
+def test_no_device_fails_cleanly():
+    """Without a usable GPU the library refuses (no CPU fallback)."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    import ssenss_b200 as S
+    with pytest.raises(S.SsgError) as ei:
+        S.Context(0)
+    assert ei.value.status == 2

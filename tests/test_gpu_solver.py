@@ -1,0 +1,181 @@
+"""GPU parity of the solve path against the CPU oracle (oracle/ssg_oracle.c),
+through the C ABI.
+
+Tolerances: integer pairing and DSS are bitwise; element operators agree to
+1e-13 relative (summation order and FMA differ from the oracle); solves stop
+at the reference's absolute criterion sqrt((r.r)_w) <= 1e-10 and their
+solutions agree to 1e-11 relative.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from ssenss_b200.mesh import box_mesh, channel_mesh, tgv_box
+
+pytestmark = pytest.mark.gpu
+
+CASES = {
+    "tgv3_n8": (lambda: tgv_box(3), 8),
+    "tgv4_n6": (lambda: tgv_box(4), 6),
+    "channel433_n7": (lambda: channel_mesh((4, 3, 3), seed=7), 7),
+    "periodic233_n5": (lambda: box_mesh((2, 3, 3)), 5),
+    "tgv3_n10": (lambda: tgv_box(3), 10),
+}
+
+_cache = {}
+
+
+def setup_case(name, gpu_ctx_factory):
+    if name not in _cache:
+        mk, n = CASES[name]
+        mesh = mk()
+        orc = O.Oracle(mesh, n)
+        ctx = gpu_ctx_factory(mesh, n)
+        _cache[name] = (mesh, n, orc, ctx)
+    return _cache[name]
+
+
+def rel(a, b):
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def weights(n):
+    x = np.empty(n)
+    w = np.empty(n)
+    L = O.Oracle.lib()
+    L.og_gll(n, x.ctypes.data_as(O._dp), w.ctypes.data_as(O._dp))
+    return x, w
+
+
+def smooth_field(orc, kx=1.0, ky=1.0, kz=1.0, ph=(0.3, 0.7, 1.1)):
+    X, Y, Z = orc.geometry(0, 7), orc.geometry(0, 8), orc.geometry(0, 9)
+    return np.cos(kx * X + ph[0]) * np.cos(ky * Y + ph[1]) * np.cos(kz * Z + ph[2])
+
+
+def weak_rhs(orc, g):
+    n = orc.n
+    _, w = weights(n)
+    rho = w[None, None, None, :] * w[None, None, :, None] * w[None, :, None, None]
+    return orc.dss(rho * orc.geometry(0, 6) * g)
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_level_data_matches_oracle(name, gpu_ctx_factory):
+    mesh, n, orc, ctx = setup_case(name, gpu_ctx_factory)
+    assert ctx.orders == orc.orders
+    for L in range(orc.nlevels):
+        m = orc.orders[L]
+        _, w = weights(m)
+        rho = w[None, None, None, :] * w[None, None, :, None] * w[None, :, None, None]
+        bj = rho * orc.geometry(L, 6)
+        assert rel(ctx.level_data(L, 6), bj) < 1e-15
+        for a in range(6):
+            g = orc.geometry(L, a) * bj
+            d = ctx.level_data(L, a)
+            scale = max(np.max(np.abs(orc.geometry(L, 0) * bj)), 1e-300)
+            assert np.max(np.abs(d - g)) / scale < 1e-14, (L, a)
+        assert np.array_equal(ctx.level_data(L, 9), orc.precon(L, 2))   # 1/multiplicity
+        assert np.array_equal(ctx.level_data(L, 10), orc.precon(L, 3))  # mask
+        assert rel(ctx.level_data(L, 7), orc.precon(L, 0)) < 1e-14      # Poisson diag
+    assert rel(ctx.level_data(0, 8), orc.precon(0, 1)) < 1e-14          # Helmholtz diag
+    assert rel(ctx.level_data(0, 11), orc.precon(0, 4)) < 1e-14         # inverse mass
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_dss_bitwise(name, gpu_ctx_factory):
+    mesh, n, orc, ctx = setup_case(name, gpu_ctx_factory)
+    rng = np.random.default_rng(1)
+    u = rng.standard_normal((mesh.nel, n, n, n))
+    got = ctx.direct_stiffness_summation(u.copy())
+    assert np.array_equal(got, orc.dss(u))
+
+
+@pytest.mark.parametrize("name", list(CASES))
+@pytest.mark.parametrize("var", [O.PRESSURE, O.X_VELOCITY])
+def test_operator_matches_oracle(name, var, gpu_ctx_factory):
+    mesh, n, orc, ctx = setup_case(name, gpu_ctx_factory)
+    rng = np.random.default_rng(2)
+    p = rng.standard_normal((mesh.nel, n, n, n))
+    assert rel(ctx.local_opeval(var, p), orc.local_opeval(var, p)) < 1e-13
+    assert rel(ctx.global_opeval(var, p), orc.global_opeval(var, p)) < 1e-13
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_dot_matches_oracle(name, gpu_ctx_factory):
+    mesh, n, orc, ctx = setup_case(name, gpu_ctx_factory)
+    rng = np.random.default_rng(3)
+    x = rng.standard_normal((mesh.nel, n, n, n))
+    y = rng.standard_normal((mesh.nel, n, n, n))
+    a, b = ctx.global_dot_product(x, y), orc.dot(x, y)
+    assert abs(a - b) <= 1e-12 * np.sqrt(orc.dot(x, x) * orc.dot(y, y))
+
+
+@pytest.mark.parametrize("name", ["tgv3_n8", "channel433_n7", "tgv3_n10"])
+def test_multigrid_preconditioner(name, gpu_ctx_factory):
+    mesh, n, orc, ctx = setup_case(name, gpu_ctx_factory)
+    r = weak_rhs(orc, smooth_field(orc))
+    z_o = orc.mg_precon(r)
+    z_g = ctx.multigrid_preconditioner(r)
+    assert rel(z_g, z_o) < 1e-9
+
+
+@pytest.mark.parametrize("name", ["tgv3_n8", "tgv4_n6", "channel433_n7", "periodic233_n5",
+                                  "tgv3_n10"])
+def test_poisson_solve(name, gpu_ctx_factory):
+    mesh, n, orc, ctx = setup_case(name, gpu_ctx_factory)
+    f = weak_rhs(orc, 3.0 * smooth_field(orc))
+    u0 = np.zeros_like(f)
+    u_o, h_o = orc.solve_poisson(f, u0)
+    u_g, info = ctx.solve_poisson_cg(f, u0.copy())
+    assert info["status"] == "SSG_OK"
+    assert info["iterations"] == len(h_o)
+    assert info["residual"] <= 1e-10
+    assert rel(u_g, u_o) < 1e-11
+    # residual histories: identical down to the rounding floor near eps
+    h_g = info["history"]
+    assert len(h_g) == len(h_o)
+    assert np.all(np.abs(h_g - h_o) <= 1e-6 * h_o + 1e-13)
+
+
+@pytest.mark.parametrize("name", ["tgv3_n8", "channel433_n7", "tgv4_n6"])
+@pytest.mark.parametrize("var", [O.X_VELOCITY, O.Z_VELOCITY])
+def test_helmholtz_solve(name, var, gpu_ctx_factory):
+    mesh, n, orc, ctx = setup_case(name, gpu_ctx_factory)
+    f = weak_rhs(orc, smooth_field(orc))
+    u0 = np.zeros_like(f)
+    u_o, h_o = orc.solve_helmholtz(var, f, u0)
+    u_g, info = ctx.solve_helmholtz_cg(var, f, u0.copy())
+    assert info["status"] == "SSG_OK"
+    assert info["iterations"] == len(h_o)
+    assert rel(u_g, u_o) < 1e-12
+    assert np.all(np.abs(info["history"] - h_o) <= 1e-9 * h_o + 1e-14)
+
+
+def test_device_pointers(gpu_ctx_factory):
+    """CUDA tensors are used in place (no staging)."""
+    import torch
+    mesh, n, orc, ctx = setup_case("tgv3_n8", gpu_ctx_factory)
+    rng = np.random.default_rng(4)
+    p = rng.standard_normal((mesh.nel, n, n, n))
+    pd = torch.from_numpy(p).cuda()
+    out = ctx.global_opeval(O.PRESSURE, pd)
+    torch.cuda.synchronize()
+    assert rel(out.cpu().numpy(), orc.global_opeval(O.PRESSURE, p)) < 1e-13
+
+
+@pytest.mark.parametrize("name", ["tgv3_n8", "channel433_n7"])
+def test_mixed_precision_solve(name, gpu_ctx_factory):
+    """FP32 V-cycle inside the FP64 FCG reaches the same 1e-10 residual; the
+    solution differs from the FP64 oracle only by the solver tolerance."""
+    mk, n = CASES[name]
+    mesh = mk()
+    orc = O.Oracle(mesh, n)
+    ctx = gpu_ctx_factory(mesh, n, precision="mixed")
+    f = weak_rhs(orc, 3.0 * smooth_field(orc))
+    u0 = np.zeros_like(f)
+    u_o, h_o = orc.solve_poisson(f, u0)
+    u_g, info = ctx.solve_poisson_cg(f, u0.copy())
+    assert info["status"] == "SSG_OK"
+    assert info["residual"] <= 1e-10
+    assert info["iterations"] <= len(h_o) + 3
+    assert rel(u_g, u_o) < 1e-8
