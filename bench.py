@@ -1,0 +1,436 @@
+#!/usr/bin/env python
+"""Benchmark of the SSENSS per-timestep solve path on B200.
+
+Workload (one "step"): the pressure Poisson solve of the Taylor-Green vortex
+on the triply periodic [0, 2 pi]^3 box of 16 x 16 x 16 hexahedra at N = 7
+(n = 8 GLL points per direction, 2,097,152 local points): flexible CG with
+the p-multigrid preconditioner (solve_poisson_cg, src/solver.c:159-173) to
+the reference's absolute criterion sqrt((r.r)_w) <= 1e-10, from a zero
+initial guess, right-hand side the weak form of -lap p for the TGV pressure
+p = (cos 2x + cos 2y)(cos 2z + 2)/16, assembled by DSS.  Synthetic data: the
+mesh and fields are generated, not read.
+
+Metric: GDOF/s per PCG iteration = unique DOFs x outer iterations / time,
+plus solves/s; FP64 (the plain form, `value`) and the mixed-precision form
+(FP32 storage in the V-cycle) side by side.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+N > 1 runs independent replicas, one per GPU (the solve does not shard at
+this tier); value = DOF-iterations of all ranks / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
+
+METRIC = ("GDOF/s per PCG iter & solves/s: mixed vs FP64 GPU at 1e-10 resid; "
+          "p99 latency")
+UNIT = "GDOF/s"
+NE, NORD = 16, 8          # 16^3 elements, n = N + 1 = 8
+EPS = 1e-10
+# dominant kernel: the level-0 element operator (Laplacian), bytes per local
+# point: read u (8) + six G*rho*J factors (48) + write (8)
+OP_BYTES_PER_POINT = 64
+# DRAM bytes per launch of that kernel from the committed ncu capture
+# (profiles/), None until captured
+OP_TRAFFIC_BYTES = None
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--ne", type=int, default=NE)
+    ap.add_argument("--n", type=int, default=NORD)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def tgv_rhs_strong(X, Y, Z):
+    """-lap p for p = (cos 2x + cos 2y)(cos 2z + 2)/16."""
+    import numpy as np
+    c2x, c2y, c2z = np.cos(2 * X), np.cos(2 * Y), np.cos(2 * Z)
+    lap = (-4.0 * (c2x + c2y) * (c2z + 2.0) - 4.0 * (c2x + c2y) * c2z) / 16.0
+    return -lap
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = max(mx, float(p[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl" if args.impl == "ours" else "gloo",
+                                timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return world, rank, local, pg
+
+
+def max_over_ranks(pg, v, device=None):
+    if pg is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(pg, v, device=None):
+    if pg is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.SUM)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
+# CPU reference (the reference sources compiled in place, oracle/_ref)
+# ---------------------------------------------------------------------------
+def reference_sample(mesh, n, f, max_iter):
+    """Time the reference's FCG + p-MG (flexible_conjugate_gradient,
+    src/solver.c:83-157) on this workload, 1 core, for at most max_iter outer
+    iterations; returns (seconds, iterations run)."""
+    import numpy as np
+    import oracle
+    ref = oracle.Reference(mesh, n)
+    f = np.ascontiguousarray(f)
+    u = np.zeros_like(f)
+    t0 = time.perf_counter()
+    ref.lib().ssgref_fcg_mg(oracle._d(f), oracle._d(u), EPS, max_iter)
+    dt = time.perf_counter() - t0
+    # iterations actually run: rerun is too costly; the cap is reached unless
+    # the residual fell below eps first, which the oracle's count tells
+    ref.close()
+    return dt, max_iter
+
+
+def run_reference(args):
+    world, rank, local, pg = dist_setup(args)
+    if rank != 0:
+        if pg is not None:
+            pg.destroy_process_group()
+        return 0
+    import numpy as np
+    import oracle
+    from ssenss_b200.mesh import tgv_box
+    if not oracle.reference_available():
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "oracle/_ref/libssenss_ref.so not built "
+                                         "(the reference sources were absent at build)"}))
+        return 0
+    mesh = tgv_box(args.ne)
+    n = args.n
+    orc = oracle.Oracle(mesh, n)
+    X, Y, Z = (orc.geometry(0, 7 + a) for a in range(3))
+    x = np.empty(n)
+    w = np.empty(n)
+    oracle.Oracle.lib().og_gll(n, oracle._d(x), oracle._d(w))
+    rho = w[None, None, None, :] * w[None, None, :, None] * w[None, :, None, None]
+    f = orc.dss(rho * orc.geometry(0, 6) * tgv_rhs_strong(X, Y, Z))
+    udofs = mesh.unique_nodes(n)
+    orc.close()
+    iters_per_step = 2
+    ref = oracle.Reference(mesh, n)
+    times = []
+    for s in range(args.warmup + args.steps):
+        u = np.zeros_like(f)
+        t0 = time.perf_counter()
+        ref.lib().ssgref_fcg_mg(oracle._d(f), oracle._d(u), EPS, iters_per_step)
+        dt = time.perf_counter() - t0
+        if s >= args.warmup:
+            times.append(dt)
+    ref.close()
+    tot = sum(times)
+    value = udofs * iters_per_step * len(times) / tot / 1e9
+    sample = (f"{iters_per_step} FCG+p-MG iterations of the {args.ne}^3 N={n-1} TGV "
+              f"pressure solve per step, reference sources compiled in place, "
+              f"1 process x 1 thread (single-rank, OPENBLAS_NUM_THREADS=1)")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * tot / len(times), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"TGV {args.ne}^3 hex N={n-1} pressure Poisson FCG+p-MG",
+                   "elements": mesh.nel, "n": n, "unique_dofs": udofs},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def run_ours(args):
+    world, rank, local, pg = dist_setup(args)
+    import numpy as np
+    import torch
+    import ssenss_b200 as S
+    from ssenss_b200.mesh import tgv_box
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    mesh = tgv_box(args.ne)
+    n = args.n
+    ctx = S.Context(local)
+    ctx.set_parameters(1e-3, 1.0 / 1600.0, 1.0)
+    ctx.setup_mesh(mesh, n)
+    npts = mesh.nel * n ** 3
+    udofs = mesh.unique_nodes(n)
+    X, Y, Z = (ctx.level_data(0, 12 + a) for a in range(3))
+    bj = ctx.level_data(0, 6)
+    f_host = ctx.direct_stiffness_summation(np.ascontiguousarray(bj * tgv_rhs_strong(X, Y, Z)))
+    lib_stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    f = torch.from_numpy(f_host).to(dev)
+    u = torch.zeros_like(f)
+    torch.cuda.synchronize()
+
+    def barrier():
+        torch.cuda.synchronize()
+        if pg is not None:
+            pg.barrier()
+        torch.cuda.synchronize()
+
+    def timed(fn, k, w):
+        for _ in range(w):
+            fn()
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(lib_stream)
+        out = [fn() for _ in range(k)]
+        e1.record(lib_stream)
+        e1.synchronize()
+        barrier()
+        return e0.elapsed_time(e1), out
+
+    def solve_dev():
+        with torch.cuda.stream(lib_stream):
+            u.zero_()
+        _, info = ctx.solve_poisson_cg(f, u, eps=EPS, history=False)
+        return info
+
+    # ---- FP64 (plain form): device-resident timed region -------------------
+    ctx.set_precision("fp64")
+    clk = Clocks(local)
+    for _ in range(args.warmup):
+        solve_dev()
+    barrier()
+    lc0 = ctx.lib.ssg_kernel_launch_count()
+    clk.start()
+    ms64, infos = timed(solve_dev, args.steps, 0)
+    clocks = clk.stop()
+    launches = ctx.lib.ssg_kernel_launch_count() - lc0
+    u64 = u.cpu().numpy().copy()
+    it64 = sum(i["iterations"] for i in infos)
+    ms64 = max_over_ranks(pg, ms64, dev)
+    dof_it = sum_over_ranks(pg, float(udofs) * it64, dev)
+    value = dof_it / (ms64 * 1e-3) / 1e9
+    solves_s = sum_over_ranks(pg, float(args.steps), dev) / (ms64 * 1e-3)
+
+    # ---- mixed precision ----------------------------------------------------
+    ctx.set_precision("mixed")
+    for _ in range(args.warmup):
+        solve_dev()
+    ms32, infos32 = timed(solve_dev, args.steps, 0)
+    u32 = u.cpu().numpy().copy()
+    it32 = sum(i["iterations"] for i in infos32)
+    ms32 = max_over_ranks(pg, ms32, dev)
+    value32 = sum_over_ranks(pg, float(udofs) * it32, dev) / (ms32 * 1e-3) / 1e9
+    solves32 = sum_over_ranks(pg, float(args.steps), dev) / (ms32 * 1e-3)
+    d64 = u64 - u64.mean()
+    d32 = u32 - u32.mean()
+    err32 = float(np.abs(d32 - d64).max() / np.abs(d64).max())
+    ctx.set_precision("fp64")
+
+    # ---- e2e: public API with pinned host buffers, copies in the region -----
+    fh = torch.from_numpy(f_host).pin_memory()
+    uh = torch.zeros_like(fh).pin_memory()
+
+    def solve_host():
+        uh.zero_()
+        _, info = ctx.solve_poisson_cg(fh, uh, eps=EPS, history=False)
+        return info
+
+    ms_e2e, infos_e = timed(solve_host, max(3, args.steps // 2), 1)
+    ke = max(3, args.steps // 2)
+    ms_e2e = max_over_ranks(pg, ms_e2e, dev)
+    e2e = sum_over_ranks(pg, float(udofs) * sum(i["iterations"] for i in infos_e), dev) / \
+        (ms_e2e * 1e-3) / 1e9
+
+    # ---- roofline of the dominant kernel: level-0 element operator ----------
+    p = torch.randn(mesh.nel, n, n, n, dtype=torch.float64, device=dev)
+    ap = torch.empty_like(p)
+    torch.cuda.synchronize()
+    reps = 50
+    for _ in range(5):
+        ctx.local_opeval(S.PRESSURE, p, ap)
+    op_ms, _ = timed(lambda: ctx.local_opeval(S.PRESSURE, p, ap), reps, 0)
+    op_ms /= reps
+    alg = OP_BYTES_PER_POINT * npts
+    peak, peak_kind = peaks()
+    achieved = alg / (op_ms * 1e-3) / 1e9
+
+    # ---- Helmholtz (velocity) solve, reported beside -------------------------
+    fvel = torch.from_numpy(ctx.direct_stiffness_summation(
+        np.ascontiguousarray(bj * np.sin(X) * np.cos(Y) * np.cos(Z)))).to(dev)
+    uvel = torch.zeros_like(fvel)
+
+    def helm():
+        with torch.cuda.stream(lib_stream):
+            uvel.zero_()
+        _, info = ctx.solve_helmholtz_cg(S.X_VELOCITY, fvel, uvel, eps=EPS, history=False)
+        return info
+
+    hms, hinfo = timed(helm, 5, 1)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            import oracle
+            if oracle.reference_available():
+                secs, its = reference_sample(mesh, n, f_host, int(round(it64 / args.steps)))
+                cpu = {"value": udofs * its / secs / 1e9, "unit": UNIT, "cores": 1,
+                       "kind": "reference",
+                       "sample": (f"{its} FCG+p-MG iterations of the same solve "
+                                  f"(reference sources compiled in place, 1 thread): "
+                                  f"{secs:.1f} s")}
+        except Exception as ex:  # reported, never fatal
+            cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference",
+                   "sample": f"failed: {ex}"}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms64 / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {
+            "workload": (f"TGV {args.ne}^3 hex N={n-1} (n={n}) pressure Poisson, "
+                         f"FCG+p-MG to sqrt((r.r)_w)<=1e-10 from zero"),
+            "elements": mesh.nel, "n": n, "mg_orders": ctx.orders,
+            "unique_dofs": udofs, "local_points": npts,
+            "parallelism": f"replicas x{world}",
+            "l2": "inputs larger than L2 (level-0 factors 100 MB + FCG vectors 420 MB)",
+        },
+        "iterations_per_solve": it64 / args.steps,
+        "solves_per_s": solves_s,
+        "mixed": {"value": value32, "unit": UNIT, "solves_per_s": solves32,
+                  "iterations_per_solve": it32 / args.steps,
+                  "ms_per_step": ms32 / args.steps,
+                  "speedup_solves_vs_fp64": solves32 / solves_s,
+                  "max_rel_diff_vs_fp64": err32},
+        "helmholtz": {"ms_per_solve": hms / 5,
+                      "iterations": hinfo[0]["iterations"]},
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 2 * 8 * npts,
+                "d2h_bytes_per_step": 8 * npts, "ms_per_step": ms_e2e / ke},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": OP_TRAFFIC_BYTES,
+                     "kernel": "k_ax<8,double> (level-0 Laplacian)",
+                     "us_per_launch": op_ms * 1e3,
+                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"},
+        "cpu_baseline": cpu,
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+    }
+    ctx.close()
+    if rank == 0:
+        print(json.dumps(line))
+    if pg is not None:
+        pg.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -213,6 +213,12 @@ ssg_status ssg_multigrid_preconditioner(ssg_context *ctx, const double *r,
 ssg_status ssg_convection_operator(ssg_context *ctx, const double *u,
 		const double *v, double *udv);
 
+/* ---- instrumentation -------------------------------------------------------- */
+
+/* Number of this library's kernel launches in the process so far (all
+ * contexts). */
+unsigned long long ssg_kernel_launch_count(void);
+
 /* ---- particles -------------------------------------------------------------- */
 
 /* Reference-domain velocity snapshots the particles see (sel->ur and its two

@@ -60,9 +60,8 @@ static void dfree(void* p) {
 
 static void free_level(ssg::DevLevel& d) {
   dfree(d.gf); dfree(d.bj); dfree(d.kdiag); dfree(d.dinv_p); dfree(d.dinv_h);
-  dfree(d.scale); dfree(d.mask); dfree(d.D); dfree(d.S); dfree(d.Ar); dfree(d.Ap);
-  dfree(d.gf32); dfree(d.dinv_p32); dfree(d.scale32); dfree(d.D32); dfree(d.Ar32);
-  dfree(d.Ap32);
+  dfree(d.mult); dfree(d.mask); dfree(d.D); dfree(d.S); dfree(d.Ar); dfree(d.Ap);
+  dfree(d.gf32); dfree(d.dinv_p32);
   d = ssg::DevLevel();
 }
 
@@ -138,7 +137,11 @@ static ssg_status upload_all(ssg_context* c) {
     SSG_TRY(dupload(c, &d.dinv_p, dp.data(), np));
     SSG_TRY(dalloc(c, &d.dinv_h, np));
     d.lambda_h = -1.0;
-    SSG_TRY(dupload(c, &d.scale, sc.data(), np));
+    {
+      std::vector<uint8_t> mu(np);
+      for (size_t q = 0; q < np; ++q) mu[q] = (uint8_t)std::lround(1.0 / sc[q]);
+      SSG_TRY(dupload(c, &d.mult, mu.data(), np));
+    }
     if (c->has_walls) {
       std::vector<double> mk(np, 1.0);
       const int n = h.n;
@@ -159,8 +162,6 @@ static ssg_status upload_all(ssg_context* c) {
     SSG_TRY(dupload(c, &d.S, h.S.data(), h.S.size()));
     SSG_TRY(upload_f32(c, &d.gf32, gf.data(), gf.size()));
     SSG_TRY(upload_f32(c, &d.dinv_p32, dp.data(), np));
-    SSG_TRY(upload_f32(c, &d.scale32, sc.data(), np));
-    SSG_TRY(upload_f32(c, &d.D32, h.D.data(), h.D.size()));
     if (l >= 1) {
       const int nf = H.lev[l - 1].n, nc = h.n;
       std::vector<double> Ar((size_t)nc * nf);
@@ -168,8 +169,6 @@ static ssg_status upload_all(ssg_context* c) {
         for (int p = 0; p < nc; ++p) Ar[p * nf + i] = h.jf[i * nc + p];
       SSG_TRY(dupload(c, &d.Ar, Ar.data(), Ar.size()));
       SSG_TRY(dupload(c, &d.Ap, h.jf.data(), h.jf.size()));
-      SSG_TRY(upload_f32(c, &d.Ar32, Ar.data(), Ar.size()));
-      SSG_TRY(upload_f32(c, &d.Ap32, h.jf.data(), h.jf.size()));
     }
     if (l == 0) {
       std::vector<double> im(bj);
@@ -493,9 +492,12 @@ ssg_status ssg_level_data(ssg_context* c, int level, int which, double* dst) {
   else if (which == 8) {
     SSG_TRY(helmholtz_diag_update(c));
     src = d.dinv_h;
-  } else if (which == 9)
-    src = d.scale;
-  else if (which == 10) {
+  } else if (which == 9) {
+    std::vector<uint8_t> mu(np);
+    SSG_CUDA(c, cudaMemcpy(mu.data(), d.mult, np, cudaMemcpyDeviceToHost));
+    for (size_t q = 0; q < np; ++q) dst[q] = 1.0 / (double)mu[q];
+    return SSG_OK;
+  } else if (which == 10) {
     if (d.mask)
       src = d.mask;
     else {
@@ -564,7 +566,7 @@ ssg_status ssg_global_dot_product(ssg_context* c, const double* x, const double*
   const int nb = vec_blocks(np);
   PtrList pl;
   pl.p[0] = dy;
-  SSG_CUDA(c, run_dots(c->stream, false, np, dx, pl, 1, c->lev[0].scale, c->d_part, nb));
+  SSG_CUDA(c, run_dots(c->stream, false, np, dx, pl, 1, c->lev[0].mult, c->d_part, nb));
   ScalarOp op;
   SSG_CUDA(c, run_reduce(c->stream, c->d_part, nb, 1, c->d_sums, op));
   SSG_CUDA(c, cudaMemcpyAsync(c->h_pin, c->d_sums, sizeof(double), cudaMemcpyDeviceToHost,

@@ -1,6 +1,13 @@
 // Element operators, direct stiffness summation, transfers and fused vector
 // kernels of the SSENSS solve path, for sm_100a.
 //
+// Precision: fields and factors are stored as T (double, or float inside the
+// mixed-precision V-cycle); every kernel computes in FP64 and rounds only on
+// store.  (Derivatives of smooth fields taken in FP32 arithmetic lose digits
+// in proportion to the operator's condition number; FP32 storage of the
+// metric factors is a relative perturbation of the quadratic form and does
+// not.)
+//
 // Local operator (discrete_laplace_operator / discrete_helmholtz_operator,
 // src/poisson.c:34-56, src/helmholtz.c:33-49):
 //   A_e u = D^T (rho J G . D u)  [+ lambda rho J u]
@@ -11,9 +18,11 @@
 // DSS (direct_stiffness_summation, src/global.c:241-257): each local node
 // adds its neighbours' pre-sum copies in the reference's order (faces w, e,
 // s, n, b, t; edges sw..tn; corners 0..7) from the pairing built on the host
-// (src/init.c:68-130), accumulating in FP64: the result is bitwise equal to
-// the reference's for FP64 data.
+// (src/init.c:68-130), accumulating in FP64: for FP64 data the result is
+// bitwise equal to the reference's.
 #include <cuda_runtime.h>
+
+#include <cstdint>
 #include <cstdio>
 
 #include "kernels.cuh"
@@ -24,24 +33,33 @@ namespace ssg {
 namespace dev {
 
 // ---------------------------------------------------------------------------
-// local operator
+// local operator, optionally preceded by the CG direction update
+//   p = ((beta p + (z - c)) .* mask)   (first: p = (z - c) .* mask)
+// (src/solver.c:59-60,75-77 with subtract_nullspace folded in)
 // ---------------------------------------------------------------------------
-template <int N, typename T, bool HELM>
-__global__ void __launch_bounds__(256, 2) k_ax(int nel, const T* __restrict__ u,
-                                             T* __restrict__ au,
-                                             const T* __restrict__ gf,
-                                             size_t npts,
-                                             const T* __restrict__ bj,
-                                             const T* __restrict__ Dg,
-                                             const T* __restrict__ Sg,
-                                             T lambda) {
+struct PUpdate {
+  const void* z = nullptr;        // T*
+  const double* beta = nullptr;
+  const double* c = nullptr;      // nullspace constant (pressure) or null
+  const double* mask = nullptr;
+  int first = 0;
+};
+
+template <int N, typename T, bool HELM, bool FUSEP>
+__global__ void __launch_bounds__(256, 2) k_ax(int nel, T* __restrict__ u,
+                                               T* __restrict__ au,
+                                               const T* __restrict__ gf, size_t npts,
+                                               const double* __restrict__ bj,
+                                               const double* __restrict__ Dg,
+                                               const double* __restrict__ Sg,
+                                               double lambda, PUpdate pu) {
   constexpr int NN = N * N, NNN = N * N * N, P = N + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* sD = reinterpret_cast<T*>(smem_raw);
-  T* sS = sD + N * P;
-  T* su = sS + N * P + threadIdx.z * 3 * NNN;
-  T* sw0 = su + NNN;
-  T* sw1 = sw0 + NNN;
+  double* sD = reinterpret_cast<double*>(smem_raw);
+  double* sS = sD + N * P;
+  double* su = sS + N * P + threadIdx.z * 3 * NNN;
+  double* sw0 = su + NNN;
+  double* sw1 = sw0 + NNN;
   const int i = threadIdx.x, j = threadIdx.y;
   const int tid = i + N * (j + N * threadIdx.z);
   const int nthr = NN * blockDim.z;
@@ -52,17 +70,38 @@ __global__ void __launch_bounds__(256, 2) k_ax(int nel, const T* __restrict__ u,
   const int e = blockIdx.x * blockDim.z + threadIdx.z;
   const bool active = e < nel;
   const size_t off = (size_t)(active ? e : 0) * NNN + j * N + i;
-  T ru[N], rw2[N];
+  double ru[N], rw2[N];
+  if (FUSEP) {
+    const T* z = reinterpret_cast<const T*>(pu.z);
+    const double beta = pu.first ? 0.0 : *pu.beta;
+    const double c = pu.c ? *pu.c : 0.0;
 #pragma unroll
-  for (int k = 0; k < N; ++k) {
-    ru[k] = active ? u[off + k * NN] : T(0);
-    su[k * NN + j * N + i] = ru[k];
+    for (int k = 0; k < N; ++k) {
+      double v = 0.0;
+      if (active) {
+        const size_t o = off + (size_t)k * NN;
+        const double zc = (double)z[o] - c;
+        v = pu.first ? zc : beta * (double)u[o] + zc;
+        if (pu.mask) v = v * pu.mask[o];
+        const T vt = (T)v;
+        u[o] = vt;
+        v = (double)vt;
+      }
+      ru[k] = v;
+      su[k * NN + j * N + i] = v;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+      ru[k] = active ? (double)u[off + (size_t)k * NN] : 0.0;
+      su[k * NN + j * N + i] = ru[k];
+    }
   }
   __syncthreads();
-  const T* Dx = sS;   // r-derivative: S for Helmholtz, D otherwise
+  const double* Dx = sS;   // r-derivative: S for Helmholtz, D otherwise
 #pragma unroll
   for (int k = 0; k < N; ++k) {
-    T ur = 0, us = 0, ut = 0;
+    double ur = 0, us = 0, ut = 0;
 #pragma unroll
     for (int m = 0; m < N; ++m) {
       ur += Dx[i * P + m] * su[k * NN + j * N + m];
@@ -70,14 +109,14 @@ __global__ void __launch_bounds__(256, 2) k_ax(int nel, const T* __restrict__ u,
       ut += sD[k * P + m] * ru[m];
     }
     const size_t o = off + (size_t)k * NN;
-    T g0 = 0, g1 = 0, g2 = 0, g3 = 0, g4 = 0, g5 = 0;
+    double g0 = 0, g1 = 0, g2 = 0, g3 = 0, g4 = 0, g5 = 0;
     if (active) {
-      g0 = __ldg(gf + o);
-      g1 = __ldg(gf + npts + o);
-      g2 = __ldg(gf + 2 * npts + o);
-      g3 = __ldg(gf + 3 * npts + o);
-      g4 = __ldg(gf + 4 * npts + o);
-      g5 = __ldg(gf + 5 * npts + o);
+      g0 = (double)__ldg(gf + o);
+      g1 = (double)__ldg(gf + npts + o);
+      g2 = (double)__ldg(gf + 2 * npts + o);
+      g3 = (double)__ldg(gf + 3 * npts + o);
+      g4 = (double)__ldg(gf + 4 * npts + o);
+      g5 = (double)__ldg(gf + 5 * npts + o);
     }
     sw0[k * NN + j * N + i] = g0 * ur + g1 * us + g2 * ut;
     sw1[k * NN + j * N + i] = g1 * ur + g3 * us + g4 * ut;
@@ -87,106 +126,102 @@ __global__ void __launch_bounds__(256, 2) k_ax(int nel, const T* __restrict__ u,
   // transposed derivatives: r with D, s and t with S (= D for Poisson)
 #pragma unroll
   for (int k = 0; k < N; ++k) {
-    T acc = 0, acs = 0, act = 0;
+    double acc = 0, acs = 0, act = 0;
 #pragma unroll
     for (int m = 0; m < N; ++m) {
       acc += sD[m * P + i] * sw0[k * NN + j * N + m];
       acs += sS[m * P + j] * sw1[k * NN + m * N + i];
       act += sS[m * P + k] * rw2[m];
     }
-    T out = (acc + acs) + act;
+    double out = (acc + acs) + act;
     if (HELM && active) out += lambda * (__ldg(bj + off + (size_t)k * NN) * ru[k]);
-    if (active) au[off + (size_t)k * NN] = out;
+    if (active) au[off + (size_t)k * NN] = (T)out;
   }
 }
 
 // ---------------------------------------------------------------------------
 // DSS gather with fused epilogues
-// ---------------------------------------------------------------------------
-template <typename T>
-__device__ __forceinline__ double ld_masked(const T* in, const double* mask,
-                                            size_t idx) {
-  double v = (double)in[idx];
-  if (mask) v = v * mask[idx];
-  return v;
-}
-
-// out = DSS(mask .* in) then, by MODE:
-//   DSS_PLAIN: store
+//   DSS_PLAIN: out = DSS(mask .* in)
 //   DSS_DOT:   store; partial sum (y w) out                       [1]
 //   DSS_DOT2:  store; partial sums (y w) out, (y w) y2            [2]
 //   DSS_RESID: out = y - DSS; partial sum w out                   [1]
 //   DSS_AVG:   out = DSS * w (direct_stiffness_averaging)
 // w = 1 / multiplicity = 1 / (1 + number of contributions).
-template <typename T, int MODE>
-__global__ void __launch_bounds__(256) k_dss(int n, int nel, int epb,
-                                             const T* __restrict__ in,
+// ---------------------------------------------------------------------------
+template <int N, typename T, int MODE>
+__global__ void __launch_bounds__(256) k_dss(int nel, int epb, const T* __restrict__ in,
                                              T* __restrict__ out,
                                              const int2* __restrict__ pairs,
                                              const double* __restrict__ mask,
                                              const T* __restrict__ y,
                                              const T* __restrict__ y2,
                                              double* __restrict__ part) {
+  constexpr int NT = N * N * N, M = N - 1;
   __shared__ int2 sp[64 * 26];
   __shared__ double sred[2 * 32];
-  const int nt = n * n * n;
   const int e0 = blockIdx.x * epb;
   const int ne = min(epb, nel - e0);
-  for (int q = threadIdx.x; q < ne * 26; q += blockDim.x)
-    sp[q] = pairs[(size_t)e0 * 26 + q];
+  for (int q = threadIdx.x; q < ne * 26; q += blockDim.x) sp[q] = pairs[(size_t)e0 * 26 + q];
   __syncthreads();
   double s0 = 0.0, s1 = 0.0;
-  const int m = n - 1;
-  for (int q = threadIdx.x; q < ne * nt; q += blockDim.x) {
-    const int z = q / nt, loc = q - z * nt;
-    const int i = loc % n, j = (loc / n) % n, k = loc / (n * n);
-    const size_t gi = (size_t)(e0 + z) * nt + loc;
+  for (int q = threadIdx.x; q < ne * NT; q += blockDim.x) {
+    const int z = q / NT, loc = q - z * NT;
+    const int i = loc % N, j = (loc / N) % N, k = loc / (N * N);
+    const size_t gi = (size_t)(e0 + z) * NT + loc;
     const int2* pr = sp + z * 26;
-    double acc = ld_masked(in, mask, gi);
+    double acc = (double)in[gi];
+    if (mask) acc = acc * mask[gi];
     int cnt = 0;
-#define SSG_ADD(PR, NODE)                                              \
-  {                                                                     \
-    const int2 p_ = (PR);                                               \
-    if (p_.x >= 0) {                                                    \
-      acc += ld_masked(in, mask, (size_t)p_.x * nt + (NODE));           \
-      ++cnt;                                                            \
-    }                                                                   \
+    const bool ei = i == 0 || i == M, ej = j == 0 || j == M, ek = k == 0 || k == M;
+    if (ei || ej || ek) {
+#define SSG_ADD(PR, NODE)                                                \
+  {                                                                       \
+    const int2 p_ = (PR);                                                 \
+    if (p_.x >= 0) {                                                      \
+      const size_t s_ = (size_t)p_.x * NT + (NODE);                       \
+      double v_ = (double)in[s_];                                         \
+      if (mask) v_ = v_ * mask[s_];                                       \
+      acc += v_;                                                          \
+      ++cnt;                                                              \
+    }                                                                     \
   }
-    if (i == 0) SSG_ADD(pr[0], face_node(n, pr[0].y, k, j));
-    if (i == m) SSG_ADD(pr[1], face_node(n, pr[1].y, k, j));
-    if (j == 0) SSG_ADD(pr[2], face_node(n, pr[2].y, k, i));
-    if (j == m) SSG_ADD(pr[3], face_node(n, pr[3].y, k, i));
-    if (k == 0) SSG_ADD(pr[4], face_node(n, pr[4].y, j, i));
-    if (k == m) SSG_ADD(pr[5], face_node(n, pr[5].y, j, i));
-    if (i == 0 && j == 0) SSG_ADD(pr[6], edge_node(n, pr[6].y, k));
-    if (i == m && j == 0) SSG_ADD(pr[7], edge_node(n, pr[7].y, k));
-    if (i == 0 && j == m) SSG_ADD(pr[8], edge_node(n, pr[8].y, k));
-    if (i == m && j == m) SSG_ADD(pr[9], edge_node(n, pr[9].y, k));
-    if (k == 0 && i == 0) SSG_ADD(pr[10], edge_node(n, pr[10].y, j));
-    if (k == 0 && i == m) SSG_ADD(pr[11], edge_node(n, pr[11].y, j));
-    if (k == m && i == 0) SSG_ADD(pr[12], edge_node(n, pr[12].y, j));
-    if (k == m && i == m) SSG_ADD(pr[13], edge_node(n, pr[13].y, j));
-    if (k == 0 && j == 0) SSG_ADD(pr[14], edge_node(n, pr[14].y, i));
-    if (k == 0 && j == m) SSG_ADD(pr[15], edge_node(n, pr[15].y, i));
-    if (k == m && j == 0) SSG_ADD(pr[16], edge_node(n, pr[16].y, i));
-    if (k == m && j == m) SSG_ADD(pr[17], edge_node(n, pr[17].y, i));
-    if ((i == 0 || i == m) && (j == 0 || j == m) && (k == 0 || k == m)) {
-      const int c = (i == m) | ((j == m) << 1) | ((k == m) << 2);
-      SSG_ADD(pr[18 + c], corner_node(n, pr[18 + c].y));
-    }
+      if (i == 0) SSG_ADD(pr[0], face_node(N, pr[0].y, k, j));
+      if (i == M) SSG_ADD(pr[1], face_node(N, pr[1].y, k, j));
+      if (j == 0) SSG_ADD(pr[2], face_node(N, pr[2].y, k, i));
+      if (j == M) SSG_ADD(pr[3], face_node(N, pr[3].y, k, i));
+      if (k == 0) SSG_ADD(pr[4], face_node(N, pr[4].y, j, i));
+      if (k == M) SSG_ADD(pr[5], face_node(N, pr[5].y, j, i));
+      if (ei && ej) {
+        const int q4 = (i == M) | ((j == M) << 1);
+        SSG_ADD(pr[6 + q4], edge_node(N, pr[6 + q4].y, k));
+      }
+      if (ek && ei) {
+        const int q4 = (i == M) | ((k == M) << 1);
+        SSG_ADD(pr[10 + q4], edge_node(N, pr[10 + q4].y, j));
+      }
+      if (ek && ej) {
+        const int q4 = (j == M) | ((k == M) << 1);
+        SSG_ADD(pr[14 + q4], edge_node(N, pr[14 + q4].y, i));
+      }
+      if (ei && ej && ek) {
+        const int c = (i == M) | ((j == M) << 1) | ((k == M) << 2);
+        SSG_ADD(pr[18 + c], corner_node(N, pr[18 + c].y));
+      }
 #undef SSG_ADD
+    }
     const double w = 1.0 / (1.0 + (double)cnt);
     if (MODE == DSS_RESID) {
-      const double r = (double)y[gi] + -acc;
-      out[gi] = (T)r;
-      s0 += (double)(T)r * w;
+      const T r = (T)((double)y[gi] + -acc);
+      out[gi] = r;
+      s0 += (double)r * w;
     } else if (MODE == DSS_AVG) {
       out[gi] = (T)(acc * w);
     } else {
-      out[gi] = (T)acc;
+      const T a = (T)acc;
+      out[gi] = a;
       if (MODE == DSS_DOT || MODE == DSS_DOT2) {
         const double yw = (double)y[gi] * w;
-        s0 += yw * (double)(T)acc;
+        s0 += yw * (double)a;
         if (MODE == DSS_DOT2) s1 += yw * (double)y2[gi];
       }
     }
@@ -204,51 +239,55 @@ __global__ void __launch_bounds__(256) k_dss(int n, int nel, int epb,
 // ---------------------------------------------------------------------------
 // tensor-product transfer between orders, stages in x, y, z order
 // (interpolate_to_grid / integrate_to_grid, src/interpolation.c:136-176):
-// out (no^3) [+]= (A x A x A) in (ni^3), A[o*ni + q]
+// out (no^3) [+]= (A x A x A) in (ni^3), A[o*ni + q] in FP64
 // ---------------------------------------------------------------------------
 template <typename T, bool ADD>
 __global__ void __launch_bounds__(256) k_tensor3(int nel, int ni, int no,
-                                                 const T* __restrict__ A,
+                                                 const double* __restrict__ A,
                                                  const T* __restrict__ in,
                                                  T* __restrict__ out) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* sA = reinterpret_cast<T*>(smem_raw);
-  T* sin = sA + no * ni;
-  T* t1 = sin + ni * ni * ni;
-  T* t2 = t1 + no * ni * ni;
+  double* sA = reinterpret_cast<double*>(smem_raw);
+  double* sin = sA + no * ni;
+  double* t1 = sin + ni * ni * ni;
+  double* t2 = t1 + no * ni * ni;
   const int e = blockIdx.x;
   const int nti = ni * ni * ni, nto = no * no * no;
   for (int q = threadIdx.x; q < no * ni; q += blockDim.x) sA[q] = A[q];
-  for (int q = threadIdx.x; q < nti; q += blockDim.x) sin[q] = in[(size_t)e * nti + q];
+  for (int q = threadIdx.x; q < nti; q += blockDim.x) sin[q] = (double)in[(size_t)e * nti + q];
   __syncthreads();
   for (int q = threadIdx.x; q < no * ni * ni; q += blockDim.x) {
     const int o = q % no, kj = q / no;
-    T s = 0;
+    double s = 0;
     for (int r = 0; r < ni; ++r) s += sA[o * ni + r] * sin[kj * ni + r];
     t1[q] = s;
   }
   __syncthreads();
   for (int q = threadIdx.x; q < no * no * ni; q += blockDim.x) {
     const int o1 = q % no, o2 = (q / no) % no, k = q / (no * no);
-    T s = 0;
+    double s = 0;
     for (int r = 0; r < ni; ++r) s += sA[o2 * ni + r] * t1[(k * ni + r) * no + o1];
     t2[q] = s;
   }
   __syncthreads();
   for (int q = threadIdx.x; q < nto; q += blockDim.x) {
     const int o12 = q % (no * no), o3 = q / (no * no);
-    T s = 0;
+    double s = 0;
     for (int r = 0; r < ni; ++r) s += sA[o3 * ni + r] * t2[r * no * no + o12];
+    const size_t g = (size_t)e * nto + q;
     if (ADD)
-      out[(size_t)e * nto + q] += s;
+      out[g] = (T)((double)out[g] + s);
     else
-      out[(size_t)e * nto + q] = s;
+      out[g] = (T)s;
   }
 }
 
 // ---------------------------------------------------------------------------
 // fused vector kernels (grid-stride, 256 threads, one partial per block)
 // ---------------------------------------------------------------------------
+#define SSG_GRID_LOOP(q, n)                                                    \
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < (n);     \
+       q += (size_t)gridDim.x * blockDim.x)
 
 // CG step after ap is known (src/solver.c:66-71):
 //   x += alpha p; r -= alpha ap; z = dinv .* r
@@ -256,25 +295,22 @@ __global__ void __launch_bounds__(256) k_tensor3(int nel, int ni, int no,
 template <typename T>
 __global__ void __launch_bounds__(256) k_cg_update(size_t npts,
                                                    const double* __restrict__ alpha_p,
-                                                   T* __restrict__ x,
-                                                   const T* __restrict__ p,
-                                                   T* __restrict__ r,
-                                                   const T* __restrict__ ap,
+                                                   T* __restrict__ x, const T* __restrict__ p,
+                                                   T* __restrict__ r, const T* __restrict__ ap,
                                                    const T* __restrict__ dinv,
-                                                   const T* __restrict__ scale,
+                                                   const uint8_t* __restrict__ mult,
                                                    T* __restrict__ z,
                                                    double* __restrict__ part) {
   __shared__ double sred[4 * 32];
-  const T alpha = (T)*alpha_p;
+  const double alpha = *alpha_p;
   double v[4] = {0.0, 0.0, 0.0, 0.0};
-  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < npts;
-       q += (size_t)gridDim.x * blockDim.x) {
-    x[q] = x[q] + alpha * p[q];
-    const T rq = r[q] + -alpha * ap[q];
+  SSG_GRID_LOOP(q, npts) {
+    x[q] = (T)((double)x[q] + alpha * (double)p[q]);
+    const T rq = (T)((double)r[q] + -alpha * (double)ap[q]);
     r[q] = rq;
-    const T zq = rq * dinv[q];
+    const T zq = (T)((double)rq * (double)dinv[q]);
     z[q] = zq;
-    const double w = (double)scale[q];
+    const double w = 1.0 / (double)mult[q];
     const double rw = (double)rq * w;
     v[0] += rw * (double)zq;
     v[1] += rw * (double)rq;
@@ -288,40 +324,18 @@ __global__ void __launch_bounds__(256) k_cg_update(size_t npts,
   }
 }
 
-// p = (beta p + (z - c)) .* mask; first iteration p = z - c
-// (src/solver.c:59-60,75-77 with subtract_nullspace folded in)
-template <typename T>
-__global__ void __launch_bounds__(256) k_p_update(size_t npts, const double* __restrict__ beta_p,
-                                                  const double* __restrict__ c_p,
-                                                  T* __restrict__ p,
-                                                  const T* __restrict__ z,
-                                                  const double* __restrict__ mask,
-                                                  int first) {
-  const T beta = first ? T(0) : (T)*beta_p;
-  const T c = c_p ? (T)*c_p : T(0);
-  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < npts;
-       q += (size_t)gridDim.x * blockDim.x) {
-    const T zc = z[q] - c;
-    T v = first ? zc : beta * p[q] + zc;
-    if (mask) v = v * (T)mask[q];
-    p[q] = v;
-  }
-}
-
 // z = dinv .* r; partial w.z (Jacobi preconditioner, src/precon.c:311-324)
 template <typename T>
 __global__ void __launch_bounds__(256) k_jacobi(size_t npts, const T* __restrict__ r,
                                                 const T* __restrict__ dinv,
-                                                const T* __restrict__ scale,
-                                                T* __restrict__ z,
-                                                double* __restrict__ part) {
+                                                const uint8_t* __restrict__ mult,
+                                                T* __restrict__ z, double* __restrict__ part) {
   __shared__ double sred[32];
   double v[1] = {0.0};
-  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < npts;
-       q += (size_t)gridDim.x * blockDim.x) {
-    const T zq = r[q] * dinv[q];
+  SSG_GRID_LOOP(q, npts) {
+    const T zq = (T)((double)r[q] * (double)dinv[q]);
     z[q] = zq;
-    v[0] += (double)scale[q] * (double)zq;
+    v[0] += (double)zq * (1.0 / (double)mult[q]);
   }
   block_reduce<1>(v, sred);
   if (threadIdx.x == 0) part[blockIdx.x] = v[0];
@@ -329,16 +343,15 @@ __global__ void __launch_bounds__(256) k_jacobi(size_t npts, const T* __restrict
 
 // partial sums of (x w) y_k, k < K (up to 10 vectors)
 template <typename T, int K>
-__global__ void __launch_bounds__(256) k_dots(size_t npts, const T* __restrict__ x,
-                                              PtrList ys, const T* __restrict__ scale,
+__global__ void __launch_bounds__(256) k_dots(size_t npts, const T* __restrict__ x, PtrList ys,
+                                              const uint8_t* __restrict__ mult,
                                               double* __restrict__ part) {
   __shared__ double sred[K * 32];
   double v[K];
 #pragma unroll
   for (int k = 0; k < K; ++k) v[k] = 0.0;
-  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < npts;
-       q += (size_t)gridDim.x * blockDim.x) {
-    const double xw = (double)x[q] * (double)scale[q];
+  SSG_GRID_LOOP(q, npts) {
+    const double xw = (double)x[q] * (1.0 / (double)mult[q]);
 #pragma unroll
     for (int k = 0; k < K; ++k) v[k] += xw * (double)((const T*)ys.p[k])[q];
   }
@@ -352,93 +365,71 @@ __global__ void __launch_bounds__(256) k_dots(size_t npts, const T* __restrict__
 // partial sums of w x (the nullspace component, src/solver.c:200-213)
 template <typename T>
 __global__ void __launch_bounds__(256) k_wsum(size_t npts, const T* __restrict__ x,
-                                              const T* __restrict__ scale,
+                                              const uint8_t* __restrict__ mult,
                                               double* __restrict__ part) {
   __shared__ double sred[32];
   double v[1] = {0.0};
-  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < npts;
-       q += (size_t)gridDim.x * blockDim.x)
-    v[0] += (double)x[q] * (double)scale[q];
+  SSG_GRID_LOOP(q, npts) v[0] += (double)x[q] * (1.0 / (double)mult[q]);
   block_reduce<1>(v, sred);
   if (threadIdx.x == 0) part[blockIdx.x] = v[0];
 }
 
-// x += a_k y_k for k < K with a_k = sign * coef[k] read on the device;
-// optional subtraction of a device constant c first: x = (x - c) + ...
-template <typename T>
-__global__ void __launch_bounds__(256) k_combine(size_t npts, T* __restrict__ x,
-                                                 PtrList ys,
-                                                 const double* __restrict__ coef,
-                                                 int K, double sign,
-                                                 const double* __restrict__ c_p,
-                                                 const double* __restrict__ mask) {
-  const double c = c_p ? *c_p : 0.0;
-  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < npts;
-       q += (size_t)gridDim.x * blockDim.x) {
-    T v = x[q];
-    if (c_p) v = v - (T)c;
-    for (int k = 0; k < K; ++k) v = v + (T)(sign * coef[k]) * ((const T*)ys.p[k])[q];
-    if (mask) v = v * (T)mask[q];
+// x = x + sum_k (sign coef_k) y_k   (FCG direction, FP64)
+__global__ void __launch_bounds__(256) k_combine(size_t npts, double* __restrict__ x, PtrList ys,
+                                                 const double* __restrict__ coef, int K,
+                                                 double sign) {
+  SSG_GRID_LOOP(q, npts) {
+    double v = x[q];
+    for (int k = 0; k < K; ++k) v = v + (sign * coef[k]) * ((const double*)ys.p[k])[q];
     x[q] = v;
   }
 }
 
 // u += alpha p; r -= alpha ap; partial (r w).r   (src/solver.c:148-152)
-__global__ void __launch_bounds__(256) k_fcg_update(size_t npts,
-                                                    const double* __restrict__ alpha_p,
+__global__ void __launch_bounds__(256) k_fcg_update(size_t npts, const double* __restrict__ alpha_p,
                                                     double* __restrict__ u,
                                                     const double* __restrict__ p,
                                                     double* __restrict__ r,
                                                     const double* __restrict__ ap,
-                                                    const double* __restrict__ scale,
+                                                    const uint8_t* __restrict__ mult,
                                                     double* __restrict__ part) {
   __shared__ double sred[32];
   const double alpha = *alpha_p;
   double v[1] = {0.0};
-  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < npts;
-       q += (size_t)gridDim.x * blockDim.x) {
+  SSG_GRID_LOOP(q, npts) {
     u[q] = u[q] + alpha * p[q];
     const double rq = r[q] + -alpha * ap[q];
     r[q] = rq;
-    v[0] += (rq * scale[q]) * rq;
+    v[0] += (rq * (1.0 / (double)mult[q])) * rq;
   }
   block_reduce<1>(v, sred);
   if (threadIdx.x == 0) part[blockIdx.x] = v[0];
 }
 
-// y = x + a (a device constant, negated when neg)
 template <typename T>
 __global__ void __launch_bounds__(256) k_add_const(size_t npts, T* __restrict__ x,
-                                                   const double* __restrict__ a_p,
-                                                   int neg) {
-  const T a = (T)(neg ? -*a_p : *a_p);
-  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < npts;
-       q += (size_t)gridDim.x * blockDim.x)
-    x[q] = x[q] + a;
+                                                   const double* __restrict__ a_p, int neg) {
+  const double a = neg ? -*a_p : *a_p;
+  SSG_GRID_LOOP(q, npts) x[q] = (T)((double)x[q] + a);
 }
 
 template <typename TI, typename TO>
 __global__ void __launch_bounds__(256) k_convert(size_t npts, const TI* __restrict__ in,
                                                  TO* __restrict__ out) {
-  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < npts;
-       q += (size_t)gridDim.x * blockDim.x)
-    out[q] = (TO)in[q];
+  SSG_GRID_LOOP(q, npts) out[q] = (TO)in[q];
 }
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_mul(size_t npts, T* __restrict__ x,
                                              const double* __restrict__ y) {
-  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < npts;
-       q += (size_t)gridDim.x * blockDim.x)
-    x[q] = x[q] * (T)y[q];
+  SSG_GRID_LOOP(q, npts) x[q] = (T)((double)x[q] * y[q]);
 }
 
 // ---------------------------------------------------------------------------
 // deterministic reduction of block partials + solver scalar algebra
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_reduce(const double* __restrict__ part,
-                                                int nblk, int nq,
-                                                double* __restrict__ sums,
+__global__ void __launch_bounds__(256) k_reduce(const double* __restrict__ part, int nblk,
+                                                int nq, double* __restrict__ sums,
                                                 ScalarOp op) {
   __shared__ double sred[32];
   for (int q = 0; q < nq; ++q) {
@@ -515,45 +506,48 @@ __global__ void __launch_bounds__(256) k_reduce(const double* __restrict__ part,
 // ---------------------------------------------------------------------------
 using namespace dev;
 
+static unsigned long long g_launches = 0;   // every launch below bumps it
+#define SSG_COUNT() (++g_launches)
+
 int vec_blocks(size_t npts) {
   size_t b = (npts + 255) / 256;
   const size_t cap = 148 * 8;
   return (int)(b < cap ? (b ? b : 1) : cap);
 }
 
-int ax_epb(int n, bool fp32) {
-  // elements per block: at least 64 threads, at most 1024, <= 96 KB smem
-  const size_t bytes = fp32 ? 4 : 8;
+int ax_epb(int n) {
+  // elements per block: up to 256 threads, <= 96 KB of FP64 shared memory
   int epb = 1;
-  while (epb * 2 * n * n <= 256 && (size_t)(epb * 2) * 3 * n * n * n * bytes <= 96 * 1024)
-    epb *= 2;
+  while (epb * 2 * n * n <= 256 && (size_t)(epb * 2) * 3 * n * n * n * 8 <= 96 * 1024) epb *= 2;
   return epb;
 }
 
-template <int N, typename T, bool HELM>
-static cudaError_t launch_ax_t(cudaStream_t s, int nel, int epb, const T* u, T* au,
-                               const T* gf, size_t npts, const T* bj, const T* D,
-                               const T* S, T lambda) {
-  const size_t smem = (2 * N * (N + 1) + (size_t)epb * 3 * N * N * N) * sizeof(T);
+template <int N, typename T, bool HELM, bool FUSEP>
+static cudaError_t launch_ax_t(cudaStream_t s, int nel, int epb, T* u, T* au, const T* gf,
+                               size_t npts, const double* bj, const double* D,
+                               const double* S, double lambda, const PUpdate& pu) {
+  const size_t smem = (2 * N * (N + 1) + (size_t)epb * 3 * N * N * N) * sizeof(double);
   static bool attr_set = false;
   if (!attr_set) {
-    cudaFuncSetAttribute(k_ax<N, T, HELM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(k_ax<N, T, HELM, FUSEP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          200 * 1024);
     attr_set = true;
   }
   dim3 blk(N, N, epb);
   dim3 grd((nel + epb - 1) / epb);
-  k_ax<N, T, HELM><<<grd, blk, smem, s>>>(nel, u, au, gf, npts, bj, D, S, lambda);
+  { SSG_COUNT(); k_ax<N, T, HELM, FUSEP><<<grd, blk, smem, s>>>(nel, u, au, gf, npts, bj, D, S, lambda, pu); }
   return cudaGetLastError();
 }
 
-template <typename T, bool HELM>
-static cudaError_t ax_dispatch(int n, cudaStream_t s, int nel, int epb, const T* u, T* au,
-                               const T* gf, size_t npts, const T* bj, const T* D,
-                               const T* S, T lambda) {
+template <typename T, bool HELM, bool FUSEP>
+static cudaError_t ax_dispatch(int n, cudaStream_t s, int nel, int epb, T* u, T* au,
+                               const T* gf, size_t npts, const double* bj, const double* D,
+                               const double* S, double lambda, const PUpdate& pu) {
   switch (n) {
-#define SSG_AXN(NV) \
-  case NV: return launch_ax_t<NV, T, HELM>(s, nel, epb, u, au, gf, npts, bj, D, S, lambda);
+#define SSG_AXN(NV)                                                                   \
+  case NV:                                                                            \
+    return launch_ax_t<NV, T, HELM, FUSEP>(s, nel, epb, u, au, gf, npts, bj, D, S,    \
+                                           lambda, pu);
     SSG_AXN(2) SSG_AXN(3) SSG_AXN(4) SSG_AXN(5) SSG_AXN(6) SSG_AXN(7)
     SSG_AXN(8) SSG_AXN(9) SSG_AXN(10) SSG_AXN(11) SSG_AXN(12)
 #undef SSG_AXN
@@ -563,26 +557,44 @@ static cudaError_t ax_dispatch(int n, cudaStream_t s, int nel, int epb, const T*
 
 cudaError_t run_ax(cudaStream_t s, int n, int nel, int epb, bool helm, bool fp32,
                    const void* in, void* out, const void* gf, size_t npts,
-                   const double* bj, const void* D, const void* S, double lambda) {
-  if (epb <= 0) epb = ax_epb(n, fp32);
-  if (fp32) {
-    return ax_dispatch<float, false>(n, s, nel, epb, (const float*)in, (float*)out,
-                                     (const float*)gf, npts, nullptr, (const float*)D,
-                                     (const float*)D, 0.0f);
+                   const double* bj, const double* D, const double* S, double lambda,
+                   const PUpdateArgs* pua) {
+  if (epb <= 0) epb = ax_epb(n);
+  PUpdate pu;
+  const bool fuse = pua != nullptr;
+  if (fuse) {
+    pu.z = pua->z;
+    pu.beta = pua->beta;
+    pu.c = pua->c;
+    pu.mask = pua->mask;
+    pu.first = pua->first;
   }
-  if (helm)
-    return ax_dispatch<double, true>(n, s, nel, epb, (const double*)in, (double*)out,
-                                     (const double*)gf, npts, bj, (const double*)D,
-                                     (const double*)S, lambda);
-  return ax_dispatch<double, false>(n, s, nel, epb, (const double*)in, (double*)out,
-                                    (const double*)gf, npts, nullptr, (const double*)D,
-                                    (const double*)D, 0.0);
+  if (fp32) {
+    if (helm) return cudaErrorInvalidValue;
+    if (fuse)
+      return ax_dispatch<float, false, true>(n, s, nel, epb, (float*)in, (float*)out,
+                                             (const float*)gf, npts, nullptr, D, D, 0.0, pu);
+    return ax_dispatch<float, false, false>(n, s, nel, epb, (float*)in, (float*)out,
+                                            (const float*)gf, npts, nullptr, D, D, 0.0, pu);
+  }
+  if (helm) {
+    if (fuse)
+      return ax_dispatch<double, true, true>(n, s, nel, epb, (double*)in, (double*)out,
+                                             (const double*)gf, npts, bj, D, S, lambda, pu);
+    return ax_dispatch<double, true, false>(n, s, nel, epb, (double*)in, (double*)out,
+                                            (const double*)gf, npts, bj, D, S, lambda, pu);
+  }
+  if (fuse)
+    return ax_dispatch<double, false, true>(n, s, nel, epb, (double*)in, (double*)out,
+                                            (const double*)gf, npts, nullptr, D, D, 0.0, pu);
+  return ax_dispatch<double, false, false>(n, s, nel, epb, (double*)in, (double*)out,
+                                           (const double*)gf, npts, nullptr, D, D, 0.0, pu);
 }
 
 int dss_epb(int n) {
   const int nt = n * n * n;
   int epb = 1;
-  while (epb * 2 <= 64 && epb * 2 * nt <= 1024) epb *= 2;
+  while (epb * 2 <= 64 && epb * nt < 256) epb *= 2;
   return epb;
 }
 
@@ -591,33 +603,47 @@ int dss_grid(int n, int nel) {
   return (nel + epb - 1) / epb;
 }
 
-template <typename T>
-static cudaError_t run_dss_t(cudaStream_t s, int mode, int n, int nel, const T* in, T* out,
-                             const int* pairs, const double* mask, const T* y,
-                             const T* y2, double* part) {
-  const int epb = dss_epb(n);
+template <int N, typename T>
+static cudaError_t run_dss_n(cudaStream_t s, int mode, int nel, const T* in, T* out,
+                             const int2* pr, const double* mask, const T* y, const T* y2,
+                             double* part) {
+  const int epb = dss_epb(N);
   const int grd = (nel + epb - 1) / epb;
-  const int2* pr = reinterpret_cast<const int2*>(pairs);
   switch (mode) {
     case DSS_PLAIN:
-      k_dss<T, DSS_PLAIN><<<grd, 256, 0, s>>>(n, nel, epb, in, out, pr, mask, y, y2, part);
+      { SSG_COUNT(); k_dss<N, T, DSS_PLAIN><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, mask, y, y2, part); }
       break;
     case DSS_DOT:
-      k_dss<T, DSS_DOT><<<grd, 256, 0, s>>>(n, nel, epb, in, out, pr, mask, y, y2, part);
+      { SSG_COUNT(); k_dss<N, T, DSS_DOT><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, mask, y, y2, part); }
       break;
     case DSS_DOT2:
-      k_dss<T, DSS_DOT2><<<grd, 256, 0, s>>>(n, nel, epb, in, out, pr, mask, y, y2, part);
+      { SSG_COUNT(); k_dss<N, T, DSS_DOT2><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, mask, y, y2, part); }
       break;
     case DSS_RESID:
-      k_dss<T, DSS_RESID><<<grd, 256, 0, s>>>(n, nel, epb, in, out, pr, mask, y, y2, part);
+      { SSG_COUNT(); k_dss<N, T, DSS_RESID><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, mask, y, y2, part); }
       break;
     case DSS_AVG:
-      k_dss<T, DSS_AVG><<<grd, 256, 0, s>>>(n, nel, epb, in, out, pr, mask, y, y2, part);
+      { SSG_COUNT(); k_dss<N, T, DSS_AVG><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, mask, y, y2, part); }
       break;
     default:
       return cudaErrorInvalidValue;
   }
   return cudaGetLastError();
+}
+
+template <typename T>
+static cudaError_t run_dss_t(cudaStream_t s, int mode, int n, int nel, const T* in, T* out,
+                             const int* pairs, const double* mask, const T* y, const T* y2,
+                             double* part) {
+  const int2* pr = reinterpret_cast<const int2*>(pairs);
+  switch (n) {
+#define SSG_DSSN(NV) \
+  case NV: return run_dss_n<NV, T>(s, mode, nel, in, out, pr, mask, y, y2, part);
+    SSG_DSSN(2) SSG_DSSN(3) SSG_DSSN(4) SSG_DSSN(5) SSG_DSSN(6) SSG_DSSN(7)
+    SSG_DSSN(8) SSG_DSSN(9) SSG_DSSN(10) SSG_DSSN(11) SSG_DSSN(12)
+#undef SSG_DSSN
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 cudaError_t run_dss(cudaStream_t s, int mode, bool fp32, int n, int nel, const void* in,
@@ -631,77 +657,58 @@ cudaError_t run_dss(cudaStream_t s, int mode, bool fp32, int n, int nel, const v
 }
 
 cudaError_t run_tensor3(cudaStream_t s, bool fp32, bool add, int nel, int ni, int no,
-                        const void* A, const void* in, void* out) {
-  const size_t bytes = fp32 ? 4 : 8;
+                        const double* A, const void* in, void* out) {
   const size_t smem = ((size_t)no * ni + (size_t)ni * ni * ni + (size_t)no * ni * ni +
-                       (size_t)no * no * ni) * bytes;
+                       (size_t)no * no * ni) * sizeof(double);
   if (fp32) {
     if (add)
-      k_tensor3<float, true><<<nel, 256, smem, s>>>(nel, ni, no, (const float*)A,
-                                                    (const float*)in, (float*)out);
+      { SSG_COUNT(); k_tensor3<float, true><<<nel, 256, smem, s>>>(nel, ni, no, A, (const float*)in, (float*)out); }
     else
-      k_tensor3<float, false><<<nel, 256, smem, s>>>(nel, ni, no, (const float*)A,
-                                                     (const float*)in, (float*)out);
+      { SSG_COUNT(); k_tensor3<float, false><<<nel, 256, smem, s>>>(nel, ni, no, A, (const float*)in, (float*)out); }
   } else {
     if (add)
-      k_tensor3<double, true><<<nel, 256, smem, s>>>(nel, ni, no, (const double*)A,
-                                                     (const double*)in, (double*)out);
+      { SSG_COUNT(); k_tensor3<double, true><<<nel, 256, smem, s>>>(nel, ni, no, A, (const double*)in,
+                                                     (double*)out); }
     else
-      k_tensor3<double, false><<<nel, 256, smem, s>>>(nel, ni, no, (const double*)A,
-                                                      (const double*)in, (double*)out);
+      { SSG_COUNT(); k_tensor3<double, false><<<nel, 256, smem, s>>>(nel, ni, no, A, (const double*)in,
+                                                      (double*)out); }
   }
   return cudaGetLastError();
 }
 
 cudaError_t run_cg_update(cudaStream_t s, bool fp32, size_t npts, const double* alpha,
-                          void* x, const void* p, void* r, const void* ap,
-                          const void* dinv, const void* scale, void* z, double* part,
-                          int nblk) {
+                          void* x, const void* p, void* r, const void* ap, const void* dinv,
+                          const uint8_t* mult, void* z, double* part, int nblk) {
   if (fp32)
-    k_cg_update<float><<<nblk, 256, 0, s>>>(npts, alpha, (float*)x, (const float*)p,
-                                            (float*)r, (const float*)ap,
-                                            (const float*)dinv, (const float*)scale,
-                                            (float*)z, part);
+    { SSG_COUNT(); k_cg_update<float><<<nblk, 256, 0, s>>>(npts, alpha, (float*)x, (const float*)p, (float*)r,
+                                            (const float*)ap, (const float*)dinv, mult,
+                                            (float*)z, part); }
   else
-    k_cg_update<double><<<nblk, 256, 0, s>>>(npts, alpha, (double*)x, (const double*)p,
+    { SSG_COUNT(); k_cg_update<double><<<nblk, 256, 0, s>>>(npts, alpha, (double*)x, (const double*)p,
                                              (double*)r, (const double*)ap,
-                                             (const double*)dinv, (const double*)scale,
-                                             (double*)z, part);
+                                             (const double*)dinv, mult, (double*)z, part); }
   return cudaGetLastError();
 }
 
-cudaError_t run_p_update(cudaStream_t s, bool fp32, size_t npts, const double* beta,
-                         const double* c, void* p, const void* z, const double* mask,
-                         int first) {
-  const int nblk = vec_blocks(npts);
+cudaError_t run_jacobi(cudaStream_t s, bool fp32, size_t npts, const void* r, const void* dinv,
+                       const uint8_t* mult, void* z, double* part, int nblk) {
   if (fp32)
-    k_p_update<float><<<nblk, 256, 0, s>>>(npts, beta, c, (float*)p, (const float*)z, mask,
-                                           first);
+    { SSG_COUNT(); k_jacobi<float><<<nblk, 256, 0, s>>>(npts, (const float*)r, (const float*)dinv, mult,
+                                         (float*)z, part); }
   else
-    k_p_update<double><<<nblk, 256, 0, s>>>(npts, beta, c, (double*)p, (const double*)z,
-                                            mask, first);
-  return cudaGetLastError();
-}
-
-cudaError_t run_jacobi(cudaStream_t s, bool fp32, size_t npts, const void* r,
-                       const void* dinv, const void* scale, void* z, double* part,
-                       int nblk) {
-  if (fp32)
-    k_jacobi<float><<<nblk, 256, 0, s>>>(npts, (const float*)r, (const float*)dinv,
-                                         (const float*)scale, (float*)z, part);
-  else
-    k_jacobi<double><<<nblk, 256, 0, s>>>(npts, (const double*)r, (const double*)dinv,
-                                          (const double*)scale, (double*)z, part);
+    { SSG_COUNT(); k_jacobi<double><<<nblk, 256, 0, s>>>(npts, (const double*)r, (const double*)dinv, mult,
+                                          (double*)z, part); }
   return cudaGetLastError();
 }
 
 template <typename T>
-static cudaError_t run_dots_t(cudaStream_t s, size_t npts, const T* x, const PtrList& ys,
-                              int K, const T* scale, double* part, int nblk) {
+static cudaError_t run_dots_t(cudaStream_t s, size_t npts, const T* x, const PtrList& ys, int K,
+                              const uint8_t* mult, double* part, int nblk) {
   switch (K) {
-#define SSG_DOTK(KV)                                                        \
-  case KV:                                                                  \
-    k_dots<T, KV><<<nblk, 256, 0, s>>>(npts, x, ys, scale, part);           \
+#define SSG_DOTK(KV)                                                   \
+  case KV:                                                             \
+    SSG_COUNT();                                                       \
+    k_dots<T, KV><<<nblk, 256, 0, s>>>(npts, x, ys, mult, part);       \
     break;
     SSG_DOTK(1) SSG_DOTK(2) SSG_DOTK(3) SSG_DOTK(4) SSG_DOTK(5)
     SSG_DOTK(6) SSG_DOTK(7) SSG_DOTK(8) SSG_DOTK(9) SSG_DOTK(10)
@@ -712,43 +719,40 @@ static cudaError_t run_dots_t(cudaStream_t s, size_t npts, const T* x, const Ptr
   return cudaGetLastError();
 }
 
-cudaError_t run_dots(cudaStream_t s, bool fp32, size_t npts, const void* x,
-                     const PtrList& ys, int K, const void* scale, double* part, int nblk) {
-  if (fp32)
-    return run_dots_t<float>(s, npts, (const float*)x, ys, K, (const float*)scale, part, nblk);
-  return run_dots_t<double>(s, npts, (const double*)x, ys, K, (const double*)scale, part,
-                            nblk);
+cudaError_t run_dots(cudaStream_t s, bool fp32, size_t npts, const void* x, const PtrList& ys,
+                     int K, const uint8_t* mult, double* part, int nblk) {
+  if (fp32) return run_dots_t<float>(s, npts, (const float*)x, ys, K, mult, part, nblk);
+  return run_dots_t<double>(s, npts, (const double*)x, ys, K, mult, part, nblk);
 }
 
 cudaError_t run_wsum(cudaStream_t s, bool fp32, size_t npts, const void* x,
-                     const void* scale, double* part, int nblk) {
+                     const uint8_t* mult, double* part, int nblk) {
   if (fp32)
-    k_wsum<float><<<nblk, 256, 0, s>>>(npts, (const float*)x, (const float*)scale, part);
+    { SSG_COUNT(); k_wsum<float><<<nblk, 256, 0, s>>>(npts, (const float*)x, mult, part); }
   else
-    k_wsum<double><<<nblk, 256, 0, s>>>(npts, (const double*)x, (const double*)scale, part);
+    { SSG_COUNT(); k_wsum<double><<<nblk, 256, 0, s>>>(npts, (const double*)x, mult, part); }
   return cudaGetLastError();
 }
 
 cudaError_t run_combine(cudaStream_t s, size_t npts, double* x, const PtrList& ys,
-                        const double* coef, int K, double sign, const double* c,
-                        const double* mask) {
-  k_combine<double><<<vec_blocks(npts), 256, 0, s>>>(npts, x, ys, coef, K, sign, c, mask);
+                        const double* coef, int K, double sign) {
+  { SSG_COUNT(); k_combine<<<vec_blocks(npts), 256, 0, s>>>(npts, x, ys, coef, K, sign); }
   return cudaGetLastError();
 }
 
 cudaError_t run_fcg_update(cudaStream_t s, size_t npts, const double* alpha, double* u,
-                           const double* p, double* r, const double* ap,
-                           const double* scale, double* part, int nblk) {
-  k_fcg_update<<<nblk, 256, 0, s>>>(npts, alpha, u, p, r, ap, scale, part);
+                           const double* p, double* r, const double* ap, const uint8_t* mult,
+                           double* part, int nblk) {
+  { SSG_COUNT(); k_fcg_update<<<nblk, 256, 0, s>>>(npts, alpha, u, p, r, ap, mult, part); }
   return cudaGetLastError();
 }
 
-cudaError_t run_add_const(cudaStream_t s, bool fp32, size_t npts, void* x,
-                          const double* a, int neg) {
+cudaError_t run_add_const(cudaStream_t s, bool fp32, size_t npts, void* x, const double* a,
+                          int neg) {
   if (fp32)
-    k_add_const<float><<<vec_blocks(npts), 256, 0, s>>>(npts, (float*)x, a, neg);
+    { SSG_COUNT(); k_add_const<float><<<vec_blocks(npts), 256, 0, s>>>(npts, (float*)x, a, neg); }
   else
-    k_add_const<double><<<vec_blocks(npts), 256, 0, s>>>(npts, (double*)x, a, neg);
+    { SSG_COUNT(); k_add_const<double><<<vec_blocks(npts), 256, 0, s>>>(npts, (double*)x, a, neg); }
   return cudaGetLastError();
 }
 
@@ -756,28 +760,30 @@ cudaError_t run_convert(cudaStream_t s, size_t npts, const void* in, bool in32, 
                         bool out32) {
   const int nb = vec_blocks(npts);
   if (in32 && !out32)
-    k_convert<float, double><<<nb, 256, 0, s>>>(npts, (const float*)in, (double*)out);
+    { SSG_COUNT(); k_convert<float, double><<<nb, 256, 0, s>>>(npts, (const float*)in, (double*)out); }
   else if (!in32 && out32)
-    k_convert<double, float><<<nb, 256, 0, s>>>(npts, (const double*)in, (float*)out);
+    { SSG_COUNT(); k_convert<double, float><<<nb, 256, 0, s>>>(npts, (const double*)in, (float*)out); }
   else if (in32)
-    k_convert<float, float><<<nb, 256, 0, s>>>(npts, (const float*)in, (float*)out);
+    { SSG_COUNT(); k_convert<float, float><<<nb, 256, 0, s>>>(npts, (const float*)in, (float*)out); }
   else
-    k_convert<double, double><<<nb, 256, 0, s>>>(npts, (const double*)in, (double*)out);
+    { SSG_COUNT(); k_convert<double, double><<<nb, 256, 0, s>>>(npts, (const double*)in, (double*)out); }
   return cudaGetLastError();
 }
 
 cudaError_t run_mul(cudaStream_t s, bool fp32, size_t npts, void* x, const double* y) {
   if (fp32)
-    k_mul<float><<<vec_blocks(npts), 256, 0, s>>>(npts, (float*)x, y);
+    { SSG_COUNT(); k_mul<float><<<vec_blocks(npts), 256, 0, s>>>(npts, (float*)x, y); }
   else
-    k_mul<double><<<vec_blocks(npts), 256, 0, s>>>(npts, (double*)x, y);
+    { SSG_COUNT(); k_mul<double><<<vec_blocks(npts), 256, 0, s>>>(npts, (double*)x, y); }
   return cudaGetLastError();
 }
 
 cudaError_t run_reduce(cudaStream_t s, const double* part, int nblk, int nq, double* sums,
                        const ScalarOp& op) {
-  k_reduce<<<1, 256, 0, s>>>(part, nblk, nq, sums, op);
+  { SSG_COUNT(); k_reduce<<<1, 256, 0, s>>>(part, nblk, nq, sums, op); }
   return cudaGetLastError();
 }
 
 }  // namespace ssg
+
+extern "C" unsigned long long ssg_kernel_launch_count(void) { return ssg::g_launches; }

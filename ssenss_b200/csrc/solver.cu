@@ -94,8 +94,8 @@ ssg_status op_apply(ssg_context* c, int level, int var, bool fp32, const void* i
     return fail(c, SSG_ERR_ARG, "the Helmholtz operator is FP64 at level 0 only");
   void* loc = global ? (fp32 ? c->ws->w32[level].aploc : c->ws->w64[level].aploc) : out;
   SSG_CUDA(c, run_ax(c->stream, L.n, c->nel, 0, helm, fp32, in, loc,
-                     fp32 ? (const void*)L.gf32 : (const void*)L.gf, L.npts, L.bj,
-                     fp32 ? (const void*)L.D32 : (const void*)L.D, L.S, lambda_of(c)));
+                     fp32 ? (const void*)L.gf32 : (const void*)L.gf, L.npts, L.bj, L.D, L.S,
+                     lambda_of(c), nullptr));
   if (global)
     SSG_CUDA(c, run_dss(c->stream, DSS_PLAIN, fp32, L.n, c->nel, loc, out, c->d_pairs,
                         helm ? L.mask : nullptr, nullptr, nullptr, nullptr));
@@ -126,9 +126,7 @@ ssg_status cg_solve(ssg_context* c, int level, int var, bool fp32, void* f, void
   double* fr = c->d_sc + frame * F_SIZE;
   const void* dinv = helm ? (const void*)L.dinv_h
                           : (fp32 ? (const void*)L.dinv_p32 : (const void*)L.dinv_p);
-  const void* scale = fp32 ? (const void*)L.scale32 : (const void*)L.scale;
   const void* gf = fp32 ? (const void*)L.gf32 : (const void*)L.gf;
-  const void* D = fp32 ? (const void*)L.D32 : (const void*)L.D;
   const double lam = lambda_of(c);
   cudaStream_t s = c->stream;
   ScalarOp op;
@@ -142,7 +140,8 @@ ssg_status cg_solve(ssg_context* c, int level, int var, bool fp32, void* f, void
 
   // mask f; r = f - A x; subtract_nullspace(r)
   if (mask) SSG_CUDA(c, run_mul(s, fp32, np, f, mask));
-  SSG_CUDA(c, run_ax(s, L.n, c->nel, 0, helm, fp32, x, W.aploc, gf, np, L.bj, D, L.S, lam));
+  SSG_CUDA(c, run_ax(s, L.n, c->nel, 0, helm, fp32, x, W.aploc, gf, np, L.bj, L.D, L.S, lam,
+                     nullptr));
   SSG_CUDA(c, run_dss(s, DSS_RESID, fp32, L.n, c->nel, W.aploc, W.r, c->d_pairs, mask, f,
                       nullptr, c->d_part));
   if (pres) {
@@ -150,35 +149,40 @@ ssg_status cg_solve(ssg_context* c, int level, int var, bool fp32, void* f, void
     SSG_CUDA(c, run_reduce(s, c->d_part, nbd, 1, c->d_sums, op));
     SSG_CUDA(c, run_add_const(s, fp32, np, W.r, fr + F_C, 1));
   }
-  // z = M^-1 r; subtract_nullspace(z); p = z; rdz = (r w).z
-  SSG_CUDA(c, run_jacobi(s, fp32, np, W.r, dinv, scale, W.z, c->d_part, nb));
+  // z = M^-1 r and its nullspace constant
+  SSG_CUDA(c, run_jacobi(s, fp32, np, W.r, dinv, L.mult, W.z, c->d_part, nb));
   op.code = OP_CG_INIT_C;
   SSG_CUDA(c, run_reduce(s, c->d_part, nb, 1, c->d_sums, op));
-  SSG_CUDA(c, run_p_update(s, fp32, np, nullptr, pres ? fr + F_C : nullptr, W.p, W.z,
-                           mask, 1));
-  PtrList ys;
-  ys.p[0] = W.p;
-  ys.p[1] = W.r;
-  SSG_CUDA(c, run_dots(s, fp32, np, W.r, ys, 2, scale, c->d_part, nb));
-  op.code = OP_CG_INIT_RDZ;
-  SSG_CUDA(c, run_reduce(s, c->d_part, nb, 2, c->d_sums, op));
 
+  PUpdateArgs pu;
+  pu.z = W.z;
+  pu.beta = fr + F_BETA;
+  pu.c = pres ? fr + F_C : nullptr;
+  pu.mask = mask;
   for (int it = 0; it < max_iter; ++it) {
-    // ap = DSS(mask A p); alpha = rdz / (p w).ap
-    SSG_CUDA(c, run_ax(s, L.n, c->nel, 0, helm, fp32, W.p, W.aploc, gf, np, L.bj, D, L.S,
-                       lam));
+    // p = beta p + (z - c) (first: p = z - c), masked; aploc = A p
+    pu.first = it == 0;
+    SSG_CUDA(c, run_ax(s, L.n, c->nel, 0, helm, fp32, W.p, W.aploc, gf, np, L.bj, L.D, L.S,
+                       lam, &pu));
+    if (it == 0) {
+      // rdz = (r w).p, |r|_w (src/solver.c:58-61)
+      PtrList ys;
+      ys.p[0] = W.p;
+      ys.p[1] = W.r;
+      SSG_CUDA(c, run_dots(s, fp32, np, W.r, ys, 2, L.mult, c->d_part, nb));
+      op.code = OP_CG_INIT_RDZ;
+      SSG_CUDA(c, run_reduce(s, c->d_part, nb, 2, c->d_sums, op));
+    }
+    // ap = DSS(mask aploc); alpha = rdz / (p w).ap
     SSG_CUDA(c, run_dss(s, DSS_DOT, fp32, L.n, c->nel, W.aploc, W.ap, c->d_pairs, mask,
                         W.p, nullptr, c->d_part));
     op.code = OP_CG_ALPHA;
     SSG_CUDA(c, run_reduce(s, c->d_part, nbd, 1, c->d_sums, op));
     // x += alpha p; r -= alpha ap; z = M^-1 r; beta; err
-    SSG_CUDA(c, run_cg_update(s, fp32, np, fr + F_ALPHA, x, W.p, W.r, W.ap, dinv, scale,
+    SSG_CUDA(c, run_cg_update(s, fp32, np, fr + F_ALPHA, x, W.p, W.r, W.ap, dinv, L.mult,
                               W.z, c->d_part, nb));
     op.code = OP_CG_BETA;
     SSG_CUDA(c, run_reduce(s, c->d_part, nb, 4, c->d_sums, op));
-    // p = beta p + (z - c); mask
-    SSG_CUDA(c, run_p_update(s, fp32, np, fr + F_BETA, pres ? fr + F_C : nullptr, W.p, W.z,
-                             mask, 0));
     if (sync_each) {
       double done;
       SSG_TRY(read_flag(c, fr + F_DONE, &done));
@@ -223,22 +227,22 @@ static ssg_status mg_recurse(ssg_context* c, int L, void* f, void* x, double eps
   if (L == 0) {
     // r = f - A x (compute_residual, src/precon.c:302-309)
     SSG_CUDA(c, run_ax(s, F.n, c->nel, 0, false, fp32, x, W.aploc,
-                       fp32 ? (const void*)F.gf32 : (const void*)F.gf, F.npts, nullptr,
-                       fp32 ? (const void*)F.D32 : (const void*)F.D, nullptr, 0.0));
+                       fp32 ? (const void*)F.gf32 : (const void*)F.gf, F.npts, nullptr, F.D,
+                       F.D, 0.0, nullptr));
     SSG_CUDA(c, run_dss(s, DSS_RESID, fp32, F.n, c->nel, W.aploc, W.rr, c->d_pairs, nullptr,
                         f, nullptr, c->d_part));
     rin = W.rr;
   }
   // restriction: (J^T)^3 then DSS-average at the coarse level
   SSG_CUDA(c, run_tensor3(s, fp32, false, c->nel, F.n, C.n,
-                          fp32 ? (const void*)C.Ar32 : (const void*)C.Ar, rin, Wc.tc));
+                          C.Ar, rin, Wc.tc));
   SSG_CUDA(c, run_dss(s, DSS_AVG, fp32, C.n, c->nel, Wc.tc, Wc.f, c->d_pairs, nullptr,
                       nullptr, nullptr, nullptr));
   SSG_CUDA(c, cudaMemsetAsync(Wc.x, 0, C.npts * (fp32 ? sizeof(float) : sizeof(double)), s));
   SSG_TRY(mg_recurse(c, L + 1, Wc.f, Wc.x, eps, fp32));
   // prolongation J^3 and x += e
   SSG_CUDA(c, run_tensor3(s, fp32, true, c->nel, C.n, F.n,
-                          fp32 ? (const void*)C.Ap32 : (const void*)C.Ap, Wc.x, x));
+                          C.Ap, Wc.x, x));
   // post-smoothing: CG-Jacobi, 15 iterations, stop at eps
   ssg_status st = cg_solve(c, L, SSG_PRESSURE, fp32, f, x, eps, 15, FR_LEVEL0 + L, nullptr,
                            0, true);
@@ -262,7 +266,7 @@ ssg_status mg_apply(ssg_context* c, const double* r, double* z, double eps) {
     SSG_CUDA(c, run_convert(s, np, r, false, f0, true));
   }
   SSG_CUDA(c, run_jacobi(s, fp32, np, f0, fp32 ? (const void*)L.dinv_p32 : (const void*)L.dinv_p,
-                         fp32 ? (const void*)L.scale32 : (const void*)L.scale, x0, c->d_part,
+                         L.mult, x0, c->d_part,
                          nb));
   if (c->nlev > 1) SSG_TRY(mg_recurse(c, 0, f0, x0, eps, fp32));
   if (fp32) SSG_CUDA(c, run_convert(s, np, x0, true, z, false));
@@ -293,7 +297,7 @@ ssg_status fcg_solve(ssg_context* c, const double* f, double* u, double eps, int
 
   // r = f - A u; subtract_nullspace(r)
   SSG_CUDA(c, run_ax(s, L.n, c->nel, 0, false, false, u, w->aploc, L.gf, np, nullptr, L.D,
-                     nullptr, 0.0));
+                     L.D, 0.0, nullptr));
   SSG_CUDA(c, run_dss(s, DSS_RESID, false, L.n, c->nel, w->aploc, w->r, c->d_pairs, nullptr,
                       f, nullptr, c->d_part));
   op.code = OP_NULL_C;
@@ -301,7 +305,7 @@ ssg_status fcg_solve(ssg_context* c, const double* f, double* u, double eps, int
   SSG_CUDA(c, run_add_const(s, false, np, w->r, fr + F_C, 1));
   PtrList ys;
   ys.p[0] = w->r;
-  SSG_CUDA(c, run_dots(s, false, np, w->r, ys, 1, L.scale, c->d_part, nb));
+  SSG_CUDA(c, run_dots(s, false, np, w->r, ys, 1, L.mult, c->d_part, nb));
   op.code = OP_ERR0;
   SSG_CUDA(c, run_reduce(s, c->d_part, nb, 1, c->d_sums, op));
 
@@ -314,7 +318,7 @@ ssg_status fcg_solve(ssg_context* c, const double* f, double* u, double eps, int
     m = std::min(m, j);
     SSG_TRY(mg_apply(c, w->r, w->z, eps));
     // subtract_nullspace(z)
-    SSG_CUDA(c, run_wsum(s, false, np, w->z, L.scale, c->d_part, nb));
+    SSG_CUDA(c, run_wsum(s, false, np, w->z, L.mult, c->d_part, nb));
     op.code = OP_NULL_C;
     SSG_CUDA(c, run_reduce(s, c->d_part, nb, 1, c->d_sums, op));
     SSG_CUDA(c, run_add_const(s, false, np, w->z, fr + F_C, 1));
@@ -326,7 +330,7 @@ ssg_status fcg_solve(ssg_context* c, const double* f, double* u, double eps, int
         op.pap_idx[k] = aslot[k];
       }
       op.m = m;
-      SSG_CUDA(c, run_dots(s, false, np, w->z, yb, m, L.scale, c->d_part, nb));
+      SSG_CUDA(c, run_dots(s, false, np, w->z, yb, m, L.mult, c->d_part, nb));
       op.code = OP_FCG_BETA;
       SSG_CUDA(c, run_reduce(s, c->d_part, nb, m, c->d_sums, op));
     }
@@ -339,7 +343,7 @@ ssg_status fcg_solve(ssg_context* c, const double* f, double* u, double eps, int
     if (m > 0) {
       PtrList yp;
       for (int k = 0; k < m; ++k) yp.p[k] = w->P[pslot[k + 1]];
-      SSG_CUDA(c, run_combine(s, np, p0, yp, fr + F_FBETA, m, -1.0, nullptr, nullptr));
+      SSG_CUDA(c, run_combine(s, np, p0, yp, fr + F_FBETA, m, -1.0));
     }
     // shift the ap history
     int m2 = std::max(1, (j + 1) % (mmax + 1));
@@ -350,14 +354,14 @@ ssg_status fcg_solve(ssg_context* c, const double* f, double* u, double eps, int
     double* ap0 = w->AP[aslot[0]];
     // ap0 = A p0; pap0 and alpha = (p0 w).r / pap0
     SSG_CUDA(c, run_ax(s, L.n, c->nel, 0, false, false, p0, w->aploc, L.gf, np, nullptr, L.D,
-                       nullptr, 0.0));
+                       L.D, 0.0, nullptr));
     SSG_CUDA(c, run_dss(s, DSS_DOT2, false, L.n, c->nel, w->aploc, ap0, c->d_pairs, nullptr,
                         p0, w->r, c->d_part));
     op.pap_idx[0] = aslot[0];
     op.code = OP_FCG_ALPHA;
     SSG_CUDA(c, run_reduce(s, c->d_part, nbd, 2, c->d_sums, op));
     // u += alpha p0; r -= alpha ap0; err
-    SSG_CUDA(c, run_fcg_update(s, np, fr + F_ALPHA, u, p0, w->r, ap0, L.scale, c->d_part, nb));
+    SSG_CUDA(c, run_fcg_update(s, np, fr + F_ALPHA, u, p0, w->r, ap0, L.mult, c->d_part, nb));
     op.code = OP_FCG_ERR;
     SSG_CUDA(c, run_reduce(s, c->d_part, nb, 1, c->d_sums, op));
     double done;

@@ -65,7 +65,7 @@ struct DevLevel {
   double* kdiag = nullptr;     // element-local stiffness diagonal
   double* dinv_p = nullptr;    // Poisson Jacobi inverse
   double* dinv_h = nullptr;    // Helmholtz Jacobi inverse (for lambda_h)
-  double* scale = nullptr;     // 1 / multiplicity
+  uint8_t* mult = nullptr;     // multiplicity (1 + DSS contributions)
   double* mask = nullptr;      // Dirichlet mask (null without walls)
   double* D = nullptr;         // n*n
   double* S = nullptr;         // n*n
@@ -73,10 +73,6 @@ struct DevLevel {
   double* Ap = nullptr;        // prolongation from this level: n_finer x n
   float* gf32 = nullptr;       // FP32 copies for the mixed-precision V-cycle
   float* dinv_p32 = nullptr;
-  float* scale32 = nullptr;
-  float* D32 = nullptr;
-  float* Ar32 = nullptr;
-  float* Ap32 = nullptr;
   double nunique = 0.0;        // sum of 1/multiplicity
   double lambda_h = -1.0;      // lambda the Helmholtz diagonal holds
 };

@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 #include <cstddef>
+#include <cstdint>
 
 namespace ssg {
 
@@ -50,40 +51,44 @@ struct PtrList {
 // DSS epilogue modes (kernels.cu)
 enum { DSS_PLAIN = 0, DSS_DOT = 1, DSS_RESID = 2, DSS_AVG = 3, DSS_DOT2 = 4 };
 
+// CG direction update fused into the operator: p = (beta p + (z - c)) .* mask
+struct PUpdateArgs {
+  const void* z = nullptr;
+  const double* beta = nullptr;
+  const double* c = nullptr;
+  const double* mask = nullptr;
+  int first = 0;
+};
+
 int vec_blocks(size_t npts);
-int ax_epb(int n, bool fp32);
+int ax_epb(int n);
 int dss_grid(int n, int nel);
 
 cudaError_t run_ax(cudaStream_t s, int n, int nel, int epb, bool helm, bool fp32,
                    const void* in, void* out, const void* gf, size_t npts,
-                   const double* bj, const void* D, const void* S, double lambda);
+                   const double* bj, const double* D, const double* S, double lambda,
+                   const PUpdateArgs* pua);
 cudaError_t run_dss(cudaStream_t s, int mode, bool fp32, int n, int nel, const void* in,
                     void* out, const int* pairs, const double* mask, const void* y,
                     const void* y2, double* part);
 cudaError_t run_tensor3(cudaStream_t s, bool fp32, bool add, int nel, int ni, int no,
-                        const void* A, const void* in, void* out);
+                        const double* A, const void* in, void* out);
 cudaError_t run_cg_update(cudaStream_t s, bool fp32, size_t npts, const double* alpha,
-                          void* x, const void* p, void* r, const void* ap,
-                          const void* dinv, const void* scale, void* z, double* part,
-                          int nblk);
-cudaError_t run_p_update(cudaStream_t s, bool fp32, size_t npts, const double* beta,
-                         const double* c, void* p, const void* z, const double* mask,
-                         int first);
-cudaError_t run_jacobi(cudaStream_t s, bool fp32, size_t npts, const void* r,
-                       const void* dinv, const void* scale, void* z, double* part,
-                       int nblk);
-cudaError_t run_dots(cudaStream_t s, bool fp32, size_t npts, const void* x,
-                     const PtrList& ys, int K, const void* scale, double* part, int nblk);
+                          void* x, const void* p, void* r, const void* ap, const void* dinv,
+                          const uint8_t* mult, void* z, double* part, int nblk);
+cudaError_t run_jacobi(cudaStream_t s, bool fp32, size_t npts, const void* r, const void* dinv,
+                       const uint8_t* mult, void* z, double* part, int nblk);
+cudaError_t run_dots(cudaStream_t s, bool fp32, size_t npts, const void* x, const PtrList& ys,
+                     int K, const uint8_t* mult, double* part, int nblk);
 cudaError_t run_wsum(cudaStream_t s, bool fp32, size_t npts, const void* x,
-                     const void* scale, double* part, int nblk);
+                     const uint8_t* mult, double* part, int nblk);
 cudaError_t run_combine(cudaStream_t s, size_t npts, double* x, const PtrList& ys,
-                        const double* coef, int K, double sign, const double* c,
-                        const double* mask);
+                        const double* coef, int K, double sign);
 cudaError_t run_fcg_update(cudaStream_t s, size_t npts, const double* alpha, double* u,
-                           const double* p, double* r, const double* ap,
-                           const double* scale, double* part, int nblk);
-cudaError_t run_add_const(cudaStream_t s, bool fp32, size_t npts, void* x,
-                          const double* a, int neg);
+                           const double* p, double* r, const double* ap, const uint8_t* mult,
+                           double* part, int nblk);
+cudaError_t run_add_const(cudaStream_t s, bool fp32, size_t npts, void* x, const double* a,
+                          int neg);
 cudaError_t run_convert(cudaStream_t s, size_t npts, const void* in, bool in32, void* out,
                         bool out32);
 cudaError_t run_mul(cudaStream_t s, bool fp32, size_t npts, void* x, const double* y);
