@@ -180,6 +180,22 @@ ssg_status ssg_direct_stiffness_summation(ssg_context *ctx, double *u);
  * (src/global.c:270-282). */
 ssg_status ssg_global_dot_product(ssg_context *ctx, const double *x,
 		const double *y, double *out);
+/* Weighted inner product sum (x * w) * y over n doubles, the quantity
+ * ssg_global_dot_product computes, from three caller-owned device arrays
+ * (w = 1/multiplicity, as ssg_level_data selector 9 returns it).  The result
+ * is written to the device double *result; the work is enqueued on
+ * cuda_stream (a cudaStream_t, NULL = the default stream) without waiting.
+ * Allocates no device memory, for applications that cannot let a library
+ * call cudaMalloc (a process that hands all device memory to its own pool
+ * under a fixed budget, or a loop that must not take cudaMalloc's implicit
+ * synchronisation).  Its block partial sums live in one fixed 512 KiB array
+ * per GPU shared by every call: n above 134,217,728 is rejected with
+ * SSG_ERR_ARG, host pointers likewise, and calls that overlap on the GPU
+ * race on the array.  The first call on a device looks the array's address
+ * up; make that call before any stream capture on the device.
+ * No counterpart in the reference. */
+ssg_status ssg_weighted_dot_noalloc(const double *x, const double *y,
+		const double *w, size_t n, double *result, void *cuda_stream);
 /* u *= inverse assembled mass -- global_inverse_mass_matrix_operator
  * (src/poisson.c:77-87). */
 ssg_status ssg_inverse_mass(ssg_context *ctx, double *u);

@@ -51,6 +51,8 @@ SIGNATURES = [
     ("ssg_local_opeval", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     ("ssg_direct_stiffness_summation", C.c_int, [C.c_void_p, C.c_void_p]),
     ("ssg_global_dot_product", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, _dp]),
+    ("ssg_weighted_dot_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t,
+                                           C.c_void_p, C.c_void_p]),
     ("ssg_inverse_mass", C.c_int, [C.c_void_p, C.c_void_p]),
     ("ssg_solve_poisson_cg", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
                                        C.c_int, C.POINTER(SolveInfo)]),
