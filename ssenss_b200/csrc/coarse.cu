@@ -1,0 +1,302 @@
+// Coarsest p-multigrid level (n = 2): the whole Jacobi-preconditioned CG
+// solve in one persistent cooperative kernel.
+//
+// The reference solves the coarsest level with conjugate_gradient +
+// jacobi_preconditioner to the absolute eps, at most 500 iterations
+// (src/precon.c:242-244, src/solver.c:33-81).  The level is tiny (8 points
+// per element), so one kernel launch per CG iteration would be pure launch
+// latency; here every iteration runs inside one launch, with grid-wide
+// barriers between the element operator, the DSS and the vector update.
+// Each block reduces the same block partials in the same order, so every
+// block takes the same alpha, beta and stop decision, and the result does
+// not depend on timing.  The loop is bounded by max_iter.
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+
+#include "kernels.cuh"
+#include "ssg_internal.h"
+#include "ssg_kernels.h"
+
+namespace cg = cooperative_groups;
+
+namespace ssg {
+namespace dev {
+
+struct CoarseArgs {
+  int nel = 0;
+  size_t npts = 0;
+  const double* f = nullptr;
+  double* x = nullptr;
+  double *r = nullptr, *z = nullptr, *p = nullptr, *aploc = nullptr, *ap = nullptr;
+  const double* gf = nullptr;     // 6 x npts
+  const double* D = nullptr;      // 2 x 2, D[i*2+m]
+  const double* dinv = nullptr;
+  const uint8_t* mult = nullptr;
+  const int2* pairs = nullptr;
+  double nunique = 1.0;
+  double eps = 0.0;
+  int max_iter = 0;
+  double* partA = nullptr;        // >= 4 * gridDim.x
+  double* partB = nullptr;        // >= 3 * gridDim.x
+  double* frame = nullptr;
+};
+
+// A_e u for one n = 2 element (8 points), same contraction order as k_ax
+__device__ __forceinline__ void elem_op2(const CoarseArgs& a, const double* sD, const double* u8,
+                                         double* out8, size_t e) {
+  double w0[8], w1[8], w2[8];
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    const int i = q & 1, j = (q >> 1) & 1, k = q >> 2;
+    double ur = 0, us = 0, ut = 0;
+#pragma unroll
+    for (int m = 0; m < 2; ++m) {
+      ur += sD[i * 2 + m] * u8[(k * 2 + j) * 2 + m];
+      us += sD[j * 2 + m] * u8[(k * 2 + m) * 2 + i];
+      ut += sD[k * 2 + m] * u8[(m * 2 + j) * 2 + i];
+    }
+    const size_t o = e * 8 + q;
+    const double g0 = a.gf[o], g1 = a.gf[a.npts + o], g2 = a.gf[2 * a.npts + o],
+                 g3 = a.gf[3 * a.npts + o], g4 = a.gf[4 * a.npts + o],
+                 g5 = a.gf[5 * a.npts + o];
+    w0[q] = g0 * ur + g1 * us + g2 * ut;
+    w1[q] = g1 * ur + g3 * us + g4 * ut;
+    w2[q] = g2 * ur + g4 * us + g5 * ut;
+  }
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    const int i = q & 1, j = (q >> 1) & 1, k = q >> 2;
+    double acc = 0, acs = 0, act = 0;
+#pragma unroll
+    for (int m = 0; m < 2; ++m) {
+      acc += sD[m * 2 + i] * w0[(k * 2 + j) * 2 + m];
+      acs += sD[m * 2 + j] * w1[(k * 2 + m) * 2 + i];
+      act += sD[m * 2 + k] * w2[(m * 2 + j) * 2 + i];
+    }
+    out8[q] = (acc + acs) + act;
+  }
+}
+
+// sum over all blocks of NQ partial arrays, identical in every block
+template <int NQ>
+__device__ __forceinline__ void grid_sums(const double* part, int G, double (&s)[NQ],
+                                          double* sred, double* sbc) {
+  double v[NQ];
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+    v[q] = 0.0;
+    for (int b = threadIdx.x; b < G; b += blockDim.x) v[q] += part[q * G + b];
+  }
+  block_reduce<NQ>(v, sred);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) sbc[q] = v[q];
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) s[q] = sbc[q];
+  __syncthreads();
+}
+
+template <int NQ>
+__device__ __forceinline__ void block_partials(double (&v)[NQ], double* part, double* sred) {
+  block_reduce<NQ>(v, sred);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) part[q * gridDim.x + blockIdx.x] = v[q];
+}
+
+__global__ void __launch_bounds__(256) k_coarse_cg(CoarseArgs a) {
+  cg::grid_group grid = cg::this_grid();
+  __shared__ double sred[4 * 32];
+  __shared__ double sbc[4];
+  __shared__ double sD[4];
+  if (threadIdx.x < 4) sD[threadIdx.x] = a.D[threadIdx.x];
+  __syncthreads();
+  const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t nthr = (size_t)gridDim.x * blockDim.x;
+  const int G = gridDim.x;
+
+  // r = f - DSS(A x); nullspace of r (src/solver.c:49-53)
+  for (size_t e = tid; e < (size_t)a.nel; e += nthr) {
+    double u8[8], o8[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) u8[q] = a.x[e * 8 + q];
+    elem_op2(a, sD, u8, o8, e);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) a.aploc[e * 8 + q] = o8[q];
+  }
+  grid.sync();
+  {
+    double v[1] = {0.0};
+    for (size_t q = tid; q < a.npts; q += nthr) {
+      int cnt;
+      const double acc = dss_gather<2, double>(a.aploc, nullptr, a.pairs + (q >> 3) * 26, q,
+                                               (int)(q & 7), cnt);
+      const double rq = a.f[q] + -acc;
+      a.r[q] = rq;
+      v[0] += rq * (1.0 / (1.0 + (double)cnt));
+    }
+    block_partials<1>(v, a.partA, sred);
+  }
+  grid.sync();
+  double s[4];
+  {
+    double t[1];
+    grid_sums<1>(a.partA, G, t, sred, sbc);
+    const double c = t[0] / a.nunique;
+    double v[1] = {0.0};
+    for (size_t q = tid; q < a.npts; q += nthr) {
+      const double rq = a.r[q] + -c;
+      a.r[q] = rq;
+      const double zq = rq * a.dinv[q];
+      a.z[q] = zq;
+      v[0] += zq * (1.0 / (double)a.mult[q]);
+    }
+    block_partials<1>(v, a.partB, sred);
+  }
+  grid.sync();
+  double cz, rdz = 0.0, beta = 0.0, err = 0.0, err0 = 0.0;
+  {
+    double t[1];
+    grid_sums<1>(a.partB, G, t, sred, sbc);
+    cz = t[0] / a.nunique;
+  }
+  int it = 0;
+  for (; it < a.max_iter; ++it) {
+    const bool first = it == 0;
+    // p = beta p + (z - c) (first: p = z - c); aploc = A_e p
+    for (size_t e = tid; e < (size_t)a.nel; e += nthr) {
+      double u8[8], o8[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const size_t g = e * 8 + q;
+        const double zc = a.z[g] - cz;
+        const double pv = first ? zc : beta * a.p[g] + zc;
+        a.p[g] = pv;
+        u8[q] = pv;
+      }
+      elem_op2(a, sD, u8, o8, e);
+#pragma unroll
+      for (int q = 0; q < 8; ++q) a.aploc[e * 8 + q] = o8[q];
+    }
+    grid.sync();
+    // ap = DSS(aploc); (p w).ap; first: (r w).p and (r w).r
+    {
+      double v[3] = {0.0, 0.0, 0.0};
+      for (size_t q = tid; q < a.npts; q += nthr) {
+        int cnt;
+        const double acc = dss_gather<2, double>(a.aploc, nullptr, a.pairs + (q >> 3) * 26, q,
+                                                 (int)(q & 7), cnt);
+        a.ap[q] = acc;
+        const double w = 1.0 / (1.0 + (double)cnt);
+        const double pw = a.p[q] * w;
+        v[0] += pw * acc;
+        if (first) {
+          const double rw = a.r[q] * w;
+          v[1] += rw * a.p[q];
+          v[2] += rw * a.r[q];
+        }
+      }
+      block_partials<3>(v, a.partB, sred);
+    }
+    grid.sync();
+    // alpha; x += alpha p; r -= alpha ap; z = M^-1 r
+    {
+      double t[3];
+      grid_sums<3>(a.partB, G, t, sred, sbc);
+      if (first) {
+        rdz = t[1];
+        err0 = sqrt(t[2]);
+      }
+      const double alpha = rdz / t[0];
+      double v[4] = {0.0, 0.0, 0.0, 0.0};
+      for (size_t q = tid; q < a.npts; q += nthr) {
+        a.x[q] = a.x[q] + alpha * a.p[q];
+        const double rq = a.r[q] + -alpha * a.ap[q];
+        a.r[q] = rq;
+        const double zq = rq * a.dinv[q];
+        a.z[q] = zq;
+        const double w = 1.0 / (double)a.mult[q];
+        const double rw = rq * w;
+        v[0] += rw * zq;
+        v[1] += rw * rq;
+        v[2] += w * zq;
+        v[3] += rw;
+      }
+      block_partials<4>(v, a.partA, sred);
+    }
+    grid.sync();
+    grid_sums<4>(a.partA, G, s, sred, sbc);
+    cz = s[2] / a.nunique;
+    const double rdz_new = s[0] - cz * s[3];
+    beta = rdz_new / rdz;
+    rdz = rdz_new;
+    err = sqrt(s[1]);
+    if (!(err > a.eps) || it + 1 >= a.max_iter) {
+      ++it;
+      break;
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    a.frame[F_ITER] = (double)it;
+    a.frame[F_ERR] = err;
+    a.frame[F_ERR0] = err0;
+    a.frame[F_DONE] = 1.0;
+  }
+}
+
+}  // namespace dev
+
+static int g_coarse_grid[SSG_MAXLEV * 8] = {0};
+
+cudaError_t run_coarse_cg(cudaStream_t s, int device, int nel, const double* f, double* x,
+                          double* r, double* z, double* p, double* aploc, double* ap,
+                          const double* gf, const double* D, const double* dinv,
+                          const uint8_t* mult, const int* pairs, double nunique, double eps,
+                          int max_iter, double* part, size_t part_cap, double* frame) {
+  dev::CoarseArgs a;
+  a.nel = nel;
+  a.npts = (size_t)nel * 8;
+  a.f = f;
+  a.x = x;
+  a.r = r;
+  a.z = z;
+  a.p = p;
+  a.aploc = aploc;
+  a.ap = ap;
+  a.gf = gf;
+  a.D = D;
+  a.dinv = dinv;
+  a.mult = mult;
+  a.pairs = reinterpret_cast<const int2*>(pairs);
+  a.nunique = nunique;
+  a.eps = eps;
+  a.max_iter = max_iter;
+  a.frame = frame;
+  int& cap = g_coarse_grid[device & (SSG_MAXLEV * 8 - 1)];
+  if (cap == 0) {
+    int per_sm = 0, nsm = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dev::k_coarse_cg,
+                                                                  256, 0);
+    if (e != cudaSuccess) return e;
+    e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
+    if (e != cudaSuccess) return e;
+    cap = per_sm * nsm;
+    if (cap < 1) return cudaErrorCooperativeLaunchTooLarge;
+  }
+  int G = (int)((a.npts + 255) / 256);
+  if (G > cap) G = cap;
+  // blocks per SM beyond what the occupancy query guarantees are never used
+  if ((size_t)7 * G > part_cap) G = (int)(part_cap / 7);
+  if (G < 1) return cudaErrorInvalidValue;
+  a.partA = part;
+  a.partB = part + 4 * (size_t)G;
+  void* args[] = {&a};
+  ++g_launches;
+  return cudaLaunchCooperativeKernel((const void*)dev::k_coarse_cg, dim3(G), dim3(256), args,
+                                     0, s);
+}
+
+}  // namespace ssg

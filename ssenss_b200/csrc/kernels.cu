@@ -42,6 +42,7 @@ struct PUpdate {
   const double* beta = nullptr;
   const double* c = nullptr;      // nullspace constant (pressure) or null
   const double* mask = nullptr;
+  const double* stop = nullptr;   // solver's stop flag: skip when set
   int first = 0;
 };
 
@@ -54,6 +55,7 @@ __global__ void __launch_bounds__(256, 2) k_ax(int nel, T* __restrict__ u,
                                                const double* __restrict__ Sg,
                                                double lambda, PUpdate pu) {
   constexpr int NN = N * N, NNN = N * N * N, P = N + 1;
+  if (FUSEP && pu.stop && *pu.stop != 0.0) return;   // uniform over the block
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double* sD = reinterpret_cast<double*>(smem_raw);
   double* sS = sD + N * P;
@@ -155,8 +157,10 @@ __global__ void __launch_bounds__(256) k_dss(int nel, int epb, const T* __restri
                                              const double* __restrict__ mask,
                                              const T* __restrict__ y,
                                              const T* __restrict__ y2,
-                                             double* __restrict__ part) {
-  constexpr int NT = N * N * N, M = N - 1;
+                                             double* __restrict__ part,
+                                             const double* __restrict__ stop) {
+  constexpr int NT = N * N * N;
+  if (stop && *stop != 0.0) return;   // uniform over the block
   __shared__ int2 sp[64 * 26];
   __shared__ double sred[2 * 32];
   const int e0 = blockIdx.x * epb;
@@ -166,49 +170,9 @@ __global__ void __launch_bounds__(256) k_dss(int nel, int epb, const T* __restri
   double s0 = 0.0, s1 = 0.0;
   for (int q = threadIdx.x; q < ne * NT; q += blockDim.x) {
     const int z = q / NT, loc = q - z * NT;
-    const int i = loc % N, j = (loc / N) % N, k = loc / (N * N);
     const size_t gi = (size_t)(e0 + z) * NT + loc;
-    const int2* pr = sp + z * 26;
-    double acc = (double)in[gi];
-    if (mask) acc = acc * mask[gi];
     int cnt = 0;
-    const bool ei = i == 0 || i == M, ej = j == 0 || j == M, ek = k == 0 || k == M;
-    if (ei || ej || ek) {
-#define SSG_ADD(PR, NODE)                                                \
-  {                                                                       \
-    const int2 p_ = (PR);                                                 \
-    if (p_.x >= 0) {                                                      \
-      const size_t s_ = (size_t)p_.x * NT + (NODE);                       \
-      double v_ = (double)in[s_];                                         \
-      if (mask) v_ = v_ * mask[s_];                                       \
-      acc += v_;                                                          \
-      ++cnt;                                                              \
-    }                                                                     \
-  }
-      if (i == 0) SSG_ADD(pr[0], face_node(N, pr[0].y, k, j));
-      if (i == M) SSG_ADD(pr[1], face_node(N, pr[1].y, k, j));
-      if (j == 0) SSG_ADD(pr[2], face_node(N, pr[2].y, k, i));
-      if (j == M) SSG_ADD(pr[3], face_node(N, pr[3].y, k, i));
-      if (k == 0) SSG_ADD(pr[4], face_node(N, pr[4].y, j, i));
-      if (k == M) SSG_ADD(pr[5], face_node(N, pr[5].y, j, i));
-      if (ei && ej) {
-        const int q4 = (i == M) | ((j == M) << 1);
-        SSG_ADD(pr[6 + q4], edge_node(N, pr[6 + q4].y, k));
-      }
-      if (ek && ei) {
-        const int q4 = (i == M) | ((k == M) << 1);
-        SSG_ADD(pr[10 + q4], edge_node(N, pr[10 + q4].y, j));
-      }
-      if (ek && ej) {
-        const int q4 = (j == M) | ((k == M) << 1);
-        SSG_ADD(pr[14 + q4], edge_node(N, pr[14 + q4].y, i));
-      }
-      if (ei && ej && ek) {
-        const int c = (i == M) | ((j == M) << 1) | ((k == M) << 2);
-        SSG_ADD(pr[18 + c], corner_node(N, pr[18 + c].y));
-      }
-#undef SSG_ADD
-    }
+    const double acc = dss_gather<N, T>(in, mask, sp + z * 26, gi, loc, cnt);
     const double w = 1.0 / (1.0 + (double)cnt);
     if (MODE == DSS_RESID) {
       const T r = (T)((double)y[gi] + -acc);
@@ -300,7 +264,9 @@ __global__ void __launch_bounds__(256) k_cg_update(size_t npts,
                                                    const T* __restrict__ dinv,
                                                    const uint8_t* __restrict__ mult,
                                                    T* __restrict__ z,
-                                                   double* __restrict__ part) {
+                                                   double* __restrict__ part,
+                                                   const double* __restrict__ stop) {
+  if (stop && *stop != 0.0) return;
   __shared__ double sred[4 * 32];
   const double alpha = *alpha_p;
   double v[4] = {0.0, 0.0, 0.0, 0.0};
@@ -431,6 +397,7 @@ __global__ void __launch_bounds__(256) k_mul(size_t npts, T* __restrict__ x,
 __global__ void __launch_bounds__(256) k_reduce(const double* __restrict__ part, int nblk,
                                                 int nq, double* __restrict__ sums,
                                                 ScalarOp op) {
+  if (op.stop && *op.stop != 0.0) return;
   __shared__ double sred[32];
   for (int q = 0; q < nq; ++q) {
     double v[1] = {0.0};
@@ -443,8 +410,10 @@ __global__ void __launch_bounds__(256) k_reduce(const double* __restrict__ part,
   switch (op.code) {
     case OP_NONE:
       break;
-    case OP_CG_INIT_C:   // c = (w.z)/nunique (pressure)
+    case OP_CG_INIT_C:   // c = (w.z)/nunique (pressure); a new solve starts
       f[F_C] = op.pressure ? sums[0] / op.nunique : 0.0;
+      f[F_ITER] = 0.0;
+      f[F_DONE] = 0.0;
       break;
     case OP_CG_INIT_RDZ:  // rdz = (r w).p, |r|_w ; reset counters
       f[F_RDZ] = sums[0];
@@ -506,7 +475,7 @@ __global__ void __launch_bounds__(256) k_reduce(const double* __restrict__ part,
 // ---------------------------------------------------------------------------
 using namespace dev;
 
-static unsigned long long g_launches = 0;   // every launch below bumps it
+unsigned long long g_launches = 0;   // every launch of this library bumps it
 #define SSG_COUNT() (++g_launches)
 
 int vec_blocks(size_t npts) {
@@ -567,6 +536,7 @@ cudaError_t run_ax(cudaStream_t s, int n, int nel, int epb, bool helm, bool fp32
     pu.beta = pua->beta;
     pu.c = pua->c;
     pu.mask = pua->mask;
+    pu.stop = pua->stop;
     pu.first = pua->first;
   }
   if (fp32) {
@@ -606,24 +576,24 @@ int dss_grid(int n, int nel) {
 template <int N, typename T>
 static cudaError_t run_dss_n(cudaStream_t s, int mode, int nel, const T* in, T* out,
                              const int2* pr, const double* mask, const T* y, const T* y2,
-                             double* part) {
+                             double* part, const double* stop) {
   const int epb = dss_epb(N);
   const int grd = (nel + epb - 1) / epb;
   switch (mode) {
     case DSS_PLAIN:
-      { SSG_COUNT(); k_dss<N, T, DSS_PLAIN><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, mask, y, y2, part); }
+      { SSG_COUNT(); k_dss<N, T, DSS_PLAIN><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, mask, y, y2, part, stop); }
       break;
     case DSS_DOT:
-      { SSG_COUNT(); k_dss<N, T, DSS_DOT><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, mask, y, y2, part); }
+      { SSG_COUNT(); k_dss<N, T, DSS_DOT><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, mask, y, y2, part, stop); }
       break;
     case DSS_DOT2:
-      { SSG_COUNT(); k_dss<N, T, DSS_DOT2><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, mask, y, y2, part); }
+      { SSG_COUNT(); k_dss<N, T, DSS_DOT2><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, mask, y, y2, part, stop); }
       break;
     case DSS_RESID:
-      { SSG_COUNT(); k_dss<N, T, DSS_RESID><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, mask, y, y2, part); }
+      { SSG_COUNT(); k_dss<N, T, DSS_RESID><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, mask, y, y2, part, stop); }
       break;
     case DSS_AVG:
-      { SSG_COUNT(); k_dss<N, T, DSS_AVG><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, mask, y, y2, part); }
+      { SSG_COUNT(); k_dss<N, T, DSS_AVG><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, mask, y, y2, part, stop); }
       break;
     default:
       return cudaErrorInvalidValue;
@@ -634,11 +604,11 @@ static cudaError_t run_dss_n(cudaStream_t s, int mode, int nel, const T* in, T* 
 template <typename T>
 static cudaError_t run_dss_t(cudaStream_t s, int mode, int n, int nel, const T* in, T* out,
                              const int* pairs, const double* mask, const T* y, const T* y2,
-                             double* part) {
+                             double* part, const double* stop) {
   const int2* pr = reinterpret_cast<const int2*>(pairs);
   switch (n) {
 #define SSG_DSSN(NV) \
-  case NV: return run_dss_n<NV, T>(s, mode, nel, in, out, pr, mask, y, y2, part);
+  case NV: return run_dss_n<NV, T>(s, mode, nel, in, out, pr, mask, y, y2, part, stop);
     SSG_DSSN(2) SSG_DSSN(3) SSG_DSSN(4) SSG_DSSN(5) SSG_DSSN(6) SSG_DSSN(7)
     SSG_DSSN(8) SSG_DSSN(9) SSG_DSSN(10) SSG_DSSN(11) SSG_DSSN(12)
 #undef SSG_DSSN
@@ -648,12 +618,12 @@ static cudaError_t run_dss_t(cudaStream_t s, int mode, int n, int nel, const T* 
 
 cudaError_t run_dss(cudaStream_t s, int mode, bool fp32, int n, int nel, const void* in,
                     void* out, const int* pairs, const double* mask, const void* y,
-                    const void* y2, double* part) {
+                    const void* y2, double* part, const double* stop) {
   if (fp32)
     return run_dss_t<float>(s, mode, n, nel, (const float*)in, (float*)out, pairs, mask,
-                            (const float*)y, (const float*)y2, part);
+                            (const float*)y, (const float*)y2, part, stop);
   return run_dss_t<double>(s, mode, n, nel, (const double*)in, (double*)out, pairs, mask,
-                           (const double*)y, (const double*)y2, part);
+                           (const double*)y, (const double*)y2, part, stop);
 }
 
 cudaError_t run_tensor3(cudaStream_t s, bool fp32, bool add, int nel, int ni, int no,
@@ -678,15 +648,16 @@ cudaError_t run_tensor3(cudaStream_t s, bool fp32, bool add, int nel, int ni, in
 
 cudaError_t run_cg_update(cudaStream_t s, bool fp32, size_t npts, const double* alpha,
                           void* x, const void* p, void* r, const void* ap, const void* dinv,
-                          const uint8_t* mult, void* z, double* part, int nblk) {
+                          const uint8_t* mult, void* z, double* part, int nblk,
+                          const double* stop) {
   if (fp32)
     { SSG_COUNT(); k_cg_update<float><<<nblk, 256, 0, s>>>(npts, alpha, (float*)x, (const float*)p, (float*)r,
                                             (const float*)ap, (const float*)dinv, mult,
-                                            (float*)z, part); }
+                                            (float*)z, part, stop); }
   else
     { SSG_COUNT(); k_cg_update<double><<<nblk, 256, 0, s>>>(npts, alpha, (double*)x, (const double*)p,
                                              (double*)r, (const double*)ap,
-                                             (const double*)dinv, mult, (double*)z, part); }
+                                             (const double*)dinv, mult, (double*)z, part, stop); }
   return cudaGetLastError();
 }
 

@@ -51,6 +51,58 @@ __device__ __forceinline__ int corner_node(int n, int c) {
 }
 
 // ---------------------------------------------------------------------------
+// DSS of one local node (direct_stiffness_summation, src/global.c:241-257):
+// the node's own value plus its neighbours' pre-sum copies, in the
+// reference's order -- faces w, e, s, n, b, t, then edges sw..tn, then
+// corners -- through the pairing pr (26 (element, matched index) pairs of
+// this node's element).  FP64 accumulation; cnt = contributions added.
+// ---------------------------------------------------------------------------
+template <int N, typename T>
+__device__ __forceinline__ double dss_gather(const T* __restrict__ in,
+                                             const double* __restrict__ mask,
+                                             const int2* pr, size_t gi, int loc, int& cnt) {
+  constexpr int NT = N * N * N, M = N - 1;
+  const int i = loc % N, j = (loc / N) % N, k = loc / (N * N);
+  double acc = (double)in[gi];
+  if (mask) acc = acc * mask[gi];
+  cnt = 0;
+  const bool ei = i == 0 || i == M, ej = j == 0 || j == M, ek = k == 0 || k == M;
+  if (!(ei || ej || ek)) return acc;
+  auto add = [&](int2 p, int node) {
+    if (p.x >= 0) {
+      const size_t s = (size_t)p.x * NT + node;
+      double v = (double)in[s];
+      if (mask) v = v * mask[s];
+      acc += v;
+      ++cnt;
+    }
+  };
+  if (i == 0) add(pr[0], face_node(N, pr[0].y, k, j));
+  if (i == M) add(pr[1], face_node(N, pr[1].y, k, j));
+  if (j == 0) add(pr[2], face_node(N, pr[2].y, k, i));
+  if (j == M) add(pr[3], face_node(N, pr[3].y, k, i));
+  if (k == 0) add(pr[4], face_node(N, pr[4].y, j, i));
+  if (k == M) add(pr[5], face_node(N, pr[5].y, j, i));
+  if (ei && ej) {
+    const int q = 6 + ((i == M) | ((j == M) << 1));
+    add(pr[q], edge_node(N, pr[q].y, k));
+  }
+  if (ek && ei) {
+    const int q = 10 + ((i == M) | ((k == M) << 1));
+    add(pr[q], edge_node(N, pr[q].y, j));
+  }
+  if (ek && ej) {
+    const int q = 14 + ((j == M) | ((k == M) << 1));
+    add(pr[q], edge_node(N, pr[q].y, i));
+  }
+  if (ei && ej && ek) {
+    const int q = 18 + ((i == M) | ((j == M) << 1) | ((k == M) << 2));
+    add(pr[q], corner_node(N, pr[q].y));
+  }
+  return acc;
+}
+
+// ---------------------------------------------------------------------------
 // block reduction of NQ doubles over a 1-D block whose size is a multiple of
 // 32; fixed shuffle pattern, so the result is deterministic.  Valid in
 // thread 0.  sred: NQ * 32 doubles of shared memory.

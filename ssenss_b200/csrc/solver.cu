@@ -159,6 +159,11 @@ ssg_status cg_solve(ssg_context* c, int level, int var, bool fp32, void* f, void
   pu.beta = fr + F_BETA;
   pu.c = pres ? fr + F_C : nullptr;
   pu.mask = mask;
+  // Once the stop flag is set every kernel of a later iteration returns at
+  // once, so iterations are enqueued ahead without waiting for the flag:
+  // all of them for a smoother (sync_each false), chunks of 8 otherwise.
+  const double* stop = fr + F_DONE;
+  pu.stop = stop;
   for (int it = 0; it < max_iter; ++it) {
     // p = beta p + (z - c) (first: p = z - c), masked; aploc = A p
     pu.first = it == 0;
@@ -175,25 +180,44 @@ ssg_status cg_solve(ssg_context* c, int level, int var, bool fp32, void* f, void
     }
     // ap = DSS(mask aploc); alpha = rdz / (p w).ap
     SSG_CUDA(c, run_dss(s, DSS_DOT, fp32, L.n, c->nel, W.aploc, W.ap, c->d_pairs, mask,
-                        W.p, nullptr, c->d_part));
+                        W.p, nullptr, c->d_part, stop));
     op.code = OP_CG_ALPHA;
+    op.stop = stop;
     SSG_CUDA(c, run_reduce(s, c->d_part, nbd, 1, c->d_sums, op));
     // x += alpha p; r -= alpha ap; z = M^-1 r; beta; err
     SSG_CUDA(c, run_cg_update(s, fp32, np, fr + F_ALPHA, x, W.p, W.r, W.ap, dinv, L.mult,
-                              W.z, c->d_part, nb));
+                              W.z, c->d_part, nb, stop));
     op.code = OP_CG_BETA;
     SSG_CUDA(c, run_reduce(s, c->d_part, nb, 4, c->d_sums, op));
-    if (sync_each) {
+    op.stop = nullptr;
+    if (sync_each && (it % 8 == 7)) {
       double done;
       SSG_TRY(read_flag(c, fr + F_DONE, &done));
       if (done != 0.0) break;
     }
   }
+  if (!sync_each) return SSG_OK;   // smoother: outcome stays on the device
   double err, iters;
   SSG_TRY(read_flag(c, fr + F_ERR, &err));
   SSG_TRY(read_flag(c, fr + F_ITER, &iters));
   if (!std::isfinite(err)) return fail(c, SSG_NONFINITE, "non-finite CG residual");
   if (!(err <= eps) && iters >= max_iter) return SSG_MAXITER;
+  return SSG_OK;
+}
+
+// coarsest level (n = 2): CG-Jacobi, 500 iterations, in one cooperative launch
+static ssg_status coarse_solve(ssg_context* c, int L, double* f, double* x, double eps,
+                               int max_iter) {
+  const DevLevel& C = c->lev[L];
+  LevelWork& W = c->ws->w64[L];
+  if (C.n != 2) {
+    return cg_solve(c, L, SSG_PRESSURE, false, f, x, eps, max_iter, FR_LEVEL0 + L, nullptr,
+                    0, false);
+  }
+  SSG_CUDA(c, run_coarse_cg(c->stream, c->device, c->nel, f, x, (double*)W.r, (double*)W.z,
+                            (double*)W.p, (double*)W.aploc, (double*)W.ap, C.gf, C.D,
+                            C.dinv_p, C.mult, c->d_pairs, C.nunique, eps, max_iter, c->d_part,
+                            c->part_cap, c->d_sc + (FR_LEVEL0 + L) * F_SIZE));
   return SSG_OK;
 }
 
@@ -209,15 +233,11 @@ static ssg_status mg_recurse(ssg_context* c, int L, void* f, void* x, double eps
       const size_t np = c->lev[L].npts;
       SSG_CUDA(c, run_convert(s, np, f, true, W64.f, false));
       SSG_CUDA(c, cudaMemsetAsync(W64.x, 0, np * sizeof(double), s));
-      ssg_status st = cg_solve(c, L, SSG_PRESSURE, false, W64.f, W64.x, eps, 500,
-                               FR_LEVEL0 + L, nullptr, 0, true);
-      if (st != SSG_OK && st != SSG_MAXITER) return st;
+      SSG_TRY(coarse_solve(c, L, (double*)W64.f, (double*)W64.x, eps, 500));
       SSG_CUDA(c, run_convert(s, np, W64.x, false, x, true));
       return SSG_OK;
     }
-    ssg_status st = cg_solve(c, L, SSG_PRESSURE, false, f, x, eps, 500, FR_LEVEL0 + L,
-                             nullptr, 0, true);
-    return st == SSG_MAXITER ? SSG_OK : st;
+    return coarse_solve(c, L, (double*)f, (double*)x, eps, 500);
   }
   const DevLevel& F = c->lev[L];
   const DevLevel& C = c->lev[L + 1];
@@ -244,9 +264,7 @@ static ssg_status mg_recurse(ssg_context* c, int L, void* f, void* x, double eps
   SSG_CUDA(c, run_tensor3(s, fp32, true, c->nel, C.n, F.n,
                           C.Ap, Wc.x, x));
   // post-smoothing: CG-Jacobi, 15 iterations, stop at eps
-  ssg_status st = cg_solve(c, L, SSG_PRESSURE, fp32, f, x, eps, 15, FR_LEVEL0 + L, nullptr,
-                           0, true);
-  return st == SSG_MAXITER ? SSG_OK : st;
+  return cg_solve(c, L, SSG_PRESSURE, fp32, f, x, eps, 15, FR_LEVEL0 + L, nullptr, 0, false);
 }
 
 // z = M^-1 r: Jacobi then one V-cycle (multigrid_preconditioner,

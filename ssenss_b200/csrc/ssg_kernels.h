@@ -40,6 +40,7 @@ struct ScalarOp {
   int hist_cap = 0;
   int m = 0;
   int pap_idx[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  const double* stop = nullptr;   // skip when *stop != 0 (finished solve)
 };
 
 // up to 10 vectors passed by value to a kernel (capturable: no upload)
@@ -57,8 +58,11 @@ struct PUpdateArgs {
   const double* beta = nullptr;
   const double* c = nullptr;
   const double* mask = nullptr;
+  const double* stop = nullptr;
   int first = 0;
 };
+
+extern unsigned long long g_launches;   // kernel launches of this library
 
 int vec_blocks(size_t npts);
 int ax_epb(int n);
@@ -70,12 +74,13 @@ cudaError_t run_ax(cudaStream_t s, int n, int nel, int epb, bool helm, bool fp32
                    const PUpdateArgs* pua);
 cudaError_t run_dss(cudaStream_t s, int mode, bool fp32, int n, int nel, const void* in,
                     void* out, const int* pairs, const double* mask, const void* y,
-                    const void* y2, double* part);
+                    const void* y2, double* part, const double* stop = nullptr);
 cudaError_t run_tensor3(cudaStream_t s, bool fp32, bool add, int nel, int ni, int no,
                         const double* A, const void* in, void* out);
 cudaError_t run_cg_update(cudaStream_t s, bool fp32, size_t npts, const double* alpha,
                           void* x, const void* p, void* r, const void* ap, const void* dinv,
-                          const uint8_t* mult, void* z, double* part, int nblk);
+                          const uint8_t* mult, void* z, double* part, int nblk,
+                          const double* stop = nullptr);
 cudaError_t run_jacobi(cudaStream_t s, bool fp32, size_t npts, const void* r, const void* dinv,
                        const uint8_t* mult, void* z, double* part, int nblk);
 cudaError_t run_dots(cudaStream_t s, bool fp32, size_t npts, const void* x, const PtrList& ys,
@@ -94,5 +99,11 @@ cudaError_t run_convert(cudaStream_t s, size_t npts, const void* in, bool in32, 
 cudaError_t run_mul(cudaStream_t s, bool fp32, size_t npts, void* x, const double* y);
 cudaError_t run_reduce(cudaStream_t s, const double* part, int nblk, int nq, double* sums,
                        const ScalarOp& op);
+// whole CG-Jacobi solve of an n = 2 level in one cooperative launch (coarse.cu)
+cudaError_t run_coarse_cg(cudaStream_t s, int device, int nel, const double* f, double* x,
+                          double* r, double* z, double* p, double* aploc, double* ap,
+                          const double* gf, const double* D, const double* dinv,
+                          const uint8_t* mult, const int* pairs, double nunique, double eps,
+                          int max_iter, double* part, size_t part_cap, double* frame);
 
 }  // namespace ssg
