@@ -320,6 +320,8 @@ static ssg_status create_impl(int device, void* stream, ssg_context** out) {
     c->own_stream = true;
   }
   if (cudaMalloc(&c->d_sums, 16 * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&c->d_counter, sizeof(unsigned)) != cudaSuccess ||
+      cudaMemset(c->d_counter, 0, sizeof(unsigned)) != cudaSuccess ||
       cudaMalloc(&c->d_sc, FR_COUNT * F_SIZE * sizeof(double)) != cudaSuccess ||
       cudaMallocHost(&c->h_pin, 64 * sizeof(double)) != cudaSuccess ||
       cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
@@ -343,6 +345,7 @@ void ssg_destroy(ssg_context* c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   free_mesh(c);
   dfree(c->d_sums);
+  dfree(c->d_counter);
   dfree(c->d_sc);
   if (c->h_pin) cudaFreeHost(c->h_pin);
   if (c->ev0) cudaEventDestroy(c->ev0);
@@ -566,9 +569,10 @@ ssg_status ssg_global_dot_product(ssg_context* c, const double* x, const double*
   const int nb = vec_blocks(np);
   PtrList pl;
   pl.p[0] = dy;
-  SSG_CUDA(c, run_dots(c->stream, false, np, dx, pl, 1, c->lev[0].mult, c->d_part, nb));
   ScalarOp op;
-  SSG_CUDA(c, run_reduce(c->stream, c->d_part, nb, 1, c->d_sums, op));
+  op.sums = c->d_sums;
+  op.counter = c->d_counter;
+  SSG_CUDA(c, run_dots(c->stream, false, np, dx, pl, 1, c->lev[0].mult, c->d_part, nb, &op));
   SSG_CUDA(c, cudaMemcpyAsync(c->h_pin, c->d_sums, sizeof(double), cudaMemcpyDeviceToHost,
                               c->stream));
   SSG_CUDA(c, cudaStreamSynchronize(c->stream));

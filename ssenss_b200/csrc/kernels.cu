@@ -33,6 +33,113 @@ namespace ssg {
 namespace dev {
 
 // ---------------------------------------------------------------------------
+// solver scalar algebra on the reduced sums (one thread)
+// ---------------------------------------------------------------------------
+__device__ void apply_scalar_op(const ScalarOp& op, const double* __restrict__ sums) {
+  double* f = op.frame;
+  switch (op.code) {
+    case OP_NONE:
+      break;
+    case OP_CG_INIT_C:   // c = (w.z)/nunique (pressure); a new solve starts
+      f[F_C] = op.pressure ? sums[0] / op.nunique : 0.0;
+      f[F_ITER] = 0.0;
+      f[F_DONE] = 0.0;
+      break;
+    case OP_CG_INIT_RDZ:  // rdz = (r w).p, |r|_w ; reset counters
+      f[F_RDZ] = sums[0];
+      f[F_ERR0] = sqrt(sums[1]);
+      f[F_ITER] = 0.0;
+      f[F_DONE] = 0.0;
+      f[F_ERR] = sqrt(sums[1]);
+      break;
+    case OP_CG_ALPHA:     // alpha = rdz / (p w).ap
+      f[F_PAP] = sums[0];
+      f[F_ALPHA] = f[F_RDZ] / sums[0];
+      break;
+    case OP_CG_BETA: {    // sums: (r w).z, (r w).r, w.z, w.r
+      const double c = op.pressure ? sums[2] / op.nunique : 0.0;
+      const double rdz = sums[0] - c * sums[3];
+      f[F_C] = c;
+      f[F_BETA] = rdz / f[F_RDZ];
+      f[F_RDZ] = rdz;
+      const double err = sqrt(sums[1]);
+      f[F_ERR] = err;
+      f[F_ITER] += 1.0;
+      const bool go = (err > op.eps) && (f[F_ITER] < (double)op.max_iter);
+      f[F_DONE] = go ? 0.0 : 1.0;
+      if (op.hist && (int)f[F_ITER] <= op.hist_cap) op.hist[(int)f[F_ITER] - 1] = err;
+      break;
+    }
+    case OP_NULL_C:       // c = (w.x)/nunique into frame slot
+      f[F_C] = sums[0] / op.nunique;
+      break;
+    case OP_FCG_BETA:     // beta_k = sums[k] / pap[k]
+      for (int k = 0; k < op.m; ++k) f[F_FBETA + k] = sums[k] / f[F_FPAP + op.pap_idx[k]];
+      break;
+    case OP_FCG_ALPHA:    // pap0 and alpha = (p0 w).r / pap0
+      f[F_FPAP + op.pap_idx[0]] = sums[0];
+      f[F_ALPHA] = sums[1] / sums[0];
+      break;
+    case OP_FCG_ERR: {
+      const double err = sqrt(sums[0]);
+      f[F_ERR] = err;
+      f[F_ITER] += 1.0;
+      const bool go = (err > op.eps) && (f[F_ITER] < (double)op.max_iter);
+      f[F_DONE] = go ? 0.0 : 1.0;
+      if (op.hist && (int)f[F_ITER] <= op.hist_cap) op.hist[(int)f[F_ITER] - 1] = err;
+      break;
+    }
+    case OP_ERR0:
+      f[F_ERR0] = sqrt(sums[0]);
+      f[F_ITER] = 0.0;
+      f[F_DONE] = 0.0;
+      f[F_ERR] = sqrt(sums[0]);
+      break;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// end of a reducing kernel: thread 0 holds the block's NQ partial sums.  They
+// are stored at part[q * gridDim.x + block]; when op.counter is set, the
+// last block to arrive sums all partials in index order (so the result does
+// not depend on which block is last), stores them in op.sums, applies the
+// solver scalar algebra and re-arms the counter.
+// ---------------------------------------------------------------------------
+template <int NQ>
+__device__ __forceinline__ void finish(const double (&v)[NQ], double* __restrict__ part,
+                                       const ScalarOp& op, double* sred) {
+  __shared__ int s_last;
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) part[q * gridDim.x + blockIdx.x] = v[q];
+    s_last = 0;
+    if (op.counter) {
+      __threadfence();
+      const unsigned prev = atomicAdd(op.counter, 1u);
+      s_last = prev == gridDim.x - 1;
+    }
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  double s[NQ];
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+    s[q] = 0.0;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x)
+      s[q] += __ldcg(part + (size_t)q * gridDim.x + b);
+  }
+  block_reduce<NQ>(s, sred);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) op.sums[q] = s[q];
+    apply_scalar_op(op, op.sums);
+    *op.counter = 0u;
+  }
+}
+
+
+// ---------------------------------------------------------------------------
 // local operator, optionally preceded by the CG direction update
 //   p = ((beta p + (z - c)) .* mask)   (first: p = (z - c) .* mask)
 // (src/solver.c:59-60,75-77 with subtract_nullspace folded in)
@@ -46,32 +153,93 @@ struct PUpdate {
   int first = 0;
 };
 
+// padded row stride of the shared 1-D matrices: even (16-byte aligned rows
+// for double2 loads) and chosen so the rows fall on distinct bank groups
+template <int N>
+struct AxLayout {
+  static constexpr int P = (N % 2 == 0) ? N + 2 : N + 1;   // matrix rows
+  static constexpr int Q = N + (N & 1);                    // field rows
+};
+
+// sum_m a[m] b[m] over m = 0..N-1 in order, both rows 16-byte aligned
+template <int N>
+__device__ __forceinline__ double row_dot(const double* a, const double* b) {
+  double s = 0.0;
+#pragma unroll
+  for (int m = 0; m + 1 < N; m += 2) {
+    const double2 x = *reinterpret_cast<const double2*>(a + m);
+    const double2 y = *reinterpret_cast<const double2*>(b + m);
+    s += x.x * y.x;
+    s += x.y * y.y;
+  }
+  if (N & 1) s += a[N - 1] * b[N - 1];
+  return s;
+}
+
+// sum_m a[m] b[m * stride] over m in order; a a 16-byte aligned row
+template <int N>
+__device__ __forceinline__ double row_col_dot(const double* a, const double* b, int stride) {
+  double s = 0.0;
+#pragma unroll
+  for (int m = 0; m + 1 < N; m += 2) {
+    const double2 x = *reinterpret_cast<const double2*>(a + m);
+    s += x.x * b[m * stride];
+    s += x.y * b[(m + 1) * stride];
+  }
+  if (N & 1) s += a[N - 1] * b[(N - 1) * stride];
+  return s;
+}
+
+// sum_m a[m] r[m] over m in order; a a 16-byte aligned row, r registers
+template <int N>
+__device__ __forceinline__ double row_reg_dot(const double* a, const double (&r)[N]) {
+  double s = 0.0;
+#pragma unroll
+  for (int m = 0; m + 1 < N; m += 2) {
+    const double2 x = *reinterpret_cast<const double2*>(a + m);
+    s += x.x * r[m];
+    s += x.y * r[m + 1];
+  }
+  if (N & 1) s += a[N - 1] * r[N - 1];
+  return s;
+}
+
+// Shared memory: D, D^T, S, S^T rows (padded), then per element the u plane
+// stack and the r/s fluxes.  Every per-thread access to a 1-D matrix is a
+// row, read as double2.
 template <int N, typename T, bool HELM, bool FUSEP>
-__global__ void __launch_bounds__(256, 2) k_ax(int nel, T* __restrict__ u,
+__global__ void __launch_bounds__(256, (N >= 10 ? 1 : 2)) k_ax(int nel, T* __restrict__ u,
                                                T* __restrict__ au,
                                                const T* __restrict__ gf, size_t npts,
                                                const double* __restrict__ bj,
                                                const double* __restrict__ Dg,
                                                const double* __restrict__ Sg,
                                                double lambda, PUpdate pu) {
-  constexpr int NN = N * N, NNN = N * N * N, P = N + 1;
+  constexpr int NN = N * N, P = AxLayout<N>::P, Q = AxLayout<N>::Q;
+  constexpr int PLANE = N * Q, BLK = N * PLANE;
   if (FUSEP && pu.stop && *pu.stop != 0.0) return;   // uniform over the block
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  double* sD = reinterpret_cast<double*>(smem_raw);
-  double* sS = sD + N * P;
-  double* su = sS + N * P + threadIdx.z * 3 * NNN;
-  double* sw0 = su + NNN;
-  double* sw1 = sw0 + NNN;
+  double* sD = reinterpret_cast<double*>(smem_raw);   // D[i][m]
+  double* sDT = sD + N * P;                            // D^T[i][m] = D[m][i]
+  double* sS = sDT + N * P;                            // S (Helmholtz) or D
+  double* sST = sS + N * P;
+  double* su = sST + N * P + threadIdx.z * 3 * BLK;
+  double* sw0 = su + BLK;
+  double* sw1 = sw0 + BLK;
   const int i = threadIdx.x, j = threadIdx.y;
   const int tid = i + N * (j + N * threadIdx.z);
   const int nthr = NN * blockDim.z;
   for (int q = tid; q < NN; q += nthr) {
-    sD[(q / N) * P + q % N] = Dg[q];
-    sS[(q / N) * P + q % N] = HELM ? Sg[q] : Dg[q];
+    const int r = q / N, c = q % N;
+    const double d = Dg[q], sv = HELM ? Sg[q] : Dg[q];
+    sD[r * P + c] = d;
+    sDT[c * P + r] = d;
+    sS[r * P + c] = sv;
+    sST[c * P + r] = sv;
   }
   const int e = blockIdx.x * blockDim.z + threadIdx.z;
   const bool active = e < nel;
-  const size_t off = (size_t)(active ? e : 0) * NNN + j * N + i;
+  const size_t off = (size_t)(active ? e : 0) * (NN * N) + j * N + i;
   double ru[N], rw2[N];
   if (FUSEP) {
     const T* z = reinterpret_cast<const T*>(pu.z);
@@ -90,26 +258,23 @@ __global__ void __launch_bounds__(256, 2) k_ax(int nel, T* __restrict__ u,
         v = (double)vt;
       }
       ru[k] = v;
-      su[k * NN + j * N + i] = v;
+      su[k * PLANE + j * Q + i] = v;
     }
   } else {
 #pragma unroll
     for (int k = 0; k < N; ++k) {
       ru[k] = active ? (double)u[off + (size_t)k * NN] : 0.0;
-      su[k * NN + j * N + i] = ru[k];
+      su[k * PLANE + j * Q + i] = ru[k];
     }
   }
   __syncthreads();
-  const double* Dx = sS;   // r-derivative: S for Helmholtz, D otherwise
+  // r-derivative with S for Helmholtz (the swapped deriv_matrix), D otherwise
+  const double* Dx = HELM ? sS : sD;
 #pragma unroll
   for (int k = 0; k < N; ++k) {
-    double ur = 0, us = 0, ut = 0;
-#pragma unroll
-    for (int m = 0; m < N; ++m) {
-      ur += Dx[i * P + m] * su[k * NN + j * N + m];
-      us += sD[j * P + m] * su[k * NN + m * N + i];
-      ut += sD[k * P + m] * ru[m];
-    }
+    const double ur = row_dot<N>(Dx + i * P, su + k * PLANE + j * Q);
+    const double us = row_col_dot<N>(sD + j * P, su + k * PLANE + i, Q);
+    const double ut = row_reg_dot<N>(sD + k * P, ru);
     const size_t o = off + (size_t)k * NN;
     double g0 = 0, g1 = 0, g2 = 0, g3 = 0, g4 = 0, g5 = 0;
     if (active) {
@@ -120,21 +285,17 @@ __global__ void __launch_bounds__(256, 2) k_ax(int nel, T* __restrict__ u,
       g4 = (double)__ldg(gf + 4 * npts + o);
       g5 = (double)__ldg(gf + 5 * npts + o);
     }
-    sw0[k * NN + j * N + i] = g0 * ur + g1 * us + g2 * ut;
-    sw1[k * NN + j * N + i] = g1 * ur + g3 * us + g4 * ut;
+    sw0[k * PLANE + j * Q + i] = g0 * ur + g1 * us + g2 * ut;
+    sw1[k * PLANE + j * Q + i] = g1 * ur + g3 * us + g4 * ut;
     rw2[k] = g2 * ur + g4 * us + g5 * ut;
   }
   __syncthreads();
-  // transposed derivatives: r with D, s and t with S (= D for Poisson)
+  // transposed derivatives: r with D^T, s and t with S^T (= D^T for Poisson)
 #pragma unroll
   for (int k = 0; k < N; ++k) {
-    double acc = 0, acs = 0, act = 0;
-#pragma unroll
-    for (int m = 0; m < N; ++m) {
-      acc += sD[m * P + i] * sw0[k * NN + j * N + m];
-      acs += sS[m * P + j] * sw1[k * NN + m * N + i];
-      act += sS[m * P + k] * rw2[m];
-    }
+    const double acc = row_dot<N>(sDT + i * P, sw0 + k * PLANE + j * Q);
+    const double acs = row_col_dot<N>(sST + j * P, sw1 + k * PLANE + i, Q);
+    const double act = row_reg_dot<N>(sST + k * P, rw2);
     double out = (acc + acs) + act;
     if (HELM && active) out += lambda * (__ldg(bj + off + (size_t)k * NN) * ru[k]);
     if (active) au[off + (size_t)k * NN] = (T)out;
@@ -158,7 +319,7 @@ __global__ void __launch_bounds__(256) k_dss(int nel, int epb, const T* __restri
                                              const T* __restrict__ y,
                                              const T* __restrict__ y2,
                                              double* __restrict__ part,
-                                             const double* __restrict__ stop) {
+                                             const double* __restrict__ stop, ScalarOp op) {
   constexpr int NT = N * N * N;
   if (stop && *stop != 0.0) return;   // uniform over the block
   __shared__ int2 sp[64 * 26];
@@ -169,7 +330,8 @@ __global__ void __launch_bounds__(256) k_dss(int nel, int epb, const T* __restri
   __syncthreads();
   double s0 = 0.0, s1 = 0.0;
   for (int q = threadIdx.x; q < ne * NT; q += blockDim.x) {
-    const int z = q / NT, loc = q - z * NT;
+    const int z = q / NT;
+    const int loc = class_ordered_node<N>(q - z * NT);
     const size_t gi = (size_t)(e0 + z) * NT + loc;
     int cnt = 0;
     const double acc = dss_gather<N, T>(in, mask, sp + z * 26, gi, loc, cnt);
@@ -190,13 +352,14 @@ __global__ void __launch_bounds__(256) k_dss(int nel, int epb, const T* __restri
       }
     }
   }
-  if (MODE == DSS_DOT || MODE == DSS_RESID || MODE == DSS_DOT2) {
+  if (MODE == DSS_DOT || MODE == DSS_RESID) {
+    double v[1] = {s0};
+    block_reduce<1>(v, sred);
+    finish<1>(v, part, op, sred);
+  } else if (MODE == DSS_DOT2) {
     double v[2] = {s0, s1};
     block_reduce<2>(v, sred);
-    if (threadIdx.x == 0) {
-      part[blockIdx.x] = v[0];
-      if (MODE == DSS_DOT2) part[gridDim.x + blockIdx.x] = v[1];
-    }
+    finish<2>(v, part, op, sred);
   }
 }
 
@@ -265,7 +428,8 @@ __global__ void __launch_bounds__(256) k_cg_update(size_t npts,
                                                    const uint8_t* __restrict__ mult,
                                                    T* __restrict__ z,
                                                    double* __restrict__ part,
-                                                   const double* __restrict__ stop) {
+                                                   const double* __restrict__ stop,
+                                                   ScalarOp op) {
   if (stop && *stop != 0.0) return;
   __shared__ double sred[4 * 32];
   const double alpha = *alpha_p;
@@ -284,10 +448,7 @@ __global__ void __launch_bounds__(256) k_cg_update(size_t npts,
     v[3] += rw;
   }
   block_reduce<4>(v, sred);
-  if (threadIdx.x == 0) {
-#pragma unroll
-    for (int k = 0; k < 4; ++k) part[k * gridDim.x + blockIdx.x] = v[k];
-  }
+  finish<4>(v, part, op, sred);
 }
 
 // z = dinv .* r; partial w.z (Jacobi preconditioner, src/precon.c:311-324)
@@ -295,7 +456,8 @@ template <typename T>
 __global__ void __launch_bounds__(256) k_jacobi(size_t npts, const T* __restrict__ r,
                                                 const T* __restrict__ dinv,
                                                 const uint8_t* __restrict__ mult,
-                                                T* __restrict__ z, double* __restrict__ part) {
+                                                T* __restrict__ z, double* __restrict__ part,
+                                                ScalarOp op) {
   __shared__ double sred[32];
   double v[1] = {0.0};
   SSG_GRID_LOOP(q, npts) {
@@ -304,14 +466,14 @@ __global__ void __launch_bounds__(256) k_jacobi(size_t npts, const T* __restrict
     v[0] += (double)zq * (1.0 / (double)mult[q]);
   }
   block_reduce<1>(v, sred);
-  if (threadIdx.x == 0) part[blockIdx.x] = v[0];
+  finish<1>(v, part, op, sred);
 }
 
 // partial sums of (x w) y_k, k < K (up to 10 vectors)
 template <typename T, int K>
 __global__ void __launch_bounds__(256) k_dots(size_t npts, const T* __restrict__ x, PtrList ys,
                                               const uint8_t* __restrict__ mult,
-                                              double* __restrict__ part) {
+                                              double* __restrict__ part, ScalarOp op) {
   __shared__ double sred[K * 32];
   double v[K];
 #pragma unroll
@@ -322,22 +484,19 @@ __global__ void __launch_bounds__(256) k_dots(size_t npts, const T* __restrict__
     for (int k = 0; k < K; ++k) v[k] += xw * (double)((const T*)ys.p[k])[q];
   }
   block_reduce<K>(v, sred);
-  if (threadIdx.x == 0) {
-#pragma unroll
-    for (int k = 0; k < K; ++k) part[k * gridDim.x + blockIdx.x] = v[k];
-  }
+  finish<K>(v, part, op, sred);
 }
 
 // partial sums of w x (the nullspace component, src/solver.c:200-213)
 template <typename T>
 __global__ void __launch_bounds__(256) k_wsum(size_t npts, const T* __restrict__ x,
                                               const uint8_t* __restrict__ mult,
-                                              double* __restrict__ part) {
+                                              double* __restrict__ part, ScalarOp op) {
   __shared__ double sred[32];
   double v[1] = {0.0};
   SSG_GRID_LOOP(q, npts) v[0] += (double)x[q] * (1.0 / (double)mult[q]);
   block_reduce<1>(v, sred);
-  if (threadIdx.x == 0) part[blockIdx.x] = v[0];
+  finish<1>(v, part, op, sred);
 }
 
 // x = x + sum_k (sign coef_k) y_k   (FCG direction, FP64)
@@ -358,7 +517,7 @@ __global__ void __launch_bounds__(256) k_fcg_update(size_t npts, const double* _
                                                     double* __restrict__ r,
                                                     const double* __restrict__ ap,
                                                     const uint8_t* __restrict__ mult,
-                                                    double* __restrict__ part) {
+                                                    double* __restrict__ part, ScalarOp op) {
   __shared__ double sred[32];
   const double alpha = *alpha_p;
   double v[1] = {0.0};
@@ -369,7 +528,7 @@ __global__ void __launch_bounds__(256) k_fcg_update(size_t npts, const double* _
     v[0] += (rq * (1.0 / (double)mult[q])) * rq;
   }
   block_reduce<1>(v, sred);
-  if (threadIdx.x == 0) part[blockIdx.x] = v[0];
+  finish<1>(v, part, op, sred);
 }
 
 template <typename T>
@@ -391,9 +550,7 @@ __global__ void __launch_bounds__(256) k_mul(size_t npts, T* __restrict__ x,
   SSG_GRID_LOOP(q, npts) x[q] = (T)((double)x[q] * y[q]);
 }
 
-// ---------------------------------------------------------------------------
-// deterministic reduction of block partials + solver scalar algebra
-// ---------------------------------------------------------------------------
+// one-block reduction of partials written without a counter
 __global__ void __launch_bounds__(256) k_reduce(const double* __restrict__ part, int nblk,
                                                 int nq, double* __restrict__ sums,
                                                 ScalarOp op) {
@@ -405,67 +562,7 @@ __global__ void __launch_bounds__(256) k_reduce(const double* __restrict__ part,
     block_reduce<1>(v, sred);
     if (threadIdx.x == 0) sums[q] = v[0];
   }
-  if (threadIdx.x != 0) return;
-  double* f = op.frame;
-  switch (op.code) {
-    case OP_NONE:
-      break;
-    case OP_CG_INIT_C:   // c = (w.z)/nunique (pressure); a new solve starts
-      f[F_C] = op.pressure ? sums[0] / op.nunique : 0.0;
-      f[F_ITER] = 0.0;
-      f[F_DONE] = 0.0;
-      break;
-    case OP_CG_INIT_RDZ:  // rdz = (r w).p, |r|_w ; reset counters
-      f[F_RDZ] = sums[0];
-      f[F_ERR0] = sqrt(sums[1]);
-      f[F_ITER] = 0.0;
-      f[F_DONE] = 0.0;
-      f[F_ERR] = sqrt(sums[1]);
-      break;
-    case OP_CG_ALPHA:     // alpha = rdz / (p w).ap
-      f[F_PAP] = sums[0];
-      f[F_ALPHA] = f[F_RDZ] / sums[0];
-      break;
-    case OP_CG_BETA: {    // sums: (r w).z, (r w).r, w.z, w.r
-      const double c = op.pressure ? sums[2] / op.nunique : 0.0;
-      const double rdz = sums[0] - c * sums[3];
-      f[F_C] = c;
-      f[F_BETA] = rdz / f[F_RDZ];
-      f[F_RDZ] = rdz;
-      const double err = sqrt(sums[1]);
-      f[F_ERR] = err;
-      f[F_ITER] += 1.0;
-      const bool go = (err > op.eps) && (f[F_ITER] < (double)op.max_iter);
-      f[F_DONE] = go ? 0.0 : 1.0;
-      if (op.hist && (int)f[F_ITER] <= op.hist_cap) op.hist[(int)f[F_ITER] - 1] = err;
-      break;
-    }
-    case OP_NULL_C:       // c = (w.x)/nunique into frame slot
-      f[F_C] = sums[0] / op.nunique;
-      break;
-    case OP_FCG_BETA:     // beta_k = sums[k] / pap[k]
-      for (int k = 0; k < op.m; ++k) f[F_FBETA + k] = sums[k] / f[F_FPAP + op.pap_idx[k]];
-      break;
-    case OP_FCG_ALPHA:    // pap0 and alpha = (p0 w).r / pap0
-      f[F_FPAP + op.pap_idx[0]] = sums[0];
-      f[F_ALPHA] = sums[1] / sums[0];
-      break;
-    case OP_FCG_ERR: {
-      const double err = sqrt(sums[0]);
-      f[F_ERR] = err;
-      f[F_ITER] += 1.0;
-      const bool go = (err > op.eps) && (f[F_ITER] < (double)op.max_iter);
-      f[F_DONE] = go ? 0.0 : 1.0;
-      if (op.hist && (int)f[F_ITER] <= op.hist_cap) op.hist[(int)f[F_ITER] - 1] = err;
-      break;
-    }
-    case OP_ERR0:
-      f[F_ERR0] = sqrt(sums[0]);
-      f[F_ITER] = 0.0;
-      f[F_DONE] = 0.0;
-      f[F_ERR] = sqrt(sums[0]);
-      break;
-  }
+  if (threadIdx.x == 0) apply_scalar_op(op, sums);
 }
 
 }  // namespace dev
@@ -474,6 +571,8 @@ __global__ void __launch_bounds__(256) k_reduce(const double* __restrict__ part,
 // launchers
 // ---------------------------------------------------------------------------
 using namespace dev;
+
+static ScalarOp op_or_none(const ScalarOp* op) { return op ? *op : ScalarOp(); }
 
 unsigned long long g_launches = 0;   // every launch of this library bumps it
 #define SSG_COUNT() (++g_launches)
@@ -486,8 +585,9 @@ int vec_blocks(size_t npts) {
 
 int ax_epb(int n) {
   // elements per block: up to 256 threads, <= 96 KB of FP64 shared memory
+  const int q = n + (n & 1);
   int epb = 1;
-  while (epb * 2 * n * n <= 256 && (size_t)(epb * 2) * 3 * n * n * n * 8 <= 96 * 1024) epb *= 2;
+  while (epb * 2 * n * n <= 256 && (size_t)(epb * 2) * 3 * n * n * q * 8 <= 96 * 1024) epb *= 2;
   return epb;
 }
 
@@ -495,7 +595,8 @@ template <int N, typename T, bool HELM, bool FUSEP>
 static cudaError_t launch_ax_t(cudaStream_t s, int nel, int epb, T* u, T* au, const T* gf,
                                size_t npts, const double* bj, const double* D,
                                const double* S, double lambda, const PUpdate& pu) {
-  const size_t smem = (2 * N * (N + 1) + (size_t)epb * 3 * N * N * N) * sizeof(double);
+  const size_t smem = (4 * N * AxLayout<N>::P + (size_t)epb * 3 * N * N * AxLayout<N>::Q) *
+                      sizeof(double);
   static bool attr_set = false;
   if (!attr_set) {
     cudaFuncSetAttribute(k_ax<N, T, HELM, FUSEP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -576,24 +677,24 @@ int dss_grid(int n, int nel) {
 template <int N, typename T>
 static cudaError_t run_dss_n(cudaStream_t s, int mode, int nel, const T* in, T* out,
                              const int2* pr, const double* mask, const T* y, const T* y2,
-                             double* part, const double* stop) {
+                             double* part, const double* stop, const ScalarOp& op) {
   const int epb = dss_epb(N);
   const int grd = (nel + epb - 1) / epb;
   switch (mode) {
     case DSS_PLAIN:
-      { SSG_COUNT(); k_dss<N, T, DSS_PLAIN><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, mask, y, y2, part, stop); }
+      { SSG_COUNT(); k_dss<N, T, DSS_PLAIN><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, mask, y, y2, part, stop, op); }
       break;
     case DSS_DOT:
-      { SSG_COUNT(); k_dss<N, T, DSS_DOT><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, mask, y, y2, part, stop); }
+      { SSG_COUNT(); k_dss<N, T, DSS_DOT><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, mask, y, y2, part, stop, op); }
       break;
     case DSS_DOT2:
-      { SSG_COUNT(); k_dss<N, T, DSS_DOT2><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, mask, y, y2, part, stop); }
+      { SSG_COUNT(); k_dss<N, T, DSS_DOT2><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, mask, y, y2, part, stop, op); }
       break;
     case DSS_RESID:
-      { SSG_COUNT(); k_dss<N, T, DSS_RESID><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, mask, y, y2, part, stop); }
+      { SSG_COUNT(); k_dss<N, T, DSS_RESID><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, mask, y, y2, part, stop, op); }
       break;
     case DSS_AVG:
-      { SSG_COUNT(); k_dss<N, T, DSS_AVG><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, mask, y, y2, part, stop); }
+      { SSG_COUNT(); k_dss<N, T, DSS_AVG><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, mask, y, y2, part, stop, op); }
       break;
     default:
       return cudaErrorInvalidValue;
@@ -604,11 +705,11 @@ static cudaError_t run_dss_n(cudaStream_t s, int mode, int nel, const T* in, T* 
 template <typename T>
 static cudaError_t run_dss_t(cudaStream_t s, int mode, int n, int nel, const T* in, T* out,
                              const int* pairs, const double* mask, const T* y, const T* y2,
-                             double* part, const double* stop) {
+                             double* part, const double* stop, const ScalarOp& op) {
   const int2* pr = reinterpret_cast<const int2*>(pairs);
   switch (n) {
 #define SSG_DSSN(NV) \
-  case NV: return run_dss_n<NV, T>(s, mode, nel, in, out, pr, mask, y, y2, part, stop);
+  case NV: return run_dss_n<NV, T>(s, mode, nel, in, out, pr, mask, y, y2, part, stop, op);
     SSG_DSSN(2) SSG_DSSN(3) SSG_DSSN(4) SSG_DSSN(5) SSG_DSSN(6) SSG_DSSN(7)
     SSG_DSSN(8) SSG_DSSN(9) SSG_DSSN(10) SSG_DSSN(11) SSG_DSSN(12)
 #undef SSG_DSSN
@@ -618,12 +719,14 @@ static cudaError_t run_dss_t(cudaStream_t s, int mode, int n, int nel, const T* 
 
 cudaError_t run_dss(cudaStream_t s, int mode, bool fp32, int n, int nel, const void* in,
                     void* out, const int* pairs, const double* mask, const void* y,
-                    const void* y2, double* part, const double* stop) {
+                    const void* y2, double* part, const double* stop,
+                    const ScalarOp* op) {
+  const ScalarOp o = op_or_none(op);
   if (fp32)
     return run_dss_t<float>(s, mode, n, nel, (const float*)in, (float*)out, pairs, mask,
-                            (const float*)y, (const float*)y2, part, stop);
+                            (const float*)y, (const float*)y2, part, stop, o);
   return run_dss_t<double>(s, mode, n, nel, (const double*)in, (double*)out, pairs, mask,
-                           (const double*)y, (const double*)y2, part, stop);
+                           (const double*)y, (const double*)y2, part, stop, o);
 }
 
 cudaError_t run_tensor3(cudaStream_t s, bool fp32, bool add, int nel, int ni, int no,
@@ -649,37 +752,40 @@ cudaError_t run_tensor3(cudaStream_t s, bool fp32, bool add, int nel, int ni, in
 cudaError_t run_cg_update(cudaStream_t s, bool fp32, size_t npts, const double* alpha,
                           void* x, const void* p, void* r, const void* ap, const void* dinv,
                           const uint8_t* mult, void* z, double* part, int nblk,
-                          const double* stop) {
+                          const double* stop, const ScalarOp* op) {
+  const ScalarOp o = op_or_none(op);
   if (fp32)
     { SSG_COUNT(); k_cg_update<float><<<nblk, 256, 0, s>>>(npts, alpha, (float*)x, (const float*)p, (float*)r,
                                             (const float*)ap, (const float*)dinv, mult,
-                                            (float*)z, part, stop); }
+                                            (float*)z, part, stop, o); }
   else
     { SSG_COUNT(); k_cg_update<double><<<nblk, 256, 0, s>>>(npts, alpha, (double*)x, (const double*)p,
                                              (double*)r, (const double*)ap,
-                                             (const double*)dinv, mult, (double*)z, part, stop); }
+                                             (const double*)dinv, mult, (double*)z, part, stop, o); }
   return cudaGetLastError();
 }
 
 cudaError_t run_jacobi(cudaStream_t s, bool fp32, size_t npts, const void* r, const void* dinv,
-                       const uint8_t* mult, void* z, double* part, int nblk) {
+                       const uint8_t* mult, void* z, double* part, int nblk,
+                       const ScalarOp* op) {
+  const ScalarOp o = op_or_none(op);
   if (fp32)
     { SSG_COUNT(); k_jacobi<float><<<nblk, 256, 0, s>>>(npts, (const float*)r, (const float*)dinv, mult,
-                                         (float*)z, part); }
+                                         (float*)z, part, o); }
   else
     { SSG_COUNT(); k_jacobi<double><<<nblk, 256, 0, s>>>(npts, (const double*)r, (const double*)dinv, mult,
-                                          (double*)z, part); }
+                                          (double*)z, part, o); }
   return cudaGetLastError();
 }
 
 template <typename T>
 static cudaError_t run_dots_t(cudaStream_t s, size_t npts, const T* x, const PtrList& ys, int K,
-                              const uint8_t* mult, double* part, int nblk) {
+                              const uint8_t* mult, double* part, int nblk, const ScalarOp& o) {
   switch (K) {
 #define SSG_DOTK(KV)                                                   \
   case KV:                                                             \
     SSG_COUNT();                                                       \
-    k_dots<T, KV><<<nblk, 256, 0, s>>>(npts, x, ys, mult, part);       \
+    k_dots<T, KV><<<nblk, 256, 0, s>>>(npts, x, ys, mult, part, o);    \
     break;
     SSG_DOTK(1) SSG_DOTK(2) SSG_DOTK(3) SSG_DOTK(4) SSG_DOTK(5)
     SSG_DOTK(6) SSG_DOTK(7) SSG_DOTK(8) SSG_DOTK(9) SSG_DOTK(10)
@@ -691,17 +797,19 @@ static cudaError_t run_dots_t(cudaStream_t s, size_t npts, const T* x, const Ptr
 }
 
 cudaError_t run_dots(cudaStream_t s, bool fp32, size_t npts, const void* x, const PtrList& ys,
-                     int K, const uint8_t* mult, double* part, int nblk) {
-  if (fp32) return run_dots_t<float>(s, npts, (const float*)x, ys, K, mult, part, nblk);
-  return run_dots_t<double>(s, npts, (const double*)x, ys, K, mult, part, nblk);
+                     int K, const uint8_t* mult, double* part, int nblk, const ScalarOp* op) {
+  const ScalarOp o = op_or_none(op);
+  if (fp32) return run_dots_t<float>(s, npts, (const float*)x, ys, K, mult, part, nblk, o);
+  return run_dots_t<double>(s, npts, (const double*)x, ys, K, mult, part, nblk, o);
 }
 
 cudaError_t run_wsum(cudaStream_t s, bool fp32, size_t npts, const void* x,
-                     const uint8_t* mult, double* part, int nblk) {
+                     const uint8_t* mult, double* part, int nblk, const ScalarOp* op) {
+  const ScalarOp o = op_or_none(op);
   if (fp32)
-    { SSG_COUNT(); k_wsum<float><<<nblk, 256, 0, s>>>(npts, (const float*)x, mult, part); }
+    { SSG_COUNT(); k_wsum<float><<<nblk, 256, 0, s>>>(npts, (const float*)x, mult, part, o); }
   else
-    { SSG_COUNT(); k_wsum<double><<<nblk, 256, 0, s>>>(npts, (const double*)x, mult, part); }
+    { SSG_COUNT(); k_wsum<double><<<nblk, 256, 0, s>>>(npts, (const double*)x, mult, part, o); }
   return cudaGetLastError();
 }
 
@@ -713,8 +821,9 @@ cudaError_t run_combine(cudaStream_t s, size_t npts, double* x, const PtrList& y
 
 cudaError_t run_fcg_update(cudaStream_t s, size_t npts, const double* alpha, double* u,
                            const double* p, double* r, const double* ap, const uint8_t* mult,
-                           double* part, int nblk) {
-  { SSG_COUNT(); k_fcg_update<<<nblk, 256, 0, s>>>(npts, alpha, u, p, r, ap, mult, part); }
+                           double* part, int nblk, const ScalarOp* op) {
+  const ScalarOp o = op_or_none(op);
+  { SSG_COUNT(); k_fcg_update<<<nblk, 256, 0, s>>>(npts, alpha, u, p, r, ap, mult, part, o); }
   return cudaGetLastError();
 }
 

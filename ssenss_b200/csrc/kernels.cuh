@@ -68,38 +68,74 @@ __device__ __forceinline__ double dss_gather(const T* __restrict__ in,
   cnt = 0;
   const bool ei = i == 0 || i == M, ej = j == 0 || j == M, ek = k == 0 || k == M;
   if (!(ei || ej || ek)) return acc;
-  auto add = [&](int2 p, int node) {
-    if (p.x >= 0) {
-      const size_t s = (size_t)p.x * NT + node;
-      double v = (double)in[s];
-      if (mask) v = v * mask[s];
-      acc += v;
-      ++cnt;
-    }
-  };
-  if (i == 0) add(pr[0], face_node(N, pr[0].y, k, j));
-  if (i == M) add(pr[1], face_node(N, pr[1].y, k, j));
-  if (j == 0) add(pr[2], face_node(N, pr[2].y, k, i));
-  if (j == M) add(pr[3], face_node(N, pr[3].y, k, i));
-  if (k == 0) add(pr[4], face_node(N, pr[4].y, j, i));
-  if (k == M) add(pr[5], face_node(N, pr[5].y, j, i));
+  // source of every possible contribution, in the reference's order: the
+  // x-face (w/e), y-face (s/n), z-face (b/t), the xy-, xz-, yz-edge, the
+  // corner; -1 where the node has none.  All loads are issued before the
+  // additions, which then run in that order.
+  long long s0 = -1, s1 = -1, s2 = -1, s3 = -1, s4 = -1, s5 = -1, s6 = -1;
+  if (ei) {
+    const int2 p = pr[i == M];
+    if (p.x >= 0) s0 = (long long)p.x * NT + face_node(N, p.y, k, j);
+  }
+  if (ej) {
+    const int2 p = pr[2 + (j == M)];
+    if (p.x >= 0) s1 = (long long)p.x * NT + face_node(N, p.y, k, i);
+  }
+  if (ek) {
+    const int2 p = pr[4 + (k == M)];
+    if (p.x >= 0) s2 = (long long)p.x * NT + face_node(N, p.y, j, i);
+  }
   if (ei && ej) {
-    const int q = 6 + ((i == M) | ((j == M) << 1));
-    add(pr[q], edge_node(N, pr[q].y, k));
+    const int2 p = pr[6 + ((i == M) | ((j == M) << 1))];
+    if (p.x >= 0) s3 = (long long)p.x * NT + edge_node(N, p.y, k);
   }
   if (ek && ei) {
-    const int q = 10 + ((i == M) | ((k == M) << 1));
-    add(pr[q], edge_node(N, pr[q].y, j));
+    const int2 p = pr[10 + ((i == M) | ((k == M) << 1))];
+    if (p.x >= 0) s4 = (long long)p.x * NT + edge_node(N, p.y, j);
   }
   if (ek && ej) {
-    const int q = 14 + ((j == M) | ((k == M) << 1));
-    add(pr[q], edge_node(N, pr[q].y, i));
+    const int2 p = pr[14 + ((j == M) | ((k == M) << 1))];
+    if (p.x >= 0) s5 = (long long)p.x * NT + edge_node(N, p.y, i);
   }
   if (ei && ej && ek) {
-    const int q = 18 + ((i == M) | ((j == M) << 1) | ((k == M) << 2));
-    add(pr[q], corner_node(N, pr[q].y));
+    const int2 p = pr[18 + ((i == M) | ((j == M) << 1) | ((k == M) << 2))];
+    if (p.x >= 0) s6 = (long long)p.x * NT + corner_node(N, p.y);
   }
+#define SSG_LD(S) ((S) >= 0 ? (mask ? (double)in[(S)] * mask[(S)] : (double)in[(S)]) : 0.0)
+  const double v0 = SSG_LD(s0), v1 = SSG_LD(s1), v2 = SSG_LD(s2), v3 = SSG_LD(s3),
+               v4 = SSG_LD(s4), v5 = SSG_LD(s5), v6 = SSG_LD(s6);
+#undef SSG_LD
+  if (s0 >= 0) { acc += v0; ++cnt; }
+  if (s1 >= 0) { acc += v1; ++cnt; }
+  if (s2 >= 0) { acc += v2; ++cnt; }
+  if (s3 >= 0) { acc += v3; ++cnt; }
+  if (s4 >= 0) { acc += v4; ++cnt; }
+  if (s5 >= 0) { acc += v5; ++cnt; }
+  if (s6 >= 0) { acc += v6; ++cnt; }
   return acc;
+}
+
+// Node visited by task t of an element, tasks ordered by node class so a
+// warp's nodes share one branch path: face interiors (6 (N-2)^2), edge
+// interiors (12 (N-2)), corners (8), interior nodes ((N-2)^3).
+template <int N>
+__device__ __forceinline__ int class_ordered_node(int t) {
+  if constexpr (N <= 2) {
+    return t;   // every node is a corner
+  } else {
+    constexpr int I = N - 2, F = 6 * I * I, E = 12 * I;
+    if (t < F) {
+      const int f = t / (I * I), r = t % (I * I);
+      return face_node(N, f, 1 + r / I, 1 + r % I);
+    }
+    t -= F;
+    if (t < E) return edge_node(N, t / I, 1 + t % I);
+    t -= E;
+    if (t < 8) return corner_node(N, t);
+    t -= 8;
+    const int a = t / (I * I), b = (t / I) % I, c = t % I;
+    return ((1 + a) * N + 1 + b) * N + 1 + c;
+  }
 }
 
 // ---------------------------------------------------------------------------

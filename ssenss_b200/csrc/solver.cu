@@ -130,6 +130,8 @@ ssg_status cg_solve(ssg_context* c, int level, int var, bool fp32, void* f, void
   const double lam = lambda_of(c);
   cudaStream_t s = c->stream;
   ScalarOp op;
+  op.sums = c->d_sums;
+  op.counter = c->d_counter;
   op.frame = fr;
   op.pressure = pres;
   op.nunique = L.nunique;
@@ -142,17 +144,13 @@ ssg_status cg_solve(ssg_context* c, int level, int var, bool fp32, void* f, void
   if (mask) SSG_CUDA(c, run_mul(s, fp32, np, f, mask));
   SSG_CUDA(c, run_ax(s, L.n, c->nel, 0, helm, fp32, x, W.aploc, gf, np, L.bj, L.D, L.S, lam,
                      nullptr));
+  op.code = OP_NULL_C;
   SSG_CUDA(c, run_dss(s, DSS_RESID, fp32, L.n, c->nel, W.aploc, W.r, c->d_pairs, mask, f,
-                      nullptr, c->d_part));
-  if (pres) {
-    op.code = OP_NULL_C;
-    SSG_CUDA(c, run_reduce(s, c->d_part, nbd, 1, c->d_sums, op));
-    SSG_CUDA(c, run_add_const(s, fp32, np, W.r, fr + F_C, 1));
-  }
+                      nullptr, c->d_part, nullptr, &op));
+  if (pres) SSG_CUDA(c, run_add_const(s, fp32, np, W.r, fr + F_C, 1));
   // z = M^-1 r and its nullspace constant
-  SSG_CUDA(c, run_jacobi(s, fp32, np, W.r, dinv, L.mult, W.z, c->d_part, nb));
   op.code = OP_CG_INIT_C;
-  SSG_CUDA(c, run_reduce(s, c->d_part, nb, 1, c->d_sums, op));
+  SSG_CUDA(c, run_jacobi(s, fp32, np, W.r, dinv, L.mult, W.z, c->d_part, nb, &op));
 
   PUpdateArgs pu;
   pu.z = W.z;
@@ -174,22 +172,17 @@ ssg_status cg_solve(ssg_context* c, int level, int var, bool fp32, void* f, void
       PtrList ys;
       ys.p[0] = W.p;
       ys.p[1] = W.r;
-      SSG_CUDA(c, run_dots(s, fp32, np, W.r, ys, 2, L.mult, c->d_part, nb));
       op.code = OP_CG_INIT_RDZ;
-      SSG_CUDA(c, run_reduce(s, c->d_part, nb, 2, c->d_sums, op));
+      SSG_CUDA(c, run_dots(s, fp32, np, W.r, ys, 2, L.mult, c->d_part, nb, &op));
     }
     // ap = DSS(mask aploc); alpha = rdz / (p w).ap
-    SSG_CUDA(c, run_dss(s, DSS_DOT, fp32, L.n, c->nel, W.aploc, W.ap, c->d_pairs, mask,
-                        W.p, nullptr, c->d_part, stop));
     op.code = OP_CG_ALPHA;
-    op.stop = stop;
-    SSG_CUDA(c, run_reduce(s, c->d_part, nbd, 1, c->d_sums, op));
+    SSG_CUDA(c, run_dss(s, DSS_DOT, fp32, L.n, c->nel, W.aploc, W.ap, c->d_pairs, mask,
+                        W.p, nullptr, c->d_part, stop, &op));
     // x += alpha p; r -= alpha ap; z = M^-1 r; beta; err
-    SSG_CUDA(c, run_cg_update(s, fp32, np, fr + F_ALPHA, x, W.p, W.r, W.ap, dinv, L.mult,
-                              W.z, c->d_part, nb, stop));
     op.code = OP_CG_BETA;
-    SSG_CUDA(c, run_reduce(s, c->d_part, nb, 4, c->d_sums, op));
-    op.stop = nullptr;
+    SSG_CUDA(c, run_cg_update(s, fp32, np, fr + F_ALPHA, x, W.p, W.r, W.ap, dinv, L.mult,
+                              W.z, c->d_part, nb, stop, &op));
     if (sync_each && (it % 8 == 7)) {
       double done;
       SSG_TRY(read_flag(c, fr + F_DONE, &done));
@@ -305,6 +298,8 @@ ssg_status fcg_solve(ssg_context* c, const double* f, double* u, double eps, int
                        ? std::min(std::min(info->history_cap, max_iter), w->hist_cap)
                        : 0;
   ScalarOp op;
+  op.sums = c->d_sums;
+  op.counter = c->d_counter;
   op.frame = fr;
   op.pressure = 1;
   op.nunique = L.nunique;
@@ -316,16 +311,14 @@ ssg_status fcg_solve(ssg_context* c, const double* f, double* u, double eps, int
   // r = f - A u; subtract_nullspace(r)
   SSG_CUDA(c, run_ax(s, L.n, c->nel, 0, false, false, u, w->aploc, L.gf, np, nullptr, L.D,
                      L.D, 0.0, nullptr));
-  SSG_CUDA(c, run_dss(s, DSS_RESID, false, L.n, c->nel, w->aploc, w->r, c->d_pairs, nullptr,
-                      f, nullptr, c->d_part));
   op.code = OP_NULL_C;
-  SSG_CUDA(c, run_reduce(s, c->d_part, nbd, 1, c->d_sums, op));
+  SSG_CUDA(c, run_dss(s, DSS_RESID, false, L.n, c->nel, w->aploc, w->r, c->d_pairs, nullptr,
+                      f, nullptr, c->d_part, nullptr, &op));
   SSG_CUDA(c, run_add_const(s, false, np, w->r, fr + F_C, 1));
   PtrList ys;
   ys.p[0] = w->r;
-  SSG_CUDA(c, run_dots(s, false, np, w->r, ys, 1, L.mult, c->d_part, nb));
   op.code = OP_ERR0;
-  SSG_CUDA(c, run_reduce(s, c->d_part, nb, 1, c->d_sums, op));
+  SSG_CUDA(c, run_dots(s, false, np, w->r, ys, 1, L.mult, c->d_part, nb, &op));
 
   int pslot[11], aslot[10];
   for (int k = 0; k < 11; ++k) pslot[k] = k;
@@ -336,9 +329,8 @@ ssg_status fcg_solve(ssg_context* c, const double* f, double* u, double eps, int
     m = std::min(m, j);
     SSG_TRY(mg_apply(c, w->r, w->z, eps));
     // subtract_nullspace(z)
-    SSG_CUDA(c, run_wsum(s, false, np, w->z, L.mult, c->d_part, nb));
     op.code = OP_NULL_C;
-    SSG_CUDA(c, run_reduce(s, c->d_part, nb, 1, c->d_sums, op));
+    SSG_CUDA(c, run_wsum(s, false, np, w->z, L.mult, c->d_part, nb, &op));
     SSG_CUDA(c, run_add_const(s, false, np, w->z, fr + F_C, 1));
     // beta_k = (z w).ap_k / pap_k
     if (m > 0) {
@@ -348,9 +340,8 @@ ssg_status fcg_solve(ssg_context* c, const double* f, double* u, double eps, int
         op.pap_idx[k] = aslot[k];
       }
       op.m = m;
-      SSG_CUDA(c, run_dots(s, false, np, w->z, yb, m, L.mult, c->d_part, nb));
       op.code = OP_FCG_BETA;
-      SSG_CUDA(c, run_reduce(s, c->d_part, nb, m, c->d_sums, op));
+      SSG_CUDA(c, run_dots(s, false, np, w->z, yb, m, L.mult, c->d_part, nb, &op));
     }
     // shift the directions and form p0 = z - sum beta_k p_k
     const int tail = pslot[m];
@@ -373,15 +364,14 @@ ssg_status fcg_solve(ssg_context* c, const double* f, double* u, double eps, int
     // ap0 = A p0; pap0 and alpha = (p0 w).r / pap0
     SSG_CUDA(c, run_ax(s, L.n, c->nel, 0, false, false, p0, w->aploc, L.gf, np, nullptr, L.D,
                        L.D, 0.0, nullptr));
-    SSG_CUDA(c, run_dss(s, DSS_DOT2, false, L.n, c->nel, w->aploc, ap0, c->d_pairs, nullptr,
-                        p0, w->r, c->d_part));
     op.pap_idx[0] = aslot[0];
     op.code = OP_FCG_ALPHA;
-    SSG_CUDA(c, run_reduce(s, c->d_part, nbd, 2, c->d_sums, op));
+    SSG_CUDA(c, run_dss(s, DSS_DOT2, false, L.n, c->nel, w->aploc, ap0, c->d_pairs, nullptr,
+                        p0, w->r, c->d_part, nullptr, &op));
     // u += alpha p0; r -= alpha ap0; err
-    SSG_CUDA(c, run_fcg_update(s, np, fr + F_ALPHA, u, p0, w->r, ap0, L.mult, c->d_part, nb));
     op.code = OP_FCG_ERR;
-    SSG_CUDA(c, run_reduce(s, c->d_part, nb, 1, c->d_sums, op));
+    SSG_CUDA(c, run_fcg_update(s, np, fr + F_ALPHA, u, p0, w->r, ap0, L.mult, c->d_part, nb,
+                               &op));
     double done;
     SSG_TRY(read_flag(c, fr + F_DONE, &done));
     if (done != 0.0) break;

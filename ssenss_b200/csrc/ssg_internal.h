@@ -114,6 +114,7 @@ struct ssg_context {
   double* d_part = nullptr;     // block partial sums
   size_t part_cap = 0;
   double* d_sums = nullptr;     // 16 raw sums
+  unsigned* d_counter = nullptr;  // last-block counter of the fused reductions
   double* d_sc = nullptr;       // solver frames
   double* h_pin = nullptr;      // pinned host scalars
   // staging for host arguments

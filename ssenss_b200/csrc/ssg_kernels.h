@@ -41,6 +41,8 @@ struct ScalarOp {
   int m = 0;
   int pap_idx[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
   const double* stop = nullptr;   // skip when *stop != 0 (finished solve)
+  double* sums = nullptr;         // raw reduced sums (16 doubles)
+  unsigned* counter = nullptr;    // last-block counter; null: partials only
 };
 
 // up to 10 vectors passed by value to a kernel (capturable: no upload)
@@ -74,24 +76,28 @@ cudaError_t run_ax(cudaStream_t s, int n, int nel, int epb, bool helm, bool fp32
                    const PUpdateArgs* pua);
 cudaError_t run_dss(cudaStream_t s, int mode, bool fp32, int n, int nel, const void* in,
                     void* out, const int* pairs, const double* mask, const void* y,
-                    const void* y2, double* part, const double* stop = nullptr);
+                    const void* y2, double* part, const double* stop = nullptr,
+                    const ScalarOp* op = nullptr);
 cudaError_t run_tensor3(cudaStream_t s, bool fp32, bool add, int nel, int ni, int no,
                         const double* A, const void* in, void* out);
 cudaError_t run_cg_update(cudaStream_t s, bool fp32, size_t npts, const double* alpha,
                           void* x, const void* p, void* r, const void* ap, const void* dinv,
                           const uint8_t* mult, void* z, double* part, int nblk,
-                          const double* stop = nullptr);
+                          const double* stop = nullptr, const ScalarOp* op = nullptr);
 cudaError_t run_jacobi(cudaStream_t s, bool fp32, size_t npts, const void* r, const void* dinv,
-                       const uint8_t* mult, void* z, double* part, int nblk);
+                       const uint8_t* mult, void* z, double* part, int nblk,
+                       const ScalarOp* op = nullptr);
 cudaError_t run_dots(cudaStream_t s, bool fp32, size_t npts, const void* x, const PtrList& ys,
-                     int K, const uint8_t* mult, double* part, int nblk);
+                     int K, const uint8_t* mult, double* part, int nblk,
+                     const ScalarOp* op = nullptr);
 cudaError_t run_wsum(cudaStream_t s, bool fp32, size_t npts, const void* x,
-                     const uint8_t* mult, double* part, int nblk);
+                     const uint8_t* mult, double* part, int nblk,
+                     const ScalarOp* op = nullptr);
 cudaError_t run_combine(cudaStream_t s, size_t npts, double* x, const PtrList& ys,
                         const double* coef, int K, double sign);
 cudaError_t run_fcg_update(cudaStream_t s, size_t npts, const double* alpha, double* u,
                            const double* p, double* r, const double* ap, const uint8_t* mult,
-                           double* part, int nblk);
+                           double* part, int nblk, const ScalarOp* op = nullptr);
 cudaError_t run_add_const(cudaStream_t s, bool fp32, size_t npts, void* x, const double* a,
                           int neg);
 cudaError_t run_convert(cudaStream_t s, size_t npts, const void* in, bool in32, void* out,
