@@ -20,6 +20,7 @@
 // s, n, b, t; edges sw..tn; corners 0..7) from the pairing built on the host
 // (src/init.c:68-130), accumulating in FP64: for FP64 data the result is
 // bitwise equal to the reference's.
+#include <cuda/atomic>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -114,14 +115,15 @@ __device__ __forceinline__ void finish(const double (&v)[NQ], double* __restrict
     for (int q = 0; q < NQ; ++q) part[q * gridDim.x + blockIdx.x] = v[q];
     s_last = 0;
     if (op.counter) {
-      __threadfence();
-      const unsigned prev = atomicAdd(op.counter, 1u);
+      // release: this block's partials are visible before its arrival
+      // counts; acquire: the last block sees every partial
+      cuda::atomic_ref<unsigned, cuda::thread_scope_device> arrived(*op.counter);
+      const unsigned prev = arrived.fetch_add(1u, cuda::memory_order_acq_rel);
       s_last = prev == gridDim.x - 1;
     }
   }
   __syncthreads();
   if (!s_last) return;
-  __threadfence();
   double s[NQ];
 #pragma unroll
   for (int q = 0; q < NQ; ++q) {
@@ -320,35 +322,69 @@ __global__ void __launch_bounds__(256) k_dss(int nel, int epb, const T* __restri
                                              const T* __restrict__ y2,
                                              double* __restrict__ part,
                                              const double* __restrict__ stop, ScalarOp op) {
-  constexpr int NT = N * N * N;
+  constexpr int NT = N * N * N, NN = N * N;
+  constexpr int I = N > 2 ? N - 2 : 0, F = 6 * I * I, EC = 12 * I + 8;
+  constexpr int ID = I > 0 ? I : 1, II = ID * ID;   // divisors (N = 2 has no
+                                                    // face or interior nodes)
   if (stop && *stop != 0.0) return;   // uniform over the block
   __shared__ int2 sp[64 * 26];
+  __shared__ short sface[6 * NN];     // node of face f at face position p
   __shared__ double sred[2 * 32];
-  const int e0 = blockIdx.x * epb;
-  const int ne = min(epb, nel - e0);
-  for (int q = threadIdx.x; q < ne * 26; q += blockDim.x) sp[q] = pairs[(size_t)e0 * 26 + q];
-  __syncthreads();
+  for (int q = threadIdx.x; q < 6 * NN; q += blockDim.x)
+    sface[q] = (short)face_node(N, q / NN, (q % NN) / N, q % N);
   double s0 = 0.0, s1 = 0.0;
-  for (int q = threadIdx.x; q < ne * NT; q += blockDim.x) {
-    const int z = q / NT;
-    const int loc = class_ordered_node<N>(q - z * NT);
-    const size_t gi = (size_t)(e0 + z) * NT + loc;
-    int cnt = 0;
-    const double acc = dss_gather<N, T>(in, mask, sp + z * 26, gi, loc, cnt);
-    const double w = 1.0 / (1.0 + (double)cnt);
-    if (MODE == DSS_RESID) {
-      const T r = (T)((double)y[gi] + -acc);
-      out[gi] = r;
-      s0 += (double)r * w;
-    } else if (MODE == DSS_AVG) {
-      out[gi] = (T)(acc * w);
-    } else {
-      const T a = (T)acc;
-      out[gi] = a;
-      if (MODE == DSS_DOT || MODE == DSS_DOT2) {
-        const double yw = (double)y[gi] * w;
-        s0 += yw * (double)a;
-        if (MODE == DSS_DOT2) s1 += yw * (double)y2[gi];
+  for (int e0 = blockIdx.x * epb; e0 < nel; e0 += gridDim.x * epb) {
+    const int ne = min(epb, nel - e0);
+    __syncthreads();
+    for (int q = threadIdx.x; q < ne * 26; q += blockDim.x) sp[q] = pairs[(size_t)e0 * 26 + q];
+    __syncthreads();
+    for (int q = threadIdx.x; q < ne * NT; q += blockDim.x) {
+      const int z = q / NT, t = q - z * NT;
+      const size_t eb = (size_t)(e0 + z) * NT;
+      int loc, cnt = 0;
+      double acc;
+      if (t < F) {
+        // face interior: own value plus the one neighbour face copy
+        const int f = t / II, r = t - f * II;
+        const int pos = (1 + r / ID) * N + 1 + r % ID;
+        loc = sface[f * NN + pos];
+        const int2 p = sp[z * 26 + f];
+        acc = (double)in[eb + loc];
+        if (mask) acc = acc * mask[eb + loc];
+        if (p.x >= 0) {
+          const size_t src = (size_t)p.x * NT + sface[p.y * NN + pos];
+          double v = (double)in[src];
+          if (mask) v = v * mask[src];
+          acc += v;
+          cnt = 1;
+        }
+      } else if (t < F + EC) {
+        // edges and corners: the general ordered gather
+        loc = class_ordered_node<N>(t);
+        acc = dss_gather<N, T>(in, mask, sp + z * 26, eb + loc, loc, cnt);
+      } else {
+        // element interior: no neighbour shares the node
+        const int u = t - F - EC;
+        loc = ((1 + u / II) * N + 1 + (u / ID) % ID) * N + 1 + u % ID;
+        acc = (double)in[eb + loc];
+        if (mask) acc = acc * mask[eb + loc];
+      }
+      const size_t gi = eb + loc;
+      const double w = 1.0 / (1.0 + (double)cnt);
+      if (MODE == DSS_RESID) {
+        const T rv = (T)((double)y[gi] + -acc);
+        out[gi] = rv;
+        s0 += (double)rv * w;
+      } else if (MODE == DSS_AVG) {
+        out[gi] = (T)(acc * w);
+      } else {
+        const T av = (T)acc;
+        out[gi] = av;
+        if (MODE == DSS_DOT || MODE == DSS_DOT2) {
+          const double yw = (double)y[gi] * w;
+          s0 += yw * (double)av;
+          if (MODE == DSS_DOT2) s1 += yw * (double)y2[gi];
+        }
       }
     }
   }
@@ -579,7 +615,7 @@ unsigned long long g_launches = 0;   // every launch of this library bumps it
 
 int vec_blocks(size_t npts) {
   size_t b = (npts + 255) / 256;
-  const size_t cap = 148 * 8;
+  const size_t cap = 148 * 4;
   return (int)(b < cap ? (b ? b : 1) : cap);
 }
 
@@ -671,7 +707,8 @@ int dss_epb(int n) {
 
 int dss_grid(int n, int nel) {
   const int epb = dss_epb(n);
-  return (nel + epb - 1) / epb;
+  const int g = (nel + epb - 1) / epb;
+  return g < 148 * 4 ? g : 148 * 4;
 }
 
 template <int N, typename T>
@@ -679,7 +716,7 @@ static cudaError_t run_dss_n(cudaStream_t s, int mode, int nel, const T* in, T* 
                              const int2* pr, const double* mask, const T* y, const T* y2,
                              double* part, const double* stop, const ScalarOp& op) {
   const int epb = dss_epb(N);
-  const int grd = (nel + epb - 1) / epb;
+  const int grd = dss_grid(N, nel);
   switch (mode) {
     case DSS_PLAIN:
       { SSG_COUNT(); k_dss<N, T, DSS_PLAIN><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, mask, y, y2, part, stop, op); }
