@@ -615,7 +615,7 @@ unsigned long long g_launches = 0;   // every launch of this library bumps it
 
 int vec_blocks(size_t npts) {
   size_t b = (npts + 255) / 256;
-  const size_t cap = 148 * 4;
+  const size_t cap = 148 * 8;
   return (int)(b < cap ? (b ? b : 1) : cap);
 }
 
