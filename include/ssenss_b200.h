@@ -147,11 +147,15 @@ ssg_status ssg_setup_dealias(ssg_context *ctx, int m, const double *deriv,
 		const double *weights, const double *tinv_jac,
 		const double *jac_det, const double *interp);
 
-/* Geometry of level 0 for particles: jac (9 x nel x n^3, J[a][b] =
- * dx_a/dr_b) and tinv_jac (9 x nel x n^3) as the reference stores them.
- * Drop-in path only; ssg_setup_mesh builds them itself. */
-ssg_status ssg_setup_particle_geometry(ssg_context *ctx, const double *jac,
-		const double *tinv_jac);
+/* Level-0 data the particle walk reads (src/particles.c:493-539): the GLL
+ * points (n; sel->basis->points, which the reference computes by an
+ * eigenvalue solve, so they may differ in the last bit from this library's
+ * own; NULL keeps the library's), jac (9 x nel x n^3, J[a][b] = dx_a/dr_b)
+ * and tinv_jac (9 x nel x n^3) as the reference stores them.  Passing the
+ * reference's arrays makes the walk bitwise the reference's. ssg_setup_mesh
+ * builds its own; this call replaces them (before or after setup). */
+ssg_status ssg_setup_particle_geometry(ssg_context *ctx, const double *points,
+		const double *jac, const double *tinv_jac);
 
 ssg_status ssg_mesh_info(const ssg_context *ctx, int *n, int *nel,
 		int *nlevels, int *orders /* >= 8 entries or NULL */);

@@ -68,6 +68,13 @@ class _Common:
         n = self.n if n is None else n
         return (self.nel, n, n, n)
 
+    @staticmethod
+    def gll(n):
+        """The oracle's GLL points and weights of order n."""
+        x, w = np.empty(n), np.empty(n)
+        Oracle.lib().og_gll(n, _d(x), _d(w))
+        return x, w
+
     def _vshape(self, n=None):
         n = self.n if n is None else n
         return (3, self.nel, n, n, n)
@@ -115,6 +122,7 @@ class Oracle(_Common):
             L.og_particles_advance.argtypes = [C.c_void_p, C.c_size_t, _dp, _ip,
                                                _dp]
             L.og_particles_advance.restype = C.c_int
+            L.og_set_particle_basis.argtypes = [C.c_void_p, _dp, _dp, _dp]
             L.og_point_interp.argtypes = [C.c_int, _dp, _dp, C.c_double,
                                           C.c_double, C.c_double]
             L.og_point_interp.restype = C.c_double
@@ -220,6 +228,19 @@ class Oracle(_Common):
         self.lib().og_convection(self.h, _d(u), _d(v), _d(out))
         return out
 
+    def particle_geometry(self):
+        """(points, jac, tinv) the particle walk reads; jac/tinv (9, nel, n, n, n)."""
+        x, _ = self.gll(self.n)
+        jac = np.stack([self.geometry(0, 10 + a) for a in range(9)])
+        tinv = np.stack([self.geometry(0, 19 + a) for a in range(9)])
+        return x, jac, tinv
+
+    def set_particle_basis(self, points, jac, tinv):
+        """Walk particles on these GLL points and level-0 factors (bitwise
+        parity with a caller whose points differ in the last bit)."""
+        self._pb = (_f64(points), _f64(jac), _f64(tinv))
+        self.lib().og_set_particle_basis(self.h, *(_d(a) for a in self._pb))
+
     def particles_advance(self, state, ints, ur):
         state = _f64(state).copy()
         ints = np.ascontiguousarray(ints, dtype=np.int32).copy()
@@ -274,6 +295,7 @@ class Reference(_Common):
             L.ssgref_get_field.argtypes = [C.c_int, C.c_int, _dp]
             L.ssgref_set_field.argtypes = [C.c_int, C.c_int, _dp]
             L.ssgref_particles_advance.argtypes = [C.c_size_t, _dp, _ip]
+            L.ssgref_set_level0_factor.argtypes = [C.c_int, _dp]
             L.ssgref_particles_advance.restype = C.c_int
             cls._lib = L
         return cls._lib
@@ -398,6 +420,20 @@ class Reference(_Common):
 
     def set_field(self, which, hist_level, src):
         self.lib().ssgref_set_field(which, hist_level, _d(_f64(src)))
+
+    def particle_geometry(self):
+        """(points, jac, tinv) the reference's particle walk reads."""
+        x = self.basis(0)[0]
+        jac = np.stack([self.geometry(0, 10 + a) for a in range(9)])
+        tinv = np.stack([self.geometry(0, 19 + a) for a in range(9)])
+        return x, jac, tinv
+
+    def set_particle_factors(self, jac, tinv):
+        """Overwrite the level-0 jac / tinv_jac (9, nel, n, n, n) the
+        reference's particle walk reads."""
+        for a in range(9):
+            self.lib().ssgref_set_level0_factor(10 + a, _d(_f64(jac[a])))
+            self.lib().ssgref_set_level0_factor(19 + a, _d(_f64(tinv[a])))
 
     def particles_advance(self, state, ints, ur):
         """ur: (3 levels, 3 comps, nel, n, n, n), oldest level first."""

@@ -224,7 +224,12 @@ static double ***geom_component(struct element *s, int which)
 	case 7: return g->grid->x;
 	case 8: return g->grid->y;
 	case 9: return g->grid->z;
-	default: return (double ***) NULL;
+	default:
+		if (which >= 10 && which < 19)
+			return *g->jac->ind[(which - 10) / 3][(which - 10) % 3];
+		if (which >= 19 && which < 28)
+			return *g->tinv_jac->ind[(which - 19) / 3][(which - 19) % 3];
+		return (double ***) NULL;
 	}
 }
 
@@ -238,12 +243,28 @@ static void switch_level(int level)
 }
 
 /* Geometric factors of a level: comp 0..5 = G11,G12,G13,G22,G23,G33,
- * 6 = det J, 7..9 = x,y,z of the GLL grid. */
+ * 6 = det J, 7..9 = x,y,z of the GLL grid, 10..18 = jac[a][b] = dx_a/dr_b,
+ * 19..27 = tinv_jac[a][b] (level 0: the factors the particle walk reads,
+ * src/particles.c:517-539). */
 void ssgref_level_geometry(int level, int comp, double *dst)
 {
 	switch_level(level);
 	put_field(dst, geom_component, level, comp);
 	switch_level(0);
+}
+
+/* Overwrite a level-0 factor the particle walk reads (comp 10..27 as
+ * above), so that a particle test can run the reference on factors it
+ * also hands to another implementation bit for bit. */
+void ssgref_set_level0_factor(int comp, const double *src)
+{
+	if (comp < 10 || comp >= 28)
+		return;
+	const int m = (*H_sel)->basis->n;
+	const size_t nt = (size_t) m * m * m;
+	for (int e = 0; e < H_nel; ++e)
+		memcpy(**geom_component(H_sel[e], comp), src + e * nt,
+				nt * sizeof(double));
 }
 
 /* Per-level preconditioner arrays, contiguous over elements:

@@ -55,6 +55,9 @@ struct og_ctx {
 	level_t conv;
 	double jconv[MAXN * MAXN];  /* jconv[i*n+p] = l_p^n(x_i^m) */
 	double *inv_mass;
+	/* particle walk: GLL points and level-0 jac / tinv it reads; NULL =
+	 * the oracle's own (og_set_particle_basis overrides them) */
+	double *ppts, *pjac, *ptinv;
 };
 
 static double *dalloc(size_t n)
@@ -792,7 +795,28 @@ void og_destroy(og_ctx *c)
 	free(c->pairs);
 	free(c->bc);
 	free(c->inv_mass);
+	free(c->ppts);
+	free(c->pjac);
+	free(c->ptinv);
 	free(c);
+}
+
+/* The reference's GLL points come from an eigenvalue solve, so they can
+ * differ from og_gll's in the last bit; a bitwise particle walk has to read
+ * the caller's points and factors (jac, tinv: 9 x nel x n^3 each). */
+void og_set_particle_basis(og_ctx *c, const double *points, const double *jac,
+		const double *tinv)
+{
+	const size_t np = c->lev[0].nt * c->nel;
+	free(c->ppts);
+	free(c->pjac);
+	free(c->ptinv);
+	c->ppts = dalloc(c->n);
+	c->pjac = dalloc(9 * np);
+	c->ptinv = dalloc(9 * np);
+	memcpy(c->ppts, points, c->n * sizeof(double));
+	memcpy(c->pjac, jac, 9 * np * sizeof(double));
+	memcpy(c->ptinv, tinv, 9 * np * sizeof(double));
 }
 
 void og_set_params(og_ctx *c, double t, double dt, double visc)
@@ -1264,7 +1288,18 @@ double og_point_interp(int n, const double *x, const double *f, double xp,
 typedef struct {
 	og_ctx *c;
 	const double *ur;     /* [lev][comp][e][n^3] */
+	const double *x;      /* GLL points */
 } pctx;
+
+static const double *pfactor(const pctx *P, int tinv, int a, int e)
+{
+	const og_ctx *c = P->c;
+	const level_t *L = &c->lev[0];
+	const double *stored = tinv ? c->ptinv : c->pjac;
+	if (stored)
+		return stored + ((size_t) a * c->nel + e) * L->nt;
+	return (tinv ? L->tinv[a] : L->jac[a]) + e * L->nt;
+}
 
 static const double *ur_block(const pctx *P, int lev, int comp, int e)
 {
@@ -1288,13 +1323,13 @@ static double fluid_velocity(const pctx *P, int e, const double *y, double t,
 	const double cc = 0.5 * d0 * d1 / dt2;
 	double u0 = 0.0, u1 = 0.0, u2 = 0.0;
 	if (fabs(a) > eps)
-		u0 = og_point_interp(L->n, L->b.x, ur_block(P, 0, comp, e),
+		u0 = og_point_interp(L->n, P->x, ur_block(P, 0, comp, e),
 				y[0], y[1], y[2]);
 	if (fabs(b) > eps)
-		u1 = og_point_interp(L->n, L->b.x, ur_block(P, 1, comp, e),
+		u1 = og_point_interp(L->n, P->x, ur_block(P, 1, comp, e),
 				y[0], y[1], y[2]);
 	if (fabs(cc) > eps)
-		u2 = og_point_interp(L->n, L->b.x, ur_block(P, 2, comp, e),
+		u2 = og_point_interp(L->n, P->x, ur_block(P, 2, comp, e),
 				y[0], y[1], y[2]);
 	return a * u0 + b * u1 + cc * u2;
 }
@@ -1407,12 +1442,10 @@ static int closest_face(const double *s)
 }
 
 /* interpolate a 3x3 geometric factor component block at the particle */
-static double factor_at(const pctx *P, double *const *fac, int a, int e,
-		const double *s)
+static double factor_at(const pctx *P, int tinv, int a, int e, const double *s)
 {
-	const level_t *L = &P->c->lev[0];
-	return og_point_interp(L->n, L->b.x, fac[a] + e * L->nt, s[0], s[1],
-			s[2]);
+	return og_point_interp(P->c->lev[0].n, P->x, pfactor(P, tinv, a, e), s[0],
+			s[1], s[2]);
 }
 
 /* Cross into the neighbour through the closest face, converting the
@@ -1426,13 +1459,12 @@ static void new_element(const pctx *P, double *s, int *st)
 	const int e = st[0];
 	const int j = closest_face(s);
 	const int nb = c->neigh[26 * e + j];
-	const level_t *L = &c->lev[0];
 	if (nb >= 0) {
 		st[0] = nb;
 		for (int comp = 0; comp < 3; ++comp) {
 			double dx[3];
 			for (int i = 0; i < 3; ++i)
-				dx[i] = factor_at(P, L->jac, 3 * comp + i, e, s);
+				dx[i] = factor_at(P, 0, 3 * comp + i, e, s);
 			s[3 + comp] = s[3] * dx[0] + s[4] * dx[1] + s[5] * dx[2];
 		}
 	} else {
@@ -1448,7 +1480,6 @@ static void new_element(const pctx *P, double *s, int *st)
 static void new_location(const pctx *P, double *s, int *st)
 {
 	const og_ctx *c = P->c;
-	const level_t *L = &c->lev[0];
 	const int e = st[0];
 	double y0[6], x[2];
 	memcpy(y0, s, sizeof(y0));
@@ -1467,7 +1498,7 @@ static void new_location(const pctx *P, double *s, int *st)
 			s[i] = x[j++];
 		double dx[3];
 		for (int a = 0; a < 3; ++a)
-			dx[a] = factor_at(P, L->tinv, 3 * a + i, e, s);
+			dx[a] = factor_at(P, 1, 3 * a + i, e, s);
 		s[3 + i] = s[3] * dx[0] + s[4] * dx[1] + s[5] * dx[2];
 	}
 	st[1] = st[0];
@@ -1477,7 +1508,7 @@ static void new_location(const pctx *P, double *s, int *st)
 int og_particles_advance(og_ctx *c, size_t np, double *state, int *ints,
 		const double *ur)
 {
-	pctx P = { c, ur };
+	pctx P = { c, ur, c->ppts ? c->ppts : c->lev[0].b.x };
 	for (size_t i = 0; i < np; ++i)
 		ints[3 * i + 2] = ST_OUTSIDE;
 	int pass = 0, unfinished;

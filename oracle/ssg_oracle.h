@@ -76,6 +76,10 @@ void og_convection(og_ctx *c, const double *u, const double *v, double *out);
 /* ur: 3 history levels (t-2dt, t-dt, t) x 3 components x nel x n^3.
  * state: np x {x,y,z,u,v,w,t,tau}; ints: np x {el, old_el, status}.
  * Returns the number of walk passes. */
+/* particle walk on the caller's GLL points and level-0 jac / tinv
+ * (9 x nel x n^3 each), e.g. the reference's own */
+void og_set_particle_basis(og_ctx *c, const double *points, const double *jac,
+		const double *tinv);
 int og_particles_advance(og_ctx *c, size_t np, double *state, int *ints,
 		const double *ur);
 double og_point_interp(int n, const double *x, const double *f, double xp,

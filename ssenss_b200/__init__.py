@@ -107,6 +107,44 @@ class Context:
             neigh.ctypes.data_as(_lib._ip)), "setup_mesh")
         self._info()
 
+    # -- drop-in set-up from the caller's own discretisation -------------------
+    @staticmethod
+    def _dbl(a):
+        if a is None:
+            return None, None
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        return a, a.ctypes.data_as(_lib._dp)
+
+    def setup_connectivity(self, neigh):
+        """ssg_setup_connectivity: the reference's 26-neighbour table (nel, 26)."""
+        neigh = np.ascontiguousarray(neigh, dtype=np.int32)
+        self._check(self.lib.ssg_setup_connectivity(
+            self.h, int(neigh.shape[0]), neigh.ctypes.data_as(_lib._ip)), "setup_connectivity")
+
+    def setup_level(self, level, n, deriv, svv_deriv, weights, geom, jac_det, interp=None):
+        """ssg_setup_level with the reference's stored arrays (deriv d[j][i],
+        geom (6, nel, n, n, n), jac_det (nel, n, n, n), interp n_coarse x n_fine)."""
+        keep = [self._dbl(a) for a in (deriv, svv_deriv, weights, geom, jac_det, interp)]
+        self._check(self.lib.ssg_setup_level(self.h, int(level), int(n),
+                                             *(k[1] for k in keep)), "setup_level")
+
+    def setup_finish(self):
+        self._check(self.lib.ssg_setup_finish(self.h), "setup_finish")
+        self._info()
+
+    def setup_dealias(self, m, deriv, weights, tinv_jac, jac_det, interp):
+        """ssg_setup_dealias: conv_basis order m and its stored factors."""
+        keep = [self._dbl(a) for a in (deriv, weights, tinv_jac, jac_det, interp)]
+        self._check(self.lib.ssg_setup_dealias(self.h, int(m), *(k[1] for k in keep)),
+                    "setup_dealias")
+
+    def setup_particle_geometry(self, points, jac, tinv_jac):
+        """ssg_setup_particle_geometry: the walk's GLL points (None: the
+        library's) and level-0 jac / tinv_jac (9, nel, n, n, n)."""
+        keep = [self._dbl(a) for a in (points, jac, tinv_jac)]
+        self._check(self.lib.ssg_setup_particle_geometry(self.h, *(k[1] for k in keep)),
+                    "setup_particle_geometry")
+
     def _info(self):
         n, nel, nl = C.c_int(), C.c_int(), C.c_int()
         orders = (C.c_int * 8)()

@@ -44,7 +44,7 @@ SIGNATURES = [
                                   _dp, _dp]),
     ("ssg_setup_finish", C.c_int, [C.c_void_p]),
     ("ssg_setup_dealias", C.c_int, [C.c_void_p, C.c_int, _dp, _dp, _dp, _dp, _dp]),
-    ("ssg_setup_particle_geometry", C.c_int, [C.c_void_p, _dp, _dp]),
+    ("ssg_setup_particle_geometry", C.c_int, [C.c_void_p, _dp, _dp, _dp]),
     ("ssg_mesh_info", C.c_int, [C.c_void_p, _ip, _ip, _ip, _ip]),
     ("ssg_level_data", C.c_int, [C.c_void_p, C.c_int, C.c_int, _dp]),
     ("ssg_global_opeval", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),

@@ -74,9 +74,18 @@ static void free_mesh(ssg_context* c) {
   dfree(c->d_pairs); c->d_pairs = nullptr;
   dfree(c->inv_mass); c->inv_mass = nullptr;
   dfree(c->conv_tinv); dfree(c->conv_bj); dfree(c->conv_D); dfree(c->conv_J);
-  c->conv_tinv = c->conv_bj = c->conv_D = c->conv_J = nullptr;
+  dfree(c->conv_scratch);
+  c->conv_tinv = c->conv_bj = c->conv_D = c->conv_J = c->conv_scratch = nullptr;
+  c->m = 0;
   dfree(c->p_jac); dfree(c->p_tinv); dfree(c->p_ur); dfree(c->p_x);
   c->p_jac = c->p_tinv = c->p_ur = c->p_x = nullptr;
+  dfree(c->d_neigh); c->d_neigh = nullptr;
+  dfree(c->d_passes); c->d_passes = nullptr;
+  c->has_ur = false;
+  dfree(c->p_state); c->p_state = nullptr;
+  if (c->p_ints) cudaFree(c->p_ints);
+  c->p_ints = nullptr;
+  c->p_cap = 0;
   dfree(c->d_part); c->d_part = nullptr;
   for (auto& s : c->d_stage) { dfree(s); s = nullptr; }
   c->stage_cap = 0;
@@ -91,6 +100,57 @@ static std::vector<double> rho3(const std::vector<double>& w) {
     for (int j = 0; j < n; ++j)
       for (int i = 0; i < n; ++i) r[(k * n + j) * n + i] = (w[i] * w[j]) * w[k];
   return r;
+}
+
+// Dealiasing-grid factors: tinv (9 x nel x m^3), rho J at the m points, the
+// m-point derivative matrix and the n -> m interpolation matrix
+// (initialise_convection_geometry, src/main.c:60-64, src/geometry.c).
+static ssg_status upload_conv(ssg_context* c) {
+  const ssg::HostMesh& H = c->host;
+  const ssg::HostLevel& m = H.conv;
+  const int nel = H.nel;
+  dfree(c->conv_tinv); dfree(c->conv_bj); dfree(c->conv_D); dfree(c->conv_J);
+  dfree(c->conv_scratch);
+  c->conv_tinv = c->conv_bj = c->conv_D = c->conv_J = c->conv_scratch = nullptr;
+  c->m = m.n;
+  const size_t mp = m.nt * nel;
+  std::vector<double> tv(9 * mp), cb(mp);
+  for (int a = 0; a < 9; ++a) std::copy(m.tinv[a].begin(), m.tinv[a].end(), tv.begin() + a * mp);
+  const std::vector<double> rho = rho3(m.w);
+  for (int e = 0; e < nel; ++e)
+    for (size_t q = 0; q < m.nt; ++q) cb[e * m.nt + q] = rho[q] * m.det[e * m.nt + q];
+  SSG_TRY(dupload(c, &c->conv_tinv, tv.data(), tv.size()));
+  SSG_TRY(dupload(c, &c->conv_bj, cb.data(), cb.size()));
+  SSG_TRY(dupload(c, &c->conv_D, m.D.data(), m.D.size()));
+  SSG_TRY(dupload(c, &c->conv_J, H.jconv.data(), H.jconv.size()));
+  const size_t scr = convection_scratch_doubles(H.n, m.n);
+  if (scr) SSG_TRY(dalloc(c, &c->conv_scratch, scr));
+  return SSG_OK;
+}
+
+// Level-0 Jacobian and its transposed inverse for the particle walk
+// (sel->geom->jac / tinv_jac, src/geometry.c).
+static ssg_status upload_particle_geom(ssg_context* c) {
+  const ssg::HostLevel& h = c->host.lev[0];
+  const size_t np0 = h.nt * (size_t)c->host.nel;
+  dfree(c->p_jac); dfree(c->p_tinv);
+  c->p_jac = c->p_tinv = nullptr;
+  std::vector<double> ja(9 * np0), ti(9 * np0);
+  for (int a = 0; a < 9; ++a) {
+    std::copy(h.jac[a].begin(), h.jac[a].end(), ja.begin() + a * np0);
+    std::copy(h.tinv[a].begin(), h.tinv[a].end(), ti.begin() + a * np0);
+  }
+  SSG_TRY(dupload(c, &c->p_jac, ja.data(), ja.size()));
+  SSG_TRY(dupload(c, &c->p_tinv, ti.data(), ti.size()));
+  const std::vector<double>& px = c->host.ppoints.empty() ? h.x : c->host.ppoints;
+  dfree(c->p_x);
+  c->p_x = nullptr;
+  SSG_TRY(dupload(c, &c->p_x, px.data(), px.size()));
+  if (!c->p_ur) {
+    SSG_TRY(dalloc(c, &c->p_ur, 9 * np0));
+    SSG_CUDA(c, cudaMemset(c->p_ur, 0, 9 * np0 * sizeof(double)));
+  }
+  return SSG_OK;
 }
 
 // Upload every level (and the optional dealiasing / particle data) from
@@ -178,33 +238,11 @@ static ssg_status upload_all(ssg_context* c) {
     }
   }
   const size_t np0 = c->lev[0].npts;
-  if (H.has_conv) {
-    const ssg::HostLevel& m = H.conv;
-    c->m = m.n;
-    const size_t mp = m.nt * nel;
-    std::vector<double> tv(9 * mp), cb(mp);
-    for (int a = 0; a < 9; ++a) std::copy(m.tinv[a].begin(), m.tinv[a].end(), tv.begin() + a * mp);
-    const std::vector<double> rho = rho3(m.w);
-    for (int e = 0; e < nel; ++e)
-      for (size_t q = 0; q < m.nt; ++q) cb[e * m.nt + q] = rho[q] * m.det[e * m.nt + q];
-    SSG_TRY(dupload(c, &c->conv_tinv, tv.data(), tv.size()));
-    SSG_TRY(dupload(c, &c->conv_bj, cb.data(), cb.size()));
-    SSG_TRY(dupload(c, &c->conv_D, m.D.data(), m.D.size()));
-    SSG_TRY(dupload(c, &c->conv_J, H.jconv.data(), H.jconv.size()));
-  }
-  if (H.has_particle_geom) {
-    const ssg::HostLevel& h = H.lev[0];
-    std::vector<double> ja(9 * np0), ti(9 * np0);
-    for (int a = 0; a < 9; ++a) {
-      std::copy(h.jac[a].begin(), h.jac[a].end(), ja.begin() + a * np0);
-      std::copy(h.tinv[a].begin(), h.tinv[a].end(), ti.begin() + a * np0);
-    }
-    SSG_TRY(dupload(c, &c->p_jac, ja.data(), ja.size()));
-    SSG_TRY(dupload(c, &c->p_tinv, ti.data(), ti.size()));
-    SSG_TRY(dalloc(c, &c->p_ur, 9 * np0));
-    SSG_CUDA(c, cudaMemset(c->p_ur, 0, 9 * np0 * sizeof(double)));
-  }
-  SSG_TRY(dupload(c, &c->p_x, H.lev[0].x.data(), H.lev[0].x.size()));
+  if (H.has_conv) SSG_TRY(upload_conv(c));
+  if (H.has_particle_geom) SSG_TRY(upload_particle_geom(c));
+  if (!c->p_x) SSG_TRY(dupload(c, &c->p_x, H.lev[0].x.data(), H.lev[0].x.size()));
+  SSG_TRY(dupload(c, &c->d_neigh, H.neigh.data(), H.neigh.size()));
+  SSG_TRY(dalloc(c, &c->d_passes, 1));
   // reduction partials: enough for 10 dot products over the largest grid
   const size_t vb = (size_t)vec_blocks(np0);
   const size_t db = (size_t)dss_grid(c->n, nel);
@@ -682,6 +720,141 @@ ssg_status ssg_multigrid_preconditioner(ssg_context* c, const double* r, double*
   SSG_TRY(ensure_workspace(c));
   SSG_TRY(mg_apply(c, dr, dz, eps));
   return stage_back(c, z, dz, np);
+}
+
+ssg_status ssg_setup_dealias(ssg_context* c, int m, const double* deriv,
+                             const double* weights, const double* tinv_jac,
+                             const double* jac_det, const double* interp) {
+  if (!c || !deriv || !weights || !tinv_jac || !jac_det || !interp) return SSG_ERR_ARG;
+  ssg::HostMesh& H = c->host;
+  if (H.nel <= 0 || H.lev[0].n == 0)
+    return fail(c, SSG_ERR_STATE, "connectivity and level 0 first");
+  if (m < 2 || m > SSG_MAXN) return fail(c, SSG_ERR_ARG, "bad dealiasing order");
+  const int n = H.lev[0].n;
+  ssg::HostLevel& L = H.conv;
+  L = ssg::HostLevel();
+  L.n = m;
+  L.nt = (size_t)m * m * m;
+  const size_t mp = L.nt * H.nel;
+  L.x.resize(m);
+  gll_basis(m, L.x.data(), std::vector<double>(m).data());
+  L.w.assign(weights, weights + m);
+  L.D.resize((size_t)m * m);
+  // stored d[j][i] = D_ij  ->  D[i*m+j]
+  for (int i = 0; i < m; ++i)
+    for (int j = 0; j < m; ++j) L.D[i * m + j] = deriv[j * m + i];
+  for (int a = 0; a < 9; ++a) L.tinv[a].assign(tinv_jac + a * mp, tinv_jac + (a + 1) * mp);
+  L.det.assign(jac_det, jac_det + mp);
+  // stored interp[p][i] (p: n-point node, i: m-point node) -> jconv[i*n+p]
+  H.jconv.resize((size_t)m * n);
+  for (int p = 0; p < n; ++p)
+    for (int i = 0; i < m; ++i) H.jconv[i * n + p] = interp[p * m + i];
+  H.has_conv = true;
+  if (!c->ready) return SSG_OK;
+  SSG_CUDA(c, cudaSetDevice(c->device));
+  return upload_conv(c);
+}
+
+ssg_status ssg_setup_particle_geometry(ssg_context* c, const double* points,
+                                       const double* jac, const double* tinv_jac) {
+  if (!c || !jac || !tinv_jac) return SSG_ERR_ARG;
+  ssg::HostMesh& H = c->host;
+  if (H.nel <= 0 || H.lev[0].n == 0)
+    return fail(c, SSG_ERR_STATE, "connectivity and level 0 first");
+  ssg::HostLevel& L = H.lev[0];
+  const size_t np = L.nt * H.nel;
+  for (int a = 0; a < 9; ++a) {
+    L.jac[a].assign(jac + a * np, jac + (a + 1) * np);
+    L.tinv[a].assign(tinv_jac + a * np, tinv_jac + (a + 1) * np);
+  }
+  if (points)
+    H.ppoints.assign(points, points + L.n);
+  else
+    H.ppoints.clear();
+  H.has_particle_geom = true;
+  if (!c->ready) return SSG_OK;
+  SSG_CUDA(c, cudaSetDevice(c->device));
+  return upload_particle_geom(c);
+}
+
+ssg_status ssg_convection_operator(ssg_context* c, const double* u, const double* v,
+                                   double* udv) {
+  SSG_TRY(need_ready(c));
+  if (!c->conv_tinv) return fail(c, SSG_ERR_STATE, "no dealiasing grid set up");
+  const size_t np = 3 * c->lev[0].npts;
+  const double *du, *dv;
+  double* dout;
+  SSG_TRY(stage_in(c, 0, u, np, &du));
+  SSG_TRY(stage_in(c, 1, v, np, &dv));
+  SSG_TRY(stage_out(c, 2, udv, np, &dout));
+  SSG_CUDA(c, run_convection(c->stream, c->nel, c->n, c->m, du, dv, dout, c->conv_tinv,
+                             c->conv_bj, c->conv_D, c->conv_J, c->conv_scratch));
+  return stage_back(c, udv, dout, np);
+}
+
+ssg_status ssg_set_particle_velocity(ssg_context* c, const double* ur) {
+  SSG_TRY(need_ready(c));
+  if (!ur) return fail(c, SSG_ERR_ARG, "null velocity");
+  if (!c->p_jac) return fail(c, SSG_ERR_STATE, "no particle geometry set up");
+  const size_t count = 9 * c->lev[0].npts;
+  SSG_CUDA(c, cudaMemcpyAsync(c->p_ur, ur, count * sizeof(double), cudaMemcpyDefault,
+                              c->stream));
+  SSG_CUDA(c, cudaStreamSynchronize(c->stream));
+  c->has_ur = true;
+  return SSG_OK;
+}
+
+ssg_status ssg_integrate_particle_equations(ssg_context* c, size_t np, double* state,
+                                            int* ints, double t, double dt, int* passes) {
+  SSG_TRY(need_ready(c));
+  if (!c->p_jac) return fail(c, SSG_ERR_STATE, "no particle geometry set up");
+  if (!c->has_ur) return fail(c, SSG_ERR_STATE, "ssg_set_particle_velocity first");
+  if (!(dt > 0.0)) return fail(c, SSG_ERR_ARG, "dt must be > 0");
+  if (np > 0 && (!state || !ints)) return fail(c, SSG_ERR_ARG, "null particle arrays");
+  const bool dev_state = np > 0 && is_device_ptr(state);
+  const bool dev_ints = np > 0 && is_device_ptr(ints);
+  double* ds = state;
+  int* di = ints;
+  if (np > 0 && (!dev_state || !dev_ints) && np > c->p_cap) {
+    dfree(c->p_state);
+    if (c->p_ints) cudaFree(c->p_ints);
+    c->p_state = nullptr;
+    c->p_ints = nullptr;
+    c->p_cap = 0;
+    SSG_TRY(dalloc(c, &c->p_state, 8 * np));
+    if (cudaMalloc(&c->p_ints, 3 * np * sizeof(int)) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(c, SSG_ERR_NOMEM, "particle staging");
+    }
+    c->p_cap = np;
+  }
+  if (np > 0 && !dev_state) {
+    ds = c->p_state;
+    SSG_CUDA(c, cudaMemcpyAsync(ds, state, 8 * np * sizeof(double), cudaMemcpyHostToDevice,
+                                c->stream));
+  }
+  if (np > 0 && !dev_ints) {
+    di = c->p_ints;
+    SSG_CUDA(c, cudaMemcpyAsync(di, ints, 3 * np * sizeof(int), cudaMemcpyHostToDevice,
+                                c->stream));
+  }
+  SSG_CUDA(c, cudaMemsetAsync(c->d_passes, 0, sizeof(int), c->stream));
+  SSG_CUDA(c, run_particles(c->stream, c->n, c->nel, c->lev[0].npts, c->p_x, c->p_ur,
+                            c->p_jac, c->p_tinv, c->d_neigh, t, dt, np, ds, di, c->d_passes));
+  if (np > 0 && !dev_state)
+    SSG_CUDA(c, cudaMemcpyAsync(state, ds, 8 * np * sizeof(double), cudaMemcpyDeviceToHost,
+                                c->stream));
+  if (np > 0 && !dev_ints)
+    SSG_CUDA(c, cudaMemcpyAsync(ints, di, 3 * np * sizeof(int), cudaMemcpyDeviceToHost,
+                                c->stream));
+  int hp = 0;
+  SSG_CUDA(c, cudaMemcpyAsync(c->h_pin, c->d_passes, sizeof(int), cudaMemcpyDeviceToHost,
+                              c->stream));
+  SSG_CUDA(c, cudaStreamSynchronize(c->stream));
+  std::memcpy(&hp, c->h_pin, sizeof(int));
+  // the reference's pass loop runs at least once, also without particles
+  if (passes) *passes = hp > 1 ? hp : 1;
+  return SSG_OK;
 }
 
 }  // extern "C"

@@ -1,0 +1,194 @@
+// Dealiased skew-symmetric convection (convection_operator ->
+// antialiased_convection_operator, src/convection.c:31-140), one element per
+// block, all in FP64:
+//   1. interpolate the advecting u and advected v (3 components each) from
+//      the n-point to the m = 3n/2-point GLL grid (interpolate_to_grid,
+//      src/interpolation.c:136-155);
+//   2. per dealiasing point, convective form (u . grad) v_c with grad from the
+//      conv-grid tinv (src/convection.c:71-93) and conservative form
+//      sum_a sum_b tinv[a][b] d_b(u_b v_c) (src/convection.c:95-127), both
+//      weighted by rho J, averaged with weights 1/2 (src/convection.c:129-140);
+//   3. project back with (J^T)^3 (integrate_to_grid, src/interpolation.c:
+//      157-176).
+// The derivatives of the products u_b v_c are taken on the fly from the
+// interpolated fields, so only the six interpolated fields and the three
+// averaged components are stored per element: in shared memory while they
+// fit (m <= 13, n <= 9), else in a global scratch region of 9 m^3 doubles
+// per block.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "kernels.cuh"
+#include "ssg_internal.h"
+#include "ssg_kernels.h"
+
+namespace ssg {
+namespace dev {
+
+// out (no^3) = (A x A x A) in (ni^3), stages x, y, z; A[o*ni + q]
+// (transpose = true: A[q*no + o], the weak projection).  Block-cooperative.
+__device__ void block_tensor3(int ni, int no, const double* A, bool transpose,
+                              const double* in, double* t1, double* t2, double* out,
+                              double* gout) {
+  auto a = [&](int o, int q) { return transpose ? A[q * no + o] : A[o * ni + q]; };
+  for (int q = threadIdx.x; q < ni * ni * no; q += blockDim.x) {
+    const int o = q % no, kj = q / no;
+    double s = 0;
+    for (int r = 0; r < ni; ++r) s += a(o, r) * in[kj * ni + r];
+    t1[q] = s;
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < ni * no * no; q += blockDim.x) {
+    const int o1 = q % no, o2 = (q / no) % no, k = q / (no * no);
+    double s = 0;
+    for (int r = 0; r < ni; ++r) s += a(o2, r) * t1[(k * ni + r) * no + o1];
+    t2[q] = s;
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < no * no * no; q += blockDim.x) {
+    const int o12 = q % (no * no), o3 = q / (no * no);
+    double s = 0;
+    for (int r = 0; r < ni; ++r) s += a(o3, r) * t2[r * no * no + o12];
+    if (gout)
+      gout[q] = s;
+    else
+      out[q] = s;
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(512) k_convection(int nel, int n, int m,
+                                                   const double* __restrict__ u,
+                                                   const double* __restrict__ v,
+                                                   double* __restrict__ udv,
+                                                   const double* __restrict__ tinv,
+                                                   const double* __restrict__ bj,
+                                                   const double* __restrict__ Dm,
+                                                   const double* __restrict__ J,
+                                                   double* __restrict__ gscr) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int nt = n * n * n, mt = m * m * m;
+  const int tmax = n * m * m > n * n * m ? n * m * m : n * n * m;
+  double* sD = reinterpret_cast<double*>(smem_raw);
+  double* sJ = sD + m * m;                    // J[i*n + p] = l_p^n(x_i^m)
+  double* t1 = sJ + m * n;
+  double* t2 = t1 + tmax;
+  double* stage = t2 + tmax;                  // nt
+  double* ui = gscr ? gscr + (size_t)blockIdx.x * 9 * mt : stage + nt;   // 3 x mt
+  double* vi = ui + 3 * mt;                   // 3 x mt
+  double* sk = vi + 3 * mt;                   // 3 x mt
+  const size_t nptsn = (size_t)nel * nt, nptsm = (size_t)nel * mt;
+  for (int q = threadIdx.x; q < m * m; q += blockDim.x) sD[q] = Dm[q];
+  for (int q = threadIdx.x; q < m * n; q += blockDim.x) sJ[q] = J[q];
+  for (size_t e = blockIdx.x; e < (size_t)nel; e += gridDim.x) {
+    // 1. interpolate the six components to the dealiasing grid
+    for (int f = 0; f < 6; ++f) {
+      const double* src = (f < 3 ? u : v) + (size_t)(f % 3) * nptsn + e * nt;
+      __syncthreads();
+      for (int q = threadIdx.x; q < nt; q += blockDim.x) stage[q] = src[q];
+      __syncthreads();
+      block_tensor3(n, m, sJ, false, stage, t1, t2, (f < 3 ? ui : vi) + (f % 3) * mt, nullptr);
+    }
+    // 2. convective and conservative forms at every dealiasing point
+    for (int q = threadIdx.x; q < mt; q += blockDim.x) {
+      const int i = q % m, j = (q / m) % m, k = q / (m * m);
+      const size_t g = e * mt + q;
+      double t[3][3];
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b) t[a][b] = tinv[(size_t)(3 * a + b) * nptsm + g];
+      const double w = bj[g];
+      const double* Di = sD + i * m;
+      const double* Dj = sD + j * m;
+      const double* Dk = sD + k * m;
+      const int rbase = (k * m + j) * m, sbase = k * m * m + i, tbase = j * m + i;
+      for (int c = 0; c < 3; ++c) {
+        const double* vc = vi + c * mt;
+        // convective: d v_c / d r_b, then grad through tinv, dotted with u
+        double dr = 0, ds = 0, dt = 0;
+        for (int l = 0; l < m; ++l) {
+          dr += Di[l] * vc[rbase + l];
+          ds += Dj[l] * vc[sbase + l * m];
+          dt += Dk[l] * vc[tbase + l * m * m];
+        }
+        double d[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          double s = t[a][0] * dr;
+          s = t[a][1] * ds + s;
+          s = t[a][2] * dt + s;
+          d[a] = s;
+        }
+        double cv = ui[q] * d[0];
+        cv = ui[mt + q] * d[1] + cv;
+        cv = ui[2 * mt + q] * d[2] + cv;
+        cv = cv * w;
+        // conservative: d_r(u_x v_c), d_s(u_y v_c), d_t(u_z v_c) through tinv
+        double er = 0, es = 0, et = 0;
+        for (int l = 0; l < m; ++l) {
+          er += Di[l] * (ui[rbase + l] * vc[rbase + l]);
+          es += Dj[l] * (ui[mt + sbase + l * m] * vc[sbase + l * m]);
+          et += Dk[l] * (ui[2 * mt + tbase + l * m * m] * vc[tbase + l * m * m]);
+        }
+        double cs = 0;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          double s = t[a][0] * er;
+          s = t[a][1] * es + s;
+          s = t[a][2] * et + s;
+          cs += s;
+        }
+        cs = cs * w;
+        sk[c * mt + q] = 0.5 * cv + 0.5 * cs;
+      }
+    }
+    __syncthreads();
+    // 3. weak projection back to the n-point grid
+    for (int c = 0; c < 3; ++c)
+      block_tensor3(m, n, sJ, true, sk + c * mt, t1, t2, nullptr, udv + (size_t)c * nptsn + e * nt);
+    __syncthreads();
+  }
+}
+
+}  // namespace dev
+
+static size_t convection_smem(int n, int m, bool fields) {
+  const size_t nt = (size_t)n * n * n, mt = (size_t)m * m * m;
+  const size_t tmax = std::max((size_t)n * m * m, (size_t)n * n * m);
+  return (m * m + m * n + 2 * tmax + nt + (fields ? 9 * mt : 0)) * sizeof(double);
+}
+
+static constexpr size_t kConvSmemMax = 220 * 1024;
+
+size_t convection_scratch_doubles(int n, int m) {
+  if (convection_smem(n, m, true) <= kConvSmemMax) return 0;
+  return (size_t)kConvScratchBlocks * 9 * m * m * m;
+}
+
+cudaError_t run_convection(cudaStream_t s, int nel, int n, int m, const double* u,
+                           const double* v, double* udv, const double* tinv,
+                           const double* bj, const double* Dm, const double* J,
+                           double* scratch) {
+  const bool in_smem = convection_smem(n, m, true) <= kConvSmemMax;
+  if (!in_smem && !scratch) return cudaErrorInvalidValue;
+  const size_t smem = convection_smem(n, m, in_smem);
+  if (smem > kConvSmemMax) return cudaErrorInvalidValue;
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(
+        dev::k_convection, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kConvSmemMax);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  if (nel <= 0) return cudaSuccess;
+  const int grid = in_smem ? nel : std::min(nel, kConvScratchBlocks);
+  ++g_launches;
+  dev::k_convection<<<grid, 512, smem, s>>>(nel, n, m, u, v, udv, tinv, bj, Dm, J,
+                                           in_smem ? nullptr : scratch);
+  return cudaGetLastError();
+}
+
+}  // namespace ssg

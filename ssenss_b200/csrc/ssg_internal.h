@@ -40,6 +40,7 @@ struct HostMesh {
   std::vector<double> jconv;            // jconv[i*n+p] = l_p^n(x_i^m)
   bool has_conv = false;
   bool has_particle_geom = false;
+  std::vector<double> ppoints;          // GLL points of the particle walk (empty: lev[0].x)
 };
 
 int level_orders(int n, int* orders);
@@ -105,11 +106,18 @@ struct ssg_context {
   double* conv_bj = nullptr;    // rho * J at m
   double* conv_D = nullptr;     // m*m
   double* conv_J = nullptr;     // m*n, jconv[i*n+p]
+  double* conv_scratch = nullptr;  // interpolated fields when m^3 exceeds shared memory
   // particles
   double* p_jac = nullptr;      // 9 x npts (level 0)
   double* p_tinv = nullptr;     // 9 x npts
   double* p_ur = nullptr;       // 3 x 3 x npts
   double* p_x = nullptr;        // GLL points of level 0
+  int* d_neigh = nullptr;       // nel x 26 face/edge/corner neighbours
+  int* d_passes = nullptr;      // particle pass count
+  bool has_ur = false;          // particle velocity snapshots set
+  double* p_state = nullptr;    // staging of host particle arrays
+  int* p_ints = nullptr;
+  size_t p_cap = 0;
   // reductions / scalars
   double* d_part = nullptr;     // block partial sums
   size_t part_cap = 0;

@@ -111,5 +111,20 @@ cudaError_t run_coarse_cg(cudaStream_t s, int device, int nel, const double* f, 
                           const double* gf, const double* D, const double* dinv,
                           const uint8_t* mult, const int* pairs, double nunique, double eps,
                           int max_iter, double* part, size_t part_cap, double* frame);
+// dealiased skew-symmetric convection of 3-component fields (convection.cu);
+// for m^3 fields beyond shared memory, scratch holds
+// convection_scratch_doubles(n, m) doubles (0: none needed)
+constexpr int kConvScratchBlocks = 296;
+size_t convection_scratch_doubles(int n, int m);
+cudaError_t run_convection(cudaStream_t s, int nel, int n, int m, const double* u,
+                           const double* v, double* udv, const double* tinv,
+                           const double* bj, const double* Dm, const double* J,
+                           double* scratch);
+// Lagrangian particle advance to time t (particles.cu); passes: device int
+// that receives the largest per-particle pass count (atomicMax, caller zeroes)
+cudaError_t run_particles(cudaStream_t s, int n, int nel, size_t npts, const double* x,
+                          const double* ur, const double* jac, const double* tinv,
+                          const int* neigh, double t, double dt, size_t np, double* state,
+                          int* ints, int* passes);
 
 }  // namespace ssg

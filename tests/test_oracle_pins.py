@@ -1,0 +1,163 @@
+"""Pins of the CPU oracle (oracle/ssg_oracle.c) to the reference.
+
+1. Golden fixtures (tests/golden/*.npz, written by tests/golden/make_golden.py
+   from the reference compiled in place): the oracle reproduces them --
+   DSS bitwise, operators and the inner product to 1e-13, the solves'
+   iteration counts exactly and solutions to 1e-11, one multigrid
+   application to 1e-9, convection to 1e-13, and the particle walk bitwise.
+2. Live comparison with the compiled reference (oracle/_ref), where it has
+   been built: random inputs on more meshes and orders.
+
+The oracle is the checker of the GPU path, so these tests run on CPU.
+"""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+import oracle as O
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "golden"))
+import golden_inputs as G  # noqa: E402
+
+
+def rel(a, b):
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def load(name):
+    return dict(np.load(os.path.join(HERE, "golden", f"{name}.npz")))
+
+
+_orc = {}
+
+
+def oracle_for(name):
+    if name not in _orc:
+        mk, n = G.CASES[name]
+        mesh = mk()
+        orc = O.Oracle(mesh, n, dt=G.DT, visc=G.VISC, dens=G.DENS)
+        orc.set_params(0.0, G.DT, G.VISC)
+        _orc[name] = (mesh, n, orc)
+    return _orc[name]
+
+
+@pytest.mark.parametrize("name", list(G.CASES))
+def test_golden_operators(name):
+    mesh, n, orc = oracle_for(name)
+    g = load(name)
+    assert list(g["orders"]) == orc.orders
+    shp = (mesh.nel, n, n, n)
+    u, v = G.hash_field(shp, 1), G.hash_field(shp, 2)
+    assert np.array_equal(orc.dss(u), g["dss"])
+    assert rel(orc.global_opeval(O.PRESSURE, u), g["op_p"]) < 1e-13
+    assert rel(orc.global_opeval(O.X_VELOCITY, u), g["op_h"]) < 1e-13
+    assert abs(orc.dot(u, v) - float(g["dot"])) <= 1e-13 * orc.dot(u, u)
+    u3, v3 = G.hash_field((3,) + shp, 4), G.hash_field((3,) + shp, 5)
+    assert rel(orc.convection(u3, v3), g["conv"]) < 1e-13
+
+
+@pytest.mark.parametrize("name", list(G.CASES))
+def test_golden_solves(name):
+    mesh, n, orc = oracle_for(name)
+    g = load(name)
+    f = g["f"]
+    sol, hist = orc.solve_poisson(f, np.zeros_like(f))
+    assert len(hist) == int(g["it_p"])
+    assert rel(sol, g["sol_p"]) < 1e-11
+    assert np.all(np.abs(hist - g["hist_p"]) <= 1e-7 * g["hist_p"][0])
+    sol, hist = orc.solve_helmholtz(O.X_VELOCITY, f, np.zeros_like(f))
+    assert len(hist) == int(g["it_h"])
+    assert rel(sol, g["sol_h"]) < 1e-12
+    assert rel(orc.mg_precon(f), g["mg"]) < 1e-9
+
+
+def test_golden_particles_bitwise():
+    name = G.PARTICLE_CASE
+    mesh, n, orc = oracle_for(name)
+    g = load(name)
+    jac, tinv = G.particle_factors(mesh, n)
+    orc.set_particle_basis(g["points"], jac, tinv)
+    orc.set_params(G.PART_T, G.PART_DT, G.VISC)
+    ur = G.particle_velocity(mesh, g["points"], G.PART_T, G.PART_DT)
+    state, ints = G.particle_states(mesh, g["p_state"].shape[0], 7)
+    s, i, _ = orc.particles_advance(state, ints, ur)
+    done = g["p_ints"][:, 2] == 0          # the reference reseeds the others at random
+    assert np.sum(i[:, 0] != ints[:, 0]) > 100
+    assert np.array_equal(i[:, 2] == 0, done)
+    assert np.array_equal(i[done], g["p_ints"][done])
+    assert np.array_equal(s[done].view(np.uint64), g["p_state"][done].view(np.uint64))
+
+
+# --------------------------------------------------------------------------
+# live reference (where oracle/_ref was built from the reference sources)
+# --------------------------------------------------------------------------
+needs_ref = pytest.mark.skipif(not O.reference_available(),
+                               reason="reference library not built")
+
+LIVE = {
+    "tgv3_n8": (lambda: G.tgv_box(3), 8),
+    "channel433_n7": (lambda: G.channel_mesh((4, 3, 3), seed=7), 7),
+    "tgv3_n5": (lambda: G.tgv_box(3), 5),
+}
+
+
+def live_pair(name):
+    mk, n = LIVE[name]
+    mesh = mk()
+    return mesh, n, O.Oracle(mesh, n), O.Reference(mesh, n)
+
+
+@needs_ref
+@pytest.mark.parametrize("name", list(LIVE))
+def test_live_dss_operator_convection(name):
+    mesh, n, orc, ref = live_pair(name)
+    rng = np.random.default_rng(21)
+    u = rng.standard_normal((mesh.nel, n, n, n))
+    assert np.array_equal(orc.dss(u), ref.dss(u))
+    assert rel(orc.global_opeval(O.PRESSURE, u), ref.global_opeval(O.PRESSURE, u)) < 1e-13
+    u3 = rng.standard_normal((3, mesh.nel, n, n, n))
+    v3 = rng.standard_normal((3, mesh.nel, n, n, n))
+    assert rel(orc.convection(u3, v3), ref.convection(u3, v3)) < 1e-13
+
+
+@needs_ref
+@pytest.mark.parametrize("name", list(LIVE))
+def test_live_particles(name):
+    """Bitwise for n > 5 on the reference's own GLL points and factors.
+    For n <= 5 the reference interpolates with BLAS dgemv/ddot, whose
+    summation order belongs to the BLAS build: element ids and statuses
+    still agree, values to rounding."""
+    mesh, n, orc, ref = live_pair(name)
+    orc.set_particle_basis(*ref.particle_geometry())
+    t, dt = 0.1, 0.05
+    orc.set_params(t, dt, 1.0 / 1600.0)
+    ref.set_params(t, dt, 1.0 / 1600.0)
+    X = [orc.geometry(0, 7 + c) for c in range(3)]
+    ur = np.empty((3, 3, mesh.nel, n, n, n))
+    for lev in range(3):
+        tt = t - (2 - lev) * dt
+        ur[lev, 0] = 3.0 * np.sin(X[0] + tt) * np.cos(X[1])
+        ur[lev, 1] = -3.0 * np.cos(X[0]) * np.sin(X[1] + 2 * tt)
+        ur[lev, 2] = 2.0 * np.cos(X[2] + tt)
+    rng = np.random.default_rng(3)
+    npart = 400
+    state = np.zeros((npart, 8))
+    ints = np.zeros((npart, 3), np.int32)
+    state[:, :3] = rng.uniform(-0.99, 0.99, (npart, 3))
+    state[:, 3:6] = rng.standard_normal((npart, 3)) * 20.0
+    state[:, 6] = t - dt
+    state[:, 7] = rng.uniform(0.05, 2.0, npart)
+    ints[:, 0] = rng.integers(0, mesh.nel, npart)
+    ints[:, 1] = ints[:, 0]
+    s1, i1, _ = orc.particles_advance(state, ints, ur)
+    s2, i2 = ref.particles_advance(state, ints, ur)
+    done = i1[:, 2] == 0
+    assert np.sum(i1[:, 0] != ints[:, 0]) > 100
+    assert np.array_equal(i1[done], i2[done])
+    if n > 5:
+        assert np.array_equal(s1[done].view(np.uint64), s2[done].view(np.uint64))
+    else:
+        assert rel(s1[done], s2[done]) < 1e-12
