@@ -57,6 +57,10 @@ def parse():
     ap.add_argument("--ne", type=int, default=NE)
     ap.add_argument("--n", type=int, default=NORD)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="keep the default launch shapes (skip ssg_autotune)")
+    ap.add_argument("--no-graphs", action="store_true",
+                    help="launch the V-cycle kernels directly (no CUDA graph)")
     ap.add_argument("--sections", default="all", choices=["all", "fp64", "op"],
                     help="fp64: only the FP64 solves; op: only the operator "
                          "launches (for profiler captures)")
@@ -263,6 +267,8 @@ def run_ours(args):
     ctx = S.Context(local)
     ctx.set_parameters(1e-3, 1.0 / 1600.0, 1.0)
     ctx.setup_mesh(mesh, n)
+    ctx.set_graphs(not args.no_graphs)
+    tuned = None if args.no_tune else ctx.autotune()
     npts = mesh.nel * n ** 3
     udofs = mesh.unique_nodes(n)
     X, Y, Z = (ctx.level_data(0, 12 + a) for a in range(3))
@@ -418,6 +424,9 @@ def run_ours(args):
             "elements": mesh.nel, "n": n, "mg_orders": ctx.orders,
             "unique_dofs": udofs, "local_points": npts,
             "parallelism": f"replicas x{world}",
+            "launch_shapes": ({str(k): v for k, v in tuned.items()} if tuned
+                              else "default (autotuner off)"),
+            "cuda_graphs": "V-cycle captured" if not args.no_graphs else "off",
             "l2": "inputs larger than L2 (level-0 factors 100 MB + FCG vectors 420 MB)",
         },
         "iterations_per_solve": it64 / args.steps,

@@ -233,6 +233,19 @@ ssg_status ssg_multigrid_preconditioner(ssg_context *ctx, const double *r,
 ssg_status ssg_convection_operator(ssg_context *ctx, const double *u,
 		const double *v, double *udv);
 
+/* ---- launch-shape autotuner (no reference counterpart) ---------------------- */
+
+/* Time every candidate launch shape of the operator (elements per block),
+ * the DSS (blocks per SM) and the vector kernels (blocks per SM) on this
+ * context's mesh and levels, reps launches per trial (<= 0: 10), and keep
+ * the fastest for every later launch in the process (keyed by order n).
+ * Results are unchanged: every shape computes the same sums in the same
+ * order. */
+ssg_status ssg_autotune(ssg_context *ctx, int reps);
+/* Launch shapes in use for order n (tuned or default). */
+ssg_status ssg_tuning(int n, int *ax_elements_per_block,
+		int *dss_blocks_per_sm, int *vector_blocks_per_sm);
+
 /* ---- instrumentation -------------------------------------------------------- */
 
 /* Number of this library's kernel launches in the process so far (all

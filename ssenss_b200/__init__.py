@@ -52,6 +52,22 @@ def _ptr(a):
     raise TypeError(f"unsupported field type {type(a)}")
 
 
+def tuning(n: int) -> dict:
+    """Launch shapes in use for order n (ssg_tuning)."""
+    lib = _lib.load()
+    a, d, v = C.c_int(), C.c_int(), C.c_int()
+    st = lib.ssg_tuning(int(n), C.byref(a), C.byref(d), C.byref(v))
+    if st != 0:
+        raise SsgError(st, "tuning")
+    return {"ax_elements_per_block": a.value, "dss_blocks_per_sm": d.value,
+            "vector_blocks_per_sm": v.value}
+
+
+def kernel_launch_count() -> int:
+    """Kernel launches of the library in this process so far."""
+    return int(_lib.load().ssg_kernel_launch_count())
+
+
 class Context:
     """One GPU context (ssg_context): mesh, factors, workspace, stream."""
 
@@ -98,6 +114,12 @@ class Context:
 
     def set_graphs(self, enable: bool):
         self._check(self.lib.ssg_set_graphs(self.h, int(bool(enable))), "set_graphs")
+
+    def autotune(self, reps: int = 10):
+        """ssg_autotune: time the launch-shape candidates on this mesh and
+        keep the fastest (process-wide, per order); returns the shapes."""
+        self._check(self.lib.ssg_autotune(self.h, int(reps)), "autotune")
+        return {n: tuning(n) for n in sorted(set(self.orders))}
 
     def setup_mesh(self, mesh, n: int):
         vert = np.ascontiguousarray(mesh.vertices, dtype=np.float64)

@@ -65,6 +65,8 @@ SIGNATURES = [
     ("ssg_convection_operator", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p,
                                           C.c_void_p]),
     ("ssg_kernel_launch_count", C.c_ulonglong, []),
+    ("ssg_autotune", C.c_int, [C.c_void_p, C.c_int]),
+    ("ssg_tuning", C.c_int, [C.c_int, _ip, _ip, _ip]),
     ("ssg_set_particle_velocity", C.c_int, [C.c_void_p, C.c_void_p]),
     ("ssg_integrate_particle_equations", C.c_int, [C.c_void_p, C.c_size_t, C.c_void_p,
                                                    C.c_void_p, C.c_double, C.c_double,

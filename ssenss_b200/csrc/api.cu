@@ -61,7 +61,7 @@ static void dfree(void* p) {
 static void free_level(ssg::DevLevel& d) {
   dfree(d.gf); dfree(d.bj); dfree(d.kdiag); dfree(d.dinv_p); dfree(d.dinv_h);
   dfree(d.mult); dfree(d.mask); dfree(d.D); dfree(d.S); dfree(d.Ar); dfree(d.Ap);
-  dfree(d.gf32); dfree(d.dinv_p32);
+  dfree(d.gf32); dfree(d.dinv_p32); dfree(d.dss_ec);
   d = ssg::DevLevel();
 }
 
@@ -165,6 +165,8 @@ static ssg_status upload_all(ssg_context* c) {
   c->has_walls = false;
   for (int e = 0; e < nel; ++e)
     if (H.bc[e]) c->has_walls = true;
+  if ((size_t)nel * H.lev[0].nt >= (size_t)INT32_MAX)
+    return fail(c, SSG_ERR_ARG, "mesh exceeds 2^31 local points (32-bit node indices)");
   SSG_TRY(dupload(c, &c->d_pairs, H.pairs.data(), H.pairs.size()));
   for (int l = 0; l < H.nlev; ++l) {
     const ssg::HostLevel& h = H.lev[l];
@@ -218,6 +220,11 @@ static ssg_status upload_all(ssg_context* c) {
                 }
       SSG_TRY(dupload(c, &d.mask, mk.data(), np));
     }
+    {
+      std::vector<int> ec;
+      dss_ec_table(H, h.n, ec);
+      SSG_TRY(dupload(c, &d.dss_ec, ec.data(), ec.size()));
+    }
     SSG_TRY(dupload(c, &d.D, h.D.data(), h.D.size()));
     SSG_TRY(dupload(c, &d.S, h.S.data(), h.S.size()));
     SSG_TRY(upload_f32(c, &d.gf32, gf.data(), gf.size()));
@@ -244,8 +251,10 @@ static ssg_status upload_all(ssg_context* c) {
   SSG_TRY(dupload(c, &c->d_neigh, H.neigh.data(), H.neigh.size()));
   SSG_TRY(dalloc(c, &c->d_passes, 1));
   // reduction partials: enough for 10 dot products over the largest grid
-  const size_t vb = (size_t)vec_blocks(np0);
-  const size_t db = (size_t)dss_grid(c->n, nel);
+  // sized for the largest grids the autotuner may pick: 32 blocks per SM
+  // for the vector kernels (up to 16 partial sums each), 16 for the DSS
+  const size_t vb = std::min((np0 + 255) / 256, (size_t)148 * 32);
+  const size_t db = (size_t)148 * 16;
   c->part_cap = std::max(16 * vb, 2 * db) + 64;
   SSG_TRY(dalloc(c, &c->d_part, c->part_cap));
   // staging for host arguments: up to three vector fields
@@ -592,6 +601,7 @@ ssg_status ssg_direct_stiffness_summation(ssg_context* c, double* u) {
   double* dout = (double*)du;
   if (!is_device_ptr(u)) dout = c->d_stage[0];
   SSG_CUDA(c, run_dss(c->stream, DSS_PLAIN, false, c->n, c->nel, tmp, dout, c->d_pairs,
+                      c->lev[0].dss_ec,
                       nullptr, nullptr, nullptr, nullptr));
   return stage_back(c, u, dout, np);
 }

@@ -136,7 +136,7 @@ __global__ void __launch_bounds__(256) k_coarse_cg(CoarseArgs a) {
                                                (int)(q & 7), cnt);
       const double rq = a.f[q] + -acc;
       a.r[q] = rq;
-      v[0] += rq * (1.0 / (1.0 + (double)cnt));
+      v[0] += rq * inv_count(1u + (unsigned)cnt);
     }
     block_partials<1>(v, a.partA, sred);
   }
@@ -152,7 +152,7 @@ __global__ void __launch_bounds__(256) k_coarse_cg(CoarseArgs a) {
       a.r[q] = rq;
       const double zq = rq * a.dinv[q];
       a.z[q] = zq;
-      v[0] += zq * (1.0 / (double)a.mult[q]);
+      v[0] += zq * inv_count(a.mult[q]);
     }
     block_partials<1>(v, a.partB, sred);
   }
@@ -190,7 +190,7 @@ __global__ void __launch_bounds__(256) k_coarse_cg(CoarseArgs a) {
         const double acc = dss_gather<2, double>(a.aploc, nullptr, a.pairs + (q >> 3) * 26, q,
                                                  (int)(q & 7), cnt);
         a.ap[q] = acc;
-        const double w = 1.0 / (1.0 + (double)cnt);
+        const double w = inv_count(1u + (unsigned)cnt);
         const double pw = a.p[q] * w;
         v[0] += pw * acc;
         if (first) {
@@ -218,7 +218,7 @@ __global__ void __launch_bounds__(256) k_coarse_cg(CoarseArgs a) {
         a.r[q] = rq;
         const double zq = rq * a.dinv[q];
         a.z[q] = zq;
-        const double w = 1.0 / (double)a.mult[q];
+        const double w = inv_count(a.mult[q]);
         const double rw = rq * w;
         v[0] += rw * zq;
         v[1] += rw * rq;

@@ -317,6 +317,7 @@ template <int N, typename T, int MODE>
 __global__ void __launch_bounds__(256) k_dss(int nel, int epb, const T* __restrict__ in,
                                              T* __restrict__ out,
                                              const int2* __restrict__ pairs,
+                                             const int4* __restrict__ ec,
                                              const double* __restrict__ mask,
                                              const T* __restrict__ y,
                                              const T* __restrict__ y2,
@@ -359,9 +360,34 @@ __global__ void __launch_bounds__(256) k_dss(int nel, int epb, const T* __restri
           cnt = 1;
         }
       } else if (t < F + EC) {
-        // edges and corners: the general ordered gather
+        // edges and corners: the ordered source lists of the set-up table
+        // (3 sources per edge node, 7 per corner node, -1 = none)
         loc = class_ordered_node<N>(t);
-        acc = dss_gather<N, T>(in, mask, sp + z * 26, eb + loc, loc, cnt);
+        const int c = t - F;
+        constexpr int ECI = 12 * I;
+        const int4* rec = ec + (size_t)(e0 + z) * (ECI + 16) +
+                          (c < ECI ? c : ECI + 2 * (c - ECI));
+        const int4 a = __ldg(rec);
+        int4 b = make_int4(-1, -1, -1, -1);
+        if (c >= ECI) b = __ldg(rec + 1);
+        acc = (double)in[eb + loc];
+        if (mask) acc = acc * mask[eb + loc];
+        const int src[7] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z};
+        double v[7];
+#pragma unroll
+        for (int m = 0; m < 7; ++m) {
+          v[m] = 0.0;
+          if (src[m] >= 0) {
+            v[m] = (double)in[src[m]];
+            if (mask) v[m] = v[m] * mask[src[m]];
+          }
+        }
+#pragma unroll
+        for (int m = 0; m < 7; ++m)
+          if (src[m] >= 0) {
+            acc += v[m];
+            ++cnt;
+          }
       } else {
         // element interior: no neighbour shares the node
         const int u = t - F - EC;
@@ -370,7 +396,7 @@ __global__ void __launch_bounds__(256) k_dss(int nel, int epb, const T* __restri
         if (mask) acc = acc * mask[eb + loc];
       }
       const size_t gi = eb + loc;
-      const double w = 1.0 / (1.0 + (double)cnt);
+      const double w = inv_count(1u + (unsigned)cnt);
       if (MODE == DSS_RESID) {
         const T rv = (T)((double)y[gi] + -acc);
         out[gi] = rv;
@@ -476,7 +502,7 @@ __global__ void __launch_bounds__(256) k_cg_update(size_t npts,
     r[q] = rq;
     const T zq = (T)((double)rq * (double)dinv[q]);
     z[q] = zq;
-    const double w = 1.0 / (double)mult[q];
+    const double w = inv_count(mult[q]);
     const double rw = (double)rq * w;
     v[0] += rw * (double)zq;
     v[1] += rw * (double)rq;
@@ -499,7 +525,7 @@ __global__ void __launch_bounds__(256) k_jacobi(size_t npts, const T* __restrict
   SSG_GRID_LOOP(q, npts) {
     const T zq = (T)((double)r[q] * (double)dinv[q]);
     z[q] = zq;
-    v[0] += (double)zq * (1.0 / (double)mult[q]);
+    v[0] += (double)zq * inv_count(mult[q]);
   }
   block_reduce<1>(v, sred);
   finish<1>(v, part, op, sred);
@@ -515,7 +541,7 @@ __global__ void __launch_bounds__(256) k_dots(size_t npts, const T* __restrict__
 #pragma unroll
   for (int k = 0; k < K; ++k) v[k] = 0.0;
   SSG_GRID_LOOP(q, npts) {
-    const double xw = (double)x[q] * (1.0 / (double)mult[q]);
+    const double xw = (double)x[q] * inv_count(mult[q]);
 #pragma unroll
     for (int k = 0; k < K; ++k) v[k] += xw * (double)((const T*)ys.p[k])[q];
   }
@@ -530,7 +556,7 @@ __global__ void __launch_bounds__(256) k_wsum(size_t npts, const T* __restrict__
                                               double* __restrict__ part, ScalarOp op) {
   __shared__ double sred[32];
   double v[1] = {0.0};
-  SSG_GRID_LOOP(q, npts) v[0] += (double)x[q] * (1.0 / (double)mult[q]);
+  SSG_GRID_LOOP(q, npts) v[0] += (double)x[q] * inv_count(mult[q]);
   block_reduce<1>(v, sred);
   finish<1>(v, part, op, sred);
 }
@@ -561,7 +587,7 @@ __global__ void __launch_bounds__(256) k_fcg_update(size_t npts, const double* _
     u[q] = u[q] + alpha * p[q];
     const double rq = r[q] + -alpha * ap[q];
     r[q] = rq;
-    v[0] += (rq * (1.0 / (double)mult[q])) * rq;
+    v[0] += (rq * inv_count(mult[q])) * rq;
   }
   block_reduce<1>(v, sred);
   finish<1>(v, part, op, sred);
@@ -613,18 +639,29 @@ static ScalarOp op_or_none(const ScalarOp* op) { return op ? *op : ScalarOp(); }
 unsigned long long g_launches = 0;   // every launch of this library bumps it
 #define SSG_COUNT() (++g_launches)
 
-int vec_blocks(size_t npts) {
-  size_t b = (npts + 255) / 256;
-  const size_t cap = 148 * 8;
-  return (int)(b < cap ? (b ? b : 1) : cap);
-}
+// Launch shapes chosen by the autotuner (tune.cu); 0 = the default rule.
+// Process-wide: they depend on the order and the device, not on the mesh.
+int g_tune_ax_epb[SSG_MAXN + 1] = {0};
+int g_tune_dss_bps[SSG_MAXN + 1] = {0};
+int g_tune_vec_bps = 0;
 
-int ax_epb(int n) {
+int ax_epb_max(int n) {
   // elements per block: up to 256 threads, <= 96 KB of FP64 shared memory
   const int q = n + (n & 1);
   int epb = 1;
   while (epb * 2 * n * n <= 256 && (size_t)(epb * 2) * 3 * n * n * q * 8 <= 96 * 1024) epb *= 2;
   return epb;
+}
+
+int vec_blocks(size_t npts) {
+  size_t b = (npts + 255) / 256;
+  const size_t cap = (size_t)148 * (g_tune_vec_bps > 0 ? g_tune_vec_bps : 8);
+  return (int)(b < cap ? (b ? b : 1) : cap);
+}
+
+int ax_epb(int n) {
+  if (n >= 0 && n <= SSG_MAXN && g_tune_ax_epb[n] > 0) return g_tune_ax_epb[n];
+  return ax_epb_max(n);
 }
 
 template <int N, typename T, bool HELM, bool FUSEP>
@@ -708,30 +745,32 @@ int dss_epb(int n) {
 int dss_grid(int n, int nel) {
   const int epb = dss_epb(n);
   const int g = (nel + epb - 1) / epb;
-  return g < 148 * 4 ? g : 148 * 4;
+  const int bps = (n >= 0 && n <= SSG_MAXN && g_tune_dss_bps[n] > 0) ? g_tune_dss_bps[n] : 4;
+  return g < 148 * bps ? g : 148 * bps;
 }
 
 template <int N, typename T>
 static cudaError_t run_dss_n(cudaStream_t s, int mode, int nel, const T* in, T* out,
-                             const int2* pr, const double* mask, const T* y, const T* y2,
-                             double* part, const double* stop, const ScalarOp& op) {
+                             const int2* pr, const int4* ec, const double* mask, const T* y,
+                             const T* y2, double* part, const double* stop,
+                             const ScalarOp& op) {
   const int epb = dss_epb(N);
   const int grd = dss_grid(N, nel);
   switch (mode) {
     case DSS_PLAIN:
-      { SSG_COUNT(); k_dss<N, T, DSS_PLAIN><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, mask, y, y2, part, stop, op); }
+      { SSG_COUNT(); k_dss<N, T, DSS_PLAIN><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, ec, mask, y, y2, part, stop, op); }
       break;
     case DSS_DOT:
-      { SSG_COUNT(); k_dss<N, T, DSS_DOT><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, mask, y, y2, part, stop, op); }
+      { SSG_COUNT(); k_dss<N, T, DSS_DOT><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, ec, mask, y, y2, part, stop, op); }
       break;
     case DSS_DOT2:
-      { SSG_COUNT(); k_dss<N, T, DSS_DOT2><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, mask, y, y2, part, stop, op); }
+      { SSG_COUNT(); k_dss<N, T, DSS_DOT2><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, ec, mask, y, y2, part, stop, op); }
       break;
     case DSS_RESID:
-      { SSG_COUNT(); k_dss<N, T, DSS_RESID><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, mask, y, y2, part, stop, op); }
+      { SSG_COUNT(); k_dss<N, T, DSS_RESID><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, ec, mask, y, y2, part, stop, op); }
       break;
     case DSS_AVG:
-      { SSG_COUNT(); k_dss<N, T, DSS_AVG><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, mask, y, y2, part, stop, op); }
+      { SSG_COUNT(); k_dss<N, T, DSS_AVG><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, ec, mask, y, y2, part, stop, op); }
       break;
     default:
       return cudaErrorInvalidValue;
@@ -741,12 +780,14 @@ static cudaError_t run_dss_n(cudaStream_t s, int mode, int nel, const T* in, T* 
 
 template <typename T>
 static cudaError_t run_dss_t(cudaStream_t s, int mode, int n, int nel, const T* in, T* out,
-                             const int* pairs, const double* mask, const T* y, const T* y2,
-                             double* part, const double* stop, const ScalarOp& op) {
+                             const int* pairs, const int* ec_tab, const double* mask,
+                             const T* y, const T* y2, double* part, const double* stop,
+                             const ScalarOp& op) {
   const int2* pr = reinterpret_cast<const int2*>(pairs);
+  const int4* ec = reinterpret_cast<const int4*>(ec_tab);
   switch (n) {
 #define SSG_DSSN(NV) \
-  case NV: return run_dss_n<NV, T>(s, mode, nel, in, out, pr, mask, y, y2, part, stop, op);
+  case NV: return run_dss_n<NV, T>(s, mode, nel, in, out, pr, ec, mask, y, y2, part, stop, op);
     SSG_DSSN(2) SSG_DSSN(3) SSG_DSSN(4) SSG_DSSN(5) SSG_DSSN(6) SSG_DSSN(7)
     SSG_DSSN(8) SSG_DSSN(9) SSG_DSSN(10) SSG_DSSN(11) SSG_DSSN(12)
 #undef SSG_DSSN
@@ -755,15 +796,16 @@ static cudaError_t run_dss_t(cudaStream_t s, int mode, int n, int nel, const T* 
 }
 
 cudaError_t run_dss(cudaStream_t s, int mode, bool fp32, int n, int nel, const void* in,
-                    void* out, const int* pairs, const double* mask, const void* y,
-                    const void* y2, double* part, const double* stop,
+                    void* out, const int* pairs, const int* ec_tab, const double* mask,
+                    const void* y, const void* y2, double* part, const double* stop,
                     const ScalarOp* op) {
   const ScalarOp o = op_or_none(op);
+  if (!ec_tab) return cudaErrorInvalidValue;
   if (fp32)
-    return run_dss_t<float>(s, mode, n, nel, (const float*)in, (float*)out, pairs, mask,
-                            (const float*)y, (const float*)y2, part, stop, o);
-  return run_dss_t<double>(s, mode, n, nel, (const double*)in, (double*)out, pairs, mask,
-                           (const double*)y, (const double*)y2, part, stop, o);
+    return run_dss_t<float>(s, mode, n, nel, (const float*)in, (float*)out, pairs, ec_tab,
+                            mask, (const float*)y, (const float*)y2, part, stop, o);
+  return run_dss_t<double>(s, mode, n, nel, (const double*)in, (double*)out, pairs, ec_tab,
+                           mask, (const double*)y, (const double*)y2, part, stop, o);
 }
 
 cudaError_t run_tensor3(cudaStream_t s, bool fp32, bool add, int nel, int ni, int no,

@@ -12,6 +12,15 @@
 namespace ssg {
 namespace dev {
 
+// 1/m for a node multiplicity m >= 1, bitwise the IEEE quotient 1.0 / m:
+// powers of two (every multiplicity of a conforming mesh: 1, 2, 4, 8) by
+// their exponent alone, anything else by the division.
+__device__ __forceinline__ double inv_count(unsigned m) {
+  if ((m & (m - 1)) == 0u)
+    return __longlong_as_double((long long)(1023 - (__ffs((int)m) - 1)) << 52);
+  return 1.0 / (double)m;
+}
+
 // ---------------------------------------------------------------------------
 // node numbering of faces / edges / corners (src/global.c:38-177)
 // ---------------------------------------------------------------------------

@@ -342,6 +342,64 @@ void host_dss(const HostMesh& m, int n, double* u) {
   }
 }
 
+// Ordered DSS sources of one local node (element e, node loc): its
+// neighbours' copies in the reference's order -- the x-, y- and z-face
+// (w/e, s/n, b/t), the xy-, xz- and yz-edge, the corner -- as
+// element * n^3 + node, -1 for none.  Same pairing and order as host_dss.
+static void node_sources(const HostMesh& m, int n, int e, int loc, int (&src)[7]) {
+  const long long nt = (long long)n * n * n;
+  const int M = n - 1;
+  const int i = loc % n, j = (loc / n) % n, k = loc / (n * n);
+  const int* pr = m.pairs.data() + 52 * (size_t)e;
+  for (auto& v : src) v = -1;
+  const bool ei = i == 0 || i == M, ej = j == 0 || j == M, ek = k == 0 || k == M;
+  auto put = [&](int a, int sl, int node) {
+    if (pr[2 * sl] >= 0) src[a] = (int)(pr[2 * sl] * nt + node);
+  };
+  if (ei) { const int sl = i == M; put(0, sl, face_node(n, pr[2 * sl + 1], k, j)); }
+  if (ej) { const int sl = 2 + (j == M); put(1, sl, face_node(n, pr[2 * sl + 1], k, i)); }
+  if (ek) { const int sl = 4 + (k == M); put(2, sl, face_node(n, pr[2 * sl + 1], j, i)); }
+  if (ei && ej) {
+    const int sl = 6 + ((i == M) | ((j == M) << 1));
+    put(3, sl, edge_node(n, pr[2 * sl + 1], k));
+  }
+  if (ek && ei) {
+    const int sl = 10 + ((i == M) | ((k == M) << 1));
+    put(4, sl, edge_node(n, pr[2 * sl + 1], j));
+  }
+  if (ek && ej) {
+    const int sl = 14 + ((j == M) | ((k == M) << 1));
+    put(5, sl, edge_node(n, pr[2 * sl + 1], i));
+  }
+  if (ei && ej && ek) {
+    const int sl = 18 + ((i == M) | ((j == M) << 1) | ((k == M) << 2));
+    put(6, sl, corner_node(n, pr[2 * sl + 1]));
+  }
+}
+
+void dss_ec_table(const HostMesh& m, int n, std::vector<int>& tab) {
+  const int I = n > 2 ? n - 2 : 0;
+  const size_t per = (size_t)12 * I * 4 + 8 * 8;
+  tab.assign(per * m.nel, -1);
+  for (int e = 0; e < m.nel; ++e) {
+    int* t = tab.data() + per * e;
+    int src[7];
+    for (int q = 0; q < 12; ++q)
+      for (int p = 1; p <= I; ++p, t += 4) {
+        node_sources(m, n, e, edge_node(n, q, p), src);
+        int w = 0;
+        for (int a = 0; a < 7; ++a)
+          if (src[a] >= 0) t[w++] = src[a];
+      }
+    for (int c = 0; c < 8; ++c, t += 8) {
+      node_sources(m, n, e, corner_node(n, c), src);
+      int w = 0;
+      for (int a = 0; a < 7; ++a)
+        if (src[a] >= 0) t[w++] = src[a];
+    }
+  }
+}
+
 // Element-local Jacobi diagonal of the Laplacian in the reference's form
 // (helmholtz_diagonal with lambda = 0, src/helmholtz.c:51-68): the metric
 // terms G11, G22, G33 without the Jacobian determinant.  The Helmholtz

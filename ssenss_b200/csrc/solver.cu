@@ -36,12 +36,29 @@ struct Workspace {
   double* hist = nullptr;
   int hist_cap = 0;
   std::vector<void*> blocks;
+  // the V-cycle r -> z as one CUDA graph (its launch sequence is static:
+  // smoother iterations past convergence exit on a device flag)
+  cudaGraphExec_t vcycle = nullptr;
+  double vcycle_eps = -1.0;
+  int vcycle_precision = -1;
+  unsigned long long vcycle_kernels = 0;
+  bool vcycle_failed = false;
+  double warm_eps = -1.0;   // eps / precision of the last direct V-cycle
+  int warm_precision = -1;
 };
 
 void free_workspace(Workspace* w) {
   if (!w) return;
+  if (w->vcycle) cudaGraphExecDestroy(w->vcycle);
   for (void* p : w->blocks) cudaFree(p);
   delete w;
+}
+
+void invalidate_graphs(ssg_context* c) {
+  if (!c->ws) return;
+  if (c->ws->vcycle) cudaGraphExecDestroy(c->ws->vcycle);
+  c->ws->vcycle = nullptr;
+  c->ws->vcycle_failed = false;
 }
 
 static ssg_status wsalloc(ssg_context* c, Workspace* w, void** p, size_t bytes) {
@@ -76,6 +93,7 @@ ssg_status ensure_workspace(ssg_context* c) {
     for (int l = 0; l < c->nlev; ++l)
       SSG_TRY(alloc_level_work(c, c->ws, c->ws->w32[l], c->lev[l].npts, sizeof(float)));
     c->ws->have32 = true;
+    invalidate_graphs(c);
   }
   return SSG_OK;
 }
@@ -97,7 +115,7 @@ ssg_status op_apply(ssg_context* c, int level, int var, bool fp32, const void* i
                      fp32 ? (const void*)L.gf32 : (const void*)L.gf, L.npts, L.bj, L.D, L.S,
                      lambda_of(c), nullptr));
   if (global)
-    SSG_CUDA(c, run_dss(c->stream, DSS_PLAIN, fp32, L.n, c->nel, loc, out, c->d_pairs,
+    SSG_CUDA(c, run_dss(c->stream, DSS_PLAIN, fp32, L.n, c->nel, loc, out, c->d_pairs, L.dss_ec,
                         helm ? L.mask : nullptr, nullptr, nullptr, nullptr));
   return SSG_OK;
 }
@@ -145,7 +163,7 @@ ssg_status cg_solve(ssg_context* c, int level, int var, bool fp32, void* f, void
   SSG_CUDA(c, run_ax(s, L.n, c->nel, 0, helm, fp32, x, W.aploc, gf, np, L.bj, L.D, L.S, lam,
                      nullptr));
   op.code = OP_NULL_C;
-  SSG_CUDA(c, run_dss(s, DSS_RESID, fp32, L.n, c->nel, W.aploc, W.r, c->d_pairs, mask, f,
+  SSG_CUDA(c, run_dss(s, DSS_RESID, fp32, L.n, c->nel, W.aploc, W.r, c->d_pairs, L.dss_ec, mask, f,
                       nullptr, c->d_part, nullptr, &op));
   if (pres) SSG_CUDA(c, run_add_const(s, fp32, np, W.r, fr + F_C, 1));
   // z = M^-1 r and its nullspace constant
@@ -177,7 +195,7 @@ ssg_status cg_solve(ssg_context* c, int level, int var, bool fp32, void* f, void
     }
     // ap = DSS(mask aploc); alpha = rdz / (p w).ap
     op.code = OP_CG_ALPHA;
-    SSG_CUDA(c, run_dss(s, DSS_DOT, fp32, L.n, c->nel, W.aploc, W.ap, c->d_pairs, mask,
+    SSG_CUDA(c, run_dss(s, DSS_DOT, fp32, L.n, c->nel, W.aploc, W.ap, c->d_pairs, L.dss_ec, mask,
                         W.p, nullptr, c->d_part, stop, &op));
     // x += alpha p; r -= alpha ap; z = M^-1 r; beta; err
     op.code = OP_CG_BETA;
@@ -242,14 +260,14 @@ static ssg_status mg_recurse(ssg_context* c, int L, void* f, void* x, double eps
     SSG_CUDA(c, run_ax(s, F.n, c->nel, 0, false, fp32, x, W.aploc,
                        fp32 ? (const void*)F.gf32 : (const void*)F.gf, F.npts, nullptr, F.D,
                        F.D, 0.0, nullptr));
-    SSG_CUDA(c, run_dss(s, DSS_RESID, fp32, F.n, c->nel, W.aploc, W.rr, c->d_pairs, nullptr,
+    SSG_CUDA(c, run_dss(s, DSS_RESID, fp32, F.n, c->nel, W.aploc, W.rr, c->d_pairs, F.dss_ec, nullptr,
                         f, nullptr, c->d_part));
     rin = W.rr;
   }
   // restriction: (J^T)^3 then DSS-average at the coarse level
   SSG_CUDA(c, run_tensor3(s, fp32, false, c->nel, F.n, C.n,
                           C.Ar, rin, Wc.tc));
-  SSG_CUDA(c, run_dss(s, DSS_AVG, fp32, C.n, c->nel, Wc.tc, Wc.f, c->d_pairs, nullptr,
+  SSG_CUDA(c, run_dss(s, DSS_AVG, fp32, C.n, c->nel, Wc.tc, Wc.f, c->d_pairs, C.dss_ec, nullptr,
                       nullptr, nullptr, nullptr));
   SSG_CUDA(c, cudaMemsetAsync(Wc.x, 0, C.npts * (fp32 ? sizeof(float) : sizeof(double)), s));
   SSG_TRY(mg_recurse(c, L + 1, Wc.f, Wc.x, eps, fp32));
@@ -284,6 +302,54 @@ ssg_status mg_apply(ssg_context* c, const double* r, double* z, double eps) {
   return SSG_OK;
 }
 
+// z = M^-1 r for the FCG workspace vectors (r = ws->r, z = ws->z): replays
+// the captured V-cycle graph, capturing it on first use for this eps and
+// precision.  A capture the driver refuses falls back to direct launches.
+static ssg_status vcycle_ws(ssg_context* c, double eps) {
+  Workspace* w = c->ws;
+  if (!c->graphs || w->vcycle_failed) return mg_apply(c, w->r, w->z, eps);
+  cudaStream_t s = c->stream;
+  if (w->vcycle && (w->vcycle_eps != eps || w->vcycle_precision != c->precision))
+    invalidate_graphs(c);
+  if (!w->vcycle && (w->warm_eps != eps || w->warm_precision != c->precision)) {
+    // first V-cycle of this configuration runs directly: one-time kernel
+    // attribute settings happen outside any capture
+    w->warm_eps = eps;
+    w->warm_precision = c->precision;
+    return mg_apply(c, w->r, w->z, eps);
+  }
+  if (!w->vcycle) {
+    const unsigned long long before = g_launches;
+    cudaGraph_t g = nullptr;
+    if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+      cudaGetLastError();
+      w->vcycle_failed = true;
+      return mg_apply(c, w->r, w->z, eps);
+    }
+    const ssg_status st = mg_apply(c, w->r, w->z, eps);
+    const cudaError_t ce = cudaStreamEndCapture(s, &g);
+    const unsigned long long captured = g_launches - before;
+    g_launches = before;
+    cudaGraphExec_t ex = nullptr;
+    if (st != SSG_OK || ce != cudaSuccess || !g ||
+        cudaGraphInstantiate(&ex, g, 0) != cudaSuccess) {
+      cudaGetLastError();
+      if (g) cudaGraphDestroy(g);
+      w->vcycle_failed = true;
+      c->err.clear();
+      return mg_apply(c, w->r, w->z, eps);
+    }
+    cudaGraphDestroy(g);
+    w->vcycle = ex;
+    w->vcycle_eps = eps;
+    w->vcycle_precision = c->precision;
+    w->vcycle_kernels = captured;
+  }
+  SSG_CUDA(c, cudaGraphLaunch(w->vcycle, s));
+  g_launches += w->vcycle_kernels;
+  return SSG_OK;
+}
+
 ssg_status fcg_solve(ssg_context* c, const double* f, double* u, double eps, int max_iter,
                      ssg_solve_info* info) {
   SSG_TRY(ensure_workspace(c));
@@ -312,7 +378,7 @@ ssg_status fcg_solve(ssg_context* c, const double* f, double* u, double eps, int
   SSG_CUDA(c, run_ax(s, L.n, c->nel, 0, false, false, u, w->aploc, L.gf, np, nullptr, L.D,
                      L.D, 0.0, nullptr));
   op.code = OP_NULL_C;
-  SSG_CUDA(c, run_dss(s, DSS_RESID, false, L.n, c->nel, w->aploc, w->r, c->d_pairs, nullptr,
+  SSG_CUDA(c, run_dss(s, DSS_RESID, false, L.n, c->nel, w->aploc, w->r, c->d_pairs, L.dss_ec, nullptr,
                       f, nullptr, c->d_part, nullptr, &op));
   SSG_CUDA(c, run_add_const(s, false, np, w->r, fr + F_C, 1));
   PtrList ys;
@@ -327,7 +393,7 @@ ssg_status fcg_solve(ssg_context* c, const double* f, double* u, double eps, int
   for (int j = 0; j < max_iter; ++j) {
     int m = std::max(1, j % (mmax + 1));
     m = std::min(m, j);
-    SSG_TRY(mg_apply(c, w->r, w->z, eps));
+    SSG_TRY(vcycle_ws(c, eps));
     // subtract_nullspace(z)
     op.code = OP_NULL_C;
     SSG_CUDA(c, run_wsum(s, false, np, w->z, L.mult, c->d_part, nb, &op));
@@ -366,7 +432,7 @@ ssg_status fcg_solve(ssg_context* c, const double* f, double* u, double eps, int
                        L.D, 0.0, nullptr));
     op.pap_idx[0] = aslot[0];
     op.code = OP_FCG_ALPHA;
-    SSG_CUDA(c, run_dss(s, DSS_DOT2, false, L.n, c->nel, w->aploc, ap0, c->d_pairs, nullptr,
+    SSG_CUDA(c, run_dss(s, DSS_DOT2, false, L.n, c->nel, w->aploc, ap0, c->d_pairs, L.dss_ec, nullptr,
                         p0, w->r, c->d_part, nullptr, &op));
     // u += alpha p0; r -= alpha ap0; err
     op.code = OP_FCG_ERR;

@@ -54,6 +54,11 @@ ssg_status build_mesh(HostMesh& m, int n, int nel, const double* vertices,
 ssg_status build_pairs(HostMesh& m, std::string& err);
 void stiffness_diagonal(const HostLevel& L, int nel, double* out);
 void host_dss(const HostMesh& m, int n, double* u);
+// Per element, in the DSS kernel's node order, the ordered source lists of
+// the edge nodes (12 (n-2) records of 4 ints: 3 sources + pad) and corner
+// nodes (8 records of 8 ints: 7 sources + pad); a source is
+// element * n^3 + node, -1 where the node has none.
+void dss_ec_table(const HostMesh& m, int n, std::vector<int>& tab);
 
 // ---------------------------------------------------------------------------
 // device-side level
@@ -67,6 +72,7 @@ struct DevLevel {
   double* dinv_p = nullptr;    // Poisson Jacobi inverse
   double* dinv_h = nullptr;    // Helmholtz Jacobi inverse (for lambda_h)
   uint8_t* mult = nullptr;     // multiplicity (1 + DSS contributions)
+  int* dss_ec = nullptr;       // edge/corner DSS source table (dss_ec_table)
   double* mask = nullptr;      // Dirichlet mask (null without walls)
   double* D = nullptr;         // n*n
   double* S = nullptr;         // n*n
@@ -162,5 +168,7 @@ ssg_status mg_apply(ssg_context* c, const double* r, double* z, double eps);
 ssg_status fcg_solve(ssg_context* c, const double* f, double* u, double eps, int max_iter,
                      ssg_solve_info* info);
 ssg_status helmholtz_diag_update(ssg_context* c);
+// drop captured CUDA graphs (launch shapes or buffers changed)
+void invalidate_graphs(ssg_context* c);
 
 }  // namespace ssg

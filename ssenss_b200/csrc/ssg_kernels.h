@@ -68,14 +68,21 @@ extern unsigned long long g_launches;   // kernel launches of this library
 
 int vec_blocks(size_t npts);
 int ax_epb(int n);
+int ax_epb_max(int n);
 int dss_grid(int n, int nel);
+// autotuned launch shapes (0 = default rule), indexed by order n
+extern int g_tune_ax_epb[];
+extern int g_tune_dss_bps[];
+extern int g_tune_vec_bps;
 
 cudaError_t run_ax(cudaStream_t s, int n, int nel, int epb, bool helm, bool fp32,
                    const void* in, void* out, const void* gf, size_t npts,
                    const double* bj, const double* D, const double* S, double lambda,
                    const PUpdateArgs* pua);
+// ec_tab: ordered edge/corner source table of order n (dss_ec_table)
 cudaError_t run_dss(cudaStream_t s, int mode, bool fp32, int n, int nel, const void* in,
-                    void* out, const int* pairs, const double* mask, const void* y,
+                    void* out, const int* pairs, const int* ec_tab, const double* mask,
+                    const void* y,
                     const void* y2, double* part, const double* stop = nullptr,
                     const ScalarOp* op = nullptr);
 cudaError_t run_tensor3(cudaStream_t s, bool fp32, bool add, int nel, int ni, int no,

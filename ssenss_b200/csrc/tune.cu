@@ -1,0 +1,159 @@
+// Launch-shape autotuner.
+//
+// The element kernels have one free shape parameter per order n and the
+// vector kernels one overall:
+//   * elements per block of the operator (k_ax): 1, 2, 4, ... up to the
+//     256-thread / 96 KB limit of ax_epb_max(n);
+//   * blocks per SM of the persistent DSS grid: 1 .. 16;
+//   * blocks per SM of the grid-stride vector kernels: 2 .. 32.
+// ssg_autotune times every candidate on the context's own mesh and levels
+// (CUDA events on the context stream, best of three runs of ten launches)
+// and keeps the fastest in the process-wide tables the launchers read.  The
+// tables are keyed by order only, so one tuning serves every mesh of that
+// order on the device.  Captured CUDA graphs hold the old shapes and are
+// dropped.  Nothing here changes results: each candidate computes the same
+// sums in the same order.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "ssg_internal.h"
+#include "ssg_kernels.h"
+
+namespace ssg {
+namespace {
+
+// best-of-3 time of `reps` launches of f (ms)
+template <typename F>
+ssg_status time_launches(ssg_context* c, int reps, F&& f, float* best) {
+  *best = 1e30f;
+  for (int trial = 0; trial < 3; ++trial) {
+    SSG_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+    for (int r = 0; r < reps; ++r) SSG_CUDA(c, f());
+    SSG_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+    SSG_CUDA(c, cudaEventSynchronize(c->ev1));
+    float ms = 0.f;
+    SSG_CUDA(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    *best = std::min(*best, ms);
+  }
+  return SSG_OK;
+}
+
+}  // namespace
+
+// scratch vectors of the tuning runs: three level-sized FP64 buffers
+static ssg_status tune_level(ssg_context* c, int level, double* a, double* b, double* y,
+                             int reps) {
+  const DevLevel& L = c->lev[level];
+  const int n = L.n;
+  // operator: elements per block
+  {
+    int best_epb = 0;
+    float best = 1e30f;
+    for (int epb = 1; epb <= ax_epb_max(n); epb *= 2) {
+      g_tune_ax_epb[n] = epb;
+      SSG_CUDA(c, run_ax(c->stream, n, c->nel, epb, false, false, a, b, L.gf, L.npts, nullptr,
+                         L.D, L.D, 0.0, nullptr));
+      float t = 0.f;
+      SSG_TRY(time_launches(c, reps, [&] {
+        return run_ax(c->stream, n, c->nel, epb, false, false, a, b, L.gf, L.npts, nullptr,
+                      L.D, L.D, 0.0, nullptr);
+      }, &t));
+      if (t < best) {
+        best = t;
+        best_epb = epb;
+      }
+    }
+    g_tune_ax_epb[n] = best_epb;
+  }
+  // DSS: blocks per SM of the persistent grid
+  {
+    int best_bps = 0;
+    float best = 1e30f;
+    for (int bps = 1; bps <= 16; bps *= 2) {
+      g_tune_dss_bps[n] = bps;
+      float t = 0.f;
+      SSG_TRY(time_launches(c, reps, [&] {
+        return run_dss(c->stream, DSS_DOT, false, n, c->nel, a, b, c->d_pairs, L.dss_ec,
+                       nullptr, y, nullptr, c->d_part, nullptr, nullptr);
+      }, &t));
+      if (t < best) {
+        best = t;
+        best_bps = bps;
+      }
+    }
+    g_tune_dss_bps[n] = best_bps;
+  }
+  return SSG_OK;
+}
+
+}  // namespace ssg
+
+using namespace ssg;
+
+extern "C" {
+
+ssg_status ssg_autotune(ssg_context* c, int reps) {
+  if (!c) return SSG_ERR_ARG;
+  if (!c->ready) return fail(c, SSG_ERR_STATE, "no mesh set up on this context");
+  if (reps <= 0) reps = 10;
+  SSG_CUDA(c, cudaSetDevice(c->device));
+  const size_t np0 = c->lev[0].npts;
+  std::vector<double*> buf(3, nullptr);
+  for (auto& p : buf) {
+    if (cudaMalloc(&p, np0 * sizeof(double)) != cudaSuccess) {
+      cudaGetLastError();
+      for (auto& q : buf)
+        if (q) cudaFree(q);
+      return fail(c, SSG_ERR_NOMEM, "autotune scratch");
+    }
+    cudaMemsetAsync(p, 0, np0 * sizeof(double), c->stream);
+  }
+  ssg_status st = SSG_OK;
+  bool seen[SSG_MAXN + 1] = {false};
+  for (int l = 0; l < c->nlev && st == SSG_OK; ++l) {
+    const int n = c->lev[l].n;
+    if (seen[n]) continue;
+    seen[n] = true;
+    st = tune_level(c, l, buf[0], buf[1], buf[2], reps);
+  }
+  // vector kernels: blocks per SM of the grid-stride loops (a two-vector
+  // weighted dot, read-only)
+  if (st == SSG_OK) {
+    int best_bps = 0;
+    float best = 1e30f;
+    PtrList ys;
+    ys.p[0] = buf[1];
+    ys.p[1] = buf[2];
+    for (int bps = 2; bps <= 32 && st == SSG_OK; bps *= 2) {
+      g_tune_vec_bps = bps;
+      const int nb = vec_blocks(np0);
+      float t = 0.f;
+      st = time_launches(c, reps, [&] {
+        return run_dots(c->stream, false, np0, buf[0], ys, 2, c->lev[0].mult, c->d_part, nb,
+                        nullptr);
+      }, &t);
+      if (t < best) {
+        best = t;
+        best_bps = bps;
+      }
+    }
+    g_tune_vec_bps = best_bps;
+  }
+  cudaStreamSynchronize(c->stream);
+  for (auto& p : buf) cudaFree(p);
+  invalidate_graphs(c);
+  return st;
+}
+
+ssg_status ssg_tuning(int n, int* ax_elements_per_block, int* dss_blocks_per_sm,
+                      int* vector_blocks_per_sm) {
+  if (n < 2 || n > SSG_MAXN) return SSG_ERR_ARG;
+  if (ax_elements_per_block) *ax_elements_per_block = ax_epb(n);
+  if (dss_blocks_per_sm) *dss_blocks_per_sm = g_tune_dss_bps[n] > 0 ? g_tune_dss_bps[n] : 4;
+  if (vector_blocks_per_sm) *vector_blocks_per_sm = g_tune_vec_bps > 0 ? g_tune_vec_bps : 8;
+  return SSG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,85 @@
+"""CUDA-graph replay of the V-cycle and the launch-shape autotuner.
+
+The captured graph launches the same kernels with the same arguments as the
+direct path, so a solve with graphs is bitwise the solve without.  The
+autotuner changes only launch shapes: element-local results and the DSS stay
+bitwise, while block-partial sums of the inner products may associate
+differently, so solves are compared to the oracle at the usual tolerance.
+(Named to run after the other GPU tests: the tuned shapes are process-wide.)
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+import ssenss_b200 as S
+from ssenss_b200.mesh import channel_mesh, tgv_box
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def rhs(orc, n):
+    X, Y, Z = orc.geometry(0, 7), orc.geometry(0, 8), orc.geometry(0, 9)
+    g = 3.0 * np.cos(X + 0.3) * np.cos(Y + 0.7) * np.cos(Z + 1.1)
+    x, w = orc.gll(n)
+    rho = w[None, None, None, :] * w[None, None, :, None] * w[None, :, None, None]
+    return orc.dss(rho * orc.geometry(0, 6) * g)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_graph_replay_is_bitwise_direct(precision, gpu_ctx_factory):
+    mesh, n = tgv_box(3), 8
+    orc = O.Oracle(mesh, n)
+    f = rhs(orc, n)
+    ctx = gpu_ctx_factory(mesh, n, precision=precision)
+    ctx.set_graphs(False)
+    u_d, info_d = ctx.solve_poisson_cg(f, np.zeros_like(f))
+    ctx.set_graphs(True)
+    runs = [ctx.solve_poisson_cg(f, np.zeros_like(f)) for _ in range(3)]
+    for u_g, info_g in runs:      # warm-up run, capture run, replay run
+        assert info_g["iterations"] == info_d["iterations"]
+        assert np.array_equal(u_g, u_d)
+        assert np.array_equal(info_g["history"], info_d["history"])
+
+
+def test_graph_launch_count_is_kept(gpu_ctx_factory):
+    mesh, n = tgv_box(3), 6
+    orc = O.Oracle(mesh, n)
+    f = rhs(orc, n)
+    ctx = gpu_ctx_factory(mesh, n)
+    ctx.set_graphs(False)
+    c0 = S.kernel_launch_count()
+    ctx.solve_poisson_cg(f, np.zeros_like(f))
+    direct = S.kernel_launch_count() - c0
+    ctx.set_graphs(True)
+    ctx.solve_poisson_cg(f, np.zeros_like(f))      # warm-up of the V-cycle
+    ctx.solve_poisson_cg(f, np.zeros_like(f))      # capture
+    c0 = S.kernel_launch_count()
+    ctx.solve_poisson_cg(f, np.zeros_like(f))      # replay
+    assert S.kernel_launch_count() - c0 == direct
+
+
+@pytest.mark.parametrize("mk,n", [(lambda: tgv_box(3), 8),
+                                  (lambda: channel_mesh((4, 3, 3), seed=7), 7)])
+def test_autotuned_shapes_keep_parity(mk, n, gpu_ctx_factory):
+    mesh = mk()
+    orc = O.Oracle(mesh, n)
+    ctx = gpu_ctx_factory(mesh, n)
+    shapes = ctx.autotune(reps=3)
+    assert set(shapes) == set(ctx.orders)
+    for n_l, sh in shapes.items():
+        assert sh["ax_elements_per_block"] >= 1
+        assert 1 <= sh["dss_blocks_per_sm"] <= 16
+        assert 2 <= sh["vector_blocks_per_sm"] <= 32
+    rng = np.random.default_rng(9)
+    u = rng.standard_normal((mesh.nel, n, n, n))
+    assert np.array_equal(ctx.direct_stiffness_summation(u.copy()), orc.dss(u))
+    assert rel(ctx.global_opeval(O.PRESSURE, u), orc.global_opeval(O.PRESSURE, u)) < 1e-13
+    f = rhs(orc, n)
+    u_o, h_o = orc.solve_poisson(f, np.zeros_like(f))
+    u_g, info = ctx.solve_poisson_cg(f, np.zeros_like(f))
+    assert info["iterations"] == len(h_o)
+    assert rel(u_g, u_o) < 1e-11
