@@ -105,6 +105,15 @@ ssg_status ssg_set_graphs(ssg_context *ctx, int enable);
 
 /* ---- discretisation set-up ------------------------------------------- */
 
+/* Set-up options of the next ssg_setup_mesh (no reference counterpart):
+ * skip the dealiasing grid (convection unavailable) and/or the particle
+ * geometry, for contexts that only solve -- e.g. the serving loop's. */
+#define SSG_SETUP_NO_DEALIAS 1u
+#define SSG_SETUP_NO_PARTICLES 2u
+ssg_status ssg_set_setup_options(ssg_context *ctx, unsigned flags);
+/* Device memory (bytes) the context holds now. */
+ssg_status ssg_memory_info(const ssg_context *ctx, size_t *device_bytes);
+
 /* Build the whole discretisation from grid records, as read_grid +
  * connect_elements + initialise_preconditioners do (src/dataio.c:197-227,
  * src/init.c:38-50, src/precon.c:196-205): GLL bases of all p-multigrid
@@ -245,6 +254,61 @@ ssg_status ssg_autotune(ssg_context *ctx, int reps);
 /* Launch shapes in use for order n (tuned or default). */
 ssg_status ssg_tuning(int n, int *ax_elements_per_block,
 		int *dss_blocks_per_sm, int *vector_blocks_per_sm);
+
+/* ---- serving loop (no reference counterpart) ------------------------------- */
+
+/* Independent solve requests of different meshes and orders, admitted in
+ * arrival order by an HBM budget and run concurrently (continuous batching:
+ * up to max_active at once, each on its own stream, new ones starting as
+ * slots and memory free up).  Meshes, factors and Krylov workspaces stay
+ * resident between requests of the same mesh_key. */
+typedef struct ssg_server ssg_server;
+
+typedef struct {
+	int nel;                  /* mesh: elements, vertices (nel x 3 x 8), */
+	const double *vertices;   /* neighbour table (nel x 26), copied at */
+	const int *neigh;         /* submission */
+	unsigned long long mesh_key;  /* caller's identity of the mesh; 0 = none */
+	int n;                    /* GLL points per direction (N + 1), 2..12 */
+	double lambda;            /* Helmholtz coefficient; 0 = Poisson */
+	double eps;               /* stopping tolerance on sqrt((r.r)_w) */
+	int relative;             /* 1: eps relative to sqrt((f.f)_w) */
+	int precision;            /* SSG_PRECISION_FP64 / _MIXED (Poisson V-cycle) */
+	int max_iter;             /* <= 0: 5000 */
+	double deadline_ms;       /* <= 0: none; counted from submission */
+} ssg_request;
+
+typedef struct {
+	unsigned long long submitted, completed, failed, cancelled, rejected;
+	double p50_ms, p99_ms, mean_ms, max_ms;  /* submission -> result */
+	double queue_p50_ms, queue_p99_ms;       /* submission -> start */
+	double solves_per_s;      /* completed / (last result - first submission) */
+	size_t hbm_in_use, hbm_peak, hbm_budget;
+	unsigned long long mesh_hits, mesh_misses, evictions;
+	int max_active_seen, resident_contexts;
+} ssg_server_stats;
+
+/* Admission estimate of a request's resident context (bytes); host only. */
+size_t ssg_request_bytes(int n, int nel, int precision);
+ssg_status ssg_server_create(int device, size_t hbm_budget, int max_active,
+		ssg_server **out);
+/* rhs (host, nel x n^3, an assembled weak right-hand side) is copied at
+ * submission; the solution is written to `solution` (host) before the
+ * request completes.  Initial guess zero. */
+ssg_status ssg_server_submit(ssg_server *srv, const ssg_request *req,
+		const double *rhs, double *solution, unsigned long long *id);
+/* Block until request id is done (timeout_ms < 0: no limit; else
+ * SSG_ERR_TIMEOUT when it is not done in time).  *result is the request's
+ * own status: SSG_OK, SSG_MAXITER, SSG_ERR_BUDGET (larger than the whole
+ * budget), SSG_ERR_CANCELLED, SSG_ERR_TIMEOUT (deadline), ... */
+ssg_status ssg_server_wait(ssg_server *srv, unsigned long long id,
+		double timeout_ms, ssg_status *result, ssg_solve_info *info);
+ssg_status ssg_server_cancel(ssg_server *srv, unsigned long long id);
+/* Block until the queue is empty and nothing runs. */
+ssg_status ssg_server_drain(ssg_server *srv, double timeout_ms);
+ssg_status ssg_server_get_stats(ssg_server *srv, ssg_server_stats *out);
+/* Cancels queued requests, waits for running ones, frees every context. */
+void ssg_server_destroy(ssg_server *srv);
 
 /* ---- instrumentation -------------------------------------------------------- */
 

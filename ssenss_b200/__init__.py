@@ -121,6 +121,16 @@ class Context:
         self._check(self.lib.ssg_autotune(self.h, int(reps)), "autotune")
         return {n: tuning(n) for n in sorted(set(self.orders))}
 
+    def set_setup_options(self, no_dealias=False, no_particles=False):
+        """ssg_set_setup_options for the next setup_mesh."""
+        flags = (1 if no_dealias else 0) | (2 if no_particles else 0)
+        self._check(self.lib.ssg_set_setup_options(self.h, flags), "set_setup_options")
+
+    def memory_bytes(self) -> int:
+        b = C.c_size_t()
+        self._check(self.lib.ssg_memory_info(self.h, C.byref(b)), "memory_info")
+        return int(b.value)
+
     def setup_mesh(self, mesh, n: int):
         vert = np.ascontiguousarray(mesh.vertices, dtype=np.float64)
         neigh = np.ascontiguousarray(mesh.neigh, dtype=np.int32)
@@ -284,3 +294,102 @@ class Context:
             self.h, state.shape[0], _ptr(state), _ptr(ints), t, dt, C.byref(passes)),
             "integrate_particle_equations")
         return state, ints, passes.value
+
+
+# ---------------------------------------------------------------------------
+# serving loop (ssg_server_*)
+# ---------------------------------------------------------------------------
+def request_bytes(n: int, nel: int, precision="mixed") -> int:
+    """Admission estimate (bytes) of a request's resident context."""
+    p = {"fp64": FP64, "mixed": MIXED}.get(precision, precision)
+    return int(_lib.load().ssg_request_bytes(int(n), int(nel), int(p)))
+
+
+def mesh_key(mesh, n: int) -> int:
+    """Stable 64-bit identity of (mesh, order) for the server's context cache."""
+    import hashlib
+    h = hashlib.blake2b(digest_size=8)
+    h.update(np.ascontiguousarray(mesh.vertices, dtype=np.float64).tobytes())
+    h.update(np.ascontiguousarray(mesh.neigh, dtype=np.int32).tobytes())
+    h.update(int(n).to_bytes(4, "little"))
+    return int.from_bytes(h.digest(), "little") or 1
+
+
+class Server:
+    """Continuous-batching solve server on one GPU (ssg_server)."""
+
+    def __init__(self, device: int = 0, hbm_budget: float = 150e9, max_active: int = 8):
+        self.lib = _lib.load()
+        h = C.c_void_p()
+        st = self.lib.ssg_server_create(int(device), C.c_size_t(int(hbm_budget)),
+                                        int(max_active), C.byref(h))
+        if st != 0:
+            raise SsgError(st, "ssg_server_create")
+        self.h = h
+        self._pending = {}
+
+    def submit(self, mesh, n, rhs, lam=0.0, eps=1e-10, relative=False, precision="mixed",
+               max_iter=0, deadline_ms=0.0, key=None):
+        vert = np.ascontiguousarray(mesh.vertices, dtype=np.float64)
+        neigh = np.ascontiguousarray(mesh.neigh, dtype=np.int32)
+        rhs = np.ascontiguousarray(rhs, dtype=np.float64)
+        out = np.zeros_like(rhs)
+        r = _lib.Request()
+        r.nel = int(mesh.nel)
+        r.vertices = vert.ctypes.data_as(_lib._dp)
+        r.neigh = neigh.ctypes.data_as(_lib._ip)
+        r.mesh_key = int(mesh_key(mesh, n) if key is None else key)
+        r.n = int(n)
+        r.lam = float(lam)
+        r.eps = float(eps)
+        r.relative = int(bool(relative))
+        r.precision = {"fp64": FP64, "mixed": MIXED}.get(precision, precision)
+        r.max_iter = int(max_iter)
+        r.deadline_ms = float(deadline_ms)
+        rid = C.c_ulonglong()
+        st = self.lib.ssg_server_submit(self.h, C.byref(r), rhs.ctypes.data_as(_lib._dp),
+                                        out.ctypes.data_as(_lib._dp), C.byref(rid))
+        if st != 0:
+            raise SsgError(st, "ssg_server_submit")
+        self._pending[rid.value] = out
+        return rid.value
+
+    def wait(self, rid, timeout_ms=-1.0):
+        """(solution, status name, info) of request rid."""
+        res = C.c_int()
+        info = _lib.SolveInfo()
+        st = self.lib.ssg_server_wait(self.h, C.c_ulonglong(rid), float(timeout_ms),
+                                      C.byref(res), C.byref(info))
+        if st != 0:
+            raise SsgError(st, "ssg_server_wait")
+        out = self._pending.pop(rid, None)
+        return out, STATUS.get(res.value, res.value), {
+            "iterations": info.iterations, "residual": info.residual,
+            "initial_residual": info.initial_residual, "latency_ms": info.solve_ms}
+
+    def cancel(self, rid):
+        self._check(self.lib.ssg_server_cancel(self.h, C.c_ulonglong(rid)), "cancel")
+
+    def drain(self, timeout_ms=-1.0):
+        self._check(self.lib.ssg_server_drain(self.h, float(timeout_ms)), "drain")
+
+    def stats(self) -> dict:
+        s = _lib.ServerStats()
+        self._check(self.lib.ssg_server_get_stats(self.h, C.byref(s)), "stats")
+        return {name: getattr(s, name) for name, _ in s._fields_}
+
+    def _check(self, st, what):
+        if st != 0:
+            raise SsgError(st, what)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.ssg_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+

@@ -27,6 +27,37 @@ class SolveInfo(C.Structure):
     ]
 
 
+class Request(C.Structure):
+    _fields_ = [
+        ("nel", C.c_int),
+        ("vertices", _dp),
+        ("neigh", _ip),
+        ("mesh_key", C.c_ulonglong),
+        ("n", C.c_int),
+        ("lam", C.c_double),
+        ("eps", C.c_double),
+        ("relative", C.c_int),
+        ("precision", C.c_int),
+        ("max_iter", C.c_int),
+        ("deadline_ms", C.c_double),
+    ]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [
+        ("submitted", C.c_ulonglong), ("completed", C.c_ulonglong),
+        ("failed", C.c_ulonglong), ("cancelled", C.c_ulonglong),
+        ("rejected", C.c_ulonglong),
+        ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("mean_ms", C.c_double),
+        ("max_ms", C.c_double), ("queue_p50_ms", C.c_double), ("queue_p99_ms", C.c_double),
+        ("solves_per_s", C.c_double),
+        ("hbm_in_use", C.c_size_t), ("hbm_peak", C.c_size_t), ("hbm_budget", C.c_size_t),
+        ("mesh_hits", C.c_ulonglong), ("mesh_misses", C.c_ulonglong),
+        ("evictions", C.c_ulonglong),
+        ("max_active_seen", C.c_int), ("resident_contexts", C.c_int),
+    ]
+
+
 # (name, restype, argtypes) of every symbol include/ssenss_b200.h declares
 SIGNATURES = [
     ("ssg_create", C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
@@ -66,6 +97,18 @@ SIGNATURES = [
                                           C.c_void_p]),
     ("ssg_kernel_launch_count", C.c_ulonglong, []),
     ("ssg_autotune", C.c_int, [C.c_void_p, C.c_int]),
+    ("ssg_set_setup_options", C.c_int, [C.c_void_p, C.c_uint]),
+    ("ssg_memory_info", C.c_int, [C.c_void_p, C.POINTER(C.c_size_t)]),
+    ("ssg_request_bytes", C.c_size_t, [C.c_int, C.c_int, C.c_int]),
+    ("ssg_server_create", C.c_int, [C.c_int, C.c_size_t, C.c_int, C.POINTER(C.c_void_p)]),
+    ("ssg_server_submit", C.c_int, [C.c_void_p, C.POINTER(Request), _dp, _dp,
+                                    C.POINTER(C.c_ulonglong)]),
+    ("ssg_server_wait", C.c_int, [C.c_void_p, C.c_ulonglong, C.c_double,
+                                  C.POINTER(C.c_int), C.POINTER(SolveInfo)]),
+    ("ssg_server_cancel", C.c_int, [C.c_void_p, C.c_ulonglong]),
+    ("ssg_server_drain", C.c_int, [C.c_void_p, C.c_double]),
+    ("ssg_server_get_stats", C.c_int, [C.c_void_p, C.POINTER(ServerStats)]),
+    ("ssg_server_destroy", None, [C.c_void_p]),
     ("ssg_tuning", C.c_int, [C.c_int, _ip, _ip, _ip]),
     ("ssg_set_particle_velocity", C.c_int, [C.c_void_p, C.c_void_p]),
     ("ssg_integrate_particle_equations", C.c_int, [C.c_void_p, C.c_size_t, C.c_void_p,

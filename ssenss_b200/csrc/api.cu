@@ -39,6 +39,7 @@ static ssg_status dalloc(ssg_context* c, T** p, size_t count) {
   *p = nullptr;
   if (count == 0) return SSG_OK;
   SSG_CUDA(c, cudaMalloc((void**)p, count * sizeof(T)));
+  c->dev_bytes += count * sizeof(T);
   return SSG_OK;
 }
 
@@ -61,11 +62,12 @@ static void dfree(void* p) {
 static void free_level(ssg::DevLevel& d) {
   dfree(d.gf); dfree(d.bj); dfree(d.kdiag); dfree(d.dinv_p); dfree(d.dinv_h);
   dfree(d.mult); dfree(d.mask); dfree(d.D); dfree(d.S); dfree(d.Ar); dfree(d.Ap);
-  dfree(d.gf32); dfree(d.dinv_p32); dfree(d.dss_ec);
+  dfree(d.gf32); dfree(d.dinv_p32); dfree(d.dss_ec); dfree(d.det); dfree(d.rho);
   d = ssg::DevLevel();
 }
 
 static void free_mesh(ssg_context* c) {
+  c->dev_bytes = 0;
   if (c->ws) {
     free_workspace(c->ws);
     c->ws = nullptr;
@@ -238,6 +240,8 @@ static ssg_status upload_all(ssg_context* c) {
       SSG_TRY(dupload(c, &d.Ap, h.jf.data(), h.jf.size()));
     }
     if (l == 0) {
+      SSG_TRY(dupload(c, &d.det, h.det.data(), np));
+      SSG_TRY(dupload(c, &d.rho, rho.data(), rho.size()));
       std::vector<double> im(bj);
       host_dss(H, h.n, im.data());
       for (auto& v : im) v = 1.0 / v;
@@ -258,7 +262,9 @@ static ssg_status upload_all(ssg_context* c) {
   c->part_cap = std::max(16 * vb, 2 * db) + 64;
   SSG_TRY(dalloc(c, &c->d_part, c->part_cap));
   // staging for host arguments: up to three vector fields
-  c->stage_cap = 3 * std::max(np0, (size_t)nel * c->m * c->m * c->m);
+  // (one field unless the dealiasing grid is set up: convection stages
+  // three-component fields)
+  c->stage_cap = H.has_conv ? 3 * np0 : np0;
   for (auto& s : c->d_stage) SSG_TRY(dalloc(c, &s, c->stage_cap));
   SSG_CUDA(c, cudaDeviceSynchronize());
   c->ready = true;
@@ -266,23 +272,19 @@ static ssg_status upload_all(ssg_context* c) {
 }
 
 // Helmholtz Jacobi inverse for lambda = (11/6)/(dt visc) at level 0
-// (initialise_diagonal_precon, src/precon.c:336-359): DSS(kdiag +
-// (lambda rho) J), reciprocal.
+// (initialise_diagonal_precon, src/precon.c:336-359, with
+// helmholtz_diagonal, src/helmholtz.c:51-68): DSS(kdiag + (lambda rho) J),
+// reciprocal -- on the device, from the stored stiffness diagonal.
 ssg_status helmholtz_diag_update(ssg_context* c) {
   const double lam = (11.0 / 6.0) * 1.0 / (c->dt * c->visc);
   ssg::DevLevel& d = c->lev[0];
   if (d.lambda_h == lam) return SSG_OK;
-  const ssg::HostLevel& h = c->host.lev[0];
-  const size_t np = d.npts;
-  std::vector<double> kd(np), hd(np);
-  stiffness_diagonal(h, c->nel, kd.data());
-  const std::vector<double> rho = rho3(h.w);
-  for (int e = 0; e < c->nel; ++e)
-    for (size_t q = 0; q < h.nt; ++q)
-      hd[e * h.nt + q] = kd[e * h.nt + q] + lam * rho[q] * h.det[e * h.nt + q];
-  host_dss(c->host, h.n, hd.data());
-  for (auto& v : hd) v = 1.0 / v;
-  SSG_CUDA(c, cudaMemcpy(d.dinv_h, hd.data(), np * sizeof(double), cudaMemcpyHostToDevice));
+  SSG_TRY(ensure_workspace(c));
+  double* tmp = workspace_scratch(c);
+  SSG_CUDA(c, run_helm_diag(c->stream, d.npts, d.nt, d.kdiag, d.rho, d.det, lam, tmp));
+  SSG_CUDA(c, run_dss(c->stream, DSS_PLAIN, false, d.n, c->nel, tmp, d.dinv_h, c->d_pairs,
+                      d.dss_ec, nullptr, nullptr, nullptr, nullptr));
+  SSG_CUDA(c, run_recip(c->stream, d.npts, d.dinv_h));
   d.lambda_h = lam;
   return SSG_OK;
 }
@@ -451,9 +453,23 @@ ssg_status ssg_setup_mesh(ssg_context* c, int n, int nel, const double* vertices
   SSG_CUDA(c, cudaSetDevice(c->device));
   free_mesh(c);
   c->host = ssg::HostMesh();
-  ssg_status st = build_mesh(c->host, n, nel, vertices, neigh, c->err);
+  ssg_status st = build_mesh(c->host, n, nel, vertices, neigh, c->err, c->setup_opts);
   if (st != SSG_OK) return st;
   return upload_all(c);
+}
+
+ssg_status ssg_set_setup_options(ssg_context* c, unsigned flags) {
+  if (!c) return SSG_ERR_ARG;
+  if (flags & ~(SSG_SETUP_NO_DEALIAS | SSG_SETUP_NO_PARTICLES))
+    return fail(c, SSG_ERR_ARG, "unknown set-up option");
+  c->setup_opts = flags;
+  return SSG_OK;
+}
+
+ssg_status ssg_memory_info(const ssg_context* c, size_t* bytes) {
+  if (!c || !bytes) return SSG_ERR_ARG;
+  *bytes = c->dev_bytes;
+  return SSG_OK;
 }
 
 ssg_status ssg_setup_connectivity(ssg_context* c, int nel, const int* neigh) {
@@ -563,6 +579,7 @@ ssg_status ssg_level_data(ssg_context* c, int level, int which, double* dst) {
     return SSG_OK;
   } else
     return fail(c, SSG_ERR_ARG, "bad selector");
+  SSG_CUDA(c, cudaStreamSynchronize(c->stream));
   SSG_CUDA(c, cudaMemcpy(dst, src, np * sizeof(double), cudaMemcpyDeviceToHost));
   return SSG_OK;
 }

@@ -294,7 +294,7 @@ cudaError_t run_coarse_cg(cudaStream_t s, int device, int nel, const double* f, 
   a.partA = part;
   a.partB = part + 4 * (size_t)G;
   void* args[] = {&a};
-  ++g_launches;
+  count_launch();
   return cudaLaunchCooperativeKernel((const void*)dev::k_coarse_cg, dim3(G), dim3(256), args,
                                      0, s);
 }

@@ -185,7 +185,7 @@ cudaError_t run_convection(cudaStream_t s, int nel, int n, int m, const double* 
   }
   if (nel <= 0) return cudaSuccess;
   const int grid = in_smem ? nel : std::min(nel, kConvScratchBlocks);
-  ++g_launches;
+  count_launch();
   dev::k_convection<<<grid, 512, smem, s>>>(nel, n, m, u, v, udv, tinv, bj, Dm, J,
                                            in_smem ? nullptr : scratch);
   return cudaGetLastError();

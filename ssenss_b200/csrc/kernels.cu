@@ -478,6 +478,20 @@ __global__ void __launch_bounds__(256) k_tensor3(int nel, int ni, int no,
   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < (n);     \
        q += (size_t)gridDim.x * blockDim.x)
 
+// Helmholtz diagonal before DSS: kdiag + (lambda rho) J, the reference's
+// association (src/helmholtz.c:66)
+__global__ void __launch_bounds__(256) k_helm_diag(size_t npts, size_t nt,
+                                                   const double* __restrict__ kd,
+                                                   const double* __restrict__ rho,
+                                                   const double* __restrict__ det, double lam,
+                                                   double* __restrict__ out) {
+  SSG_GRID_LOOP(q, npts) out[q] = kd[q] + (lam * rho[q % nt]) * det[q];
+}
+
+__global__ void __launch_bounds__(256) k_recip(size_t npts, double* __restrict__ x) {
+  SSG_GRID_LOOP(q, npts) x[q] = 1.0 / x[q];
+}
+
 // CG step after ap is known (src/solver.c:66-71):
 //   x += alpha p; r -= alpha ap; z = dinv .* r
 // partials: (r w).z, (r w).r, w.z, w.r
@@ -636,8 +650,9 @@ using namespace dev;
 
 static ScalarOp op_or_none(const ScalarOp* op) { return op ? *op : ScalarOp(); }
 
-unsigned long long g_launches = 0;   // every launch of this library bumps it
-#define SSG_COUNT() (++g_launches)
+std::atomic<unsigned long long> g_launches{0};   // every launch of this library bumps it
+thread_local unsigned long long t_launches = 0;
+#define SSG_COUNT() count_launch()
 
 // Launch shapes chosen by the autotuner (tune.cu); 0 = the default rule.
 // Process-wide: they depend on the order and the device, not on the mesh.
@@ -828,6 +843,19 @@ cudaError_t run_tensor3(cudaStream_t s, bool fp32, bool add, int nel, int ni, in
   return cudaGetLastError();
 }
 
+cudaError_t run_helm_diag(cudaStream_t s, size_t npts, size_t nt, const double* kd,
+                          const double* rho, const double* det, double lam, double* out) {
+  SSG_COUNT();
+  k_helm_diag<<<vec_blocks(npts), 256, 0, s>>>(npts, nt, kd, rho, det, lam, out);
+  return cudaGetLastError();
+}
+
+cudaError_t run_recip(cudaStream_t s, size_t npts, double* x) {
+  SSG_COUNT();
+  k_recip<<<vec_blocks(npts), 256, 0, s>>>(npts, x);
+  return cudaGetLastError();
+}
+
 cudaError_t run_cg_update(cudaStream_t s, bool fp32, size_t npts, const double* alpha,
                           void* x, const void* p, void* r, const void* ap, const void* dinv,
                           const uint8_t* mult, void* z, double* part, int nblk,
@@ -945,4 +973,4 @@ cudaError_t run_reduce(cudaStream_t s, const double* part, int nblk, int nq, dou
 
 }  // namespace ssg
 
-extern "C" unsigned long long ssg_kernel_launch_count(void) { return ssg::g_launches; }
+extern "C" unsigned long long ssg_kernel_launch_count(void) { return ssg::g_launches.load(); }

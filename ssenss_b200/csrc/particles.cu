@@ -300,7 +300,7 @@ cudaError_t run_particles(cudaStream_t s, int n, int nel, size_t npts, const dou
   P.dt = dt;
   if (np == 0) return cudaSuccess;
   const unsigned blocks = (unsigned)((np + 127) / 128);
-  ++g_launches;
+  count_launch();
   dev::k_particles<<<blocks, 128, 0, s>>>(P, np, state, ints, passes);
   return cudaGetLastError();
 }

@@ -5,11 +5,34 @@
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "ssg_internal.h"
 
 namespace ssg {
+
+// Run f(e0, e1) over element ranges on up to 32 host threads.  Every
+// element is computed by one thread with the same arithmetic as a serial
+// loop, so the results do not depend on the thread count.
+template <class F>
+static void parallel_elements(int nel, F&& f) {
+  unsigned hw = std::thread::hardware_concurrency();
+  int nth = (int)std::min<unsigned>(hw ? hw : 1, 32u);
+  nth = std::max(1, std::min(nth, nel / 8));
+  if (nth <= 1) {
+    f(0, nel);
+    return;
+  }
+  std::vector<std::thread> th;
+  const int chunk = (nel + nth - 1) / nth;
+  for (int t = 0; t < nth; ++t) {
+    const int e0 = t * chunk, e1 = std::min(nel, e0 + chunk);
+    if (e0 >= e1) break;
+    th.emplace_back([&f, e0, e1] { f(e0, e1); });
+  }
+  for (auto& x : th) x.join();
+}
 
 int level_orders(int n, int* orders) {
   // nmg[i] = max(2, (n-1)/2^i + 1), stopping at 2 (src/precon.c:62-69)
@@ -166,7 +189,8 @@ static void compute_factors(HostLevel& L, int nel, bool keep_jac) {
   const size_t nt = L.nt;
   std::vector<double> jac[9];
   for (auto& a : jac) a.assign(nt * nel, 0.0);
-  for (int e = 0; e < nel; ++e) {
+  parallel_elements(nel, [&](int e0, int e1) {
+  for (int e = e0; e < e1; ++e) {
     const size_t o = e * nt;
     for (int a = 0; a < 3; ++a) {
       const double* g = L.grid[a].data() + o;
@@ -186,9 +210,11 @@ static void compute_factors(HostLevel& L, int nel, bool keep_jac) {
           }
     }
   }
+  });
   static const int k0[3] = {1, 0, 0}, k1[3] = {2, 2, 1}, k2[3] = {2, 0, 1}, k3[3] = {1, 2, 0};
   static const double sg[3] = {1.0, -1.0, 1.0};
-  for (size_t q = 0; q < nt * nel; ++q) {
+  parallel_elements(nel, [&](int e0, int e1) {
+  for (size_t q = e0 * nt; q < e1 * nt; ++q) {
     double a[3][3], ai[3][3];
     for (int r = 0; r < 3; ++r)
       for (int c = 0; c < 3; ++c) a[r][c] = jac[3 * r + c][q];
@@ -227,6 +253,7 @@ static void compute_factors(HostLevel& L, int nel, bool keep_jac) {
           L.tinv[3 * r + c][q] = ai[c][r];
         }
   }
+  });
 }
 
 static void make_basis(HostLevel& L, int n, int msvv, double csvv) {
@@ -243,9 +270,11 @@ static void grid_from_vertices(HostLevel& L, int nel, const double* vert) {
   const double xv[2] = {-1.0, 1.0};
   std::vector<double> J(L.n * 2);
   interp_matrix(L.n, L.x.data(), 2, xv, J.data());
-  for (int e = 0; e < nel; ++e)
-    for (int a = 0; a < 3; ++a)
-      tensor3(2, L.n, J.data(), vert + 24 * (size_t)e + 8 * a, L.grid[a].data() + e * L.nt);
+  parallel_elements(nel, [&](int e0, int e1) {
+    for (int e = e0; e < e1; ++e)
+      for (int a = 0; a < 3; ++a)
+        tensor3(2, L.n, J.data(), vert + 24 * (size_t)e + 8 * a, L.grid[a].data() + e * L.nt);
+  });
 }
 
 // Pairing of faces, edges and corners: the neighbour's matching entry is the
@@ -407,7 +436,8 @@ void dss_ec_table(const HostMesh& m, int n, std::vector<int>& tab) {
 void stiffness_diagonal(const HostLevel& L, int nel, double* out) {
   const int n = L.n;
   const double *D = L.D.data(), *w = L.w.data();
-  for (int e = 0; e < nel; ++e) {
+  parallel_elements(nel, [&](int e0, int e1) {
+  for (int e = e0; e < e1; ++e) {
     const size_t o = e * L.nt;
     for (int k = 0; k < n; ++k)
       for (int j = 0; j < n; ++j)
@@ -422,10 +452,11 @@ void stiffness_diagonal(const HostLevel& L, int nel, double* out) {
           out[o + (k * n + j) * n + i] = t;
         }
   }
+  });
 }
 
 ssg_status build_mesh(HostMesh& m, int n, int nel, const double* vert, const int* neigh,
-                      std::string& err) {
+                      std::string& err, unsigned opts) {
   if (n < 2 || n > 12 || (3 * n) / 2 > SSG_MAXN) {
     err = "order n must be in [2, 12]";
     return SSG_ERR_ARG;
@@ -446,9 +477,10 @@ ssg_status build_mesh(HostMesh& m, int n, int nel, const double* vert, const int
     alloc_level(m.lev[l], orders[l], nel, l == 0);
     make_basis(m.lev[l], orders[l], msvv, 0.0);
   }
+  const bool particles = !(opts & SSG_SETUP_NO_PARTICLES);
   grid_from_vertices(m.lev[0], nel, vert);
-  compute_factors(m.lev[0], nel, true);
-  m.has_particle_geom = true;
+  compute_factors(m.lev[0], nel, particles);
+  m.has_particle_geom = particles;
   for (int l = 1; l < m.nlev; ++l) {
     HostLevel &F = m.lev[l - 1], &L = m.lev[l];
     L.jf.resize((size_t)F.n * L.n);
@@ -456,11 +488,15 @@ ssg_status build_mesh(HostMesh& m, int n, int nel, const double* vert, const int
     // coarse grid = fine grid evaluated at the coarse nodes (src/precon.c:151-160)
     std::vector<double> Jc((size_t)L.n * F.n);
     interp_matrix(L.n, L.x.data(), F.n, F.x.data(), Jc.data());
-    for (int e = 0; e < nel; ++e)
-      for (int a = 0; a < 3; ++a)
-        tensor3(F.n, L.n, Jc.data(), F.grid[a].data() + e * F.nt, L.grid[a].data() + e * L.nt);
+    parallel_elements(nel, [&](int e0, int e1) {
+      for (int e = e0; e < e1; ++e)
+        for (int a = 0; a < 3; ++a)
+          tensor3(F.n, L.n, Jc.data(), F.grid[a].data() + e * F.nt,
+                  L.grid[a].data() + e * L.nt);
+    });
     compute_factors(L, nel, false);
   }
+  if (opts & SSG_SETUP_NO_DEALIAS) return SSG_OK;
   // dealiasing grid, m = 3n/2, from the vertices (src/main.c:53,71)
   const int mc = (3 * n) / 2;
   alloc_level(m.conv, mc, nel, true);

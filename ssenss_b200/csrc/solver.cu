@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 
@@ -35,6 +36,7 @@ struct Workspace {
   double* AP[10] = {};
   double* hist = nullptr;
   int hist_cap = 0;
+  double* scratch = nullptr;   // level-0 vector for set-up work (Helmholtz diagonal)
   std::vector<void*> blocks;
   // the V-cycle r -> z as one CUDA graph (its launch sequence is static:
   // smoother iterations past convergence exit on a device flag)
@@ -64,6 +66,7 @@ void invalidate_graphs(ssg_context* c) {
 static ssg_status wsalloc(ssg_context* c, Workspace* w, void** p, size_t bytes) {
   SSG_CUDA(c, cudaMalloc(p, bytes));
   w->blocks.push_back(*p);
+  c->dev_bytes += bytes;
   return SSG_OK;
 }
 
@@ -88,6 +91,7 @@ ssg_status ensure_workspace(ssg_context* c) {
     for (auto& p : w->AP) SSG_TRY(wsalloc(c, w, (void**)&p, np));
     w->hist_cap = 8192;
     SSG_TRY(wsalloc(c, w, (void**)&w->hist, w->hist_cap * sizeof(double)));
+    SSG_TRY(wsalloc(c, w, (void**)&w->scratch, np));
   }
   if (c->precision == SSG_PRECISION_MIXED && !c->ws->have32) {
     for (int l = 0; l < c->nlev; ++l)
@@ -97,6 +101,8 @@ ssg_status ensure_workspace(ssg_context* c) {
   }
   return SSG_OK;
 }
+
+double* workspace_scratch(ssg_context* c) { return c->ws ? c->ws->scratch : nullptr; }
 
 static inline double lambda_of(const ssg_context* c) {
   return (11.0 / 6.0) / (c->dt * c->visc);
@@ -117,6 +123,20 @@ ssg_status op_apply(ssg_context* c, int level, int var, bool fp32, const void* i
   if (global)
     SSG_CUDA(c, run_dss(c->stream, DSS_PLAIN, fp32, L.n, c->nel, loc, out, c->d_pairs, L.dss_ec,
                         helm ? L.mask : nullptr, nullptr, nullptr, nullptr));
+  return SSG_OK;
+}
+
+// cancellation flag and deadline of the running solve, checked where the
+// host already synchronises with the stream (a kernel in flight is never
+// interrupted)
+static ssg_status check_interrupt(ssg_context* c) {
+  if (c->cancel && *c->cancel) return fail(c, SSG_ERR_CANCELLED, "solve cancelled");
+  if (c->deadline > 0.0) {
+    const double now =
+        std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch())
+            .count();
+    if (now > c->deadline) return fail(c, SSG_ERR_TIMEOUT, "solve deadline expired");
+  }
   return SSG_OK;
 }
 
@@ -204,6 +224,7 @@ ssg_status cg_solve(ssg_context* c, int level, int var, bool fp32, void* f, void
     if (sync_each && (it % 8 == 7)) {
       double done;
       SSG_TRY(read_flag(c, fr + F_DONE, &done));
+      SSG_TRY(check_interrupt(c));
       if (done != 0.0) break;
     }
   }
@@ -319,7 +340,7 @@ static ssg_status vcycle_ws(ssg_context* c, double eps) {
     return mg_apply(c, w->r, w->z, eps);
   }
   if (!w->vcycle) {
-    const unsigned long long before = g_launches;
+    const unsigned long long before = t_launches;
     cudaGraph_t g = nullptr;
     if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
       cudaGetLastError();
@@ -328,8 +349,9 @@ static ssg_status vcycle_ws(ssg_context* c, double eps) {
     }
     const ssg_status st = mg_apply(c, w->r, w->z, eps);
     const cudaError_t ce = cudaStreamEndCapture(s, &g);
-    const unsigned long long captured = g_launches - before;
-    g_launches = before;
+    const unsigned long long captured = t_launches - before;
+    g_launches -= captured;   // recorded, not launched
+    t_launches = before;
     cudaGraphExec_t ex = nullptr;
     if (st != SSG_OK || ce != cudaSuccess || !g ||
         cudaGraphInstantiate(&ex, g, 0) != cudaSuccess) {
@@ -347,6 +369,7 @@ static ssg_status vcycle_ws(ssg_context* c, double eps) {
   }
   SSG_CUDA(c, cudaGraphLaunch(w->vcycle, s));
   g_launches += w->vcycle_kernels;
+  t_launches += w->vcycle_kernels;
   return SSG_OK;
 }
 
@@ -441,6 +464,7 @@ ssg_status fcg_solve(ssg_context* c, const double* f, double* u, double eps, int
     double done;
     SSG_TRY(read_flag(c, fr + F_DONE, &done));
     if (done != 0.0) break;
+    SSG_TRY(check_interrupt(c));
   }
   double h[F_SIZE];
   SSG_CUDA(c, cudaMemcpyAsync(c->h_pin, fr, F_SIZE * sizeof(double), cudaMemcpyDeviceToHost,

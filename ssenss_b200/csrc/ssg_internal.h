@@ -50,7 +50,7 @@ void svv_deriv_matrix(int n, const double* x, const double* w, int msvv, double 
                       double* S);
 void interp_matrix(int nto, const double* xto, int nfrom, const double* xfrom, double* J);
 ssg_status build_mesh(HostMesh& m, int n, int nel, const double* vertices,
-                      const int* neigh, std::string& err);
+                      const int* neigh, std::string& err, unsigned opts = 0);
 ssg_status build_pairs(HostMesh& m, std::string& err);
 void stiffness_diagonal(const HostLevel& L, int nel, double* out);
 void host_dss(const HostMesh& m, int n, double* u);
@@ -71,6 +71,8 @@ struct DevLevel {
   double* kdiag = nullptr;     // element-local stiffness diagonal
   double* dinv_p = nullptr;    // Poisson Jacobi inverse
   double* dinv_h = nullptr;    // Helmholtz Jacobi inverse (for lambda_h)
+  double* det = nullptr;       // det J (level 0: the Helmholtz diagonal's lambda term)
+  double* rho = nullptr;       // GLL weight products rho_ijk (n^3, level 0)
   uint8_t* mult = nullptr;     // multiplicity (1 + DSS contributions)
   int* dss_ec = nullptr;       // edge/corner DSS source table (dss_ec_table)
   double* mask = nullptr;      // Dirichlet mask (null without walls)
@@ -99,6 +101,10 @@ struct ssg_context {
   int precision = SSG_PRECISION_FP64;
   bool graphs = true;
   bool ready = false;
+  unsigned setup_opts = 0;      // SSG_SETUP_* flags of the next ssg_setup_mesh
+  size_t dev_bytes = 0;         // device memory this context holds
+  const volatile int* cancel = nullptr;   // nonzero: stop the running solve
+  double deadline = 0.0;        // steady-clock seconds; 0 = none
   int n = 0, nel = 0, nlev = 0;
   int orders[SSG_MAXLEV] = {0};
   ssg::HostMesh host;
@@ -159,6 +165,7 @@ enum Frame { FR_LEVEL0 = 0, FR_HELM = 8, FR_FCG = 9, FR_MISC = 10, FR_COUNT = 12
 
 // solver.cu
 ssg_status ensure_workspace(ssg_context* c);
+double* workspace_scratch(ssg_context* c);   // one level-0 FP64 vector
 ssg_status op_apply(ssg_context* c, int level, int var, bool fp32, const void* in,
                     void* out, bool global);
 ssg_status cg_solve(ssg_context* c, int level, int var, bool fp32, void* f, void* x,

@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <atomic>
 #include <cstddef>
 #include <cstdint>
 
@@ -64,7 +65,14 @@ struct PUpdateArgs {
   int first = 0;
 };
 
-extern unsigned long long g_launches;   // kernel launches of this library
+// kernel launches of this library: process-wide, and per host thread (the
+// per-thread count tells a stream capture how many launches it recorded)
+extern std::atomic<unsigned long long> g_launches;
+extern thread_local unsigned long long t_launches;
+inline void count_launch() {
+  ++g_launches;
+  ++t_launches;
+}
 
 int vec_blocks(size_t npts);
 int ax_epb(int n);
@@ -110,6 +118,10 @@ cudaError_t run_add_const(cudaStream_t s, bool fp32, size_t npts, void* x, const
 cudaError_t run_convert(cudaStream_t s, size_t npts, const void* in, bool in32, void* out,
                         bool out32);
 cudaError_t run_mul(cudaStream_t s, bool fp32, size_t npts, void* x, const double* y);
+// Helmholtz diagonal: out = kd + (lam rho[q mod nt]) det; then x = 1 / x
+cudaError_t run_helm_diag(cudaStream_t s, size_t npts, size_t nt, const double* kd,
+                          const double* rho, const double* det, double lam, double* out);
+cudaError_t run_recip(cudaStream_t s, size_t npts, double* x);
 cudaError_t run_reduce(cudaStream_t s, const double* part, int nblk, int nq, double* sums,
                        const ScalarOp& op);
 // whole CG-Jacobi solve of an n = 2 level in one cooperative launch (coarse.cu)

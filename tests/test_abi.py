@@ -48,3 +48,20 @@ def test_no_device_fails_cleanly():
     with pytest.raises(S.SsgError) as ei:
         S.Context(0)
     assert ei.value.status == 2
+
+
+def test_request_bytes_estimate_is_monotone():
+    """The serving loop's admission estimate (host only, no GPU)."""
+    import ssenss_b200 as S
+    assert S.request_bytes(8, 0) == 0
+    assert S.request_bytes(13, 27) == 0
+    prev = 0
+    for nel in (8, 27, 512, 4096):
+        b = S.request_bytes(8, nel, "fp64")
+        assert b > prev
+        prev = b
+        assert S.request_bytes(8, nel, "mixed") > b
+    for n in (6, 8, 10, 12):
+        assert S.request_bytes(n, 64) < S.request_bytes(n + 1 if n < 12 else 12, 64) or n == 12
+    # at least the level-0 operator factors and the 24 FCG vectors
+    assert S.request_bytes(8, 4096, "fp64") > 4096 * 512 * (48 + 24 * 8)

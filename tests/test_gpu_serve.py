@@ -1,0 +1,150 @@
+"""Serving loop: continuous admission of independent solves of different
+meshes, orders and Helmholtz coefficients on one GPU.
+
+Each request runs the same deterministic kernels whatever else is in flight,
+so a result in the mix is bitwise the result alone (stated tolerance: 0).
+Against the CPU oracle: Helmholtz (FP64 Jacobi CG) 1e-11, Poisson in mixed
+precision (FP32 V-cycle inside the FP64 FCG) 1e-8, both relative to the
+largest entry, with the absolute stop sqrt((r.r)_w) <= 1e-10.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+import ssenss_b200 as S
+from ssenss_b200.mesh import box_mesh, tgv_box
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def fourier_rhs(orc, n, seed):
+    """Weak, assembled right-hand side of 8 random periodic Fourier modes,
+    mean zero."""
+    rng = np.random.default_rng(seed)
+    X, Y, Z = orc.geometry(0, 7), orc.geometry(0, 8), orc.geometry(0, 9)
+    g = np.zeros_like(X)
+    for _ in range(8):
+        k = rng.integers(-2, 3, 3)
+        g += rng.standard_normal() * np.cos(k[0] * X + k[1] * Y + k[2] * Z + rng.uniform(0, 6.3))
+    g -= g.mean()
+    x, w = orc.gll(n)
+    rho = w[None, None, None, :] * w[None, None, :, None] * w[None, :, None, None]
+    return orc.dss(rho * orc.geometry(0, 6) * g)
+
+
+# (mesh shape, n, lambda): Poisson (lambda 0) and Helmholtz requests
+MIX = [((3, 3, 3), 8, 0.0), ((4, 3, 3), 6, 12.5), ((3, 4, 5), 8, 0.0),
+       ((3, 3, 3), 10, 60.0), ((5, 3, 3), 6, 0.0), ((3, 3, 4), 12, 0.0),
+       ((4, 4, 4), 8, 3.0), ((3, 3, 3), 8, 0.0), ((3, 5, 3), 10, 0.0),
+       ((4, 3, 3), 6, 99.0)]
+
+_inputs = {}
+
+
+def inputs(i):
+    if i not in _inputs:
+        shape, n, lam = MIX[i]
+        mesh = box_mesh(shape)
+        orc = O.Oracle(mesh, n, dt=(11.0 / (6.0 * lam)) if lam > 0 else 1.0, visc=1.0)
+        _inputs[i] = (mesh, n, lam, orc, fourier_rhs(orc, n, 100 + i))
+    return _inputs[i]
+
+
+def test_mix_equals_alone_and_oracle():
+    alone = []
+    srv = S.Server(0, hbm_budget=40e9, max_active=1)
+    try:
+        for i in range(len(MIX)):
+            mesh, n, lam, orc, f = inputs(i)
+            rid = srv.submit(mesh, n, f, lam=lam, precision="mixed")
+            u, st, info = srv.wait(rid)
+            assert st == "SSG_OK", (i, st)
+            alone.append(u)
+    finally:
+        srv.close()
+    srv = S.Server(0, hbm_budget=40e9, max_active=4)
+    try:
+        ids = [srv.submit(*inputs(i)[:2], inputs(i)[4], lam=inputs(i)[2], precision="mixed")
+               for i in range(len(MIX))]
+        mixed = [srv.wait(r) for r in ids]
+        st = srv.stats()
+    finally:
+        srv.close()
+    assert st["completed"] == len(MIX)
+    assert st["max_active_seen"] >= 2          # requests overlapped on the device
+    for i, (u, status, info) in enumerate(mixed):
+        assert status == "SSG_OK"
+        assert np.array_equal(u, alone[i]), i
+    # against the oracle
+    for i in (0, 1, 3):
+        mesh, n, lam, orc, f = inputs(i)
+        if lam > 0:
+            u_o, _ = orc.solve_helmholtz(O.X_VELOCITY, f, np.zeros_like(f))
+            assert rel(alone[i], u_o) < 1e-11
+        else:
+            u_o, _ = orc.solve_poisson(f, np.zeros_like(f))
+            assert rel(alone[i] - alone[i].mean(), u_o - u_o.mean()) < 1e-8
+
+
+def test_budget_admission_and_residency():
+    mesh, n, lam, orc, f = inputs(2)
+    need = S.request_bytes(n, mesh.nel, "mixed")
+    srv = S.Server(0, hbm_budget=int(1.5 * need), max_active=4)
+    try:
+        ids = [srv.submit(mesh, n, f, precision="mixed") for _ in range(4)]
+        outs = [srv.wait(r) for r in ids]
+        st = srv.stats()
+    finally:
+        srv.close()
+    assert all(o[1] == "SSG_OK" for o in outs)
+    for o in outs[1:]:
+        assert np.array_equal(o[0], outs[0][0])
+    assert st["hbm_peak"] <= st["hbm_budget"]
+    assert st["max_active_seen"] == 1          # one context fits the budget
+    assert st["mesh_hits"] == 3 and st["mesh_misses"] == 1
+
+
+def test_reject_cancel_deadline():
+    mesh, n, lam, orc, f = inputs(5)          # n = 12, the largest request
+    small = inputs(0)
+    srv = S.Server(0, hbm_budget=S.request_bytes(n, mesh.nel, "mixed") // 2, max_active=1)
+    try:
+        rid = srv.submit(mesh, n, f)
+        _, st, _ = srv.wait(rid)
+        assert st == "SSG_ERR_BUDGET"
+    finally:
+        srv.close()
+    srv = S.Server(0, hbm_budget=40e9, max_active=1)
+    try:
+        first = srv.submit(mesh, n, f)
+        queued = srv.submit(small[0], small[1], small[4])
+        late = srv.submit(small[0], small[1], small[4], deadline_ms=1e-3)
+        srv.cancel(queued)
+        assert srv.wait(first)[1] == "SSG_OK"
+        assert srv.wait(queued)[1] == "SSG_ERR_CANCELLED"
+        assert srv.wait(late)[1] == "SSG_ERR_TIMEOUT"
+        st = srv.stats()
+        assert st["cancelled"] == 1 and st["completed"] == 1
+    finally:
+        srv.close()
+
+
+def test_request_bytes_covers_the_context():
+    for i in (0, 3, 5):
+        mesh, n, lam, orc, f = inputs(i)
+        ctx = S.Context(0)
+        try:
+            ctx.set_setup_options(no_dealias=True, no_particles=True)
+            ctx.setup_mesh(mesh, n)
+            ctx.set_precision("mixed")
+            ctx.solve_poisson_cg(f, np.zeros_like(f), history=False)
+            used = ctx.memory_bytes()
+        finally:
+            ctx.close()
+        est = S.request_bytes(n, mesh.nel, "mixed")
+        assert used <= est, (i, used, est)
+        assert used >= 0.7 * est, (i, used, est)
