@@ -61,7 +61,14 @@ def parse():
                     help="keep the default launch shapes (skip ssg_autotune)")
     ap.add_argument("--no-graphs", action="store_true",
                     help="launch the V-cycle kernels directly (no CUDA graph)")
-    ap.add_argument("--sections", default="all", choices=["all", "fp64", "op"],
+    ap.add_argument("--serve-requests", type=int, default=300,
+                    help="requests of the serving stream (the full stream is 2000)")
+    ap.add_argument("--serve-rate", type=float, default=40.0,
+                    help="Poisson arrival rate of the serving stream (requests/s)")
+    ap.add_argument("--serve-slots", type=int, default=8,
+                    help="requests in flight at once in the serving loop")
+    ap.add_argument("--sections", default="all",
+                    choices=["all", "fp64", "mixed", "op", "serve"],
                     help="fp64: only the FP64 solves; op: only the operator "
                          "launches (for profiler captures)")
     return ap.parse_args()
@@ -251,6 +258,112 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------------------
+# serving stream (periodic boxes of E elements, orders N in {5,7,9,11})
+# ---------------------------------------------------------------------------
+def near_cube_shapes(lo=3, hi=16):
+    """Element counts a*b*c with lo <= a <= b <= c <= a + 1 (near-cubes)."""
+    out = {}
+    for a in range(lo, hi + 1):
+        for b in (a, a + 1):
+            for c in (b, b + 1):
+                if c <= a + 1:
+                    out.setdefault(a * b * c, (a, b, c))
+    return sorted(out.items())
+
+
+def serve_stream(nreq, rate, seed=2024):
+    """Requests (arrival s, shape, n, lambda, rhs seed): E log-uniform in
+    [8, 4096] rounded to the nearest near-cube product with all factors >= 3
+    (smaller counts carry the reference's periodic pairing defect), n
+    uniform in {6, 8, 10, 12}, Poisson (lambda = 0) or Helmholtz with lambda
+    uniform in (0, 100] with probability 1/2 each, Poisson arrivals."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    shapes = near_cube_shapes()
+    counts = np.array([e for e, _ in shapes], dtype=float)
+    t = 0.0
+    out = []
+    for i in range(nreq):
+        t += rng.exponential(1.0 / rate)
+        e = math.exp(rng.uniform(math.log(8.0), math.log(4096.0)))
+        shape = shapes[int(np.argmin(np.abs(np.log(counts) - math.log(e))))][1]
+        n = int(rng.choice([6, 8, 10, 12]))
+        lam = 0.0 if rng.uniform() < 0.5 else float(rng.uniform(1e-9, 100.0))
+        out.append((t, shape, n, lam, int(rng.integers(1 << 31))))
+    return out
+
+
+def run_serving(args, device):
+    """Open-loop serving stream through ssg_server (mixed precision, up to
+    --serve-slots in flight, 150 GB budget) beside the plain FP64
+    one-at-a-time path on the same stream; closed-loop throughput of both."""
+    import numpy as np
+    import ssenss_b200 as S
+    from ssenss_b200.mesh import box_mesh, periodic_box_fourier_rhs
+    stream = serve_stream(args.serve_requests, args.serve_rate)
+    meshes, keys, rhs = {}, {}, []
+    for (_, shape, n, lam, sd) in stream:
+        if shape not in meshes:
+            meshes[shape] = box_mesh(shape)
+        if (shape, n) not in keys:
+            keys[(shape, n)] = S.mesh_key(meshes[shape], n)
+        rhs.append(periodic_box_fourier_rhs(shape, n, sd))
+
+    def run(slots, precision, open_loop):
+        srv = S.Server(device, hbm_budget=150e9, max_active=slots)
+        ids = []
+        t0 = time.perf_counter()
+        for i, (ta, shape, n, lam, _) in enumerate(stream):
+            if open_loop:
+                dt = ta - (time.perf_counter() - t0)
+                if dt > 0:
+                    time.sleep(dt)
+            ids.append(srv.submit(meshes[shape], n, rhs[i], lam=lam, eps=EPS,
+                                  precision=precision, key=keys[(shape, n)]))
+        outs = [srv.wait(r) for r in ids]
+        wall = time.perf_counter() - t0
+        st = srv.stats()
+        srv.close()
+        bad = [o[1] for o in outs if o[1] != "SSG_OK"]
+        return outs, st, wall, bad
+
+    served, st_s, wall_s, bad_s = run(args.serve_slots, "mixed", True)
+    plain, st_p, wall_p, bad_p = run(1, "fp64", True)
+    _, st_sc, wall_sc, _ = run(args.serve_slots, "mixed", False)
+    _, st_pc, wall_pc, _ = run(1, "fp64", False)
+    diff = 0.0
+    for (u_s, _, _), (u_p, _, _), (_, _, _, lam, _) in zip(served, plain, stream):
+        if u_s is None or u_p is None:
+            continue
+        a, b = (u_s - u_s.mean(), u_p - u_p.mean()) if lam == 0 else (u_s, u_p)
+        diff = max(diff, float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)))
+    npois = sum(1 for r in stream if r[3] == 0.0)
+
+    def pick(st, wall):
+        return {"p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"],
+                "max_ms": st["max_ms"], "queue_p99_ms": st["queue_p99_ms"],
+                "solves_per_s": st["completed"] / wall, "completed": st["completed"],
+                "hbm_peak_gb": st["hbm_peak"] / 1e9, "mesh_hits": st["mesh_hits"],
+                "mesh_misses": st["mesh_misses"], "evictions": st["evictions"],
+                "max_in_flight": st["max_active_seen"]}
+
+    return {
+        "workload": (f"{len(stream)} requests ({npois} Poisson FCG+p-MG, "
+                     f"{len(stream) - npois} Helmholtz CG-Jacobi), periodic boxes E in "
+                     f"[27, 4096] near-cube, n in {{6,8,10,12}}, Poisson arrivals "
+                     f"{args.serve_rate}/s, stop sqrt((r.r)_w) <= {EPS}, HBM budget 150 GB"),
+        "served_mixed": pick(st_s, wall_s),
+        "plain_fp64_one_at_a_time": pick(st_p, wall_p),
+        "closed_loop_solves_per_s": {"served_mixed": st_sc["completed"] / wall_sc,
+                                     "plain_fp64_one_at_a_time":
+                                         st_pc["completed"] / wall_pc},
+        "failed": len(bad_s) + len(bad_p),
+        "max_rel_diff_mixed_vs_fp64": diff,
+        "slots": args.serve_slots,
+    }
+
+
+# ---------------------------------------------------------------------------
 # GPU arm
 # ---------------------------------------------------------------------------
 def run_ours(args):
@@ -304,6 +417,15 @@ def run_ours(args):
         _, info = ctx.solve_poisson_cg(f, u, eps=EPS, history=False)
         return info
 
+    if args.sections == "serve":
+        out = run_serving(args, local)
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "sections": "serve", "serving": out}))
+        ctx.close()
+        if pg is not None:
+            pg.destroy_process_group()
+        return 0
+
     if args.sections == "op":
         p = torch.randn(mesh.nel, n, n, n, dtype=torch.float64, device=dev)
         ap = torch.empty_like(p)
@@ -311,6 +433,19 @@ def run_ours(args):
             ctx.local_opeval(S.PRESSURE, p, ap)
             ctx.global_opeval(S.PRESSURE, p, ap)
         torch.cuda.synchronize()
+        ctx.close()
+        return 0
+
+    if args.sections == "mixed":
+        ctx.set_precision("mixed")
+        for _ in range(args.warmup):
+            solve_dev()
+        ms, infos = timed(solve_dev, args.steps, 0)
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "sections": "mixed",
+                              "ms_per_step": ms / args.steps,
+                              "iterations_per_solve":
+                                  sum(i["iterations"] for i in infos) / args.steps}))
         ctx.close()
         return 0
 
@@ -398,6 +533,8 @@ def run_ours(args):
 
     hms, hinfo = timed(helm, 5, 1)
 
+    serving = run_serving(args, local) if args.serve_requests > 0 else None
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -445,6 +582,7 @@ def run_ours(args):
                      "kernel": "k_ax<8,double> (level-0 Laplacian)",
                      "us_per_launch": op_ms * 1e3,
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"},
+        "serving": serving,
         "cpu_baseline": cpu,
         "gpu_launches": int(launches),
         "clocks": clocks,

@@ -288,6 +288,9 @@ typedef struct {
 	int max_active_seen, resident_contexts;
 } ssg_server_stats;
 
+/* GLL points and quadrature weights of n points on [-1, 1] (gll_basis,
+ * src/basis.c:31-177); host only. */
+ssg_status ssg_gll(int n, double *points, double *weights);
 /* Admission estimate of a request's resident context (bytes); host only. */
 size_t ssg_request_bytes(int n, int nel, int precision);
 ssg_status ssg_server_create(int device, size_t hbm_budget, int max_active,

@@ -100,6 +100,7 @@ SIGNATURES = [
     ("ssg_set_setup_options", C.c_int, [C.c_void_p, C.c_uint]),
     ("ssg_memory_info", C.c_int, [C.c_void_p, C.POINTER(C.c_size_t)]),
     ("ssg_request_bytes", C.c_size_t, [C.c_int, C.c_int, C.c_int]),
+    ("ssg_gll", C.c_int, [C.c_int, _dp, _dp]),
     ("ssg_server_create", C.c_int, [C.c_int, C.c_size_t, C.c_int, C.POINTER(C.c_void_p)]),
     ("ssg_server_submit", C.c_int, [C.c_void_p, C.POINTER(Request), _dp, _dp,
                                     C.POINTER(C.c_ulonglong)]),

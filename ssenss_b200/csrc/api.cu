@@ -458,6 +458,12 @@ ssg_status ssg_setup_mesh(ssg_context* c, int n, int nel, const double* vertices
   return upload_all(c);
 }
 
+ssg_status ssg_gll(int n, double* points, double* weights) {
+  if (n < 2 || n > SSG_MAXN || !points || !weights) return SSG_ERR_ARG;
+  gll_basis(n, points, weights);
+  return SSG_OK;
+}
+
 ssg_status ssg_set_setup_options(ssg_context* c, unsigned flags) {
   if (!c) return SSG_ERR_ARG;
   if (flags & ~(SSG_SETUP_NO_DEALIAS | SSG_SETUP_NO_PARTICLES))

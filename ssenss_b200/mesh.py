@@ -218,3 +218,49 @@ def factor3(e: int) -> tuple:
     if best is None:
         return (1, 1, e)
     return best[1]
+
+
+def gll(n: int):
+    """GLL points and weights of n points (the library's gll_basis)."""
+    from . import _lib
+    x, w = np.empty(n), np.empty(n)
+    st = _lib.load().ssg_gll(int(n), x.ctypes.data_as(_lib._dp), w.ctypes.data_as(_lib._dp))
+    if st != 0:
+        raise ValueError(f"no GLL basis of {n} points")
+    return x, w
+
+
+def periodic_box_fourier_rhs(shape, n: int, seed: int, modes: int = 8, kmax: int = 3,
+                             length: float = 2 * math.pi) -> np.ndarray:
+    """Weak, assembled right-hand side on the undeformed periodic box
+    box_mesh(shape) (element e = ex + nx (ey + ny ez), local i along x) of
+    `modes` seeded Fourier modes g = sum a cos(k.x + phi), a ~ N(0, 1),
+    k integer in [-kmax, kmax]^3 (k != 0, so mean zero): DSS(rho J g), the
+    local products summed over the copies of each global node."""
+    nx, ny, nz = shape
+    x, w = gll(n)
+    h = length / np.array([nx, ny, nz], dtype=float)
+    e = np.arange(nx * ny * nz)
+    ex, ey, ez = e % nx, (e // nx) % ny, e // (nx * ny)
+    m = n - 1
+    ar = np.arange(n)
+    gx = (ex[:, None, None, None] * m + ar[None, None, None, :]) % (nx * m)
+    gy = (ey[:, None, None, None] * m + ar[None, None, :, None]) % (ny * m)
+    gz = (ez[:, None, None, None] * m + ar[None, :, None, None]) % (nz * m)
+    gid = (gx + nx * m * (gy + ny * m * gz)).ravel()
+    X = (ex[:, None, None, None] + (1 + x[None, None, None, :]) / 2) * h[0]
+    Y = (ey[:, None, None, None] + (1 + x[None, None, :, None]) / 2) * h[1]
+    Z = (ez[:, None, None, None] + (1 + x[None, :, None, None]) / 2) * h[2]
+    rng = np.random.default_rng(seed)
+    g = np.zeros((nx * ny * nz, n, n, n))
+    for _ in range(modes):
+        k = rng.integers(-kmax, kmax + 1, 3)
+        if not k.any():
+            k[0] = 1
+        g += rng.standard_normal() * np.cos(k[0] * X + k[1] * Y + k[2] * Z +
+                                            rng.uniform(0, 2 * math.pi))
+    rho = w[None, None, None, :] * w[None, None, :, None] * w[None, :, None, None]
+    loc = (rho * (h[0] * h[1] * h[2] / 8.0) * g).ravel()
+    tot = np.bincount(gid, weights=loc, minlength=int(gid.max()) + 1)
+    return tot[gid].reshape(nx * ny * nz, n, n, n)
+

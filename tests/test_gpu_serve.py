@@ -12,28 +12,13 @@ import pytest
 
 import oracle as O
 import ssenss_b200 as S
-from ssenss_b200.mesh import box_mesh, tgv_box
+from ssenss_b200.mesh import box_mesh, periodic_box_fourier_rhs
 
 pytestmark = pytest.mark.gpu
 
 
 def rel(a, b):
     return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
-
-
-def fourier_rhs(orc, n, seed):
-    """Weak, assembled right-hand side of 8 random periodic Fourier modes,
-    mean zero."""
-    rng = np.random.default_rng(seed)
-    X, Y, Z = orc.geometry(0, 7), orc.geometry(0, 8), orc.geometry(0, 9)
-    g = np.zeros_like(X)
-    for _ in range(8):
-        k = rng.integers(-2, 3, 3)
-        g += rng.standard_normal() * np.cos(k[0] * X + k[1] * Y + k[2] * Z + rng.uniform(0, 6.3))
-    g -= g.mean()
-    x, w = orc.gll(n)
-    rho = w[None, None, None, :] * w[None, None, :, None] * w[None, :, None, None]
-    return orc.dss(rho * orc.geometry(0, 6) * g)
 
 
 # (mesh shape, n, lambda): Poisson (lambda 0) and Helmholtz requests
@@ -46,12 +31,17 @@ _inputs = {}
 
 
 def inputs(i):
+    """mesh, n, lambda, right-hand side (8 seeded Fourier modes, weak and
+    assembled) of request i"""
     if i not in _inputs:
         shape, n, lam = MIX[i]
-        mesh = box_mesh(shape)
-        orc = O.Oracle(mesh, n, dt=(11.0 / (6.0 * lam)) if lam > 0 else 1.0, visc=1.0)
-        _inputs[i] = (mesh, n, lam, orc, fourier_rhs(orc, n, 100 + i))
+        _inputs[i] = (box_mesh(shape), n, lam, periodic_box_fourier_rhs(shape, n, 100 + i))
     return _inputs[i]
+
+
+def oracle_for(i):
+    mesh, n, lam, f = inputs(i)
+    return O.Oracle(mesh, n, dt=(11.0 / (6.0 * lam)) if lam > 0 else 1.0, visc=1.0)
 
 
 def test_mix_equals_alone_and_oracle():
@@ -59,7 +49,7 @@ def test_mix_equals_alone_and_oracle():
     srv = S.Server(0, hbm_budget=40e9, max_active=1)
     try:
         for i in range(len(MIX)):
-            mesh, n, lam, orc, f = inputs(i)
+            mesh, n, lam, f = inputs(i)
             rid = srv.submit(mesh, n, f, lam=lam, precision="mixed")
             u, st, info = srv.wait(rid)
             assert st == "SSG_OK", (i, st)
@@ -68,7 +58,7 @@ def test_mix_equals_alone_and_oracle():
         srv.close()
     srv = S.Server(0, hbm_budget=40e9, max_active=4)
     try:
-        ids = [srv.submit(*inputs(i)[:2], inputs(i)[4], lam=inputs(i)[2], precision="mixed")
+        ids = [srv.submit(*inputs(i)[:2], inputs(i)[3], lam=inputs(i)[2], precision="mixed")
                for i in range(len(MIX))]
         mixed = [srv.wait(r) for r in ids]
         st = srv.stats()
@@ -81,7 +71,8 @@ def test_mix_equals_alone_and_oracle():
         assert np.array_equal(u, alone[i]), i
     # against the oracle
     for i in (0, 1, 3):
-        mesh, n, lam, orc, f = inputs(i)
+        mesh, n, lam, f = inputs(i)
+        orc = oracle_for(i)
         if lam > 0:
             u_o, _ = orc.solve_helmholtz(O.X_VELOCITY, f, np.zeros_like(f))
             assert rel(alone[i], u_o) < 1e-11
@@ -91,7 +82,7 @@ def test_mix_equals_alone_and_oracle():
 
 
 def test_budget_admission_and_residency():
-    mesh, n, lam, orc, f = inputs(2)
+    mesh, n, lam, f = inputs(2)
     need = S.request_bytes(n, mesh.nel, "mixed")
     srv = S.Server(0, hbm_budget=int(1.5 * need), max_active=4)
     try:
@@ -109,7 +100,7 @@ def test_budget_admission_and_residency():
 
 
 def test_reject_cancel_deadline():
-    mesh, n, lam, orc, f = inputs(5)          # n = 12, the largest request
+    mesh, n, lam, f = inputs(5)               # n = 12, the largest request
     small = inputs(0)
     srv = S.Server(0, hbm_budget=S.request_bytes(n, mesh.nel, "mixed") // 2, max_active=1)
     try:
@@ -121,8 +112,8 @@ def test_reject_cancel_deadline():
     srv = S.Server(0, hbm_budget=40e9, max_active=1)
     try:
         first = srv.submit(mesh, n, f)
-        queued = srv.submit(small[0], small[1], small[4])
-        late = srv.submit(small[0], small[1], small[4], deadline_ms=1e-3)
+        queued = srv.submit(small[0], small[1], small[3])
+        late = srv.submit(small[0], small[1], small[3], deadline_ms=1e-3)
         srv.cancel(queued)
         assert srv.wait(first)[1] == "SSG_OK"
         assert srv.wait(queued)[1] == "SSG_ERR_CANCELLED"
@@ -135,7 +126,7 @@ def test_reject_cancel_deadline():
 
 def test_request_bytes_covers_the_context():
     for i in (0, 3, 5):
-        mesh, n, lam, orc, f = inputs(i)
+        mesh, n, lam, f = inputs(i)
         ctx = S.Context(0)
         try:
             ctx.set_setup_options(no_dealias=True, no_particles=True)
