@@ -63,7 +63,7 @@ def parse():
                     help="launch the V-cycle kernels directly (no CUDA graph)")
     ap.add_argument("--serve-requests", type=int, default=300,
                     help="requests of the serving stream (the full stream is 2000)")
-    ap.add_argument("--serve-rate", type=float, default=40.0,
+    ap.add_argument("--serve-rate", type=float, default=20.0,
                     help="Poisson arrival rate of the serving stream (requests/s)")
     ap.add_argument("--serve-slots", type=int, default=8,
                     help="requests in flight at once in the serving loop")
@@ -327,13 +327,21 @@ def run_serving(args, device):
         bad = [o[1] for o in outs if o[1] != "SSG_OK"]
         return outs, st, wall, bad
 
+    # warm-up: module loading and first-use attributes outside the runs
+    wsrv = S.Server(device, hbm_budget=150e9, max_active=args.serve_slots)
+    wid = [wsrv.submit(meshes[shape], n, rhs[i], lam=lam, eps=EPS, precision=p,
+                       key=keys[(shape, n)])
+           for i, (_, shape, n, lam, _) in enumerate(stream[:16]) for p in ("mixed", "fp64")]
+    for r in wid:
+        wsrv.wait(r)
+    wsrv.close()
     served, st_s, wall_s, bad_s = run(args.serve_slots, "mixed", True)
     plain, st_p, wall_p, bad_p = run(1, "fp64", True)
     _, st_sc, wall_sc, _ = run(args.serve_slots, "mixed", False)
     _, st_pc, wall_pc, _ = run(1, "fp64", False)
     diff = 0.0
-    for (u_s, _, _), (u_p, _, _), (_, _, _, lam, _) in zip(served, plain, stream):
-        if u_s is None or u_p is None:
+    for (u_s, st1, _), (u_p, st2, _), (_, _, _, lam, _) in zip(served, plain, stream):
+        if u_s is None or u_p is None or st1 != "SSG_OK" or st2 != "SSG_OK":
             continue
         a, b = (u_s - u_s.mean(), u_p - u_p.mean()) if lam == 0 else (u_s, u_p)
         diff = max(diff, float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)))
@@ -358,6 +366,7 @@ def run_serving(args, device):
                                      "plain_fp64_one_at_a_time":
                                          st_pc["completed"] / wall_pc},
         "failed": len(bad_s) + len(bad_p),
+        "failed_statuses": sorted(set(bad_s + bad_p)),
         "max_rel_diff_mixed_vs_fp64": diff,
         "slots": args.serve_slots,
     }

@@ -266,7 +266,9 @@ static ssg_status upload_all(ssg_context* c) {
   // three-component fields)
   c->stage_cap = H.has_conv ? 3 * np0 : np0;
   for (auto& s : c->d_stage) SSG_TRY(dalloc(c, &s, c->stage_cap));
-  SSG_CUDA(c, cudaDeviceSynchronize());
+  // (uploads are synchronous copies; no device-wide synchronisation, which
+  // would collide with another thread's stream capture)
+  SSG_CUDA(c, cudaStreamSynchronize(c->stream));
   c->ready = true;
   return SSG_OK;
 }

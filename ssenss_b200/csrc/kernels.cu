@@ -495,6 +495,24 @@ __global__ void __launch_bounds__(256) k_recip(size_t npts, double* __restrict__
 // CG step after ap is known (src/solver.c:66-71):
 //   x += alpha p; r -= alpha ap; z = dinv .* r
 // partials: (r w).z, (r w).r, w.z, w.r
+// Grid-stride loops with four points in flight per thread: the loads of
+// points q, q + S, q + 2S, q + 3S (S = grid stride) are issued before any of
+// them is used, then the tail runs one point at a time.  Each thread's
+// partial sums follow that fixed visiting order (deterministic).
+#define SSG_U4_LOOP(q, n, LOAD, USE)                                            \
+  {                                                                            \
+    const size_t S_ = (size_t)gridDim.x * blockDim.x;                          \
+    size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x;                  \
+    for (; q + 3 * S_ < (n); q += 4 * S_) {                                    \
+      _Pragma("unroll") for (int u_ = 0; u_ < 4; ++u_) { LOAD(u_, q + u_ * S_) } \
+      _Pragma("unroll") for (int u_ = 0; u_ < 4; ++u_) { USE(u_, q + u_ * S_) }  \
+    }                                                                          \
+    for (; q < (n); q += S_) {                                                 \
+      LOAD(0, q)                                                               \
+      USE(0, q)                                                                \
+    }                                                                          \
+  }
+
 template <typename T>
 __global__ void __launch_bounds__(256) k_cg_update(size_t npts,
                                                    const double* __restrict__ alpha_p,
@@ -510,19 +528,27 @@ __global__ void __launch_bounds__(256) k_cg_update(size_t npts,
   __shared__ double sred[4 * 32];
   const double alpha = *alpha_p;
   double v[4] = {0.0, 0.0, 0.0, 0.0};
-  SSG_GRID_LOOP(q, npts) {
-    x[q] = (T)((double)x[q] + alpha * (double)p[q]);
-    const T rq = (T)((double)r[q] + -alpha * (double)ap[q]);
-    r[q] = rq;
-    const T zq = (T)((double)rq * (double)dinv[q]);
-    z[q] = zq;
-    const double w = inv_count(mult[q]);
-    const double rw = (double)rq * w;
-    v[0] += rw * (double)zq;
-    v[1] += rw * (double)rq;
-    v[2] += w * (double)zq;
-    v[3] += rw;
+  T xv[4], pv[4], rv[4], av[4], dv[4];
+  unsigned mv[4];
+#define SSG_LD(u, i) xv[u] = x[i]; pv[u] = p[i]; rv[u] = r[i]; av[u] = ap[i]; \
+  dv[u] = dinv[i]; mv[u] = mult[i];
+#define SSG_USE(u, i)                                                         \
+  {                                                                           \
+    x[i] = (T)((double)xv[u] + alpha * (double)pv[u]);                        \
+    const T rq = (T)((double)rv[u] + -alpha * (double)av[u]);                 \
+    r[i] = rq;                                                                \
+    const T zq = (T)((double)rq * (double)dv[u]);                             \
+    z[i] = zq;                                                                \
+    const double w = inv_count(mv[u]);                                        \
+    const double rw = (double)rq * w;                                         \
+    v[0] += rw * (double)zq;                                                  \
+    v[1] += rw * (double)rq;                                                  \
+    v[2] += w * (double)zq;                                                   \
+    v[3] += rw;                                                               \
   }
+  SSG_U4_LOOP(q, npts, SSG_LD, SSG_USE)
+#undef SSG_LD
+#undef SSG_USE
   block_reduce<4>(v, sred);
   finish<4>(v, part, op, sred);
 }
@@ -536,11 +562,18 @@ __global__ void __launch_bounds__(256) k_jacobi(size_t npts, const T* __restrict
                                                 ScalarOp op) {
   __shared__ double sred[32];
   double v[1] = {0.0};
-  SSG_GRID_LOOP(q, npts) {
-    const T zq = (T)((double)r[q] * (double)dinv[q]);
-    z[q] = zq;
-    v[0] += (double)zq * inv_count(mult[q]);
+  T rv[4], dv[4];
+  unsigned mv[4];
+#define SSG_LD(u, i) rv[u] = r[i]; dv[u] = dinv[i]; mv[u] = mult[i];
+#define SSG_USE(u, i)                                   \
+  {                                                     \
+    const T zq = (T)((double)rv[u] * (double)dv[u]);    \
+    z[i] = zq;                                          \
+    v[0] += (double)zq * inv_count(mv[u]);              \
   }
+  SSG_U4_LOOP(q, npts, SSG_LD, SSG_USE)
+#undef SSG_LD
+#undef SSG_USE
   block_reduce<1>(v, sred);
   finish<1>(v, part, op, sred);
 }
@@ -570,7 +603,13 @@ __global__ void __launch_bounds__(256) k_wsum(size_t npts, const T* __restrict__
                                               double* __restrict__ part, ScalarOp op) {
   __shared__ double sred[32];
   double v[1] = {0.0};
-  SSG_GRID_LOOP(q, npts) v[0] += (double)x[q] * inv_count(mult[q]);
+  T xv[4];
+  unsigned mv[4];
+#define SSG_LD(u, i) xv[u] = x[i]; mv[u] = mult[i];
+#define SSG_USE(u, i) v[0] += (double)xv[u] * inv_count(mv[u]);
+  SSG_U4_LOOP(q, npts, SSG_LD, SSG_USE)
+#undef SSG_LD
+#undef SSG_USE
   block_reduce<1>(v, sred);
   finish<1>(v, part, op, sred);
 }
@@ -597,12 +636,19 @@ __global__ void __launch_bounds__(256) k_fcg_update(size_t npts, const double* _
   __shared__ double sred[32];
   const double alpha = *alpha_p;
   double v[1] = {0.0};
-  SSG_GRID_LOOP(q, npts) {
-    u[q] = u[q] + alpha * p[q];
-    const double rq = r[q] + -alpha * ap[q];
-    r[q] = rq;
-    v[0] += (rq * inv_count(mult[q])) * rq;
+  double uv[4], pv[4], rv[4], av[4];
+  unsigned mv[4];
+#define SSG_LD(k, i) uv[k] = u[i]; pv[k] = p[i]; rv[k] = r[i]; av[k] = ap[i]; mv[k] = mult[i];
+#define SSG_USE(k, i)                                  \
+  {                                                    \
+    u[i] = uv[k] + alpha * pv[k];                      \
+    const double rq = rv[k] + -alpha * av[k];          \
+    r[i] = rq;                                         \
+    v[0] += (rq * inv_count(mv[k])) * rq;              \
   }
+  SSG_U4_LOOP(q, npts, SSG_LD, SSG_USE)
+#undef SSG_LD
+#undef SSG_USE
   block_reduce<1>(v, sred);
   finish<1>(v, part, op, sred);
 }
