@@ -251,7 +251,8 @@ ssg_status ssg_convection_operator(ssg_context *ctx, const double *u,
  * Results are unchanged: every shape computes the same sums in the same
  * order. */
 ssg_status ssg_autotune(ssg_context *ctx, int reps);
-/* Launch shapes in use for order n (tuned or default). */
+/* Launch shapes in use for order n (tuned or default); elements per block
+ * 0 = the FP64 tensor-core operator (n = 8: one warp per element). */
 ssg_status ssg_tuning(int n, int *ax_elements_per_block,
 		int *dss_blocks_per_sm, int *vector_blocks_per_sm);
 

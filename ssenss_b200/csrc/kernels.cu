@@ -146,14 +146,6 @@ __device__ __forceinline__ void finish(const double (&v)[NQ], double* __restrict
 //   p = ((beta p + (z - c)) .* mask)   (first: p = (z - c) .* mask)
 // (src/solver.c:59-60,75-77 with subtract_nullspace folded in)
 // ---------------------------------------------------------------------------
-struct PUpdate {
-  const void* z = nullptr;        // T*
-  const double* beta = nullptr;
-  const double* c = nullptr;      // nullspace constant (pressure) or null
-  const double* mask = nullptr;
-  const double* stop = nullptr;   // solver's stop flag: skip when set
-  int first = 0;
-};
 
 // padded row stride of the shared 1-D matrices: even (16-byte aligned rows
 // for double2 loads) and chosen so the rows fall on distinct bank groups
@@ -328,20 +320,21 @@ __global__ void __launch_bounds__(256) k_dss(int nel, int epb, const T* __restri
   constexpr int ID = I > 0 ? I : 1, II = ID * ID;   // divisors (N = 2 has no
                                                     // face or interior nodes)
   if (stop && *stop != 0.0) return;   // uniform over the block
-  __shared__ int2 sp[64 * 26];
   __shared__ short sface[6 * NN];     // node of face f at face position p
   __shared__ double sred[2 * 32];
   for (int q = threadIdx.x; q < 6 * NN; q += blockDim.x)
     sface[q] = (short)face_node(N, q / NN, (q % NN) / N, q % N);
+  __syncthreads();
+  (void)epb;
   double s0 = 0.0, s1 = 0.0;
-  for (int e0 = blockIdx.x * epb; e0 < nel; e0 += gridDim.x * epb) {
-    const int ne = min(epb, nel - e0);
-    __syncthreads();
-    for (int q = threadIdx.x; q < ne * 26; q += blockDim.x) sp[q] = pairs[(size_t)e0 * 26 + q];
-    __syncthreads();
-    for (int q = threadIdx.x; q < ne * NT; q += blockDim.x) {
-      const int z = q / NT, t = q - z * NT;
-      const size_t eb = (size_t)(e0 + z) * NT;
+  // one node task per thread, grid-stride over all elements' tasks; no
+  // block-wide staging, so no barrier inside the loop
+  const size_t ntask = (size_t)nel * NT;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < ntask;
+       q += (size_t)gridDim.x * blockDim.x) {
+    {
+      const int e = (int)(q / NT), t = (int)(q - (size_t)e * NT);
+      const size_t eb = (size_t)e * NT;
       int loc, cnt = 0;
       double acc;
       if (t < F) {
@@ -349,7 +342,7 @@ __global__ void __launch_bounds__(256) k_dss(int nel, int epb, const T* __restri
         const int f = t / II, r = t - f * II;
         const int pos = (1 + r / ID) * N + 1 + r % ID;
         loc = sface[f * NN + pos];
-        const int2 p = sp[z * 26 + f];
+        const int2 p = __ldg(pairs + (size_t)e * 26 + f);
         acc = (double)in[eb + loc];
         if (mask) acc = acc * mask[eb + loc];
         if (p.x >= 0) {
@@ -365,7 +358,7 @@ __global__ void __launch_bounds__(256) k_dss(int nel, int epb, const T* __restri
         loc = class_ordered_node<N>(t);
         const int c = t - F;
         constexpr int ECI = 12 * I;
-        const int4* rec = ec + (size_t)(e0 + z) * (ECI + 16) +
+        const int4* rec = ec + (size_t)e * (ECI + 16) +
                           (c < ECI ? c : ECI + 2 * (c - ECI));
         const int4 a = __ldg(rec);
         int4 b = make_int4(-1, -1, -1, -1);
@@ -705,6 +698,7 @@ thread_local unsigned long long t_launches = 0;
 int g_tune_ax_epb[SSG_MAXN + 1] = {0};
 int g_tune_dss_bps[SSG_MAXN + 1] = {0};
 int g_tune_vec_bps = 0;
+int g_tune_ax_kind[SSG_MAXN + 1] = {0};
 
 int ax_epb_max(int n) {
   // elements per block: up to 256 threads, <= 96 KB of FP64 shared memory
@@ -714,9 +708,11 @@ int ax_epb_max(int n) {
   return epb;
 }
 
+// grid of the vector kernels: four points per thread in one pass where the
+// cap (bps blocks per SM) allows; beyond it the kernels loop grid-stride
 int vec_blocks(size_t npts) {
-  size_t b = (npts + 255) / 256;
-  const size_t cap = (size_t)148 * (g_tune_vec_bps > 0 ? g_tune_vec_bps : 8);
+  size_t b = (npts + 1023) / 1024;
+  const size_t cap = (size_t)148 * (g_tune_vec_bps > 0 ? g_tune_vec_bps : 32);
   return (int)(b < cap ? (b ? b : 1) : cap);
 }
 
@@ -763,7 +759,6 @@ cudaError_t run_ax(cudaStream_t s, int n, int nel, int epb, bool helm, bool fp32
                    const void* in, void* out, const void* gf, size_t npts,
                    const double* bj, const double* D, const double* S, double lambda,
                    const PUpdateArgs* pua) {
-  if (epb <= 0) epb = ax_epb(n);
   PUpdate pu;
   const bool fuse = pua != nullptr;
   if (fuse) {
@@ -774,6 +769,14 @@ cudaError_t run_ax(cudaStream_t s, int n, int nel, int epb, bool helm, bool fp32
     pu.stop = pua->stop;
     pu.first = pua->first;
   }
+  // n = 8: the FP64 tensor-core kernel (FP32 or FP64 storage) unless the
+  // autotuner (or the caller, epb > 0) picked the shared-memory one
+  const bool dmma = n == 8 &&
+                    (epb == AX_DMMA || (epb == 0 && g_tune_ax_kind[8] != AX_KIND_CLASSIC));
+  if (dmma)
+    return run_ax8_dmma(s, nel, helm, fp32, (void*)in, out, gf, npts, bj, D, S, lambda,
+                        fuse ? &pu : nullptr);
+  if (epb <= 0) epb = ax_epb(n);
   if (fp32) {
     if (helm) return cudaErrorInvalidValue;
     if (fuse)
@@ -803,11 +806,14 @@ int dss_epb(int n) {
   return epb;
 }
 
+// one 256-thread block per 256 node tasks, capped at bps blocks per SM
+// (the kernel walks the rest grid-stride)
 int dss_grid(int n, int nel) {
-  const int epb = dss_epb(n);
-  const int g = (nel + epb - 1) / epb;
-  const int bps = (n >= 0 && n <= SSG_MAXN && g_tune_dss_bps[n] > 0) ? g_tune_dss_bps[n] : 4;
-  return g < 148 * bps ? g : 148 * bps;
+  const size_t tasks = (size_t)nel * n * n * n;
+  const size_t g = (tasks + 255) / 256;
+  const int bps = (n >= 0 && n <= SSG_MAXN && g_tune_dss_bps[n] > 0) ? g_tune_dss_bps[n] : 8;
+  const size_t cap = (size_t)148 * bps;
+  return (int)(g < cap ? (g ? g : 1) : cap);
 }
 
 template <int N, typename T>

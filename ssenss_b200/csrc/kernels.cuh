@@ -147,6 +147,16 @@ __device__ __forceinline__ int class_ordered_node(int t) {
   }
 }
 
+// CG direction update fused into the operator (device copy of PUpdateArgs)
+struct PUpdate {
+  const void* z = nullptr;        // T*
+  const double* beta = nullptr;
+  const double* c = nullptr;      // nullspace constant (pressure) or null
+  const double* mask = nullptr;
+  const double* stop = nullptr;   // solver's stop flag: skip when set
+  int first = 0;
+};
+
 // ---------------------------------------------------------------------------
 // block reduction of NQ doubles over a 1-D block whose size is a multiple of
 // 32; fixed shuffle pattern, so the result is deterministic.  Valid in

@@ -82,6 +82,15 @@ int dss_grid(int n, int nel);
 extern int g_tune_ax_epb[];
 extern int g_tune_dss_bps[];
 extern int g_tune_vec_bps;
+// operator kernel kind per order: default, the shared-memory kernel, or the
+// FP64 tensor-core kernel (n = 8 only); run_ax's epb = AX_DMMA forces the
+// latter
+enum { AX_KIND_DEFAULT = 0, AX_KIND_CLASSIC = 1, AX_KIND_DMMA = 2, AX_DMMA = -1 };
+extern int g_tune_ax_kind[];
+namespace dev { struct PUpdate; }
+cudaError_t run_ax8_dmma(cudaStream_t s, int nel, bool helm, bool fp32, void* u, void* au,
+                         const void* gf, size_t npts, const double* bj, const double* D,
+                         const double* S, double lambda, const dev::PUpdate* pu);
 
 cudaError_t run_ax(cudaStream_t s, int n, int nel, int epb, bool helm, bool fp32,
                    const void* in, void* out, const void* gf, size_t npts,

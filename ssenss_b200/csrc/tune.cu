@@ -2,8 +2,9 @@
 //
 // The element kernels have one free shape parameter per order n and the
 // vector kernels one overall:
-//   * elements per block of the operator (k_ax): 1, 2, 4, ... up to the
-//     256-thread / 96 KB limit of ax_epb_max(n);
+//   * the operator kernel: elements per block of the shared-memory kernel
+//     (k_ax: 1, 2, 4, ... up to the 256-thread / 96 KB limit of
+//     ax_epb_max(n)) and, for n = 8, the FP64 tensor-core kernel k_ax8_dmma;
 //   * blocks per SM of the persistent DSS grid: 1 .. 16;
 //   * blocks per SM of the grid-stride vector kernels: 2 .. 32.
 // ssg_autotune times every candidate on the context's own mesh and levels
@@ -66,6 +67,18 @@ static ssg_status tune_level(ssg_context* c, int level, double* a, double* b, do
       }
     }
     g_tune_ax_epb[n] = best_epb;
+    g_tune_ax_kind[n] = AX_KIND_CLASSIC;
+    if (n == 8) {
+      // the FP64 tensor-core kernel of this order
+      SSG_CUDA(c, run_ax(c->stream, n, c->nel, AX_DMMA, false, false, a, b, L.gf, L.npts,
+                         nullptr, L.D, L.D, 0.0, nullptr));
+      float t = 0.f;
+      SSG_TRY(time_launches(c, reps, [&] {
+        return run_ax(c->stream, n, c->nel, AX_DMMA, false, false, a, b, L.gf, L.npts,
+                      nullptr, L.D, L.D, 0.0, nullptr);
+      }, &t));
+      if (t < best) g_tune_ax_kind[n] = AX_KIND_DMMA;
+    }
   }
   // DSS: blocks per SM of the persistent grid
   {
@@ -150,9 +163,11 @@ ssg_status ssg_autotune(ssg_context* c, int reps) {
 ssg_status ssg_tuning(int n, int* ax_elements_per_block, int* dss_blocks_per_sm,
                       int* vector_blocks_per_sm) {
   if (n < 2 || n > SSG_MAXN) return SSG_ERR_ARG;
-  if (ax_elements_per_block) *ax_elements_per_block = ax_epb(n);
-  if (dss_blocks_per_sm) *dss_blocks_per_sm = g_tune_dss_bps[n] > 0 ? g_tune_dss_bps[n] : 4;
-  if (vector_blocks_per_sm) *vector_blocks_per_sm = g_tune_vec_bps > 0 ? g_tune_vec_bps : 8;
+  // 0: the FP64 tensor-core operator (one warp per element)
+  const bool dmma = n == 8 && g_tune_ax_kind[8] != AX_KIND_CLASSIC;
+  if (ax_elements_per_block) *ax_elements_per_block = dmma ? 0 : ax_epb(n);
+  if (dss_blocks_per_sm) *dss_blocks_per_sm = g_tune_dss_bps[n] > 0 ? g_tune_dss_bps[n] : 8;
+  if (vector_blocks_per_sm) *vector_blocks_per_sm = g_tune_vec_bps > 0 ? g_tune_vec_bps : 32;
   return SSG_OK;
 }
 
