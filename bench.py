@@ -57,6 +57,8 @@ def parse():
     ap.add_argument("--ne", type=int, default=NE)
     ap.add_argument("--n", type=int, default=NORD)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the channel (C3), particle (C4) and convection sections")
     ap.add_argument("--no-tune", action="store_true",
                     help="keep the default launch shapes (skip ssg_autotune)")
     ap.add_argument("--no-graphs", action="store_true",
@@ -68,7 +70,7 @@ def parse():
     ap.add_argument("--serve-slots", type=int, default=8,
                     help="requests in flight at once in the serving loop")
     ap.add_argument("--sections", default="all",
-                    choices=["all", "fp64", "mixed", "op", "serve"],
+                    choices=["all", "fp64", "mixed", "op", "serve", "extra"],
                     help="fp64: only the FP64 solves; op: only the operator "
                          "launches (for profiler captures)")
     return ap.parse_args()
@@ -373,6 +375,167 @@ def run_serving(args, device):
 
 
 # ---------------------------------------------------------------------------
+# other configurations: channel Poisson (C3), particles (C4), convection
+# ---------------------------------------------------------------------------
+def cuda_timed(lib_stream, fn, k, w=1):
+    """Device time (ms) of k calls of fn on the library's stream."""
+    import torch
+    for _ in range(w):
+        fn()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(lib_stream)
+    out = [fn() for _ in range(k)]
+    e1.record(lib_stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1), out
+
+
+def run_channel(args, device):
+    """C3: deformed channel 32 x 16 x 16, N = 9 (n = 10, 8.2M local points),
+    Poisson solve of 8 seeded Fourier modes (Neumann-compatible in y, mean
+    zero), FP64 vs mixed, autotuned shapes, graph-captured V-cycle."""
+    import numpy as np
+    import torch
+    import ssenss_b200 as S
+    from ssenss_b200.mesh import channel_mesh
+    mesh = channel_mesh((32, 16, 16))
+    n = 10
+    ctx = S.Context(device)
+    ctx.set_setup_options(no_dealias=True, no_particles=True)
+    t0 = time.perf_counter()
+    ctx.setup_mesh(mesh, n)
+    setup_s = time.perf_counter() - t0
+    tuned = ctx.autotune()
+    X, Y, Z = (ctx.level_data(0, 12 + a) for a in range(3))
+    rng = np.random.default_rng(20241203)
+    g = np.zeros_like(X)
+    for _ in range(8):
+        kx, kz = rng.integers(1, 4) / 2.0, rng.integers(-3, 4)
+        ky = rng.integers(0, 3)
+        g += rng.standard_normal() * np.cos(kx * X + kz * Z + rng.uniform(0, 6.28)) * \
+            np.cos(math.pi * ky * (Y + 1) / 2)
+    bj = ctx.level_data(0, 6)
+    g -= (bj * g).sum() / bj.sum()
+    f = torch.from_numpy(ctx.direct_stiffness_summation(np.ascontiguousarray(bj * g))).cuda(device)
+    u = torch.zeros_like(f)
+    lib_stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", device))
+    udofs = mesh.unique_nodes(n)
+    out = {"workload": "channel 32x16x16 tanh(2.0) y-stretch, perturb 0.1, N=9 (n=10), "
+                       "8 Fourier modes, Poisson FCG+p-MG to 1e-10 abs",
+           "local_points": mesh.nel * n ** 3, "unique_dofs": udofs,
+           "host_setup_s": setup_s,
+           "launch_shapes": {str(k): v for k, v in tuned.items()}}
+    sols = {}
+    for prec in ("fp64", "mixed"):
+        ctx.set_precision(prec)
+
+        def solve():
+            with torch.cuda.stream(lib_stream):
+                u.zero_()
+            return ctx.solve_poisson_cg(f, u, eps=EPS, history=False)[1]
+
+        ms, infos = cuda_timed(lib_stream, solve, 3, 2)
+        it = sum(i["iterations"] for i in infos) / 3
+        sols[prec] = u.cpu().numpy().copy()
+        out[prec] = {"ms_per_solve": ms / 3, "iterations": it,
+                     "gdof_per_s": udofs * it / (ms / 3 * 1e-3) / 1e9,
+                     "solves_per_s": 3 / (ms * 1e-3),
+                     "residual": infos[-1]["residual"]}
+    d64 = sols["fp64"] - sols["fp64"].mean()
+    d32 = sols["mixed"] - sols["mixed"].mean()
+    out["mixed"]["max_rel_diff_vs_fp64"] = float(np.abs(d32 - d64).max() / np.abs(d64).max())
+    out["mixed"]["speedup_solves_vs_fp64"] = out["mixed"]["solves_per_s"] / \
+        out["fp64"]["solves_per_s"]
+    ctx.close()
+    return out
+
+
+def run_particles(args, ctx, mesh, n, device, nsteps=100, npart=1_000_000):
+    """C4: 1M particles in the 16^3 N=7 TGV flow: nsteps calls of
+    integrate_particle_equations, each advancing 2 dt (the reference's
+    cadence, flow dt = 1e-3), on frozen velocity snapshots (the reference
+    computes ur once, src/main.c:84) of the TGV field in reference
+    components; particles start at rest, tau in {0.1, ..., 1.0}.  The walk
+    runs on the oracle's GLL points and factors, and a 2000-particle sample of
+    the first call is checked bitwise against the oracle on the CPU."""
+    import numpy as np
+    import torch
+    import oracle
+    X, Y, Z = (ctx.level_data(0, 12 + a) for a in range(3))
+    dt = 1e-3
+    h = 2 * math.pi / args.ne          # element width: ur = u / (h / 2)
+    snaps = np.stack([np.stack([np.sin(X) * np.cos(Y) * np.cos(Z),
+                                -np.cos(X) * np.sin(Y) * np.cos(Z), 0 * X]) * (2.0 / h)
+                      for _ in range(3)])
+    orc = oracle.Oracle(mesh, n)
+    pts, jac, tinv = orc.particle_geometry()
+    ctx.setup_particle_geometry(pts, jac, tinv)
+    ctx.set_particle_velocity(torch.from_numpy(snaps).cuda(device))
+    rng = np.random.default_rng(7)
+    state = np.zeros((npart, 8))
+    ints = np.zeros((npart, 3), np.int32)
+    state[:, :3] = rng.uniform(-1, 1, (npart, 3))
+    state[:, 7] = np.linspace(0.1, 1.0, 10)[np.arange(npart) % 10]
+    ints[:, 0] = rng.integers(0, mesh.nel, npart)
+    ints[:, 1] = ints[:, 0]
+    sample = slice(0, 2000)
+    s_in, i_in = state[sample].copy(), ints[sample].copy()
+    sd = torch.from_numpy(state).cuda(device)
+    idv = torch.from_numpy(ints).cuda(device)
+    lib_stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", device))
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    t, total_ms, passes, first = 0.0, 0.0, [], None
+    for step in range(nsteps):
+        t += 2 * dt
+        e0.record(lib_stream)
+        _, _, p = ctx.integrate_particle_equations(sd, idv, t, dt)
+        e1.record(lib_stream)
+        e1.synchronize()
+        total_ms += e0.elapsed_time(e1)
+        passes.append(p)
+        if step == 0:
+            first = (sd[sample].cpu().numpy().copy(), idv[sample].cpu().numpy().copy())
+    orc.set_params(2 * dt, dt, 1.0 / 1600.0)
+    s_o, i_o, _ = orc.particles_advance(s_in, i_in, snaps)
+    orc.close()
+    final = idv.cpu().numpy()
+    moved = int((final[:, 0] != ints[:, 0]).sum())
+    return {"workload": f"{npart} particles in TGV {args.ne}^3 N={n-1}, {nsteps} calls of "
+                        "integrate_particle_equations, each over 2 dt (dt = 1e-3)",
+            "ms_per_call": total_ms / nsteps,
+            "particle_steps_per_s": npart * nsteps / (total_ms * 1e-3),
+            "max_passes": max(passes), "changed_element": moved,
+            "reseeded": int((final[:, 2] == 5).sum()),
+            "sample_vs_oracle_first_call": {
+                "particles": 2000,
+                "element_ids_bitwise": bool(np.array_equal(i_o, first[1])),
+                "state_bitwise": bool(np.array_equal(s_o.view(np.uint64),
+                                                     first[0].view(np.uint64)))}}
+
+
+def run_convection(args, ctx, mesh, n, device, calls=25):
+    """Dealiased convection over all elements, the 25 calls of one step."""
+    import numpy as np
+    import torch
+    X, Y, Z = (ctx.level_data(0, 12 + a) for a in range(3))
+    u = torch.from_numpy(np.stack([np.sin(X) * np.cos(Y) * np.cos(Z),
+                                   -np.cos(X) * np.sin(Y) * np.cos(Z), 0 * X])).cuda(device)
+    out = torch.empty_like(u)
+    lib_stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", device))
+    ms, _ = cuda_timed(lib_stream, lambda: ctx.convection_operator(u, u, out), calls, 2)
+    npts = mesh.nel * n ** 3
+    m = (3 * n) // 2
+    alg = (6 * 8 + 3 * 8) * npts + 10 * 8 * mesh.nel * m ** 3
+    return {"workload": f"TGV {args.ne}^3 N={n-1}, m={m} dealiasing grid, {calls} calls",
+            "ms_per_call": ms / calls, "ms_per_step_25_calls": ms,
+            "achieved_gbs": alg / (ms / calls * 1e-3) / 1e9,
+            "algorithmic_bytes_per_call": alg}
+
+
+# ---------------------------------------------------------------------------
 # GPU arm
 # ---------------------------------------------------------------------------
 def run_ours(args):
@@ -433,6 +596,15 @@ def run_ours(args):
         ctx.close()
         if pg is not None:
             pg.destroy_process_group()
+        return 0
+
+    if args.sections == "extra":
+        res = {"convection": run_convection(args, ctx, mesh, n, local),
+               "particles": run_particles(args, ctx, mesh, n, local),
+               "channel": run_channel(args, local)}
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "sections": "extra", **res}))
+        ctx.close()
         return 0
 
     if args.sections == "op":
@@ -517,14 +689,10 @@ def run_ours(args):
         (ms_e2e * 1e-3) / 1e9
 
     # ---- roofline of the dominant kernel: level-0 element operator ----------
-    p = torch.randn(mesh.nel, n, n, n, dtype=torch.float64, device=dev)
-    ap = torch.empty_like(p)
-    torch.cuda.synchronize()
-    reps = 50
-    for _ in range(5):
-        ctx.local_opeval(S.PRESSURE, p, ap)
-    op_ms, _ = timed(lambda: ctx.local_opeval(S.PRESSURE, p, ap), reps, 0)
-    op_ms /= reps
+    # 50 launches back to back on the library's stream between CUDA events
+    # (ssg_time_operator), best of three
+    op_ms = ctx.time_operator(S.PRESSURE, 50) * 1e-3
+    op_ms_h = ctx.time_operator(S.X_VELOCITY, 50) * 1e-3
     alg = OP_BYTES_PER_POINT * npts
     peak, peak_kind = peaks()
     achieved = alg / (op_ms * 1e-3) / 1e9
@@ -543,6 +711,11 @@ def run_ours(args):
     hms, hinfo = timed(helm, 5, 1)
 
     serving = run_serving(args, local) if args.serve_requests > 0 else None
+    extra = {}
+    if not args.no_extra:
+        extra["convection"] = run_convection(args, ctx, mesh, n, local)
+        extra["particles"] = run_particles(args, ctx, mesh, n, local)
+        extra["channel"] = run_channel(args, local)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -588,10 +761,18 @@ def run_ours(args):
                 "d2h_bytes_per_step": 8 * npts, "ms_per_step": ms_e2e / ke},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": OP_TRAFFIC_BYTES,
-                     "kernel": "k_ax<8,double> (level-0 Laplacian)",
+                     "kernel": ("k_ax8_dmma<double> (level-0 Laplacian, FP64 DMMA)"
+                                if n == 8 else f"k_ax<{n},double> (level-0 Laplacian)"),
                      "us_per_launch": op_ms * 1e3,
+                     "bytes_per_point": OP_BYTES_PER_POINT,
+                     "helmholtz": {"us_per_launch": op_ms_h * 1e3,
+                                   "achieved": 72 * npts / (op_ms_h * 1e-3) / 1e9,
+                                   "frac": 72 * npts / (op_ms_h * 1e-3) / 1e9 / peak},
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"},
         "serving": serving,
+        "channel_c3": extra.get("channel"),
+        "particles_c4": extra.get("particles"),
+        "convection": extra.get("convection"),
         "cpu_baseline": cpu,
         "gpu_launches": int(launches),
         "clocks": clocks,

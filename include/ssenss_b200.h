@@ -251,6 +251,11 @@ ssg_status ssg_convection_operator(ssg_context *ctx, const double *u,
  * Results are unchanged: every shape computes the same sums in the same
  * order. */
 ssg_status ssg_autotune(ssg_context *ctx, int reps);
+/* Device time of the level-0 element operator (var: Poisson or Helmholtz,
+ * FP64) in microseconds per apply: reps launches back to back on the
+ * context's stream between two CUDA events, best of three trials. */
+ssg_status ssg_time_operator(ssg_context *ctx, int var, int reps,
+		double *us_per_apply);
 /* Launch shapes in use for order n (tuned or default); elements per block
  * 0 = the FP64 tensor-core operator (n = 8: one warp per element). */
 ssg_status ssg_tuning(int n, int *ax_elements_per_block,

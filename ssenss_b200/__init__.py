@@ -115,6 +115,13 @@ class Context:
     def set_graphs(self, enable: bool):
         self._check(self.lib.ssg_set_graphs(self.h, int(bool(enable))), "set_graphs")
 
+    def time_operator(self, var=PRESSURE, reps: int = 50) -> float:
+        """Device microseconds per level-0 operator apply (ssg_time_operator)."""
+        us = C.c_double()
+        self._check(self.lib.ssg_time_operator(self.h, int(var), int(reps), C.byref(us)),
+                    "time_operator")
+        return float(us.value)
+
     def autotune(self, reps: int = 10):
         """ssg_autotune: time the launch-shape candidates on this mesh and
         keep the fastest (process-wide, per order); returns the shapes."""

@@ -180,10 +180,14 @@ static ssg_status upload_all(ssg_context* c) {
     const size_t np = d.npts;
     const std::vector<double> rho = rho3(h.w);
     std::vector<double> bj(np), gf(6 * np);
-    for (int e = 0; e < nel; ++e)
-      for (size_t q = 0; q < h.nt; ++q) bj[e * h.nt + q] = rho[q] * h.det[e * h.nt + q];
-    for (int a = 0; a < 6; ++a)
-      for (size_t q = 0; q < np; ++q) gf[a * np + q] = h.g[a][q] * bj[q];
+    parallel_elements(nel, [&](int e0, int e1) {
+      for (int e = e0; e < e1; ++e)
+        for (size_t q = 0; q < h.nt; ++q) {
+          const size_t i = e * h.nt + q;
+          bj[i] = rho[q] * h.det[i];
+          for (int a = 0; a < 6; ++a) gf[a * np + i] = h.g[a][i] * bj[i];
+        }
+    });
     std::vector<double> kd(np);
     stiffness_diagonal(h, nel, kd.data());
     std::vector<double> dp(kd);
@@ -195,6 +199,18 @@ static ssg_status upload_all(ssg_context* c) {
     double nun = 0.0;
     for (double v : sc) nun += v;
     d.nunique = nun;
+    if (h.n == 8) {
+      // the tensor-core operator's fragment order (see ax8.cu)
+      std::vector<double> nat(gf);
+      parallel_elements(nel, [&](int e0, int e1) {
+        for (int a = 0; a < 6; ++a)
+          for (int e = e0; e < e1; ++e)
+            for (size_t q = 0; q < h.nt; ++q) {
+              const size_t i = e * h.nt + q;
+              gf[a * np + e * h.nt + ax8_fragment_index((int)q)] = nat[a * np + i];
+            }
+      });
+    }
     SSG_TRY(dupload(c, &d.gf, gf.data(), gf.size()));
     SSG_TRY(dupload(c, &d.bj, bj.data(), np));
     SSG_TRY(dupload(c, &d.kdiag, kd.data(), np));
@@ -557,9 +573,18 @@ ssg_status ssg_level_data(ssg_context* c, int level, int which, double* dst) {
   const size_t np = d.npts;
   const double* src = nullptr;
   std::vector<double> tmp;
-  if (which >= 0 && which < 6)
-    src = d.gf + which * np;
-  else if (which == 6)
+  if (which >= 0 && which < 6) {
+    SSG_CUDA(c, cudaStreamSynchronize(c->stream));
+    SSG_CUDA(c, cudaMemcpy(dst, d.gf + which * np, np * sizeof(double), cudaMemcpyDeviceToHost));
+    if (d.n == 8) {
+      // back from the tensor-core operator's fragment order
+      std::vector<double> frag(dst, dst + np);
+      for (size_t e = 0; e < np / d.nt; ++e)
+        for (size_t q = 0; q < d.nt; ++q)
+          dst[e * d.nt + q] = frag[e * d.nt + ax8_fragment_index((int)q)];
+    }
+    return SSG_OK;
+  } else if (which == 6)
     src = d.bj;
   else if (which == 7)
     src = d.dinv_p;

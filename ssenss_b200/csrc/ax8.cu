@@ -20,10 +20,15 @@
 //   backward t: sum_l D[l][k] w2[l][j][i]               registers
 // so the three derivatives of a point and the three transposed
 // contributions to it all land in the lane that owns it: the metric product
-// and the final sum need no exchange.  Shared memory holds D, S and, per
+// and the final sum need no exchange.  The metric factors of this order are
+// stored in that ownership ("fragment order", ax8_fragment_index) so each
+// lane reads its two points of a plane with one 2-wide load.  Shared memory
+// holds D, S and, per
 // warp, the per-plane results the t-direction needs at the end (each lane
 // touches only its own slots).
 #include <cuda_runtime.h>
+
+#include <type_traits>
 
 #include "kernels.cuh"
 #include "ssg_internal.h"
@@ -48,6 +53,7 @@ __global__ void __launch_bounds__(128, 4) k_ax8_dmma(int nel, T* __restrict__ u,
                                                      const double* __restrict__ Sg,
                                                      double lambda, PUpdate pu) {
   constexpr int N = 8, NN = 64, NT = 512, WPB = 4;
+  using V2 = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
   if (FUSEP && pu.stop && *pu.stop != 0.0) return;   // uniform over the grid
   __shared__ double sD[NN], sS[NN];
   // per warp: the transposed r/s contributions and the t-flux of every
@@ -101,12 +107,17 @@ __global__ void __launch_bounds__(128, 4) k_ax8_dmma(int nel, T* __restrict__ u,
       // forward r: B = u[k][j = g][l = 4c + t]; forward s: A = u[k][l = 4c + t][i = g]
       const double b0 = val(k * NN + g * N + t), b1 = val(k * NN + g * N + 4 + t);
       const double a0 = val(k * NN + t * N + g), a1 = val(k * NN + (4 + t) * N + g);
+      // metric factors in fragment order: this lane's two points of plane k
+      // are adjacent (ax8_fragment_index), one 2-wide load per factor
       double gg[2][6];
+      {
+        const size_t o = base + k * NN + 2 * lane;
 #pragma unroll
-      for (int s = 0; s < 2; ++s) {
-        const size_t o = base + k * NN + (2 * t + s) * N + g;
-#pragma unroll
-        for (int a = 0; a < 6; ++a) gg[s][a] = (double)__ldg(gf + a * npts + o);
+        for (int a = 0; a < 6; ++a) {
+          const V2 v = __ldg(reinterpret_cast<const V2*>(gf + a * npts + o));
+          gg[0][a] = (double)v.x;
+          gg[1][a] = (double)v.y;
+        }
       }
       double ur0 = 0.0, ur1 = 0.0, us0 = 0.0, us1 = 0.0;
       dmma(ur0, ur1, fA[0], b0, ur0, ur1);
@@ -149,13 +160,18 @@ __global__ void __launch_bounds__(128, 4) k_ax8_dmma(int nel, T* __restrict__ u,
     }
     // backward t (each lane reads only its own column of w2), the sum, the
     // Helmholtz mass term
+    double w2r[N][2];
+#pragma unroll
+    for (int l = 0; l < N; ++l)
+#pragma unroll
+      for (int s = 0; s < 2; ++s) w2r[l][s] = w2[l][s][lane];
 #pragma unroll
     for (int k = 0; k < N; ++k)
 #pragma unroll
       for (int s = 0; s < 2; ++s) {
         double ot = 0.0;
 #pragma unroll
-        for (int l = 0; l < N; ++l) ot += Xt[l * N + k] * w2[l][s][lane];
+        for (int l = 0; l < N; ++l) ot += Xt[l * N + k] * w2r[l][s];
         const size_t o = base + k * NN + (2 * t + s) * N + g;
         double out = acc[k][s][lane] + ot;
         if (HELM) out += lambda * (__ldg(bj + o) * uo[k][s]);

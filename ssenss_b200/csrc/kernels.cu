@@ -769,10 +769,10 @@ cudaError_t run_ax(cudaStream_t s, int n, int nel, int epb, bool helm, bool fp32
     pu.stop = pua->stop;
     pu.first = pua->first;
   }
-  // n = 8: the FP64 tensor-core kernel (FP32 or FP64 storage) unless the
-  // autotuner (or the caller, epb > 0) picked the shared-memory one
-  const bool dmma = n == 8 &&
-                    (epb == AX_DMMA || (epb == 0 && g_tune_ax_kind[8] != AX_KIND_CLASSIC));
+  // n = 8: the FP64 tensor-core kernel (FP32 or FP64 storage)
+  // (order 8 stores its metric factors in the tensor-core kernel's fragment
+  // order, so that kernel is the only operator of this order)
+  const bool dmma = n == 8;
   if (dmma)
     return run_ax8_dmma(s, nel, helm, fp32, (void*)in, out, gf, npts, bj, D, S, lambda,
                         fuse ? &pu : nullptr);

@@ -12,27 +12,6 @@
 
 namespace ssg {
 
-// Run f(e0, e1) over element ranges on up to 32 host threads.  Every
-// element is computed by one thread with the same arithmetic as a serial
-// loop, so the results do not depend on the thread count.
-template <class F>
-static void parallel_elements(int nel, F&& f) {
-  unsigned hw = std::thread::hardware_concurrency();
-  int nth = (int)std::min<unsigned>(hw ? hw : 1, 32u);
-  nth = std::max(1, std::min(nth, nel / 8));
-  if (nth <= 1) {
-    f(0, nel);
-    return;
-  }
-  std::vector<std::thread> th;
-  const int chunk = (nel + nth - 1) / nth;
-  for (int t = 0; t < nth; ++t) {
-    const int e0 = t * chunk, e1 = std::min(nel, e0 + chunk);
-    if (e0 >= e1) break;
-    th.emplace_back([&f, e0, e1] { f(e0, e1); });
-  }
-  for (auto& x : th) x.join();
-}
 
 int level_orders(int n, int* orders) {
   // nmg[i] = max(2, (n-1)/2^i + 1), stopping at 2 (src/precon.c:62-69)
@@ -354,7 +333,8 @@ static int corner_node(int n, int c) {
 void host_dss(const HostMesh& m, int n, double* u) {
   const size_t nt = (size_t)n * n * n;
   std::vector<double> pre(u, u + nt * m.nel);
-  for (int e = 0; e < m.nel; ++e) {
+  parallel_elements(m.nel, [&](int e0, int e1) {
+  for (int e = e0; e < e1; ++e) {
     double* ue = u + e * nt;
     const int* pr = m.pairs.data() + 52 * (size_t)e;
     for (int f = 0; f < 6; ++f, pr += 2)
@@ -369,6 +349,7 @@ void host_dss(const HostMesh& m, int n, double* u) {
     for (int c = 0; c < 8; ++c, pr += 2)
       if (pr[0] >= 0) ue[corner_node(n, c)] += pre[pr[0] * nt + corner_node(n, pr[1])];
   }
+  });
 }
 
 // Ordered DSS sources of one local node (element e, node loc): its
@@ -410,7 +391,8 @@ void dss_ec_table(const HostMesh& m, int n, std::vector<int>& tab) {
   const int I = n > 2 ? n - 2 : 0;
   const size_t per = (size_t)12 * I * 4 + 8 * 8;
   tab.assign(per * m.nel, -1);
-  for (int e = 0; e < m.nel; ++e) {
+  parallel_elements(m.nel, [&](int e0, int e1) {
+  for (int e = e0; e < e1; ++e) {
     int* t = tab.data() + per * e;
     int src[7];
     for (int q = 0; q < 12; ++q)
@@ -427,6 +409,7 @@ void dss_ec_table(const HostMesh& m, int n, std::vector<int>& tab) {
         if (src[a] >= 0) t[w++] = src[a];
     }
   }
+  });
 }
 
 // Element-local Jacobi diagonal of the Laplacian in the reference's form

@@ -4,7 +4,9 @@
 #include <cuda_runtime.h>
 #include <cstddef>
 #include <cstdint>
+#include <algorithm>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "ssenss_b200.h"
@@ -42,6 +44,37 @@ struct HostMesh {
   bool has_particle_geom = false;
   std::vector<double> ppoints;          // GLL points of the particle walk (empty: lev[0].x)
 };
+
+// Run f(e0, e1) over element ranges on up to 32 host threads.  Every
+// element is computed by one thread with the same arithmetic as a serial
+// loop, so the results do not depend on the thread count.
+template <class F>
+inline void parallel_elements(int nel, F&& f) {
+  unsigned hw = std::thread::hardware_concurrency();
+  int nth = (int)std::min<unsigned>(hw ? hw : 1, 32u);
+  nth = std::max(1, std::min(nth, nel / 8));
+  if (nth <= 1) {
+    f(0, nel);
+    return;
+  }
+  std::vector<std::thread> th;
+  const int chunk = (nel + nth - 1) / nth;
+  for (int t = 0; t < nth; ++t) {
+    const int e0 = t * chunk, e1 = std::min(nel, e0 + chunk);
+    if (e0 >= e1) break;
+    th.emplace_back([&f, e0, e1] { f(e0, e1); });
+  }
+  for (auto& x : th) x.join();
+}
+
+// Position of natural node q = (k n + j) n + i of an n = 8 element in the
+// tensor-core operator's fragment order: plane k, lane 4i + j/2, slot j%2
+// (the lane that owns the point, ax8.cu), so a lane's two points of a plane
+// are adjacent.
+inline int ax8_fragment_index(int q) {
+  const int k = q >> 6, j = (q >> 3) & 7, i = q & 7;
+  return k * 64 + (4 * i + (j >> 1)) * 2 + (j & 1);
+}
 
 int level_orders(int n, int* orders);
 void gll_basis(int n, double* x, double* w);

@@ -2,9 +2,9 @@
 //
 // The element kernels have one free shape parameter per order n and the
 // vector kernels one overall:
-//   * the operator kernel: elements per block of the shared-memory kernel
-//     (k_ax: 1, 2, 4, ... up to the 256-thread / 96 KB limit of
-//     ax_epb_max(n)) and, for n = 8, the FP64 tensor-core kernel k_ax8_dmma;
+//   * elements per block of the shared-memory operator (k_ax: 1, 2, 4, ...
+//     up to the 256-thread / 96 KB limit of ax_epb_max(n)); order 8 runs the
+//     FP64 tensor-core operator k_ax8_dmma, which has no shape parameter;
 //   * blocks per SM of the persistent DSS grid: 1 .. 16;
 //   * blocks per SM of the grid-stride vector kernels: 2 .. 32.
 // ssg_autotune times every candidate on the context's own mesh and levels
@@ -48,8 +48,8 @@ static ssg_status tune_level(ssg_context* c, int level, double* a, double* b, do
                              int reps) {
   const DevLevel& L = c->lev[level];
   const int n = L.n;
-  // operator: elements per block
-  {
+  // operator: elements per block (order 8 has the tensor-core kernel only)
+  if (n != 8) {
     int best_epb = 0;
     float best = 1e30f;
     for (int epb = 1; epb <= ax_epb_max(n); epb *= 2) {
@@ -67,18 +67,6 @@ static ssg_status tune_level(ssg_context* c, int level, double* a, double* b, do
       }
     }
     g_tune_ax_epb[n] = best_epb;
-    g_tune_ax_kind[n] = AX_KIND_CLASSIC;
-    if (n == 8) {
-      // the FP64 tensor-core kernel of this order
-      SSG_CUDA(c, run_ax(c->stream, n, c->nel, AX_DMMA, false, false, a, b, L.gf, L.npts,
-                         nullptr, L.D, L.D, 0.0, nullptr));
-      float t = 0.f;
-      SSG_TRY(time_launches(c, reps, [&] {
-        return run_ax(c->stream, n, c->nel, AX_DMMA, false, false, a, b, L.gf, L.npts,
-                      nullptr, L.D, L.D, 0.0, nullptr);
-      }, &t));
-      if (t < best) g_tune_ax_kind[n] = AX_KIND_DMMA;
-    }
   }
   // DSS: blocks per SM of the persistent grid
   {
@@ -160,11 +148,34 @@ ssg_status ssg_autotune(ssg_context* c, int reps) {
   return st;
 }
 
+ssg_status ssg_time_operator(ssg_context* c, int var, int reps, double* us_per_apply) {
+  if (!c || !us_per_apply || reps <= 0) return SSG_ERR_ARG;
+  if (!c->ready) return fail(c, SSG_ERR_STATE, "no mesh set up on this context");
+  SSG_CUDA(c, cudaSetDevice(c->device));
+  SSG_TRY(ensure_workspace(c));
+  if (var != SSG_PRESSURE) SSG_TRY(helmholtz_diag_update(c));
+  const DevLevel& L = c->lev[0];
+  const bool helm = var != SSG_PRESSURE;
+  const double lam = (11.0 / 6.0) / (c->dt * c->visc);
+  double* in = workspace_scratch(c);
+  double* out = c->d_stage[0];
+  SSG_CUDA(c, cudaMemsetAsync(in, 0, L.npts * sizeof(double), c->stream));
+  auto launch = [&] {
+    return run_ax(c->stream, L.n, c->nel, 0, helm, false, in, out, L.gf, L.npts, L.bj, L.D,
+                  L.S, lam, nullptr);
+  };
+  SSG_CUDA(c, launch());
+  float best = 0.f;
+  SSG_TRY(time_launches(c, reps, launch, &best));
+  *us_per_apply = 1e3 * (double)best / reps;
+  return SSG_OK;
+}
+
 ssg_status ssg_tuning(int n, int* ax_elements_per_block, int* dss_blocks_per_sm,
                       int* vector_blocks_per_sm) {
   if (n < 2 || n > SSG_MAXN) return SSG_ERR_ARG;
   // 0: the FP64 tensor-core operator (one warp per element)
-  const bool dmma = n == 8 && g_tune_ax_kind[8] != AX_KIND_CLASSIC;
+  const bool dmma = n == 8;
   if (ax_elements_per_block) *ax_elements_per_block = dmma ? 0 : ax_epb(n);
   if (dss_blocks_per_sm) *dss_blocks_per_sm = g_tune_dss_bps[n] > 0 ? g_tune_dss_bps[n] : 8;
   if (vector_blocks_per_sm) *vector_blocks_per_sm = g_tune_vec_bps > 0 ? g_tune_vec_bps : 32;
