@@ -51,7 +51,7 @@ __global__ void __launch_bounds__(128, 4) k_ax8_dmma(int nel, T* __restrict__ u,
                                                      size_t npts, const double* __restrict__ bj,
                                                      const double* __restrict__ Dg,
                                                      const double* __restrict__ Sg,
-                                                     double lambda, PUpdate pu) {
+                                                     double lambda, PUpdate pu, ScalarOp dop) {
   constexpr int N = 8, NN = 64, NT = 512, WPB = 4;
   using V2 = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
   if (FUSEP && pu.stop && *pu.stop != 0.0) return;   // uniform over the grid
@@ -84,6 +84,7 @@ __global__ void __launch_bounds__(128, 4) k_ax8_dmma(int nel, T* __restrict__ u,
   double (*acc)[2][32] = sAcc[wid];
   double (*w2)[2][32] = sW2[wid];
   const int warps = WPB * gridDim.x;
+  double pap = 0.0;   // p . (A p) over this lane's points (FUSEP with a dot)
   for (int e = blockIdx.x * WPB + wid; e < nel; e += warps) {
     const size_t base = (size_t)e * NT;
     // value of the input field at local node q of this element (FUSEP: the
@@ -176,6 +177,7 @@ __global__ void __launch_bounds__(128, 4) k_ax8_dmma(int nel, T* __restrict__ u,
         double out = acc[k][s][lane] + ot;
         if (HELM) out += lambda * (__ldg(bj + o) * uo[k][s]);
         au[o] = (T)out;
+        if (FUSEP) pap += uo[k][s] * (double)(T)out;
       }
     if (FUSEP) {
       // every lane has read this element's old direction: store the new one
@@ -185,6 +187,12 @@ __global__ void __launch_bounds__(128, 4) k_ax8_dmma(int nel, T* __restrict__ u,
 #pragma unroll
         for (int s = 0; s < 2; ++s) u[base + k * NN + (2 * t + s) * N + g] = (T)uo[k][s];
     }
+  }
+  if (FUSEP && pu.part) {
+    __shared__ double sred[32];
+    double v[1] = {pap};
+    block_reduce<1>(v, sred);
+    finish<1>(v, pu.part, dop, sred);
   }
 }
 
@@ -196,7 +204,7 @@ __global__ void __launch_bounds__(128, 4) k_ax8_dmma(int nel, T* __restrict__ u,
 template <typename T>
 static cudaError_t launch_ax8(cudaStream_t s, int nel, bool helm, T* u, T* au, const T* gf,
                               size_t npts, const double* bj, const double* D, const double* S,
-                              double lambda, const dev::PUpdate* pu) {
+                              double lambda, const dev::PUpdate* pu, const ScalarOp& dop) {
   const int wpb = 4;
   int grid = (nel + wpb - 1) / wpb;
   if (grid > 148 * 8) grid = 148 * 8;
@@ -206,31 +214,33 @@ static cudaError_t launch_ax8(cudaStream_t s, int nel, bool helm, T* u, T* au, c
   if (helm) {
     if (pu)
       dev::k_ax8_dmma<T, true, true><<<grid, 32 * wpb, 0, s>>>(nel, u, au, gf, npts, bj, D, S,
-                                                             lambda, p);
+                                                             lambda, p, dop);
     else
       dev::k_ax8_dmma<T, true, false><<<grid, 32 * wpb, 0, s>>>(nel, u, au, gf, npts, bj, D, S,
-                                                              lambda, p);
+                                                              lambda, p, dop);
   } else {
     if (pu)
       dev::k_ax8_dmma<T, false, true><<<grid, 32 * wpb, 0, s>>>(nel, u, au, gf, npts, bj, D,
-                                                              D, 0.0, p);
+                                                              D, 0.0, p, dop);
     else
       dev::k_ax8_dmma<T, false, false><<<grid, 32 * wpb, 0, s>>>(nel, u, au, gf, npts, bj, D,
-                                                               D, 0.0, p);
+                                                               D, 0.0, p, dop);
   }
   return cudaGetLastError();
 }
 
 cudaError_t run_ax8_dmma(cudaStream_t s, int nel, bool helm, bool fp32, void* u, void* au,
                          const void* gf, size_t npts, const double* bj, const double* D,
-                         const double* S, double lambda, const dev::PUpdate* pu) {
+                         const double* S, double lambda, const dev::PUpdate* pu,
+                         const ScalarOp* dop) {
+  const ScalarOp o = dop ? *dop : ScalarOp();
   if (fp32) {
     if (helm) return cudaErrorInvalidValue;
     return launch_ax8<float>(s, nel, false, (float*)u, (float*)au, (const float*)gf, npts, bj,
-                             D, S, lambda, pu);
+                             D, S, lambda, pu, o);
   }
   return launch_ax8<double>(s, nel, helm, (double*)u, (double*)au, (const double*)gf, npts, bj,
-                            D, S, lambda, pu);
+                            D, S, lambda, pu, o);
 }
 
 }  // namespace ssg

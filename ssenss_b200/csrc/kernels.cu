@@ -36,112 +36,6 @@ namespace dev {
 // ---------------------------------------------------------------------------
 // solver scalar algebra on the reduced sums (one thread)
 // ---------------------------------------------------------------------------
-__device__ void apply_scalar_op(const ScalarOp& op, const double* __restrict__ sums) {
-  double* f = op.frame;
-  switch (op.code) {
-    case OP_NONE:
-      break;
-    case OP_CG_INIT_C:   // c = (w.z)/nunique (pressure); a new solve starts
-      f[F_C] = op.pressure ? sums[0] / op.nunique : 0.0;
-      f[F_ITER] = 0.0;
-      f[F_DONE] = 0.0;
-      break;
-    case OP_CG_INIT_RDZ:  // rdz = (r w).p, |r|_w ; reset counters
-      f[F_RDZ] = sums[0];
-      f[F_ERR0] = sqrt(sums[1]);
-      f[F_ITER] = 0.0;
-      f[F_DONE] = 0.0;
-      f[F_ERR] = sqrt(sums[1]);
-      break;
-    case OP_CG_ALPHA:     // alpha = rdz / (p w).ap
-      f[F_PAP] = sums[0];
-      f[F_ALPHA] = f[F_RDZ] / sums[0];
-      break;
-    case OP_CG_BETA: {    // sums: (r w).z, (r w).r, w.z, w.r
-      const double c = op.pressure ? sums[2] / op.nunique : 0.0;
-      const double rdz = sums[0] - c * sums[3];
-      f[F_C] = c;
-      f[F_BETA] = rdz / f[F_RDZ];
-      f[F_RDZ] = rdz;
-      const double err = sqrt(sums[1]);
-      f[F_ERR] = err;
-      f[F_ITER] += 1.0;
-      const bool go = (err > op.eps) && (f[F_ITER] < (double)op.max_iter);
-      f[F_DONE] = go ? 0.0 : 1.0;
-      if (op.hist && (int)f[F_ITER] <= op.hist_cap) op.hist[(int)f[F_ITER] - 1] = err;
-      break;
-    }
-    case OP_NULL_C:       // c = (w.x)/nunique into frame slot
-      f[F_C] = sums[0] / op.nunique;
-      break;
-    case OP_FCG_BETA:     // beta_k = sums[k] / pap[k]
-      for (int k = 0; k < op.m; ++k) f[F_FBETA + k] = sums[k] / f[F_FPAP + op.pap_idx[k]];
-      break;
-    case OP_FCG_ALPHA:    // pap0 and alpha = (p0 w).r / pap0
-      f[F_FPAP + op.pap_idx[0]] = sums[0];
-      f[F_ALPHA] = sums[1] / sums[0];
-      break;
-    case OP_FCG_ERR: {
-      const double err = sqrt(sums[0]);
-      f[F_ERR] = err;
-      f[F_ITER] += 1.0;
-      const bool go = (err > op.eps) && (f[F_ITER] < (double)op.max_iter);
-      f[F_DONE] = go ? 0.0 : 1.0;
-      if (op.hist && (int)f[F_ITER] <= op.hist_cap) op.hist[(int)f[F_ITER] - 1] = err;
-      break;
-    }
-    case OP_ERR0:
-      f[F_ERR0] = sqrt(sums[0]);
-      f[F_ITER] = 0.0;
-      f[F_DONE] = 0.0;
-      f[F_ERR] = sqrt(sums[0]);
-      break;
-  }
-}
-
-// ---------------------------------------------------------------------------
-// end of a reducing kernel: thread 0 holds the block's NQ partial sums.  They
-// are stored at part[q * gridDim.x + block]; when op.counter is set, the
-// last block to arrive sums all partials in index order (so the result does
-// not depend on which block is last), stores them in op.sums, applies the
-// solver scalar algebra and re-arms the counter.
-// ---------------------------------------------------------------------------
-template <int NQ>
-__device__ __forceinline__ void finish(const double (&v)[NQ], double* __restrict__ part,
-                                       const ScalarOp& op, double* sred) {
-  __shared__ int s_last;
-  if (threadIdx.x == 0) {
-#pragma unroll
-    for (int q = 0; q < NQ; ++q) part[q * gridDim.x + blockIdx.x] = v[q];
-    s_last = 0;
-    if (op.counter) {
-      // release: this block's partials are visible before its arrival
-      // counts; acquire: the last block sees every partial
-      cuda::atomic_ref<unsigned, cuda::thread_scope_device> arrived(*op.counter);
-      const unsigned prev = arrived.fetch_add(1u, cuda::memory_order_acq_rel);
-      s_last = prev == gridDim.x - 1;
-    }
-  }
-  __syncthreads();
-  if (!s_last) return;
-  double s[NQ];
-#pragma unroll
-  for (int q = 0; q < NQ; ++q) {
-    s[q] = 0.0;
-    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x)
-      s[q] += __ldcg(part + (size_t)q * gridDim.x + b);
-  }
-  block_reduce<NQ>(s, sred);
-  if (threadIdx.x == 0) {
-#pragma unroll
-    for (int q = 0; q < NQ; ++q) op.sums[q] = s[q];
-    apply_scalar_op(op, op.sums);
-    *op.counter = 0u;
-  }
-}
-
-
-// ---------------------------------------------------------------------------
 // local operator, optionally preceded by the CG direction update
 //   p = ((beta p + (z - c)) .* mask)   (first: p = (z - c) .* mask)
 // (src/solver.c:59-60,75-77 with subtract_nullspace folded in)
@@ -208,7 +102,7 @@ __global__ void __launch_bounds__(256, (N >= 10 ? 1 : 2)) k_ax(int nel, T* __res
                                                const double* __restrict__ bj,
                                                const double* __restrict__ Dg,
                                                const double* __restrict__ Sg,
-                                               double lambda, PUpdate pu) {
+                                               double lambda, PUpdate pu, ScalarOp dop) {
   constexpr int NN = N * N, P = AxLayout<N>::P, Q = AxLayout<N>::Q;
   constexpr int PLANE = N * Q, BLK = N * PLANE;
   if (FUSEP && pu.stop && *pu.stop != 0.0) return;   // uniform over the block
@@ -285,6 +179,7 @@ __global__ void __launch_bounds__(256, (N >= 10 ? 1 : 2)) k_ax(int nel, T* __res
   }
   __syncthreads();
   // transposed derivatives: r with D^T, s and t with S^T (= D^T for Poisson)
+  double pap = 0.0;   // p . (A p) over this thread's points (FUSEP)
 #pragma unroll
   for (int k = 0; k < N; ++k) {
     const double acc = row_dot<N>(sDT + i * P, sw0 + k * PLANE + j * Q);
@@ -293,6 +188,11 @@ __global__ void __launch_bounds__(256, (N >= 10 ? 1 : 2)) k_ax(int nel, T* __res
     double out = (acc + acs) + act;
     if (HELM && active) out += lambda * (__ldg(bj + off + (size_t)k * NN) * ru[k]);
     if (active) au[off + (size_t)k * NN] = (T)out;
+    if (FUSEP && active) pap += ru[k] * (double)(T)out;
+  }
+  if (FUSEP && pu.part) {
+    __shared__ double sflat[256];
+    finish_flat(pap, tid, nthr, pu.part, dop, sflat);
   }
 }
 
@@ -314,7 +214,8 @@ __global__ void __launch_bounds__(256) k_dss(int nel, int epb, const T* __restri
                                              const T* __restrict__ y,
                                              const T* __restrict__ y2,
                                              double* __restrict__ part,
-                                             const double* __restrict__ stop, ScalarOp op) {
+                                             const double* __restrict__ stop, ScalarOp op,
+                                             DssCg cg) {
   constexpr int NT = N * N * N, NN = N * N;
   constexpr int I = N > 2 ? N - 2 : 0, F = 6 * I * I, EC = 12 * I + 8;
   constexpr int ID = I > 0 ? I : 1, II = ID * ID;   // divisors (N = 2 has no
@@ -322,11 +223,18 @@ __global__ void __launch_bounds__(256) k_dss(int nel, int epb, const T* __restri
   if (stop && *stop != 0.0) return;   // uniform over the block
   __shared__ short sface[6 * NN];     // node of face f at face position p
   __shared__ double sred[2 * 32];
+  __shared__ double sred4[MODE == DSS_CGUPD ? 4 * 32 : 1];
   for (int q = threadIdx.x; q < 6 * NN; q += blockDim.x)
     sface[q] = (short)face_node(N, q / NN, (q % NN) / N, q % N);
   __syncthreads();
   (void)epb;
-  double s0 = 0.0, s1 = 0.0;
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+  const double alpha = MODE == DSS_CGUPD ? *cg.alpha : 0.0;
+  T* const cx = reinterpret_cast<T*>(cg.x);
+  const T* const cp = reinterpret_cast<const T*>(cg.p);
+  T* const cr = reinterpret_cast<T*>(cg.r);
+  const T* const cd = reinterpret_cast<const T*>(cg.dinv);
+  T* const cz = reinterpret_cast<T*>(cg.z);
   // one node task per thread, grid-stride over all elements' tasks; no
   // block-wide staging, so no barrier inside the loop
   const size_t ntask = (size_t)nel * NT;
@@ -390,7 +298,19 @@ __global__ void __launch_bounds__(256) k_dss(int nel, int epb, const T* __restri
       }
       const size_t gi = eb + loc;
       const double w = inv_count(1u + (unsigned)cnt);
-      if (MODE == DSS_RESID) {
+      if (MODE == DSS_CGUPD) {
+        // ap = acc: x += alpha p; r -= alpha ap; z = dinv r  (src/solver.c:66-71)
+        cx[gi] = (T)((double)cx[gi] + alpha * (double)cp[gi]);
+        const T rq = (T)((double)cr[gi] + -alpha * acc);
+        cr[gi] = rq;
+        const T zq = (T)((double)rq * (double)cd[gi]);
+        cz[gi] = zq;
+        const double rw = (double)rq * w;
+        s0 += rw * (double)zq;
+        s1 += rw * (double)rq;
+        s2 += w * (double)zq;
+        s3 += rw;
+      } else if (MODE == DSS_RESID) {
         const T rv = (T)((double)y[gi] + -acc);
         out[gi] = rv;
         s0 += (double)rv * w;
@@ -415,6 +335,10 @@ __global__ void __launch_bounds__(256) k_dss(int nel, int epb, const T* __restri
     double v[2] = {s0, s1};
     block_reduce<2>(v, sred);
     finish<2>(v, part, op, sred);
+  } else if (MODE == DSS_CGUPD) {
+    double v[4] = {s0, s1, s2, s3};
+    block_reduce<4>(v, sred4);
+    finish<4>(v, part, op, sred4);
   }
 }
 
@@ -724,7 +648,8 @@ int ax_epb(int n) {
 template <int N, typename T, bool HELM, bool FUSEP>
 static cudaError_t launch_ax_t(cudaStream_t s, int nel, int epb, T* u, T* au, const T* gf,
                                size_t npts, const double* bj, const double* D,
-                               const double* S, double lambda, const PUpdate& pu) {
+                               const double* S, double lambda, const PUpdate& pu,
+                               const ScalarOp& dop) {
   const size_t smem = (4 * N * AxLayout<N>::P + (size_t)epb * 3 * N * N * AxLayout<N>::Q) *
                       sizeof(double);
   static bool attr_set = false;
@@ -735,19 +660,20 @@ static cudaError_t launch_ax_t(cudaStream_t s, int nel, int epb, T* u, T* au, co
   }
   dim3 blk(N, N, epb);
   dim3 grd((nel + epb - 1) / epb);
-  { SSG_COUNT(); k_ax<N, T, HELM, FUSEP><<<grd, blk, smem, s>>>(nel, u, au, gf, npts, bj, D, S, lambda, pu); }
+  { SSG_COUNT(); k_ax<N, T, HELM, FUSEP><<<grd, blk, smem, s>>>(nel, u, au, gf, npts, bj, D, S, lambda, pu, dop); }
   return cudaGetLastError();
 }
 
 template <typename T, bool HELM, bool FUSEP>
 static cudaError_t ax_dispatch(int n, cudaStream_t s, int nel, int epb, T* u, T* au,
                                const T* gf, size_t npts, const double* bj, const double* D,
-                               const double* S, double lambda, const PUpdate& pu) {
+                               const double* S, double lambda, const PUpdate& pu,
+                               const ScalarOp& dop) {
   switch (n) {
 #define SSG_AXN(NV)                                                                   \
   case NV:                                                                            \
     return launch_ax_t<NV, T, HELM, FUSEP>(s, nel, epb, u, au, gf, npts, bj, D, S,    \
-                                           lambda, pu);
+                                           lambda, pu, dop);
     SSG_AXN(2) SSG_AXN(3) SSG_AXN(4) SSG_AXN(5) SSG_AXN(6) SSG_AXN(7)
     SSG_AXN(8) SSG_AXN(9) SSG_AXN(10) SSG_AXN(11) SSG_AXN(12)
 #undef SSG_AXN
@@ -761,6 +687,7 @@ cudaError_t run_ax(cudaStream_t s, int n, int nel, int epb, bool helm, bool fp32
                    const PUpdateArgs* pua) {
   PUpdate pu;
   const bool fuse = pua != nullptr;
+  ScalarOp dop;
   if (fuse) {
     pu.z = pua->z;
     pu.beta = pua->beta;
@@ -768,6 +695,10 @@ cudaError_t run_ax(cudaStream_t s, int n, int nel, int epb, bool helm, bool fp32
     pu.mask = pua->mask;
     pu.stop = pua->stop;
     pu.first = pua->first;
+    if (pua->dot) {
+      pu.part = pua->part;
+      dop = *pua->dot;
+    }
   }
   // n = 8: the FP64 tensor-core kernel (FP32 or FP64 storage)
   // (order 8 stores its metric factors in the tensor-core kernel's fragment
@@ -775,28 +706,28 @@ cudaError_t run_ax(cudaStream_t s, int n, int nel, int epb, bool helm, bool fp32
   const bool dmma = n == 8;
   if (dmma)
     return run_ax8_dmma(s, nel, helm, fp32, (void*)in, out, gf, npts, bj, D, S, lambda,
-                        fuse ? &pu : nullptr);
+                        fuse ? &pu : nullptr, &dop);
   if (epb <= 0) epb = ax_epb(n);
   if (fp32) {
     if (helm) return cudaErrorInvalidValue;
     if (fuse)
       return ax_dispatch<float, false, true>(n, s, nel, epb, (float*)in, (float*)out,
-                                             (const float*)gf, npts, nullptr, D, D, 0.0, pu);
+                                             (const float*)gf, npts, nullptr, D, D, 0.0, pu, dop);
     return ax_dispatch<float, false, false>(n, s, nel, epb, (float*)in, (float*)out,
-                                            (const float*)gf, npts, nullptr, D, D, 0.0, pu);
+                                            (const float*)gf, npts, nullptr, D, D, 0.0, pu, dop);
   }
   if (helm) {
     if (fuse)
       return ax_dispatch<double, true, true>(n, s, nel, epb, (double*)in, (double*)out,
-                                             (const double*)gf, npts, bj, D, S, lambda, pu);
+                                             (const double*)gf, npts, bj, D, S, lambda, pu, dop);
     return ax_dispatch<double, true, false>(n, s, nel, epb, (double*)in, (double*)out,
-                                            (const double*)gf, npts, bj, D, S, lambda, pu);
+                                            (const double*)gf, npts, bj, D, S, lambda, pu, dop);
   }
   if (fuse)
     return ax_dispatch<double, false, true>(n, s, nel, epb, (double*)in, (double*)out,
-                                            (const double*)gf, npts, nullptr, D, D, 0.0, pu);
+                                            (const double*)gf, npts, nullptr, D, D, 0.0, pu, dop);
   return ax_dispatch<double, false, false>(n, s, nel, epb, (double*)in, (double*)out,
-                                           (const double*)gf, npts, nullptr, D, D, 0.0, pu);
+                                           (const double*)gf, npts, nullptr, D, D, 0.0, pu, dop);
 }
 
 int dss_epb(int n) {
@@ -820,24 +751,27 @@ template <int N, typename T>
 static cudaError_t run_dss_n(cudaStream_t s, int mode, int nel, const T* in, T* out,
                              const int2* pr, const int4* ec, const double* mask, const T* y,
                              const T* y2, double* part, const double* stop,
-                             const ScalarOp& op) {
+                             const ScalarOp& op, const DssCg& cg) {
   const int epb = dss_epb(N);
   const int grd = dss_grid(N, nel);
   switch (mode) {
     case DSS_PLAIN:
-      { SSG_COUNT(); k_dss<N, T, DSS_PLAIN><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, ec, mask, y, y2, part, stop, op); }
+      { SSG_COUNT(); k_dss<N, T, DSS_PLAIN><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, ec, mask, y, y2, part, stop, op, cg); }
       break;
     case DSS_DOT:
-      { SSG_COUNT(); k_dss<N, T, DSS_DOT><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, ec, mask, y, y2, part, stop, op); }
+      { SSG_COUNT(); k_dss<N, T, DSS_DOT><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, ec, mask, y, y2, part, stop, op, cg); }
       break;
     case DSS_DOT2:
-      { SSG_COUNT(); k_dss<N, T, DSS_DOT2><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, ec, mask, y, y2, part, stop, op); }
+      { SSG_COUNT(); k_dss<N, T, DSS_DOT2><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, ec, mask, y, y2, part, stop, op, cg); }
       break;
     case DSS_RESID:
-      { SSG_COUNT(); k_dss<N, T, DSS_RESID><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, ec, mask, y, y2, part, stop, op); }
+      { SSG_COUNT(); k_dss<N, T, DSS_RESID><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, ec, mask, y, y2, part, stop, op, cg); }
       break;
     case DSS_AVG:
-      { SSG_COUNT(); k_dss<N, T, DSS_AVG><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, ec, mask, y, y2, part, stop, op); }
+      { SSG_COUNT(); k_dss<N, T, DSS_AVG><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, ec, mask, y, y2, part, stop, op, cg); }
+      break;
+    case DSS_CGUPD:
+      { SSG_COUNT(); k_dss<N, T, DSS_CGUPD><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, ec, mask, y, y2, part, stop, op, cg); }
       break;
     default:
       return cudaErrorInvalidValue;
@@ -849,12 +783,12 @@ template <typename T>
 static cudaError_t run_dss_t(cudaStream_t s, int mode, int n, int nel, const T* in, T* out,
                              const int* pairs, const int* ec_tab, const double* mask,
                              const T* y, const T* y2, double* part, const double* stop,
-                             const ScalarOp& op) {
+                             const ScalarOp& op, const DssCg& cg) {
   const int2* pr = reinterpret_cast<const int2*>(pairs);
   const int4* ec = reinterpret_cast<const int4*>(ec_tab);
   switch (n) {
 #define SSG_DSSN(NV) \
-  case NV: return run_dss_n<NV, T>(s, mode, nel, in, out, pr, ec, mask, y, y2, part, stop, op);
+  case NV: return run_dss_n<NV, T>(s, mode, nel, in, out, pr, ec, mask, y, y2, part, stop, op, cg);
     SSG_DSSN(2) SSG_DSSN(3) SSG_DSSN(4) SSG_DSSN(5) SSG_DSSN(6) SSG_DSSN(7)
     SSG_DSSN(8) SSG_DSSN(9) SSG_DSSN(10) SSG_DSSN(11) SSG_DSSN(12)
 #undef SSG_DSSN
@@ -865,14 +799,15 @@ static cudaError_t run_dss_t(cudaStream_t s, int mode, int n, int nel, const T* 
 cudaError_t run_dss(cudaStream_t s, int mode, bool fp32, int n, int nel, const void* in,
                     void* out, const int* pairs, const int* ec_tab, const double* mask,
                     const void* y, const void* y2, double* part, const double* stop,
-                    const ScalarOp* op) {
+                    const ScalarOp* op, const DssCg* cg) {
   const ScalarOp o = op_or_none(op);
-  if (!ec_tab) return cudaErrorInvalidValue;
+  const DssCg g = cg ? *cg : DssCg();
+  if (!ec_tab || (mode == DSS_CGUPD && !cg)) return cudaErrorInvalidValue;
   if (fp32)
     return run_dss_t<float>(s, mode, n, nel, (const float*)in, (float*)out, pairs, ec_tab,
-                            mask, (const float*)y, (const float*)y2, part, stop, o);
+                            mask, (const float*)y, (const float*)y2, part, stop, o, g);
   return run_dss_t<double>(s, mode, n, nel, (const double*)in, (double*)out, pairs, ec_tab,
-                           mask, (const double*)y, (const double*)y2, part, stop, o);
+                           mask, (const double*)y, (const double*)y2, part, stop, o, g);
 }
 
 cudaError_t run_tensor3(cudaStream_t s, bool fp32, bool add, int nel, int ni, int no,

@@ -6,8 +6,11 @@
 // the 1-D matrices live in dynamic shared memory.
 #pragma once
 
+#include <cuda/atomic>
 #include <cuda_runtime.h>
 #include <cstdint>
+
+#include "ssg_kernels.h"
 
 namespace ssg {
 namespace dev {
@@ -155,6 +158,7 @@ struct PUpdate {
   const double* mask = nullptr;
   const double* stop = nullptr;   // solver's stop flag: skip when set
   int first = 0;
+  double* part = nullptr;         // set: also reduce p . (A p) (unweighted)
 };
 
 // ---------------------------------------------------------------------------
@@ -185,6 +189,164 @@ __device__ __forceinline__ void block_reduce(double (&v)[NQ], double* sred) {
   }
   __syncthreads();
 }
+
+// ---------------------------------------------------------------------------
+__device__ inline void apply_scalar_op(const ScalarOp& op, const double* __restrict__ sums) {
+  double* f = op.frame;
+  switch (op.code) {
+    case OP_NONE:
+      break;
+    case OP_CG_INIT_C:   // c = (w.z)/nunique (pressure); a new solve starts
+      f[F_C] = op.pressure ? sums[0] / op.nunique : 0.0;
+      f[F_ITER] = 0.0;
+      f[F_DONE] = 0.0;
+      break;
+    case OP_CG_INIT_RDZ:  // rdz = (r w).p, |r|_w ; reset counters
+      f[F_RDZ] = sums[0];
+      f[F_ERR0] = sqrt(sums[1]);
+      f[F_ITER] = 0.0;
+      f[F_DONE] = 0.0;
+      f[F_ERR] = sqrt(sums[1]);
+      break;
+    case OP_CG_ALPHA:     // alpha = rdz / (p w).ap
+      f[F_PAP] = sums[0];
+      f[F_ALPHA] = f[F_RDZ] / sums[0];
+      break;
+    case OP_CG_BETA: {    // sums: (r w).z, (r w).r, w.z, w.r
+      const double c = op.pressure ? sums[2] / op.nunique : 0.0;
+      const double rdz = sums[0] - c * sums[3];
+      f[F_C] = c;
+      f[F_BETA] = rdz / f[F_RDZ];
+      f[F_RDZ] = rdz;
+      const double err = sqrt(sums[1]);
+      f[F_ERR] = err;
+      f[F_ITER] += 1.0;
+      const bool go = (err > op.eps) && (f[F_ITER] < (double)op.max_iter);
+      f[F_DONE] = go ? 0.0 : 1.0;
+      if (op.hist && (int)f[F_ITER] <= op.hist_cap) op.hist[(int)f[F_ITER] - 1] = err;
+      break;
+    }
+    case OP_NULL_C:       // c = (w.x)/nunique into frame slot
+      f[F_C] = sums[0] / op.nunique;
+      break;
+    case OP_FCG_BETA:     // beta_k = sums[k] / pap[k]
+      for (int k = 0; k < op.m; ++k) f[F_FBETA + k] = sums[k] / f[F_FPAP + op.pap_idx[k]];
+      break;
+    case OP_FCG_ALPHA:    // pap0 and alpha = (p0 w).r / pap0
+      f[F_FPAP + op.pap_idx[0]] = sums[0];
+      f[F_ALPHA] = sums[1] / sums[0];
+      break;
+    case OP_FCG_ERR: {
+      const double err = sqrt(sums[0]);
+      f[F_ERR] = err;
+      f[F_ITER] += 1.0;
+      const bool go = (err > op.eps) && (f[F_ITER] < (double)op.max_iter);
+      f[F_DONE] = go ? 0.0 : 1.0;
+      if (op.hist && (int)f[F_ITER] <= op.hist_cap) op.hist[(int)f[F_ITER] - 1] = err;
+      break;
+    }
+    case OP_ERR0:
+      f[F_ERR0] = sqrt(sums[0]);
+      f[F_ITER] = 0.0;
+      f[F_DONE] = 0.0;
+      f[F_ERR] = sqrt(sums[0]);
+      break;
+    case OP_STORE_PAP:
+      f[F_PAP] = sums[0];
+      break;
+    case OP_CG_INIT_RDZ_ALPHA:
+      f[F_RDZ] = sums[0];
+      f[F_ERR0] = sqrt(sums[1]);
+      f[F_ITER] = 0.0;
+      f[F_DONE] = 0.0;
+      f[F_ERR] = sqrt(sums[1]);
+      f[F_ALPHA] = sums[0] / f[F_PAP];
+      break;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// end of a reducing kernel: thread 0 holds the block's NQ partial sums.  They
+// are stored at part[q * gridDim.x + block]; when op.counter is set, the
+// last block to arrive sums all partials in index order (so the result does
+// not depend on which block is last), stores them in op.sums, applies the
+// solver scalar algebra and re-arms the counter.
+// ---------------------------------------------------------------------------
+template <int NQ>
+__device__ __forceinline__ void finish(const double (&v)[NQ], double* __restrict__ part,
+                                       const ScalarOp& op, double* sred) {
+  __shared__ int s_last;
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) part[q * gridDim.x + blockIdx.x] = v[q];
+    s_last = 0;
+    if (op.counter) {
+      // release: this block's partials are visible before its arrival
+      // counts; acquire: the last block sees every partial
+      cuda::atomic_ref<unsigned, cuda::thread_scope_device> arrived(*op.counter);
+      const unsigned prev = arrived.fetch_add(1u, cuda::memory_order_acq_rel);
+      s_last = prev == gridDim.x - 1;
+    }
+  }
+  __syncthreads();
+  if (!s_last) return;
+  double s[NQ];
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+    s[q] = 0.0;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x)
+      s[q] += __ldcg(part + (size_t)q * gridDim.x + b);
+  }
+  block_reduce<NQ>(s, sred);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) op.sums[q] = s[q];
+    apply_scalar_op(op, op.sums);
+    *op.counter = 0u;
+  }
+}
+
+
+// One value per thread of a block of any shape (flat index tid < nthr <=
+// 256): block sum in a fixed order, then finish<1>'s last-block protocol.
+__device__ __forceinline__ void finish_flat(double v, int tid, int nthr,
+                                            double* __restrict__ part, const ScalarOp& op,
+                                            double* sflat) {
+  __shared__ int s_last;
+  auto block_sum = [&](double x) -> double {
+    sflat[tid] = x;
+    __syncthreads();
+    double t = 0.0;
+    if (tid < 32) {
+      for (int q = tid; q < nthr; q += 32) t += sflat[q];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+    }
+    __syncthreads();
+    return t;   // valid in tid 0
+  };
+  const double b = block_sum(v);
+  if (tid == 0) {
+    part[blockIdx.x] = b;
+    s_last = 0;
+    if (op.counter) {
+      cuda::atomic_ref<unsigned, cuda::thread_scope_device> arrived(*op.counter);
+      const unsigned prev = arrived.fetch_add(1u, cuda::memory_order_acq_rel);
+      s_last = prev == gridDim.x - 1;
+    }
+  }
+  __syncthreads();
+  if (!s_last) return;
+  double x = 0.0;
+  for (int q = tid; q < (int)gridDim.x; q += nthr) x += __ldcg(part + q);
+  const double total = block_sum(x);
+  if (tid == 0) {
+    op.sums[0] = total;
+    apply_scalar_op(op, op.sums);
+    *op.counter = 0u;
+  }
+}
+
 
 }  // namespace dev
 }  // namespace ssg

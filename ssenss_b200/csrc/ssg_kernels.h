@@ -18,7 +18,9 @@ enum OpCode {
   OP_FCG_BETA,      // beta_k = (z w).ap_k / pap_k
   OP_FCG_ALPHA,     // pap_0, alpha = (p0 w).r / pap_0
   OP_FCG_ERR,       // err, iteration count, done flag
-  OP_ERR0           // initial residual norm
+  OP_ERR0,          // initial residual norm
+  OP_STORE_PAP,     // pap = sum (first CG iteration: rdz comes next)
+  OP_CG_INIT_RDZ_ALPHA   // OP_CG_INIT_RDZ, then alpha = rdz / pap
 };
 
 // slots of one solver frame (doubles)
@@ -52,8 +54,19 @@ struct PtrList {
                        nullptr, nullptr, nullptr, nullptr, nullptr};
 };
 
-// DSS epilogue modes (kernels.cu)
-enum { DSS_PLAIN = 0, DSS_DOT = 1, DSS_RESID = 2, DSS_AVG = 3, DSS_DOT2 = 4 };
+// DSS epilogue modes (kernels.cu); DSS_CGUPD: the gathered ap feeds the CG
+// update x += alpha p, r -= alpha ap, z = dinv r with its four partial sums
+enum { DSS_PLAIN = 0, DSS_DOT = 1, DSS_RESID = 2, DSS_AVG = 3, DSS_DOT2 = 4, DSS_CGUPD = 5 };
+
+// vectors of the DSS_CGUPD epilogue (storage type of the level)
+struct DssCg {
+  void* x = nullptr;
+  const void* p = nullptr;
+  void* r = nullptr;
+  const void* dinv = nullptr;
+  void* z = nullptr;
+  const double* alpha = nullptr;
+};
 
 // CG direction update fused into the operator: p = (beta p + (z - c)) .* mask
 struct PUpdateArgs {
@@ -63,6 +76,10 @@ struct PUpdateArgs {
   const double* mask = nullptr;
   const double* stop = nullptr;
   int first = 0;
+  // set: the operator also reduces p . (A p) (unweighted; for a continuous p
+  // this is the weighted (p w).DSS(A p)) and applies *dot to the sum
+  const ScalarOp* dot = nullptr;
+  double* part = nullptr;
 };
 
 // kernel launches of this library: process-wide, and per host thread (the
@@ -90,7 +107,8 @@ extern int g_tune_ax_kind[];
 namespace dev { struct PUpdate; }
 cudaError_t run_ax8_dmma(cudaStream_t s, int nel, bool helm, bool fp32, void* u, void* au,
                          const void* gf, size_t npts, const double* bj, const double* D,
-                         const double* S, double lambda, const dev::PUpdate* pu);
+                         const double* S, double lambda, const dev::PUpdate* pu,
+                         const ScalarOp* dop);
 
 cudaError_t run_ax(cudaStream_t s, int n, int nel, int epb, bool helm, bool fp32,
                    const void* in, void* out, const void* gf, size_t npts,
@@ -99,9 +117,8 @@ cudaError_t run_ax(cudaStream_t s, int n, int nel, int epb, bool helm, bool fp32
 // ec_tab: ordered edge/corner source table of order n (dss_ec_table)
 cudaError_t run_dss(cudaStream_t s, int mode, bool fp32, int n, int nel, const void* in,
                     void* out, const int* pairs, const int* ec_tab, const double* mask,
-                    const void* y,
-                    const void* y2, double* part, const double* stop = nullptr,
-                    const ScalarOp* op = nullptr);
+                    const void* y, const void* y2, double* part, const double* stop = nullptr,
+                    const ScalarOp* op = nullptr, const DssCg* cg = nullptr);
 cudaError_t run_tensor3(cudaStream_t s, bool fp32, bool add, int nel, int ni, int no,
                         const double* A, const void* in, void* out);
 cudaError_t run_cg_update(cudaStream_t s, bool fp32, size_t npts, const double* alpha,
