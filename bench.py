@@ -43,9 +43,10 @@ EPS = 1e-10
 # dominant kernel: the level-0 element operator (Laplacian), bytes per local
 # point: read u (8) + six G*rho*J factors (48) + write (8)
 OP_BYTES_PER_POINT = 64
-# DRAM bytes per launch of that kernel from the committed ncu capture
-# (profiles/), None until captured
-OP_TRAFFIC_BYTES = None
+# DRAM bytes per launch of that kernel (dram__bytes_read.sum +
+# dram__bytes_write.sum) from the ncu capture of the same workload
+# summarised in profiles/k_ax8_dmma_tgv16_n8.md
+OP_TRAFFIC_BYTES = 117469952 + 4272384
 
 
 def parse():
@@ -760,7 +761,8 @@ def run_ours(args):
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 2 * 8 * npts,
                 "d2h_bytes_per_step": 8 * npts, "ms_per_step": ms_e2e / ke},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": OP_TRAFFIC_BYTES,
+                     "frac": achieved / peak,
+                     "traffic": OP_TRAFFIC_BYTES if (n == 8 and args.ne == NE) else None,
                      "kernel": ("k_ax8_dmma<double> (level-0 Laplacian, FP64 DMMA)"
                                 if n == 8 else f"k_ax<{n},double> (level-0 Laplacian)"),
                      "us_per_launch": op_ms * 1e3,

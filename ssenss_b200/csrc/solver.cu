@@ -200,12 +200,19 @@ ssg_status cg_solve(ssg_context* c, int level, int var, bool fp32, void* f, void
   // all of them for a smoother (sync_each false), chunks of 8 otherwise.
   const double* stop = fr + F_DONE;
   pu.stop = stop;
-  // (p w).DSS(mask A p) = p . (mask A p) for a continuous, masked p: the
-  // operator kernel reduces it, so alpha is known before the DSS, and the
-  // DSS gather feeds the update directly (ap is never stored)
+  // Mixed precision (FP32 storage): (p w).DSS(mask A p) = p . (mask A p)
+  // for a continuous, masked p, so the operator kernel reduces it, alpha is
+  // known before the DSS, and the DSS gather feeds the update directly (two
+  // kernels per iteration, ap never stored).  FP64 keeps the reference's
+  // arithmetic: alpha from the weighted dot of the assembled ap
+  // (src/solver.c:62-65), then the update -- the rounding of the fused form
+  // moves a well-converged solution by a few 1e-11.
+  const bool fused = fp32;
   ScalarOp dop = op;
-  pu.dot = &dop;
-  pu.part = c->d_part;
+  if (fused) {
+    pu.dot = &dop;
+    pu.part = c->d_part;
+  }
   DssCg cg;
   cg.x = x;
   cg.p = W.p;
@@ -214,24 +221,35 @@ ssg_status cg_solve(ssg_context* c, int level, int var, bool fp32, void* f, void
   cg.z = W.z;
   cg.alpha = fr + F_ALPHA;
   for (int it = 0; it < max_iter; ++it) {
-    // p = beta p + (z - c) (first: p = z - c), masked; aploc = A p;
-    // pap = p . aploc and alpha = rdz / pap (first: pap only)
+    // p = beta p + (z - c) (first: p = z - c), masked; aploc = A p
+    // (fused: pap = p . aploc and alpha = rdz / pap; first: pap only)
     pu.first = it == 0;
     dop.code = it == 0 ? OP_STORE_PAP : OP_CG_ALPHA;
     SSG_CUDA(c, run_ax(s, L.n, c->nel, 0, helm, fp32, W.p, W.aploc, gf, np, L.bj, L.D, L.S,
                        lam, &pu));
     if (it == 0) {
-      // rdz = (r w).p, |r|_w (src/solver.c:58-61), alpha
+      // rdz = (r w).p, |r|_w (src/solver.c:58-61) (fused: and alpha)
       PtrList ys;
       ys.p[0] = W.p;
       ys.p[1] = W.r;
-      op.code = OP_CG_INIT_RDZ_ALPHA;
+      op.code = fused ? OP_CG_INIT_RDZ_ALPHA : OP_CG_INIT_RDZ;
       SSG_CUDA(c, run_dots(s, fp32, np, W.r, ys, 2, L.mult, c->d_part, nb, &op));
     }
-    // ap = DSS(mask aploc); x += alpha p; r -= alpha ap; z = M^-1 r; beta; err
-    op.code = OP_CG_BETA;
-    SSG_CUDA(c, run_dss(s, DSS_CGUPD, fp32, L.n, c->nel, W.aploc, nullptr, c->d_pairs,
-                        L.dss_ec, mask, nullptr, nullptr, c->d_part, stop, &op, &cg));
+    if (fused) {
+      // ap = DSS(mask aploc); x += alpha p; r -= alpha ap; z = M^-1 r; beta; err
+      op.code = OP_CG_BETA;
+      SSG_CUDA(c, run_dss(s, DSS_CGUPD, fp32, L.n, c->nel, W.aploc, nullptr, c->d_pairs,
+                          L.dss_ec, mask, nullptr, nullptr, c->d_part, stop, &op, &cg));
+    } else {
+      // ap = DSS(mask aploc); alpha = rdz / (p w).ap
+      op.code = OP_CG_ALPHA;
+      SSG_CUDA(c, run_dss(s, DSS_DOT, fp32, L.n, c->nel, W.aploc, W.ap, c->d_pairs, L.dss_ec,
+                          mask, W.p, nullptr, c->d_part, stop, &op));
+      // x += alpha p; r -= alpha ap; z = M^-1 r; beta; err
+      op.code = OP_CG_BETA;
+      SSG_CUDA(c, run_cg_update(s, fp32, np, fr + F_ALPHA, x, W.p, W.r, W.ap, dinv, L.mult,
+                                W.z, c->d_part, nb, stop, &op));
+    }
     if (sync_each && (it % 8 == 7)) {
       double done;
       SSG_TRY(read_flag(c, fr + F_DONE, &done));
