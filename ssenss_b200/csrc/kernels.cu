@@ -221,11 +221,26 @@ __global__ void __launch_bounds__(256) k_dss(int nel, int epb, const T* __restri
   constexpr int ID = I > 0 ? I : 1, II = ID * ID;   // divisors (N = 2 has no
                                                     // face or interior nodes)
   if (stop && *stop != 0.0) return;   // uniform over the block
+  constexpr int ECI = 12 * I;
   __shared__ short sface[6 * NN];     // node of face f at face position p
+  // class of every node in natural order: 0 interior; 1<<16 | f<<8 | pos a
+  // face interior; 2<<16 | record an edge node, 3<<16 | record a corner
+  __shared__ int scls[NT];
   __shared__ double sred[2 * 32];
   __shared__ double sred4[MODE == DSS_CGUPD ? 4 * 32 : 1];
   for (int q = threadIdx.x; q < 6 * NN; q += blockDim.x)
     sface[q] = (short)face_node(N, q / NN, (q % NN) / N, q % N);
+  for (int tc = threadIdx.x; tc < NT; tc += blockDim.x) {
+    int code = 0;
+    if (tc < F) {
+      const int f = tc / II, r = tc - f * II;
+      code = (1 << 16) | (f << 8) | ((1 + r / ID) * N + 1 + r % ID);
+    } else if (tc < F + EC) {
+      const int c = tc - F;
+      code = c < ECI ? ((2 << 16) | c) : ((3 << 16) | (ECI + 2 * (c - ECI)));
+    }
+    scls[class_ordered_node<N>(tc)] = code;
+  }
   __syncthreads();
   (void)epb;
   double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
@@ -241,15 +256,15 @@ __global__ void __launch_bounds__(256) k_dss(int nel, int epb, const T* __restri
   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < ntask;
        q += (size_t)gridDim.x * blockDim.x) {
     {
+      // nodes in natural order: a warp's own loads and stores are coalesced
       const int e = (int)(q / NT), t = (int)(q - (size_t)e * NT);
       const size_t eb = (size_t)e * NT;
-      int loc, cnt = 0;
+      const int loc = t, code = scls[t], kind = code >> 16;
+      int cnt = 0;
       double acc;
-      if (t < F) {
+      if (kind == 1) {
         // face interior: own value plus the one neighbour face copy
-        const int f = t / II, r = t - f * II;
-        const int pos = (1 + r / ID) * N + 1 + r % ID;
-        loc = sface[f * NN + pos];
+        const int f = (code >> 8) & 0xff, pos = code & 0xff;
         const int2 p = __ldg(pairs + (size_t)e * 26 + f);
         acc = (double)in[eb + loc];
         if (mask) acc = acc * mask[eb + loc];
@@ -260,17 +275,13 @@ __global__ void __launch_bounds__(256) k_dss(int nel, int epb, const T* __restri
           acc += v;
           cnt = 1;
         }
-      } else if (t < F + EC) {
+      } else if (kind >= 2) {
         // edges and corners: the ordered source lists of the set-up table
         // (3 sources per edge node, 7 per corner node, -1 = none)
-        loc = class_ordered_node<N>(t);
-        const int c = t - F;
-        constexpr int ECI = 12 * I;
-        const int4* rec = ec + (size_t)e * (ECI + 16) +
-                          (c < ECI ? c : ECI + 2 * (c - ECI));
+        const int4* rec = ec + (size_t)e * (ECI + 16) + (code & 0xffff);
         const int4 a = __ldg(rec);
         int4 b = make_int4(-1, -1, -1, -1);
-        if (c >= ECI) b = __ldg(rec + 1);
+        if (kind == 3) b = __ldg(rec + 1);
         acc = (double)in[eb + loc];
         if (mask) acc = acc * mask[eb + loc];
         const int src[7] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z};
@@ -291,8 +302,6 @@ __global__ void __launch_bounds__(256) k_dss(int nel, int epb, const T* __restri
           }
       } else {
         // element interior: no neighbour shares the node
-        const int u = t - F - EC;
-        loc = ((1 + u / II) * N + 1 + (u / ID) % ID) * N + 1 + u % ID;
         acc = (double)in[eb + loc];
         if (mask) acc = acc * mask[eb + loc];
       }
