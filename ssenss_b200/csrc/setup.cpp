@@ -150,13 +150,18 @@ static void alloc_level(HostLevel& L, int n, int nel, bool full) {
   L.n = n;
   L.nt = (size_t)n * n * n;
   const size_t len = L.nt * nel;
-  for (auto& a : L.g) a.assign(len, 0.0);
-  L.det.assign(len, 0.0);
-  for (auto& a : L.grid) a.assign(len, 0.0);
+  std::vector<std::vector<double>*> arrays;
+  for (auto& a : L.g) arrays.push_back(&a);
+  arrays.push_back(&L.det);
+  for (auto& a : L.grid) arrays.push_back(&a);
   if (full) {
-    for (auto& a : L.jac) a.assign(len, 0.0);
-    for (auto& a : L.tinv) a.assign(len, 0.0);
+    for (auto& a : L.jac) arrays.push_back(&a);
+    for (auto& a : L.tinv) arrays.push_back(&a);
   }
+  // zero-filled in parallel (one host thread per array)
+  std::vector<std::thread> th;
+  for (auto* a : arrays) th.emplace_back([a, len] { a->assign(len, 0.0); });
+  for (auto& t : th) t.join();
 }
 
 // Jacobian from the grid, determinant by first-row cofactors, inverse by
@@ -166,9 +171,14 @@ static void alloc_level(HostLevel& L, int n, int nel, bool full) {
 static void compute_factors(HostLevel& L, int nel, bool keep_jac) {
   const int n = L.n;
   const size_t nt = L.nt;
-  std::vector<double> jac[9];
-  for (auto& a : jac) a.assign(nt * nel, 0.0);
+  static const int k0[3] = {1, 0, 0}, k1[3] = {2, 2, 1}, k2[3] = {2, 0, 1}, k3[3] = {1, 2, 0};
+  static const double sg[3] = {1.0, -1.0, 1.0};
+  // one element at a time per thread: its Jacobian in a local buffer, then
+  // the per-point algebra
   parallel_elements(nel, [&](int e0, int e1) {
+  std::vector<double> jbuf(9 * nt);
+  double* jac[9];
+  for (int a = 0; a < 9; ++a) jac[a] = jbuf.data() + a * nt;
   for (int e = e0; e < e1; ++e) {
     const size_t o = e * nt;
     for (int a = 0; a < 3; ++a) {
@@ -182,21 +192,17 @@ static void compute_factors(HostLevel& L, int nel, bool keep_jac) {
               ss += L.D[j * n + m] * g[(k * n + m) * n + i];
               st += L.D[k * n + m] * g[(m * n + j) * n + i];
             }
-            const size_t q = o + (k * n + j) * n + i;
+            const size_t q = (k * n + j) * n + i;
             jac[3 * a + 0][q] = sr;
             jac[3 * a + 1][q] = ss;
             jac[3 * a + 2][q] = st;
           }
     }
-  }
-  });
-  static const int k0[3] = {1, 0, 0}, k1[3] = {2, 2, 1}, k2[3] = {2, 0, 1}, k3[3] = {1, 2, 0};
-  static const double sg[3] = {1.0, -1.0, 1.0};
-  parallel_elements(nel, [&](int e0, int e1) {
-  for (size_t q = e0 * nt; q < e1 * nt; ++q) {
+  for (size_t ql = 0; ql < nt; ++ql) {
+    const size_t q = o + ql;
     double a[3][3], ai[3][3];
     for (int r = 0; r < 3; ++r)
-      for (int c = 0; c < 3; ++c) a[r][c] = jac[3 * r + c][q];
+      for (int c = 0; c < 3; ++c) a[r][c] = jac[3 * r + c][ql];
     double det = 0.0;
     for (int i = 0; i < 3; ++i) {
       const int j = (2 - i) / 2, k = 3 - i - j;
@@ -231,6 +237,7 @@ static void compute_factors(HostLevel& L, int nel, bool keep_jac) {
           L.jac[3 * r + c][q] = a[r][c];
           L.tinv[3 * r + c][q] = ai[c][r];
         }
+  }
   }
   });
 }
@@ -457,7 +464,7 @@ ssg_status build_mesh(HostMesh& m, int n, int nel, const double* vert, const int
   m.nlev = level_orders(n, orders);
   const int msvv = 2 * n / 3;
   for (int l = 0; l < m.nlev; ++l) {
-    alloc_level(m.lev[l], orders[l], nel, l == 0);
+    alloc_level(m.lev[l], orders[l], nel, l == 0 && !(opts & SSG_SETUP_NO_PARTICLES));
     make_basis(m.lev[l], orders[l], msvv, 0.0);
   }
   const bool particles = !(opts & SSG_SETUP_NO_PARTICLES);
