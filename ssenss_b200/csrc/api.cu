@@ -271,11 +271,12 @@ static ssg_status upload_all(ssg_context* c) {
   SSG_TRY(dupload(c, &c->d_neigh, H.neigh.data(), H.neigh.size()));
   SSG_TRY(dalloc(c, &c->d_passes, 1));
   // reduction partials: enough for 10 dot products over the largest grid
-  // sized for the largest grids the autotuner may pick: 32 blocks per SM
-  // for the vector kernels (up to 16 partial sums each), 16 for the DSS
-  const size_t vb = std::min((np0 + 255) / 256, (size_t)148 * 32);
-  const size_t db = (size_t)148 * 16;
-  c->part_cap = std::max(16 * vb, 2 * db) + 64;
+  // sized for the largest grids the autotuner may pick: 64 blocks per SM
+  // for the vector kernels (up to 16 partial sums each) and for the DSS (up
+  // to 4)
+  const size_t vb = std::min((np0 + 255) / 256, (size_t)148 * 64);
+  const size_t db = (size_t)148 * 64;
+  c->part_cap = std::max(16 * vb, 4 * db) + 64;
   SSG_TRY(dalloc(c, &c->d_part, c->part_cap));
   // staging for host arguments: up to three vector fields
   // (one field unless the dealiasing grid is set up: convection stages

@@ -641,10 +641,11 @@ int ax_epb_max(int n) {
   return epb;
 }
 
-// grid of the vector kernels: four points per thread in one pass where the
-// cap (bps blocks per SM) allows; beyond it the kernels loop grid-stride
+// grid of the vector kernels: one point per thread up to the cap of bps
+// blocks per SM (latency is hidden by resident warps); beyond it the
+// kernels loop grid-stride with four points in flight per thread
 int vec_blocks(size_t npts) {
-  size_t b = (npts + 1023) / 1024;
+  size_t b = (npts + 255) / 256;
   const size_t cap = (size_t)148 * (g_tune_vec_bps > 0 ? g_tune_vec_bps : 32);
   return (int)(b < cap ? (b ? b : 1) : cap);
 }
@@ -751,7 +752,7 @@ int dss_epb(int n) {
 int dss_grid(int n, int nel) {
   const size_t tasks = (size_t)nel * n * n * n;
   const size_t g = (tasks + 255) / 256;
-  const int bps = (n >= 0 && n <= SSG_MAXN && g_tune_dss_bps[n] > 0) ? g_tune_dss_bps[n] : 8;
+  const int bps = (n >= 0 && n <= SSG_MAXN && g_tune_dss_bps[n] > 0) ? g_tune_dss_bps[n] : 64;
   const size_t cap = (size_t)148 * bps;
   return (int)(g < cap ? (g ? g : 1) : cap);
 }

@@ -115,8 +115,8 @@ size_t estimate_bytes(int n, int nel, int precision) {
   b += np0 * (8 + 8 + 8);                  // inverse mass, det J, workspace scratch
   b += np0 * 4 * 8;                        // staging (one field per slot)
   b += np0 * 24 * 8;                       // FCG: r, z, A p local, 11 + 10 directions
-  const size_t vb = std::min((np0 + 255) / 256, (size_t)148 * 32);
-  b += (std::max(16 * vb, (size_t)2 * 148 * 16) + 64) * 8;   // reduction partials
+  const size_t vb = std::min((np0 + 255) / 256, (size_t)148 * 64);
+  b += (std::max(16 * vb, (size_t)4 * 148 * 64) + 64) * 8;   // reduction partials
   b += 8192 * 8 + (1 << 20);               // history, small buffers
   return b;
 }

@@ -5,8 +5,10 @@
 //   * elements per block of the shared-memory operator (k_ax: 1, 2, 4, ...
 //     up to the 256-thread / 96 KB limit of ax_epb_max(n)); order 8 runs the
 //     FP64 tensor-core operator k_ax8_dmma, which has no shape parameter;
-//   * blocks per SM of the persistent DSS grid: 1 .. 16;
-//   * blocks per SM of the grid-stride vector kernels: 2 .. 32.
+//   * the cap of the DSS grid (one node per thread below it): 4 .. 64
+//     blocks per SM;
+//   * the cap of the vector kernels' grid (one point per thread below it):
+//     8 .. 64 blocks per SM.
 // ssg_autotune times every candidate on the context's own mesh and levels
 // (CUDA events on the context stream, best of three runs of ten launches)
 // and keeps the fastest in the process-wide tables the launchers read.  The
@@ -72,7 +74,7 @@ static ssg_status tune_level(ssg_context* c, int level, double* a, double* b, do
   {
     int best_bps = 0;
     float best = 1e30f;
-    for (int bps = 1; bps <= 16; bps *= 2) {
+    for (int bps = 4; bps <= 64; bps *= 2) {
       g_tune_dss_bps[n] = bps;
       float t = 0.f;
       SSG_TRY(time_launches(c, reps, [&] {
@@ -127,7 +129,7 @@ ssg_status ssg_autotune(ssg_context* c, int reps) {
     PtrList ys;
     ys.p[0] = buf[1];
     ys.p[1] = buf[2];
-    for (int bps = 2; bps <= 32 && st == SSG_OK; bps *= 2) {
+    for (int bps = 8; bps <= 64 && st == SSG_OK; bps *= 2) {
       g_tune_vec_bps = bps;
       const int nb = vec_blocks(np0);
       float t = 0.f;
@@ -177,7 +179,7 @@ ssg_status ssg_tuning(int n, int* ax_elements_per_block, int* dss_blocks_per_sm,
   // 0: the FP64 tensor-core operator (one warp per element)
   const bool dmma = n == 8;
   if (ax_elements_per_block) *ax_elements_per_block = dmma ? 0 : ax_epb(n);
-  if (dss_blocks_per_sm) *dss_blocks_per_sm = g_tune_dss_bps[n] > 0 ? g_tune_dss_bps[n] : 8;
+  if (dss_blocks_per_sm) *dss_blocks_per_sm = g_tune_dss_bps[n] > 0 ? g_tune_dss_bps[n] : 64;
   if (vector_blocks_per_sm) *vector_blocks_per_sm = g_tune_vec_bps > 0 ? g_tune_vec_bps : 32;
   return SSG_OK;
 }
