@@ -240,7 +240,7 @@ static ssg_status upload_all(ssg_context* c) {
     }
     {
       std::vector<int> ec;
-      dss_ec_table(H, h.n, ec);
+      dss_map_table(H, h.n, ec);
       SSG_TRY(dupload(c, &d.dss_ec, ec.data(), ec.size()));
     }
     SSG_TRY(dupload(c, &d.D, h.D.data(), h.D.size()));

@@ -209,7 +209,7 @@ template <int N, typename T, int MODE>
 __global__ void __launch_bounds__(256) k_dss(int nel, int epb, const T* __restrict__ in,
                                              T* __restrict__ out,
                                              const int2* __restrict__ pairs,
-                                             const int4* __restrict__ ec,
+                                             const int* __restrict__ map,
                                              const double* __restrict__ mask,
                                              const T* __restrict__ y,
                                              const T* __restrict__ y2,
@@ -217,31 +217,17 @@ __global__ void __launch_bounds__(256) k_dss(int nel, int epb, const T* __restri
                                              const double* __restrict__ stop, ScalarOp op,
                                              DssCg cg) {
   constexpr int NT = N * N * N, NN = N * N;
-  constexpr int I = N > 2 ? N - 2 : 0, F = 6 * I * I, EC = 12 * I + 8;
-  constexpr int ID = I > 0 ? I : 1, II = ID * ID;   // divisors (N = 2 has no
-                                                    // face or interior nodes)
+  constexpr int I = N > 2 ? N - 2 : 0, ECI = 12 * I;
   if (stop && *stop != 0.0) return;   // uniform over the block
-  constexpr int ECI = 12 * I;
-  __shared__ short sface[6 * NN];     // node of face f at face position p
-  // class of every node in natural order: 0 interior; 1<<16 | f<<8 | pos a
-  // face interior; 2<<16 | record an edge node, 3<<16 | record a corner
-  __shared__ int scls[NT];
+  // the order's DSS map, built once at set-up (dss_map_table): the class of
+  // every node in natural order (0 interior; 1<<16 | f<<8 | pos a face
+  // interior; 2<<16 | record an edge node, 3<<16 | record a corner), the node
+  // of face f at face position pos, then the edge/corner source records
+  const int* __restrict__ scls = map;
+  const short* __restrict__ sface = reinterpret_cast<const short*>(map + NT);
+  const int4* __restrict__ ec = reinterpret_cast<const int4*>(map + dss_map_header(N));
   __shared__ double sred[2 * 32];
   __shared__ double sred4[MODE == DSS_CGUPD ? 4 * 32 : 1];
-  for (int q = threadIdx.x; q < 6 * NN; q += blockDim.x)
-    sface[q] = (short)face_node(N, q / NN, (q % NN) / N, q % N);
-  for (int tc = threadIdx.x; tc < NT; tc += blockDim.x) {
-    int code = 0;
-    if (tc < F) {
-      const int f = tc / II, r = tc - f * II;
-      code = (1 << 16) | (f << 8) | ((1 + r / ID) * N + 1 + r % ID);
-    } else if (tc < F + EC) {
-      const int c = tc - F;
-      code = c < ECI ? ((2 << 16) | c) : ((3 << 16) | (ECI + 2 * (c - ECI)));
-    }
-    scls[class_ordered_node<N>(tc)] = code;
-  }
-  __syncthreads();
   (void)epb;
   double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
   const double alpha = MODE == DSS_CGUPD ? *cg.alpha : 0.0;
@@ -259,7 +245,7 @@ __global__ void __launch_bounds__(256) k_dss(int nel, int epb, const T* __restri
       // nodes in natural order: a warp's own loads and stores are coalesced
       const int e = (int)(q / NT), t = (int)(q - (size_t)e * NT);
       const size_t eb = (size_t)e * NT;
-      const int loc = t, code = scls[t], kind = code >> 16;
+      const int loc = t, code = __ldg(scls + t), kind = code >> 16;
       int cnt = 0;
       double acc;
       if (kind == 1) {
@@ -269,7 +255,7 @@ __global__ void __launch_bounds__(256) k_dss(int nel, int epb, const T* __restri
         acc = (double)in[eb + loc];
         if (mask) acc = acc * mask[eb + loc];
         if (p.x >= 0) {
-          const size_t src = (size_t)p.x * NT + sface[p.y * NN + pos];
+          const size_t src = (size_t)p.x * NT + __ldg(sface + p.y * NN + pos);
           double v = (double)in[src];
           if (mask) v = v * mask[src];
           acc += v;
@@ -646,7 +632,7 @@ int ax_epb_max(int n) {
 // kernels loop grid-stride with four points in flight per thread
 int vec_blocks(size_t npts) {
   size_t b = (npts + 255) / 256;
-  const size_t cap = (size_t)148 * (g_tune_vec_bps > 0 ? g_tune_vec_bps : 32);
+  const size_t cap = (size_t)148 * (g_tune_vec_bps > 0 ? g_tune_vec_bps : 8);
   return (int)(b < cap ? (b ? b : 1) : cap);
 }
 
@@ -752,36 +738,36 @@ int dss_epb(int n) {
 int dss_grid(int n, int nel) {
   const size_t tasks = (size_t)nel * n * n * n;
   const size_t g = (tasks + 255) / 256;
-  const int bps = (n >= 0 && n <= SSG_MAXN && g_tune_dss_bps[n] > 0) ? g_tune_dss_bps[n] : 64;
+  const int bps = (n >= 0 && n <= SSG_MAXN && g_tune_dss_bps[n] > 0) ? g_tune_dss_bps[n] : 8;
   const size_t cap = (size_t)148 * bps;
   return (int)(g < cap ? (g ? g : 1) : cap);
 }
 
 template <int N, typename T>
 static cudaError_t run_dss_n(cudaStream_t s, int mode, int nel, const T* in, T* out,
-                             const int2* pr, const int4* ec, const double* mask, const T* y,
+                             const int2* pr, const int* ec_tab, const double* mask, const T* y,
                              const T* y2, double* part, const double* stop,
                              const ScalarOp& op, const DssCg& cg) {
   const int epb = dss_epb(N);
   const int grd = dss_grid(N, nel);
   switch (mode) {
     case DSS_PLAIN:
-      { SSG_COUNT(); k_dss<N, T, DSS_PLAIN><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, ec, mask, y, y2, part, stop, op, cg); }
+      { SSG_COUNT(); k_dss<N, T, DSS_PLAIN><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, ec_tab, mask, y, y2, part, stop, op, cg); }
       break;
     case DSS_DOT:
-      { SSG_COUNT(); k_dss<N, T, DSS_DOT><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, ec, mask, y, y2, part, stop, op, cg); }
+      { SSG_COUNT(); k_dss<N, T, DSS_DOT><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, ec_tab, mask, y, y2, part, stop, op, cg); }
       break;
     case DSS_DOT2:
-      { SSG_COUNT(); k_dss<N, T, DSS_DOT2><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, ec, mask, y, y2, part, stop, op, cg); }
+      { SSG_COUNT(); k_dss<N, T, DSS_DOT2><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, ec_tab, mask, y, y2, part, stop, op, cg); }
       break;
     case DSS_RESID:
-      { SSG_COUNT(); k_dss<N, T, DSS_RESID><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, ec, mask, y, y2, part, stop, op, cg); }
+      { SSG_COUNT(); k_dss<N, T, DSS_RESID><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, ec_tab, mask, y, y2, part, stop, op, cg); }
       break;
     case DSS_AVG:
-      { SSG_COUNT(); k_dss<N, T, DSS_AVG><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, ec, mask, y, y2, part, stop, op, cg); }
+      { SSG_COUNT(); k_dss<N, T, DSS_AVG><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, ec_tab, mask, y, y2, part, stop, op, cg); }
       break;
     case DSS_CGUPD:
-      { SSG_COUNT(); k_dss<N, T, DSS_CGUPD><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, ec, mask, y, y2, part, stop, op, cg); }
+      { SSG_COUNT(); k_dss<N, T, DSS_CGUPD><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, ec_tab, mask, y, y2, part, stop, op, cg); }
       break;
     default:
       return cudaErrorInvalidValue;
@@ -795,10 +781,9 @@ static cudaError_t run_dss_t(cudaStream_t s, int mode, int n, int nel, const T* 
                              const T* y, const T* y2, double* part, const double* stop,
                              const ScalarOp& op, const DssCg& cg) {
   const int2* pr = reinterpret_cast<const int2*>(pairs);
-  const int4* ec = reinterpret_cast<const int4*>(ec_tab);
   switch (n) {
 #define SSG_DSSN(NV) \
-  case NV: return run_dss_n<NV, T>(s, mode, nel, in, out, pr, ec, mask, y, y2, part, stop, op, cg);
+  case NV: return run_dss_n<NV, T>(s, mode, nel, in, out, pr, ec_tab, mask, y, y2, part, stop, op, cg);
     SSG_DSSN(2) SSG_DSSN(3) SSG_DSSN(4) SSG_DSSN(5) SSG_DSSN(6) SSG_DSSN(7)
     SSG_DSSN(8) SSG_DSSN(9) SSG_DSSN(10) SSG_DSSN(11) SSG_DSSN(12)
 #undef SSG_DSSN

@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "ssg_internal.h"
+#include "ssg_kernels.h"
 
 namespace ssg {
 
@@ -394,13 +395,30 @@ static void node_sources(const HostMesh& m, int n, int e, int loc, int (&src)[7]
   }
 }
 
-void dss_ec_table(const HostMesh& m, int n, std::vector<int>& tab) {
+void dss_map_table(const HostMesh& m, int n, std::vector<int>& tab) {
   const int I = n > 2 ? n - 2 : 0;
+  const int nt = n * n * n, nn = n * n;
+  const int head = dss_map_header(n);
   const size_t per = (size_t)12 * I * 4 + 8 * 8;
-  tab.assign(per * m.nel, -1);
+  tab.assign(head + per * m.nel, -1);
+  // node classes, natural order
+  for (int t = 0; t < nt; ++t) tab[t] = 0;
+  for (int f = 0; f < 6; ++f)
+    for (int a = 1; a <= I; ++a)
+      for (int b = 1; b <= I; ++b)
+        tab[face_node(n, f, a, b)] = (1 << 16) | (f << 8) | (a * n + b);
+  for (int q = 0; q < 12; ++q)
+    for (int p = 1; p <= I; ++p) tab[edge_node(n, q, p)] = (2 << 16) | (q * I + p - 1);
+  for (int c = 0; c < 8; ++c) tab[corner_node(n, c)] = (3 << 16) | (12 * I + 2 * c);
+  // face table
+  short* face = reinterpret_cast<short*>(tab.data() + nt);
+  for (int f = 0; f < 6; ++f)
+    for (int a = 0; a < n; ++a)
+      for (int b = 0; b < n; ++b) face[f * nn + a * n + b] = (short)face_node(n, f, a, b);
+  // edge / corner records
   parallel_elements(m.nel, [&](int e0, int e1) {
   for (int e = e0; e < e1; ++e) {
-    int* t = tab.data() + per * e;
+    int* t = tab.data() + head + per * e;
     int src[7];
     for (int q = 0; q < 12; ++q)
       for (int p = 1; p <= I; ++p, t += 4) {

@@ -87,11 +87,17 @@ ssg_status build_mesh(HostMesh& m, int n, int nel, const double* vertices,
 ssg_status build_pairs(HostMesh& m, std::string& err);
 void stiffness_diagonal(const HostLevel& L, int nel, double* out);
 void host_dss(const HostMesh& m, int n, double* u);
-// Per element, in the DSS kernel's node order, the ordered source lists of
-// the edge nodes (12 (n-2) records of 4 ints: 3 sources + pad) and corner
-// nodes (8 records of 8 ints: 7 sources + pad); a source is
-// element * n^3 + node, -1 where the node has none.
-void dss_ec_table(const HostMesh& m, int n, std::vector<int>& tab);
+// DSS map of order n (one int array, dss_map_header(n) ints of header):
+//   [0, n^3)          class of every node in natural order: 0 interior;
+//                     1<<16 | f<<8 | pos a face-interior node (face f,
+//                     position pos); 2<<16 | r an edge node, 3<<16 | r a
+//                     corner node (r: its record below, in int4 units)
+//   [n^3, ...)        node of face f at face position pos (6 n^2 shorts)
+//   then per element, in class order, the ordered source lists of the edge
+//   nodes (12 (n-2) records of 4 ints: 3 sources + pad) and corner nodes (8
+//   records of 8 ints: 7 sources + pad); a source is element * n^3 + node,
+//   -1 where the node has none.
+void dss_map_table(const HostMesh& m, int n, std::vector<int>& tab);
 
 // ---------------------------------------------------------------------------
 // device-side level
@@ -107,7 +113,7 @@ struct DevLevel {
   double* det = nullptr;       // det J (level 0: the Helmholtz diagonal's lambda term)
   double* rho = nullptr;       // GLL weight products rho_ijk (n^3, level 0)
   uint8_t* mult = nullptr;     // multiplicity (1 + DSS contributions)
-  int* dss_ec = nullptr;       // edge/corner DSS source table (dss_ec_table)
+  int* dss_ec = nullptr;       // DSS map of this order (dss_map_table)
   double* mask = nullptr;      // Dirichlet mask (null without walls)
   double* D = nullptr;         // n*n
   double* S = nullptr;         // n*n

@@ -8,7 +8,7 @@
 //   * the cap of the DSS grid (one node per thread below it): 4 .. 64
 //     blocks per SM;
 //   * the cap of the vector kernels' grid (one point per thread below it):
-//     8 .. 64 blocks per SM.
+//     4 .. 64 blocks per SM, timed on the CG update.
 // ssg_autotune times every candidate on the context's own mesh and levels
 // (CUDA events on the context stream, best of three runs of ten launches)
 // and keeps the fastest in the process-wide tables the launchers read.  The
@@ -103,7 +103,7 @@ ssg_status ssg_autotune(ssg_context* c, int reps) {
   if (reps <= 0) reps = 10;
   SSG_CUDA(c, cudaSetDevice(c->device));
   const size_t np0 = c->lev[0].npts;
-  std::vector<double*> buf(3, nullptr);
+  std::vector<double*> buf(6, nullptr);
   for (auto& p : buf) {
     if (cudaMalloc(&p, np0 * sizeof(double)) != cudaSuccess) {
       cudaGetLastError();
@@ -121,21 +121,18 @@ ssg_status ssg_autotune(ssg_context* c, int reps) {
     seen[n] = true;
     st = tune_level(c, l, buf[0], buf[1], buf[2], reps);
   }
-  // vector kernels: blocks per SM of the grid-stride loops (a two-vector
-  // weighted dot, read-only)
+  // vector kernels: the grid cap, timed on the heaviest of them, the CG
+  // update (x += alpha p, r -= alpha ap, z = dinv r, four partial sums)
   if (st == SSG_OK) {
     int best_bps = 0;
     float best = 1e30f;
-    PtrList ys;
-    ys.p[0] = buf[1];
-    ys.p[1] = buf[2];
-    for (int bps = 8; bps <= 64 && st == SSG_OK; bps *= 2) {
+    for (int bps = 4; bps <= 64 && st == SSG_OK; bps *= 2) {
       g_tune_vec_bps = bps;
       const int nb = vec_blocks(np0);
       float t = 0.f;
       st = time_launches(c, reps, [&] {
-        return run_dots(c->stream, false, np0, buf[0], ys, 2, c->lev[0].mult, c->d_part, nb,
-                        nullptr);
+        return run_cg_update(c->stream, false, np0, c->d_sums, buf[0], buf[1], buf[2], buf[3],
+                             buf[4], c->lev[0].mult, buf[5], c->d_part, nb, nullptr, nullptr);
       }, &t);
       if (t < best) {
         best = t;
@@ -179,8 +176,8 @@ ssg_status ssg_tuning(int n, int* ax_elements_per_block, int* dss_blocks_per_sm,
   // 0: the FP64 tensor-core operator (one warp per element)
   const bool dmma = n == 8;
   if (ax_elements_per_block) *ax_elements_per_block = dmma ? 0 : ax_epb(n);
-  if (dss_blocks_per_sm) *dss_blocks_per_sm = g_tune_dss_bps[n] > 0 ? g_tune_dss_bps[n] : 64;
-  if (vector_blocks_per_sm) *vector_blocks_per_sm = g_tune_vec_bps > 0 ? g_tune_vec_bps : 32;
+  if (dss_blocks_per_sm) *dss_blocks_per_sm = g_tune_dss_bps[n] > 0 ? g_tune_dss_bps[n] : 8;
+  if (vector_blocks_per_sm) *vector_blocks_per_sm = g_tune_vec_bps > 0 ? g_tune_vec_bps : 8;
   return SSG_OK;
 }
 
