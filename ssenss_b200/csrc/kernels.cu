@@ -239,86 +239,95 @@ __global__ void __launch_bounds__(256) k_dss(int nel, int epb, const T* __restri
   // one node task per thread, grid-stride over all elements' tasks; no
   // block-wide staging, so no barrier inside the loop
   const size_t ntask = (size_t)nel * NT;
-  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < ntask;
-       q += (size_t)gridDim.x * blockDim.x) {
-    {
+  const size_t S = (size_t)gridDim.x * blockDim.x;
+  // two node tasks in flight per thread (q and q + S): every source of both
+  // is resolved and loaded before any sum, branch-free, so their load
+  // chains (class -> pairing or record -> neighbour value) overlap
+  constexpr int U = 2;
+  for (size_t q0 = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q0 < ntask; q0 += U * S) {
+    size_t gi[U];
+    bool ok[U];
+    int src[U][7];
+    double own[U], v[U][7];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const size_t q = q0 + u * S;
+      ok[u] = q < ntask;
+      const size_t qq = ok[u] ? q : 0;
       // nodes in natural order: a warp's own loads and stores are coalesced
-      const int e = (int)(q / NT), t = (int)(q - (size_t)e * NT);
-      const size_t eb = (size_t)e * NT;
-      const int loc = t, code = __ldg(scls + t), kind = code >> 16;
-      int cnt = 0;
-      double acc;
-      if (kind == 1) {
-        // face interior: own value plus the one neighbour face copy
-        const int f = (code >> 8) & 0xff, pos = code & 0xff;
-        const int2 p = __ldg(pairs + (size_t)e * 26 + f);
-        acc = (double)in[eb + loc];
-        if (mask) acc = acc * mask[eb + loc];
-        if (p.x >= 0) {
-          const size_t src = (size_t)p.x * NT + __ldg(sface + p.y * NN + pos);
-          double v = (double)in[src];
-          if (mask) v = v * mask[src];
-          acc += v;
-          cnt = 1;
-        }
-      } else if (kind >= 2) {
-        // edges and corners: the ordered source lists of the set-up table
-        // (3 sources per edge node, 7 per corner node, -1 = none)
-        const int4* rec = ec + (size_t)e * (ECI + 16) + (code & 0xffff);
-        const int4 a = __ldg(rec);
-        int4 b = make_int4(-1, -1, -1, -1);
-        if (kind == 3) b = __ldg(rec + 1);
-        acc = (double)in[eb + loc];
-        if (mask) acc = acc * mask[eb + loc];
-        const int src[7] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z};
-        double v[7];
+      const int e = (int)(qq / NT), t = (int)(qq - (size_t)e * NT);
+      gi[u] = qq;
+      const int code = __ldg(scls + t), kind = code >> 16;
+      // face interior: one source, the neighbour face copy; edges and
+      // corners: the ordered lists of the set-up records (-1 = none)
+      int2 p = make_int2(-1, 0);
+      if (kind == 1) p = __ldg(pairs + (size_t)e * 26 + ((code >> 8) & 0xff));
+      int4 a = make_int4(-1, -1, -1, -1), b = make_int4(-1, -1, -1, -1);
+      const int4* rec = ec + (size_t)e * (ECI + 16) + (code & 0xffff);
+      if (kind >= 2) a = __ldg(rec);
+      if (kind == 3) b = __ldg(rec + 1);
+      const int fsrc = p.x >= 0 ? p.x * NT + __ldg(sface + p.y * NN + (code & 0xff)) : -1;
+      src[u][0] = kind == 1 ? fsrc : a.x;
+      src[u][1] = a.y;
+      src[u][2] = a.z;
+      src[u][3] = a.w;
+      src[u][4] = b.x;
+      src[u][5] = b.y;
+      src[u][6] = b.z;
+      own[u] = (double)in[qq];
+      if (mask) own[u] = own[u] * mask[qq];
+    }
 #pragma unroll
-        for (int m = 0; m < 7; ++m) {
-          v[m] = 0.0;
-          if (src[m] >= 0) {
-            v[m] = (double)in[src[m]];
-            if (mask) v[m] = v[m] * mask[src[m]];
-          }
+    for (int u = 0; u < U; ++u)
+#pragma unroll 7
+      for (int m = 0; m < 7; ++m) {
+        v[u][m] = 0.0;
+        if (src[u][m] >= 0) {
+          v[u][m] = (double)in[src[u][m]];
+          if (mask) v[u][m] = v[u][m] * mask[src[u][m]];
         }
-#pragma unroll
-        for (int m = 0; m < 7; ++m)
-          if (src[m] >= 0) {
-            acc += v[m];
-            ++cnt;
-          }
-      } else {
-        // element interior: no neighbour shares the node
-        acc = (double)in[eb + loc];
-        if (mask) acc = acc * mask[eb + loc];
       }
-      const size_t gi = eb + loc;
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (ok[u]) {
+      // the reference's order: own value, then the sources in slot order
+      double acc = own[u];
+      int cnt = 0;
+#pragma unroll 7
+      for (int m = 0; m < 7; ++m)
+        if (src[u][m] >= 0) {
+          acc += v[u][m];
+          ++cnt;
+        }
+      const size_t g = gi[u];
       const double w = inv_count(1u + (unsigned)cnt);
       if (MODE == DSS_CGUPD) {
         // ap = acc: x += alpha p; r -= alpha ap; z = dinv r  (src/solver.c:66-71)
-        cx[gi] = (T)((double)cx[gi] + alpha * (double)cp[gi]);
-        const T rq = (T)((double)cr[gi] + -alpha * acc);
-        cr[gi] = rq;
-        const T zq = (T)((double)rq * (double)cd[gi]);
-        cz[gi] = zq;
+        cx[g] = (T)((double)cx[g] + alpha * (double)cp[g]);
+        const T rq = (T)((double)cr[g] + -alpha * acc);
+        cr[g] = rq;
+        const T zq = (T)((double)rq * (double)cd[g]);
+        cz[g] = zq;
         const double rw = (double)rq * w;
         s0 += rw * (double)zq;
         s1 += rw * (double)rq;
         s2 += w * (double)zq;
         s3 += rw;
       } else if (MODE == DSS_RESID) {
-        const T rv = (T)((double)y[gi] + -acc);
-        out[gi] = rv;
+        const T rv = (T)((double)y[g] + -acc);
+        out[g] = rv;
         s0 += (double)rv * w;
       } else if (MODE == DSS_AVG) {
-        out[gi] = (T)(acc * w);
+        out[g] = (T)(acc * w);
       } else {
         const T av = (T)acc;
-        out[gi] = av;
+        out[g] = av;
         if (MODE == DSS_DOT || MODE == DSS_DOT2) {
-          const double yw = (double)y[gi] * w;
+          const double yw = (double)y[g] * w;
           s0 += yw * (double)av;
-          if (MODE == DSS_DOT2) s1 += yw * (double)y2[gi];
+          if (MODE == DSS_DOT2) s1 += yw * (double)y2[g];
         }
+      }
       }
     }
   }
@@ -408,20 +417,22 @@ __global__ void __launch_bounds__(256) k_recip(size_t npts, double* __restrict__
 //   x += alpha p; r -= alpha ap; z = dinv .* r
 // partials: (r w).z, (r w).r, w.z, w.r
 // Grid-stride loops with four points in flight per thread: the loads of
-// points q, q + S, q + 2S, q + 3S (S = grid stride) are issued before any of
-// them is used, then the tail runs one point at a time.  Each thread's
+// points q, q + S, q + 2S, q + 3S (S = grid stride; those past the end
+// predicated off) are issued before any of them is used.  Each thread's
 // partial sums follow that fixed visiting order (deterministic).
 #define SSG_U4_LOOP(q, n, LOAD, USE)                                            \
   {                                                                            \
     const size_t S_ = (size_t)gridDim.x * blockDim.x;                          \
-    size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x;                  \
-    for (; q + 3 * S_ < (n); q += 4 * S_) {                                    \
-      _Pragma("unroll") for (int u_ = 0; u_ < 4; ++u_) { LOAD(u_, q + u_ * S_) } \
-      _Pragma("unroll") for (int u_ = 0; u_ < 4; ++u_) { USE(u_, q + u_ * S_) }  \
-    }                                                                          \
-    for (; q < (n); q += S_) {                                                 \
-      LOAD(0, q)                                                               \
-      USE(0, q)                                                                \
+    for (size_t q0_ = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q0_ < (n); \
+         q0_ += 4 * S_) {                                                      \
+      _Pragma("unroll") for (int u_ = 0; u_ < 4; ++u_) {                       \
+        const size_t q = q0_ + u_ * S_;                                        \
+        if (q < (n)) { LOAD(u_, q) }                                           \
+      }                                                                        \
+      _Pragma("unroll") for (int u_ = 0; u_ < 4; ++u_) {                       \
+        const size_t q = q0_ + u_ * S_;                                        \
+        if (q < (n)) { USE(u_, q) }                                            \
+      }                                                                        \
     }                                                                          \
   }
 
@@ -632,7 +643,7 @@ int ax_epb_max(int n) {
 // kernels loop grid-stride with four points in flight per thread
 int vec_blocks(size_t npts) {
   size_t b = (npts + 255) / 256;
-  const size_t cap = (size_t)148 * (g_tune_vec_bps > 0 ? g_tune_vec_bps : 8);
+  const size_t cap = (size_t)148 * (g_tune_vec_bps > 0 ? g_tune_vec_bps : 4);
   return (int)(b < cap ? (b ? b : 1) : cap);
 }
 

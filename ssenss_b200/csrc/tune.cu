@@ -8,7 +8,7 @@
 //   * the cap of the DSS grid (one node per thread below it): 4 .. 64
 //     blocks per SM;
 //   * the cap of the vector kernels' grid (one point per thread below it):
-//     4 .. 64 blocks per SM, timed on the CG update.
+//     2 .. 64 blocks per SM, timed on the CG update.
 // ssg_autotune times every candidate on the context's own mesh and levels
 // (CUDA events on the context stream, best of three runs of ten launches)
 // and keeps the fastest in the process-wide tables the launchers read.  The
@@ -126,7 +126,7 @@ ssg_status ssg_autotune(ssg_context* c, int reps) {
   if (st == SSG_OK) {
     int best_bps = 0;
     float best = 1e30f;
-    for (int bps = 4; bps <= 64 && st == SSG_OK; bps *= 2) {
+    for (int bps = 2; bps <= 64 && st == SSG_OK; bps *= 2) {
       g_tune_vec_bps = bps;
       const int nb = vec_blocks(np0);
       float t = 0.f;
@@ -177,7 +177,7 @@ ssg_status ssg_tuning(int n, int* ax_elements_per_block, int* dss_blocks_per_sm,
   const bool dmma = n == 8;
   if (ax_elements_per_block) *ax_elements_per_block = dmma ? 0 : ax_epb(n);
   if (dss_blocks_per_sm) *dss_blocks_per_sm = g_tune_dss_bps[n] > 0 ? g_tune_dss_bps[n] : 8;
-  if (vector_blocks_per_sm) *vector_blocks_per_sm = g_tune_vec_bps > 0 ? g_tune_vec_bps : 8;
+  if (vector_blocks_per_sm) *vector_blocks_per_sm = g_tune_vec_bps > 0 ? g_tune_vec_bps : 4;
   return SSG_OK;
 }
 

@@ -74,7 +74,7 @@ def test_autotuned_shapes_keep_parity(mk, n, gpu_ctx_factory):
     for n_l, sh in shapes.items():
         assert sh["ax_elements_per_block"] >= (0 if n_l == 8 else 1)
         assert 4 <= sh["dss_blocks_per_sm"] <= 64
-        assert 4 <= sh["vector_blocks_per_sm"] <= 64
+        assert 2 <= sh["vector_blocks_per_sm"] <= 64
     rng = np.random.default_rng(9)
     u = rng.standard_normal((mesh.nel, n, n, n))
     assert np.array_equal(ctx.direct_stiffness_summation(u.copy()), orc.dss(u))
