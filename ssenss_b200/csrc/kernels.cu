@@ -249,6 +249,8 @@ __global__ void __launch_bounds__(256) k_dss(int nel, int epb, const T* __restri
     bool ok[U];
     int src[U][7];
     double own[U], v[U][7];
+    // epilogue operands, loaded with the gather (independent of it)
+    double ex[U], ep[U], er[U], ed[U], ey[U], ey2[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const size_t q = q0 + u * S;
@@ -276,6 +278,14 @@ __global__ void __launch_bounds__(256) k_dss(int nel, int epb, const T* __restri
       src[u][6] = b.z;
       own[u] = (double)in[qq];
       if (mask) own[u] = own[u] * mask[qq];
+      if (MODE == DSS_CGUPD) {
+        ex[u] = (double)cx[qq];
+        ep[u] = (double)cp[qq];
+        er[u] = (double)cr[qq];
+        ed[u] = (double)cd[qq];
+      }
+      if (MODE == DSS_RESID || MODE == DSS_DOT || MODE == DSS_DOT2) ey[u] = (double)y[qq];
+      if (MODE == DSS_DOT2) ey2[u] = (double)y2[qq];
     }
 #pragma unroll
     for (int u = 0; u < U; ++u)
@@ -303,10 +313,10 @@ __global__ void __launch_bounds__(256) k_dss(int nel, int epb, const T* __restri
       const double w = inv_count(1u + (unsigned)cnt);
       if (MODE == DSS_CGUPD) {
         // ap = acc: x += alpha p; r -= alpha ap; z = dinv r  (src/solver.c:66-71)
-        cx[g] = (T)((double)cx[g] + alpha * (double)cp[g]);
-        const T rq = (T)((double)cr[g] + -alpha * acc);
+        cx[g] = (T)(ex[u] + alpha * ep[u]);
+        const T rq = (T)(er[u] + -alpha * acc);
         cr[g] = rq;
-        const T zq = (T)((double)rq * (double)cd[g]);
+        const T zq = (T)((double)rq * ed[u]);
         cz[g] = zq;
         const double rw = (double)rq * w;
         s0 += rw * (double)zq;
@@ -314,7 +324,7 @@ __global__ void __launch_bounds__(256) k_dss(int nel, int epb, const T* __restri
         s2 += w * (double)zq;
         s3 += rw;
       } else if (MODE == DSS_RESID) {
-        const T rv = (T)((double)y[g] + -acc);
+        const T rv = (T)(ey[u] + -acc);
         out[g] = rv;
         s0 += (double)rv * w;
       } else if (MODE == DSS_AVG) {
@@ -323,9 +333,9 @@ __global__ void __launch_bounds__(256) k_dss(int nel, int epb, const T* __restri
         const T av = (T)acc;
         out[g] = av;
         if (MODE == DSS_DOT || MODE == DSS_DOT2) {
-          const double yw = (double)y[g] * w;
+          const double yw = ey[u] * w;
           s0 += yw * (double)av;
-          if (MODE == DSS_DOT2) s1 += yw * (double)y2[g];
+          if (MODE == DSS_DOT2) s1 += yw * ey2[u];
         }
       }
       }
