@@ -37,6 +37,7 @@ struct CoarseArgs {
   const int2* pairs = nullptr;
   double nunique = 1.0;
   double eps = 0.0;
+  double rel = 0.0;   // also stop once err <= rel * err0 (0: eps only)
   int max_iter = 0;
   double* partA = nullptr;        // >= 4 * gridDim.x
   double* partB = nullptr;        // >= 3 * gridDim.x
@@ -234,7 +235,7 @@ __global__ void __launch_bounds__(256) k_coarse_cg(CoarseArgs a) {
     beta = rdz_new / rdz;
     rdz = rdz_new;
     err = sqrt(s[1]);
-    if (!(err > a.eps) || it + 1 >= a.max_iter) {
+    if (!(err > a.eps) || !(err > a.rel * err0) || it + 1 >= a.max_iter) {
       ++it;
       break;
     }
@@ -255,7 +256,8 @@ cudaError_t run_coarse_cg(cudaStream_t s, int device, int nel, const double* f, 
                           double* r, double* z, double* p, double* aploc, double* ap,
                           const double* gf, const double* D, const double* dinv,
                           const uint8_t* mult, const int* pairs, double nunique, double eps,
-                          int max_iter, double* part, size_t part_cap, double* frame) {
+                          double rel, int max_iter, double* part, size_t part_cap,
+                          double* frame) {
   dev::CoarseArgs a;
   a.nel = nel;
   a.npts = (size_t)nel * 8;
@@ -273,6 +275,7 @@ cudaError_t run_coarse_cg(cudaStream_t s, int device, int nel, const double* f, 
   a.pairs = reinterpret_cast<const int2*>(pairs);
   a.nunique = nunique;
   a.eps = eps;
+  a.rel = rel;
   a.max_iter = max_iter;
   a.frame = frame;
   int& cap = g_coarse_grid[device & (SSG_MAXLEV * 8 - 1)];

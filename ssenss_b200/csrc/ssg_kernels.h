@@ -155,11 +155,13 @@ cudaError_t run_helm_diag(cudaStream_t s, size_t npts, size_t nt, const double* 
 cudaError_t run_recip(cudaStream_t s, size_t npts, double* x);
 cudaError_t run_reduce(cudaStream_t s, const double* part, int nblk, int nq, double* sums,
                        const ScalarOp& op);
-// whole CG-Jacobi solve of an n = 2 level in one cooperative launch (coarse.cu)
+// whole CG-Jacobi solve of an n = 2 level in one cooperative launch
+// (coarse.cu); it stops at sqrt((r.r)_w) <= eps, or <= rel times the first
+// residual when rel > 0
 cudaError_t run_coarse_cg(cudaStream_t s, int device, int nel, const double* f, double* x,
                           double* r, double* z, double* p, double* aploc, double* ap,
                           const double* gf, const double* D, const double* dinv,
-                          const uint8_t* mult, const int* pairs, double nunique, double eps,
+                          const uint8_t* mult, const int* pairs, double nunique, double eps, double rel,
                           int max_iter, double* part, size_t part_cap, double* frame);
 // dealiased skew-symmetric convection of 3-component fields (convection.cu);
 // for m^3 fields beyond shared memory, scratch holds
