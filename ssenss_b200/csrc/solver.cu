@@ -104,9 +104,6 @@ ssg_status ensure_workspace(ssg_context* c) {
 
 double* workspace_scratch(ssg_context* c) { return c->ws ? c->ws->scratch : nullptr; }
 
-// relative stop of the coarse solve inside the mixed-precision V-cycle
-static constexpr double kMixedCoarseRel = 1e-6;
-
 static inline double lambda_of(const ssg_context* c) {
   return (11.0 / 6.0) / (c->dt * c->visc);
 }
@@ -298,11 +295,7 @@ static ssg_status mg_recurse(ssg_context* c, int L, void* f, void* x, double eps
       const size_t np = c->lev[L].npts;
       SSG_CUDA(c, run_convert(s, np, f, true, W64.f, false));
       SSG_CUDA(c, cudaMemsetAsync(W64.x, 0, np * sizeof(double), s));
-      // the right-hand side carries the FP32 V-cycle's rounding (~1e-7
-      // relative): solving past 1e-6 of its first residual buys the
-      // preconditioner nothing, so the FP64 coarse CG stops there (or at
-      // eps, whichever comes first)
-      SSG_TRY(coarse_solve(c, L, (double*)W64.f, (double*)W64.x, eps, 500, kMixedCoarseRel));
+      SSG_TRY(coarse_solve(c, L, (double*)W64.f, (double*)W64.x, eps, 500));
       SSG_CUDA(c, run_convert(s, np, W64.x, false, x, true));
       return SSG_OK;
     }
