@@ -21,7 +21,7 @@ enum { VAR_PRESSURE = 0 };
 enum { ST_NORMAL = 0, ST_COLLISION = 1, ST_OUTSIDE = 2, ST_RESEED = 5 };
 
 #define MAXLEV 8
-#define MAXN 16
+#define MAXN 18
 
 typedef struct {
 	int n;

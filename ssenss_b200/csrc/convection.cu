@@ -11,10 +11,10 @@
 //   3. project back with (J^T)^3 (integrate_to_grid, src/interpolation.c:
 //      157-176).
 // The derivatives of the products u_b v_c are taken on the fly from the
-// interpolated fields, so only the six interpolated fields and the three
-// averaged components are stored per element: in shared memory while they
-// fit (m <= 13, n <= 9), else in a global scratch region of 9 m^3 doubles
-// per block.
+// interpolated fields; per element the three advecting components, one
+// advected component and its result are stored (the advected components
+// are taken one at a time): in shared memory while they fit, else in a
+// global scratch region of 5 m^3 doubles per block.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -59,7 +59,7 @@ __device__ void block_tensor3(int ni, int no, const double* A, bool transpose,
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(512) k_convection(int nel, int n, int m,
+__global__ void __launch_bounds__(512, 2) k_convection(int nel, int n, int m,
                                                    const double* __restrict__ u,
                                                    const double* __restrict__ v,
                                                    double* __restrict__ udv,
@@ -76,37 +76,43 @@ __global__ void __launch_bounds__(512) k_convection(int nel, int n, int m,
   double* t1 = sJ + m * n;
   double* t2 = t1 + tmax;
   double* stage = t2 + tmax;                  // nt
-  double* ui = gscr ? gscr + (size_t)blockIdx.x * 9 * mt : stage + nt;   // 3 x mt
-  double* vi = ui + 3 * mt;                   // 3 x mt
-  double* sk = vi + 3 * mt;                   // 3 x mt
+  double* ui = gscr ? gscr + (size_t)blockIdx.x * 5 * mt : stage + nt;   // 3 x mt
+  double* vc = ui + 3 * mt;                   // advected component c
+  double* sk = vc + mt;                       // its skew-symmetric term
   const size_t nptsn = (size_t)nel * nt, nptsm = (size_t)nel * mt;
   for (int q = threadIdx.x; q < m * m; q += blockDim.x) sD[q] = Dm[q];
   for (int q = threadIdx.x; q < m * n; q += blockDim.x) sJ[q] = J[q];
   for (size_t e = blockIdx.x; e < (size_t)nel; e += gridDim.x) {
-    // 1. interpolate the six components to the dealiasing grid
-    for (int f = 0; f < 6; ++f) {
-      const double* src = (f < 3 ? u : v) + (size_t)(f % 3) * nptsn + e * nt;
+    // 1. the advecting field on the dealiasing grid
+    for (int f = 0; f < 3; ++f) {
+      const double* src = u + (size_t)f * nptsn + e * nt;
       __syncthreads();
       for (int q = threadIdx.x; q < nt; q += blockDim.x) stage[q] = src[q];
       __syncthreads();
-      block_tensor3(n, m, sJ, false, stage, t1, t2, (f < 3 ? ui : vi) + (f % 3) * mt, nullptr);
+      block_tensor3(n, m, sJ, false, stage, t1, t2, ui + f * mt, nullptr);
     }
-    // 2. convective and conservative forms at every dealiasing point
-    for (int q = threadIdx.x; q < mt; q += blockDim.x) {
-      const int i = q % m, j = (q / m) % m, k = q / (m * m);
-      const size_t g = e * mt + q;
-      double t[3][3];
+    // 2. one advected component at a time (half the shared memory of
+    // holding all three: two blocks per SM): interpolate, convective and
+    // conservative forms at every dealiasing point, weak projection back
+    for (int c = 0; c < 3; ++c) {
+      const double* src = v + (size_t)c * nptsn + e * nt;
+      __syncthreads();
+      for (int q = threadIdx.x; q < nt; q += blockDim.x) stage[q] = src[q];
+      __syncthreads();
+      block_tensor3(n, m, sJ, false, stage, t1, t2, vc, nullptr);
+      for (int q = threadIdx.x; q < mt; q += blockDim.x) {
+        const int i = q % m, j = (q / m) % m, k = q / (m * m);
+        const size_t g = e * mt + q;
+        double t[3][3];
 #pragma unroll
-      for (int a = 0; a < 3; ++a)
+        for (int a = 0; a < 3; ++a)
 #pragma unroll
-        for (int b = 0; b < 3; ++b) t[a][b] = tinv[(size_t)(3 * a + b) * nptsm + g];
-      const double w = bj[g];
-      const double* Di = sD + i * m;
-      const double* Dj = sD + j * m;
-      const double* Dk = sD + k * m;
-      const int rbase = (k * m + j) * m, sbase = k * m * m + i, tbase = j * m + i;
-      for (int c = 0; c < 3; ++c) {
-        const double* vc = vi + c * mt;
+          for (int b = 0; b < 3; ++b) t[a][b] = __ldg(tinv + (size_t)(3 * a + b) * nptsm + g);
+        const double w = __ldg(bj + g);
+        const double* Di = sD + i * m;
+        const double* Dj = sD + j * m;
+        const double* Dk = sD + k * m;
+        const int rbase = (k * m + j) * m, sbase = k * m * m + i, tbase = j * m + i;
         // convective: d v_c / d r_b, then grad through tinv, dotted with u
         double dr = 0, ds = 0, dt = 0;
         for (int l = 0; l < m; ++l) {
@@ -142,13 +148,11 @@ __global__ void __launch_bounds__(512) k_convection(int nel, int n, int m,
           cs += s;
         }
         cs = cs * w;
-        sk[c * mt + q] = 0.5 * cv + 0.5 * cs;
+        sk[q] = 0.5 * cv + 0.5 * cs;
       }
+      __syncthreads();
+      block_tensor3(m, n, sJ, true, sk, t1, t2, nullptr, udv + (size_t)c * nptsn + e * nt);
     }
-    __syncthreads();
-    // 3. weak projection back to the n-point grid
-    for (int c = 0; c < 3; ++c)
-      block_tensor3(m, n, sJ, true, sk + c * mt, t1, t2, nullptr, udv + (size_t)c * nptsn + e * nt);
     __syncthreads();
   }
 }
@@ -158,14 +162,14 @@ __global__ void __launch_bounds__(512) k_convection(int nel, int n, int m,
 static size_t convection_smem(int n, int m, bool fields) {
   const size_t nt = (size_t)n * n * n, mt = (size_t)m * m * m;
   const size_t tmax = std::max((size_t)n * m * m, (size_t)n * n * m);
-  return (m * m + m * n + 2 * tmax + nt + (fields ? 9 * mt : 0)) * sizeof(double);
+  return (m * m + m * n + 2 * tmax + nt + (fields ? 5 * mt : 0)) * sizeof(double);
 }
 
 static constexpr size_t kConvSmemMax = 220 * 1024;
 
 size_t convection_scratch_doubles(int n, int m) {
   if (convection_smem(n, m, true) <= kConvSmemMax) return 0;
-  return (size_t)kConvScratchBlocks * 9 * m * m * m;
+  return (size_t)kConvScratchBlocks * 5 * m * m * m;
 }
 
 cudaError_t run_convection(cudaStream_t s, int nel, int n, int m, const double* u,

@@ -18,11 +18,12 @@ from ssenss_b200.mesh import box_mesh, channel_mesh, tgv_box
 pytestmark = pytest.mark.gpu
 
 CONV_CASES = {
-    # m = 12: six interpolated fields held in shared memory
+    # m = 12, 15: per-element fields held in shared memory
     "tgv3_n8": (lambda: tgv_box(3), 8),
     "channel433_n7": (lambda: channel_mesh((4, 3, 3), seed=7), 7),
-    # m = 15: interpolated fields in the global scratch region
     "tgv3_n10": (lambda: tgv_box(3), 10),
+    # m = 18: per-element fields in the global scratch region
+    "tgv2_n12": (lambda: tgv_box(2), 12),
     "tgv4_n4": (lambda: tgv_box(4), 4),
 }
 
