@@ -697,6 +697,17 @@ def run_ours(args):
     alg = OP_BYTES_PER_POINT * npts
     peak, peak_kind = peaks()
     achieved = alg / (op_ms * 1e-3) / 1e9
+    # the three kernels of a smoother CG iteration at every level, each timed
+    # alone; algorithmic bytes per point: DSS + dot 24 (in, y, out), CG update
+    # 65 (x, p, r, ap, dinv, multiplicity in; x, r, z out)
+    smoother = {}
+    for lev, m in enumerate(ctx.orders):
+        t = ctx.time_smoother(lev, 50)
+        pts = mesh.nel * m ** 3
+        smoother[str(m)] = {
+            "us_per_launch": t,
+            "dss_dot_frac": 24 * pts / (t["dss_dot"] * 1e-6) / 1e9 / peak,
+            "cg_update_frac": 65 * pts / (t["cg_update"] * 1e-6) / 1e9 / peak}
 
     # ---- Helmholtz (velocity) solve, reported beside -------------------------
     fvel = torch.from_numpy(ctx.direct_stiffness_summation(
@@ -771,6 +782,7 @@ def run_ours(args):
                                    "achieved": 72 * npts / (op_ms_h * 1e-3) / 1e9,
                                    "frac": 72 * npts / (op_ms_h * 1e-3) / 1e9 / peak},
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"},
+        "smoother_kernels": smoother,
         "serving": serving,
         "channel_c3": extra.get("channel"),
         "particles_c4": extra.get("particles"),

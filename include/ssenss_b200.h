@@ -256,6 +256,12 @@ ssg_status ssg_autotune(ssg_context *ctx, int reps);
  * context's stream between two CUDA events, best of three trials. */
 ssg_status ssg_time_operator(ssg_context *ctx, int var, int reps,
 		double *us_per_apply);
+/* Device time of the three kernels of one smoother CG iteration at a
+ * multigrid level, FP64, in microseconds per launch, each timed alone as
+ * in ssg_time_operator (no reference counterpart: a measurement aid):
+ * us[0] the element operator, us[1] the DSS with the p.(Ap) partial sums,
+ * us[2] the CG update (x, r, z and four partial sums). */
+ssg_status ssg_time_smoother(ssg_context *ctx, int level, int reps, double *us);
 /* Launch shapes in use for order n (tuned or default); elements per block
  * 0 = the FP64 tensor-core operator (n = 8: one warp per element). */
 ssg_status ssg_tuning(int n, int *ax_elements_per_block,

@@ -111,6 +111,7 @@ class Oracle(_Common):
             L.og_dss.argtypes = [C.c_void_p, C.c_int, _dp]
             L.og_dot.argtypes = [C.c_void_p, C.c_int, _dp, _dp]
             L.og_dot.restype = C.c_double
+            L.og_set_dot_perturbation.argtypes = [C.c_void_p, C.c_double, C.c_ulonglong]
             L.og_solve_poisson.argtypes = [C.c_void_p, _dp, _dp, C.c_double,
                                            C.c_int, _dp, C.c_int]
             L.og_solve_poisson.restype = C.c_int
@@ -215,6 +216,25 @@ class Oracle(_Common):
         k = self.lib().og_solve_helmholtz(self.h, var, _d(f), _d(u), eps,
                                           max_iter, _d(hist), len(hist))
         return u, hist[:min(k, len(hist))]
+
+    def rounding_spread(self, solve, f, seeds=8, rel_pert=2e-16):
+        """How far the solution of solve(f, 0) (a bound method of this
+        oracle, e.g. self.solve_poisson) is determined by the arithmetic:
+        the largest relative difference (max |du| / max |u|) between the
+        plain solve and `seeds` solves whose every global dot product is
+        scaled by (1 + rel_pert * xi), xi in [-1, 1) (og_set_dot_perturbation).
+        Any other correct summation order lands inside this spread."""
+        u0, _ = solve(f, np.zeros_like(f))
+        scale = max(float(np.max(np.abs(u0))), 1e-300)
+        worst = 0.0
+        try:
+            for s in range(1, seeds + 1):
+                self.lib().og_set_dot_perturbation(self.h, rel_pert, s)
+                u, _ = solve(f, np.zeros_like(f))
+                worst = max(worst, float(np.max(np.abs(u - u0))) / scale)
+        finally:
+            self.lib().og_set_dot_perturbation(self.h, 0.0, 1)
+        return worst
 
     def mg_precon(self, r, eps=1e-10):
         r = _f64(r)

@@ -58,6 +58,9 @@ struct og_ctx {
 	/* particle walk: GLL points and level-0 jac / tinv it reads; NULL =
 	 * the oracle's own (og_set_particle_basis overrides them) */
 	double *ppts, *pjac, *ptinv;
+	/* conditioning probe (og_set_dot_perturbation): 0 = off */
+	double dot_pert;
+	unsigned long long dot_seed;
 };
 
 static double *dalloc(size_t n)
@@ -541,7 +544,27 @@ double og_dot(og_ctx *c, int level, const double *x, const double *y)
 	double s = 0.0;
 	for (size_t q = 0; q < len; ++q)
 		s += (x[q] * L->scale[q]) * y[q];
+	if (c->dot_pert != 0.0) {
+		/* 64-bit LCG (Knuth's MMIX constants); xi uniform in [-1, 1) */
+		c->dot_seed = c->dot_seed * 6364136223846793005ULL +
+			1442695040888963407ULL;
+		const double xi = (double) (c->dot_seed >> 11) *
+			(2.0 / 9007199254740992.0) - 1.0;
+		s *= 1.0 + c->dot_pert * xi;
+	}
 	return s;
+}
+
+/* Conditioning probe, not part of the reference's algorithm: every later
+ * og_dot result is scaled by (1 + rel * xi), xi drawn per call from a
+ * seeded generator.  With rel at the size of one rounding (2e-16) the
+ * spread of the perturbed solves is how far the solution is determined by
+ * the arithmetic at all: any other correct summation order (the
+ * reference's BLAS ddot, a parallel reduction) lands inside it. */
+void og_set_dot_perturbation(og_ctx *c, double rel, unsigned long long seed)
+{
+	c->dot_pert = rel;
+	c->dot_seed = seed;
 }
 
 /* ------------------------------------------------------------------ */

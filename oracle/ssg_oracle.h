@@ -60,6 +60,9 @@ void og_global_opeval(og_ctx *c, int level, int var, const double *p,
 		double *ap);
 void og_dss(og_ctx *c, int level, double *u);
 double og_dot(og_ctx *c, int level, const double *x, const double *y);
+/* conditioning probe: later og_dot results are scaled by (1 + rel * xi),
+ * xi uniform in [-1, 1) from a generator seeded with seed; rel = 0 off */
+void og_set_dot_perturbation(og_ctx *c, double rel, unsigned long long seed);
 
 /* ---- solvers (src/solver.c, src/precon.c) ---- */
 int og_solve_poisson(og_ctx *c, const double *f, double *u, double eps,

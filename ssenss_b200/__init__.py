@@ -122,6 +122,14 @@ class Context:
                     "time_operator")
         return float(us.value)
 
+    def time_smoother(self, level: int = 0, reps: int = 50) -> dict:
+        """Device microseconds per launch of the smoother CG kernels at a
+        level (ssg_time_smoother): operator, DSS + dot, CG update."""
+        us = (C.c_double * 3)()
+        self._check(self.lib.ssg_time_smoother(self.h, int(level), int(reps), us),
+                    "time_smoother")
+        return {"operator": us[0], "dss_dot": us[1], "cg_update": us[2]}
+
     def autotune(self, reps: int = 10):
         """ssg_autotune: time the launch-shape candidates on this mesh and
         keep the fastest (process-wide, per order); returns the shapes."""

@@ -112,6 +112,7 @@ SIGNATURES = [
     ("ssg_server_destroy", None, [C.c_void_p]),
     ("ssg_tuning", C.c_int, [C.c_int, _ip, _ip, _ip]),
     ("ssg_time_operator", C.c_int, [C.c_void_p, C.c_int, C.c_int, _dp]),
+    ("ssg_time_smoother", C.c_int, [C.c_void_p, C.c_int, C.c_int, _dp]),
     ("ssg_set_particle_velocity", C.c_int, [C.c_void_p, C.c_void_p]),
     ("ssg_integrate_particle_equations", C.c_int, [C.c_void_p, C.c_size_t, C.c_void_p,
                                                    C.c_void_p, C.c_double, C.c_double,

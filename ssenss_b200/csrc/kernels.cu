@@ -447,7 +447,7 @@ __global__ void __launch_bounds__(256) k_recip(size_t npts, double* __restrict__
   }
 
 template <typename T>
-__global__ void __launch_bounds__(256) k_cg_update(size_t npts,
+__global__ void __launch_bounds__(256, 3) k_cg_update(size_t npts,
                                                    const double* __restrict__ alpha_p,
                                                    T* __restrict__ x, const T* __restrict__ p,
                                                    T* __restrict__ r, const T* __restrict__ ap,
@@ -653,7 +653,7 @@ int ax_epb_max(int n) {
 // kernels loop grid-stride with four points in flight per thread
 int vec_blocks(size_t npts) {
   size_t b = (npts + 255) / 256;
-  const size_t cap = (size_t)148 * (g_tune_vec_bps > 0 ? g_tune_vec_bps : 4);
+  const size_t cap = (size_t)148 * (g_tune_vec_bps > 0 ? g_tune_vec_bps : kVecBpsDefault);
   return (int)(b < cap ? (b ? b : 1) : cap);
 }
 

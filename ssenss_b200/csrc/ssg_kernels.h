@@ -99,6 +99,9 @@ int dss_grid(int n, int nel);
 extern int g_tune_ax_epb[];
 extern int g_tune_dss_bps[];
 extern int g_tune_vec_bps;
+// untuned vector-kernel blocks per SM: the CG update's residency (3 x 256
+// threads at <= 85 registers), so its grid is one full wave
+constexpr int kVecBpsDefault = 3;
 // operator kernel kind per order: default, the shared-memory kernel, or the
 // FP64 tensor-core kernel (n = 8 only); run_ax's epb = AX_DMMA forces the
 // latter

@@ -126,7 +126,8 @@ ssg_status ssg_autotune(ssg_context* c, int reps) {
   if (st == SSG_OK) {
     int best_bps = 0;
     float best = 1e30f;
-    for (int bps = 2; bps <= 64 && st == SSG_OK; bps *= 2) {
+    for (int bps : {2, 3, 4, 6, 8, 16, 32, 64}) {
+      if (st != SSG_OK) break;
       g_tune_vec_bps = bps;
       const int nb = vec_blocks(np0);
       float t = 0.f;
@@ -170,6 +171,49 @@ ssg_status ssg_time_operator(ssg_context* c, int var, int reps, double* us_per_a
   return SSG_OK;
 }
 
+ssg_status ssg_time_smoother(ssg_context* c, int level, int reps, double* us) {
+  if (!c || !us || reps <= 0) return SSG_ERR_ARG;
+  if (!c->ready) return fail(c, SSG_ERR_STATE, "no mesh set up on this context");
+  if (level < 0 || level >= c->nlev) return fail(c, SSG_ERR_ARG, "level out of range");
+  SSG_CUDA(c, cudaSetDevice(c->device));
+  const DevLevel& L = c->lev[level];
+  const size_t np = L.npts;
+  std::vector<double*> buf(6, nullptr);
+  for (auto& p : buf) {
+    if (cudaMalloc(&p, np * sizeof(double)) != cudaSuccess) {
+      cudaGetLastError();
+      for (auto& q : buf)
+        if (q) cudaFree(q);
+      return fail(c, SSG_ERR_NOMEM, "timing scratch");
+    }
+    cudaMemsetAsync(p, 0, np * sizeof(double), c->stream);
+  }
+  const int nb = vec_blocks(np);
+  auto op = [&] {
+    return run_ax(c->stream, L.n, c->nel, 0, false, false, buf[0], buf[1], L.gf, np, nullptr,
+                  L.D, L.D, 0.0, nullptr);
+  };
+  auto dss = [&] {
+    return run_dss(c->stream, DSS_DOT, false, L.n, c->nel, buf[1], buf[2], c->d_pairs,
+                   L.dss_ec, nullptr, buf[0], nullptr, c->d_part, nullptr, nullptr);
+  };
+  auto upd = [&] {
+    return run_cg_update(c->stream, false, np, c->d_sums, buf[3], buf[0], buf[4], buf[2],
+                         L.dinv_p, L.mult, buf[5], c->d_part, nb, nullptr, nullptr);
+  };
+  ssg_status st = SSG_OK;
+  float t = 0.f;
+  if (st == SSG_OK) st = time_launches(c, reps, op, &t);
+  us[0] = 1e3 * (double)t / reps;
+  if (st == SSG_OK) st = time_launches(c, reps, dss, &t);
+  us[1] = 1e3 * (double)t / reps;
+  if (st == SSG_OK) st = time_launches(c, reps, upd, &t);
+  us[2] = 1e3 * (double)t / reps;
+  cudaStreamSynchronize(c->stream);
+  for (auto& p : buf) cudaFree(p);
+  return st;
+}
+
 ssg_status ssg_tuning(int n, int* ax_elements_per_block, int* dss_blocks_per_sm,
                       int* vector_blocks_per_sm) {
   if (n < 2 || n > SSG_MAXN) return SSG_ERR_ARG;
@@ -177,7 +221,7 @@ ssg_status ssg_tuning(int n, int* ax_elements_per_block, int* dss_blocks_per_sm,
   const bool dmma = n == 8;
   if (ax_elements_per_block) *ax_elements_per_block = dmma ? 0 : ax_epb(n);
   if (dss_blocks_per_sm) *dss_blocks_per_sm = g_tune_dss_bps[n] > 0 ? g_tune_dss_bps[n] : 8;
-  if (vector_blocks_per_sm) *vector_blocks_per_sm = g_tune_vec_bps > 0 ? g_tune_vec_bps : 4;
+  if (vector_blocks_per_sm) *vector_blocks_per_sm = g_tune_vec_bps > 0 ? g_tune_vec_bps : kVecBpsDefault;
   return SSG_OK;
 }
 

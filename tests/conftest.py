@@ -1,6 +1,7 @@
 import os
 import sys
 
+import numpy as np
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -33,6 +34,24 @@ def gpu_ctx_factory():
 
 
 EPS = 1e-10
+
+
+SOLVE_REL = 1e-11
+
+
+def assert_solution_close(u_g, u_o, orc, solve, f):
+    """GPU solution u_g against the oracle's u_o = solve(f, 0): within 1e-11
+    relative (max |du| / max |u|), or, where the solve itself is not
+    determined that closely by FP64 arithmetic, within twice the oracle's
+    own rounding spread (Oracle.rounding_spread: the same oracle solve with
+    its dot products perturbed by one rounding).  Both tolerances stated
+    here; the spread is only measured when the plain bound is missed."""
+    d = float(np.max(np.abs(u_g - u_o)) / max(np.max(np.abs(u_o)), 1e-300))
+    if d < SOLVE_REL:
+        return d
+    spread = orc.rounding_spread(solve, f)
+    assert d < 2.0 * spread, (d, spread)
+    return d
 
 
 def same_stop(it_g, h_g, h_o):

@@ -4,13 +4,16 @@ through the C ABI.
 Tolerances: integer pairing and DSS are bitwise; element operators agree to
 1e-13 relative (summation order and FMA differ from the oracle); solves stop
 at the reference's absolute criterion sqrt((r.r)_w) <= 1e-10 and their
-solutions agree to 1e-11 relative.
+solutions agree to 1e-11 relative, or to twice the oracle's own rounding
+spread where the solve is not determined that closely by FP64 arithmetic
+(conftest.assert_solution_close; TGV 3^3 at n = 10 is such a case: one
+rounding of the oracle's dot products moves its solution by 2e-11).
 """
 import numpy as np
 import pytest
 
 import oracle as O
-from conftest import same_stop
+from conftest import assert_solution_close, same_stop
 from ssenss_b200.mesh import box_mesh, channel_mesh, tgv_box
 
 pytestmark = pytest.mark.gpu
@@ -134,7 +137,7 @@ def test_poisson_solve(name, gpu_ctx_factory):
     assert info["status"] == "SSG_OK"
     assert info["residual"] <= 1e-10
     if same_stop(info["iterations"], info["history"], h_o):
-        assert rel(u_g, u_o) < 1e-11
+        assert_solution_close(u_g, u_o, orc, orc.solve_poisson, f)
     # residual histories: while the residual is well above the rounding floor
     # they agree to 1e-9 relative; near eps the floor itself differs between
     # any two FP64 implementations (the oracle and the reference build differ

@@ -11,7 +11,7 @@ import numpy as np
 import pytest
 
 import oracle as O
-from conftest import same_stop
+from conftest import assert_solution_close, same_stop
 import ssenss_b200 as S
 from ssenss_b200.mesh import channel_mesh, tgv_box
 
@@ -83,4 +83,4 @@ def test_autotuned_shapes_keep_parity(mk, n, gpu_ctx_factory):
     u_o, h_o = orc.solve_poisson(f, np.zeros_like(f))
     u_g, info = ctx.solve_poisson_cg(f, np.zeros_like(f))
     if same_stop(info["iterations"], info["history"], h_o):
-        assert rel(u_g, u_o) < 1e-11
+        assert_solution_close(u_g, u_o, orc, orc.solve_poisson, f)
