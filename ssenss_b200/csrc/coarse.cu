@@ -248,6 +248,172 @@ __global__ void __launch_bounds__(256) k_coarse_cg(CoarseArgs a) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// The post-smoother CG of a small multigrid level (conjugate_gradient with
+// jacobi_preconditioner on the Poisson operator, src/solver.c:33-81: what
+// cg_solve launches as three kernels per iteration) in one cooperative
+// launch.  Same per-point arithmetic as those kernels (the element operator
+// is the shared ax_element, the DSS the reference-ordered dss_gather, the
+// vector updates k_add_const / k_jacobi / k_dots / k_cg_update written out);
+// the reductions are block partials summed identically by every block, so
+// every block takes the same alpha, beta and stop decision.  Three grid
+// barriers per iteration; the loop is bounded by max_iter.
+// ---------------------------------------------------------------------------
+template <typename T>
+struct LevelCgArgs {
+  int nel = 0;
+  size_t npts = 0;
+  const T* f = nullptr;
+  T* x = nullptr;
+  T *r = nullptr, *z = nullptr, *p = nullptr, *aploc = nullptr, *ap = nullptr;
+  const T* gf = nullptr;          // 6 x npts
+  const double* D = nullptr;
+  const T* dinv = nullptr;
+  const uint8_t* mult = nullptr;
+  const int2* pairs = nullptr;
+  double nunique = 1.0;
+  double eps = 0.0;
+  int max_iter = 0;
+  double* partA = nullptr;        // >= 4 * gridDim.x
+  double* partB = nullptr;        // >= 3 * gridDim.x
+};
+
+template <int N>
+constexpr size_t level_cg_smem() {
+  return (size_t)(AxSmem<N>::MATS + (256 / (N * N)) * 3 * AxSmem<N>::BLK) * sizeof(double);
+}
+
+template <int N, typename T>
+__global__ void __launch_bounds__(256) k_level_cg(LevelCgArgs<T> a) {
+  using L = AxSmem<N>;
+  static_assert(256 % (N * N) == 0, "whole element planes per block");
+  constexpr int NT = N * N * N, EPB = 256 / (N * N);
+  cg::grid_group grid = cg::this_grid();
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* sD = reinterpret_cast<double*>(smem_raw);
+  __shared__ double sred[4 * 32];
+  __shared__ double sbc[4];
+  const int tb = threadIdx.x;
+  const int i = tb % N, j = (tb / N) % N, slot = tb / (N * N);
+  double* su = sD + L::MATS + slot * 3 * L::BLK;
+  ax_load_mats<N, false>(sD, a.D, a.D, tb, 256);   // visible after the first barrier
+  const size_t tid = (size_t)blockIdx.x * blockDim.x + tb;
+  const size_t nthr = (size_t)gridDim.x * blockDim.x;
+  const int G = gridDim.x;
+  const int ngroups = (a.nel + EPB - 1) / EPB;
+  // aploc = A_e in (fusep: in = p, formed from z first); block-uniform loop
+  auto op_pass = [&](T* in, bool fusep, bool first, double beta, double cz) {
+    for (int grp = blockIdx.x; grp < ngroups; grp += G) {
+      const int e = grp * EPB + slot;
+      if (fusep)
+        ax_element<N, T, false, true>(e, e < a.nel, i, j, sD, su, su + L::BLK,
+                                      su + 2 * L::BLK, in, a.aploc, a.gf, a.npts, nullptr,
+                                      0.0, a.z, beta, cz, nullptr, first);
+      else
+        ax_element<N, T, false, false>(e, e < a.nel, i, j, sD, su, su + L::BLK,
+                                       su + 2 * L::BLK, in, a.aploc, a.gf, a.npts, nullptr,
+                                       0.0, nullptr, 0.0, 0.0, nullptr, false);
+    }
+  };
+
+  // r = f - DSS(A x) with sum w r (DSS_RESID)
+  op_pass(a.x, false, false, 0.0, 0.0);
+  grid.sync();
+  {
+    double v[1] = {0.0};
+    for (size_t q = tid; q < a.npts; q += nthr) {
+      int cnt;
+      const double acc = dss_gather<N, T>(a.aploc, nullptr, a.pairs + (q / NT) * 26, q,
+                                          (int)(q % NT), cnt);
+      const T rv = (T)((double)a.f[q] + -acc);
+      a.r[q] = rv;
+      v[0] += (double)rv * inv_count(1u + (unsigned)cnt);
+    }
+    block_partials<1>(v, a.partA, sred);
+  }
+  grid.sync();
+  // r -= c (nullspace); z = M^-1 r with sum w z (k_add_const, k_jacobi)
+  {
+    double t[1];
+    grid_sums<1>(a.partA, G, t, sred, sbc);
+    const double nc = -(t[0] / a.nunique);
+    double v[1] = {0.0};
+    for (size_t q = tid; q < a.npts; q += nthr) {
+      const T rq = (T)((double)a.r[q] + nc);
+      a.r[q] = rq;
+      const T zq = (T)((double)rq * (double)a.dinv[q]);
+      a.z[q] = zq;
+      v[0] += (double)zq * inv_count(a.mult[q]);
+    }
+    block_partials<1>(v, a.partB, sred);
+  }
+  grid.sync();
+  double cz, rdz = 0.0, beta = 0.0;
+  {
+    double t[1];
+    grid_sums<1>(a.partB, G, t, sred, sbc);
+    cz = t[0] / a.nunique;
+  }
+  for (int it = 0; it < a.max_iter; ++it) {
+    const bool first = it == 0;
+    // p = beta p + (z - c) (first: z - c); aploc = A_e p
+    op_pass(a.p, true, first, beta, cz);
+    grid.sync();
+    // ap = DSS(aploc), (p w).ap; first: (r w).p, (r w).r (k_dss DOT, k_dots)
+    {
+      double v[3] = {0.0, 0.0, 0.0};
+      for (size_t q = tid; q < a.npts; q += nthr) {
+        int cnt;
+        const double acc = dss_gather<N, T>(a.aploc, nullptr, a.pairs + (q / NT) * 26, q,
+                                            (int)(q % NT), cnt);
+        const T av = (T)acc;
+        a.ap[q] = av;
+        const double pv = (double)a.p[q];
+        v[0] += (pv * inv_count(1u + (unsigned)cnt)) * (double)av;
+        if (first) {
+          const double rw = (double)a.r[q] * inv_count(a.mult[q]);
+          v[1] += rw * pv;
+          v[2] += rw * (double)a.r[q];
+        }
+      }
+      block_partials<3>(v, a.partB, sred);
+    }
+    grid.sync();
+    // alpha; x += alpha p; r -= alpha ap; z = M^-1 r (k_cg_update)
+    {
+      double t[3];
+      grid_sums<3>(a.partB, G, t, sred, sbc);
+      if (first) rdz = t[1];
+      const double alpha = rdz / t[0];
+      double v[4] = {0.0, 0.0, 0.0, 0.0};
+      for (size_t q = tid; q < a.npts; q += nthr) {
+        a.x[q] = (T)((double)a.x[q] + alpha * (double)a.p[q]);
+        const T rq = (T)((double)a.r[q] + -alpha * (double)a.ap[q]);
+        a.r[q] = rq;
+        const T zq = (T)((double)rq * (double)a.dinv[q]);
+        a.z[q] = zq;
+        const double w = inv_count(a.mult[q]);
+        const double rw = (double)rq * w;
+        v[0] += rw * (double)zq;
+        v[1] += rw * (double)rq;
+        v[2] += w * (double)zq;
+        v[3] += rw;
+      }
+      block_partials<4>(v, a.partA, sred);
+    }
+    grid.sync();
+    // nullspace constant, beta, residual, stop (OP_CG_BETA)
+    double s4[4];
+    grid_sums<4>(a.partA, G, s4, sred, sbc);
+    cz = s4[2] / a.nunique;
+    const double rdz_new = s4[0] - cz * s4[3];
+    beta = rdz_new / rdz;
+    rdz = rdz_new;
+    const double err = sqrt(s4[1]);
+    if (!(err > a.eps) || it + 1 >= a.max_iter) break;
+  }
+}
+
 }  // namespace dev
 
 static int g_coarse_grid[SSG_MAXLEV * 8] = {0};
@@ -300,6 +466,62 @@ cudaError_t run_coarse_cg(cudaStream_t s, int device, int nel, const double* f, 
   count_launch();
   return cudaLaunchCooperativeKernel((const void*)dev::k_coarse_cg, dim3(G), dim3(256), args,
                                      0, s);
+}
+
+}  // namespace ssg
+
+namespace ssg {
+
+template <typename T>
+static cudaError_t launch_level_cg4(cudaStream_t s, int device, const LevelCgRun& L) {
+  constexpr int N = 4;
+  dev::LevelCgArgs<T> a;
+  a.nel = L.nel;
+  a.npts = (size_t)L.nel * N * N * N;
+  a.f = (const T*)L.f;
+  a.x = (T*)L.x;
+  a.r = (T*)L.r;
+  a.z = (T*)L.z;
+  a.p = (T*)L.p;
+  a.aploc = (T*)L.aploc;
+  a.ap = (T*)L.ap;
+  a.gf = (const T*)L.gf;
+  a.D = L.D;
+  a.dinv = (const T*)L.dinv;
+  a.mult = L.mult;
+  a.pairs = reinterpret_cast<const int2*>(L.pairs);
+  a.nunique = L.nunique;
+  a.eps = L.eps;
+  a.max_iter = L.max_iter;
+  const size_t smem = dev::level_cg_smem<N>();
+  // blocks the device runs at once (a cooperative launch must not exceed it)
+  static int cap[2][64] = {{0}};
+  int& c = cap[sizeof(T) == 4][device & 63];
+  if (c == 0) {
+    int per_sm = 0, nsm = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm, dev::k_level_cg<N, T>, 256, smem);
+    if (e != cudaSuccess) return e;
+    e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
+    if (e != cudaSuccess) return e;
+    c = per_sm * nsm;
+    if (c < 1) return cudaErrorCooperativeLaunchTooLarge;
+  }
+  const int groups = (L.nel + 15) / 16;
+  int G = groups < c ? groups : c;
+  if ((size_t)7 * G > L.part_cap) G = (int)(L.part_cap / 7);
+  if (G < 1) return cudaErrorInvalidValue;
+  a.partA = L.part;
+  a.partB = L.part + 4 * (size_t)G;
+  void* args[] = {&a};
+  count_launch();
+  return cudaLaunchCooperativeKernel((const void*)dev::k_level_cg<N, T>, dim3(G), dim3(256),
+                                     args, smem, s);
+}
+
+cudaError_t run_level_cg(cudaStream_t s, int device, int n, bool fp32, const LevelCgRun& L) {
+  if (n != 4) return cudaErrorInvalidValue;
+  return fp32 ? launch_level_cg4<float>(s, device, L) : launch_level_cg4<double>(s, device, L);
 }
 
 }  // namespace ssg

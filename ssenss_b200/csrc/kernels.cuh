@@ -348,5 +348,171 @@ __device__ __forceinline__ void finish_flat(double v, int tid, int nthr,
 }
 
 
+// ---------------------------------------------------------------------------
+// element operator building blocks (k_ax in kernels.cu, the small-level
+// cooperative CG in coarse.cu)
+// ---------------------------------------------------------------------------
+// padded row stride of the shared 1-D matrices: even (16-byte aligned rows
+// for double2 loads) and chosen so the rows fall on distinct bank groups
+template <int N>
+struct AxLayout {
+  static constexpr int P = (N % 2 == 0) ? N + 2 : N + 1;   // matrix rows
+  static constexpr int Q = N + (N & 1);                    // field rows
+};
+
+// sum_m a[m] b[m] over m = 0..N-1 in order, both rows 16-byte aligned
+template <int N>
+__device__ __forceinline__ double row_dot(const double* a, const double* b) {
+  double s = 0.0;
+#pragma unroll
+  for (int m = 0; m + 1 < N; m += 2) {
+    const double2 x = *reinterpret_cast<const double2*>(a + m);
+    const double2 y = *reinterpret_cast<const double2*>(b + m);
+    s += x.x * y.x;
+    s += x.y * y.y;
+  }
+  if (N & 1) s += a[N - 1] * b[N - 1];
+  return s;
+}
+
+// sum_m a[m] b[m * stride] over m in order; a a 16-byte aligned row
+template <int N>
+__device__ __forceinline__ double row_col_dot(const double* a, const double* b, int stride) {
+  double s = 0.0;
+#pragma unroll
+  for (int m = 0; m + 1 < N; m += 2) {
+    const double2 x = *reinterpret_cast<const double2*>(a + m);
+    s += x.x * b[m * stride];
+    s += x.y * b[(m + 1) * stride];
+  }
+  if (N & 1) s += a[N - 1] * b[(N - 1) * stride];
+  return s;
+}
+
+// sum_m a[m] r[m] over m in order; a a 16-byte aligned row, r registers
+template <int N>
+__device__ __forceinline__ double row_reg_dot(const double* a, const double (&r)[N]) {
+  double s = 0.0;
+#pragma unroll
+  for (int m = 0; m + 1 < N; m += 2) {
+    const double2 x = *reinterpret_cast<const double2*>(a + m);
+    s += x.x * r[m];
+    s += x.y * r[m + 1];
+  }
+  if (N & 1) s += a[N - 1] * r[N - 1];
+  return s;
+}
+
+// Shared memory: D, D^T, S, S^T rows (padded), then per element the u plane
+// stack and the r/s fluxes.  Every per-thread access to a 1-D matrix is a
+// row, read as double2.
+template <int N>
+struct AxSmem {
+  static constexpr int P = AxLayout<N>::P, Q = AxLayout<N>::Q;
+  static constexpr int PLANE = N * Q, BLK = N * PLANE;
+  static constexpr int MATS = 4 * N * P;   // doubles of D, D^T, S, S^T
+};
+
+// D, D^T, S (Helmholtz) or D, S^T into the block's shared rows
+template <int N, bool HELM>
+__device__ __forceinline__ void ax_load_mats(double* sD, const double* __restrict__ Dg,
+                                             const double* __restrict__ Sg, int tid,
+                                             int nthr) {
+  constexpr int P = AxSmem<N>::P;
+  double* sDT = sD + N * P;
+  double* sS = sDT + N * P;
+  double* sST = sS + N * P;
+  for (int q = tid; q < N * N; q += nthr) {
+    const int r = q / N, c = q % N;
+    const double d = Dg[q], sv = HELM ? Sg[q] : Dg[q];
+    sD[r * P + c] = d;
+    sDT[c * P + r] = d;
+    sS[r * P + c] = sv;
+    sST[c * P + r] = sv;
+  }
+}
+
+// One element's operator, thread (i, j) of its N x N plane owning the
+// k-column (k in registers); FUSEP first forms the direction
+// p = (first ? z - c : beta p + (z - c)) .* mask, stored back into u.  Both
+// block barriers are inside, so every thread of the block calls it (active
+// false for a padding slot).  Returns this thread's share of p . (A p)
+// (FUSEP).  sD: the four matrices (ax_load_mats); su, sw0, sw1: this
+// slot's planes.
+template <int N, typename T, bool HELM, bool FUSEP>
+__device__ __forceinline__ double ax_element(int e, bool active, int i, int j, const double* sD,
+                                             double* su, double* sw0, double* sw1,
+                                             T* __restrict__ u, T* __restrict__ au,
+                                             const T* __restrict__ gf, size_t npts,
+                                             const double* __restrict__ bj, double lambda,
+                                             const T* __restrict__ z, double beta, double c,
+                                             const double* __restrict__ mask, bool first) {
+  constexpr int NN = N * N, P = AxSmem<N>::P, Q = AxSmem<N>::Q, PLANE = AxSmem<N>::PLANE;
+  const double* sDT = sD + N * P;
+  const double* sS = sDT + N * P;
+  const double* sST = sS + N * P;
+  const size_t off = (size_t)(active ? e : 0) * (NN * N) + j * N + i;
+  double ru[N], rw2[N];
+  if (FUSEP) {
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+      double v = 0.0;
+      if (active) {
+        const size_t o = off + (size_t)k * NN;
+        const double zc = (double)z[o] - c;
+        v = first ? zc : beta * (double)u[o] + zc;
+        if (mask) v = v * mask[o];
+        const T vt = (T)v;
+        u[o] = vt;
+        v = (double)vt;
+      }
+      ru[k] = v;
+      su[k * PLANE + j * Q + i] = v;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+      ru[k] = active ? (double)u[off + (size_t)k * NN] : 0.0;
+      su[k * PLANE + j * Q + i] = ru[k];
+    }
+  }
+  __syncthreads();
+  // r-derivative with S for Helmholtz (the swapped deriv_matrix), D otherwise
+  const double* Dx = HELM ? sS : sD;
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+    const double ur = row_dot<N>(Dx + i * P, su + k * PLANE + j * Q);
+    const double us = row_col_dot<N>(sD + j * P, su + k * PLANE + i, Q);
+    const double ut = row_reg_dot<N>(sD + k * P, ru);
+    const size_t o = off + (size_t)k * NN;
+    double g0 = 0, g1 = 0, g2 = 0, g3 = 0, g4 = 0, g5 = 0;
+    if (active) {
+      g0 = (double)__ldg(gf + o);
+      g1 = (double)__ldg(gf + npts + o);
+      g2 = (double)__ldg(gf + 2 * npts + o);
+      g3 = (double)__ldg(gf + 3 * npts + o);
+      g4 = (double)__ldg(gf + 4 * npts + o);
+      g5 = (double)__ldg(gf + 5 * npts + o);
+    }
+    sw0[k * PLANE + j * Q + i] = g0 * ur + g1 * us + g2 * ut;
+    sw1[k * PLANE + j * Q + i] = g1 * ur + g3 * us + g4 * ut;
+    rw2[k] = g2 * ur + g4 * us + g5 * ut;
+  }
+  __syncthreads();
+  // transposed derivatives: r with D^T, s and t with S^T (= D^T for Poisson)
+  double pap = 0.0;   // p . (A p) over this thread's points (FUSEP)
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+    const double acc = row_dot<N>(sDT + i * P, sw0 + k * PLANE + j * Q);
+    const double acs = row_col_dot<N>(sST + j * P, sw1 + k * PLANE + i, Q);
+    const double act = row_reg_dot<N>(sST + k * P, rw2);
+    double out = (acc + acs) + act;
+    if (HELM && active) out += lambda * (__ldg(bj + off + (size_t)k * NN) * ru[k]);
+    if (active) au[off + (size_t)k * NN] = (T)out;
+    if (FUSEP && active) pap += ru[k] * (double)(T)out;
+  }
+  return pap;
+}
+
 }  // namespace dev
 }  // namespace ssg

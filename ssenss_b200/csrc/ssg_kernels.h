@@ -158,6 +158,24 @@ cudaError_t run_helm_diag(cudaStream_t s, size_t npts, size_t nt, const double* 
 cudaError_t run_recip(cudaStream_t s, size_t npts, double* x);
 cudaError_t run_reduce(cudaStream_t s, const double* part, int nblk, int nq, double* sums,
                        const ScalarOp& op);
+// post-smoother CG-Jacobi of a small level (n = 4) in one cooperative
+// launch (coarse.cu): same arithmetic per point as cg_solve's kernels
+struct LevelCgRun {
+  int nel = 0;
+  const void* f = nullptr;
+  void *x = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *aploc = nullptr,
+       *ap = nullptr;
+  const void* gf = nullptr;
+  const double* D = nullptr;
+  const void* dinv = nullptr;
+  const uint8_t* mult = nullptr;
+  const int* pairs = nullptr;
+  double nunique = 1.0, eps = 0.0;
+  int max_iter = 0;
+  double* part = nullptr;
+  size_t part_cap = 0;
+};
+cudaError_t run_level_cg(cudaStream_t s, int device, int n, bool fp32, const LevelCgRun& L);
 // whole CG-Jacobi solve of an n = 2 level in one cooperative launch
 // (coarse.cu); it stops at sqrt((r.r)_w) <= eps, or <= rel times the first
 // residual when rel > 0
