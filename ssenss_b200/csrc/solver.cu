@@ -329,8 +329,9 @@ static ssg_status mg_recurse(ssg_context* c, int L, void* f, void* x, double eps
   // (262,144 points at 4096 elements) is too small to keep the device busy
   // with one launch per kernel, so in FP64 its whole CG runs in one
   // cooperative launch (0.3 ms less per C2 solve).  The FP32-storage
-  // V-cycle keeps the fused two-kernel iteration: the cooperative form's
-  // separately rounded ap cost the outer FCG 16 iterations instead of 11.
+  // V-cycle keeps the fused two-kernel iteration: with FP32 storage the
+  // cooperative form (the unfused arithmetic, ap stored before the update)
+  // took the outer FCG 16 iterations instead of 11 on the C2 solve.
 
   if (F.n == 4 && !fp32) {
     LevelCgRun R;
