@@ -81,7 +81,10 @@ __global__ void __launch_bounds__(256, (N >= 10 ? 1 : 2)) k_ax(int nel, T* __res
 // w = 1 / multiplicity = 1 / (1 + number of contributions).
 // ---------------------------------------------------------------------------
 template <int N, typename T, int MODE>
-__global__ void __launch_bounds__(256) k_dss(int nel, int epb, const T* __restrict__ in,
+// (64 registers, four blocks per SM, except the modes with the longest
+// epilogues)
+__global__ void __launch_bounds__(256, (MODE == DSS_CGUPD || MODE == DSS_DOT2) ? 3 : 4)
+    k_dss(int nel, int epb, const T* __restrict__ in,
                                              T* __restrict__ out,
                                              const int2* __restrict__ pairs,
                                              const int* __restrict__ map,
@@ -91,16 +94,16 @@ __global__ void __launch_bounds__(256) k_dss(int nel, int epb, const T* __restri
                                              double* __restrict__ part,
                                              const double* __restrict__ stop, ScalarOp op,
                                              DssCg cg) {
-  constexpr int NT = N * N * N, NN = N * N;
+  constexpr int NT = N * N * N;
   constexpr int I = N > 2 ? N - 2 : 0, ECI = 12 * I;
   if (stop && *stop != 0.0) return;   // uniform over the block
-  // the order's DSS map, built once at set-up (dss_map_table): the class of
-  // every node in natural order (0 interior; 1<<16 | f<<8 | pos a face
-  // interior; 2<<16 | record an edge node, 3<<16 | record a corner), the node
-  // of face f at face position pos, then the edge/corner source records
-  const int* __restrict__ scls = map;
-  const short* __restrict__ sface = reinterpret_cast<const short*>(map + NT);
-  const int4* __restrict__ ec = reinterpret_cast<const int4*>(map + dss_map_header(N));
+  (void)pairs;
+  // the level's DSS map (dss_map_table): one gather word per local point,
+  // then the edge/corner source records
+  const size_t ntask = (size_t)nel * NT;
+  const int* __restrict__ gword = map;
+  const int4* __restrict__ ec =
+      reinterpret_cast<const int4*>(map + dss_map_records_offset(ntask));
   __shared__ double sred[2 * 32];
   __shared__ double sred4[MODE == DSS_CGUPD ? 4 * 32 : 1];
   (void)epb;
@@ -113,11 +116,10 @@ __global__ void __launch_bounds__(256) k_dss(int nel, int epb, const T* __restri
   T* const cz = reinterpret_cast<T*>(cg.z);
   // one node task per thread, grid-stride over all elements' tasks; no
   // block-wide staging, so no barrier inside the loop
-  const size_t ntask = (size_t)nel * NT;
   const size_t S = (size_t)gridDim.x * blockDim.x;
   // two node tasks in flight per thread (q and q + S): every source of both
   // is resolved and loaded before any sum, branch-free, so their load
-  // chains (class -> pairing or record -> neighbour value) overlap
+  // chains (gather word -> neighbour value, or -> record -> values) overlap
   constexpr int U = 2;
   for (size_t q0 = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q0 < ntask; q0 += U * S) {
     size_t gi[U];
@@ -132,19 +134,19 @@ __global__ void __launch_bounds__(256) k_dss(int nel, int epb, const T* __restri
       ok[u] = q < ntask;
       const size_t qq = ok[u] ? q : 0;
       // nodes in natural order: a warp's own loads and stores are coalesced
-      const int e = (int)(qq / NT), t = (int)(qq - (size_t)e * NT);
+      const int e = (int)(qq / NT);
       gi[u] = qq;
-      const int code = __ldg(scls + t), kind = code >> 16;
-      // face interior: one source, the neighbour face copy; edges and
+      const int gw = __ldg(gword + qq);
+      // face interior: the gather word is the neighbour's copy; edges and
       // corners: the ordered lists of the set-up records (-1 = none)
-      int2 p = make_int2(-1, 0);
-      if (kind == 1) p = __ldg(pairs + (size_t)e * 26 + ((code >> 8) & 0xff));
       int4 a = make_int4(-1, -1, -1, -1), b = make_int4(-1, -1, -1, -1);
-      const int4* rec = ec + (size_t)e * (ECI + 16) + (code & 0xffff);
-      if (kind >= 2) a = __ldg(rec);
-      if (kind == 3) b = __ldg(rec + 1);
-      const int fsrc = p.x >= 0 ? p.x * NT + __ldg(sface + p.y * NN + (code & 0xff)) : -1;
-      src[u][0] = kind == 1 ? fsrc : a.x;
+      if (gw <= -2) {
+        const int code = -gw - 2;
+        const int4* rec = ec + (size_t)e * (ECI + 16) + (code >> 1);
+        a = __ldg(rec);
+        if (code & 1) b = __ldg(rec + 1);
+      }
+      src[u][0] = gw >= 0 ? gw : a.x;
       src[u][1] = a.y;
       src[u][2] = a.z;
       src[u][3] = a.w;

@@ -107,7 +107,8 @@ size_t estimate_bytes(int n, int nel, int precision) {
     const int I = m > 2 ? m - 2 : 0;
     // gf 48, bj, kdiag, dinv_p, dinv_h 32, mult 1, gf32 24, dinv_p32 4
     b += np * 109;
-    b += (size_t)nel * (12 * I * 4 + 64) * sizeof(int);   // DSS edge/corner table
+    b += (size_t)nel * (12 * I * 4 + 64) * sizeof(int);   // DSS edge/corner records
+    b += np * sizeof(int);                                 // DSS gather words
     b += np * 9 * sizeof(double);                          // level work vectors
     if (precision == SSG_PRECISION_MIXED) b += np * 9 * sizeof(float);
   }

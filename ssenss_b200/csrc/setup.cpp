@@ -397,29 +397,34 @@ static void node_sources(const HostMesh& m, int n, int e, int loc, int (&src)[7]
 
 void dss_map_table(const HostMesh& m, int n, std::vector<int>& tab) {
   const int I = n > 2 ? n - 2 : 0;
-  const int nt = n * n * n, nn = n * n;
-  const int head = dss_map_header(n);
+  const int nt = n * n * n;
+  const size_t npts = (size_t)nt * m.nel;
+  const size_t head = dss_map_records_offset(npts);
   const size_t per = (size_t)12 * I * 4 + 8 * 8;
   tab.assign(head + per * m.nel, -1);
-  // node classes, natural order
-  for (int t = 0; t < nt; ++t) tab[t] = 0;
-  for (int f = 0; f < 6; ++f)
-    for (int a = 1; a <= I; ++a)
-      for (int b = 1; b <= I; ++b)
-        tab[face_node(n, f, a, b)] = (1 << 16) | (f << 8) | (a * n + b);
+  // per order: the record code of every edge/corner node, -1 elsewhere
+  std::vector<int> rec(nt, -1);
   for (int q = 0; q < 12; ++q)
-    for (int p = 1; p <= I; ++p) tab[edge_node(n, q, p)] = (2 << 16) | (q * I + p - 1);
-  for (int c = 0; c < 8; ++c) tab[corner_node(n, c)] = (3 << 16) | (12 * I + 2 * c);
-  // face table
-  short* face = reinterpret_cast<short*>(tab.data() + nt);
-  for (int f = 0; f < 6; ++f)
-    for (int a = 0; a < n; ++a)
-      for (int b = 0; b < n; ++b) face[f * nn + a * n + b] = (short)face_node(n, f, a, b);
-  // edge / corner records
+    for (int p = 1; p <= I; ++p) rec[edge_node(n, q, p)] = (q * I + p - 1) << 1;
+  for (int c = 0; c < 8; ++c) rec[corner_node(n, c)] = ((12 * I + 2 * c) << 1) | 1;
   parallel_elements(m.nel, [&](int e0, int e1) {
   for (int e = e0; e < e1; ++e) {
-    int* t = tab.data() + head + per * e;
+    // gather words, natural order: the face neighbour's copy, or the
+    // edge/corner record, or -1 (interior node, or a face without one)
+    int* g = tab.data() + (size_t)e * nt;
     int src[7];
+    for (int t = 0; t < nt; ++t) {
+      const int i = t % n, j = (t / n) % n, k = t / (n * n);
+      const int nb = (i == 0 || i == n - 1) + (j == 0 || j == n - 1) + (k == 0 || k == n - 1);
+      if (nb == 1) {
+        node_sources(m, n, e, t, src);
+        g[t] = src[0] >= 0 ? src[0] : (src[1] >= 0 ? src[1] : src[2]);
+      } else if (nb >= 2) {
+        g[t] = -(2 + rec[t]);
+      }
+    }
+    // edge / corner records
+    int* t = tab.data() + head + per * e;
     for (int q = 0; q < 12; ++q)
       for (int p = 1; p <= I; ++p, t += 4) {
         node_sources(m, n, e, edge_node(n, q, p), src);

@@ -87,16 +87,17 @@ ssg_status build_mesh(HostMesh& m, int n, int nel, const double* vertices,
 ssg_status build_pairs(HostMesh& m, std::string& err);
 void stiffness_diagonal(const HostLevel& L, int nel, double* out);
 void host_dss(const HostMesh& m, int n, double* u);
-// DSS map of order n (one int array, dss_map_header(n) ints of header):
-//   [0, n^3)          class of every node in natural order: 0 interior;
-//                     1<<16 | f<<8 | pos a face-interior node (face f,
-//                     position pos); 2<<16 | r an edge node, 3<<16 | r a
-//                     corner node (r: its record below, in int4 units)
-//   [n^3, ...)        node of face f at face position pos (6 n^2 shorts)
-//   then per element, in class order, the ordered source lists of the edge
-//   nodes (12 (n-2) records of 4 ints: 3 sources + pad) and corner nodes (8
-//   records of 8 ints: 7 sources + pad); a source is element * n^3 + node,
-//   -1 where the node has none.
+// DSS map of one level (one int array):
+//   [0, npts)         one gather word per local point, natural order: the
+//                     index (element * n^3 + node) of the face neighbour's
+//                     copy of a face-interior node; -(2 + (r << 1 | c)) for
+//                     an edge (c = 0) or corner (c = 1) node whose source
+//                     record starts r int4 into its element's records; -1
+//                     for an interior node or a face without a neighbour
+//   then, from dss_map_records_offset(npts), per element the ordered source
+//   lists of the edge nodes (12 (n-2) records of 4 ints: 3 sources + pad)
+//   and corner nodes (8 records of 8 ints: 7 sources + pad); a source is
+//   element * n^3 + node, -1 where the node has none.
 void dss_map_table(const HostMesh& m, int n, std::vector<int>& tab);
 
 // ---------------------------------------------------------------------------

@@ -117,10 +117,10 @@ cudaError_t run_ax(cudaStream_t s, int n, int nel, int epb, bool helm, bool fp32
                    const void* in, void* out, const void* gf, size_t npts,
                    const double* bj, const double* D, const double* S, double lambda,
                    const PUpdateArgs* pua);
-// ints before the edge/corner records of an order-n DSS map: the node class
-// table (n^3 ints) and the face table (6 n^2 shorts), rounded up to 16 bytes
-inline __host__ __device__ constexpr int dss_map_header(int n) {
-  return ((n * n * n + (6 * n * n + 1) / 2) + 3) / 4 * 4;
+// ints before the edge/corner records of a DSS map: one gather word per
+// local point, rounded up to 16 bytes
+inline __host__ __device__ constexpr size_t dss_map_records_offset(size_t npts) {
+  return (npts + 3) / 4 * 4;
 }
 // ec_tab: the DSS map of order n (dss_map_table)
 cudaError_t run_dss(cudaStream_t s, int mode, bool fp32, int n, int nel, const void* in,
