@@ -34,11 +34,11 @@ namespace ssg {
 namespace dev {
 
 // ---------------------------------------------------------------------------
-// solver scalar algebra on the reduced sums (one thread)
-// ---------------------------------------------------------------------------
-// local operator, optionally preceded by the CG direction update
-//   p = ((beta p + (z - c)) .* mask)   (first: p = (z - c) .* mask)
-// (src/solver.c:59-60,75-77 with subtract_nullspace folded in)
+// local operator of every order but 8, optionally preceded by the CG
+// direction update p = ((beta p + (z - c)) .* mask) (first: (z - c) .* mask)
+// (src/solver.c:59-60,75-77 with subtract_nullspace folded in): one element
+// per (N, N) thread plane, epb planes per block; the element body is
+// ax_element (kernels.cuh), shared with the cooperative level smoother
 // ---------------------------------------------------------------------------
 
 template <int N, typename T, bool HELM, bool FUSEP>
