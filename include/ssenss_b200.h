@@ -229,6 +229,12 @@ ssg_status ssg_solve_helmholtz_cg(ssg_context *ctx, int var, const double *f,
  * (src/solver.c:33-81). */
 ssg_status ssg_conjugate_gradient(ssg_context *ctx, int var, const double *f,
 		double *u, double eps, int max_iter, ssg_solve_info *info);
+/* z = r .* diag^-1 of the level-0 operator of var (Poisson for
+ * SSG_PRESSURE, else the Helmholtz operator at the context's lambda):
+ * jacobi_preconditioner (src/precon.c:311-315, diagonal_preconditioner with
+ * omega 1, alpha 0).  z is output only. */
+ssg_status ssg_jacobi_preconditioner(ssg_context *ctx, int var, const double *r,
+		double *z);
 /* One application z = M^-1 r of multigrid_preconditioner
  * (src/precon.c:227-236). */
 ssg_status ssg_multigrid_preconditioner(ssg_context *ctx, const double *r,

@@ -286,6 +286,13 @@ class Context:
                            "conjugate_gradient", history, max_iter)
         return u, info
 
+    def jacobi_preconditioner(self, var, r, z=None):
+        """ssg_jacobi_preconditioner: z = r .* diag^-1 of var's operator."""
+        z = self._out_like(r, z)
+        self._check(self.lib.ssg_jacobi_preconditioner(self.h, int(var), _ptr(r), _ptr(z)),
+                    "jacobi_preconditioner")
+        return z
+
     def multigrid_preconditioner(self, r, z=None, eps=1e-10):
         z = self._out_like(r, z)
         self._check(self.lib.ssg_multigrid_preconditioner(self.h, _ptr(r), _ptr(z), eps),

@@ -91,6 +91,7 @@ SIGNATURES = [
                                          C.c_double, C.c_int, C.POINTER(SolveInfo)]),
     ("ssg_conjugate_gradient", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
                                          C.c_double, C.c_int, C.POINTER(SolveInfo)]),
+    ("ssg_jacobi_preconditioner", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     ("ssg_multigrid_preconditioner", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p,
                                                C.c_double]),
     ("ssg_convection_operator", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p,

@@ -783,6 +783,24 @@ ssg_status ssg_multigrid_preconditioner(ssg_context* c, const double* r, double*
   return stage_back(c, z, dz, np);
 }
 
+ssg_status ssg_jacobi_preconditioner(ssg_context* c, int var, const double* r, double* z) {
+  SSG_TRY(need_ready(c));
+  if (var < SSG_PRESSURE || var > SSG_Z_VELOCITY) return fail(c, SSG_ERR_ARG, "bad var");
+  const DevLevel& L = c->lev[0];
+  const size_t np = L.npts;
+  const double* dr;
+  double* dz;
+  SSG_TRY(stage_in(c, 0, r, np, &dr));
+  SSG_TRY(stage_out(c, 1, z, np, &dz));
+  SSG_TRY(ensure_workspace(c));
+  if (var != SSG_PRESSURE) SSG_TRY(helmholtz_diag_update(c));
+  // z = r .* diag^-1 of the variable's operator (the partial sums of w z the
+  // kernel also forms are not used here)
+  SSG_CUDA(c, run_jacobi(c->stream, false, np, dr, var == SSG_PRESSURE ? L.dinv_p : L.dinv_h,
+                         L.mult, dz, c->d_part, vec_blocks(np)));
+  return stage_back(c, z, dz, np);
+}
+
 ssg_status ssg_setup_dealias(ssg_context* c, int m, const double* deriv,
                              const double* weights, const double* tinv_jac,
                              const double* jac_det, const double* interp) {

@@ -167,6 +167,22 @@ def test_helmholtz_solve(name, var, gpu_ctx_factory):
     assert np.all(np.abs(info["history"] - h_o) <= 1e-9 * h_o[0])
 
 
+@pytest.mark.parametrize("name", ["tgv3_n8", "channel433_n7"])
+def test_jacobi_preconditioner_bitwise(name, gpu_ctx_factory):
+    """z = r .* diag^-1: one product per point, so bitwise r times the
+    context's stored diagonal inverse, and within the diagonals' own 1e-14
+    (Poisson) / 1e-13 (Helmholtz) of the oracle's."""
+    mesh, n, orc, ctx = setup_case(name, gpu_ctx_factory)
+    rng = np.random.default_rng(17)
+    r = rng.standard_normal((mesh.nel, n, n, n))
+    z = ctx.jacobi_preconditioner(O.PRESSURE, r)
+    assert np.array_equal(z, r * ctx.level_data(0, 7))
+    assert rel(z, r * orc.precon(0, 0)) < 1e-14
+    z = ctx.jacobi_preconditioner(O.Y_VELOCITY, r)
+    assert np.array_equal(z, r * ctx.level_data(0, 8))
+    assert rel(z, r * orc.precon(0, 1)) < 1e-13
+
+
 def test_device_pointers(gpu_ctx_factory):
     """CUDA tensors are used in place (no staging)."""
     import torch
