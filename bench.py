@@ -249,8 +249,10 @@ def run_reference(args):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * tot / len(times), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"TGV {args.ne}^3 hex N={n-1} pressure Poisson FCG+p-MG",
-                   "elements": mesh.nel, "n": n, "unique_dofs": udofs},
+        "config": {"workload": (f"TGV {args.ne}^3 hex N={n-1} (n={n}) pressure Poisson, "
+                                f"FCG+p-MG to sqrt((r.r)_w)<=1e-10 from zero"),
+                   "elements": mesh.nel, "n": n, "unique_dofs": udofs,
+                   "parallelism": "1 host core (rank 0)"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
                          "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
