@@ -28,6 +28,7 @@
 // touches only its own slots).
 #include <cuda_runtime.h>
 
+#include <cstdint>
 #include <type_traits>
 
 #include "kernels.cuh"
@@ -42,6 +43,12 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b,
   asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%4,%5};\n"
                : "=d"(d0), "=d"(d1)
                : "d"(a), "d"(b), "d"(c0), "d"(c1));
+}
+
+// Ask L2 for a contiguous chunk ahead of its use (a hint: no destination,
+// no completion to wait for).  Address and size 16-byte multiples.
+__device__ __forceinline__ void bulk_prefetch_l2(const void* p, unsigned bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(p), "r"(bytes) : "memory");
 }
 
 template <typename T, bool HELM, bool FUSEP>
@@ -103,8 +110,25 @@ __global__ void __launch_bounds__(128, 4) k_ax8_dmma(int nel, T* __restrict__ u,
     for (int k = 0; k < N; ++k)
 #pragma unroll
       for (int s = 0; s < 2; ++s) uo[k][s] = val(k * NN + (2 * t + s) * N + g);
+    // the warp's next element: its field (and, fused, z) into L2 now (the
+    // caller's arrays only when 16-byte aligned, as the bulk copy requires;
+    // elements are 16-byte multiples)
+    if (e + warps < nel && lane < (FUSEP ? 2 : 1)) {
+      const T* f = lane == 0 ? (const T*)u : z;
+      if ((reinterpret_cast<uintptr_t>(f) & 15u) == 0)
+        bulk_prefetch_l2(f + (size_t)(e + warps) * NT, NT * sizeof(T));
+    }
 #pragma unroll 1
     for (int k = 0; k < N; ++k) {
+      // the next plane's six metric factors (this element's k + 1, or the
+      // next element's plane 0) into L2 while this plane computes: one
+      // contiguous 64-value chunk per factor in fragment order
+      {
+        const int kn = k + 1 < N ? k + 1 : 0;
+        const int en = k + 1 < N ? e : e + warps;
+        if (lane < 6 && en < nel)
+          bulk_prefetch_l2(gf + lane * npts + (size_t)en * NT + kn * NN, NN * sizeof(T));
+      }
       // forward r: B = u[k][j = g][l = 4c + t]; forward s: A = u[k][l = 4c + t][i = g]
       const double b0 = val(k * NN + g * N + t), b1 = val(k * NN + g * N + 4 + t);
       const double a0 = val(k * NN + t * N + g), a1 = val(k * NN + (4 + t) * N + g);
