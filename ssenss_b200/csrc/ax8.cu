@@ -45,12 +45,6 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b,
                : "d"(a), "d"(b), "d"(c0), "d"(c1));
 }
 
-// Ask L2 for a contiguous chunk ahead of its use (a hint: no destination,
-// no completion to wait for).  Address and size 16-byte multiples.
-__device__ __forceinline__ void bulk_prefetch_l2(const void* p, unsigned bytes) {
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(p), "r"(bytes) : "memory");
-}
-
 template <typename T, bool HELM, bool FUSEP>
 __global__ void __launch_bounds__(128, 4) k_ax8_dmma(int nel, T* __restrict__ u,
                                                      T* __restrict__ au,

@@ -348,6 +348,12 @@ __device__ __forceinline__ void finish_flat(double v, int tid, int nthr,
 }
 
 
+// Ask L2 for a contiguous chunk ahead of its use (a hint: no destination,
+// no completion to wait for).  Address and size 16-byte multiples.
+__device__ __forceinline__ void bulk_prefetch_l2(const void* p, unsigned bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(p), "r"(bytes) : "memory");
+}
+
 // ---------------------------------------------------------------------------
 // element operator building blocks (k_ax in kernels.cu, the small-level
 // cooperative CG in coarse.cu)
