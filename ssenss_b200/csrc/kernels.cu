@@ -238,40 +238,54 @@ __global__ void __launch_bounds__(256, (MODE == DSS_CGUPD || MODE == DSS_DOT2) ?
 // (interpolate_to_grid / integrate_to_grid, src/interpolation.c:136-176):
 // out (no^3) [+]= (A x A x A) in (ni^3), A[o*ni + q] in FP64
 // ---------------------------------------------------------------------------
-template <typename T, bool ADD>
-__global__ void __launch_bounds__(256) k_tensor3(int nel, int ni, int no,
+// epb elements per block (their stages side by side in shared memory); NI,
+// NO > 0: the orders at compile time (contractions unrolled), 0: runtime
+template <typename T, bool ADD, int NI, int NO>
+__global__ void __launch_bounds__(256) k_tensor3(int nel, int ni_rt, int no_rt, int epb,
                                                  const double* __restrict__ A,
                                                  const T* __restrict__ in,
                                                  T* __restrict__ out) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int ni = NI > 0 ? NI : ni_rt, no = NO > 0 ? NO : no_rt;
+  const int nti = ni * ni * ni, nto = no * no * no, n1 = no * ni * ni, n2 = no * no * ni;
   double* sA = reinterpret_cast<double*>(smem_raw);
-  double* sin = sA + no * ni;
-  double* t1 = sin + ni * ni * ni;
-  double* t2 = t1 + no * ni * ni;
-  const int e = blockIdx.x;
-  const int nti = ni * ni * ni, nto = no * no * no;
+  double* sin = sA + no * ni;            // epb x nti
+  double* t1 = sin + epb * nti;          // epb x n1
+  double* t2 = t1 + epb * n1;            // epb x n2
+  const int e0 = blockIdx.x * epb;
+  const int ne = nel - e0 < epb ? nel - e0 : epb;
   for (int q = threadIdx.x; q < no * ni; q += blockDim.x) sA[q] = A[q];
-  for (int q = threadIdx.x; q < nti; q += blockDim.x) sin[q] = (double)in[(size_t)e * nti + q];
+  for (int q = threadIdx.x; q < ne * nti; q += blockDim.x)
+    sin[q] = (double)in[(size_t)e0 * nti + q];
   __syncthreads();
-  for (int q = threadIdx.x; q < no * ni * ni; q += blockDim.x) {
+  for (int qq = threadIdx.x; qq < ne * n1; qq += blockDim.x) {
+    const int el = qq / n1, q = qq - el * n1;
     const int o = q % no, kj = q / no;
+    const double* x = sin + el * nti + kj * ni;
     double s = 0;
-    for (int r = 0; r < ni; ++r) s += sA[o * ni + r] * sin[kj * ni + r];
-    t1[q] = s;
+#pragma unroll
+    for (int r = 0; r < (NI > 0 ? NI : ni); ++r) s += sA[o * ni + r] * x[r];
+    t1[qq] = s;
   }
   __syncthreads();
-  for (int q = threadIdx.x; q < no * no * ni; q += blockDim.x) {
+  for (int qq = threadIdx.x; qq < ne * n2; qq += blockDim.x) {
+    const int el = qq / n2, q = qq - el * n2;
     const int o1 = q % no, o2 = (q / no) % no, k = q / (no * no);
+    const double* x = t1 + el * n1;
     double s = 0;
-    for (int r = 0; r < ni; ++r) s += sA[o2 * ni + r] * t1[(k * ni + r) * no + o1];
-    t2[q] = s;
+#pragma unroll
+    for (int r = 0; r < (NI > 0 ? NI : ni); ++r) s += sA[o2 * ni + r] * x[(k * ni + r) * no + o1];
+    t2[qq] = s;
   }
   __syncthreads();
-  for (int q = threadIdx.x; q < nto; q += blockDim.x) {
+  for (int qq = threadIdx.x; qq < ne * nto; qq += blockDim.x) {
+    const int el = qq / nto, q = qq - el * nto;
     const int o12 = q % (no * no), o3 = q / (no * no);
+    const double* x = t2 + el * n2;
     double s = 0;
-    for (int r = 0; r < ni; ++r) s += sA[o3 * ni + r] * t2[r * no * no + o12];
-    const size_t g = (size_t)e * nto + q;
+#pragma unroll
+    for (int r = 0; r < (NI > 0 ? NI : ni); ++r) s += sA[o3 * ni + r] * x[r * no * no + o12];
+    const size_t g = (size_t)e0 * nto + qq;
     if (ADD)
       out[g] = (T)((double)out[g] + s);
     else
@@ -703,24 +717,38 @@ cudaError_t run_dss(cudaStream_t s, int mode, bool fp32, int n, int nel, const v
                            mask, (const double*)y, (const double*)y2, part, stop, o, g);
 }
 
+template <typename T, bool ADD>
+static cudaError_t launch_tensor3(cudaStream_t s, int nel, int ni, int no, const double* A,
+                                  const T* in, T* out) {
+  // elements per block: their stages within 40 KB of shared memory, <= 8
+  const size_t per = (size_t)ni * ni * ni + (size_t)no * ni * ni + (size_t)no * no * ni;
+  int epb = (int)((40 * 1024 / sizeof(double) - (size_t)no * ni) / per);
+  epb = epb < 1 ? 1 : (epb > 8 ? 8 : epb);
+  const size_t smem = ((size_t)no * ni + epb * per) * sizeof(double);
+  const int grid = (nel + epb - 1) / epb;
+  if (grid < 1) return cudaSuccess;
+  auto kern = &dev::k_tensor3<T, ADD, 0, 0>;
+  // the transfers between consecutive multigrid orders (n, (n - 1)/2 + 1)
+#define SSG_T3(A_, B_)                                                         \
+  if (ni == A_ && no == B_) kern = &dev::k_tensor3<T, ADD, A_, B_>;            \
+  if (ni == B_ && no == A_) kern = &dev::k_tensor3<T, ADD, B_, A_>;
+  SSG_T3(12, 6) SSG_T3(11, 6) SSG_T3(10, 5) SSG_T3(9, 5) SSG_T3(8, 4)
+  SSG_T3(7, 4) SSG_T3(6, 3) SSG_T3(5, 3) SSG_T3(4, 2) SSG_T3(3, 2)
+#undef SSG_T3
+  SSG_COUNT();
+  kern<<<grid, 256, smem, s>>>(nel, ni, no, epb, A, in, out);
+  return cudaGetLastError();
+}
+
 cudaError_t run_tensor3(cudaStream_t s, bool fp32, bool add, int nel, int ni, int no,
                         const double* A, const void* in, void* out) {
-  const size_t smem = ((size_t)no * ni + (size_t)ni * ni * ni + (size_t)no * ni * ni +
-                       (size_t)no * no * ni) * sizeof(double);
-  if (fp32) {
-    if (add)
-      { SSG_COUNT(); k_tensor3<float, true><<<nel, 256, smem, s>>>(nel, ni, no, A, (const float*)in, (float*)out); }
-    else
-      { SSG_COUNT(); k_tensor3<float, false><<<nel, 256, smem, s>>>(nel, ni, no, A, (const float*)in, (float*)out); }
-  } else {
-    if (add)
-      { SSG_COUNT(); k_tensor3<double, true><<<nel, 256, smem, s>>>(nel, ni, no, A, (const double*)in,
-                                                     (double*)out); }
-    else
-      { SSG_COUNT(); k_tensor3<double, false><<<nel, 256, smem, s>>>(nel, ni, no, A, (const double*)in,
-                                                      (double*)out); }
-  }
-  return cudaGetLastError();
+  if (fp32)
+    return add ? launch_tensor3<float, true>(s, nel, ni, no, A, (const float*)in, (float*)out)
+               : launch_tensor3<float, false>(s, nel, ni, no, A, (const float*)in,
+                                              (float*)out);
+  return add ? launch_tensor3<double, true>(s, nel, ni, no, A, (const double*)in, (double*)out)
+             : launch_tensor3<double, false>(s, nel, ni, no, A, (const double*)in,
+                                             (double*)out);
 }
 
 cudaError_t run_helm_diag(cudaStream_t s, size_t npts, size_t nt, const double* kd,
