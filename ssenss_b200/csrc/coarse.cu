@@ -362,18 +362,35 @@ __global__ void __launch_bounds__(256) k_level_cg(LevelCgArgs<T> a) {
     // ap = DSS(aploc), (p w).ap; first: (r w).p, (r w).r (k_dss DOT, k_dots)
     {
       double v[3] = {0.0, 0.0, 0.0};
-      for (size_t q = tid; q < a.npts; q += nthr) {
-        int cnt;
-        const double acc = dss_gather<N, T>(a.aploc, nullptr, a.pairs + (q / NT) * 26, q,
-                                            (int)(q % NT), cnt);
-        const T av = (T)acc;
-        a.ap[q] = av;
-        const double pv = (double)a.p[q];
-        v[0] += (pv * inv_count(1u + (unsigned)cnt)) * (double)av;
-        if (first) {
-          const double rw = (double)a.r[q] * inv_count(a.mult[q]);
-          v[1] += rw * pv;
-          v[2] += rw * (double)a.r[q];
+      // four points per thread at a time: all their gathers are issued
+      // before any store (a store could alias the next gather), then the
+      // points are summed in the same order as one at a time
+      constexpr int U = 4;
+      for (size_t q0 = tid; q0 < a.npts; q0 += U * nthr) {
+        double acc[U];
+        int cnt[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const size_t q = q0 + u * nthr;
+          acc[u] = 0.0;
+          cnt[u] = 0;
+          if (q < a.npts)
+            acc[u] = dss_gather<N, T>(a.aploc, nullptr, a.pairs + (q / NT) * 26, q,
+                                      (int)(q % NT), cnt[u]);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const size_t q = q0 + u * nthr;
+          if (q >= a.npts) break;
+          const T av = (T)acc[u];
+          a.ap[q] = av;
+          const double pv = (double)a.p[q];
+          v[0] += (pv * inv_count(1u + (unsigned)cnt[u])) * (double)av;
+          if (first) {
+            const double rw = (double)a.r[q] * inv_count(a.mult[q]);
+            v[1] += rw * pv;
+            v[2] += rw * (double)a.r[q];
+          }
         }
       }
       block_partials<3>(v, a.partB, sred);
@@ -386,18 +403,38 @@ __global__ void __launch_bounds__(256) k_level_cg(LevelCgArgs<T> a) {
       if (first) rdz = t[1];
       const double alpha = rdz / t[0];
       double v[4] = {0.0, 0.0, 0.0, 0.0};
-      for (size_t q = tid; q < a.npts; q += nthr) {
-        a.x[q] = (T)((double)a.x[q] + alpha * (double)a.p[q]);
-        const T rq = (T)((double)a.r[q] + -alpha * (double)a.ap[q]);
-        a.r[q] = rq;
-        const T zq = (T)((double)rq * (double)a.dinv[q]);
-        a.z[q] = zq;
-        const double w = inv_count(a.mult[q]);
-        const double rw = (double)rq * w;
-        v[0] += rw * (double)zq;
-        v[1] += rw * (double)rq;
-        v[2] += w * (double)zq;
-        v[3] += rw;
+      // four points per thread: every load before any store
+      constexpr int U = 4;
+      for (size_t q0 = tid; q0 < a.npts; q0 += U * nthr) {
+        double xv[U], pv[U], rv[U], av[U], dv[U];
+        unsigned mv[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const size_t q = q0 + u * nthr;
+          const size_t qq = q < a.npts ? q : q0;
+          xv[u] = (double)a.x[qq];
+          pv[u] = (double)a.p[qq];
+          rv[u] = (double)a.r[qq];
+          av[u] = (double)a.ap[qq];
+          dv[u] = (double)a.dinv[qq];
+          mv[u] = a.mult[qq];
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const size_t q = q0 + u * nthr;
+          if (q >= a.npts) break;
+          a.x[q] = (T)(xv[u] + alpha * pv[u]);
+          const T rq = (T)(rv[u] + -alpha * av[u]);
+          a.r[q] = rq;
+          const T zq = (T)((double)rq * dv[u]);
+          a.z[q] = zq;
+          const double w = inv_count(mv[u]);
+          const double rw = (double)rq * w;
+          v[0] += rw * (double)zq;
+          v[1] += rw * (double)rq;
+          v[2] += w * (double)zq;
+          v[3] += rw;
+        }
       }
       block_partials<4>(v, a.partA, sred);
     }
