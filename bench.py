@@ -46,7 +46,7 @@ OP_BYTES_PER_POINT = 64
 # DRAM bytes per launch of that kernel (dram__bytes_read.sum +
 # dram__bytes_write.sum) from the ncu capture of the same workload
 # summarised in profiles/k_ax8_dmma_tgv16_n8.md
-OP_TRAFFIC_BYTES = 117469952 + 4272384
+OP_TRAFFIC_BYTES = 117918464 + 7999744
 
 
 def parse():
