@@ -84,9 +84,8 @@ template <int N, typename T, int MODE>
 // (64 registers, four blocks per SM, except the modes with the longest
 // epilogues)
 __global__ void __launch_bounds__(256, (MODE == DSS_CGUPD || MODE == DSS_DOT2) ? 3 : 4)
-    k_dss(int nel, int epb, const T* __restrict__ in,
+    k_dss(int nel, const T* __restrict__ in,
                                              T* __restrict__ out,
-                                             const int2* __restrict__ pairs,
                                              const int* __restrict__ map,
                                              const double* __restrict__ mask,
                                              const T* __restrict__ y,
@@ -97,7 +96,6 @@ __global__ void __launch_bounds__(256, (MODE == DSS_CGUPD || MODE == DSS_DOT2) ?
   constexpr int NT = N * N * N;
   constexpr int I = N > 2 ? N - 2 : 0, ECI = 12 * I;
   if (stop && *stop != 0.0) return;   // uniform over the block
-  (void)pairs;
   // the level's DSS map (dss_map_table): one gather word per local point,
   // then the edge/corner source records
   const size_t ntask = (size_t)nel * NT;
@@ -106,7 +104,6 @@ __global__ void __launch_bounds__(256, (MODE == DSS_CGUPD || MODE == DSS_DOT2) ?
       reinterpret_cast<const int4*>(map + dss_map_records_offset(ntask));
   __shared__ double sred[2 * 32];
   __shared__ double sred4[MODE == DSS_CGUPD ? 4 * 32 : 1];
-  (void)epb;
   double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
   const double alpha = MODE == DSS_CGUPD ? *cg.alpha : 0.0;
   T* const cx = reinterpret_cast<T*>(cg.x);
@@ -638,13 +635,6 @@ cudaError_t run_ax(cudaStream_t s, int n, int nel, int epb, bool helm, bool fp32
                                            (const double*)gf, npts, nullptr, D, D, 0.0, pu, dop);
 }
 
-int dss_epb(int n) {
-  const int nt = n * n * n;
-  int epb = 1;
-  while (epb * 2 <= 64 && epb * nt < 256) epb *= 2;
-  return epb;
-}
-
 // one 256-thread block per 256 node tasks, capped at bps blocks per SM
 // (the kernel walks the rest grid-stride)
 int dss_grid(int n, int nel) {
@@ -657,29 +647,28 @@ int dss_grid(int n, int nel) {
 
 template <int N, typename T>
 static cudaError_t run_dss_n(cudaStream_t s, int mode, int nel, const T* in, T* out,
-                             const int2* pr, const int* ec_tab, const double* mask, const T* y,
+                             const int* ec_tab, const double* mask, const T* y,
                              const T* y2, double* part, const double* stop,
                              const ScalarOp& op, const DssCg& cg) {
-  const int epb = dss_epb(N);
   const int grd = dss_grid(N, nel);
   switch (mode) {
     case DSS_PLAIN:
-      { SSG_COUNT(); k_dss<N, T, DSS_PLAIN><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, ec_tab, mask, y, y2, part, stop, op, cg); }
+      { SSG_COUNT(); k_dss<N, T, DSS_PLAIN><<<grd, 256, 0, s>>>(nel, in, out, ec_tab, mask, y, y2, part, stop, op, cg); }
       break;
     case DSS_DOT:
-      { SSG_COUNT(); k_dss<N, T, DSS_DOT><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, ec_tab, mask, y, y2, part, stop, op, cg); }
+      { SSG_COUNT(); k_dss<N, T, DSS_DOT><<<grd, 256, 0, s>>>(nel, in, out, ec_tab, mask, y, y2, part, stop, op, cg); }
       break;
     case DSS_DOT2:
-      { SSG_COUNT(); k_dss<N, T, DSS_DOT2><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, ec_tab, mask, y, y2, part, stop, op, cg); }
+      { SSG_COUNT(); k_dss<N, T, DSS_DOT2><<<grd, 256, 0, s>>>(nel, in, out, ec_tab, mask, y, y2, part, stop, op, cg); }
       break;
     case DSS_RESID:
-      { SSG_COUNT(); k_dss<N, T, DSS_RESID><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, ec_tab, mask, y, y2, part, stop, op, cg); }
+      { SSG_COUNT(); k_dss<N, T, DSS_RESID><<<grd, 256, 0, s>>>(nel, in, out, ec_tab, mask, y, y2, part, stop, op, cg); }
       break;
     case DSS_AVG:
-      { SSG_COUNT(); k_dss<N, T, DSS_AVG><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, ec_tab, mask, y, y2, part, stop, op, cg); }
+      { SSG_COUNT(); k_dss<N, T, DSS_AVG><<<grd, 256, 0, s>>>(nel, in, out, ec_tab, mask, y, y2, part, stop, op, cg); }
       break;
     case DSS_CGUPD:
-      { SSG_COUNT(); k_dss<N, T, DSS_CGUPD><<<grd, 256, 0, s>>>(nel, epb, in, out, pr, ec_tab, mask, y, y2, part, stop, op, cg); }
+      { SSG_COUNT(); k_dss<N, T, DSS_CGUPD><<<grd, 256, 0, s>>>(nel, in, out, ec_tab, mask, y, y2, part, stop, op, cg); }
       break;
     default:
       return cudaErrorInvalidValue;
@@ -692,10 +681,10 @@ static cudaError_t run_dss_t(cudaStream_t s, int mode, int n, int nel, const T* 
                              const int* pairs, const int* ec_tab, const double* mask,
                              const T* y, const T* y2, double* part, const double* stop,
                              const ScalarOp& op, const DssCg& cg) {
-  const int2* pr = reinterpret_cast<const int2*>(pairs);
+  (void)pairs;   // folded into the level's gather words at set-up
   switch (n) {
 #define SSG_DSSN(NV) \
-  case NV: return run_dss_n<NV, T>(s, mode, nel, in, out, pr, ec_tab, mask, y, y2, part, stop, op, cg);
+  case NV: return run_dss_n<NV, T>(s, mode, nel, in, out, ec_tab, mask, y, y2, part, stop, op, cg);
     SSG_DSSN(2) SSG_DSSN(3) SSG_DSSN(4) SSG_DSSN(5) SSG_DSSN(6) SSG_DSSN(7)
     SSG_DSSN(8) SSG_DSSN(9) SSG_DSSN(10) SSG_DSSN(11) SSG_DSSN(12)
 #undef SSG_DSSN
