@@ -128,14 +128,22 @@ __global__ void __launch_bounds__(512, 2) k_convection(int nel, int n_rt, int m_
         const double* Dj = sD + j * ds_;
         const double* Dk = sD + k * ds_;
         const int rbase = (k * m + j) * m, sbase = k * m * m + i, tbase = j * m + i;
-        // convective: d v_c / d r_b, then grad through tinv, dotted with u
-        double dr = 0, ds = 0, dt = 0;
+        // convective: d v_c / d r_b; conservative: d_r(u_x v_c), d_s(u_y v_c),
+        // d_t(u_z v_c) -- one pass over l, each matrix entry and each v_c
+        // value loaded once for both (every sum still runs over l in order)
+        double dr = 0, ds = 0, dt = 0, er = 0, es = 0, et = 0;
 #pragma unroll
         for (int l = 0; l < (MC > 0 ? MC : m); ++l) {
-          dr += Di[l] * vc[rbase + l];
-          ds += Dj[l] * vc[sbase + l * m];
-          dt += Dk[l] * vc[tbase + l * m * m];
+          const double di = Di[l], dj = Dj[l], dk = Dk[l];
+          const double vr = vc[rbase + l], vs = vc[sbase + l * m], vt = vc[tbase + l * m * m];
+          dr += di * vr;
+          ds += dj * vs;
+          dt += dk * vt;
+          er += di * (ui[rbase + l] * vr);
+          es += dj * (ui[mt + sbase + l * m] * vs);
+          et += dk * (ui[2 * mt + tbase + l * m * m] * vt);
         }
+        // convective form: grad through tinv, dotted with u
         double d[3];
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
@@ -148,14 +156,7 @@ __global__ void __launch_bounds__(512, 2) k_convection(int nel, int n_rt, int m_
         cv = ui[mt + q] * d[1] + cv;
         cv = ui[2 * mt + q] * d[2] + cv;
         cv = cv * w;
-        // conservative: d_r(u_x v_c), d_s(u_y v_c), d_t(u_z v_c) through tinv
-        double er = 0, es = 0, et = 0;
-#pragma unroll
-        for (int l = 0; l < (MC > 0 ? MC : m); ++l) {
-          er += Di[l] * (ui[rbase + l] * vc[rbase + l]);
-          es += Dj[l] * (ui[mt + sbase + l * m] * vc[sbase + l * m]);
-          et += Dk[l] * (ui[2 * mt + tbase + l * m * m] * vc[tbase + l * m * m]);
-        }
+        // conservative form through tinv
         double cs = 0;
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
