@@ -84,3 +84,24 @@ def test_autotuned_shapes_keep_parity(mk, n, gpu_ctx_factory):
     u_g, info = ctx.solve_poisson_cg(f, np.zeros_like(f))
     if same_stop(info["iterations"], info["history"], h_o):
         assert_solution_close(u_g, u_o, orc, orc.solve_poisson, f)
+
+
+def test_kernel_timing_entry_points(gpu_ctx_factory):
+    """ssg_time_operator / ssg_time_smoother: positive device times for the
+    operator and for the three smoother kernels at every level; a level out
+    of range is an argument error.  They time scratch buffers only, so the
+    operator afterwards still matches the oracle."""
+    mesh, n = tgv_box(3), 8
+    orc = O.Oracle(mesh, n)
+    ctx = gpu_ctx_factory(mesh, n)
+    assert ctx.time_operator(S.PRESSURE, 5) > 0.0
+    assert ctx.time_operator(S.X_VELOCITY, 5) > 0.0
+    for lev in range(len(ctx.orders)):
+        t = ctx.time_smoother(lev, 5)
+        assert set(t) == {"operator", "dss_dot", "cg_update"}
+        assert all(v > 0.0 for v in t.values())
+    with pytest.raises(S.SsgError):
+        ctx.time_smoother(len(ctx.orders), 5)
+    rng = np.random.default_rng(3)
+    u = rng.standard_normal((mesh.nel, n, n, n))
+    assert rel(ctx.global_opeval(O.PRESSURE, u), orc.global_opeval(O.PRESSURE, u)) < 1e-13
