@@ -65,3 +65,37 @@ def test_request_bytes_estimate_is_monotone():
         assert S.request_bytes(n, 64) < S.request_bytes(n + 1 if n < 12 else 12, 64) or n == 12
     # at least the level-0 operator factors and the 24 FCG vectors
     assert S.request_bytes(8, 4096, "fp64") > 4096 * 512 * (48 + 24 * 8)
+
+
+def test_gll_matches_the_oracle():
+    """ssg_gll (host only): the library's GLL points and weights against the
+    oracle's restatement of src/basis.c, every order the library builds."""
+    import numpy as np
+    import oracle as O
+    from ssenss_b200 import _lib
+    lib = _lib.load()
+    for n in range(2, 19):
+        x, w = np.empty(n), np.empty(n)
+        assert lib.ssg_gll(n, x.ctypes.data_as(_lib._dp), w.ctypes.data_as(_lib._dp)) == 0
+        xo, wo = O.Oracle.gll(n)
+        assert np.max(np.abs(x - xo)) <= 4e-16 and np.max(np.abs(w - wo)) <= 4e-16, n
+        assert x[0] == -1.0 and x[-1] == 1.0
+        assert abs(w.sum() - 2.0) < 1e-14
+    x, w = np.empty(1), np.empty(1)
+    assert lib.ssg_gll(1, x.ctypes.data_as(_lib._dp), w.ctypes.data_as(_lib._dp)) == 1
+
+
+def test_default_launch_shapes():
+    """ssg_tuning (host only) before any autotuning: the FP64 tensor-core
+    operator at n = 8, positive shapes elsewhere, orders out of range
+    rejected."""
+    import ssenss_b200 as S
+    t8 = S.tuning(8)
+    assert t8["ax_elements_per_block"] == 0
+    for n in (2, 4, 6, 10, 12):
+        t = S.tuning(n)
+        assert t["ax_elements_per_block"] >= 1
+        assert t["dss_blocks_per_sm"] >= 1 and t["vector_blocks_per_sm"] >= 1
+    for bad in (1, 19):
+        with pytest.raises(S.SsgError):
+            S.tuning(bad)
