@@ -203,9 +203,12 @@ ssg_status ssg_global_dot_product(ssg_context *ctx, const double *x,
  * under a fixed budget, or a loop that must not take cudaMalloc's implicit
  * synchronisation).  Its block partial sums live in one fixed 512 KiB array
  * per GPU shared by every call: n above 134,217,728 is rejected with
- * SSG_ERR_ARG, host pointers likewise, and calls that overlap on the GPU
- * race on the array.  The first call on a device looks the array's address
- * up; make that call before any stream capture on the device.
+ * SSG_ERR_ARG, host pointers and pointers to another GPU's memory likewise
+ * (every array must live on the current device, or be managed memory), and
+ * calls that overlap on the GPU race on the array.  The first call on a
+ * device looks the array's address up; make that call before any stream
+ * capture on the device.  The address is kept for the life of the process;
+ * calls after a cudaDeviceReset are not supported.
  * No counterpart in the reference. */
 ssg_status ssg_weighted_dot_noalloc(const double *x, const double *y,
 		const double *w, size_t n, double *result, void *cuda_stream);

@@ -10,6 +10,7 @@
 // Each block reduces the same block partials in the same order, so every
 // block takes the same alpha, beta and stop decision, and the result does
 // not depend on timing.  The loop is bounded by max_iter.
+#include <atomic>
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
@@ -453,7 +454,29 @@ __global__ void __launch_bounds__(256) k_level_cg(LevelCgArgs<T> a) {
 
 }  // namespace dev
 
-static int g_coarse_grid[SSG_MAXLEV * 8] = {0};
+// Blocks per device that a cooperative launch may use, filled on first use.
+// Serving worker threads launch concurrently, so the entries are atomics; a
+// race only repeats the same occupancy query and stores the same value.
+static constexpr int kMaxDevices = 64;
+static std::atomic<int> g_coarse_grid[kMaxDevices];
+static std::atomic<int> g_level_grid[2][kMaxDevices];
+
+static cudaError_t cooperative_cap(std::atomic<int>& slot, const void* kernel, size_t smem,
+                                   int device, int* out) {
+  int c = slot.load(std::memory_order_relaxed);
+  if (c == 0) {
+    int per_sm = 0, nsm = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, smem);
+    if (e != cudaSuccess) return e;
+    e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
+    if (e != cudaSuccess) return e;
+    c = per_sm * nsm;
+    if (c < 1) return cudaErrorCooperativeLaunchTooLarge;
+    slot.store(c, std::memory_order_relaxed);
+  }
+  *out = c;
+  return cudaSuccess;
+}
 
 cudaError_t run_coarse_cg(cudaStream_t s, int device, int nel, const double* f, double* x,
                           double* r, double* z, double* p, double* aploc, double* ap,
@@ -481,17 +504,11 @@ cudaError_t run_coarse_cg(cudaStream_t s, int device, int nel, const double* f, 
   a.rel = rel;
   a.max_iter = max_iter;
   a.frame = frame;
-  int& cap = g_coarse_grid[device & (SSG_MAXLEV * 8 - 1)];
-  if (cap == 0) {
-    int per_sm = 0, nsm = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dev::k_coarse_cg,
-                                                                  256, 0);
-    if (e != cudaSuccess) return e;
-    e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
-    if (e != cudaSuccess) return e;
-    cap = per_sm * nsm;
-    if (cap < 1) return cudaErrorCooperativeLaunchTooLarge;
-  }
+  if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
+  int cap = 0;
+  cudaError_t ce = cooperative_cap(g_coarse_grid[device], (const void*)dev::k_coarse_cg, 0,
+                                   device, &cap);
+  if (ce != cudaSuccess) return ce;
   int G = (int)((a.npts + 255) / 256);
   if (G > cap) G = cap;
   // blocks per SM beyond what the occupancy query guarantees are never used
@@ -532,18 +549,11 @@ static cudaError_t launch_level_cg4(cudaStream_t s, int device, const LevelCgRun
   a.max_iter = L.max_iter;
   const size_t smem = dev::level_cg_smem<N>();
   // blocks the device runs at once (a cooperative launch must not exceed it)
-  static int cap[2][64] = {{0}};
-  int& c = cap[sizeof(T) == 4][device & 63];
-  if (c == 0) {
-    int per_sm = 0, nsm = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &per_sm, dev::k_level_cg<N, T>, 256, smem);
-    if (e != cudaSuccess) return e;
-    e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
-    if (e != cudaSuccess) return e;
-    c = per_sm * nsm;
-    if (c < 1) return cudaErrorCooperativeLaunchTooLarge;
-  }
+  if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
+  int c = 0;
+  cudaError_t ce = cooperative_cap(g_level_grid[sizeof(T) == 4][device],
+                                   (const void*)dev::k_level_cg<N, T>, smem, device, &c);
+  if (ce != cudaSuccess) return ce;
   const int groups = (L.nel + 15) / 16;
   int G = groups < c ? groups : c;
   if ((size_t)7 * G > L.part_cap) G = (int)(L.part_cap / 7);

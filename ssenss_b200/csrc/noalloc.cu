@@ -24,7 +24,13 @@
 //
 // The first call on a device looks up the array's device address with
 // cudaGetSymbolAddress (once per device, with that device current); make
-// that first call before any stream capture on the device.
+// that first call before any stream capture on the device.  The address is
+// cached for the life of the process: a cudaDeviceReset unloads the module,
+// and calls after it are not supported.
+//
+// Every pointer must be device memory of the current device (or managed
+// memory); host memory and another GPU's memory are rejected with
+// SSG_ERR_ARG.
 #include <cuda_runtime.h>
 
 #include <cstddef>
@@ -91,19 +97,23 @@ k_wdot_final(int nblk, const double* __restrict__ partials, double* __restrict__
 std::mutex g_mu;
 double* g_partials_addr[SSG_NOALLOC_MAX_DEVICES] = {};
 
-bool on_device(const void* p) {
+// true for device memory of GPU `dev` (the current device) and for managed
+// memory; false for host memory and for another GPU's device memory, which a
+// kernel on `dev` would reach only through peer access, if at all
+bool on_device(const void* p, int dev) {
   cudaPointerAttributes a;
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
     cudaGetLastError();
     return false;
   }
-  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+  if (a.type == cudaMemoryTypeManaged) return true;
+  return a.type == cudaMemoryTypeDevice && a.device == dev;
 }
 
-// device address of g_noalloc_partials on the current device (looked up once)
-ssg_status partials_address(double** out) {
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return SSG_ERR_CUDA;
+// device address of g_noalloc_partials on device `dev`, the current device
+// (looked up once per device; the cached address does not survive a
+// cudaDeviceReset, after which the module loads anew)
+ssg_status partials_address(int dev, double** out) {
   if (dev < 0 || dev >= SSG_NOALLOC_MAX_DEVICES) return SSG_ERR_ARG;
   std::lock_guard<std::mutex> lock(g_mu);
   if (!g_partials_addr[dev]) {
@@ -126,7 +136,13 @@ extern "C" ssg_status ssg_weighted_dot_noalloc(const double* x, const double* y,
   if (!x || !y || !w || !result) return SSG_ERR_ARG;
   const size_t max_points = (size_t)SSG_NOALLOC_MAX_BLOCKS * SSG_NOALLOC_POINTS_PER_BLOCK;
   if (n > max_points) return SSG_ERR_ARG;
-  if (!on_device(x) || !on_device(y) || !on_device(w) || !on_device(result))
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return SSG_ERR_CUDA;
+  }
+  if (!on_device(x, dev) || !on_device(y, dev) || !on_device(w, dev) ||
+      !on_device(result, dev))
     return SSG_ERR_ARG;
   cudaStream_t s = (cudaStream_t)cuda_stream;
   if (n == 0) {
@@ -134,7 +150,7 @@ extern "C" ssg_status ssg_weighted_dot_noalloc(const double* x, const double* y,
     return SSG_OK;
   }
   double* partials = nullptr;
-  const ssg_status st = partials_address(&partials);
+  const ssg_status st = partials_address(dev, &partials);
   if (st != SSG_OK) return st;
   const int nblk = (int)((n + SSG_NOALLOC_POINTS_PER_BLOCK - 1) / SSG_NOALLOC_POINTS_PER_BLOCK);
   k_wdot_partials<<<nblk, SSG_NOALLOC_THREADS, 0, s>>>(n, x, y, w, partials);

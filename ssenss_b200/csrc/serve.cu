@@ -210,7 +210,13 @@ ssg_status run_request(ssg_server* S, Request* r, Resident* slot) {
     slot->ctx = c;
     ssg_set_setup_options(c, SSG_SETUP_NO_DEALIAS | SSG_SETUP_NO_PARTICLES);
     ssg_status st = ssg_setup_mesh(c, r->d.n, r->d.nel, r->vert.data(), r->neigh.data());
-    if (st != SSG_OK) return st;
+    if (st != SSG_OK) {
+      // a context whose set-up failed never serves: the worker then drops
+      // the slot, so later requests with this mesh key set up afresh
+      ssg_destroy(c);
+      slot->ctx = nullptr;
+      return st;
+    }
   }
   c->cancel = &r->cancel;
   c->deadline = r->deadline;

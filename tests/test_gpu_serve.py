@@ -139,3 +139,27 @@ def test_request_bytes_covers_the_context():
         est = S.request_bytes(n, mesh.nel, "mixed")
         assert used <= est, (i, used, est)
         assert used >= 0.7 * est, (i, used, est)
+
+
+def test_failed_setup_does_not_poison_the_mesh_key():
+    """A request whose mesh fails set-up (here a neighbour id out of range)
+    leaves no context behind: the next request with the same mesh key sets
+    the mesh up afresh and succeeds."""
+    mesh, n, lam, f = inputs(0)
+    bad = box_mesh((3, 3, 3))
+    bad.neigh = np.array(bad.neigh, copy=True)
+    bad.neigh[0, 0] = bad.nel + 5
+    srv = S.Server(0, hbm_budget=40e9, max_active=2)
+    try:
+        key = 0x5EED
+        _, st, _ = srv.wait(srv.submit(bad, n, f, key=key))
+        assert st == "SSG_ERR_MESH"
+        u, st, _ = srv.wait(srv.submit(mesh, n, f, key=key))
+        assert st == "SSG_OK"
+        stats = srv.stats()
+        assert stats["resident_contexts"] == 1
+    finally:
+        srv.close()
+    orc = oracle_for(0)
+    u_o, _ = orc.solve_poisson(f, np.zeros_like(f))
+    assert rel(u - u.mean(), u_o - u_o.mean()) < 1e-8

@@ -6,9 +6,11 @@ entry point keeps its partial sums in one fixed device array shared by all
 calls, so this file is collected last and the check runs twice in a row:
 the second call must not be disturbed by what the first left in the array.
 Results are compared, through the C ABI, with ssg_global_dot_product under
-the dot-product tolerance of the other parity tests.
+the dot-product tolerance of the other parity tests, and at a size of many
+hundred blocks with an exactly rounded sum of the same products on the host.
 """
 import ctypes as C
+import math
 
 import numpy as np
 import pytest
@@ -50,6 +52,31 @@ def test_noalloc_dot_matches_context_dot():
                         ctx.global_dot_product(y_host, y_host))
         assert abs(got - want) <= 1e-12 * scale, (call, got, want)
     ctx.close()
+
+
+def test_noalloc_dot_many_blocks_matches_exact_sum():
+    """2,000,000 points (977 partial sums, so the final kernel's strided loop
+    over the partials runs) against math.fsum of the products (x*w)*y."""
+    import torch
+
+    import ssenss_b200 as S
+
+    lib = S._lib.load()
+    rng = np.random.default_rng(12)
+    npts = 2_000_000
+    w_host = 1.0 / rng.choice([1.0, 2.0, 4.0, 8.0], npts)
+    result = torch.zeros(1, dtype=torch.float64, device="cuda")
+    for call in range(2):
+        x_host = rng.standard_normal(npts)
+        y_host = rng.standard_normal(npts)
+        x, y, w = (torch.from_numpy(a).cuda() for a in (x_host, y_host, w_host))
+        torch.cuda.synchronize()
+        assert lib.ssg_weighted_dot_noalloc(_dev(x), _dev(y), _dev(w), npts, _dev(result),
+                                            None) == 0
+        torch.cuda.synchronize()
+        want = math.fsum((x_host * w_host) * y_host)
+        scale = np.linalg.norm(x_host) * np.linalg.norm(y_host)
+        assert abs(float(result.item()) - want) <= 1e-12 * scale, (call, result.item(), want)
 
 
 def test_noalloc_rejects_bad_arguments():
