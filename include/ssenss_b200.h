@@ -107,9 +107,17 @@ ssg_status ssg_set_graphs(ssg_context *ctx, int enable);
 
 /* Set-up options of the next ssg_setup_mesh (no reference counterpart):
  * skip the dealiasing grid (convection unavailable) and/or the particle
- * geometry, for contexts that only solve -- e.g. the serving loop's. */
+ * geometry, for contexts that only solve -- e.g. the serving loop's.
+ * SSG_SETUP_OPPOSITE_PAIRING pairs each face, edge and corner with the
+ * geometrically opposite one of its neighbour (west with east, ...) instead
+ * of the reference's first match (src/init.c:68-130, 298-320), which with
+ * one or two elements along a periodic direction pairs west with west and
+ * so solves a different, wrong system.  On meshes with three or more
+ * elements in every direction both pairings are the same; the serving loop
+ * uses the opposite pairing for every request. */
 #define SSG_SETUP_NO_DEALIAS 1u
 #define SSG_SETUP_NO_PARTICLES 2u
+#define SSG_SETUP_OPPOSITE_PAIRING 4u
 ssg_status ssg_set_setup_options(ssg_context *ctx, unsigned flags);
 /* Device memory (bytes) the context holds now. */
 ssg_status ssg_memory_info(const ssg_context *ctx, size_t *device_bytes);
@@ -250,6 +258,12 @@ ssg_status ssg_multigrid_preconditioner(ssg_context *ctx, const double *r,
  * u (advecting), v (advected), udv: 3 x nel x n^3. */
 ssg_status ssg_convection_operator(ssg_context *ctx, const double *u,
 		const double *v, double *udv);
+/* convection_operator for the elements first .. first+count-1 only: the
+ * reference's own per-element call (src/convection.c:31-35, one element per
+ * call from src/time.c:115-117 and src/navier_stokes.c:82) is count = 1.
+ * u, v, udv: 3 x count x n^3 (component-major over the range). */
+ssg_status ssg_convection_elements(ssg_context *ctx, int first, int count,
+		const double *u, const double *v, double *udv);
 
 /* ---- launch-shape autotuner (no reference counterpart) ---------------------- */
 
@@ -261,8 +275,9 @@ ssg_status ssg_convection_operator(ssg_context *ctx, const double *u,
  * order. */
 ssg_status ssg_autotune(ssg_context *ctx, int reps);
 /* Device time of the level-0 element operator (var: Poisson or Helmholtz,
- * FP64) in microseconds per apply: reps launches back to back on the
- * context's stream between two CUDA events, best of three trials. */
+ * FP64) in microseconds per apply, on a deterministic pseudo-random field:
+ * reps launches back to back on the context's stream between two CUDA
+ * events, best of three trials. */
 ssg_status ssg_time_operator(ssg_context *ctx, int var, int reps,
 		double *us_per_apply);
 /* Device time of the three kernels of one smoother CG iteration at a

@@ -26,6 +26,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "libssg_oracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libssenss_ref.so")
+# the same reference with its solve path bound to libssenss_b200 through the
+# C binding ssenss_b200/shim/ssenss_gpu_shim.c (needs a GPU to run)
+REF_GPU_SO = os.path.join(HERE, "_ref", "libssenss_ref_gpu.so")
 
 PRESSURE, X_VELOCITY, Y_VELOCITY, Z_VELOCITY = 0, 1, 2, 3
 
@@ -274,13 +277,17 @@ class Reference(_Common):
     """The reference sources compiled in place (see module docstring)."""
 
     _lib = None
+    _path = REF_SO
 
     @classmethod
     def lib(cls):
         if cls._lib is None:
-            if not os.path.exists(REF_SO):
-                raise FileNotFoundError(REF_SO)
-            L = C.CDLL(REF_SO)
+            if not os.path.exists(cls._path):
+                raise FileNotFoundError(cls._path)
+            L = C.CDLL(cls._path)
+            L.ssgref_step_log_count.restype = C.c_int
+            L.ssgref_step_log_entry.argtypes = [C.c_int, _ip, _ip, _dp, C.c_int]
+            L.ssgref_step_log_entry.restype = C.c_int
             L.ssgref_setup.argtypes = [C.c_int, C.c_int, _dp, _ip, C.c_double,
                                        C.c_double, C.c_double]
             L.ssgref_setup.restype = C.c_int
@@ -430,6 +437,20 @@ class Reference(_Common):
     def ns_step(self):
         self.lib().ssgref_ns_step()
 
+    def step_log(self, clear=True):
+        """Every solve the Navier-Stokes steps ran since the last clear:
+        list of (kind 0 Poisson / 1 Helmholtz, var, residual history)."""
+        L = self.lib()
+        out = []
+        hist = np.zeros(5001)
+        kind, var = C.c_int(), C.c_int()
+        for i in range(L.ssgref_step_log_count()):
+            k = L.ssgref_step_log_entry(i, C.byref(kind), C.byref(var), _d(hist), len(hist))
+            out.append((kind.value, var.value, hist[:min(k, len(hist))].copy()))
+        if clear:
+            L.ssgref_step_log_clear()
+        return out
+
     def time(self):
         return self.lib().ssgref_time()
 
@@ -464,3 +485,15 @@ class Reference(_Common):
         ints = np.ascontiguousarray(ints, dtype=np.int32).copy()
         self.lib().ssgref_particles_advance(state.shape[0], _d(state), _i(ints))
         return state, ints
+
+
+class ReferenceGPU(Reference):
+    """The reference with its solve path on the GPU: the same harness and
+    entry points as Reference, built against the library's C binding
+    (ssenss_b200/shim/ssenss_gpu_shim.c).  Its library and Reference's can
+    live in one process (each resolves its own symbols), but a failure inside
+    the binding ends the process through the reference's fatal_error, so
+    tests run it in a child process."""
+
+    _lib = None
+    _path = REF_GPU_SO

@@ -16,6 +16,18 @@
  * flexible_conjugate_gradient (src/solver.c:72-73,151-152) is exactly the
  * residual check; the nullspace norm (x == y == ones, src/solver.c:207) is
  * filtered out.
+ *
+ * Built a second time with SSGREF_GPU_SHIM defined, into
+ * oracle/_ref/libssenss_ref_gpu.so: the same reference sources with the
+ * solve path taken by the library's C-ABI binding
+ * (ssenss_b200/shim/ssenss_gpu_shim.c), attached right after
+ * initialise_preconditioners as a host would attach it.  Histories then come
+ * from the binding's record of each solve.
+ *
+ * Navier-Stokes steps: src/navier_stokes.c is compiled with its calls to
+ * solve_poisson_cg / solve_helmholtz_cg renamed to ssgref_step_poisson /
+ * ssgref_step_helmholtz, which log every solve of a step (kind, variable,
+ * residual history) and then call the real solve.
  */
 #include <math.h>
 #include <stdio.h>
@@ -43,6 +55,9 @@
 #include "time.h"
 #include "test.h"
 #include "synth_dataio.h"
+#ifdef SSGREF_GPU_SHIM
+#include "ssenss_gpu_shim.h"
+#endif
 
 double ssgref_dot_impl(struct element **sel, double ****x, double ****y);
 void ssgref_mg_impl(struct element **sel, double ****x, double ****px,
@@ -107,6 +122,9 @@ void ssgref_teardown(void)
 {
 	if (!H_sel)
 		return;
+#ifdef SSGREF_GPU_SHIM
+	ssenss_gpu_detach();
+#endif
 	free_basis(H_gll);
 	free_basis(H_conv);
 	disconnect_elements(H_sel);
@@ -152,6 +170,9 @@ int ssgref_setup(int n, int nel, const double *vertices, const int *neigh,
 	H_sel = new_elements(H_geom, H_cgeom, H_gll, H_conv, H_params, H_comm);
 	connect_elements(H_sel);
 	initialise_preconditioners(H_sel);
+#ifdef SSGREF_GPU_SHIM
+	ssenss_gpu_attach(H_sel, 0);
+#endif
 	H_nel = nel;
 	H_n = n;
 	return (*H_sel)->precon->nlevels;
@@ -383,7 +404,85 @@ static void begin_record(double *hist, int cap)
 static int end_record(void)
 {
 	H_recording = 0;
+#ifdef SSGREF_GPU_SHIM
+	/* the binding's record of the solve just run */
+	const struct ssenss_gpu_solve *g = ssenss_gpu_last_solve();
+	H_hist_len = g->history_len;
+	memcpy(H_hist, g->history, (size_t) (H_hist_len < H_hist_cap
+			? H_hist_len : H_hist_cap) * sizeof(double));
+#endif
 	return H_hist_len;
+}
+
+/* ---- per-solve log of Navier-Stokes steps ---- */
+
+struct step_solve {
+	int kind;      /* 0 Poisson, 1 Helmholtz */
+	int var;
+	int len;
+	double *hist;
+};
+static struct step_solve *H_steplog;
+static int H_steplog_len, H_steplog_cap;
+
+static void step_record(int kind, int var, const double *hist, int len)
+{
+	if (H_steplog_len == H_steplog_cap) {
+		H_steplog_cap = H_steplog_cap ? 2 * H_steplog_cap : 64;
+		H_steplog = realloc(H_steplog, H_steplog_cap * sizeof(*H_steplog));
+	}
+	struct step_solve *r = &H_steplog[H_steplog_len++];
+	r->kind = kind;
+	r->var = var;
+	r->len = len;
+	r->hist = malloc((len ? len : 1) * sizeof(double));
+	memcpy(r->hist, hist, (size_t) len * sizeof(double));
+}
+
+void ssgref_step_log_clear(void)
+{
+	for (int i = 0; i < H_steplog_len; ++i)
+		free(H_steplog[i].hist);
+	H_steplog_len = 0;
+}
+
+int ssgref_step_log_count(void)
+{
+	return H_steplog_len;
+}
+
+/* Solve i of the log: kind, var and up to cap history values; returns the
+ * history length. */
+int ssgref_step_log_entry(int i, int *kind, int *var, double *hist, int cap)
+{
+	if (i < 0 || i >= H_steplog_len)
+		return -1;
+	const struct step_solve *r = &H_steplog[i];
+	*kind = r->kind;
+	*var = r->var;
+	memcpy(hist, r->hist, (size_t) (r->len < cap ? r->len : cap)
+			* sizeof(double));
+	return r->len;
+}
+
+static double H_step_hist[5001];
+
+void ssgref_step_poisson(struct element **sel, double ****f, int var,
+		double eps)
+{
+	begin_record(H_step_hist, 5001);
+	solve_poisson_cg(sel, f, var, eps);
+	const int len = end_record();
+	step_record(0, var, H_step_hist, len < 5001 ? len : 5001);
+}
+
+void ssgref_step_helmholtz(struct element **sel, double ****f, int var,
+		double eps)
+{
+	begin_record(H_step_hist, 5001);
+	solve_helmholtz_cg(sel, f, var, eps);
+	const int len = end_record();
+	step_record(1, var, H_step_hist, len < 5001 ? len : 5001);
 }
 
 /* Poisson: var = PRESSURE, initial guess in u (overwritten by the result). */
@@ -428,9 +527,13 @@ double ssgref_fcg_mg(const double *f, double *u, double eps, int max_iter)
 {
 	double ****F = from_flat(f);
 	double ****U = from_flat(u);
+#ifdef SSGREF_GPU_SHIM
+	void (*mg)() = (void (*)()) multigrid_preconditioner;
+#else
+	void (*mg)() = (void (*)()) ssgref_mg_hook;
+#endif
 	double err = flexible_conjugate_gradient(H_sel, F, U, PRESSURE,
-			discrete_laplace_operator, ssgref_mg_hook, eps,
-			max_iter);
+			discrete_laplace_operator, mg, eps, max_iter);
 	memcpy(u, ***U, npts() * sizeof(double));
 	free_4d_array(F);
 	free_4d_array(U);

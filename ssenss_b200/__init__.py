@@ -136,9 +136,12 @@ class Context:
         self._check(self.lib.ssg_autotune(self.h, int(reps)), "autotune")
         return {n: tuning(n) for n in sorted(set(self.orders))}
 
-    def set_setup_options(self, no_dealias=False, no_particles=False):
-        """ssg_set_setup_options for the next setup_mesh."""
-        flags = (1 if no_dealias else 0) | (2 if no_particles else 0)
+    def set_setup_options(self, no_dealias=False, no_particles=False, opposite_pairing=False):
+        """ssg_set_setup_options for the next setup_mesh (opposite_pairing:
+        SSG_SETUP_OPPOSITE_PAIRING, the correct pairing of meshes with one or
+        two elements along a periodic direction)."""
+        flags = (1 if no_dealias else 0) | (2 if no_particles else 0) | \
+            (4 if opposite_pairing else 0)
         self._check(self.lib.ssg_set_setup_options(self.h, flags), "set_setup_options")
 
     def memory_bytes(self) -> int:
@@ -304,6 +307,15 @@ class Context:
         out = self._out_like(u, out)
         self._check(self.lib.ssg_convection_operator(self.h, _ptr(u), _ptr(v), _ptr(out)),
                     "convection_operator")
+        return out
+
+    def convection_elements(self, first, u, v, out=None):
+        """ssg_convection_elements: convection of the elements first ..
+        first + count - 1, fields shaped (3, count, n, n, n)."""
+        out = self._out_like(u, out)
+        self._check(self.lib.ssg_convection_elements(self.h, int(first), int(u.shape[1]),
+                                                     _ptr(u), _ptr(v), _ptr(out)),
+                    "convection_elements")
         return out
 
     def set_particle_velocity(self, ur):

@@ -96,6 +96,8 @@ SIGNATURES = [
                                                C.c_double]),
     ("ssg_convection_operator", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p,
                                           C.c_void_p]),
+    ("ssg_convection_elements", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p,
+                                          C.c_void_p, C.c_void_p]),
     ("ssg_kernel_launch_count", C.c_ulonglong, []),
     ("ssg_autotune", C.c_int, [C.c_void_p, C.c_int]),
     ("ssg_set_setup_options", C.c_int, [C.c_void_p, C.c_uint]),

@@ -75,9 +75,9 @@ static void free_mesh(ssg_context* c) {
   for (auto& l : c->lev) free_level(l);
   dfree(c->d_pairs); c->d_pairs = nullptr;
   dfree(c->inv_mass); c->inv_mass = nullptr;
-  dfree(c->conv_tinv); dfree(c->conv_bj); dfree(c->conv_D); dfree(c->conv_J);
+  dfree(c->conv_w); dfree(c->conv_D); dfree(c->conv_J);
   dfree(c->conv_scratch);
-  c->conv_tinv = c->conv_bj = c->conv_D = c->conv_J = c->conv_scratch = nullptr;
+  c->conv_w = c->conv_D = c->conv_J = c->conv_scratch = nullptr;
   c->m = 0;
   dfree(c->p_jac); dfree(c->p_tinv); dfree(c->p_ur); dfree(c->p_x);
   c->p_jac = c->p_tinv = c->p_ur = c->p_x = nullptr;
@@ -104,25 +104,32 @@ static std::vector<double> rho3(const std::vector<double>& w) {
   return r;
 }
 
-// Dealiasing-grid factors: tinv (9 x nel x m^3), rho J at the m points, the
-// m-point derivative matrix and the n -> m interpolation matrix
-// (initialise_convection_geometry, src/main.c:60-64, src/geometry.c).
+// Dealiasing-grid factors (initialise_convection_geometry, src/main.c:60-64,
+// src/geometry.c): W[3b + a] = rho J tinv[a][b] / 2 at the m points (9 x nel
+// x m^3: the convection kernel's per-direction weights), the m-point
+// derivative matrix and the n -> m interpolation matrix.
 static ssg_status upload_conv(ssg_context* c) {
   const ssg::HostMesh& H = c->host;
   const ssg::HostLevel& m = H.conv;
   const int nel = H.nel;
-  dfree(c->conv_tinv); dfree(c->conv_bj); dfree(c->conv_D); dfree(c->conv_J);
+  dfree(c->conv_w); dfree(c->conv_D); dfree(c->conv_J);
   dfree(c->conv_scratch);
-  c->conv_tinv = c->conv_bj = c->conv_D = c->conv_J = c->conv_scratch = nullptr;
+  c->conv_w = c->conv_D = c->conv_J = c->conv_scratch = nullptr;
   c->m = m.n;
   const size_t mp = m.nt * nel;
-  std::vector<double> tv(9 * mp), cb(mp);
-  for (int a = 0; a < 9; ++a) std::copy(m.tinv[a].begin(), m.tinv[a].end(), tv.begin() + a * mp);
   const std::vector<double> rho = rho3(m.w);
-  for (int e = 0; e < nel; ++e)
-    for (size_t q = 0; q < m.nt; ++q) cb[e * m.nt + q] = rho[q] * m.det[e * m.nt + q];
-  SSG_TRY(dupload(c, &c->conv_tinv, tv.data(), tv.size()));
-  SSG_TRY(dupload(c, &c->conv_bj, cb.data(), cb.size()));
+  std::vector<double> wv(9 * mp);
+  for (int b = 0; b < 3; ++b)
+    for (int a = 0; a < 3; ++a) {
+      const double* t = m.tinv[3 * a + b].data();
+      double* dst = wv.data() + (size_t)(3 * b + a) * mp;
+      for (int e = 0; e < nel; ++e)
+        for (size_t q = 0; q < m.nt; ++q) {
+          const size_t g = e * m.nt + q;
+          dst[g] = 0.5 * ((rho[q] * m.det[g]) * t[g]);
+        }
+    }
+  SSG_TRY(dupload(c, &c->conv_w, wv.data(), wv.size()));
   SSG_TRY(dupload(c, &c->conv_D, m.D.data(), m.D.size()));
   SSG_TRY(dupload(c, &c->conv_J, H.jconv.data(), H.jconv.size()));
   const size_t scr = convection_scratch_doubles(H.n, m.n);
@@ -485,7 +492,7 @@ ssg_status ssg_gll(int n, double* points, double* weights) {
 
 ssg_status ssg_set_setup_options(ssg_context* c, unsigned flags) {
   if (!c) return SSG_ERR_ARG;
-  if (flags & ~(SSG_SETUP_NO_DEALIAS | SSG_SETUP_NO_PARTICLES))
+  if (flags & ~(SSG_SETUP_NO_DEALIAS | SSG_SETUP_NO_PARTICLES | SSG_SETUP_OPPOSITE_PAIRING))
     return fail(c, SSG_ERR_ARG, "unknown set-up option");
   c->setup_opts = flags;
   return SSG_OK;
@@ -859,15 +866,35 @@ ssg_status ssg_setup_particle_geometry(ssg_context* c, const double* points,
 ssg_status ssg_convection_operator(ssg_context* c, const double* u, const double* v,
                                    double* udv) {
   SSG_TRY(need_ready(c));
-  if (!c->conv_tinv) return fail(c, SSG_ERR_STATE, "no dealiasing grid set up");
+  if (!c->conv_w) return fail(c, SSG_ERR_STATE, "no dealiasing grid set up");
   const size_t np = 3 * c->lev[0].npts;
   const double *du, *dv;
   double* dout;
   SSG_TRY(stage_in(c, 0, u, np, &du));
   SSG_TRY(stage_in(c, 1, v, np, &dv));
   SSG_TRY(stage_out(c, 2, udv, np, &dout));
-  SSG_CUDA(c, run_convection(c->stream, c->nel, c->n, c->m, du, dv, dout, c->conv_tinv,
-                             c->conv_bj, c->conv_D, c->conv_J, c->conv_scratch));
+  SSG_CUDA(c, run_convection(c->stream, c->nel, 0, c->nel, c->n, c->m, du, dv, dout,
+                             c->conv_w, c->host.conv.D.data(), c->host.jconv.data(),
+                             c->conv_D, c->conv_J, c->conv_scratch));
+  return stage_back(c, udv, dout, np);
+}
+
+ssg_status ssg_convection_elements(ssg_context* c, int first, int count, const double* u,
+                                   const double* v, double* udv) {
+  SSG_TRY(need_ready(c));
+  if (!c->conv_w) return fail(c, SSG_ERR_STATE, "no dealiasing grid set up");
+  if (first < 0 || count < 0 || first > c->nel || count > c->nel - first)
+    return fail(c, SSG_ERR_ARG, "element range outside the mesh");
+  if (count == 0) return SSG_OK;
+  const size_t np = 3 * (size_t)count * c->lev[0].nt;
+  const double *du, *dv;
+  double* dout;
+  SSG_TRY(stage_in(c, 0, u, np, &du));
+  SSG_TRY(stage_in(c, 1, v, np, &dv));
+  SSG_TRY(stage_out(c, 2, udv, np, &dout));
+  SSG_CUDA(c, run_convection(c->stream, count, first, c->nel, c->n, c->m, du, dv, dout,
+                             c->conv_w, c->host.conv.D.data(), c->host.jconv.data(),
+                             c->conv_D, c->conv_J, c->conv_scratch));
   return stage_back(c, udv, dout, np);
 }
 

@@ -84,7 +84,7 @@ void svv_deriv_matrix(int n, const double* x, const double* w, int msvv, double 
 void interp_matrix(int nto, const double* xto, int nfrom, const double* xfrom, double* J);
 ssg_status build_mesh(HostMesh& m, int n, int nel, const double* vertices,
                       const int* neigh, std::string& err, unsigned opts = 0);
-ssg_status build_pairs(HostMesh& m, std::string& err);
+ssg_status build_pairs(HostMesh& m, std::string& err, bool opposite = false);
 void stiffness_diagonal(const HostLevel& L, int nel, double* out);
 void host_dss(const HostMesh& m, int n, double* u);
 // DSS map of one level (one int array):
@@ -154,8 +154,7 @@ struct ssg_context {
   double* inv_mass = nullptr;   // level 0
   // dealiasing grid
   int m = 0;
-  double* conv_tinv = nullptr;  // 9 x nel x m^3
-  double* conv_bj = nullptr;    // rho * J at m
+  double* conv_w = nullptr;     // 9 x nel x m^3: W[3b + a] = rho J tinv[a][b] / 2
   double* conv_D = nullptr;     // m*m
   double* conv_J = nullptr;     // m*n, jconv[i*n+p]
   double* conv_scratch = nullptr;  // interpolated fields when m^3 exceeds shared memory

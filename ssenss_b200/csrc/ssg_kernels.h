@@ -184,15 +184,21 @@ cudaError_t run_coarse_cg(cudaStream_t s, int device, int nel, const double* f, 
                           const double* gf, const double* D, const double* dinv,
                           const uint8_t* mult, const int* pairs, double nunique, double eps, double rel,
                           int max_iter, double* part, size_t part_cap, double* frame);
-// dealiased skew-symmetric convection of 3-component fields (convection.cu);
-// for m^3 fields beyond shared memory, scratch holds
-// convection_scratch_doubles(n, m) doubles (0: none needed)
+// dealiased skew-symmetric convection of 3-component fields (convection.cu)
+// of the nel elements e0 .. e0+nel-1 of a mesh of nel_fac elements (fields
+// hold the nel elements, the factors tinv and bj all nel_fac); for m^3
+// fields beyond shared memory, scratch holds convection_scratch_doubles(n, m)
+// doubles (0: none needed)
 constexpr int kConvScratchBlocks = 296;
 size_t convection_scratch_doubles(int n, int m);
-cudaError_t run_convection(cudaStream_t s, int nel, int n, int m, const double* u,
-                           const double* v, double* udv, const double* tinv,
-                           const double* bj, const double* Dm, const double* J,
-                           double* scratch);
+// W: 9 x nel_fac x m^3 in the order (b, a), W[3b + a] = rho J tinv[a][b] / 2;
+// Dh, Jh: host copies of the m-point derivative matrix D[i*m + l] and the
+// interpolation matrix J[i*n + p] (carried in the kernel's parameters);
+// Dd, Jd: the same on the device (runtime-order kernel)
+cudaError_t run_convection(cudaStream_t s, int nel, int e0, int nel_fac, int n, int m,
+                           const double* u, const double* v, double* udv, const double* W,
+                           const double* Dh, const double* Jh, const double* Dd,
+                           const double* Jd, double* scratch);
 // Lagrangian particle advance to time t (particles.cu); passes: device int
 // that receives the largest per-particle pass count (atomicMax, caller zeroes)
 cudaError_t run_particles(cudaStream_t s, int n, int nel, size_t npts, const double* x,

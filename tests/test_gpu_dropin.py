@@ -1,0 +1,218 @@
+"""The library as a drop-in under the reference's own host code.
+
+The reference compiled in place (oracle/_ref/libssenss_ref.so) runs against
+the same reference sources linked with the C binding
+ssenss_b200/shim/ssenss_gpu_shim.c (oracle/_ref/libssenss_ref_gpu.so), in
+which solve_poisson_cg, solve_helmholtz_cg, conjugate_gradient,
+flexible_conjugate_gradient, global_opeval, direct_stiffness_summation,
+global_dot_product, global_inverse_mass_matrix_operator,
+jacobi_preconditioner, multigrid_preconditioner, convection_operator and
+integrate_particle_equations run on the GPU.  Nothing else differs: set-up,
+the time integrator (src/navier_stokes.c, src/time.c) and the particle
+bookkeeping are the reference's own code in both.
+
+Each arm runs in a child process (the binding reports failures through the
+reference's fatal_error, which exits).
+
+C1 of the benchmark set: the Taylor-Green vortex on the periodic [0, 2pi]^3
+box of 4^3 elements at N = 7 (n = 8, 32,768 points), Re 1600, dt 1e-3, 20
+steps of integrate_navier_stokes (src/navier_stokes.c:224-235): per step 25
+per-element convection calls, one pressure Poisson solve (FCG + p-multigrid)
+and three Helmholtz solves (Jacobi CG), all to the reference's absolute
+1e-10.
+
+Bars (each stated where it is asserted):
+  * every solve of every step: the same number of iterations, or one apart
+    only where the residual at the deciding iteration lies within a factor 2
+    of eps (conftest.same_stop); residual histories within HIST_REL of the
+    first residual of the solve;
+  * fields u, v, w, p after 20 steps: FIELD_REL relative to the largest
+    entry while every solve stopped at the same iteration;
+  * the individual bound functions on the reference's own set-up: DSS
+    bitwise, operators, inner product and convection 1e-13, the particle
+    walk bitwise (on inputs where the reference reseeds no particle: a
+    reseed draws a random position).
+"""
+import multiprocessing as mp
+import os
+import sys
+
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import EPS
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not (os.path.exists(O.REF_SO) and os.path.exists(O.REF_GPU_SO)),
+                                 reason="reference libraries not built")]
+
+STEPS = 20
+DT, VISC = 1e-3, 1.0 / 1600.0
+HIST_REL = 1e-9
+FIELD_REL = 1e-11
+
+
+def _c1_run(gpu, steps, path):
+    os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
+    import numpy as np
+
+    import oracle as O
+    from ssenss_b200.mesh import tgv_box
+
+    cls = O.ReferenceGPU if gpu else O.Reference
+    ref = cls(tgv_box(4), 8, dt=DT, visc=VISC, dens=1.0)
+    ref.init_tgv()
+    out = {}
+    for s in range(steps):
+        ref.ns_step()
+        for i, (kind, var, hist) in enumerate(ref.step_log()):
+            out[f"s{s}_{i}_kv"] = np.array([kind, var])
+            out[f"s{s}_{i}_h"] = hist
+    for w in range(4):
+        out[f"f{w}"] = ref.get_field(w)
+    out["t"] = np.array(ref.time())
+    ref.close()
+    np.savez(path, **out)
+
+
+def _ops_run(gpu, path):
+    """The individual bound functions on TGV 3^3 at n = 8 through the
+    reference harness: the GPU arm reaches each through the binding."""
+    os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
+    import numpy as np
+
+    import oracle as O
+    from ssenss_b200.mesh import tgv_box
+
+    cls = O.ReferenceGPU if gpu else O.Reference
+    mesh, n = tgv_box(3), 8
+    ref = cls(mesh, n, dt=DT, visc=VISC, dens=1.0)
+    rng = np.random.default_rng(5)
+    shp = (mesh.nel, n, n, n)
+    u, v = rng.standard_normal(shp), rng.standard_normal(shp)
+    out = {"dss": ref.dss(u), "op_p": ref.global_opeval(O.PRESSURE, u),
+           "op_h": ref.global_opeval(O.X_VELOCITY, u)}
+    u3, v3 = rng.standard_normal((3,) + shp), rng.standard_normal((3,) + shp)
+    out["conv"] = ref.convection(u3, v3)
+    f = ref.dss(rng.standard_normal(shp))
+    out["sol_p"], out["hist_p"] = ref.solve_poisson(f, np.zeros(shp))
+    out["sol_h"], out["hist_h"] = ref.solve_helmholtz(O.X_VELOCITY, f, np.zeros(shp))
+    out["mg"] = ref.mg_precon(f)
+    # particles: the reference's own pass loop and bookkeeping around the
+    # walk, on the golden fixtures' particle inputs (tests/golden)
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    import golden_inputs as G
+
+    points = ref.basis(0)[0]
+    ur = G.particle_velocity(mesh, points, G.PART_T, G.PART_DT)
+    state, ints = G.particle_states(mesh, 2000, 7)
+    ref.set_params(G.PART_T, G.PART_DT, VISC)
+    out["p_state"], out["p_ints"] = ref.particles_advance(state, ints, ur)
+    out["p_start"] = ints
+    ref.close()
+    np.savez(path, **out)
+
+
+def _in_child(fn, *args):
+    ctx = mp.get_context("spawn")
+    p = ctx.Process(target=fn, args=args)
+    p.start()
+    p.join(900)
+    if p.is_alive():
+        p.kill()
+        p.join()
+    # the reference's fatal_error exits with status 0: the missing result
+    # file is what shows such a failure
+    assert p.exitcode == 0 and os.path.exists(args[-1]), \
+        f"{fn.__name__}{args[:-1]} ended with exit code {p.exitcode} and no result"
+
+
+@pytest.fixture(scope="module")
+def c1(tmp_path_factory):
+    d = tmp_path_factory.mktemp("c1")
+    res = []
+    for gpu in (False, True):
+        path = str(d / f"c1_{int(gpu)}.npz")
+        _in_child(_c1_run, gpu, STEPS, path)
+        res.append(dict(np.load(path)))
+    return res
+
+
+def _solves(r, s):
+    out = []
+    i = 0
+    while f"s{s}_{i}_kv" in r:
+        out.append((tuple(r[f"s{s}_{i}_kv"]), r[f"s{s}_{i}_h"]))
+        i += 1
+    return out
+
+
+def test_c1_navier_stokes_steps_through_the_binding(c1):
+    cpu, gpu = c1
+    assert float(gpu["t"]) == pytest.approx(STEPS * DT)
+    all_same_stop = True
+    worst_hist = 0.0
+    for s in range(STEPS):
+        sc, sg = _solves(cpu, s), _solves(gpu, s)
+        assert [k for k, _ in sc] == [k for k, _ in sg] == [(0, 0), (1, 1), (1, 2), (1, 3)]
+        for (kv, hc), (_, hg) in zip(sc, sg):
+            if len(hc) != len(hg):
+                all_same_stop = False
+                assert abs(len(hc) - len(hg)) == 1, (s, kv, len(hc), len(hg))
+                k = min(len(hc), len(hg)) - 1
+                for h in (hc[k], hg[k]):
+                    assert 0.5 * EPS <= h <= 2 * EPS, (s, kv, hc, hg)
+            k = min(len(hc), len(hg))
+            dev = float(np.max(np.abs(hc[:k] - hg[:k])) / hc[0]) if k else 0.0
+            worst_hist = max(worst_hist, dev)
+            assert dev <= HIST_REL, (s, kv, dev)
+    devs = []
+    for w in range(4):
+        a, b = cpu[f"f{w}"], gpu[f"f{w}"]
+        scale = max(float(np.max(np.abs(a))), 1e-300)
+        devs.append(float(np.max(np.abs(a - b))) / scale)
+    print(f"C1 drop-in: history deviation {worst_hist:.2e} of h0, fields u v w p "
+          f"{', '.join(f'{d:.2e}' for d in devs)}, every stop equal: {all_same_stop}")
+    if all_same_stop:
+        assert max(devs) <= FIELD_REL, devs
+
+
+@pytest.fixture(scope="module")
+def ops(tmp_path_factory):
+    d = tmp_path_factory.mktemp("ops")
+    res = []
+    for gpu in (False, True):
+        path = str(d / f"ops_{int(gpu)}.npz")
+        _in_child(_ops_run, gpu, path)
+        res.append(dict(np.load(path)))
+    return res
+
+
+def _rel(a, b):
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def test_bound_functions_match_the_reference(ops):
+    cpu, gpu = ops
+    assert np.array_equal(gpu["dss"], cpu["dss"])
+    assert _rel(gpu["op_p"], cpu["op_p"]) < 1e-13
+    assert _rel(gpu["op_h"], cpu["op_h"]) < 1e-13
+    assert _rel(gpu["conv"], cpu["conv"]) < 1e-13
+    assert len(gpu["hist_h"]) == len(cpu["hist_h"])
+    assert _rel(gpu["sol_h"], cpu["sol_h"]) < 1e-12
+    if len(gpu["hist_p"]) == len(cpu["hist_p"]):
+        assert _rel(gpu["sol_p"], cpu["sol_p"]) < 1e-11
+    k = min(len(gpu["hist_p"]), len(cpu["hist_p"]))
+    assert np.all(np.abs(gpu["hist_p"][:k] - cpu["hist_p"][:k]) <= HIST_REL * cpu["hist_p"][0])
+    assert _rel(gpu["mg"], cpu["mg"]) < 1e-9
+
+
+def test_particles_through_the_binding_bitwise(ops):
+    """The reference's integrate_particle_equations replaced by the binding:
+    the GPU walk reads the reference's own GLL points and factors, so
+    element ids and states agree bit for bit."""
+    cpu, gpu = ops
+    assert np.sum(cpu["p_ints"][:, 0] != cpu["p_start"][:, 0]) > 500   # walks cross faces
+    assert np.array_equal(gpu["p_ints"], cpu["p_ints"])
+    assert np.array_equal(gpu["p_state"].view(np.uint64), cpu["p_state"].view(np.uint64))
