@@ -208,7 +208,8 @@ ssg_status run_request(ssg_server* S, Request* r, Resident* slot) {
   if (!c) {
     SSG_TRY(ssg_create(S->device, &c));
     slot->ctx = c;
-    ssg_set_setup_options(c, SSG_SETUP_NO_DEALIAS | SSG_SETUP_NO_PARTICLES);
+    ssg_set_setup_options(c, SSG_SETUP_NO_DEALIAS | SSG_SETUP_NO_PARTICLES |
+                                 SSG_SETUP_OPPOSITE_PAIRING);
     ssg_status st = ssg_setup_mesh(c, r->d.n, r->d.nel, r->vert.data(), r->neigh.data());
     if (st != SSG_OK) {
       // a context whose set-up failed never serves: the worker then drops

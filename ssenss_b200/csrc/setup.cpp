@@ -266,8 +266,15 @@ static void grid_from_vertices(HostLevel& L, int nel, const double* vert) {
 
 // Pairing of faces, edges and corners: the neighbour's matching entry is the
 // FIRST of its list naming this element (src/init.c:68-130 with
-// surfind/edgeind/cornerind, src/init.c:298-320).
-ssg_status build_pairs(HostMesh& m, std::string& err) {
+// surfind/edgeind/cornerind, src/init.c:298-320).  With one or two elements
+// along a periodic direction that search pairs a face with the neighbour's
+// face on the same side (west with west), a defect of the reference the
+// drop-in path keeps.  opposite = true pairs every face, edge and corner
+// with the geometrically opposite one of the neighbour instead (west with
+// east; edge and corner sides all flipped), which is the correct pairing of
+// an aligned mesh and the same as the first match wherever every
+// direction has three or more elements.
+ssg_status build_pairs(HostMesh& m, std::string& err, bool opposite) {
   static const int base[3] = {0, 6, 18}, cnt[3] = {6, 12, 8};
   m.pairs.assign((size_t)m.nel * 52, -1);
   m.bc.assign(m.nel, 0);
@@ -284,11 +291,18 @@ ssg_status build_pairs(HostMesh& m, std::string& err) {
           return SSG_ERR_MESH;
         }
         int found = -1;
-        for (int s = 0; s < cnt[kind]; ++s)
-          if (m.neigh[26 * (size_t)nb + base[kind] + s] == e) {
-            found = s;
-            break;
-          }
+        if (opposite) {
+          // faces w,e | s,n | b,t: flip the side; edges: both sides of the
+          // group (sw,se,nw,ne | bw,be,tw,te | bs,bn,ts,tn); corners: all three
+          const int opp = kind == 0 ? (j ^ 1) : (kind == 1 ? (j ^ 3) : (j ^ 7));
+          if (m.neigh[26 * (size_t)nb + base[kind] + opp] == e) found = opp;
+        } else {
+          for (int s = 0; s < cnt[kind]; ++s)
+            if (m.neigh[26 * (size_t)nb + base[kind] + s] == e) {
+              found = s;
+              break;
+            }
+        }
         if (found < 0) {
           err = "element " + std::to_string(e) + " slot " + std::to_string(slot) +
                 ": neighbour " + std::to_string(nb) + " does not name it back";
@@ -481,7 +495,7 @@ ssg_status build_mesh(HostMesh& m, int n, int nel, const double* vert, const int
   m.n = n;
   m.nel = nel;
   m.neigh.assign(neigh, neigh + 26 * (size_t)nel);
-  ssg_status st = build_pairs(m, err);
+  ssg_status st = build_pairs(m, err, (opts & SSG_SETUP_OPPOSITE_PAIRING) != 0);
   if (st != SSG_OK) return st;
   int orders[SSG_MAXLEV];
   m.nlev = level_orders(n, orders);

@@ -1,0 +1,197 @@
+"""Parity at the benchmark configurations' own sizes, against the reference
+compiled in place (oracle/_ref), run live on the same machine.
+
+C2  the bench's headline solve: TGV periodic 16^3 elements, N = 7 (n = 8,
+    2,097,152 points), pressure Poisson right-hand side of the TGV pressure,
+    FCG + p-multigrid to the absolute 1e-10, from zero -- FP64, through the
+    library's own set-up (the bench's path).  The reference's residual
+    history on this machine is also pinned by tests/golden/c2_tgv16_n8.json.
+C3  the deformed channel at N = 9 (n = 10) on a reduced 8 x 4 x 4 mesh with
+    the configuration's stretch (tanh 2.0), perturbation (0.1 of the local
+    spacing) and seed; 8 seeded Fourier modes, Neumann-compatible, mean zero.
+C4  20,000 particles in the 16^3 N = 7 TGV flow, 100 calls of
+    integrate_particle_equations over 2 dt each (the reference's cadence) on
+    frozen velocity snapshots, every particle's element id and state compared
+    bit for bit after every 10th call and at the end.
+
+Bars: iteration counts equal, or one apart only where the stop lies within a
+factor 2 of eps at the deciding iteration (conftest.same_stop); residual
+histories within 1e-9 of the first residual wherever both are above 1e-4 of
+it (the 15-iteration inner CG solves of the V-cycle stop on the same
+absolute eps, so near the end of a solve two FP64 implementations take
+different inner iteration counts and their outer residuals drift apart at
+that level -- measured, not assumed: the oracle against the reference shows
+the same), within 1e-7 of it below; solutions 1e-11 relative to the largest
+entry (conftest.assert_solution_close); mixed precision 1e-8 against the
+FP64 reference solution.
+"""
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+import ssenss_b200 as S
+from conftest import EPS, assert_solution_close, same_stop
+from ssenss_b200.mesh import channel_mesh, tgv_box
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not O.reference_available(), reason="reference library not built")]
+
+
+def rel(a, b):
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def check_history(h_g, h_r):
+    k = min(len(h_g), len(h_r))
+    h0 = h_r[0]
+    hi = h_r[:k] > 1e-4 * h0
+    d = np.abs(np.asarray(h_g[:k]) - np.asarray(h_r[:k]))
+    assert np.all(d[hi] <= 1e-9 * h0), (d / h0)
+    assert np.all(d <= 1e-7 * h0), (d / h0)
+    return float(np.max(d) / h0)
+
+
+def tgv_pressure_rhs(ref, n):
+    """Weak, assembled -lap p of the TGV pressure on the reference's own grid
+    (what compute_pressure_rhs assembles for this p)."""
+    x, w, _, _ = ref.basis(0)
+    X, Y, Z = (ref.geometry(0, 7 + a) for a in range(3))
+    rho = w[None, None, None, :] * w[None, None, :, None] * w[None, :, None, None]
+    c2x, c2y, c2z = np.cos(2 * X), np.cos(2 * Y), np.cos(2 * Z)
+    lap = (-4.0 * (c2x + c2y) * (c2z + 2.0) - 4.0 * (c2x + c2y) * c2z) / 16.0
+    return ref.dss(rho * ref.geometry(0, 6) * (-lap))
+
+
+def test_c2_pressure_solve_full_size():
+    mesh, n = tgv_box(16), 8
+    ref = O.Reference(mesh, n)
+    try:
+        f = tgv_pressure_rhs(ref, n)
+        u_r, h_r = ref.solve_poisson(f, np.zeros_like(f))
+    finally:
+        ref.close()
+    pin = json.load(open(os.path.join(HERE, "golden", "c2_tgv16_n8.json")))
+    assert len(h_r) == pin["iterations"]
+    assert np.all(np.abs(h_r - np.array(pin["history"])) <= 1e-9 * pin["history"][0])
+    ctx = S.Context(0)
+    try:
+        ctx.set_parameters(1e-3, 1.0 / 1600.0, 1.0)
+        ctx.set_setup_options(no_dealias=True, no_particles=True)
+        ctx.setup_mesh(mesh, n)
+        u_g, info = ctx.solve_poisson_cg(f, np.zeros_like(f))
+    finally:
+        ctx.close()
+    assert info["status"] == "SSG_OK"
+    dh = check_history(info["history"], h_r)
+    d = None
+    if same_stop(info["iterations"], info["history"], h_r):
+        d = rel(u_g, u_r)
+        assert d < 1e-11, d
+    print(f"C2 full size: {info['iterations']} vs {len(h_r)} iterations, history "
+          f"{dh:.2e} of h0, solution {d}")
+
+
+def channel_rhs(ref, n, seed=20241203):
+    """The C3 right-hand side: 8 seeded Fourier modes, cos in x and z,
+    Neumann-compatible cos(pi k (y + 1) / 2) in y, made mean-zero, weak and
+    assembled (the same formula as the bench's C3 section)."""
+    X, Y, Z = (ref.geometry(0, 7 + a) for a in range(3))
+    x, w, _, _ = ref.basis(0)
+    rho = w[None, None, None, :] * w[None, None, :, None] * w[None, :, None, None]
+    bj = rho * ref.geometry(0, 6)
+    rng = np.random.default_rng(seed)
+    g = np.zeros_like(X)
+    for _ in range(8):
+        kx, kz = rng.integers(1, 4) / 2.0, rng.integers(-3, 4)
+        ky = rng.integers(0, 3)
+        g += rng.standard_normal() * np.cos(kx * X + kz * Z + rng.uniform(0, 6.28)) * \
+            np.cos(math.pi * ky * (Y + 1) / 2)
+    g -= (bj * g).sum() / bj.sum()
+    return ref.dss(bj * g)
+
+
+def test_c3_channel_n10_reduced():
+    mesh, n = channel_mesh((8, 4, 4)), 10
+    ref = O.Reference(mesh, n)
+    try:
+        f = channel_rhs(ref, n)
+        u_r, h_r = ref.solve_poisson(f, np.zeros_like(f))
+    finally:
+        ref.close()
+    out = {}
+    for prec in ("fp64", "mixed"):
+        ctx = S.Context(0)
+        try:
+            ctx.set_parameters(1e-3, 1.0 / 1600.0, 1.0)
+            ctx.set_setup_options(no_dealias=True, no_particles=True)
+            ctx.setup_mesh(mesh, n)
+            ctx.set_precision(prec)
+            out[prec] = ctx.solve_poisson_cg(f, np.zeros_like(f))
+        finally:
+            ctx.close()
+    u_g, info = out["fp64"]
+    assert info["status"] == "SSG_OK"
+    dh = check_history(info["history"], h_r)
+    d = None
+    if same_stop(info["iterations"], info["history"], h_r):
+        orc = O.Oracle(mesh, n)
+        try:
+            d = assert_solution_close(u_g, u_r, orc, orc.solve_poisson, f)
+        finally:
+            orc.close()
+    u_m, info_m = out["mixed"]
+    assert info_m["status"] == "SSG_OK" and info_m["residual"] <= EPS
+    dm = rel(u_m - u_m.mean(), u_r - u_r.mean())
+    assert dm < 1e-8, dm
+    print(f"C3 reduced (n = 10): FP64 {info['iterations']} vs {len(h_r)} iterations, "
+          f"history {dh:.2e} of h0, solution {d}; mixed {info_m['iterations']} iterations, "
+          f"{dm:.2e} from the reference")
+
+
+def test_c4_particle_trajectories_100_calls_bitwise():
+    mesh, n = tgv_box(16), 8
+    npart, calls, dt = 20000, 100, 1e-3
+    ref = O.Reference(mesh, n)
+    ctx = S.Context(0)
+    try:
+        ctx.set_parameters(dt, 1.0 / 1600.0, 1.0)
+        ctx.set_setup_options(no_dealias=True)
+        ctx.setup_mesh(mesh, n)
+        pts, jac, tinv = ref.particle_geometry()
+        ctx.setup_particle_geometry(pts, jac, tinv)
+        X, Y, Z = (ref.geometry(0, 7 + a) for a in range(3))
+        h = 2 * math.pi / 16
+        snaps = np.stack([np.stack([np.sin(X) * np.cos(Y) * np.cos(Z),
+                                    -np.cos(X) * np.sin(Y) * np.cos(Z), 0 * X]) * (2.0 / h)
+                          for _ in range(3)])
+        ctx.set_particle_velocity(snaps)
+        rng = np.random.default_rng(7)
+        state = np.zeros((npart, 8))
+        ints = np.zeros((npart, 3), np.int32)
+        state[:, :3] = rng.uniform(-1, 1, (npart, 3))
+        state[:, 7] = np.linspace(0.1, 1.0, 10)[np.arange(npart) % 10]
+        ints[:, 0] = rng.integers(0, mesh.nel, npart)
+        ints[:, 1] = ints[:, 0]
+        s_g, i_g = state.copy(), ints.copy()
+        s_r, i_r = state.copy(), ints.copy()
+        t = 0.0
+        for call in range(calls):
+            t += 2 * dt
+            s_g, i_g, _ = ctx.integrate_particle_equations(s_g, i_g, t, dt)
+            ref.set_params(t, dt, 1.0 / 1600.0)
+            s_r, i_r = ref.particles_advance(s_r, i_r, snaps)
+            assert not np.any(i_g[:, 2] == 5), call          # no reseed drawn
+            if call % 10 == 9 or call == calls - 1:
+                assert np.array_equal(i_g[:, :2], i_r[:, :2]), call
+                assert np.array_equal(s_g.view(np.uint64), s_r.view(np.uint64)), call
+    finally:
+        ctx.close()
+        ref.close()
+    moved = int(np.sum(i_g[:, 0] != ints[:, 0]))
+    assert moved > npart // 20
+    print(f"C4: {npart} particles, {calls} calls, {moved} changed element, bitwise")
