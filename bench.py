@@ -71,9 +71,9 @@ def parse():
     ap.add_argument("--serve-slots", type=int, default=8,
                     help="requests in flight at once in the serving loop")
     ap.add_argument("--sections", default="all",
-                    choices=["all", "fp64", "mixed", "op", "serve", "extra"],
-                    help="fp64: only the FP64 solves; op: only the operator "
-                         "launches (for profiler captures)")
+                    choices=["all", "fp64", "mixed", "op", "conv", "serve", "extra"],
+                    help="fp64: only the FP64 solves; op / conv: only the operator / "
+                         "convection launches (for profiler captures)")
     return ap.parse_args()
 
 
@@ -307,7 +307,7 @@ def run_reference(args):
 # ---------------------------------------------------------------------------
 # serving stream (periodic boxes of E elements, orders N in {5,7,9,11})
 # ---------------------------------------------------------------------------
-def near_cube_shapes(lo=3, hi=16):
+def near_cube_shapes(lo=2, hi=16):
     """Element counts a*b*c with lo <= a <= b <= c <= a + 1 (near-cubes)."""
     out = {}
     for a in range(lo, hi + 1):
@@ -320,10 +320,13 @@ def near_cube_shapes(lo=3, hi=16):
 
 def serve_stream(nreq, rate, seed=2024):
     """Requests (arrival s, shape, n, lambda, rhs seed): E log-uniform in
-    [8, 4096] rounded to the nearest near-cube product with all factors >= 3
-    (smaller counts carry the reference's periodic pairing defect), n
-    uniform in {6, 8, 10, 12}, Poisson (lambda = 0) or Helmholtz with lambda
-    uniform in (0, 100] with probability 1/2 each, Poisson arrivals."""
+    [8, 4096], rounded (in log E) to the nearest product a b c of three
+    integers with a <= b <= c <= a + 1 -- 8, 12, 18, 27, 36, ... -- so that
+    the boxes keep their elements near cubic; counts below 27 have two
+    elements along a periodic direction and are solved with the opposite
+    face pairing (the reference's first match pairs them wrongly), n uniform
+    in {6, 8, 10, 12}, Poisson (lambda = 0) or Helmholtz with lambda uniform
+    in (0, 100] with probability 1/2 each, Poisson arrivals."""
     import numpy as np
     rng = np.random.default_rng(seed)
     shapes = near_cube_shapes()
@@ -404,8 +407,9 @@ def run_serving(args, device):
 
     return {
         "workload": (f"{len(stream)} requests ({npois} Poisson FCG+p-MG, "
-                     f"{len(stream) - npois} Helmholtz CG-Jacobi), periodic boxes E in "
-                     f"[27, 4096] near-cube, n in {{6,8,10,12}}, Poisson arrivals "
+                     f"{len(stream) - npois} Helmholtz CG-Jacobi), periodic boxes E "
+                     f"log-uniform in [8, 4096] rounded to near-cubes a*b*c from 2*2*2 "
+                     f"(E < 27 included), n in {{6,8,10,12}}, Poisson arrivals "
                      f"{args.serve_rate}/s, stop sqrt((r.r)_w) <= {EPS}, HBM budget 150 GB"),
         "served_mixed": pick(st_s, wall_s),
         "plain_fp64_one_at_a_time": pick(st_p, wall_p),
@@ -472,6 +476,17 @@ def run_channel(args, device):
            "local_points": mesh.nel * n ** 3, "unique_dofs": udofs,
            "host_setup_s": setup_s,
            "launch_shapes": {str(k): v for k, v in tuned.items()}}
+    # the level-0 operator at n = 10 (the solve's dominant kernel at this
+    # order): 64 B per local point (u, six metric terms, out), timed alone
+    # on the library's stream (ssg_time_operator, 50 launches, best of 3)
+    peak, peak_kind = peaks()
+    op_us = ctx.time_operator(S.PRESSURE, 50)
+    op_alg = 64 * mesh.nel * n ** 3
+    out["operator_n10"] = {"us_per_launch": op_us, "bytes_per_launch": op_alg,
+                           "achieved_gbs": op_alg / (op_us * 1e-6) / 1e9,
+                           "frac": op_alg / (op_us * 1e-6) / 1e9 / peak,
+                           "peak_gbs": peak, "peak_source": peak_kind,
+                           "operator_shape": S.tuning(n)["ax_elements_per_block"]}
     sols = {}
     for prec in ("fp64", "mixed"):
         ctx.set_precision(prec)
@@ -644,6 +659,17 @@ def run_ours(args):
                "channel": run_channel(args, local)}
         if rank == 0:
             print(json.dumps({"metric": METRIC, "sections": "extra", **res}))
+        ctx.close()
+        return 0
+
+    if args.sections == "conv":
+        X3 = np.stack([np.sin(X) * np.cos(Y) * np.cos(Z), -np.cos(X) * np.sin(Y) * np.cos(Z),
+                       0 * X])
+        uc = torch.from_numpy(X3).to(dev)
+        oc = torch.empty_like(uc)
+        for _ in range(args.warmup + args.steps):
+            ctx.convection_operator(uc, uc, oc)
+        torch.cuda.synchronize()
         ctx.close()
         return 0
 

@@ -287,7 +287,9 @@ ssg_status ssg_time_operator(ssg_context *ctx, int var, int reps,
  * us[2] the CG update (x, r, z and four partial sums). */
 ssg_status ssg_time_smoother(ssg_context *ctx, int level, int reps, double *us);
 /* Launch shapes in use for order n (tuned or default); elements per block
- * 0 = the FP64 tensor-core operator (n = 8: one warp per element). */
+ * 0 = the FP64 tensor-core operator (n = 8: one warp per element), -1 = the
+ * line-form operator (each thread contracts whole element lines), 1, 2, 4,
+ * ... = the plane-form operator with that many elements per block. */
 ssg_status ssg_tuning(int n, int *ax_elements_per_block,
 		int *dss_blocks_per_sm, int *vector_blocks_per_sm);
 

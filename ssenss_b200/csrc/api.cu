@@ -206,8 +206,11 @@ static ssg_status upload_all(ssg_context* c) {
     double nun = 0.0;
     for (double v : sc) nun += v;
     d.nunique = nun;
+    // FP32 copy for the mixed-precision V-cycle, natural point order (its
+    // operator is the line-form kernel at every order)
+    SSG_TRY(upload_f32(c, &d.gf32, gf.data(), gf.size()));
     if (h.n == 8) {
-      // the tensor-core operator's fragment order (see ax8.cu)
+      // the FP64 tensor-core operator's fragment order (see ax8.cu)
       std::vector<double> nat(gf);
       parallel_elements(nel, [&](int e0, int e1) {
         for (int a = 0; a < 6; ++a)
@@ -252,7 +255,6 @@ static ssg_status upload_all(ssg_context* c) {
     }
     SSG_TRY(dupload(c, &d.D, h.D.data(), h.D.size()));
     SSG_TRY(dupload(c, &d.S, h.S.data(), h.S.size()));
-    SSG_TRY(upload_f32(c, &d.gf32, gf.data(), gf.size()));
     SSG_TRY(upload_f32(c, &d.dinv_p32, dp.data(), np));
     if (l >= 1) {
       const int nf = H.lev[l - 1].n, nc = h.n;

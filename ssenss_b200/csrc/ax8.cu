@@ -217,8 +217,7 @@ __global__ void __launch_bounds__(128, 4) k_ax8_dmma(int nel, T* __restrict__ u,
 }  // namespace dev
 
 // blocks of 4 warps (one element each), grid capped at 8 blocks per SM and
-// walking the elements; T = float stores the mixed-precision V-cycle's
-// fields (arithmetic stays FP64)
+// walking the elements (FP64 fields: T = double)
 template <typename T>
 static cudaError_t launch_ax8(cudaStream_t s, int nel, bool helm, T* u, T* au, const T* gf,
                               size_t npts, const double* bj, const double* D, const double* S,
@@ -252,11 +251,9 @@ cudaError_t run_ax8_dmma(cudaStream_t s, int nel, bool helm, bool fp32, void* u,
                          const double* S, double lambda, const dev::PUpdate* pu,
                          const ScalarOp* dop) {
   const ScalarOp o = dop ? *dop : ScalarOp();
-  if (fp32) {
-    if (helm) return cudaErrorInvalidValue;
-    return launch_ax8<float>(s, nel, false, (float*)u, (float*)au, (const float*)gf, npts, bj,
-                             D, S, lambda, pu, o);
-  }
+  // FP32 storage (the mixed V-cycle) runs the line-form operator in FP32
+  // arithmetic; this kernel is the FP64 operator of order 8
+  if (fp32) return cudaErrorInvalidValue;
   return launch_ax8<double>(s, nel, helm, (double*)u, (double*)au, (const double*)gf, npts, bj,
                             D, S, lambda, pu, o);
 }

@@ -23,6 +23,8 @@
 #include <cuda/atomic>
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include <cstdint>
 #include <cstdio>
 
@@ -68,6 +70,199 @@ __global__ void __launch_bounds__(256, (N >= 10 ? 1 : 2)) k_ax(int nel, T* __res
   if (FUSEP && pu.part) {
     __shared__ double sflat[256];
     finish_flat(pap, tid, nthr, pu.part, dop, sflat);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// local operator of every order but 8, line form: each thread contracts one
+// whole line of an element (N points along i, j or k) held in registers, so
+// a matrix row is read once per line instead of a shared row and a shared
+// field value per multiply-add.  Per element: the field is staged in shared
+// memory; three passes (lines along i, j, k) give the r-, s- and
+// t-derivatives; a point-wise pass applies the six metric terms; three
+// transposed passes sum D^T w0 + S^T w1 + S^T w2 (D for Poisson) in the
+// order (acc + acs) + act of ax_element.  The matrices sit in shared memory
+// and every lane of a warp reads the same entry (a broadcast), two entries
+// per 16-byte load.  EPB elements per block fill about 256 threads.  Same
+// interface as k_ax (optional direction update and p . (A p)).
+// ---------------------------------------------------------------------------
+template <int N>
+struct AxLine {
+  static constexpr int EPB = (256 / (N * N)) > 0 ? 256 / (N * N) : 1;
+  static constexpr int TASKS = EPB * N * N;
+  static constexpr int THREADS = (TASKS + 31) / 32 * 32;
+  static constexpr int RM = N + (N & 1);                 // matrix rows (pair-aligned)
+  static constexpr int RS = N + ((2 - N % 4) + 4) % 4;   // field rows: 2 mod 4 values
+  static constexpr int FS = N * N * RS;                  // one staged field
+  static constexpr int MATS = 4 * N * RM;
+  static constexpr int SMEM = MATS + EPB * 4 * FS;       // values of the compute type
+};
+
+// sum_l A[o][l] x[l] (A rows of RM values, pair-aligned), in l order; every
+// lane of the warp reads the same A entries
+template <int N, int RM, typename C>
+__device__ __forceinline__ C line_row(const C* A, int o, const C (&x)[N]) {
+  using V2 = typename std::conditional<sizeof(C) == 8, double2, float2>::type;
+  C acc = 0;
+#pragma unroll
+  for (int l = 0; l + 1 < N; l += 2) {
+    const V2 a = *reinterpret_cast<const V2*>(A + o * RM + l);
+    acc += a.x * x[l];
+    acc += a.y * x[l + 1];
+  }
+  if (N & 1) acc += A[o * RM + N - 1] * x[N - 1];
+  return acc;
+}
+
+// dst[o * stride] (=, or += when ADD) sum_l A[o][l] x[l] for o < N; the
+// output loop is not unrolled, so a line's matrix rows are read one row at
+// a time and the registers hold the line only
+template <int N, int RM, bool ADD, typename C>
+__device__ __forceinline__ void line_apply(const C* A, const C (&x)[N], C* dst, int stride) {
+#pragma unroll 2
+  for (int o = 0; o < N; ++o) {
+    const C v = line_row<N, RM, C>(A, o, x);
+    if (ADD)
+      dst[o * stride] += v;
+    else
+      dst[o * stride] = v;
+  }
+}
+
+// The arithmetic runs in the storage type T: FP64 for the solves, FP32 in
+// the mixed-precision V-cycle (the fused direction update and the p . (A p)
+// sum stay FP64).
+template <int N, typename T, bool HELM, bool FUSEP>
+__global__ void __launch_bounds__(AxLine<N>::THREADS)
+    k_axl(int nel, T* __restrict__ u, T* __restrict__ au, const T* __restrict__ gf,
+          size_t npts, const double* __restrict__ bj, const double* __restrict__ Dg,
+          const double* __restrict__ Sg, double lambda, PUpdate pu, ScalarOp dop) {
+  using L = AxLine<N>;
+  using C = T;
+  constexpr int NN = N * N, NT = N * N * N, RM = L::RM, RS = L::RS, FS = L::FS;
+  if (FUSEP && pu.stop && *pu.stop != 0.0) return;   // uniform over the block
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* sD = reinterpret_cast<C*>(smem_raw);
+  C* sDT = sD + N * RM;
+  C* sS = sDT + N * RM;
+  C* sST = sS + N * RM;
+  C* fld = sD + L::MATS;   // per slot: U/O, F1, F2, F3 (FS values each)
+  const int tid = threadIdx.x;
+  for (int q = tid; q < NN; q += blockDim.x) {
+    const int r = q / N, c = q % N;
+    const C d = (C)Dg[q], sv = HELM ? (C)Sg[q] : d;
+    sD[r * RM + c] = d;
+    sDT[c * RM + r] = d;
+    sS[r * RM + c] = sv;
+    sST[c * RM + r] = sv;
+  }
+  const int e0 = blockIdx.x * L::EPB;
+  const int ne = min(L::EPB, nel - e0);
+  const size_t base = (size_t)e0 * NT;
+  const int npb = ne * NT;   // points of this block
+  const T* z = FUSEP ? reinterpret_cast<const T*>(pu.z) : nullptr;
+  const double beta = (FUSEP && !pu.first) ? *pu.beta : 0.0;
+  const double c = (FUSEP && pu.c) ? *pu.c : 0.0;
+  // P0: stage the field (forming p first when fused), coalesced
+  for (int q = tid; q < npb; q += blockDim.x) {
+    const size_t o = base + q;
+    C v;
+    if (FUSEP) {
+      const double zc = (double)z[o] - c;
+      double pv = pu.first ? zc : beta * (double)u[o] + zc;
+      if (pu.mask) pv = pv * pu.mask[o];
+      const T vt = (T)pv;
+      u[o] = vt;
+      v = (C)vt;
+    } else {
+      v = (C)u[o];
+    }
+    const int sl = q / NT, p = q % NT;
+    fld[sl * 4 * FS + (p / NN) * N * RS + ((p / N) % N) * RS + p % N] = v;
+  }
+  __syncthreads();
+  const bool task = tid < ne * NN;
+  const int sl = tid / NN, a0 = (tid % NN) % N, a1 = (tid % NN) / N;
+  C* U = fld + sl * 4 * FS;
+  C* F1 = U + FS;
+  C* F2 = F1 + FS;
+  C* F3 = F2 + FS;
+  // P1-P3: derivatives along i (r, with S for Helmholtz), j (s), k (t)
+  if (task) {
+    C x[N];
+    {   // lines (j = a0, k = a1) along i
+      const C* src = U + a1 * N * RS + a0 * RS;
+#pragma unroll
+      for (int l = 0; l < N; ++l) x[l] = src[l];
+      line_apply<N, RM, false, C>(HELM ? sS : sD, x, F1 + a1 * N * RS + a0 * RS, 1);
+    }
+    {   // lines (i = a0, k = a1) along j
+      const C* src = U + a1 * N * RS + a0;
+#pragma unroll
+      for (int l = 0; l < N; ++l) x[l] = src[l * RS];
+      line_apply<N, RM, false, C>(sD, x, F2 + a1 * N * RS + a0, RS);
+    }
+    {   // lines (i = a0, j = a1) along k
+      const C* src = U + a1 * RS + a0;
+#pragma unroll
+      for (int l = 0; l < N; ++l) x[l] = src[l * N * RS];
+      line_apply<N, RM, false, C>(sD, x, F3 + a1 * RS + a0, N * RS);
+    }
+  }
+  __syncthreads();
+  // P4: w = G (ur, us, ut) at every point, in place
+  for (int q = tid; q < npb; q += blockDim.x) {
+    const size_t o = base + q;
+    const int s2 = q / NT, p = q % NT;
+    const int off = s2 * 4 * FS + (p / NN) * N * RS + ((p / N) % N) * RS + p % N;
+    const C ur = fld[off + FS], us = fld[off + 2 * FS], ut = fld[off + 3 * FS];
+    const C g0 = __ldg(gf + o), g1 = __ldg(gf + npts + o), g2 = __ldg(gf + 2 * npts + o),
+            g3 = __ldg(gf + 3 * npts + o), g4 = __ldg(gf + 4 * npts + o),
+            g5 = __ldg(gf + 5 * npts + o);
+    fld[off + FS] = g0 * ur + g1 * us + g2 * ut;
+    fld[off + 2 * FS] = g1 * ur + g3 * us + g4 * ut;
+    fld[off + 3 * FS] = g2 * ur + g4 * us + g5 * ut;
+  }
+  __syncthreads();
+  // P5-P7: (D^T w0 + S^T w1) + S^T w2, accumulated in U's place
+  if (task) {
+    C x[N];
+    const C* src = F1 + a1 * N * RS + a0 * RS;
+#pragma unroll
+    for (int l = 0; l < N; ++l) x[l] = src[l];
+    line_apply<N, RM, false, C>(sDT, x, U + a1 * N * RS + a0 * RS, 1);
+  }
+  __syncthreads();
+  if (task) {
+    C x[N];
+    const C* src = F2 + a1 * N * RS + a0;
+#pragma unroll
+    for (int l = 0; l < N; ++l) x[l] = src[l * RS];
+    line_apply<N, RM, true, C>(sST, x, U + a1 * N * RS + a0, RS);
+  }
+  __syncthreads();
+  double pap = 0.0;
+  if (task) {
+    C x[N];
+    const C* src = F3 + a1 * RS + a0;
+#pragma unroll
+    for (int l = 0; l < N; ++l) x[l] = src[l * N * RS];
+    const C* acc = U + a1 * RS + a0;
+    const size_t eo = base + (size_t)sl * NT + a1 * N + a0;
+#pragma unroll 2
+    for (int l = 0; l < N; ++l) {
+      const size_t o = eo + (size_t)l * NN;
+      C out = acc[l * N * RS] + line_row<N, RM, C>(sST, l, x);
+      C pv = 0;
+      if (HELM || FUSEP) pv = u[o];
+      if (HELM) out += (C)lambda * ((C)__ldg(bj + o) * pv);
+      au[o] = (T)out;
+      if (FUSEP) pap += (double)pv * (double)out;
+    }
+  }
+  if (FUSEP && pu.part) {
+    __shared__ double sflat[AxLine<N>::THREADS];
+    finish_flat(pap, tid, blockDim.x, pu.part, dop, sflat);
   }
 }
 
@@ -546,8 +741,8 @@ int vec_blocks(size_t npts) {
 }
 
 int ax_epb(int n) {
-  if (n >= 0 && n <= SSG_MAXN && g_tune_ax_epb[n] > 0) return g_tune_ax_epb[n];
-  return ax_epb_max(n);
+  if (n >= 0 && n <= SSG_MAXN && g_tune_ax_epb[n] != 0) return g_tune_ax_epb[n];
+  return kAxLine;
 }
 
 template <int N, typename T, bool HELM, bool FUSEP>
@@ -569,6 +764,26 @@ static cudaError_t launch_ax_t(cudaStream_t s, int nel, int epb, T* u, T* au, co
   return cudaGetLastError();
 }
 
+template <int N, typename T, bool HELM, bool FUSEP>
+static cudaError_t launch_axl_t(cudaStream_t s, int nel, T* u, T* au, const T* gf,
+                                size_t npts, const double* bj, const double* D,
+                                const double* S, double lambda, const PUpdate& pu,
+                                const ScalarOp& dop) {
+  using L = AxLine<N>;
+  constexpr size_t smem = (size_t)L::SMEM * sizeof(T);
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaError_t e = cudaFuncSetAttribute(k_axl<N, T, HELM, FUSEP>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    attr_set = true;
+  }
+  const int grd = (nel + L::EPB - 1) / L::EPB;
+  { SSG_COUNT(); k_axl<N, T, HELM, FUSEP><<<grd, L::THREADS, smem, s>>>(nel, u, au, gf, npts, bj, D, S, lambda, pu, dop); }
+  return cudaGetLastError();
+}
+
 template <typename T, bool HELM, bool FUSEP>
 static cudaError_t ax_dispatch(int n, cudaStream_t s, int nel, int epb, T* u, T* au,
                                const T* gf, size_t npts, const double* bj, const double* D,
@@ -577,6 +792,9 @@ static cudaError_t ax_dispatch(int n, cudaStream_t s, int nel, int epb, T* u, T*
   switch (n) {
 #define SSG_AXN(NV)                                                                   \
   case NV:                                                                            \
+    if (epb == kAxLine)                                                               \
+      return launch_axl_t<NV, T, HELM, FUSEP>(s, nel, u, au, gf, npts, bj, D, S,      \
+                                              lambda, pu, dop);                       \
     return launch_ax_t<NV, T, HELM, FUSEP>(s, nel, epb, u, au, gf, npts, bj, D, S,    \
                                            lambda, pu, dop);
     SSG_AXN(2) SSG_AXN(3) SSG_AXN(4) SSG_AXN(5) SSG_AXN(6) SSG_AXN(7)
@@ -605,14 +823,15 @@ cudaError_t run_ax(cudaStream_t s, int n, int nel, int epb, bool helm, bool fp32
       dop = *pua->dot;
     }
   }
-  // n = 8: the FP64 tensor-core kernel (FP32 or FP64 storage)
-  // (order 8 stores its metric factors in the tensor-core kernel's fragment
-  // order, so that kernel is the only operator of this order)
-  const bool dmma = n == 8;
+  // n = 8 in FP64: the FP64 tensor-core kernel (the level's FP64 metric
+  // factors are stored in its fragment order); in FP32 (the mixed V-cycle,
+  // whose FP32 factors are stored in natural order) the line-form kernel
+  // computing in FP32
+  const bool dmma = n == 8 && !fp32;
   if (dmma)
     return run_ax8_dmma(s, nel, helm, fp32, (void*)in, out, gf, npts, bj, D, S, lambda,
                         fuse ? &pu : nullptr, &dop);
-  if (epb <= 0) epb = ax_epb(n);
+  if (epb == 0) epb = ax_epb(n);
   if (fp32) {
     if (helm) return cudaErrorInvalidValue;
     if (fuse)

@@ -15,6 +15,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdint>
 #include <cstring>
 
 #include "ssg_internal.h"
@@ -47,10 +48,55 @@ struct Workspace {
   bool vcycle_failed = false;
   double warm_eps = -1.0;   // eps / precision of the last direct V-cycle
   int warm_precision = -1;
+  // FCG iterations as graphs: one per window state (the slot rotation of
+  // the direction history is periodic: state 0 for the first iteration,
+  // then 44 states that repeat), each an IF node that runs the iteration
+  // only while the solve has not stopped, so iterations are enqueued ahead
+  // without a host synchronisation
+  static constexpr int kFcgStates = 45;
+  cudaGraphExec_t fcg[kFcgStates] = {};
+  unsigned long long fcg_kernels[kFcgStates] = {};
+  double fcg_eps = -1.0;
+  int fcg_precision = -1, fcg_max_iter = -1, fcg_hcap = -1;
+  bool fcg_failed = false;
+  int fcg_warm = 0;          // solves run directly with this configuration
+  // the Jacobi CG loop (iterations after the first) as one WHILE graph
+  cudaGraphExec_t cgloop = nullptr;
+  unsigned long long cgloop_kernels = 0;
+  struct LoopKey {
+    const void* f = nullptr;
+    const void* x = nullptr;
+    const double* hist = nullptr;
+    double eps = -1.0, lam = 0.0;
+    int max_iter = -1, hist_cap = 0, var = -1, level = -1, frame = -1;
+    bool fp32 = false;
+    bool operator==(const LoopKey& o) const {
+      return f == o.f && x == o.x && hist == o.hist && eps == o.eps && lam == o.lam &&
+             max_iter == o.max_iter && hist_cap == o.hist_cap && var == o.var &&
+             level == o.level && frame == o.frame && fp32 == o.fp32;
+    }
+  } cgloop_key;
+  bool cgloop_failed = false;
 };
+
+static void drop_iteration_graphs(Workspace* w) {
+  for (auto& g : w->fcg)
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
+  w->fcg_failed = false;
+  w->fcg_warm = 0;
+  w->fcg_eps = -1.0;
+  if (w->cgloop) cudaGraphExecDestroy(w->cgloop);
+  w->cgloop = nullptr;
+  w->cgloop_failed = false;
+  w->cgloop_key = Workspace::LoopKey();
+}
 
 void free_workspace(Workspace* w) {
   if (!w) return;
+  drop_iteration_graphs(w);
   if (w->vcycle) cudaGraphExecDestroy(w->vcycle);
   for (void* p : w->blocks) cudaFree(p);
   delete w;
@@ -61,6 +107,71 @@ void invalidate_graphs(ssg_context* c) {
   if (c->ws->vcycle) cudaGraphExecDestroy(c->ws->vcycle);
   c->ws->vcycle = nullptr;
   c->ws->vcycle_failed = false;
+  drop_iteration_graphs(c->ws);
+}
+
+// Guard of a conditional graph node: its body runs while the solve's stop
+// flag is clear (device side, no host round trip).
+__global__ void k_set_running(cudaGraphConditionalHandle h, const double* __restrict__ done) {
+  cudaGraphSetConditional(h, *done == 0.0 ? 1u : 0u);
+}
+
+// A graph whose conditional node (IF or WHILE) holds the work `enqueue`
+// puts on the stream, guarded by k_set_running on the stop flag `done`; for
+// WHILE the body ends with the same guard.  Returns false when the driver
+// refuses any step (the caller then launches directly).
+template <typename F>
+static bool build_conditional_graph(ssg_context* c, bool loop, const double* done, F&& enqueue,
+                                    cudaGraphExec_t* exec, unsigned long long* kernels) {
+  cudaStream_t s = c->stream;
+  cudaGraph_t g = nullptr;
+  if (cudaGraphCreate(&g, 0) != cudaSuccess) return false;
+  bool ok = false;
+  do {
+    cudaGraphConditionalHandle h;
+    if (cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault) != cudaSuccess)
+      break;
+    // the guard kernel, then the conditional node after it
+    cudaGraphNode_t guard = nullptr;
+    {
+      cudaKernelNodeParams kp = {};
+      void* args[] = {&h, &done};
+      kp.func = (void*)k_set_running;
+      kp.gridDim = dim3(1);
+      kp.blockDim = dim3(1);
+      kp.kernelParams = args;
+      if (cudaGraphAddKernelNode(&guard, g, nullptr, 0, &kp) != cudaSuccess) break;
+    }
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = loop ? cudaGraphCondTypeWhile : cudaGraphCondTypeIf;
+    cp.conditional.size = 1;
+    cudaGraphNode_t cn = nullptr;
+    if (cudaGraphAddNode(&cn, g, &guard, 1, &cp) != cudaSuccess) break;
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    const unsigned long long before = t_launches;
+    if (cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0,
+                                      cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+      break;
+    const ssg_status st = enqueue();
+    if (loop && st == SSG_OK) k_set_running<<<1, 1, 0, s>>>(h, done);
+    cudaGraph_t out = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(s, &out);
+    const unsigned long long captured = t_launches - before;
+    g_launches -= captured;   // recorded, not launched
+    t_launches = before;
+    if (st != SSG_OK || ce != cudaSuccess) break;
+    if (cudaGraphInstantiate(exec, g, 0) != cudaSuccess) break;
+    *kernels = captured;
+    ok = true;
+  } while (false);
+  if (!ok) {
+    cudaGetLastError();
+    c->err.clear();
+  }
+  cudaGraphDestroy(g);
+  return ok;
 }
 
 static ssg_status wsalloc(ssg_context* c, Workspace* w, void** p, size_t bytes) {
@@ -220,7 +331,72 @@ ssg_status cg_solve(ssg_context* c, int level, int var, bool fp32, void* f, void
   cg.dinv = dinv;
   cg.z = W.z;
   cg.alpha = fr + F_ALPHA;
+  // A solve (sync_each) whose first iteration has run: the remaining ones
+  // as one WHILE graph node -- its body is one iteration, repeated on the
+  // device while the stop flag is clear, so the solve synchronises with the
+  // host once.  Captured per (operands, eps, cap, lambda, history) and
+  // replayed; a refused capture falls back to chunks of 8 launched
+  // iterations with a host check between chunks.
+  Workspace* wsp = c->ws;
+  Workspace::LoopKey key;
+  key.f = f;
+  key.x = x;
+  key.hist = hist;
+  key.eps = eps;
+  key.lam = helm ? lam : 0.0;
+  key.max_iter = max_iter;
+  key.hist_cap = hist_cap;
+  key.var = var;
+  key.level = level;
+  key.frame = frame;
+  key.fp32 = fp32;
+  const bool loop_graph = sync_each && c->graphs && !wsp->cgloop_failed && max_iter > 1;
   for (int it = 0; it < max_iter; ++it) {
+    if (loop_graph && it == 1) {
+      if (!(wsp->cgloop && wsp->cgloop_key == key)) {
+        if (wsp->cgloop) cudaGraphExecDestroy(wsp->cgloop);
+        wsp->cgloop = nullptr;
+        pu.first = 0;
+        dop.code = OP_CG_ALPHA;
+        const bool ok = build_conditional_graph(
+            c, true, stop,
+            [&]() -> ssg_status {
+              SSG_CUDA(c, run_ax(s, L.n, c->nel, 0, helm, fp32, W.p, W.aploc, gf, np, L.bj, L.D,
+                                 L.S, lam, &pu));
+              if (fused) {
+                op.code = OP_CG_BETA;
+                SSG_CUDA(c, run_dss(s, DSS_CGUPD, fp32, L.n, c->nel, W.aploc, nullptr, c->d_pairs,
+                                    L.dss_ec, mask, nullptr, nullptr, c->d_part, stop, &op, &cg));
+              } else {
+                op.code = OP_CG_ALPHA;
+                SSG_CUDA(c, run_dss(s, DSS_DOT, fp32, L.n, c->nel, W.aploc, W.ap, c->d_pairs,
+                                    L.dss_ec, mask, W.p, nullptr, c->d_part, stop, &op));
+                op.code = OP_CG_BETA;
+                SSG_CUDA(c, run_cg_update(s, fp32, np, fr + F_ALPHA, x, W.p, W.r, W.ap, dinv,
+                                          L.mult, W.z, c->d_part, nb, stop, &op));
+              }
+              return SSG_OK;
+            },
+            &wsp->cgloop, &wsp->cgloop_kernels);
+        if (ok) {
+          wsp->cgloop_key = key;
+        } else {
+          wsp->cgloop_failed = true;
+        }
+      }
+      if (wsp->cgloop) {
+        SSG_CUDA(c, cudaGraphLaunch(wsp->cgloop, s));
+        double iters;
+        SSG_TRY(read_flag(c, fr + F_ITER, &iters));
+        SSG_TRY(check_interrupt(c));
+        // guard + one body (and its guard) per iteration that ran
+        const unsigned long long k = 1 + (unsigned long long)std::max(0.0, iters - 1.0) *
+                                             (wsp->cgloop_kernels + 1);
+        g_launches += k;
+        t_launches += k;
+        break;
+      }
+    }
     // p = beta p + (z - c) (first: p = z - c), masked; aploc = A p
     // (fused: pap = p . aploc and alpha = rdz / pap; first: pap only)
     pu.first = it == 0;
@@ -473,35 +649,46 @@ ssg_status fcg_solve(ssg_context* c, const double* f, double* u, double eps, int
   for (int k = 0; k < 11; ++k) pslot[k] = k;
   for (int k = 0; k < 10; ++k) aslot[k] = k;
   const int mmax = 10;
-  for (int j = 0; j < max_iter; ++j) {
+  // Iteration j: the window m = min(j, max(1, j mod 11)) and the rotation of
+  // the direction slots; enqueue = false only advances the slots (the
+  // iteration's launches are already in a graph).  vcycle_graph: the
+  // V-cycle from its own graph (direct launches inside an iteration graph).
+  auto iteration = [&](int j, bool enqueue, bool vcycle_graph) -> ssg_status {
     int m = std::max(1, j % (mmax + 1));
     m = std::min(m, j);
-    SSG_TRY(vcycle_ws(c, eps));
-    // subtract_nullspace(z)
-    op.code = OP_NULL_C;
-    SSG_CUDA(c, run_wsum(s, false, np, w->z, L.mult, c->d_part, nb, &op));
-    SSG_CUDA(c, run_add_const(s, false, np, w->z, fr + F_C, 1));
-    // beta_k = (z w).ap_k / pap_k
-    if (m > 0) {
-      PtrList yb;
-      for (int k = 0; k < m; ++k) {
-        yb.p[k] = w->AP[aslot[k]];
-        op.pap_idx[k] = aslot[k];
+    if (enqueue) {
+      if (vcycle_graph)
+        SSG_TRY(vcycle_ws(c, eps));
+      else
+        SSG_TRY(mg_apply(c, w->r, w->z, eps));
+      // subtract_nullspace(z)
+      op.code = OP_NULL_C;
+      SSG_CUDA(c, run_wsum(s, false, np, w->z, L.mult, c->d_part, nb, &op));
+      SSG_CUDA(c, run_add_const(s, false, np, w->z, fr + F_C, 1));
+      // beta_k = (z w).ap_k / pap_k
+      if (m > 0) {
+        PtrList yb;
+        for (int k = 0; k < m; ++k) {
+          yb.p[k] = w->AP[aslot[k]];
+          op.pap_idx[k] = aslot[k];
+        }
+        op.m = m;
+        op.code = OP_FCG_BETA;
+        SSG_CUDA(c, run_dots(s, false, np, w->z, yb, m, L.mult, c->d_part, nb, &op));
       }
-      op.m = m;
-      op.code = OP_FCG_BETA;
-      SSG_CUDA(c, run_dots(s, false, np, w->z, yb, m, L.mult, c->d_part, nb, &op));
     }
     // shift the directions and form p0 = z - sum beta_k p_k
     const int tail = pslot[m];
     for (int k = m; k > 0; --k) pslot[k] = pslot[k - 1];
     pslot[0] = tail;
     double* p0 = w->P[pslot[0]];
-    SSG_CUDA(c, cudaMemcpyAsync(p0, w->z, np * sizeof(double), cudaMemcpyDeviceToDevice, s));
-    if (m > 0) {
-      PtrList yp;
-      for (int k = 0; k < m; ++k) yp.p[k] = w->P[pslot[k + 1]];
-      SSG_CUDA(c, run_combine(s, np, p0, yp, fr + F_FBETA, m, -1.0));
+    if (enqueue) {
+      SSG_CUDA(c, cudaMemcpyAsync(p0, w->z, np * sizeof(double), cudaMemcpyDeviceToDevice, s));
+      if (m > 0) {
+        PtrList yp;
+        for (int k = 0; k < m; ++k) yp.p[k] = w->P[pslot[k + 1]];
+        SSG_CUDA(c, run_combine(s, np, p0, yp, fr + F_FBETA, m, -1.0));
+      }
     }
     // shift the ap history
     int m2 = std::max(1, (j + 1) % (mmax + 1));
@@ -509,6 +696,7 @@ ssg_status fcg_solve(ssg_context* c, const double* f, double* u, double eps, int
     const int atail = aslot[m2 - 1];
     for (int k = m2 - 1; k > 0; --k) aslot[k] = aslot[k - 1];
     aslot[0] = atail;
+    if (!enqueue) return SSG_OK;
     double* ap0 = w->AP[aslot[0]];
     // ap0 = A p0; pap0 and alpha = (p0 w).r / pap0
     SSG_CUDA(c, run_ax(s, L.n, c->nel, 0, false, false, p0, w->aploc, L.gf, np, nullptr, L.D,
@@ -521,16 +709,94 @@ ssg_status fcg_solve(ssg_context* c, const double* f, double* u, double eps, int
     op.code = OP_FCG_ERR;
     SSG_CUDA(c, run_fcg_update(s, np, fr + F_ALPHA, u, p0, w->r, ap0, L.mult, c->d_part, nb,
                                &op));
-    double done;
-    SSG_TRY(read_flag(c, fr + F_DONE, &done));
-    if (done != 0.0) break;
-    SSG_TRY(check_interrupt(c));
+    return SSG_OK;
+  };
+
+  // Graph mode: once a configuration (eps, precision, iteration cap,
+  // history) has run directly, every iteration is one graph launch -- the
+  // graph of its window state, captured on first use -- and iterations are
+  // enqueued ahead in chunks of 16, 32, 64, ... with one host
+  // synchronisation per chunk (a C2 solve of 11 iterations: one).
+  // Iterations past the stop skip their work on the device.  Results are
+  // those of the direct launches (the same kernels in the same order).
+  const bool same_cfg = w->fcg_eps == eps && w->fcg_precision == c->precision &&
+                        w->fcg_max_iter == max_iter && w->fcg_hcap == hcap;
+  if (!same_cfg) {
+    drop_iteration_graphs(w);
+    w->fcg_eps = eps;
+    w->fcg_precision = c->precision;
+    w->fcg_max_iter = max_iter;
+    w->fcg_hcap = hcap;
+  }
+  const bool graph_mode = c->graphs && !w->fcg_failed && w->fcg_warm > 0 && !w->vcycle_failed;
+  bool graph_mode_used = false;
+  int graph_iters = 0;   // iteration graphs enqueued (each runs its guard)
+  if (!graph_mode) {
+    for (int j = 0; j < max_iter; ++j) {
+      SSG_TRY(iteration(j, true, true));
+      double done;
+      SSG_TRY(read_flag(c, fr + F_DONE, &done));
+      if (done != 0.0) break;
+      SSG_TRY(check_interrupt(c));
+    }
+    ++w->fcg_warm;
+  } else {
+    graph_mode_used = true;
+    int j = 0, chunk = 16;
+    while (j < max_iter) {
+      const int end = std::min(max_iter, j + chunk);
+      for (; j < end; ++j) {
+        const int key = j == 0 ? 0 : 1 + (j - 1) % (Workspace::kFcgStates - 1);
+        if (!w->fcg[key]) {
+          int ps[11], as[10];
+          std::memcpy(ps, pslot, sizeof(ps));
+          std::memcpy(as, aslot, sizeof(as));
+          const bool ok = build_conditional_graph(
+              c, false, fr + F_DONE, [&] { return iteration(j, true, false); }, &w->fcg[key],
+              &w->fcg_kernels[key]);
+          std::memcpy(pslot, ps, sizeof(ps));
+          std::memcpy(aslot, as, sizeof(as));
+          if (!ok) {
+            // finish this solve with direct launches
+            w->fcg_failed = true;
+            w->fcg[key] = nullptr;
+            for (; j < max_iter; ++j) {
+              SSG_TRY(iteration(j, true, true));
+              double done;
+              SSG_TRY(read_flag(c, fr + F_DONE, &done));
+              if (done != 0.0) break;
+              SSG_TRY(check_interrupt(c));
+            }
+            break;
+          }
+        }
+        SSG_TRY(iteration(j, false, false));
+        SSG_CUDA(c, cudaGraphLaunch(w->fcg[key], s));
+        ++graph_iters;
+      }
+      if (w->fcg_failed) break;
+      double done;
+      SSG_TRY(read_flag(c, fr + F_DONE, &done));
+      if (done != 0.0) break;
+      SSG_TRY(check_interrupt(c));
+      chunk *= 2;
+    }
   }
   double h[F_SIZE];
   SSG_CUDA(c, cudaMemcpyAsync(c->h_pin, fr, F_SIZE * sizeof(double), cudaMemcpyDeviceToHost,
                               s));
   SSG_CUDA(c, cudaStreamSynchronize(s));
   std::memcpy(h, c->h_pin, sizeof(h));
+  if (graph_mode_used) {
+    // launch count: every enqueued graph's guard, the bodies of the
+    // iterations that ran
+    unsigned long long k = (unsigned long long)graph_iters;
+    const int ran = (int)h[F_ITER];
+    for (int j = 0; j < ran && j < graph_iters; ++j)
+      k += w->fcg_kernels[j == 0 ? 0 : 1 + (j - 1) % (Workspace::kFcgStates - 1)];
+    g_launches += k;
+    t_launches += k;
+  }
   if (info) {
     info->iterations = (int)h[F_ITER];
     info->residual = h[F_ERR];

@@ -92,6 +92,11 @@ inline void count_launch() {
 }
 
 int vec_blocks(size_t npts);
+// elements-per-block value of the operator launch that selects the line-form
+// kernel (k_axl, a fixed number of elements per block) for orders other
+// than 8; 1, 2, 4, ... select the plane-form kernel k_ax with that many
+// elements per block; 0 asks for the order's default (ax_epb)
+constexpr int kAxLine = -1;
 int ax_epb(int n);
 int ax_epb_max(int n);
 int dss_grid(int n, int nel);

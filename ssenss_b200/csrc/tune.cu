@@ -2,9 +2,10 @@
 //
 // The element kernels have one free shape parameter per order n and the
 // vector kernels one overall:
-//   * elements per block of the shared-memory operator (k_ax: 1, 2, 4, ...
-//     up to the 256-thread / 96 KB limit of ax_epb_max(n)); order 8 runs the
-//     FP64 tensor-core operator k_ax8_dmma, which has no shape parameter;
+//   * the operator of every order but 8: the line-form kernel k_axl, or the
+//     plane-form k_ax with 1, 2, 4, ... elements per block up to the
+//     256-thread / 96 KB limit of ax_epb_max(n); order 8 runs the FP64
+//     tensor-core operator k_ax8_dmma, which has no shape parameter;
 //   * the cap of the DSS grid (one node per thread below it): 4 .. 64
 //     blocks per SM;
 //   * the cap of the vector kernels' grid (one point per thread below it):
@@ -54,7 +55,7 @@ static ssg_status tune_level(ssg_context* c, int level, double* a, double* b, do
   if (n != 8) {
     int best_epb = 0;
     float best = 1e30f;
-    for (int epb = 1; epb <= ax_epb_max(n); epb *= 2) {
+    for (int epb = kAxLine; epb <= ax_epb_max(n); epb = epb == kAxLine ? 1 : 2 * epb) {
       g_tune_ax_epb[n] = epb;
       SSG_CUDA(c, run_ax(c->stream, n, c->nel, epb, false, false, a, b, L.gf, L.npts, nullptr,
                          L.D, L.D, 0.0, nullptr));

@@ -71,3 +71,31 @@ def same_stop(it_g, h_g, h_o):
     for h in (h_g[k], h_o[k]):
         assert 0.5 * EPS <= h <= 2 * EPS, (it_g, it_o, h_g[k], h_o[k])
     return False
+
+
+def history_deviation(h_g, h_o):
+    """|h_g - h_o| over the common iterations of two residual histories."""
+    k = min(len(h_g), len(h_o))
+    return np.abs(np.asarray(h_g[:k], dtype=float) - np.asarray(h_o[:k], dtype=float))
+
+
+def check_history(h_g, h_o, floor=0.0):
+    """Residual histories of two runs of the same solve, over the common
+    iterations: within 1e-9 of the first residual wherever the residual is
+    above 1e-4 of it, within 1e-7 of it below.  Near the stop the residual
+    is set by the rounding of the V-cycle's inner CG solves, which stop on
+    the same absolute eps and so take different inner iteration counts in
+    any two FP64 implementations (the oracle and the reference differ there
+    by up to 20 % of the residual itself); both bounds are stated here.
+    floor: an absolute deviation always accepted (the rounding level of the
+    problem's data, stated by the caller).  Returns the largest deviation
+    relative to the first residual."""
+    d = history_deviation(h_g, h_o)
+    if d.size == 0:
+        return 0.0
+    h_o = np.asarray(h_o[:d.size], dtype=float)
+    h0 = h_o[0]
+    hi = h_o > 1e-4 * h0
+    assert np.all(d[hi] <= np.maximum(1e-9 * h0, floor)), d / h0
+    assert np.all(d <= np.maximum(1e-7 * h0, floor)), d / h0
+    return float(np.max(d) / h0)

@@ -87,14 +87,14 @@ def test_gll_matches_the_oracle():
 
 def test_default_launch_shapes():
     """ssg_tuning (host only) before any autotuning: the FP64 tensor-core
-    operator at n = 8, positive shapes elsewhere, orders out of range
-    rejected."""
+    operator at n = 8 (0), the line-form operator elsewhere (-1), positive
+    grid shapes, orders out of range rejected."""
     import ssenss_b200 as S
     t8 = S.tuning(8)
     assert t8["ax_elements_per_block"] == 0
     for n in (2, 4, 6, 10, 12):
         t = S.tuning(n)
-        assert t["ax_elements_per_block"] >= 1
+        assert t["ax_elements_per_block"] == -1
         assert t["dss_blocks_per_sm"] >= 1 and t["vector_blocks_per_sm"] >= 1
     for bad in (1, 19):
         with pytest.raises(S.SsgError):

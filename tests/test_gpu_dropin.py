@@ -24,8 +24,11 @@ and three Helmholtz solves (Jacobi CG), all to the reference's absolute
 Bars (each stated where it is asserted):
   * every solve of every step: the same number of iterations, or one apart
     only where the residual at the deciding iteration lies within a factor 2
-    of eps (conftest.same_stop); residual histories within HIST_REL of the
-    first residual of the solve;
+    of eps (conftest.same_stop); residual histories as conftest.check_history
+    (1e-9 of the first residual while above 1e-4 of it, 1e-7 below, and
+    an absolute floor of 1e-13: the fields are of order one, and the
+    pressure solves start from an extrapolated guess whose residual is
+    already small, so their differences sit at the rounding of the data);
   * fields u, v, w, p after 20 steps: FIELD_REL relative to the largest
     entry while every solve stopped at the same iteration;
   * the individual bound functions on the reference's own set-up: DSS
@@ -41,7 +44,7 @@ import numpy as np
 import pytest
 
 import oracle as O
-from conftest import EPS
+from conftest import EPS, check_history, history_deviation
 
 pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(not (os.path.exists(O.REF_SO) and os.path.exists(O.REF_GPU_SO)),
@@ -49,7 +52,6 @@ pytestmark = [pytest.mark.gpu,
 
 STEPS = 20
 DT, VISC = 1e-3, 1.0 / 1600.0
-HIST_REL = 1e-9
 FIELD_REL = 1e-11
 
 
@@ -151,30 +153,36 @@ def _solves(r, s):
 def test_c1_navier_stokes_steps_through_the_binding(c1):
     cpu, gpu = c1
     assert float(gpu["t"]) == pytest.approx(STEPS * DT)
-    all_same_stop = True
-    worst_hist = 0.0
+    # every solve of every step: iterations and history deviations (all
+    # gathered first, printed, then asserted)
+    rows = []
     for s in range(STEPS):
         sc, sg = _solves(cpu, s), _solves(gpu, s)
         assert [k for k, _ in sc] == [k for k, _ in sg] == [(0, 0), (1, 1), (1, 2), (1, 3)]
         for (kv, hc), (_, hg) in zip(sc, sg):
-            if len(hc) != len(hg):
-                all_same_stop = False
-                assert abs(len(hc) - len(hg)) == 1, (s, kv, len(hc), len(hg))
-                k = min(len(hc), len(hg)) - 1
-                for h in (hc[k], hg[k]):
-                    assert 0.5 * EPS <= h <= 2 * EPS, (s, kv, hc, hg)
-            k = min(len(hc), len(hg))
-            dev = float(np.max(np.abs(hc[:k] - hg[:k])) / hc[0]) if k else 0.0
-            worst_hist = max(worst_hist, dev)
-            assert dev <= HIST_REL, (s, kv, dev)
+            d = history_deviation(hg, hc)
+            rows.append((s, kv, len(hc), len(hg), hc, hg, float(d.max()) if d.size else 0.0))
     devs = []
     for w in range(4):
         a, b = cpu[f"f{w}"], gpu[f"f{w}"]
         scale = max(float(np.max(np.abs(a))), 1e-300)
         devs.append(float(np.max(np.abs(a - b))) / scale)
-    print(f"C1 drop-in: history deviation {worst_hist:.2e} of h0, fields u v w p "
-          f"{', '.join(f'{d:.2e}' for d in devs)}, every stop equal: {all_same_stop}")
-    if all_same_stop:
+    same = all(r[2] == r[3] for r in rows)
+    worst = max(rows, key=lambda r: r[6] / r[4][0])
+    print(f"C1 drop-in: {len(rows)} solves, every stop equal: {same}, largest history "
+          f"deviation {worst[6]:.2e} absolute ({worst[6] / worst[4][0]:.2e} of h0, step "
+          f"{worst[0]}, solve {worst[1]}), fields u v w p after {STEPS} steps "
+          f"{', '.join(f'{d:.2e}' for d in devs)}")
+    for s, kv, lc, lg, hc, hg, dmax in rows:
+        if lc != lg:
+            assert abs(lc - lg) == 1, (s, kv, lc, lg)
+            k = min(lc, lg) - 1
+            for h in (hc[k], hg[k]):
+                assert 0.5 * EPS <= h <= 2 * EPS, (s, kv, hc, hg)
+        # the fields are of order one and every solve stops at 1e-10
+        # absolute: deviations below 1e-13 are rounding of the data
+        check_history(hg, hc, floor=1e-13)
+    if same:
         assert max(devs) <= FIELD_REL, devs
 
 
@@ -203,8 +211,7 @@ def test_bound_functions_match_the_reference(ops):
     assert _rel(gpu["sol_h"], cpu["sol_h"]) < 1e-12
     if len(gpu["hist_p"]) == len(cpu["hist_p"]):
         assert _rel(gpu["sol_p"], cpu["sol_p"]) < 1e-11
-    k = min(len(gpu["hist_p"]), len(cpu["hist_p"]))
-    assert np.all(np.abs(gpu["hist_p"][:k] - cpu["hist_p"][:k]) <= HIST_REL * cpu["hist_p"][0])
+    check_history(gpu["hist_p"], cpu["hist_p"])
     assert _rel(gpu["mg"], cpu["mg"]) < 1e-9
 
 

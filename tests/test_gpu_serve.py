@@ -163,3 +163,29 @@ def test_failed_setup_does_not_poison_the_mesh_key():
     orc = oracle_for(0)
     u_o, _ = orc.solve_poisson(f, np.zeros_like(f))
     assert rel(u - u.mean(), u_o - u_o.mean()) < 1e-8
+
+
+@pytest.mark.parametrize("shape,n,lam", [((2, 2, 2), 6, 0.0), ((2, 2, 3), 8, 40.0),
+                                          ((2, 3, 3), 5, 0.0), ((1, 3, 3), 6, 7.5)])
+def test_small_boxes_against_assembled_oracle(shape, n, lam):
+    """Boxes with one or two elements along a periodic direction ("reference-
+    incorrect": the reference's first-match pairing joins a face to the
+    neighbour's face on the same side, so no reference run can check them).
+    The serving loop pairs opposite faces; its solution is checked against
+    the assembled-operator oracle with correct global numbering
+    (oracle/periodic_box.py) at 1e-8 relative to the largest entry (mixed
+    precision Poisson and FP64 Helmholtz, both stopped at sqrt((r.r)_w) <=
+    1e-10; Poisson solutions compared with their means removed)."""
+    from oracle import periodic_box as PB
+    mesh = box_mesh(shape)
+    f = periodic_box_fourier_rhs(shape, n, 31)
+    srv = S.Server(0, hbm_budget=40e9, max_active=2)
+    try:
+        u, st, info = srv.wait(srv.submit(mesh, n, f, lam=lam, precision="mixed"))
+    finally:
+        srv.close()
+    assert st == "SSG_OK", st
+    u_b = PB.solve(shape, n, f, lam)
+    if lam == 0:
+        u, u_b = u - u.mean(), u_b - u_b.mean()
+    assert rel(u, u_b) < 1e-8, (rel(u, u_b), info)

@@ -1,6 +1,8 @@
-"""CUDA-graph replay of the V-cycle and the launch-shape autotuner.
+"""CUDA-graph replay of the V-cycle, of the outer FCG iterations (one graph
+per window state, an IF node guarded by the device stop flag) and of the
+Helmholtz CG loop (a WHILE node), and the launch-shape autotuner.
 
-The captured graph launches the same kernels with the same arguments as the
+The captured graphs launch the same kernels with the same arguments as the
 direct path, so a solve with graphs is bitwise the solve without.  The
 autotuner changes only launch shapes: element-local results and the DSS stay
 bitwise, while block-partial sums of the inner products may associate
@@ -47,20 +49,43 @@ def test_graph_replay_is_bitwise_direct(precision, gpu_ctx_factory):
 
 
 def test_graph_launch_count_is_kept(gpu_ctx_factory):
+    """Replayed graphs count the kernels they run: the direct path's, plus
+    one guard kernel per enqueued FCG iteration graph (16 are enqueued for a
+    solve of at most 16 iterations)."""
     mesh, n = tgv_box(3), 6
     orc = O.Oracle(mesh, n)
     f = rhs(orc, n)
     ctx = gpu_ctx_factory(mesh, n)
     ctx.set_graphs(False)
     c0 = S.kernel_launch_count()
-    ctx.solve_poisson_cg(f, np.zeros_like(f))
+    _, info = ctx.solve_poisson_cg(f, np.zeros_like(f))
     direct = S.kernel_launch_count() - c0
+    assert info["iterations"] <= 16
     ctx.set_graphs(True)
     ctx.solve_poisson_cg(f, np.zeros_like(f))      # warm-up of the V-cycle
     ctx.solve_poisson_cg(f, np.zeros_like(f))      # capture
     c0 = S.kernel_launch_count()
     ctx.solve_poisson_cg(f, np.zeros_like(f))      # replay
-    assert S.kernel_launch_count() - c0 == direct
+    assert S.kernel_launch_count() - c0 == direct + 16
+
+
+def test_helmholtz_while_graph_is_bitwise_direct(gpu_ctx_factory):
+    """The Helmholtz CG's iterations after the first as one WHILE graph node:
+    the same iterations, solution and residual history as direct launches,
+    on capture and on replay."""
+    mesh, n = channel_mesh((4, 3, 3), seed=7), 7
+    orc = O.Oracle(mesh, n)
+    f = rhs(orc, n)
+    ctx = gpu_ctx_factory(mesh, n)
+    ctx.set_graphs(False)
+    u_d, info_d = ctx.solve_helmholtz_cg(O.X_VELOCITY, f, np.zeros_like(f))
+    assert info_d["iterations"] > 8
+    ctx.set_graphs(True)
+    for _ in range(2):                             # capture, replay
+        u_g, info_g = ctx.solve_helmholtz_cg(O.X_VELOCITY, f, np.zeros_like(f))
+        assert info_g["iterations"] == info_d["iterations"]
+        assert np.array_equal(u_g, u_d)
+        assert np.array_equal(info_g["history"], info_d["history"])
 
 
 @pytest.mark.parametrize("mk,n", [(lambda: tgv_box(3), 8),
@@ -72,7 +97,8 @@ def test_autotuned_shapes_keep_parity(mk, n, gpu_ctx_factory):
     shapes = ctx.autotune(reps=3)
     assert set(shapes) == set(ctx.orders)
     for n_l, sh in shapes.items():
-        assert sh["ax_elements_per_block"] >= (0 if n_l == 8 else 1)
+        assert sh["ax_elements_per_block"] == 0 if n_l == 8 else \
+            sh["ax_elements_per_block"] in (-1, 1, 2, 4, 8, 16, 32, 64)
         assert 4 <= sh["dss_blocks_per_sm"] <= 64
         assert 2 <= sh["vector_blocks_per_sm"] <= 64
     rng = np.random.default_rng(9)
