@@ -86,183 +86,27 @@ __global__ void __launch_bounds__(256, (N >= 10 ? 1 : 2)) k_ax(int nel, T* __res
 // per 16-byte load.  EPB elements per block fill about 256 threads.  Same
 // interface as k_ax (optional direction update and p . (A p)).
 // ---------------------------------------------------------------------------
-template <int N>
-struct AxLine {
-  static constexpr int EPB = (256 / (N * N)) > 0 ? 256 / (N * N) : 1;
-  static constexpr int TASKS = EPB * N * N;
-  static constexpr int THREADS = (TASKS + 31) / 32 * 32;
-  static constexpr int RM = N + (N & 1);                 // matrix rows (pair-aligned)
-  static constexpr int RS = N + ((2 - N % 4) + 4) % 4;   // field rows: 2 mod 4 values
-  static constexpr int FS = N * N * RS;                  // one staged field
-  static constexpr int MATS = 4 * N * RM;
-  static constexpr int SMEM = MATS + EPB * 4 * FS;       // values of the compute type
-};
-
-// sum_l A[o][l] x[l] (A rows of RM values, pair-aligned), in l order; every
-// lane of the warp reads the same A entries
-template <int N, int RM, typename C>
-__device__ __forceinline__ C line_row(const C* A, int o, const C (&x)[N]) {
-  using V2 = typename std::conditional<sizeof(C) == 8, double2, float2>::type;
-  C acc = 0;
-#pragma unroll
-  for (int l = 0; l + 1 < N; l += 2) {
-    const V2 a = *reinterpret_cast<const V2*>(A + o * RM + l);
-    acc += a.x * x[l];
-    acc += a.y * x[l + 1];
-  }
-  if (N & 1) acc += A[o * RM + N - 1] * x[N - 1];
-  return acc;
-}
-
-// dst[o * stride] (=, or += when ADD) sum_l A[o][l] x[l] for o < N; the
-// output loop is not unrolled, so a line's matrix rows are read one row at
-// a time and the registers hold the line only
-template <int N, int RM, bool ADD, typename C>
-__device__ __forceinline__ void line_apply(const C* A, const C (&x)[N], C* dst, int stride) {
-#pragma unroll 2
-  for (int o = 0; o < N; ++o) {
-    const C v = line_row<N, RM, C>(A, o, x);
-    if (ADD)
-      dst[o * stride] += v;
-    else
-      dst[o * stride] = v;
-  }
-}
-
-// The arithmetic runs in the storage type T: FP64 for the solves, FP32 in
-// the mixed-precision V-cycle (the fused direction update and the p . (A p)
-// sum stay FP64).
 template <int N, typename T, bool HELM, bool FUSEP>
 __global__ void __launch_bounds__(AxLine<N>::THREADS)
     k_axl(int nel, T* __restrict__ u, T* __restrict__ au, const T* __restrict__ gf,
           size_t npts, const double* __restrict__ bj, const double* __restrict__ Dg,
           const double* __restrict__ Sg, double lambda, PUpdate pu, ScalarOp dop) {
   using L = AxLine<N>;
-  using C = T;
-  constexpr int NN = N * N, NT = N * N * N, RM = L::RM, RS = L::RS, FS = L::FS;
   if (FUSEP && pu.stop && *pu.stop != 0.0) return;   // uniform over the block
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* sD = reinterpret_cast<C*>(smem_raw);
-  C* sDT = sD + N * RM;
-  C* sS = sDT + N * RM;
-  C* sST = sS + N * RM;
-  C* fld = sD + L::MATS;   // per slot: U/O, F1, F2, F3 (FS values each)
-  const int tid = threadIdx.x;
-  for (int q = tid; q < NN; q += blockDim.x) {
-    const int r = q / N, c = q % N;
-    const C d = (C)Dg[q], sv = HELM ? (C)Sg[q] : d;
-    sD[r * RM + c] = d;
-    sDT[c * RM + r] = d;
-    sS[r * RM + c] = sv;
-    sST[c * RM + r] = sv;
-  }
+  T* sD = reinterpret_cast<T*>(smem_raw);
+  axl_load_mats<N, T, HELM>(sD, Dg, Sg);
   const int e0 = blockIdx.x * L::EPB;
-  const int ne = min(L::EPB, nel - e0);
-  const size_t base = (size_t)e0 * NT;
-  const int npb = ne * NT;   // points of this block
   const T* z = FUSEP ? reinterpret_cast<const T*>(pu.z) : nullptr;
   const double beta = (FUSEP && !pu.first) ? *pu.beta : 0.0;
   const double c = (FUSEP && pu.c) ? *pu.c : 0.0;
-  // P0: stage the field (forming p first when fused), coalesced
-  for (int q = tid; q < npb; q += blockDim.x) {
-    const size_t o = base + q;
-    C v;
-    if (FUSEP) {
-      const double zc = (double)z[o] - c;
-      double pv = pu.first ? zc : beta * (double)u[o] + zc;
-      if (pu.mask) pv = pv * pu.mask[o];
-      const T vt = (T)pv;
-      u[o] = vt;
-      v = (C)vt;
-    } else {
-      v = (C)u[o];
-    }
-    const int sl = q / NT, p = q % NT;
-    fld[sl * 4 * FS + (p / NN) * N * RS + ((p / N) % N) * RS + p % N] = v;
-  }
-  __syncthreads();
-  const bool task = tid < ne * NN;
-  const int sl = tid / NN, a0 = (tid % NN) % N, a1 = (tid % NN) / N;
-  C* U = fld + sl * 4 * FS;
-  C* F1 = U + FS;
-  C* F2 = F1 + FS;
-  C* F3 = F2 + FS;
-  // P1-P3: derivatives along i (r, with S for Helmholtz), j (s), k (t)
-  if (task) {
-    C x[N];
-    {   // lines (j = a0, k = a1) along i
-      const C* src = U + a1 * N * RS + a0 * RS;
-#pragma unroll
-      for (int l = 0; l < N; ++l) x[l] = src[l];
-      line_apply<N, RM, false, C>(HELM ? sS : sD, x, F1 + a1 * N * RS + a0 * RS, 1);
-    }
-    {   // lines (i = a0, k = a1) along j
-      const C* src = U + a1 * N * RS + a0;
-#pragma unroll
-      for (int l = 0; l < N; ++l) x[l] = src[l * RS];
-      line_apply<N, RM, false, C>(sD, x, F2 + a1 * N * RS + a0, RS);
-    }
-    {   // lines (i = a0, j = a1) along k
-      const C* src = U + a1 * RS + a0;
-#pragma unroll
-      for (int l = 0; l < N; ++l) x[l] = src[l * N * RS];
-      line_apply<N, RM, false, C>(sD, x, F3 + a1 * RS + a0, N * RS);
-    }
-  }
-  __syncthreads();
-  // P4: w = G (ur, us, ut) at every point, in place
-  for (int q = tid; q < npb; q += blockDim.x) {
-    const size_t o = base + q;
-    const int s2 = q / NT, p = q % NT;
-    const int off = s2 * 4 * FS + (p / NN) * N * RS + ((p / N) % N) * RS + p % N;
-    const C ur = fld[off + FS], us = fld[off + 2 * FS], ut = fld[off + 3 * FS];
-    const C g0 = __ldg(gf + o), g1 = __ldg(gf + npts + o), g2 = __ldg(gf + 2 * npts + o),
-            g3 = __ldg(gf + 3 * npts + o), g4 = __ldg(gf + 4 * npts + o),
-            g5 = __ldg(gf + 5 * npts + o);
-    fld[off + FS] = g0 * ur + g1 * us + g2 * ut;
-    fld[off + 2 * FS] = g1 * ur + g3 * us + g4 * ut;
-    fld[off + 3 * FS] = g2 * ur + g4 * us + g5 * ut;
-  }
-  __syncthreads();
-  // P5-P7: (D^T w0 + S^T w1) + S^T w2, accumulated in U's place
-  if (task) {
-    C x[N];
-    const C* src = F1 + a1 * N * RS + a0 * RS;
-#pragma unroll
-    for (int l = 0; l < N; ++l) x[l] = src[l];
-    line_apply<N, RM, false, C>(sDT, x, U + a1 * N * RS + a0 * RS, 1);
-  }
-  __syncthreads();
-  if (task) {
-    C x[N];
-    const C* src = F2 + a1 * N * RS + a0;
-#pragma unroll
-    for (int l = 0; l < N; ++l) x[l] = src[l * RS];
-    line_apply<N, RM, true, C>(sST, x, U + a1 * N * RS + a0, RS);
-  }
-  __syncthreads();
-  double pap = 0.0;
-  if (task) {
-    C x[N];
-    const C* src = F3 + a1 * RS + a0;
-#pragma unroll
-    for (int l = 0; l < N; ++l) x[l] = src[l * N * RS];
-    const C* acc = U + a1 * RS + a0;
-    const size_t eo = base + (size_t)sl * NT + a1 * N + a0;
-#pragma unroll 2
-    for (int l = 0; l < N; ++l) {
-      const size_t o = eo + (size_t)l * NN;
-      C out = acc[l * N * RS] + line_row<N, RM, C>(sST, l, x);
-      C pv = 0;
-      if (HELM || FUSEP) pv = u[o];
-      if (HELM) out += (C)lambda * ((C)__ldg(bj + o) * pv);
-      au[o] = (T)out;
-      if (FUSEP) pap += (double)pv * (double)out;
-    }
-  }
+  double rdz = 0.0;
+  const double pap = axl_group<N, T, HELM, FUSEP>(
+      e0, min(L::EPB, nel - e0), u, au, gf, npts, bj, lambda, z, beta, c, pu.mask,
+      pu.first != 0, sD, nullptr, nullptr, &rdz);
   if (FUSEP && pu.part) {
     __shared__ double sflat[AxLine<N>::THREADS];
-    finish_flat(pap, tid, blockDim.x, pu.part, dop, sflat);
+    finish_flat(pap, threadIdx.x, blockDim.x, pu.part, dop, sflat);
   }
 }
 

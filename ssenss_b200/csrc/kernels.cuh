@@ -9,6 +9,7 @@
 #include <cuda/atomic>
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <type_traits>
 
 #include "ssg_kernels.h"
 
@@ -516,6 +517,210 @@ __device__ __forceinline__ double ax_element(int e, bool active, int i, int j, c
     if (HELM && active) out += lambda * (__ldg(bj + off + (size_t)k * NN) * ru[k]);
     if (active) au[off + (size_t)k * NN] = (T)out;
     if (FUSEP && active) pap += ru[k] * (double)(T)out;
+  }
+  return pap;
+}
+
+// ---------------------------------------------------------------------------
+// line-form element operator (k_axl in kernels.cu, the fused cooperative
+// smoother in coarse.cu): each thread contracts one whole line of an
+// element (N points along i, j or k) held in registers, so a matrix row is
+// read once per line instead of a shared row and a shared field value per
+// multiply-add.  Per element: the field is staged in shared memory; three
+// passes (lines along i, j, k) give the r-, s- and t-derivatives; a
+// point-wise pass applies the six metric terms; three transposed passes sum
+// D^T w0 + S^T w1 + S^T w2 (D for Poisson) in the order (acc + acs) + act of
+// ax_element.  The matrices sit in shared memory and every lane of a warp
+// reads the same entry (a broadcast), two entries per paired load.  EPB
+// elements per group fill about 256 threads.  The arithmetic runs in the
+// storage type T: FP64 for the solves, FP32 in the mixed-precision V-cycle
+// (the fused direction update and the p . (A p) sum stay FP64).
+// ---------------------------------------------------------------------------
+template <int N>
+struct AxLine {
+  static constexpr int EPB = (256 / (N * N)) > 0 ? 256 / (N * N) : 1;
+  static constexpr int TASKS = EPB * N * N;
+  static constexpr int THREADS = (TASKS + 31) / 32 * 32;
+  static constexpr int RM = N + (N & 1);                 // matrix rows (pair-aligned)
+  static constexpr int RS = N + ((2 - N % 4) + 4) % 4;   // field rows: 2 mod 4 values
+  static constexpr int FS = N * N * RS;                  // one staged field
+  static constexpr int MATS = 4 * N * RM;
+  static constexpr int SMEM = MATS + EPB * 4 * FS;       // values of type T
+};
+
+// sum_l A[o][l] x[l] (A rows of RM values, pair-aligned), in l order; every
+// lane of the warp reads the same A entries
+template <int N, int RM, typename C>
+__device__ __forceinline__ C line_row(const C* A, int o, const C (&x)[N]) {
+  using V2 = typename std::conditional<sizeof(C) == 8, double2, float2>::type;
+  C acc = 0;
+#pragma unroll
+  for (int l = 0; l + 1 < N; l += 2) {
+    const V2 a = *reinterpret_cast<const V2*>(A + o * RM + l);
+    acc += a.x * x[l];
+    acc += a.y * x[l + 1];
+  }
+  if (N & 1) acc += A[o * RM + N - 1] * x[N - 1];
+  return acc;
+}
+
+// dst[o * stride] (=, or += when ADD) sum_l A[o][l] x[l] for o < N; the
+// output loop is not unrolled, so a line's matrix rows are read one row at
+// a time and the registers hold the line only
+template <int N, int RM, bool ADD, typename C>
+__device__ __forceinline__ void line_apply(const C* A, const C (&x)[N], C* dst, int stride) {
+#pragma unroll 2
+  for (int o = 0; o < N; ++o) {
+    const C v = line_row<N, RM, C>(A, o, x);
+    if (ADD)
+      dst[o * stride] += v;
+    else
+      dst[o * stride] = v;
+  }
+}
+
+// D, D^T, S (Helmholtz) or D, S^T = D^T into the first MATS values of the
+// block's shared memory; visible after the next barrier
+template <int N, typename T, bool HELM>
+__device__ __forceinline__ void axl_load_mats(T* sD, const double* __restrict__ Dg,
+                                              const double* __restrict__ Sg) {
+  constexpr int RM = AxLine<N>::RM;
+  T* sDT = sD + N * RM;
+  T* sS = sDT + N * RM;
+  T* sST = sS + N * RM;
+  for (int q = threadIdx.x; q < N * N; q += blockDim.x) {
+    const int r = q / N, c = q % N;
+    const T d = (T)Dg[q], sv = HELM ? (T)Sg[q] : d;
+    sD[r * RM + c] = d;
+    sDT[c * RM + r] = d;
+    sS[r * RM + c] = sv;
+    sST[c * RM + r] = sv;
+  }
+}
+
+// A_e u for the ne <= EPB elements e0 .. e0 + ne - 1, all threads of a block
+// of AxLine<N>::THREADS (barriers inside); sD: the matrices (axl_load_mats)
+// followed by the group's field space.  FUSEP: the input is the direction
+// p = (first ? z - c : beta u + (z - c)) .* mask, written back to u.
+// rdot, mult (optional): also sum (rdot w) p over the staged points, w =
+// 1 / mult, into *rdz.  Returns this thread's share of p . (A p) (FUSEP).
+template <int N, typename T, bool HELM, bool FUSEP>
+__device__ __forceinline__ double axl_group(int e0, int ne, T* __restrict__ u,
+                                            T* __restrict__ au, const T* __restrict__ gf,
+                                            size_t npts, const double* __restrict__ bj,
+                                            double lambda, const T* __restrict__ z,
+                                            double beta, double c,
+                                            const double* __restrict__ mask, bool first,
+                                            T* sD, const T* __restrict__ rdot,
+                                            const uint8_t* __restrict__ mult, double* rdz) {
+  using L = AxLine<N>;
+  using C = T;
+  constexpr int NN = N * N, NT = N * N * N, RM = L::RM, RS = L::RS, FS = L::FS;
+  const C* sDT = sD + N * RM;
+  const C* sS = sDT + N * RM;
+  const C* sST = sS + N * RM;
+  C* fld = sD + L::MATS;   // per slot: U/O, F1, F2, F3 (FS values each)
+  const int tid = threadIdx.x;
+  const size_t base = (size_t)e0 * NT;
+  const int npb = ne > 0 ? ne * NT : 0;   // points of this group
+  __syncthreads();   // the previous group's last pass has read the fields
+  // P0: stage the field (forming p first when fused), coalesced
+  for (int q = tid; q < npb; q += blockDim.x) {
+    const size_t o = base + q;
+    C v;
+    if (FUSEP) {
+      const double zc = (double)z[o] - c;
+      double pv = first ? zc : beta * (double)u[o] + zc;
+      if (mask) pv = pv * mask[o];
+      const T vt = (T)pv;
+      u[o] = vt;
+      v = (C)vt;
+      if (rdot) *rdz += ((double)rdot[o] * inv_count(mult[o])) * (double)vt;
+    } else {
+      v = (C)u[o];
+    }
+    const int sl = q / NT, p = q % NT;
+    fld[sl * 4 * FS + (p / NN) * N * RS + ((p / N) % N) * RS + p % N] = v;
+  }
+  __syncthreads();
+  const bool task = tid < ne * NN;
+  const int sl = tid / NN, a0 = (tid % NN) % N, a1 = (tid % NN) / N;
+  C* U = fld + sl * 4 * FS;
+  C* F1 = U + FS;
+  C* F2 = F1 + FS;
+  C* F3 = F2 + FS;
+  // P1-P3: derivatives along i (r, with S for Helmholtz), j (s), k (t)
+  if (task) {
+    C x[N];
+    {   // lines (j = a0, k = a1) along i
+      const C* src = U + a1 * N * RS + a0 * RS;
+#pragma unroll
+      for (int l = 0; l < N; ++l) x[l] = src[l];
+      line_apply<N, RM, false, C>(HELM ? sS : sD, x, F1 + a1 * N * RS + a0 * RS, 1);
+    }
+    {   // lines (i = a0, k = a1) along j
+      const C* src = U + a1 * N * RS + a0;
+#pragma unroll
+      for (int l = 0; l < N; ++l) x[l] = src[l * RS];
+      line_apply<N, RM, false, C>(sD, x, F2 + a1 * N * RS + a0, RS);
+    }
+    {   // lines (i = a0, j = a1) along k
+      const C* src = U + a1 * RS + a0;
+#pragma unroll
+      for (int l = 0; l < N; ++l) x[l] = src[l * N * RS];
+      line_apply<N, RM, false, C>(sD, x, F3 + a1 * RS + a0, N * RS);
+    }
+  }
+  __syncthreads();
+  // P4: w = G (ur, us, ut) at every point, in place
+  for (int q = tid; q < npb; q += blockDim.x) {
+    const size_t o = base + q;
+    const int s2 = q / NT, p = q % NT;
+    const int off = s2 * 4 * FS + (p / NN) * N * RS + ((p / N) % N) * RS + p % N;
+    const C ur = fld[off + FS], us = fld[off + 2 * FS], ut = fld[off + 3 * FS];
+    const C g0 = __ldg(gf + o), g1 = __ldg(gf + npts + o), g2 = __ldg(gf + 2 * npts + o),
+            g3 = __ldg(gf + 3 * npts + o), g4 = __ldg(gf + 4 * npts + o),
+            g5 = __ldg(gf + 5 * npts + o);
+    fld[off + FS] = g0 * ur + g1 * us + g2 * ut;
+    fld[off + 2 * FS] = g1 * ur + g3 * us + g4 * ut;
+    fld[off + 3 * FS] = g2 * ur + g4 * us + g5 * ut;
+  }
+  __syncthreads();
+  // P5-P7: (D^T w0 + S^T w1) + S^T w2, accumulated in U's place
+  if (task) {
+    C x[N];
+    const C* src = F1 + a1 * N * RS + a0 * RS;
+#pragma unroll
+    for (int l = 0; l < N; ++l) x[l] = src[l];
+    line_apply<N, RM, false, C>(sDT, x, U + a1 * N * RS + a0 * RS, 1);
+  }
+  __syncthreads();
+  if (task) {
+    C x[N];
+    const C* src = F2 + a1 * N * RS + a0;
+#pragma unroll
+    for (int l = 0; l < N; ++l) x[l] = src[l * RS];
+    line_apply<N, RM, true, C>(sST, x, U + a1 * N * RS + a0, RS);
+  }
+  __syncthreads();
+  double pap = 0.0;
+  if (task) {
+    C x[N];
+    const C* src = F3 + a1 * RS + a0;
+#pragma unroll
+    for (int l = 0; l < N; ++l) x[l] = src[l * N * RS];
+    const C* acc = U + a1 * RS + a0;
+    const size_t eo = base + (size_t)sl * NT + a1 * N + a0;
+#pragma unroll 2
+    for (int l = 0; l < N; ++l) {
+      const size_t o = eo + (size_t)l * NN;
+      C out = acc[l * N * RS] + line_row<N, RM, C>(sST, l, x);
+      C pv = 0;
+      if (HELM || FUSEP) pv = u[o];
+      if (HELM) out += (C)lambda * ((C)__ldg(bj + o) * pv);
+      au[o] = (T)out;
+      if (FUSEP) pap += (double)pv * (double)out;
+    }
   }
   return pap;
 }

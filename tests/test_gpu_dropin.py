@@ -24,13 +24,14 @@ and three Helmholtz solves (Jacobi CG), all to the reference's absolute
 Bars (each stated where it is asserted):
   * every solve of every step: the same number of iterations, or one apart
     only where the residual at the deciding iteration lies within a factor 2
-    of eps (conftest.same_stop); residual histories as conftest.check_history
-    (1e-9 of the first residual while above 1e-4 of it, 1e-7 below, and
-    an absolute floor of 1e-13: the fields are of order one, and the
-    pressure solves start from an extrapolated guess whose residual is
-    already small, so their differences sit at the rounding of the data);
-  * fields u, v, w, p after 20 steps: FIELD_REL relative to the largest
-    entry while every solve stopped at the same iteration;
+    of eps (conftest.same_stop); Helmholtz (Jacobi CG) residual histories as
+    conftest.check_history, pressure (FCG + p-multigrid) histories within
+    POISSON_HIST_REL of the first residual; both within eps itself where
+    the residuals approach the stop (the late steps' pressure solves start
+    from an extrapolated guess a few eps above the stop);
+  * fields after 20 steps: the velocity relative to its largest component,
+    the pressure relative to its largest entry, FIELD_REL when every solve
+    stopped at the same iteration, FIELD_STOP_REL otherwise;
   * the individual bound functions on the reference's own set-up: DSS
     bitwise, operators, inner product and convection 1e-13, the particle
     walk bitwise (on inputs where the reference reseeds no particle: a
@@ -53,6 +54,14 @@ pytestmark = [pytest.mark.gpu,
 STEPS = 20
 DT, VISC = 1e-3, 1.0 / 1600.0
 FIELD_REL = 1e-11
+# fields after a run in which some solve stopped one iteration apart (near
+# eps): the runs are one correction of the size of the stop tolerance apart
+FIELD_STOP_REL = 1e-9
+# FCG + p-multigrid histories: the reference's own history moves by up to
+# 2.2e-4 of its first residual between two machines or against the oracle
+# (measured at C2 in tests/test_gpu_configs.py: the V-cycle's inner solves
+# stop on the absolute eps, so rounding changes their iteration counts)
+POISSON_HIST_REL = 5e-4
 
 
 def _c1_run(gpu, steps, path):
@@ -179,11 +188,19 @@ def test_c1_navier_stokes_steps_through_the_binding(c1):
             k = min(lc, lg) - 1
             for h in (hc[k], hg[k]):
                 assert 0.5 * EPS <= h <= 2 * EPS, (s, kv, hc, hg)
-        # the fields are of order one and every solve stops at 1e-10
-        # absolute: deviations below 1e-13 are rounding of the data
-        check_history(hg, hc, floor=1e-13)
-    if same:
-        assert max(devs) <= FIELD_REL, devs
+        d = history_deviation(hg, hc)
+        if kv[0] == 0:
+            # FCG + p-multigrid: within POISSON_HIST_REL of the first
+            # residual, or within eps itself once the residuals approach it
+            assert np.all(d <= max(POISSON_HIST_REL * hc[0], EPS)), (s, kv, d / hc[0])
+        else:
+            # Jacobi CG: as conftest.check_history, within eps near the stop
+            check_history(hg, hc, floor=EPS)
+    vscale = max(float(np.max(np.abs(cpu[f"f{w}"]))) for w in range(3))
+    vdev = max(float(np.max(np.abs(cpu[f"f{w}"] - gpu[f"f{w}"]))) for w in range(3)) / vscale
+    pdev = devs[3]
+    assert vdev <= (FIELD_REL if same else FIELD_STOP_REL), (vdev, same)
+    assert pdev <= (FIELD_REL if same else FIELD_STOP_REL), (pdev, same)
 
 
 @pytest.fixture(scope="module")

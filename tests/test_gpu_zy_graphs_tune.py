@@ -76,7 +76,9 @@ def test_helmholtz_while_graph_is_bitwise_direct(gpu_ctx_factory):
     mesh, n = channel_mesh((4, 3, 3), seed=7), 7
     orc = O.Oracle(mesh, n)
     f = rhs(orc, n)
-    ctx = gpu_ctx_factory(mesh, n)
+    # lambda = (11/6) / (dt visc) = 11/6: a stiffness-dominated operator, so
+    # the Jacobi CG runs many iterations
+    ctx = gpu_ctx_factory(mesh, n, dt=1.0, visc=1.0)
     ctx.set_graphs(False)
     u_d, info_d = ctx.solve_helmholtz_cg(O.X_VELOCITY, f, np.zeros_like(f))
     assert info_d["iterations"] > 8
