@@ -452,155 +452,6 @@ __global__ void __launch_bounds__(256) k_level_cg(LevelCgArgs<T> a) {
   }
 }
 
-// ---------------------------------------------------------------------------
-// Post-smoother of the mixed-precision V-cycle at any level but the
-// coarsest: the Jacobi CG of cg_solve's FP32 form (pressure, no mask) as one
-// cooperative launch.  Per iteration two grid barriers instead of two
-// kernel launches: (1) the line-form operator forms the direction p and
-// Ap, with the block partials of p . (A p) (for a continuous p it equals
-// the weighted (p w) . DSS(A p)), and on the first iteration of (r w) . p;
-// (2) after alpha = rdz / pap, the reference-ordered DSS gather of A p
-// feeds the update x += alpha p, r -= alpha ap, z = M^-1 r with the partials
-// of (r w).z, (r w).r, w.z, w.r, from which every block takes the same
-// nullspace constant, beta, residual and stop decision.  The residual
-// r = f - DSS(A x) and z = M^-1 r open the solve (three barriers).  FP32
-// storage and operator arithmetic; sums, scalars and the DSS accumulation
-// in FP64.  The loop is bounded by max_iter.
-// ---------------------------------------------------------------------------
-struct SmoothArgs {
-  int nel = 0;
-  size_t npts = 0;
-  const float* f = nullptr;
-  float* x = nullptr;
-  float *r = nullptr, *z = nullptr, *p = nullptr, *aploc = nullptr;
-  const float* gf = nullptr;      // 6 x npts, natural point order
-  const double* D = nullptr;
-  const float* dinv = nullptr;
-  const uint8_t* mult = nullptr;
-  const int2* pairs = nullptr;
-  double nunique = 1.0;
-  double eps = 0.0;
-  int max_iter = 0;
-  double* partA = nullptr;        // >= 4 * gridDim.x
-  double* partB = nullptr;        // >= 4 * gridDim.x
-};
-
-template <int N>
-__global__ void __launch_bounds__(AxLine<N>::THREADS) k_smooth_fused(SmoothArgs a) {
-  using L = AxLine<N>;
-  using T = float;
-  constexpr int NT = N * N * N, EPB = L::EPB;
-  cg::grid_group grid = cg::this_grid();
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* sD = reinterpret_cast<T*>(smem_raw);
-  __shared__ double sred[4 * 32];
-  __shared__ double sbc[4];
-  axl_load_mats<N, T, false>(sD, a.D, a.D);   // visible after axl_group's first barrier
-  const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const size_t nthr = (size_t)gridDim.x * blockDim.x;
-  const int G = gridDim.x;
-  const int ngroups = (a.nel + EPB - 1) / EPB;
-  // aploc = A_e in over every element group (block-uniform loop)
-  auto op_pass = [&](T* in, bool fusep, bool first, double beta, double cz, double* pap,
-                     double* rdz) {
-    for (int grp = blockIdx.x; grp < ngroups; grp += G) {
-      const int e0 = grp * EPB;
-      const int ne = min(EPB, a.nel - e0);
-      if (fusep)
-        *pap += axl_group<N, T, false, true>(e0, ne, in, a.aploc, a.gf, a.npts, nullptr, 0.0,
-                                             a.z, beta, cz, nullptr, first, sD,
-                                             first ? a.r : nullptr, a.mult, rdz);
-      else
-        axl_group<N, T, false, false>(e0, ne, in, a.aploc, a.gf, a.npts, nullptr, 0.0,
-                                      nullptr, 0.0, 0.0, nullptr, false, sD, nullptr, nullptr,
-                                      nullptr);
-    }
-  };
-
-  // r = f - DSS(A x), sum w r
-  op_pass(a.x, false, false, 0.0, 0.0, nullptr, nullptr);
-  grid.sync();
-  {
-    double v[1] = {0.0};
-    for (size_t q = tid; q < a.npts; q += nthr) {
-      int cnt;
-      const double acc = dss_gather<N, T>(a.aploc, nullptr, a.pairs + (q / NT) * 26, q,
-                                          (int)(q % NT), cnt);
-      const T rv = (T)((double)a.f[q] + -acc);
-      a.r[q] = rv;
-      v[0] += (double)rv * inv_count(1u + (unsigned)cnt);
-    }
-    block_partials<1>(v, a.partA, sred);
-  }
-  grid.sync();
-  // r -= c (nullspace); z = M^-1 r, sum w z
-  {
-    double t[1];
-    grid_sums<1>(a.partA, G, t, sred, sbc);
-    const double nc = -(t[0] / a.nunique);
-    double v[1] = {0.0};
-    for (size_t q = tid; q < a.npts; q += nthr) {
-      const T rq = (T)((double)a.r[q] + nc);
-      a.r[q] = rq;
-      const T zq = (T)((double)rq * (double)a.dinv[q]);
-      a.z[q] = zq;
-      v[0] += (double)zq * inv_count(a.mult[q]);
-    }
-    block_partials<1>(v, a.partB, sred);
-  }
-  grid.sync();
-  double cz, rdz = 0.0, beta = 0.0;
-  {
-    double t[1];
-    grid_sums<1>(a.partB, G, t, sred, sbc);
-    cz = t[0] / a.nunique;
-  }
-  for (int it = 0; it < a.max_iter; ++it) {
-    const bool first = it == 0;
-    // p = beta p + (z - c) (first: z - c); aploc = A_e p; p . (A p) and,
-    // first, (r w) . p
-    double v2[2] = {0.0, 0.0};
-    op_pass(a.p, true, first, beta, cz, &v2[0], &v2[1]);
-    block_partials<2>(v2, a.partA, sred);
-    grid.sync();
-    double t2[2];
-    grid_sums<2>(a.partA, G, t2, sred, sbc);
-    if (first) rdz = t2[1];
-    const double alpha = rdz / t2[0];
-    // ap = DSS(aploc); x += alpha p; r -= alpha ap; z = M^-1 r
-    {
-      double v[4] = {0.0, 0.0, 0.0, 0.0};
-      for (size_t q = tid; q < a.npts; q += nthr) {
-        int cnt;
-        const double ap = dss_gather<N, T>(a.aploc, nullptr, a.pairs + (q / NT) * 26, q,
-                                           (int)(q % NT), cnt);
-        a.x[q] = (T)((double)a.x[q] + alpha * (double)a.p[q]);
-        const T rq = (T)((double)a.r[q] + -alpha * ap);
-        a.r[q] = rq;
-        const T zq = (T)((double)rq * (double)a.dinv[q]);
-        a.z[q] = zq;
-        const double w = inv_count(a.mult[q]);
-        const double rw = (double)rq * w;
-        v[0] += rw * (double)zq;
-        v[1] += rw * (double)rq;
-        v[2] += w * (double)zq;
-        v[3] += rw;
-      }
-      block_partials<4>(v, a.partB, sred);
-    }
-    grid.sync();
-    // nullspace constant, beta, residual, stop (OP_CG_BETA)
-    double s4[4];
-    grid_sums<4>(a.partB, G, s4, sred, sbc);
-    cz = s4[2] / a.nunique;
-    const double rdz_new = s4[0] - cz * s4[3];
-    beta = rdz_new / rdz;
-    rdz = rdz_new;
-    const double err = sqrt(s4[1]);
-    if (!(err > a.eps) || it + 1 >= a.max_iter) break;
-  }
-}
-
 }  // namespace dev
 
 // Blocks per device that a cooperative launch may use, filled on first use.
@@ -713,81 +564,6 @@ static cudaError_t launch_level_cg4(cudaStream_t s, int device, const LevelCgRun
   count_launch();
   return cudaLaunchCooperativeKernel((const void*)dev::k_level_cg<N, T>, dim3(G), dim3(256),
                                      args, smem, s);
-}
-
-static std::atomic<int> g_smooth_grid[SSG_MAXN + 1][kMaxDevices];
-
-template <int N>
-static cudaError_t launch_smooth_fused(cudaStream_t s, int device, const LevelCgRun& L) {
-  using AL = dev::AxLine<N>;
-  dev::SmoothArgs a;
-  a.nel = L.nel;
-  a.npts = (size_t)L.nel * N * N * N;
-  a.f = (const float*)L.f;
-  a.x = (float*)L.x;
-  a.r = (float*)L.r;
-  a.z = (float*)L.z;
-  a.p = (float*)L.p;
-  a.aploc = (float*)L.aploc;
-  a.gf = (const float*)L.gf;
-  a.D = L.D;
-  a.dinv = (const float*)L.dinv;
-  a.mult = L.mult;
-  a.pairs = reinterpret_cast<const int2*>(L.pairs);
-  a.nunique = L.nunique;
-  a.eps = L.eps;
-  a.max_iter = L.max_iter;
-  constexpr size_t smem = (size_t)AL::SMEM * sizeof(float);
-  static bool attr = false;
-  if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(dev::k_smooth_fused<N>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    attr = true;
-  }
-  if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
-  int cap = 0;
-  {
-    std::atomic<int>& slot = g_smooth_grid[N][device];
-    int c = slot.load(std::memory_order_relaxed);
-    if (c == 0) {
-      int per_sm = 0, nsm = 0;
-      cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-          &per_sm, dev::k_smooth_fused<N>, AL::THREADS, smem);
-      if (e != cudaSuccess) return e;
-      e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
-      if (e != cudaSuccess) return e;
-      c = per_sm * nsm;
-      if (c < 1) return cudaErrorCooperativeLaunchTooLarge;
-      slot.store(c, std::memory_order_relaxed);
-    }
-    cap = c;
-  }
-  // element groups spread evenly: each block takes the same number of groups
-  const int groups = (L.nel + AL::EPB - 1) / AL::EPB;
-  const int rounds = (groups + cap - 1) / cap;
-  int G = (groups + rounds - 1) / rounds;
-  if ((size_t)8 * G > L.part_cap) G = (int)(L.part_cap / 8);
-  if (G < 1) return cudaErrorInvalidValue;
-  a.partA = L.part;
-  a.partB = L.part + 4 * (size_t)G;
-  void* args[] = {&a};
-  count_launch();
-  return cudaLaunchCooperativeKernel((const void*)dev::k_smooth_fused<N>, dim3(G),
-                                     dim3(AL::THREADS), args, smem, s);
-}
-
-cudaError_t run_smooth_fused(cudaStream_t s, int device, int n, const LevelCgRun& L) {
-  switch (n) {
-#define SSG_SMF(NV) \
-  case NV:          \
-    return launch_smooth_fused<NV>(s, device, L);
-    SSG_SMF(3) SSG_SMF(4) SSG_SMF(5) SSG_SMF(6) SSG_SMF(7) SSG_SMF(8) SSG_SMF(9) SSG_SMF(10)
-    SSG_SMF(11) SSG_SMF(12)
-#undef SSG_SMF
-    default:
-      return cudaErrorInvalidValue;
-  }
 }
 
 cudaError_t run_level_cg(cudaStream_t s, int device, int n, bool fp32, const LevelCgRun& L) {

@@ -623,6 +623,15 @@ __device__ __forceinline__ double axl_group(int e0, int ne, T* __restrict__ u,
   const int tid = threadIdx.x;
   const size_t base = (size_t)e0 * NT;
   const int npb = ne > 0 ? ne * NT : 0;   // points of this group
+  // the group's six metric chunks into L2 now: they are read only after
+  // the three derivative passes (a hint, no buffer; 16-byte aligned chunks
+  // of a multiple of 16 bytes only)
+  if (tid < 6 && npb > 0) {
+    const T* chunk = gf + (size_t)tid * npts + base;
+    const unsigned bytes = (unsigned)(npb * sizeof(T));
+    if (((reinterpret_cast<uintptr_t>(chunk) | bytes) & 15u) == 0)
+      bulk_prefetch_l2(chunk, bytes);
+  }
   __syncthreads();   // the previous group's last pass has read the fields
   // P0: stage the field (forming p first when fused), coalesced
   for (int q = tid; q < npb; q += blockDim.x) {

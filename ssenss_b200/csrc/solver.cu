@@ -509,31 +509,6 @@ static ssg_status mg_recurse(ssg_context* c, int L, void* f, void* x, double eps
   // cooperative form (the unfused arithmetic, ap stored before the update)
   // took the outer FCG 16 iterations instead of 11 on the C2 solve.
 
-  if (fp32) {
-    // mixed precision: the FP32 Jacobi CG with the fused alpha in one
-    // cooperative launch per level (run_smooth_fused)
-    LevelCgRun R;
-    R.nel = c->nel;
-    R.f = f;
-    R.x = x;
-    R.r = W.r;
-    R.z = W.z;
-    R.p = W.p;
-    R.aploc = W.aploc;
-    R.ap = W.ap;
-    R.gf = F.gf32;
-    R.D = F.D;
-    R.dinv = F.dinv_p32;
-    R.mult = F.mult;
-    R.pairs = c->d_pairs;
-    R.nunique = F.nunique;
-    R.eps = eps;
-    R.max_iter = 15;
-    R.part = c->d_part;
-    R.part_cap = c->part_cap;
-    SSG_CUDA(c, run_smooth_fused(s, c->device, F.n, R));
-    return SSG_OK;
-  }
   if (F.n == 4 && !fp32) {
     LevelCgRun R;
     R.nel = c->nel;

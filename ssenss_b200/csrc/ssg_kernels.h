@@ -181,10 +181,6 @@ struct LevelCgRun {
   size_t part_cap = 0;
 };
 cudaError_t run_level_cg(cudaStream_t s, int device, int n, bool fp32, const LevelCgRun& L);
-// the mixed-precision V-cycle's post-smoother at an n-point level (FP32
-// storage and operator, pressure): its whole Jacobi CG in one cooperative
-// launch with the fused alpha (coarse.cu); gf and dinv FP32
-cudaError_t run_smooth_fused(cudaStream_t s, int device, int n, const LevelCgRun& L);
 // whole CG-Jacobi solve of an n = 2 level in one cooperative launch
 // (coarse.cu); it stops at sqrt((r.r)_w) <= eps, or <= rel times the first
 // residual when rel > 0

@@ -25,10 +25,9 @@ Bars (each stated where it is asserted):
   * every solve of every step: the same number of iterations, or one apart
     only where the residual at the deciding iteration lies within a factor 2
     of eps (conftest.same_stop); Helmholtz (Jacobi CG) residual histories as
-    conftest.check_history, pressure (FCG + p-multigrid) histories within
-    POISSON_HIST_REL of the first residual; both within eps itself where
-    the residuals approach the stop (the late steps' pressure solves start
-    from an extrapolated guess a few eps above the stop);
+    conftest.check_history (with eps itself as the floor), pressure (FCG +
+    p-multigrid) histories within POISSON_HIST_REL of the first residual plus
+    POISSON_HIST_EPS times eps (reasons where they are defined);
   * fields after 20 steps: the velocity relative to its largest component,
     the pressure relative to its largest entry, FIELD_REL when every solve
     stopped at the same iteration, FIELD_STOP_REL otherwise;
@@ -62,6 +61,13 @@ FIELD_STOP_REL = 1e-9
 # (measured at C2 in tests/test_gpu_configs.py: the V-cycle's inner solves
 # stop on the absolute eps, so rounding changes their iteration counts)
 POISSON_HIST_REL = 5e-4
+# ... and, on top of it, a few eps: the V-cycle's inner CG solves stop on
+# the absolute eps, so the preconditioner's own inexactness is of the order
+# of eps whatever the residual it is given; the pressure solves of these
+# steps start from an extrapolated guess only a few orders above eps, where
+# that term dominates (measured: 1.4e-3 of the first residual in the
+# pressure solve of step 4; the test prints the largest deviations)
+POISSON_HIST_EPS = 10.0
 
 
 def _c1_run(gpu, steps, path):
@@ -178,6 +184,9 @@ def test_c1_navier_stokes_steps_through_the_binding(c1):
         devs.append(float(np.max(np.abs(a - b))) / scale)
     same = all(r[2] == r[3] for r in rows)
     worst = max(rows, key=lambda r: r[6] / r[4][0])
+    for r in sorted(rows, key=lambda r: -r[6])[:5]:
+        print(f"  step {r[0]} solve {tuple(int(v) for v in r[1])}: iterations {r[2]}/{r[3]}, "
+              f"first residual {r[4][0]:.3e}, largest deviation {r[6]:.3e}")
     print(f"C1 drop-in: {len(rows)} solves, every stop equal: {same}, largest history "
           f"deviation {worst[6]:.2e} absolute ({worst[6] / worst[4][0]:.2e} of h0, step "
           f"{worst[0]}, solve {worst[1]}), fields u v w p after {STEPS} steps "
@@ -191,8 +200,9 @@ def test_c1_navier_stokes_steps_through_the_binding(c1):
         d = history_deviation(hg, hc)
         if kv[0] == 0:
             # FCG + p-multigrid: within POISSON_HIST_REL of the first
-            # residual, or within eps itself once the residuals approach it
-            assert np.all(d <= max(POISSON_HIST_REL * hc[0], EPS)), (s, kv, d / hc[0])
+            # residual plus POISSON_HIST_EPS times eps
+            bound = POISSON_HIST_REL * hc[0] + POISSON_HIST_EPS * EPS
+            assert np.all(d <= bound), (s, kv, d / hc[0], hc)
         else:
             # Jacobi CG: as conftest.check_history, within eps near the stop
             check_history(hg, hc, floor=EPS)
