@@ -70,8 +70,12 @@ def parse():
                     help="Poisson arrival rate of the serving stream (requests/s)")
     ap.add_argument("--serve-slots", type=int, default=8,
                     help="requests in flight at once in the serving loop")
+    ap.add_argument("--serve-open-only", action="store_true",
+                    help="serving: only the open-loop runs (served and plain), no "
+                         "closed-loop throughput runs")
     ap.add_argument("--sections", default="all",
-                    choices=["all", "fp64", "mixed", "op", "conv", "serve", "extra", "channel"],
+                    choices=["all", "fp64", "mixed", "op", "conv", "serve", "extra", "channel",
+                             "particles"],
                     help="fp64: only the FP64 solves; op / conv: only the operator / "
                          "convection launches (for profiler captures)")
     return ap.parse_args()
@@ -392,8 +396,12 @@ def run_serving(args, device):
     wsrv.close()
     served, st_s, wall_s, bad_s = run(args.serve_slots, "mixed", True)
     plain, st_p, wall_p, bad_p = run(1, "fp64", True)
-    _, st_sc, wall_sc, _ = run(args.serve_slots, "mixed", False)
-    _, st_pc, wall_pc, _ = run(1, "fp64", False)
+    closed = None
+    if not args.serve_open_only:
+        _, st_sc, wall_sc, _ = run(args.serve_slots, "mixed", False)
+        _, st_pc, wall_pc, _ = run(1, "fp64", False)
+        closed = {"served_mixed": st_sc["completed"] / wall_sc,
+                  "plain_fp64_one_at_a_time": st_pc["completed"] / wall_pc}
     diff = 0.0
     for (u_s, st1, _), (u_p, st2, _), (_, _, _, lam, _) in zip(served, plain, stream):
         if u_s is None or u_p is None or st1 != "SSG_OK" or st2 != "SSG_OK":
@@ -418,9 +426,7 @@ def run_serving(args, device):
                      f"{args.serve_rate}/s, stop sqrt((r.r)_w) <= {EPS}, HBM budget 150 GB"),
         "served_mixed": pick(st_s, wall_s),
         "plain_fp64_one_at_a_time": pick(st_p, wall_p),
-        "closed_loop_solves_per_s": {"served_mixed": st_sc["completed"] / wall_sc,
-                                     "plain_fp64_one_at_a_time":
-                                         st_pc["completed"] / wall_pc},
+        "closed_loop_solves_per_s": closed,
         "failed": len(bad_s) + len(bad_p),
         "failed_statuses": sorted(set(bad_s + bad_p)),
         "max_rel_diff_mixed_vs_fp64": diff,
@@ -656,6 +662,13 @@ def run_ours(args):
         ctx.close()
         if pg is not None:
             pg.destroy_process_group()
+        return 0
+
+    if args.sections == "particles":
+        res = run_particles(args, ctx, mesh, n, local, nsteps=max(1, args.steps))
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "sections": "particles", "particles": res}))
+        ctx.close()
         return 0
 
     if args.sections == "channel":

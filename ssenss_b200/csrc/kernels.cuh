@@ -526,11 +526,13 @@ __device__ __forceinline__ double ax_element(int e, bool active, int i, int j, c
 // smoother in coarse.cu): each thread contracts one whole line of an
 // element (N points along i, j or k) held in registers, so a matrix row is
 // read once per line instead of a shared row and a shared field value per
-// multiply-add.  Per element: the field is staged in shared memory; three
-// passes (lines along i, j, k) give the r-, s- and t-derivatives; a
-// point-wise pass applies the six metric terms; three transposed passes sum
-// D^T w0 + S^T w1 + S^T w2 (D for Poisson) in the order (acc + acs) + act of
-// ax_element.  The matrices sit in shared memory and every lane of a warp
+// multiply-add.  Per element: the field is staged in shared memory; lines
+// along i and j give the r- and s-derivatives; the lines along k take the
+// t-derivative in registers, apply the six metric terms at their points and
+// add the t-transposed contribution S^T w2 from registers; lines along j and
+// then i sum S^T w1 and D^T w0 (D for Poisson) and write the output in the
+// order (acc + acs) + act of ax_element: four block barriers per element
+// group.  The matrices sit in shared memory and every lane of a warp
 // reads the same entry (a broadcast), two entries per paired load.  EPB
 // elements per group fill about 256 threads.  The arithmetic runs in the
 // storage type T: FP64 for the solves, FP32 in the mixed-precision V-cycle
@@ -658,7 +660,7 @@ __device__ __forceinline__ double axl_group(int e0, int ne, T* __restrict__ u,
   C* F1 = U + FS;
   C* F2 = F1 + FS;
   C* F3 = F2 + FS;
-  // P1-P3: derivatives along i (r, with S for Helmholtz), j (s), k (t)
+  // P1, P2: derivatives along i (r, with S for Helmholtz) and j (s)
   if (task) {
     C x[N];
     {   // lines (j = a0, k = a1) along i
@@ -673,57 +675,58 @@ __device__ __forceinline__ double axl_group(int e0, int ne, T* __restrict__ u,
       for (int l = 0; l < N; ++l) x[l] = src[l * RS];
       line_apply<N, RM, false, C>(sD, x, F2 + a1 * N * RS + a0, RS);
     }
-    {   // lines (i = a0, j = a1) along k
-      const C* src = U + a1 * RS + a0;
-#pragma unroll
-      for (int l = 0; l < N; ++l) x[l] = src[l * N * RS];
-      line_apply<N, RM, false, C>(sD, x, F3 + a1 * RS + a0, N * RS);
-    }
   }
   __syncthreads();
-  // P4: w = G (ur, us, ut) at every point, in place
-  for (int q = tid; q < npb; q += blockDim.x) {
-    const size_t o = base + q;
-    const int s2 = q / NT, p = q % NT;
-    const int off = s2 * 4 * FS + (p / NN) * N * RS + ((p / N) % N) * RS + p % N;
-    const C ur = fld[off + FS], us = fld[off + 2 * FS], ut = fld[off + 3 * FS];
-    const C g0 = __ldg(gf + o), g1 = __ldg(gf + npts + o), g2 = __ldg(gf + 2 * npts + o),
-            g3 = __ldg(gf + 3 * npts + o), g4 = __ldg(gf + 4 * npts + o),
-            g5 = __ldg(gf + 5 * npts + o);
-    fld[off + FS] = g0 * ur + g1 * us + g2 * ut;
-    fld[off + 2 * FS] = g1 * ur + g3 * us + g4 * ut;
-    fld[off + 3 * FS] = g2 * ur + g4 * us + g5 * ut;
-  }
-  __syncthreads();
-  // P5-P7: (D^T w0 + S^T w1) + S^T w2, accumulated in U's place
+  // P3: lines (i = a0, j = a1) along k: the t-derivative in registers, the
+  // metric product at each point of the line (w0, w1 in place of ur, us;
+  // w2 kept in registers), then the t-transposed contribution S^T w2 of the
+  // line into F3
   if (task) {
-    C x[N];
-    const C* src = F1 + a1 * N * RS + a0 * RS;
+    C x[N], w2[N];
+    const C* src = U + a1 * RS + a0;
 #pragma unroll
-    for (int l = 0; l < N; ++l) x[l] = src[l];
-    line_apply<N, RM, false, C>(sDT, x, U + a1 * N * RS + a0 * RS, 1);
+    for (int l = 0; l < N; ++l) x[l] = src[l * N * RS];
+    const size_t eo = base + (size_t)sl * NT + a1 * N + a0;
+#pragma unroll 2
+    for (int k = 0; k < N; ++k) {
+      const C ut = line_row<N, RM, C>(sD, k, x);
+      const int q = k * N * RS + a1 * RS + a0;
+      const size_t o = eo + (size_t)k * NN;
+      const C ur = F1[q], us = F2[q];
+      const C g0 = __ldg(gf + o), g1 = __ldg(gf + npts + o), g2 = __ldg(gf + 2 * npts + o),
+              g3 = __ldg(gf + 3 * npts + o), g4 = __ldg(gf + 4 * npts + o),
+              g5 = __ldg(gf + 5 * npts + o);
+      F1[q] = g0 * ur + g1 * us + g2 * ut;
+      F2[q] = g1 * ur + g3 * us + g4 * ut;
+      w2[k] = g2 * ur + g4 * us + g5 * ut;
+    }
+    line_apply<N, RM, false, C>(sST, w2, F3 + a1 * RS + a0, N * RS);
   }
   __syncthreads();
+  // P4: s-transposed S^T w1 along j into U's place
   if (task) {
     C x[N];
     const C* src = F2 + a1 * N * RS + a0;
 #pragma unroll
     for (int l = 0; l < N; ++l) x[l] = src[l * RS];
-    line_apply<N, RM, true, C>(sST, x, U + a1 * N * RS + a0, RS);
+    line_apply<N, RM, false, C>(sST, x, U + a1 * N * RS + a0, RS);
   }
   __syncthreads();
+  // P5: r-transposed D^T w0 along i, and the output (acc + acs) + act of
+  // each point of the line (rows of the element: coalesced stores)
   double pap = 0.0;
   if (task) {
     C x[N];
-    const C* src = F3 + a1 * RS + a0;
+    const C* src = F1 + a1 * N * RS + a0 * RS;
 #pragma unroll
-    for (int l = 0; l < N; ++l) x[l] = src[l * N * RS];
-    const C* acc = U + a1 * RS + a0;
-    const size_t eo = base + (size_t)sl * NT + a1 * N + a0;
+    for (int l = 0; l < N; ++l) x[l] = src[l];
+    const C* acs = U + a1 * N * RS + a0 * RS;
+    const C* act = F3 + a1 * N * RS + a0 * RS;
+    const size_t eo = base + (size_t)sl * NT + a1 * NN + a0 * N;
 #pragma unroll 2
     for (int l = 0; l < N; ++l) {
-      const size_t o = eo + (size_t)l * NN;
-      C out = acc[l * N * RS] + line_row<N, RM, C>(sST, l, x);
+      const size_t o = eo + l;
+      C out = (line_row<N, RM, C>(sDT, l, x) + acs[l]) + act[l];
       C pv = 0;
       if (HELM || FUSEP) pv = u[o];
       if (HELM) out += (C)lambda * ((C)__ldg(bj + o) * pv);

@@ -86,6 +86,27 @@ def test_level_data_matches_oracle(name, gpu_ctx_factory):
 
 
 @pytest.mark.parametrize("name", list(CASES))
+def test_inverse_mass_matches_oracle(name, gpu_ctx_factory):
+    """ssg_inverse_mass (global_inverse_mass_matrix_operator,
+    src/poisson.c:77-87): u times the stored inverse assembled mass, one
+    rounding per point -- bit for bit the product with the context's own
+    inverse mass, and within 1e-14 of the oracle's; host and device
+    operands."""
+    import torch
+    mesh, n, orc, ctx = setup_case(name, gpu_ctx_factory)
+    rng = np.random.default_rng(4)
+    u = rng.standard_normal((mesh.nel, n, n, n))
+    own = u * ctx.level_data(0, 11)
+    got = ctx.inverse_mass(u.copy())
+    assert np.array_equal(got, own)
+    assert rel(got, u * orc.precon(0, 4)) < 1e-14
+    ud = torch.from_numpy(u).cuda()
+    ctx.inverse_mass(ud)
+    torch.cuda.synchronize()
+    assert np.array_equal(ud.cpu().numpy(), own)
+
+
+@pytest.mark.parametrize("name", list(CASES))
 def test_dss_bitwise(name, gpu_ctx_factory):
     mesh, n, orc, ctx = setup_case(name, gpu_ctx_factory)
     rng = np.random.default_rng(1)
