@@ -775,7 +775,9 @@ def run_ours(args):
         _, info = ctx.solve_poisson_cg(fh, uh, eps=EPS, history=False)
         return info
 
-    ms_e2e, infos_e = timed(solve_host, max(3, args.steps // 2), 1)
+    # two untimed solves: the first runs directly, the second captures the FCG
+    # iteration graphs for these host-staged operands
+    ms_e2e, infos_e = timed(solve_host, max(3, args.steps // 2), 2)
     ke = max(3, args.steps // 2)
     ms_e2e = max_over_ranks(pg, ms_e2e, dev)
     e2e = sum_over_ranks(pg, float(udofs) * sum(i["iterations"] for i in infos_e), dev) / \

@@ -529,10 +529,10 @@ __device__ __forceinline__ double ax_element(int e, bool active, int i, int j, c
 // multiply-add.  Per element: the field is staged in shared memory; lines
 // along i and j give the r- and s-derivatives; the lines along k take the
 // t-derivative in registers, apply the six metric terms at their points and
-// add the t-transposed contribution S^T w2 from registers; lines along j and
-// then i sum S^T w1 and D^T w0 (D for Poisson) and write the output in the
-// order (acc + acs) + act of ax_element: four block barriers per element
-// group.  The matrices sit in shared memory and every lane of a warp
+// form the t-transposed contribution S^T w2 in registers; lines along i and
+// j then turn w0 and w1 into D^T w0 and S^T w1 (D for Poisson) in place, and
+// the k-lines write the output (acc + acs) + act, the order of ax_element:
+// three staged fields and four block barriers per element group.  The matrices sit in shared memory and every lane of a warp
 // reads the same entry (a broadcast), two entries per paired load.  EPB
 // elements per group fill about 256 threads.  The arithmetic runs in the
 // storage type T: FP64 for the solves, FP32 in the mixed-precision V-cycle
@@ -547,7 +547,7 @@ struct AxLine {
   static constexpr int RS = N + ((2 - N % 4) + 4) % 4;   // field rows: 2 mod 4 values
   static constexpr int FS = N * N * RS;                  // one staged field
   static constexpr int MATS = 4 * N * RM;
-  static constexpr int SMEM = MATS + EPB * 4 * FS;       // values of type T
+  static constexpr int SMEM = MATS + EPB * 3 * FS;       // values of type T
 };
 
 // sum_l A[o][l] x[l] (A rows of RM values, pair-aligned), in l order; every
@@ -621,7 +621,7 @@ __device__ __forceinline__ double axl_group(int e0, int ne, T* __restrict__ u,
   const C* sDT = sD + N * RM;
   const C* sS = sDT + N * RM;
   const C* sST = sS + N * RM;
-  C* fld = sD + L::MATS;   // per slot: U/O, F1, F2, F3 (FS values each)
+  C* fld = sD + L::MATS;   // per slot: U, F1, F2 (FS values each)
   const int tid = threadIdx.x;
   const size_t base = (size_t)e0 * NT;
   const int npb = ne > 0 ? ne * NT : 0;   // points of this group
@@ -651,15 +651,14 @@ __device__ __forceinline__ double axl_group(int e0, int ne, T* __restrict__ u,
       v = (C)u[o];
     }
     const int sl = q / NT, p = q % NT;
-    fld[sl * 4 * FS + (p / NN) * N * RS + ((p / N) % N) * RS + p % N] = v;
+    fld[sl * 3 * FS + (p / NN) * N * RS + ((p / N) % N) * RS + p % N] = v;
   }
   __syncthreads();
   const bool task = tid < ne * NN;
   const int sl = tid / NN, a0 = (tid % NN) % N, a1 = (tid % NN) / N;
-  C* U = fld + sl * 4 * FS;
+  C* U = fld + sl * 3 * FS;
   C* F1 = U + FS;
   C* F2 = F1 + FS;
-  C* F3 = F2 + FS;
   // P1, P2: derivatives along i (r, with S for Helmholtz) and j (s)
   if (task) {
     C x[N];
@@ -679,14 +678,15 @@ __device__ __forceinline__ double axl_group(int e0, int ne, T* __restrict__ u,
   __syncthreads();
   // P3: lines (i = a0, j = a1) along k: the t-derivative in registers, the
   // metric product at each point of the line (w0, w1 in place of ur, us;
-  // w2 kept in registers), then the t-transposed contribution S^T w2 of the
-  // line into F3
+  // w2 in registers), then the t-transposed contribution act = S^T w2 of
+  // the line, kept in registers for the output pass
+  C act[N];
+  const size_t eo = base + (size_t)sl * NT + a1 * N + a0;
   if (task) {
     C x[N], w2[N];
     const C* src = U + a1 * RS + a0;
 #pragma unroll
     for (int l = 0; l < N; ++l) x[l] = src[l * N * RS];
-    const size_t eo = base + (size_t)sl * NT + a1 * N + a0;
 #pragma unroll 2
     for (int k = 0; k < N; ++k) {
       const C ut = line_row<N, RM, C>(sD, k, x);
@@ -700,33 +700,38 @@ __device__ __forceinline__ double axl_group(int e0, int ne, T* __restrict__ u,
       F2[q] = g1 * ur + g3 * us + g4 * ut;
       w2[k] = g2 * ur + g4 * us + g5 * ut;
     }
-    line_apply<N, RM, false, C>(sST, w2, F3 + a1 * RS + a0, N * RS);
+#pragma unroll
+    for (int k = 0; k < N; ++k) act[k] = line_row<N, RM, C>(sST, k, w2);
   }
   __syncthreads();
-  // P4: s-transposed S^T w1 along j into U's place
+  // P4: the r-transposed D^T w0 along i and the s-transposed S^T w1 along
+  // j, each written over its own input line (a thread reads the whole line
+  // before it writes it)
   if (task) {
     C x[N];
-    const C* src = F2 + a1 * N * RS + a0;
+    {   // lines (j = a0, k = a1) along i
+      C* line = F1 + a1 * N * RS + a0 * RS;
 #pragma unroll
-    for (int l = 0; l < N; ++l) x[l] = src[l * RS];
-    line_apply<N, RM, false, C>(sST, x, U + a1 * N * RS + a0, RS);
+      for (int l = 0; l < N; ++l) x[l] = line[l];
+      line_apply<N, RM, false, C>(sDT, x, line, 1);
+    }
+    {   // lines (i = a0, k = a1) along j
+      C* line = F2 + a1 * N * RS + a0;
+#pragma unroll
+      for (int l = 0; l < N; ++l) x[l] = line[l * RS];
+      line_apply<N, RM, false, C>(sST, x, line, RS);
+    }
   }
   __syncthreads();
-  // P5: r-transposed D^T w0 along i, and the output (acc + acs) + act of
-  // each point of the line (rows of the element: coalesced stores)
+  // P5: the output (acc + acs) + act at each point of the k-line (rows of
+  // points across lanes: coalesced stores)
   double pap = 0.0;
   if (task) {
-    C x[N];
-    const C* src = F1 + a1 * N * RS + a0 * RS;
+    const int q0 = a1 * RS + a0;
 #pragma unroll
-    for (int l = 0; l < N; ++l) x[l] = src[l];
-    const C* acs = U + a1 * N * RS + a0 * RS;
-    const C* act = F3 + a1 * N * RS + a0 * RS;
-    const size_t eo = base + (size_t)sl * NT + a1 * NN + a0 * N;
-#pragma unroll 2
-    for (int l = 0; l < N; ++l) {
-      const size_t o = eo + l;
-      C out = (line_row<N, RM, C>(sDT, l, x) + acs[l]) + act[l];
+    for (int k = 0; k < N; ++k) {
+      const size_t o = eo + (size_t)k * NN;
+      C out = (F1[k * N * RS + q0] + F2[k * N * RS + q0]) + act[k];
       C pv = 0;
       if (HELM || FUSEP) pv = u[o];
       if (HELM) out += (C)lambda * ((C)__ldg(bj + o) * pv);

@@ -58,6 +58,7 @@ struct Workspace {
   unsigned long long fcg_kernels[kFcgStates] = {};
   double fcg_eps = -1.0;
   int fcg_precision = -1, fcg_max_iter = -1, fcg_hcap = -1;
+  const double* fcg_u = nullptr;   // the solution vector the graphs update
   bool fcg_failed = false;
   int fcg_warm = 0;          // solves run directly with this configuration
   // the Jacobi CG loop (iterations after the first) as one WHILE graph
@@ -88,6 +89,7 @@ static void drop_iteration_graphs(Workspace* w) {
   w->fcg_failed = false;
   w->fcg_warm = 0;
   w->fcg_eps = -1.0;
+  w->fcg_u = nullptr;
   if (w->cgloop) cudaGraphExecDestroy(w->cgloop);
   w->cgloop = nullptr;
   w->cgloop_failed = false;
@@ -720,13 +722,14 @@ ssg_status fcg_solve(ssg_context* c, const double* f, double* u, double eps, int
   // Iterations past the stop skip their work on the device.  Results are
   // those of the direct launches (the same kernels in the same order).
   const bool same_cfg = w->fcg_eps == eps && w->fcg_precision == c->precision &&
-                        w->fcg_max_iter == max_iter && w->fcg_hcap == hcap;
+                        w->fcg_max_iter == max_iter && w->fcg_hcap == hcap && w->fcg_u == u;
   if (!same_cfg) {
     drop_iteration_graphs(w);
     w->fcg_eps = eps;
     w->fcg_precision = c->precision;
     w->fcg_max_iter = max_iter;
     w->fcg_hcap = hcap;
+    w->fcg_u = u;
   }
   const bool graph_mode = c->graphs && !w->fcg_failed && w->fcg_warm > 0 && !w->vcycle_failed;
   bool graph_mode_used = false;

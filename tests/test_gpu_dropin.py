@@ -26,8 +26,10 @@ Bars (each stated where it is asserted):
     only where the residual at the deciding iteration lies within a factor 2
     of eps (conftest.same_stop); Helmholtz (Jacobi CG) residual histories as
     conftest.check_history (with eps itself as the floor), pressure (FCG +
-    p-multigrid) histories within POISSON_HIST_REL of the first residual plus
-    POISSON_HIST_EPS times eps (reasons where they are defined);
+    p-multigrid) histories: the first residual within POISSON_INPUT_EPS
+    times eps, the rest within POISSON_HIST_REL of the first residual plus
+    POISSON_HIST_EPS times eps plus the first residual's deviation (reasons
+    where they are defined);
   * fields after 20 steps: the velocity relative to its largest component,
     the pressure relative to its largest entry, FIELD_REL when every solve
     stopped at the same iteration, FIELD_STOP_REL otherwise;
@@ -63,11 +65,18 @@ FIELD_STOP_REL = 1e-9
 POISSON_HIST_REL = 5e-4
 # ... and, on top of it, a few eps: the V-cycle's inner CG solves stop on
 # the absolute eps, so the preconditioner's own inexactness is of the order
-# of eps whatever the residual it is given; the pressure solves of these
-# steps start from an extrapolated guess only a few orders above eps, where
-# that term dominates (measured: 1.4e-3 of the first residual in the
-# pressure solve of step 4; the test prints the largest deviations)
+# of eps whatever the residual it is given
 POISSON_HIST_EPS = 10.0
+# The first residual of a pressure solve is b - A x0 with b formed by the
+# reference's host code from the step's velocity and x0 extrapolated from the
+# earlier pressures: both carry the earlier solves' differences (each stops
+# once its residual is below the absolute eps), and with a first residual
+# only a few orders above eps they show in it directly (measured: 3.9e-9,
+# 39 eps, 1.4e-3 of the first residual in the pressure solve of step 4; the
+# test prints the largest deviations). The first entry is held to
+# POISSON_INPUT_EPS times eps; every later entry to the bounds above plus
+# that first deviation, which the solve carries along as a changed input.
+POISSON_INPUT_EPS = 100.0
 
 
 def _c1_run(gpu, steps, path):
@@ -199,10 +208,13 @@ def test_c1_navier_stokes_steps_through_the_binding(c1):
                 assert 0.5 * EPS <= h <= 2 * EPS, (s, kv, hc, hg)
         d = history_deviation(hg, hc)
         if kv[0] == 0:
-            # FCG + p-multigrid: within POISSON_HIST_REL of the first
-            # residual plus POISSON_HIST_EPS times eps
-            bound = POISSON_HIST_REL * hc[0] + POISSON_HIST_EPS * EPS
-            assert np.all(d <= bound), (s, kv, d / hc[0], hc)
+            # FCG + p-multigrid: the first residual (the step's input)
+            # within POISSON_INPUT_EPS times eps; the rest within
+            # POISSON_HIST_REL of the first residual plus POISSON_HIST_EPS
+            # times eps plus the input's own deviation
+            assert d.size and d[0] <= POISSON_INPUT_EPS * EPS, (s, kv, d, hc)
+            bound = POISSON_HIST_REL * hc[0] + POISSON_HIST_EPS * EPS + d[0]
+            assert np.all(d[1:] <= bound), (s, kv, d / hc[0], hc)
         else:
             # Jacobi CG: as conftest.check_history, within eps near the stop
             check_history(hg, hc, floor=EPS)
