@@ -873,7 +873,12 @@ ssg_status ssg_convection_operator(ssg_context* c, const double* u, const double
   const double *du, *dv;
   double* dout;
   SSG_TRY(stage_in(c, 0, u, np, &du));
-  SSG_TRY(stage_in(c, 1, v, np, &dv));
+  // a field advecting itself is staged once (the self-convection kernel
+  // keys on the two pointers being equal)
+  if (v == u)
+    dv = du;
+  else
+    SSG_TRY(stage_in(c, 1, v, np, &dv));
   SSG_TRY(stage_out(c, 2, udv, np, &dout));
   SSG_CUDA(c, run_convection(c->stream, c->nel, 0, c->nel, c->n, c->m, du, dv, dout,
                              c->conv_w, c->host.conv.D.data(), c->host.jconv.data(),
@@ -892,7 +897,10 @@ ssg_status ssg_convection_elements(ssg_context* c, int first, int count, const d
   const double *du, *dv;
   double* dout;
   SSG_TRY(stage_in(c, 0, u, np, &du));
-  SSG_TRY(stage_in(c, 1, v, np, &dv));
+  if (v == u)
+    dv = du;
+  else
+    SSG_TRY(stage_in(c, 1, v, np, &dv));
   SSG_TRY(stage_out(c, 2, udv, np, &dout));
   SSG_CUDA(c, run_convection(c->stream, count, first, c->nel, c->n, c->m, du, dv, dout,
                              c->conv_w, c->host.conv.D.data(), c->host.jconv.data(),

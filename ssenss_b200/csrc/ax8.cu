@@ -38,13 +38,6 @@
 namespace ssg {
 namespace dev {
 
-__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b, double c0,
-                                     double c1) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%4,%5};\n"
-               : "=d"(d0), "=d"(d1)
-               : "d"(a), "d"(b), "d"(c0), "d"(c1));
-}
-
 template <typename T, bool HELM, bool FUSEP>
 __global__ void __launch_bounds__(128, 4) k_ax8_dmma(int nel, T* __restrict__ u,
                                                      T* __restrict__ au,

@@ -1,0 +1,344 @@
+// Dealiased skew-symmetric convection of a field by itself (the call the
+// time step makes: convection_operator(sel, u, u, conv), src/navier_stokes.c:
+// 59) at n = 8, m = 12, on the FP64 tensor cores.
+//
+// Same arithmetic as k_convection (convection.cu): interpolate the three
+// components to the m-point grid (src/interpolation.c:136-155), per
+// reference direction b add A_b d_b u_c + B_b d_b(u_b u_c) with
+// A_b = sum_a u_a W[a][b], B_b = sum_a W[a][b] (src/convection.c:71-140
+// regrouped), project back with (J^T)^3 (src/interpolation.c:157-176).
+// Every contraction is a small GEMM
+//     Out[row][o] = sum_l F(row, l) M[o][l]
+// over the rows of an element's lines (64 to 144 of them), with M one of J
+// (12 x 8), D (12 x 12) or J^T (8 x 12); each warp takes 8-row tiles and
+// runs them as mma.sync.m8n8k4.f64, with the lane's B fragments of the
+// stage's matrix in registers (read per stage from a lane-ordered table in
+// shared memory that each block fills once).  The advected field is
+// the advecting one, so each element interpolates three fields, not six, and
+// a direction pass forms all three components' derivatives from the same
+// loads: one pass per direction reads the weights W once.
+//
+// Fragment layouts (lane = 4g + t): A (8x4) a = A[g][t]; B (4x8) b = B[t][g];
+// C (8x8) c0 = C[g][2t], c1 = C[g][2t+1].  Output columns o >= 12 of the
+// second column tile have zero B and are dropped.
+//
+// Twelve warps per block, one element per block at a time; shared memory
+// (88.5 KB, two blocks per SM):
+//   U  3 x [k][j][i], rows of 12, planes of 148 (= 4 mod 16 doubles)
+//   SK 3 x the same layout: the sum over the three directions
+// with the interpolation and projection stages in the region not live at
+// the time (T1, P1 in U; T2, P2 in SK).  The pitches make every A-fragment
+// load conflict-free except the j-direction tiles that straddle two planes.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "kernels.cuh"
+#include "ssg_internal.h"
+#include "ssg_kernels.h"
+
+namespace ssg {
+namespace dev {
+
+namespace cdm {
+constexpr int N = 8, M = 12;
+constexpr int NT = N * N * N, MT = M * M * M;
+constexpr int WARPS = 12, THREADS = 32 * WARPS;
+// U / SK: [k][j][i]
+constexpr int RU = M, PU = M * M + 4, FU = M * PU;
+// T1 (stage x out): [k < 8][j < 8][o < 12]
+constexpr int PT1 = N * M + 4, FT1 = N * PT1;
+// T2 (stage y out): [k < 8][o2][o1]
+constexpr int PT2 = PU, FT2 = N * PT2;
+// P1 (projection i out): [k < 12][j < 12][p < 8]
+constexpr int RP1 = N, PP1 = M * N, FP1 = M * PP1;
+// P2 (projection j out): [k < 12][p2 < 8][p1 < 8]
+constexpr int PP2 = N * N + 8, FP2 = M * PP2;
+constexpr int REGION = 3 * FU;
+// lane-ordered B fragments: J (2 column tiles x 2 k-steps), D (2 x 3),
+// J^T (3 k-steps), each [.][lane]
+constexpr int FJ = 0, FD = FJ + 4 * 32, FPJ = FD + 6 * 32, FRAGS = FPJ + 3 * 32;
+constexpr size_t SMEM = (2 * (size_t)REGION + FRAGS) * sizeof(double);
+static_assert(3 * FT1 <= REGION && 3 * FT2 <= REGION && 3 * FP1 <= REGION &&
+                  3 * FP2 <= REGION,
+              "stage scratch fits its region");
+static_assert(FU % 2 == 0 && PU % 2 == 0 && FT1 % 2 == 0 && FP1 % 2 == 0,
+              "16-byte stores land on 16-byte boundaries");
+}  // namespace cdm
+
+struct ConvDmmaMats {
+  double D[cdm::M * cdm::M];   // D[o * M + l]
+  double J[cdm::M * cdm::N];   // J[o * N + p]
+};
+
+__global__ void __launch_bounds__(cdm::THREADS, 2)
+    k_convection_dmma(int nel, int e0, int nel_fac, const double* __restrict__ u,
+                      double* __restrict__ udv, const double* __restrict__ W,
+                      const __grid_constant__ ConvDmmaMats mt) {
+  using namespace cdm;
+  extern __shared__ __align__(16) double smem[];
+  double* const U = smem;
+  double* const SK = smem + REGION;
+  double* const FR = smem + 2 * REGION;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  // B fragments b = Mx[8 ct + g][4 s + t] (zero past the matrix), once per
+  // block: a warp's fragment is then one conflict-free shared load instead
+  // of a constant load whose 32 lanes want 32 different addresses
+  for (int q = threadIdx.x; q < FRAGS; q += THREADS) {
+    const int l = q & 31, gg = l >> 2, tt = l & 3, f = q >> 5;
+    double v;
+    if (f < 4) {                       // J: f = 2 ct + s
+      const int o = 8 * (f >> 1) + gg;
+      v = o < M ? mt.J[o * N + 4 * (f & 1) + tt] : 0.0;
+    } else if (f < 10) {               // D: f - 4 = 3 ct + s
+      const int o = 8 * ((f - 4) / 3) + gg;
+      v = o < M ? mt.D[o * M + 4 * ((f - 4) % 3) + tt] : 0.0;
+    } else {                           // J^T: f - 10 = s
+      v = mt.J[(4 * (f - 10) + tt) * N + gg];
+    }
+    FR[q] = v;
+  }
+  __syncthreads();
+
+  const size_t nptsn = (size_t)nel * NT, wstride = (size_t)nel_fac * MT;
+  for (int e = blockIdx.x; e < nel; e += gridDim.x) {
+    const double* Wb = W + (size_t)(e0 + e) * MT;
+    double bJ[2][2];
+#pragma unroll
+    for (int ct = 0; ct < 2; ++ct)
+#pragma unroll
+      for (int s = 0; s < 2; ++s) bJ[ct][s] = FR[FJ + (2 * ct + s) * 32 + lane];
+    // -- interpolation x: T1[f][k][j][o] = sum_p u[k][j][p] J[o][p]; 3 x 8 tiles
+    for (int job = warp; job < 3 * N; job += WARPS) {
+      const int f = job / N, k = job % N;
+      const double* src = u + f * nptsn + (size_t)e * NT + k * N * N + g * N;
+      double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+#pragma unroll
+      for (int s = 0; s < 2; ++s) {
+        const double a = src[4 * s + t];
+#pragma unroll
+        for (int ct = 0; ct < 2; ++ct) dmma(acc[ct][0], acc[ct][1], a, bJ[ct][s], acc[ct][0], acc[ct][1]);
+      }
+      double* dst = U + f * FT1 + k * PT1 + g * M + 2 * t;
+      *reinterpret_cast<double2*>(dst) = make_double2(acc[0][0], acc[0][1]);
+      if (t < 2) *reinterpret_cast<double2*>(dst + 8) = make_double2(acc[1][0], acc[1][1]);
+    }
+    __syncthreads();
+    // -- interpolation y: T2[f][k][o2][o1] = sum_p T1[k][p][o1] J[o2][p];
+    //    rows (k, o1), 3 x 12 tiles
+    for (int job = warp; job < 3 * 12; job += WARPS) {
+      const int f = job / 12, r = 8 * (job % 12) + g;
+      const int k = r / M, o1 = r % M;
+      const double* src = U + f * FT1 + k * PT1 + o1;
+      double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+#pragma unroll
+      for (int s = 0; s < 2; ++s) {
+        const double a = src[(4 * s + t) * M];
+#pragma unroll
+        for (int ct = 0; ct < 2; ++ct) dmma(acc[ct][0], acc[ct][1], a, bJ[ct][s], acc[ct][0], acc[ct][1]);
+      }
+      double* dst = SK + f * FT2 + k * PT2 + o1;
+#pragma unroll
+      for (int ct = 0; ct < 2; ++ct)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int o2 = 8 * ct + 2 * t + h;
+          if (o2 < M) dst[o2 * M] = acc[ct][h];
+        }
+    }
+    __syncthreads();
+    // -- interpolation z: U[f][o3][o2][o1] = sum_p T2[p][o2][o1] J[o3][p];
+    //    rows (o2, o1), 3 x 18 tiles
+    for (int job = warp; job < 3 * 18; job += WARPS) {
+      const int f = job / 18, r = 8 * (job % 18) + g;
+      const double* src = SK + f * FT2 + r;
+      double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+#pragma unroll
+      for (int s = 0; s < 2; ++s) {
+        const double a = src[(4 * s + t) * PT2];
+#pragma unroll
+        for (int ct = 0; ct < 2; ++ct) dmma(acc[ct][0], acc[ct][1], a, bJ[ct][s], acc[ct][0], acc[ct][1]);
+      }
+      // U's rows of 12 are contiguous within a plane: (o3, o2, o1) -> o3 PU + r
+      double* dst = U + f * FU + r;
+#pragma unroll
+      for (int ct = 0; ct < 2; ++ct)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int o3 = 8 * ct + 2 * t + h;
+          if (o3 < M) dst[o3 * PU] = acc[ct][h];
+        }
+    }
+    __syncthreads();
+
+    // -- the three direction passes: SK_c (=, +=) A_b d_b u_c + B_b d_b(u_b u_c);
+    //    a job is one row tile and one column tile (o < 8 or 8 <= o < 12)
+#pragma unroll 1
+    for (int b = 0; b < 3; ++b) {
+      for (int job = warp; job < 36; job += WARPS) {
+        const int r = 8 * (job >> 1) + g, ct = job & 1;
+        double bD[3];
+#pragma unroll
+        for (int s = 0; s < 3; ++s) bD[s] = FR[FD + (3 * ct + s) * 32 + lane];
+        // shared base and step of this lane's line; unpadded point index base
+        int sb, ss, gb, gs;
+        if (b == 0) {
+          sb = (r / M) * PU + (r % M) * RU; ss = 1;
+          gb = r * M; gs = 1;
+        } else if (b == 1) {
+          sb = (r / M) * PU + (r % M); ss = RU;
+          gb = (r / M) * M * M + (r % M); gs = M;
+        } else {
+          sb = r; ss = PU;
+          gb = r; gs = M * M;
+        }
+        // the lane's output points o0 = 8 ct + 2 t and o0 + 1 (both below 12
+        // or neither): A_b and B_b there first, so that the weights' loads
+        // overlap the tensor-core work.  Along i (b = 0) the two points are
+        // adjacent: one 16-byte access each.
+        const int o0 = 8 * ct + 2 * t;
+        const bool out = o0 < M;
+        double fa[2] = {0.0, 0.0}, fb[2] = {0.0, 0.0};
+        if (out) {
+          const double* wp = Wb + 3 * b * wstride + gb + o0 * gs;
+          double w[3][2], ua[3][2];
+          if (b == 0) {
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+              const double2 wv = __ldg(reinterpret_cast<const double2*>(wp + a * wstride));
+              const double2 uv = *reinterpret_cast<const double2*>(U + a * FU + sb + o0);
+              w[a][0] = wv.x; w[a][1] = wv.y;
+              ua[a][0] = uv.x; ua[a][1] = uv.y;
+            }
+          } else {
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+#pragma unroll
+              for (int h = 0; h < 2; ++h) {
+                w[a][h] = __ldg(wp + a * wstride + h * gs);
+                ua[a][h] = U[a * FU + sb + (o0 + h) * ss];
+              }
+          }
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            double A = w[0][h] * ua[0][h];
+            A = fma(w[1][h], ua[1][h], A);
+            A = fma(w[2][h], ua[2][h], A);
+            fa[h] = A;
+            fb[h] = (w[0][h] + w[1][h]) + w[2][h];
+          }
+        }
+        double dv[3][2], dp[3][2];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) dv[c][0] = dv[c][1] = dp[c][0] = dp[c][1] = 0.0;
+#pragma unroll
+        for (int s = 0; s < 3; ++s) {
+          const int q = sb + (4 * s + t) * ss;
+          const double a0 = U[q], a1 = U[FU + q], a2 = U[2 * FU + q];
+          const double ab = b == 0 ? a0 : (b == 1 ? a1 : a2);
+          const double av[3] = {a0, a1, a2};
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            dmma(dv[c][0], dv[c][1], av[c], bD[s], dv[c][0], dv[c][1]);
+            dmma(dp[c][0], dp[c][1], ab * av[c], bD[s], dp[c][0], dp[c][1]);
+          }
+        }
+        if (out) {
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            double s0 = fa[0] * dv[c][0];
+            s0 = fma(fb[0], dp[c][0], s0);
+            double s1 = fa[1] * dv[c][1];
+            s1 = fma(fb[1], dp[c][1], s1);
+            if (b == 0) {
+              *reinterpret_cast<double2*>(SK + c * FU + sb + o0) = make_double2(s0, s1);
+            } else {
+              double* p = SK + c * FU + sb + o0 * ss;
+              p[0] += s0;
+              p[ss] += s1;
+            }
+          }
+        }
+      }
+      __syncthreads();
+    }
+
+    double bP[3];   // J^T[g][4 s + t]
+#pragma unroll
+    for (int s = 0; s < 3; ++s) bP[s] = FR[FPJ + s * 32 + lane];
+    // -- projection i: P1[c][k][j][p] = sum_o SK[k][j][o] J[o][p]; 3 x 18 tiles
+    for (int job = warp; job < 3 * 18; job += WARPS) {
+      const int c = job / 18, r = 8 * (job % 18) + g;
+      const double* src = SK + c * FU + (r / M) * PU + (r % M) * RU;
+      double acc0 = 0.0, acc1 = 0.0;
+#pragma unroll
+      for (int s = 0; s < 3; ++s) dmma(acc0, acc1, src[4 * s + t], bP[s], acc0, acc1);
+      *reinterpret_cast<double2*>(U + c * FP1 + (r / M) * PP1 + (r % M) * RP1 + 2 * t) =
+          make_double2(acc0, acc1);
+    }
+    __syncthreads();
+    // -- projection j: P2[c][k][p2][p1] = sum_o P1[k][o][p1] J[o][p2];
+    //    rows (k, p1), 3 x 12 tiles
+    for (int job = warp; job < 3 * 12; job += WARPS) {
+      const int c = job / 12, k = job % 12;
+      const double* src = U + c * FP1 + k * PP1 + g;
+      double acc0 = 0.0, acc1 = 0.0;
+#pragma unroll
+      for (int s = 0; s < 3; ++s) dmma(acc0, acc1, src[(4 * s + t) * RP1], bP[s], acc0, acc1);
+      double* dst = SK + c * FP2 + k * PP2 + g;
+      dst[(2 * t) * N] = acc0;
+      dst[(2 * t + 1) * N] = acc1;
+    }
+    __syncthreads();
+    // -- projection k: udv[c][p3][p2][p1] = sum_o P2[o][p2][p1] J[o][p3];
+    //    rows (p2, p1), 3 x 8 tiles
+    for (int job = warp; job < 3 * N; job += WARPS) {
+      const int c = job / N, p2 = job % N;
+      const double* src = SK + c * FP2 + p2 * N + g;
+      double acc0 = 0.0, acc1 = 0.0;
+#pragma unroll
+      for (int s = 0; s < 3; ++s) dmma(acc0, acc1, src[(4 * s + t) * PP2], bP[s], acc0, acc1);
+      double* dst = udv + c * nptsn + (size_t)e * NT + p2 * N + g;
+      dst[(2 * t) * N * N] = acc0;
+      dst[(2 * t + 1) * N * N] = acc1;
+    }
+    // the next element's interpolation x writes U only (P1 was last read
+    // before the barrier above); its stage y writes SK after a barrier
+  }
+}
+
+}  // namespace dev
+
+bool convection_dmma_applies(int n, int m, const double* u, const double* v) {
+  return n == dev::cdm::N && m == dev::cdm::M && u == v;
+}
+
+cudaError_t run_convection_dmma(cudaStream_t s, int nel, int e0, int nel_fac, const double* u,
+                                double* udv, const double* W, const double* Dh,
+                                const double* Jh) {
+  using namespace dev::cdm;
+  if (nel <= 0) return cudaSuccess;
+  dev::ConvDmmaMats mt;
+  for (int q = 0; q < M * M; ++q) mt.D[q] = Dh[q];
+  for (int q = 0; q < M * N; ++q) mt.J[q] = Jh[q];
+  int dev = 0, sms = 0;
+  cudaError_t err = cudaGetDevice(&dev);
+  if (err != cudaSuccess) return err;
+  static bool attr[64] = {};
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  if (!attr[dev]) {
+    err = cudaFuncSetAttribute(dev::k_convection_dmma,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
+    if (err != cudaSuccess) return err;
+    attr[dev] = true;
+  }
+  err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (err != cudaSuccess) return err;
+  const int grid = nel < 2 * sms ? nel : 2 * sms;
+  count_launch();
+  dev::k_convection_dmma<<<grid, THREADS, SMEM, s>>>(nel, e0, nel_fac, u, udv, W, mt);
+  return cudaGetLastError();
+}
+
+}  // namespace ssg

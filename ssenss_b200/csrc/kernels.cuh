@@ -351,6 +351,15 @@ __device__ __forceinline__ void finish_flat(double v, int tid, int nthr,
 
 // Ask L2 for a contiguous chunk ahead of its use (a hint: no destination,
 // no completion to wait for).  Address and size 16-byte multiples.
+// D = A B + C on the FP64 tensor cores, one m8n8k4 tile (lane = 4g + t):
+// a = A[g][t], b = B[t][g], {c0, c1} = C[g][2t], C[g][2t + 1]
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b, double c0,
+                                     double c1) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%4,%5};\n"
+               : "=d"(d0), "=d"(d1)
+               : "d"(a), "d"(b), "d"(c0), "d"(c1));
+}
+
 __device__ __forceinline__ void bulk_prefetch_l2(const void* p, unsigned bytes) {
   asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(p), "r"(bytes) : "memory");
 }

@@ -439,13 +439,17 @@ void convection_operator(struct element *sel, struct trivec *u,
 	const int e = sel->geom->id;
 	if (sel->basis->n != G_n || e < 0 || e >= G_nel)
 		fatal_error("ssenss_b200: convection_operator on an unknown element");
+	/* the time step advects the velocity with itself (u == v): one staged
+	 * field, which the library runs on its self-convection kernel */
+	const double *gv = u == v ? G_conv : G_conv + 3 * G_nt;
 	for (int c = 0; c < 3; ++c) {
 		memcpy(G_conv + c * G_nt, ***u->ind[c], G_nt * sizeof(double));
-		memcpy(G_conv + (3 + c) * G_nt, ***v->ind[c],
-				G_nt * sizeof(double));
+		if (u != v)
+			memcpy(G_conv + (3 + c) * G_nt, ***v->ind[c],
+					G_nt * sizeof(double));
 	}
-	check(ssg_convection_elements(G, e, 1, G_conv, G_conv + 3 * G_nt,
-			G_conv + 6 * G_nt), "convection_operator");
+	check(ssg_convection_elements(G, e, 1, G_conv, gv, G_conv + 6 * G_nt),
+			"convection_operator");
 	for (int c = 0; c < 3; ++c)
 		memcpy(***udv->ind[c], G_conv + (6 + c) * G_nt,
 				G_nt * sizeof(double));

@@ -53,6 +53,51 @@ def test_convection_matches_oracle(name, gpu_ctx_factory):
     assert rel(got, orc.convection(u, v)) < 1e-13
 
 
+SELF_CASES = {
+    # n = 8 (m = 12): the self-convection tensor-core kernel
+    "tgv3_n8": (lambda: tgv_box(3), 8),
+    "channel433_n8": (lambda: channel_mesh((4, 3, 3), seed=7), 8),
+}
+
+
+@pytest.mark.parametrize("name", list(SELF_CASES))
+def test_self_convection_matches_oracle(name, gpu_ctx_factory):
+    """convection_operator(u, u), the time step's call: at n = 8 the
+    tensor-core kernel, against the oracle and against the general kernel
+    (a copy of u as the advected field) run on the same inputs."""
+    mesh, n, orc, ctx = case(name, gpu_ctx_factory, SELF_CASES)
+    rng = np.random.default_rng(21)
+    u = rng.standard_normal((3, mesh.nel, n, n, n))
+    got = ctx.convection_operator(u, u)
+    ref = orc.convection(u, u)
+    assert rel(got, ref) < 1e-13
+    general = ctx.convection_operator(u, u.copy())
+    assert rel(general, ref) < 1e-13
+    assert rel(got, general) < 1e-13
+    # element ranges: elements 5 .. 5 + 7 of the mesh, fields of that range
+    sub = np.ascontiguousarray(u[:, 5:12])
+    part = ctx.convection_elements(5, sub, sub)
+    assert rel(part, ref[:, 5:12]) < 1e-13
+    one = np.ascontiguousarray(u[:, 3:4])
+    assert rel(ctx.convection_elements(3, one, one), ref[:, 3:4]) < 1e-13
+
+
+def test_self_convection_device_tensors_large(gpu_ctx_factory):
+    """Self-convection of device tensors on a mesh with more elements than
+    the persistent grid (2 blocks per SM), so blocks take several elements."""
+    import torch
+    mesh = tgv_box(8)
+    n = 8
+    orc = O.Oracle(mesh, n)
+    ctx = gpu_ctx_factory(mesh, n)
+    rng = np.random.default_rng(22)
+    u = rng.standard_normal((3, mesh.nel, n, n, n))
+    ud = torch.from_numpy(u).cuda()
+    out = ctx.convection_operator(ud, ud)
+    torch.cuda.synchronize()
+    assert rel(out.cpu().numpy(), orc.convection(u, u)) < 1e-13
+
+
 def test_convection_device_tensors(gpu_ctx_factory):
     import torch
     mesh, n, orc, ctx = case("tgv3_n8", gpu_ctx_factory, CONV_CASES)
