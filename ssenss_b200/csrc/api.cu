@@ -88,6 +88,10 @@ static void free_mesh(ssg_context* c) {
   if (c->p_ints) cudaFree(c->p_ints);
   c->p_ints = nullptr;
   c->p_cap = 0;
+  if (c->p_order) cudaFree(c->p_order);
+  if (c->p_bucket) cudaFree(c->p_bucket);
+  c->p_order = c->p_bucket = nullptr;
+  c->p_order_cap = 0;
   dfree(c->d_part); c->d_part = nullptr;
   for (auto& s : c->d_stage) { dfree(s); s = nullptr; }
   c->stage_cap = 0;
@@ -954,9 +958,28 @@ ssg_status ssg_integrate_particle_equations(ssg_context* c, size_t np, double* s
     SSG_CUDA(c, cudaMemcpyAsync(di, ints, 3 * np * sizeof(int), cudaMemcpyHostToDevice,
                                 c->stream));
   }
+  if (np > c->p_order_cap) {
+    if (c->p_order) cudaFree(c->p_order);
+    c->p_order = nullptr;
+    c->p_order_cap = 0;
+    if (cudaMalloc(&c->p_order, np * sizeof(int)) != cudaSuccess) {
+      cudaGetLastError();
+      c->p_order = nullptr;
+      return fail(c, SSG_ERR_NOMEM, "particle order");
+    }
+    c->p_order_cap = np;
+  }
+  if (!c->p_bucket) {
+    if (cudaMalloc(&c->p_bucket, 2 * ((size_t)c->nel + 1) * sizeof(int)) != cudaSuccess) {
+      cudaGetLastError();
+      c->p_bucket = nullptr;
+      return fail(c, SSG_ERR_NOMEM, "particle buckets");
+    }
+  }
   SSG_CUDA(c, cudaMemsetAsync(c->d_passes, 0, sizeof(int), c->stream));
   SSG_CUDA(c, run_particles(c->stream, c->n, c->nel, c->lev[0].npts, c->p_x, c->p_ur,
-                            c->p_jac, c->p_tinv, c->d_neigh, t, dt, np, ds, di, c->d_passes));
+                            c->p_jac, c->p_tinv, c->d_neigh, t, dt, np, ds, di, c->d_passes,
+                            np > 0 ? c->p_order : nullptr, c->p_bucket));
   if (np > 0 && !dev_state)
     SSG_CUDA(c, cudaMemcpyAsync(state, ds, 8 * np * sizeof(double), cudaMemcpyDeviceToHost,
                                 c->stream));

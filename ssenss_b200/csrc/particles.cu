@@ -15,7 +15,9 @@
 // is left for the host to reseed.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
+#include <cstdint>
 
 #include "ssg_internal.h"
 #include "ssg_kernels.h"
@@ -52,40 +54,63 @@ __device__ int first_point(const double* x, double xp, int n) {
   return n - 5;
 }
 
-// point value of one element block f (n^3) at reference coordinates
-__device__ double point_interp(int n, const double* x, const double* f, double xp, double yp,
-                               double zp) {
+// Lagrange weights of one point (src/interpolation.c:31-104): the full
+// n-point stencil for n <= 5, else the 5-point stencil from first_point in
+// each direction.  They depend on the position only, so one set serves
+// every field interpolated at that point (the reference recomputes them per
+// field; the values are the same).
+struct Stencil {
+  int i1, j1, k1;
+  double lx[5], ly[5], lz[5];
+};
+
+__device__ __forceinline__ void stencil_at(int n, const double* x, double xp, double yp,
+                                           double zp, Stencil& w) {
   if (n <= 5) {
-    double lx[5], ly[5], lz[5];
+    w.i1 = w.j1 = w.k1 = 0;
     for (int i = 0; i < n; ++i) {
-      lx[i] = lagrange(xp, x, i, n);
-      ly[i] = lagrange(yp, x, i, n);
-      lz[i] = lagrange(zp, x, i, n);
+      w.lx[i] = lagrange(xp, x, i, n);
+      w.ly[i] = lagrange(yp, x, i, n);
+      w.lz[i] = lagrange(zp, x, i, n);
     }
+    return;
+  }
+  w.i1 = first_point(x, xp, n);
+  w.j1 = first_point(x, yp, n);
+  w.k1 = first_point(x, zp, n);
+#pragma unroll
+  for (int i = 0; i < 5; ++i) {
+    w.lx[i] = lagrange(xp, x + w.i1, i, 5);
+    w.ly[i] = lagrange(yp, x + w.j1, i, 5);
+    w.lz[i] = lagrange(zp, x + w.k1, i, 5);
+  }
+}
+
+// point value of one element block f (n^3) with the weights w, in the
+// reference's summation order for each stencil form
+__device__ __forceinline__ double interp_at(int n, const Stencil& w, const double* f) {
+  if (n <= 5) {
     double s = 0.0;
     for (int k = 0; k < n; ++k) {
       double sj = 0.0;
       for (int j = 0; j < n; ++j) {
         double si = 0.0;
-        for (int i = 0; i < n; ++i) si += f[(k * n + j) * n + i] * lx[i];
-        sj += si * ly[j];
+        for (int i = 0; i < n; ++i) si += f[(k * n + j) * n + i] * w.lx[i];
+        sj += si * w.ly[j];
       }
-      s += sj * lz[k];
+      s += sj * w.lz[k];
     }
     return s;
   }
-  const int i1 = first_point(x, xp, n), j1 = first_point(x, yp, n), k1 = first_point(x, zp, n);
-  double lx[5], ly[5], lz[5];
-  for (int i = 0; i < 5; ++i) {
-    lx[i] = lagrange(xp, x + i1, i, 5);
-    ly[i] = lagrange(yp, x + j1, i, 5);
-    lz[i] = lagrange(zp, x + k1, i, 5);
-  }
   double s = 0.0;
+#pragma unroll 1
   for (int k = 0; k < 5; ++k)
-    for (int j = 0; j < 5; ++j)
-      for (int i = 0; i < 5; ++i)
-        s += f[((k1 + k) * n + j1 + j) * n + i1 + i] * lx[i] * ly[j] * lz[k];
+#pragma unroll
+    for (int j = 0; j < 5; ++j) {
+      const double* row = f + ((w.k1 + k) * n + w.j1 + j) * n + w.i1;
+#pragma unroll
+      for (int i = 0; i < 5; ++i) s += row[i] * w.lx[i] * w.ly[j] * w.lz[k];
+    }
   return s;
 }
 
@@ -93,27 +118,35 @@ __device__ const double* ur_block(const PartCtx& P, int lev, int comp, int e) {
   return P.ur + ((size_t)(lev * 3 + comp)) * P.npts + (size_t)e * P.n * P.n * P.n;
 }
 
-// quadratic Lagrange in time over t0-2dt, t0-dt, t0 (src/particles.c:493-515)
-__device__ double fluid_velocity(const PartCtx& P, int e, const double* y, double t, int comp) {
+// quadratic Lagrange in time over t0-2dt, t0-dt, t0 (src/particles.c:493-515),
+// the three components at one point
+__device__ void fluid_velocity3(const PartCtx& P, int e, const double* y, double t,
+                                double* uf) {
   const double eps = 1.0e-6;
   const double d0 = t - P.t + 2.0 * P.dt, d1 = t - P.t + P.dt, d2 = t - P.t;
   const double dt2 = P.dt * P.dt;
   const double a = 0.5 * d1 * d2 / dt2;
   const double b = -d0 * d2 / dt2;
   const double c = 0.5 * d0 * d1 / dt2;
-  double u0 = 0.0, u1 = 0.0, u2 = 0.0;
-  if (fabs(a) > eps) u0 = point_interp(P.n, P.x, ur_block(P, 0, comp, e), y[0], y[1], y[2]);
-  if (fabs(b) > eps) u1 = point_interp(P.n, P.x, ur_block(P, 1, comp, e), y[0], y[1], y[2]);
-  if (fabs(c) > eps) u2 = point_interp(P.n, P.x, ur_block(P, 2, comp, e), y[0], y[1], y[2]);
-  return a * u0 + b * u1 + c * u2;
+  Stencil w;
+  stencil_at(P.n, P.x, y[0], y[1], y[2], w);
+  for (int comp = 0; comp < 3; ++comp) {
+    double u0 = 0.0, u1 = 0.0, u2 = 0.0;
+    if (fabs(a) > eps) u0 = interp_at(P.n, w, ur_block(P, 0, comp, e));
+    if (fabs(b) > eps) u1 = interp_at(P.n, w, ur_block(P, 1, comp, e));
+    if (fabs(c) > eps) u2 = interp_at(P.n, w, ur_block(P, 2, comp, e));
+    uf[comp] = a * u0 + b * u1 + c * u2;
+  }
 }
 
 __device__ void particle_rhs(const PartCtx& P, int e, double tau, const double* y, double t,
                              double* f) {
   const double a = 1.0 / tau;
+  double uf[3];
+  fluid_velocity3(P, e, y, t, uf);
   for (int i = 0; i < 3; ++i) {
     f[i] = y[i + 3];
-    f[i + 3] = a * (fluid_velocity(P, e, y, t, i) - y[i + 3]);
+    f[i + 3] = a * (uf[i] - y[i + 3]);
   }
 }
 
@@ -200,9 +233,9 @@ __device__ int closest_face(const double* s) {
   return k;
 }
 
-__device__ double factor_at(const PartCtx& P, const double* fac, int a, int e, const double* s) {
-  return point_interp(P.n, P.x, fac + (size_t)a * P.npts + (size_t)e * P.n * P.n * P.n, s[0],
-                      s[1], s[2]);
+__device__ double factor_at(const PartCtx& P, const Stencil& w, const double* fac, int a,
+                           int e) {
+  return interp_at(P.n, w, fac + (size_t)a * P.npts + (size_t)e * P.n * P.n * P.n);
 }
 
 // cross into the neighbour through the closest face; physical velocity by
@@ -214,9 +247,12 @@ __device__ void new_element(const PartCtx& P, double* s, int* st) {
   const int nb = P.neigh[26 * (size_t)e + j];
   if (nb >= 0) {
     st[0] = nb;
+    // the position does not change in this loop: one set of weights
+    Stencil w;
+    stencil_at(P.n, P.x, s[0], s[1], s[2], w);
     for (int comp = 0; comp < 3; ++comp) {
       double dx[3];
-      for (int i = 0; i < 3; ++i) dx[i] = factor_at(P, P.jac, 3 * comp + i, e, s);
+      for (int i = 0; i < 3; ++i) dx[i] = factor_at(P, w, P.jac, 3 * comp + i, e);
       s[3 + comp] = s[3] * dx[0] + s[4] * dx[1] + s[5] * dx[2];
     }
   } else {
@@ -242,17 +278,67 @@ __device__ void new_location(const PartCtx& P, double* s, int* st) {
   j = 0;
   for (int i = 0; i < 3; ++i) {
     if (i != k / 2) s[i] = x[j++];
+    // the position changes from one i to the next: weights per i
+    Stencil w;
+    stencil_at(P.n, P.x, s[0], s[1], s[2], w);
     double dx[3];
-    for (int a = 0; a < 3; ++a) dx[a] = factor_at(P, P.tinv, 3 * a + i, e, s);
+    for (int a = 0; a < 3; ++a) dx[a] = factor_at(P, w, P.tinv, 3 * a + i, e);
     s[3 + i] = s[3] * dx[0] + s[4] * dx[1] + s[5] * dx[2];
   }
   st[1] = st[0];
 }
 
+// Particles are taken in element order (a counting sort of their element
+// ids each call) so that the threads of a warp interpolate in the same
+// element's fields and share their cache lines; each particle's own
+// arithmetic is unchanged, so the order does not change any result.
+__global__ void k_part_count(size_t np, const int* __restrict__ ints, int nel,
+                             int* __restrict__ count) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < np;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const int e = ints[3 * i];
+    atomicAdd(count + (e >= 0 && e < nel ? e : nel), 1);
+  }
+}
+
+// exclusive prefix sum of count[0 .. nb) into start[0 .. nb), one block
+__global__ void __launch_bounds__(1024) k_part_scan(int nb, const int* __restrict__ count,
+                                                    int* __restrict__ start) {
+  __shared__ int part[1024];
+  const int chunk = (nb + 1023) / 1024;
+  const int lo = threadIdx.x * chunk, hi = min(nb, lo + chunk);
+  int sum = 0;
+  for (int q = lo; q < hi; ++q) sum += count[q];
+  part[threadIdx.x] = sum;
+  __syncthreads();
+  for (int off = 1; off < 1024; off <<= 1) {   // inclusive scan of the chunk sums
+    const int v = threadIdx.x >= off ? part[threadIdx.x - off] : 0;
+    __syncthreads();
+    part[threadIdx.x] += v;
+    __syncthreads();
+  }
+  int run = part[threadIdx.x] - sum;
+  for (int q = lo; q < hi; ++q) {
+    start[q] = run;
+    run += count[q];
+  }
+}
+
+__global__ void k_part_scatter(size_t np, const int* __restrict__ ints, int nel,
+                               int* __restrict__ cursor, int* __restrict__ order) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < np;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const int e = ints[3 * i];
+    order[atomicAdd(cursor + (e >= 0 && e < nel ? e : nel), 1)] = (int)i;
+  }
+}
+
 __global__ void __launch_bounds__(128) k_particles(PartCtx P, size_t np, double* __restrict__ state,
-                                                   int* __restrict__ ints, int* __restrict__ passes) {
-  const size_t pi = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (pi >= np) return;
+                                                   int* __restrict__ ints, int* __restrict__ passes,
+                                                   const int* __restrict__ order) {
+  const size_t ti = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (ti >= np) return;
+  const size_t pi = order ? (size_t)order[ti] : ti;
   double s[8];
   int st[3];
   for (int a = 0; a < 8; ++a) s[a] = state[8 * pi + a];
@@ -286,7 +372,7 @@ __global__ void __launch_bounds__(128) k_particles(PartCtx P, size_t np, double*
 cudaError_t run_particles(cudaStream_t s, int n, int nel, size_t npts, const double* x,
                           const double* ur, const double* jac, const double* tinv,
                           const int* neigh, double t, double dt, size_t np, double* state,
-                          int* ints, int* passes) {
+                          int* ints, int* passes, int* order, int* bucket) {
   dev::PartCtx P;
   P.n = n;
   P.nel = nel;
@@ -299,9 +385,25 @@ cudaError_t run_particles(cudaStream_t s, int n, int nel, size_t npts, const dou
   P.t = t;
   P.dt = dt;
   if (np == 0) return cudaSuccess;
+  if (np > (size_t)INT32_MAX) return cudaErrorInvalidValue;
+  if (order) {
+    // bucket: counts then start offsets, nel + 1 each (the last bucket holds
+    // particles with an invalid element id)
+    int* count = bucket;
+    int* cursor = bucket + nel + 1;
+    cudaError_t err = cudaMemsetAsync(count, 0, (nel + 1) * sizeof(int), s);
+    if (err != cudaSuccess) return err;
+    const unsigned g = (unsigned)std::min<size_t>((np + 255) / 256, 4096);
+    count_launch();
+    dev::k_part_count<<<g, 256, 0, s>>>(np, ints, nel, count);
+    count_launch();
+    dev::k_part_scan<<<1, 1024, 0, s>>>(nel + 1, count, cursor);
+    count_launch();
+    dev::k_part_scatter<<<g, 256, 0, s>>>(np, ints, nel, cursor, order);
+  }
   const unsigned blocks = (unsigned)((np + 127) / 128);
   count_launch();
-  dev::k_particles<<<blocks, 128, 0, s>>>(P, np, state, ints, passes);
+  dev::k_particles<<<blocks, 128, 0, s>>>(P, np, state, ints, passes, order);
   return cudaGetLastError();
 }
 

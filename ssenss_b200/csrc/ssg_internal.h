@@ -169,6 +169,9 @@ struct ssg_context {
   double* p_state = nullptr;    // staging of host particle arrays
   int* p_ints = nullptr;
   size_t p_cap = 0;
+  int* p_order = nullptr;       // element-order sort of the particles:
+  int* p_bucket = nullptr;      //   permutation (p_order_cap) and 2 (nel + 1) counters
+  size_t p_order_cap = 0;
   // reductions / scalars
   double* d_part = nullptr;     // block partial sums
   size_t part_cap = 0;

@@ -211,10 +211,12 @@ cudaError_t run_convection_dmma(cudaStream_t s, int nel, int e0, int nel_fac, co
                                 double* udv, const double* W, const double* Dh,
                                 const double* Jh);
 // Lagrangian particle advance to time t (particles.cu); passes: device int
-// that receives the largest per-particle pass count (atomicMax, caller zeroes)
+// that receives the largest per-particle pass count (atomicMax, caller zeroes).
+// order (np ints) and bucket (2 (nel + 1) ints): scratch of the element-order
+// sort the particles are processed in; order == nullptr keeps array order.
 cudaError_t run_particles(cudaStream_t s, int n, int nel, size_t npts, const double* x,
                           const double* ur, const double* jac, const double* tinv,
                           const int* neigh, double t, double dt, size_t np, double* state,
-                          int* ints, int* passes);
+                          int* ints, int* passes, int* order, int* bucket);
 
 }  // namespace ssg
