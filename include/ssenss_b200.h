@@ -119,6 +119,13 @@ ssg_status ssg_set_graphs(ssg_context *ctx, int enable);
 #define SSG_SETUP_NO_PARTICLES 2u
 #define SSG_SETUP_OPPOSITE_PAIRING 4u
 ssg_status ssg_set_setup_options(ssg_context *ctx, unsigned flags);
+/* Spectral vanishing viscosity of the Helmholtz operator for the next
+ * ssg_setup_mesh (params->svvn, params->svva; src/main.c:54-55): every
+ * level's SVV derivative matrix is built with cut-off mode svvn and
+ * amplitude svva as compute_svv_derivative_matrix does (src/deriv.c:81-112,
+ * src/precon.c:130-132).  svvn < 0 takes the reference's default 2n/3; the
+ * default amplitude is 0 (the reference's). */
+ssg_status ssg_set_svv(ssg_context *ctx, int svvn, double svva);
 /* Device memory (bytes) the context holds now. */
 ssg_status ssg_memory_info(const ssg_context *ctx, size_t *device_bytes);
 

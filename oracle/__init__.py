@@ -134,14 +134,17 @@ class Oracle(_Common):
             L.og_deriv.argtypes = [C.c_int, _dp, _dp]
             L.og_svv_deriv.argtypes = [C.c_int, _dp, _dp, C.c_int, C.c_double, _dp]
             L.og_interp.argtypes = [C.c_int, _dp, C.c_int, _dp, _dp]
+            L.og_set_svv.argtypes = [C.c_int, C.c_double]
             cls._lib = L
         return cls._lib
 
-    def __init__(self, mesh, n, dt=1e-3, visc=1.0 / 1600.0, dens=1.0):
+    def __init__(self, mesh, n, dt=1e-3, visc=1.0 / 1600.0, dens=1.0, svv=(-1, 0.0)):
+        """svv: (svvn, svva) of the SVV Helmholtz operator (svvn < 0: 2n/3)."""
         L = self.lib()
         self.n, self.nel = int(n), int(mesh.nel)
         self._vert = _f64(mesh.vertices)
         self._neigh = np.ascontiguousarray(mesh.neigh, dtype=np.int32)
+        L.og_set_svv(int(svv[0]), float(svv[1]))
         self.h = L.og_create(self.n, self.nel, _d(self._vert), _i(self._neigh),
                              dt, visc, dens)
         if not self.h:
@@ -323,16 +326,20 @@ class Reference(_Common):
             L.ssgref_set_field.argtypes = [C.c_int, C.c_int, _dp]
             L.ssgref_particles_advance.argtypes = [C.c_size_t, _dp, _ip]
             L.ssgref_set_level0_factor.argtypes = [C.c_int, _dp]
+            L.ssgref_set_svv.argtypes = [C.c_int, C.c_double]
             L.ssgref_particles_advance.restype = C.c_int
             cls._lib = L
         return cls._lib
 
-    def __init__(self, mesh, n, dt=1e-3, visc=1.0 / 1600.0, dens=1.0):
+    def __init__(self, mesh, n, dt=1e-3, visc=1.0 / 1600.0, dens=1.0, svv=(-1, 0.0)):
+        """svv: (svvn, svva) of the SVV Helmholtz operator (svvn < 0: 2n/3,
+        the reference's src/main.c:54-55 values are (2n/3, 0))."""
         L = self.lib()
         self.n, self.nel = int(n), int(mesh.nel)
         # the reference keeps pointers into these during setup only
         self._vert = _f64(mesh.vertices)
         self._neigh = np.ascontiguousarray(mesh.neigh, dtype=np.int32)
+        L.ssgref_set_svv(int(svv[0]), float(svv[1]))
         self.nlevels = L.ssgref_setup(self.n, self.nel, _d(self._vert),
                                       _i(self._neigh), dt, visc, dens)
         self.orders = [L.ssgref_level_order(l) for l in range(self.nlevels)]
@@ -433,6 +440,11 @@ class Reference(_Common):
     # -- time stepping / particles -------------------------------------------
     def init_tgv(self):
         self.lib().ssgref_init_tgv()
+
+    def init_ethier_steinman(self):
+        """The reference's analytic test case (src/test.c:202-214):
+        Ethier-Steinman velocity and time-dependent Dirichlet walls."""
+        self.lib().ssgref_init_ethier_steinman()
 
     def ns_step(self):
         self.lib().ssgref_ns_step()

@@ -136,6 +136,16 @@ void ssgref_teardown(void)
 	H_sel = NULL;
 }
 
+/* SVV parameters of the next set-up (src/main.c:54-55 fixes 2n/3 and 0) */
+static int H_svvn = -1;
+static double H_svva = 0.0;
+
+void ssgref_set_svv(int svvn, double svva)
+{
+	H_svvn = svvn;
+	H_svva = svva;
+}
+
 /* Set the solver up as src/main.c:36-90 does (minus files and particles). */
 int ssgref_setup(int n, int nel, const double *vertices, const int *neigh,
 		double dt, double visc, double dens)
@@ -153,8 +163,8 @@ int ssgref_setup(int n, int nel, const double *vertices, const int *neigh,
 	H_params->visc = visc;
 	H_params->dens = dens;
 	H_params->nconv = (3 * n) / 2;
-	H_params->svvn = 2 * n / 3;
-	H_params->svva = 0.0;
+	H_params->svvn = H_svvn >= 0 ? H_svvn : 2 * n / 3;
+	H_params->svva = H_svva;
 	get_grid_size(H_params, H_comm, "");
 
 	H_gll = new_gll_basis(n);
@@ -650,6 +660,17 @@ void ssgref_init_tgv(void)
 			(**s->old->old->p)[q] = p;
 		}
 	}
+	compute_reference_domain_velocity(H_sel);
+}
+
+/* The analytic Ethier-Steinman case of the reference's --run-test
+ * (src/main.c:82-84): velocity and the time-dependent Dirichlet values of
+ * every wall from initialise_test (src/test.c:202-214), pressure left at
+ * zero as the reference leaves it without an initial file, then the
+ * reference-domain velocity. */
+void ssgref_init_ethier_steinman(void)
+{
+	initialise_test(H_sel);
 	compute_reference_domain_velocity(H_sel);
 }
 

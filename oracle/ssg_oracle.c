@@ -742,6 +742,17 @@ static void init_precon(og_ctx *c)
 /* setup (src/main.c:53-79, src/precon.c:58-183)                      */
 /* ------------------------------------------------------------------ */
 
+/* SVV cut-off mode and amplitude of the contexts created next
+ * (params->svvn, params->svva; src/main.c:54-55): svvn < 0 is 2n/3 */
+static int og_next_svvn = -1;
+static double og_next_svva = 0.0;
+
+void og_set_svv(int svvn, double svva)
+{
+	og_next_svvn = svvn;
+	og_next_svva = svva;
+}
+
 og_ctx *og_create(int n, int nel, const double *vertices, const int *neigh,
 		double dt, double visc, double dens)
 {
@@ -775,11 +786,12 @@ og_ctx *og_create(int n, int nel, const double *vertices, const int *neigh,
 			break;
 	}
 	c->nlev = nlev;
-	const int msvv = 2 * n / 3;
+	/* one cut-off mode and amplitude for every level (src/precon.c:130-132) */
+	const int msvv = og_next_svvn >= 0 ? og_next_svvn : 2 * n / 3;
 	for (int l = 0; l < nlev; ++l) {
 		level_t *L = &c->lev[l];
 		alloc_level(L, L->n, nel);
-		make_basis(&L->b, L->n, msvv, 0.0);
+		make_basis(&L->b, L->n, msvv, og_next_svva);
 	}
 	grid_from_vertices(&c->lev[0], nel, vertices);
 	compute_factors(&c->lev[0], nel);

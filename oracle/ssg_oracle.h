@@ -33,6 +33,9 @@ void og_interp(int nto, const double *xto, int nfrom, const double *xfrom,
 		double *J);
 
 /* ---- setup (src/main.c:53-79, src/precon.c:121-183,336-413) ---- */
+/* SVV cut-off mode and amplitude of the contexts created next (svvn < 0:
+ * 2n/3; the reference's defaults are 2n/3 and 0, src/main.c:54-55) */
+void og_set_svv(int svvn, double svva);
 og_ctx *og_create(int n, int nel, const double *vertices, const int *neigh,
 		double dt, double visc, double dens);
 void og_destroy(og_ctx *c);

@@ -144,6 +144,11 @@ class Context:
             (4 if opposite_pairing else 0)
         self._check(self.lib.ssg_set_setup_options(self.h, flags), "set_setup_options")
 
+    def set_svv(self, svvn=-1, svva=0.0):
+        """ssg_set_svv: SVV cut-off mode and amplitude of the Helmholtz
+        operator for the next setup_mesh (svvn < 0: 2n/3)."""
+        self._check(self.lib.ssg_set_svv(self.h, int(svvn), float(svva)), "set_svv")
+
     def memory_bytes(self) -> int:
         b = C.c_size_t()
         self._check(self.lib.ssg_memory_info(self.h, C.byref(b)), "memory_info")

@@ -485,7 +485,8 @@ ssg_status ssg_setup_mesh(ssg_context* c, int n, int nel, const double* vertices
   SSG_CUDA(c, cudaSetDevice(c->device));
   free_mesh(c);
   c->host = ssg::HostMesh();
-  ssg_status st = build_mesh(c->host, n, nel, vertices, neigh, c->err, c->setup_opts);
+  ssg_status st = build_mesh(c->host, n, nel, vertices, neigh, c->err, c->setup_opts,
+                             c->svvn, c->svva);
   if (st != SSG_OK) return st;
   return upload_all(c);
 }
@@ -501,6 +502,15 @@ ssg_status ssg_set_setup_options(ssg_context* c, unsigned flags) {
   if (flags & ~(SSG_SETUP_NO_DEALIAS | SSG_SETUP_NO_PARTICLES | SSG_SETUP_OPPOSITE_PAIRING))
     return fail(c, SSG_ERR_ARG, "unknown set-up option");
   c->setup_opts = flags;
+  return SSG_OK;
+}
+
+ssg_status ssg_set_svv(ssg_context* c, int svvn, double svva) {
+  if (!c) return SSG_ERR_ARG;
+  if (!std::isfinite(svva) || svva < 0.0)
+    return fail(c, SSG_ERR_ARG, "svva must be finite and >= 0");
+  c->svvn = svvn;
+  c->svva = svva;
   return SSG_OK;
 }
 

@@ -483,7 +483,7 @@ void stiffness_diagonal(const HostLevel& L, int nel, double* out) {
 }
 
 ssg_status build_mesh(HostMesh& m, int n, int nel, const double* vert, const int* neigh,
-                      std::string& err, unsigned opts) {
+                      std::string& err, unsigned opts, int svvn, double svva) {
   if (n < 2 || n > 12 || (3 * n) / 2 > SSG_MAXN) {
     err = "order n must be in [2, 12]";
     return SSG_ERR_ARG;
@@ -499,10 +499,11 @@ ssg_status build_mesh(HostMesh& m, int n, int nel, const double* vert, const int
   if (st != SSG_OK) return st;
   int orders[SSG_MAXLEV];
   m.nlev = level_orders(n, orders);
-  const int msvv = 2 * n / 3;
+  // one cut-off mode and amplitude for every level (src/precon.c:130-132)
+  const int msvv = svvn >= 0 ? svvn : 2 * n / 3;
   for (int l = 0; l < m.nlev; ++l) {
     alloc_level(m.lev[l], orders[l], nel, l == 0 && !(opts & SSG_SETUP_NO_PARTICLES));
-    make_basis(m.lev[l], orders[l], msvv, 0.0);
+    make_basis(m.lev[l], orders[l], msvv, svva);
   }
   const bool particles = !(opts & SSG_SETUP_NO_PARTICLES);
   grid_from_vertices(m.lev[0], nel, vert);

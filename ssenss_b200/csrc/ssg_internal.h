@@ -83,7 +83,8 @@ void svv_deriv_matrix(int n, const double* x, const double* w, int msvv, double 
                       double* S);
 void interp_matrix(int nto, const double* xto, int nfrom, const double* xfrom, double* J);
 ssg_status build_mesh(HostMesh& m, int n, int nel, const double* vertices,
-                      const int* neigh, std::string& err, unsigned opts = 0);
+                      const int* neigh, std::string& err, unsigned opts = 0,
+                      int svvn = -1, double svva = 0.0);
 ssg_status build_pairs(HostMesh& m, std::string& err, bool opposite = false);
 void stiffness_diagonal(const HostLevel& L, int nel, double* out);
 void host_dss(const HostMesh& m, int n, double* u);
@@ -142,6 +143,8 @@ struct ssg_context {
   bool graphs = true;
   bool ready = false;
   unsigned setup_opts = 0;      // SSG_SETUP_* flags of the next ssg_setup_mesh
+  int svvn = -1;                // SVV cut-off mode of the next set-up (< 0: 2n/3)
+  double svva = 0.0;            // SVV amplitude of the next set-up
   size_t dev_bytes = 0;         // device memory this context holds
   const volatile int* cancel = nullptr;   // nonzero: stop the running solve
   double deadline = 0.0;        // steady-clock seconds; 0 = none

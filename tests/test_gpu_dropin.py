@@ -21,6 +21,12 @@ per-element convection calls, one pressure Poisson solve (FCG + p-multigrid)
 and three Helmholtz solves (Jacobi CG), all to the reference's absolute
 1e-10.
 
+The reference's analytic test (--run-test, src/test.c:202-214): the
+Ethier-Steinman flow on [-1, 1]^3 with Dirichlet walls on every side whose
+values follow the exact solution in time, 3^3 elements at n = 8, unit
+viscosity, 10 steps: the same bars, and both runs within ES_EXACT of the
+exact velocity.
+
 Bars (each stated where it is asserted):
   * every solve of every step: the same number of iterations, or one apart
     only where the residual at the deciding iteration lies within a factor 2
@@ -30,7 +36,7 @@ Bars (each stated where it is asserted):
     times eps, the rest within POISSON_HIST_REL of the first residual plus
     POISSON_HIST_EPS times eps plus the first residual's deviation (reasons
     where they are defined);
-  * fields after 20 steps: the velocity relative to its largest component,
+  * fields after the last step: the velocity relative to its largest component,
     the pressure relative to its largest entry, FIELD_REL when every solve
     stopped at the same iteration, FIELD_STOP_REL otherwise;
   * the individual bound functions on the reference's own set-up: DSS
@@ -38,6 +44,7 @@ Bars (each stated where it is asserted):
     walk bitwise (on inputs where the reference reseeds no particle: a
     reseed draws a random position).
 """
+import math
 import multiprocessing as mp
 import os
 import sys
@@ -80,16 +87,35 @@ POISSON_INPUT_EPS = 100.0
 
 
 def _c1_run(gpu, steps, path):
+    _ns_run("tgv", gpu, steps, path)
+
+
+def _es_run(gpu, steps, path):
+    _ns_run("es", gpu, steps, path)
+
+
+def _ns_run(case, gpu, steps, path):
+    """Time steps of the reference's integrator, CPU alone (gpu False) or
+    with its solve path bound to the library.  case "tgv": C1's triply
+    periodic Taylor-Green box; "es": the reference's analytic
+    Ethier-Steinman test on [-1, 1]^3 with Dirichlet walls on every side."""
     os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
     import numpy as np
 
     import oracle as O
-    from ssenss_b200.mesh import tgv_box
+    from ssenss_b200.mesh import box_mesh, tgv_box
 
     cls = O.ReferenceGPU if gpu else O.Reference
-    ref = cls(tgv_box(4), 8, dt=DT, visc=VISC, dens=1.0)
-    ref.init_tgv()
+    if case == "tgv":
+        ref = cls(tgv_box(4), 8, dt=DT, visc=VISC, dens=1.0)
+        ref.init_tgv()
+    else:
+        ref = cls(box_mesh((3, 3, 3), lo=(-1.0,) * 3, hi=(1.0,) * 3,
+                           periodic=(False,) * 3), 8, dt=DT, visc=1.0, dens=1.0)
+        ref.init_ethier_steinman()
     out = {}
+    for c in range(3):
+        out[f"x{c}"] = ref.geometry(0, 7 + c)
     for s in range(steps):
         ref.ns_step()
         for i, (kind, var, hist) in enumerate(ref.step_log()):
@@ -154,6 +180,51 @@ def _in_child(fn, *args):
         f"{fn.__name__}{args[:-1]} ended with exit code {p.exitcode} and no result"
 
 
+ES_STEPS = 10
+# Ethier-Steinman: the velocity error of the reference alone against the
+# exact solution after ES_STEPS steps on 3^3 elements at n = 8 is 2.2e-8
+ES_EXACT = 1e-7
+
+
+def _ethier_steinman(x, y, z, t):
+    """The Ethier-Steinman exact velocity (a = pi/4, d = pi/2, unit
+    viscosity; Ethier and Steinman 1994), the reference's test case."""
+    a, d = math.pi / 4, math.pi / 2
+    g = np.exp(-d * d * t)
+    u = -a * (np.exp(a * x) * np.sin(a * y + d * z) + np.exp(a * z) * np.cos(a * x + d * y)) * g
+    v = -a * (np.exp(a * y) * np.sin(a * z + d * x) + np.exp(a * x) * np.cos(a * y + d * z)) * g
+    w = -a * (np.exp(a * z) * np.sin(a * x + d * y) + np.exp(a * y) * np.cos(a * z + d * x)) * g
+    return u, v, w
+
+
+@pytest.fixture(scope="module")
+def es(tmp_path_factory):
+    d = tmp_path_factory.mktemp("es")
+    res = []
+    for gpu in (False, True):
+        path = str(d / f"es_{int(gpu)}.npz")
+        _in_child(_es_run, gpu, ES_STEPS, path)
+        res.append(dict(np.load(path)))
+    return res
+
+
+def test_ethier_steinman_walls_through_the_binding(es):
+    """The reference's analytic test (--run-test: Dirichlet walls with
+    time-dependent values on every side, the pressure right-hand side's
+    surface integral, src/test.c:202-214, src/poisson.c:145-194) stepped by
+    the reference's integrator with its solve path on the GPU: the same bars
+    as C1 against the reference alone, and both runs' velocity within
+    ES_EXACT of the exact solution."""
+    cpu, gpu = es
+    _check_steps(cpu, gpu, ES_STEPS, "Ethier-Steinman drop-in")
+    t = float(cpu["t"])
+    ex = _ethier_steinman(cpu["x0"], cpu["x1"], cpu["x2"], t)
+    errs = [max(float(np.max(np.abs(r[f"f{c}"] - ex[c]))) for c in range(3)) for r in (cpu, gpu)]
+    print(f"Ethier-Steinman: velocity error against the exact solution at t = {t:g}: "
+          f"reference {errs[0]:.3e}, through the binding {errs[1]:.3e}")
+    assert errs[0] <= ES_EXACT and errs[1] <= ES_EXACT
+
+
 @pytest.fixture(scope="module")
 def c1(tmp_path_factory):
     d = tmp_path_factory.mktemp("c1")
@@ -174,13 +245,14 @@ def _solves(r, s):
     return out
 
 
-def test_c1_navier_stokes_steps_through_the_binding(c1):
-    cpu, gpu = c1
-    assert float(gpu["t"]) == pytest.approx(STEPS * DT)
+def _check_steps(cpu, gpu, steps, label):
+    """Every solve of every step and the fields at the end, with the bars of
+    the module docstring; returns the fields' deviations."""
+    assert float(gpu["t"]) == pytest.approx(steps * DT)
     # every solve of every step: iterations and history deviations (all
     # gathered first, printed, then asserted)
     rows = []
-    for s in range(STEPS):
+    for s in range(steps):
         sc, sg = _solves(cpu, s), _solves(gpu, s)
         assert [k for k, _ in sc] == [k for k, _ in sg] == [(0, 0), (1, 1), (1, 2), (1, 3)]
         for (kv, hc), (_, hg) in zip(sc, sg):
@@ -196,9 +268,9 @@ def test_c1_navier_stokes_steps_through_the_binding(c1):
     for r in sorted(rows, key=lambda r: -r[6])[:5]:
         print(f"  step {r[0]} solve {tuple(int(v) for v in r[1])}: iterations {r[2]}/{r[3]}, "
               f"first residual {r[4][0]:.3e}, largest deviation {r[6]:.3e}")
-    print(f"C1 drop-in: {len(rows)} solves, every stop equal: {same}, largest history "
+    print(f"{label}: {len(rows)} solves, every stop equal: {same}, largest history "
           f"deviation {worst[6]:.2e} absolute ({worst[6] / worst[4][0]:.2e} of h0, step "
-          f"{worst[0]}, solve {worst[1]}), fields u v w p after {STEPS} steps "
+          f"{worst[0]}, solve {worst[1]}), fields u v w p after {steps} steps "
           f"{', '.join(f'{d:.2e}' for d in devs)}")
     for s, kv, lc, lg, hc, hg, dmax in rows:
         if lc != lg:
@@ -223,6 +295,12 @@ def test_c1_navier_stokes_steps_through_the_binding(c1):
     pdev = devs[3]
     assert vdev <= (FIELD_REL if same else FIELD_STOP_REL), (vdev, same)
     assert pdev <= (FIELD_REL if same else FIELD_STOP_REL), (pdev, same)
+    return devs
+
+
+def test_c1_navier_stokes_steps_through_the_binding(c1):
+    cpu, gpu = c1
+    _check_steps(cpu, gpu, STEPS, "C1 drop-in")
 
 
 @pytest.fixture(scope="module")

@@ -232,3 +232,35 @@ def test_mixed_precision_solve(name, gpu_ctx_factory):
     assert info["residual"] <= 1e-10
     assert info["iterations"] <= len(h_o) + 3
     assert rel(u_g, u_o) < 1e-8
+
+
+@pytest.mark.parametrize("svv", [(3, 1.5), (-1, 0.3)])
+def test_svv_helmholtz(svv):
+    """Spectral vanishing viscosity on (ssg_set_svv before the set-up): the
+    Helmholtz operator to 1e-13 and the Jacobi-CG Helmholtz solve (same
+    iteration count, solution 1e-12, history 1e-9 of the first residual)
+    against the oracle set up with the same svvn and svva (the oracle's SVV
+    matrices are pinned to the reference's in tests/test_oracle_pins.py)."""
+    import ssenss_b200 as S
+    mesh, n = channel_mesh((4, 3, 3), seed=7), 8
+    orc = O.Oracle(mesh, n, svv=svv)
+    ctx = S.Context(0)
+    try:
+        ctx.set_parameters(1e-3, 1.0 / 1600.0, 1.0)
+        ctx.set_svv(*svv)
+        ctx.setup_mesh(mesh, n)
+        rng = np.random.default_rng(41)
+        u = rng.standard_normal((mesh.nel, n, n, n))
+        for var in (O.X_VELOCITY, O.Y_VELOCITY):
+            assert rel(ctx.global_opeval(var, u), orc.global_opeval(var, u)) < 1e-13
+        f = weak_rhs(orc, smooth_field(orc))
+        u0 = np.zeros_like(f)
+        u_o, h_o = orc.solve_helmholtz(O.X_VELOCITY, f, u0)
+        u_g, info = ctx.solve_helmholtz_cg(O.X_VELOCITY, f, u0.copy())
+        assert info["status"] == "SSG_OK"
+        assert info["iterations"] == len(h_o)
+        assert rel(u_g, u_o) < 1e-12
+        assert np.all(np.abs(info["history"] - h_o) <= 1e-9 * h_o[0])
+    finally:
+        ctx.close()
+        orc.close()
