@@ -243,6 +243,24 @@ ssg_status ssg_solve_poisson_cg(ssg_context *ctx, const double *f, double *u,
  * preconditioner on the Helmholtz operator. */
 ssg_status ssg_solve_helmholtz_cg(ssg_context *ctx, int var, const double *f,
 		double *u, double eps, int max_iter, ssg_solve_info *info);
+/* Helmholtz solves of several independent meshes in shared launches (no
+ * reference counterpart: the reference solves one mesh per process).  The
+ * context's mesh is the concatenation of nseg meshes: segment s is the
+ * elements seg_first[s] .. seg_first[s+1]-1 (seg_first[0] = 0,
+ * seg_first[nseg] = nel; no element may neighbour another segment's,
+ * checked).  Segment s is solved as solve_helmholtz_cg would
+ * (src/solver.c:33-81, 175-189) with Helmholtz constant lambda[s] (the
+ * context's dt and viscosity are not used) and absolute stop eps[s], with
+ * its own CG scalars, stop test and iteration count; every iteration's
+ * element operator and DSS are one launch over all segments.  f, u: the
+ * concatenated fields (u: initial guess in, solution out), host or device.
+ * info[s] receives the segment's iterations and residuals (no history).
+ * Each segment's sums are grouped differently from a solo solve's, so its
+ * iterates agree with ssg_solve_helmholtz_cg on the same mesh to rounding.
+ * Returns SSG_MAXITER when a segment hits max_iter. */
+ssg_status ssg_solve_helmholtz_segments(ssg_context *ctx, int var, int nseg,
+		const int *seg_first, const double *lambda, const double *f,
+		double *u, const double *eps, int max_iter, ssg_solve_info *info);
 /* conjugate_gradient with jacobi_preconditioner on either operator
  * (src/solver.c:33-81). */
 ssg_status ssg_conjugate_gradient(ssg_context *ctx, int var, const double *f,
@@ -335,6 +353,8 @@ typedef struct {
 	size_t hbm_in_use, hbm_peak, hbm_budget;
 	unsigned long long mesh_hits, mesh_misses, evictions;
 	int max_active_seen, resident_contexts;
+	/* shared-launch batches run, and the requests they held */
+	unsigned long long batches, batched_requests;
 } ssg_server_stats;
 
 /* GLL points and quadrature weights of n points on [-1, 1] (gll_basis,
@@ -344,6 +364,16 @@ ssg_status ssg_gll(int n, double *points, double *weights);
 size_t ssg_request_bytes(int n, int nel, int precision);
 ssg_status ssg_server_create(int device, size_t hbm_budget, int max_active,
 		ssg_server **out);
+/* Shared launches across requests (off by default, max_batch 1): a small
+ * Helmholtz request (at most max_points points, absolute eps) at the head of
+ * the queue runs together with the small Helmholtz requests of the same
+ * order queued directly behind it, up to max_batch in all, as one
+ * ssg_solve_helmholtz_segments on their concatenated meshes -- one operator
+ * and one DSS launch per iteration for all of them, each with its own
+ * lambda, CG scalars and stop.  Results agree with the solo solve to
+ * rounding (not bitwise); batched requests use no resident context. */
+ssg_status ssg_server_set_batching(ssg_server *srv, int max_batch,
+		size_t max_points);
 /* rhs (host, nel x n^3, an assembled weak right-hand side) is copied at
  * submission; the solution is written to `solution` (host) before the
  * request completes.  Initial guess zero. */

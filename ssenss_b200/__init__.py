@@ -288,6 +288,24 @@ class Context:
                            "solve_helmholtz_cg", history, max_iter)
         return u, info
 
+    def solve_helmholtz_segments(self, var, seg_first, lambdas, f, u, eps, max_iter=5000):
+        """ssg_solve_helmholtz_segments: Helmholtz solves of the independent
+        meshes concatenated in this context's mesh, in shared launches.
+        seg_first: nseg + 1 element offsets; lambdas, eps: one per segment.
+        Returns u and one info dict per segment."""
+        seg = np.ascontiguousarray(seg_first, dtype=np.int32)
+        lam = np.ascontiguousarray(lambdas, dtype=np.float64)
+        ep = np.ascontiguousarray(np.broadcast_to(np.asarray(eps, dtype=np.float64),
+                                                  lam.shape))
+        nseg = len(lam)
+        infos = (SolveInfo * nseg)()
+        st = self.lib.ssg_solve_helmholtz_segments(
+            self.h, int(var), nseg, seg.ctypes.data, lam.ctypes.data, _ptr(f), _ptr(u),
+            ep.ctypes.data, int(max_iter), infos)
+        self._check(st, "solve_helmholtz_segments", ok=(0, 5))
+        return u, [{"status": STATUS[st], "iterations": i.iterations, "residual": i.residual,
+                    "initial_residual": i.initial_residual} for i in infos]
+
     def conjugate_gradient(self, var, f, u, eps=1e-10, max_iter=5000, history=True):
         info = self._solve(self.lib.ssg_conjugate_gradient,
                            (self.h, var, _ptr(f), _ptr(u), eps, max_iter),
@@ -405,6 +423,14 @@ class Server:
         return out, STATUS.get(res.value, res.value), {
             "iterations": info.iterations, "residual": info.residual,
             "initial_residual": info.initial_residual, "latency_ms": info.solve_ms}
+
+    def set_batching(self, max_batch=16, max_points=65536):
+        """ssg_server_set_batching: shared-launch batches of up to max_batch
+        small (<= max_points points) Helmholtz requests of one order
+        (max_batch 1: off, the default)."""
+        self._check(self.lib.ssg_server_set_batching(self.h, int(max_batch),
+                                                     C.c_size_t(int(max_points))),
+                    "set_batching")
 
     def cancel(self, rid):
         self._check(self.lib.ssg_server_cancel(self.h, C.c_ulonglong(rid)), "cancel")

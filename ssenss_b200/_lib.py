@@ -55,6 +55,7 @@ class ServerStats(C.Structure):
         ("mesh_hits", C.c_ulonglong), ("mesh_misses", C.c_ulonglong),
         ("evictions", C.c_ulonglong),
         ("max_active_seen", C.c_int), ("resident_contexts", C.c_int),
+        ("batches", C.c_ulonglong), ("batched_requests", C.c_ulonglong),
     ]
 
 
@@ -91,6 +92,9 @@ SIGNATURES = [
                                          C.c_double, C.c_int, C.POINTER(SolveInfo)]),
     ("ssg_conjugate_gradient", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
                                          C.c_double, C.c_int, C.POINTER(SolveInfo)]),
+    ("ssg_solve_helmholtz_segments", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p,
+                                               C.c_void_p, C.c_void_p, C.c_void_p,
+                                               C.c_void_p, C.c_int, C.POINTER(SolveInfo)]),
     ("ssg_jacobi_preconditioner", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     ("ssg_multigrid_preconditioner", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p,
                                                C.c_double]),
@@ -113,6 +117,7 @@ SIGNATURES = [
     ("ssg_server_cancel", C.c_int, [C.c_void_p, C.c_ulonglong]),
     ("ssg_server_drain", C.c_int, [C.c_void_p, C.c_double]),
     ("ssg_server_get_stats", C.c_int, [C.c_void_p, C.POINTER(ServerStats)]),
+    ("ssg_server_set_batching", C.c_int, [C.c_void_p, C.c_int, C.c_size_t]),
     ("ssg_server_destroy", None, [C.c_void_p]),
     ("ssg_tuning", C.c_int, [C.c_int, _ip, _ip, _ip]),
     ("ssg_time_operator", C.c_int, [C.c_void_p, C.c_int, C.c_int, _dp]),

@@ -19,6 +19,14 @@
 //     its own CUDA stream and host thread; a request that arrives while
 //     others are on the GPU starts as soon as a slot and memory free up, and
 //     its kernels interleave with theirs on the device.
+//   * Shared launches (ssg_server_set_batching): when the head of the queue
+//     is a small Helmholtz request and the requests right behind it are
+//     small Helmholtz requests of the same order, up to max_batch of them
+//     run as one segmented solve (ssg_solve_helmholtz_segments) on a
+//     context built for their concatenated meshes: every operator and DSS
+//     launch of an iteration serves all of them, each with its own lambda,
+//     CG scalars and stop.  Off by default: a batched result agrees with
+//     the request's solo result to rounding, not bitwise.
 //   * Cancellation and deadlines: queued requests end at once; running ones
 //     at their next host synchronisation point (once per outer iteration).
 #include <cuda_runtime.h>
@@ -77,6 +85,8 @@ struct ssg_server {
   int device = 0;
   size_t budget = 0;
   int max_active = 1;
+  int max_batch = 1;                 // > 1: shared-launch Helmholtz batches
+  size_t batch_points = 0;           // largest request (points) that batches
   std::mutex mu;
   std::condition_variable cv;        // queue / budget / completion changes
   std::deque<Request*> queue;
@@ -91,6 +101,7 @@ struct ssg_server {
   std::vector<double> lat_ms, queue_ms;
   unsigned long long submitted = 0, completed = 0, failed = 0, cancelled = 0, rejected = 0;
   unsigned long long hits = 0, misses = 0, evictions = 0;
+  unsigned long long batches = 0, batched = 0;
   double t_first = 0, t_last = 0;
 };
 
@@ -140,9 +151,33 @@ void finish_request(ssg_server* S, Request* r, ssg_status st) {
   }
 }
 
+bool batchable(const ssg_server* S, const Request* r) {
+  return S->max_batch > 1 && r->d.lambda > 0.0 && !r->d.relative && !r->cancel &&
+         (size_t)r->d.nel * r->d.n * r->d.n * r->d.n <= S->batch_points;
+}
+
+// evict idle contexts, least recently used first, until `need` fits; false
+// when it cannot fit yet (lock held)
+bool make_room(ssg_server* S, size_t need, std::vector<ssg_context*>& evict) {
+  while (S->in_use + need > S->budget) {
+    auto lru = S->resident.end();
+    for (auto it = S->resident.begin(); it != S->resident.end(); ++it)
+      if (!it->busy && (lru == S->resident.end() || it->last_used < lru->last_used)) lru = it;
+    if (lru == S->resident.end()) break;
+    S->in_use -= lru->bytes;
+    evict.push_back(lru->ctx);
+    S->resident.erase(lru);
+    ++S->evictions;
+  }
+  return S->in_use + need <= S->budget;
+}
+
 // Decide for the head of the queue (lock held).  Returns the request to run
 // and the resident slot it uses (new ones already reserved), or nullptr.
-Request* admit(ssg_server* S, Resident** slot, std::vector<ssg_context*>& evict) {
+// A shared-launch batch: *batch receives its requests (the head first) and
+// *batch_bytes the bytes reserved for its context; *slot stays null.
+Request* admit(ssg_server* S, Resident** slot, std::vector<ssg_context*>& evict,
+               std::vector<Request*>* batch, size_t* batch_bytes) {
   while (!S->queue.empty()) {
     Request* r = S->queue.front();
     if (r->cancel) {
@@ -158,6 +193,33 @@ Request* admit(ssg_server* S, Resident** slot, std::vector<ssg_context*>& evict)
       continue;
     }
     if (S->active >= S->max_active) return nullptr;
+    // small Helmholtz requests of one order queued back to back: one
+    // shared-launch batch (arrival order kept: only the run at the head)
+    if (batchable(S, r)) {
+      std::vector<Request*> b{r};
+      int nel = r->d.nel;
+      for (size_t i = 1; i < S->queue.size() && (int)b.size() < S->max_batch; ++i) {
+        Request* q = S->queue[i];
+        if (!batchable(S, q) || q->d.n != r->d.n) break;
+        b.push_back(q);
+        nel += q->d.nel;
+      }
+      if (b.size() >= 2) {
+        const size_t need = estimate_bytes(r->d.n, nel, SSG_PRECISION_FP64) +
+                            (size_t)nel * r->d.n * r->d.n * r->d.n * 12 * sizeof(double);
+        if (need <= S->budget) {
+          if (!make_room(S, need, evict)) return nullptr;   // wait for a completion
+          S->in_use += need;
+          S->peak = std::max(S->peak, S->in_use);
+          for (size_t k = 0; k < b.size(); ++k) S->queue.pop_front();
+          *batch = std::move(b);
+          *batch_bytes = need;
+          ++S->batches;
+          S->batched += batch->size();
+          return r;
+        }
+      }
+    }
     // an idle resident context of this mesh and precision
     if (r->d.mesh_key != 0)
       for (auto& x : S->resident)
@@ -176,17 +238,7 @@ Request* admit(ssg_server* S, Resident** slot, std::vector<ssg_context*>& evict)
       continue;
     }
     // evict idle contexts, least recently used first, until it fits
-    while (S->in_use + need > S->budget) {
-      auto lru = S->resident.end();
-      for (auto it = S->resident.begin(); it != S->resident.end(); ++it)
-        if (!it->busy && (lru == S->resident.end() || it->last_used < lru->last_used)) lru = it;
-      if (lru == S->resident.end()) break;
-      S->in_use -= lru->bytes;
-      evict.push_back(lru->ctx);
-      S->resident.erase(lru);
-      ++S->evictions;
-    }
-    if (S->in_use + need > S->budget) return nullptr;   // wait for a completion
+    if (!make_room(S, need, evict)) return nullptr;   // wait for a completion
     S->in_use += need;
     S->peak = std::max(S->peak, S->in_use);
     Resident res;
@@ -243,16 +295,60 @@ ssg_status run_request(ssg_server* S, Request* r, Resident* slot) {
   return st;
 }
 
+// A shared-launch batch: the requests' meshes concatenated in one context
+// (built for the batch and dropped after it), solved as segments.
+ssg_status run_batch(ssg_server* S, std::vector<Request*>& b) {
+  const int n = b[0]->d.n;
+  const size_t nt = (size_t)n * n * n;
+  std::vector<double> vert, f, lam, eps;
+  std::vector<int> neigh, first{0};
+  for (Request* r : b) {
+    const int off = first.back();
+    vert.insert(vert.end(), r->vert.begin(), r->vert.end());
+    for (int v : r->neigh) neigh.push_back(v >= 0 ? v + off : v);
+    f.insert(f.end(), r->rhs.begin(), r->rhs.end());
+    lam.push_back(r->d.lambda);
+    eps.push_back(r->d.eps);
+    first.push_back(off + r->d.nel);
+  }
+  const int nel = first.back();
+  ssg_context* c = nullptr;
+  SSG_TRY(ssg_create(S->device, &c));
+  ssg_set_setup_options(c, SSG_SETUP_NO_DEALIAS | SSG_SETUP_NO_PARTICLES |
+                               SSG_SETUP_OPPOSITE_PAIRING);
+  ssg_status st = ssg_setup_mesh(c, n, nel, vert.data(), neigh.data());
+  std::vector<double> u((size_t)nel * nt, 0.0);
+  std::vector<ssg_solve_info> info(b.size());
+  int max_iter = 0;
+  for (Request* r : b) max_iter = std::max(max_iter, r->d.max_iter > 0 ? r->d.max_iter : 5000);
+  if (st == SSG_OK) {
+    c->cancel = &b[0]->cancel;
+    st = ssg_solve_helmholtz_segments(c, SSG_X_VELOCITY, (int)b.size(), first.data(), lam.data(),
+                                      f.data(), u.data(), eps.data(), max_iter, info.data());
+    c->cancel = nullptr;
+  }
+  ssg_destroy(c);
+  if (st != SSG_OK && st != SSG_MAXITER) return st;
+  for (size_t k = 0; k < b.size(); ++k) {
+    Request* r = b[k];
+    std::memcpy(r->out, u.data() + (size_t)first[k] * nt, sizeof(double) * r->d.nel * nt);
+    r->info = info[k];
+  }
+  return SSG_OK;
+}
+
 void worker(ssg_server* S) {
   cudaSetDevice(S->device);
   std::unique_lock<std::mutex> lk(S->mu);
   for (;;) {
     Resident* slot = nullptr;
     std::vector<ssg_context*> evict;
+    std::vector<Request*> batch;
+    size_t batch_bytes = 0;
     Request* r = nullptr;
     S->cv.wait(lk, [&] {
       if (S->stop && S->queue.empty()) return true;
-      r = admit(S, &slot, evict);
+      r = admit(S, &slot, evict, &batch, &batch_bytes);
       return r != nullptr || !evict.empty();
     });
     if (!r && evict.empty() && S->stop && S->queue.empty()) return;
@@ -266,6 +362,23 @@ void worker(ssg_server* S) {
     ++S->active;
     S->max_active_seen = std::max(S->max_active_seen, S->active);
     r->t_start = now_s();
+    if (!batch.empty()) {
+      for (Request* q : batch) q->t_start = r->t_start;
+      lk.unlock();
+      for (ssg_context* c : evict) ssg_destroy(c);
+      const ssg_status bst = run_batch(S, batch);
+      lk.lock();
+      --S->active;
+      S->in_use -= batch_bytes;
+      for (Request* q : batch) {
+        // each request's own outcome: its segment's stop
+        ssg_status qs = bst;
+        if (bst == SSG_OK && !(q->info.residual <= q->d.eps)) qs = SSG_MAXITER;
+        finish_request(S, q, qs);
+      }
+      S->cv.notify_all();
+      continue;
+    }
     lk.unlock();
     for (ssg_context* c : evict) ssg_destroy(c);
     const ssg_status st = run_request(S, r, slot);
@@ -333,6 +446,15 @@ ssg_status ssg_server_create(int device, size_t hbm_budget, int max_active, ssg_
   S->max_active = max_active;
   for (int i = 0; i < max_active; ++i) S->workers.emplace_back(worker, S);
   *out = S;
+  return SSG_OK;
+}
+
+ssg_status ssg_server_set_batching(ssg_server* S, int max_batch, size_t max_points) {
+  if (!S || max_batch < 1 || max_batch > 1024) return SSG_ERR_ARG;
+  std::lock_guard<std::mutex> lk(S->mu);
+  S->max_batch = max_batch;
+  S->batch_points = max_points;
+  S->cv.notify_all();
   return SSG_OK;
 }
 
@@ -438,6 +560,8 @@ ssg_status ssg_server_get_stats(ssg_server* S, ssg_server_stats* o) {
   o->evictions = S->evictions;
   o->max_active_seen = S->max_active_seen;
   o->resident_contexts = (int)S->resident.size();
+  o->batches = S->batches;
+  o->batched_requests = S->batched;
   return SSG_OK;
 }
 

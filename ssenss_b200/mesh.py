@@ -175,6 +175,26 @@ def box_mesh(shape, lo=(0.0, 0.0, 0.0), hi=(2 * math.pi,) * 3,
                 (nx, ny, nz))
 
 
+def concat_meshes(meshes) -> tuple:
+    """Independent meshes as one mesh: elements of mesh k follow those of
+    meshes 0 .. k-1, neighbour ids shifted by the element offset, wall codes
+    kept.  Returns (mesh, seg_first) with seg_first[k] the first element of
+    mesh k and seg_first[-1] the total (the segment table of
+    ssg_solve_helmholtz_segments)."""
+    first = [0]
+    verts, neigh = [], []
+    for m in meshes:
+        off = first[-1]
+        verts.append(np.asarray(m.vertices, dtype=np.float64))
+        nb = np.asarray(m.neigh, dtype=np.int32).copy()
+        nb[nb >= 0] += off
+        neigh.append(nb)
+        first.append(off + m.nel)
+    mesh = Mesh(np.concatenate(verts), np.concatenate(neigh), (first[-1], 1, 1),
+                "concatenation of " + ", ".join(m.description or "mesh" for m in meshes))
+    return mesh, np.array(first, dtype=np.int32)
+
+
 def tgv_box(nel_per_dir: int) -> Mesh:
     """Triply periodic [0, 2 pi]^3 box of equal hexahedra (Taylor-Green)."""
     m = box_mesh((nel_per_dir,) * 3)

@@ -189,3 +189,102 @@ def test_small_boxes_against_assembled_oracle(shape, n, lam):
     if lam == 0:
         u, u_b = u - u.mean(), u_b - u_b.mean()
     assert rel(u, u_b) < 1e-8, (rel(u, u_b), info)
+
+
+# segments of one shared-launch Helmholtz solve: (shape, lambda, eps) at n = 6
+SEGMENTS = [((3, 3, 3), 3.0, 1e-10), ((4, 3, 3), 40.0, 1e-10), ((3, 4, 3), 0.7, 1e-9),
+            ((3, 3, 5), 12.5, 1e-10), ((5, 3, 3), 99.0, 1e-10)]
+
+
+def test_segmented_helmholtz_matches_solo():
+    """ssg_solve_helmholtz_segments: five independent boxes (different
+    shapes, lambdas and stops) concatenated in one context share every
+    operator and DSS launch; each segment against its own solo
+    ssg_solve_helmholtz_cg: the same iteration count (one apart only with
+    both final residuals within a factor 2 of the segment's eps), solution
+    within 1e-11 relative.  The segment's sums are grouped differently from
+    the solo solve's, so rounding, not bitwise."""
+    from ssenss_b200.mesh import concat_meshes
+    n = 6
+    meshes, fs, solo = [], [], []
+    for k, (shape, lam, eps) in enumerate(SEGMENTS):
+        mesh = box_mesh(shape)
+        f = periodic_box_fourier_rhs(shape, n, 300 + k)
+        ctx = S.Context(0)
+        try:
+            ctx.set_parameters(11.0 / (6.0 * lam), 1.0, 1.0)
+            ctx.set_setup_options(no_dealias=True, no_particles=True, opposite_pairing=True)
+            ctx.setup_mesh(mesh, n)
+            u, info = ctx.solve_helmholtz_cg(S.X_VELOCITY, f, np.zeros_like(f), eps=eps,
+                                             history=False)
+        finally:
+            ctx.close()
+        meshes.append(mesh)
+        fs.append(f)
+        solo.append((u.copy(), info))
+    big, first = concat_meshes(meshes)
+    ctx = S.Context(0)
+    try:
+        ctx.set_setup_options(no_dealias=True, no_particles=True, opposite_pairing=True)
+        ctx.setup_mesh(big, n)
+        f = np.concatenate(fs)
+        u, infos = ctx.solve_helmholtz_segments(S.X_VELOCITY, first, [s[1] for s in SEGMENTS],
+                                                f, np.zeros_like(f), [s[2] for s in SEGMENTS])
+        for k, (shape, lam, eps) in enumerate(SEGMENTS):
+            us, inf = solo[k]
+            ub = u[first[k]:first[k + 1]]
+            ib = infos[k]
+            print(f"segment {k} {shape} lambda {lam}: iterations {ib['iterations']} "
+                  f"(solo {inf['iterations']}), residual {ib['residual']:.3e} "
+                  f"(solo {inf['residual']:.3e}), solution {rel(ub, us):.2e}")
+            assert ib["status"] == "SSG_OK" and ib["residual"] <= eps
+            if ib["iterations"] != inf["iterations"]:
+                assert abs(ib["iterations"] - inf["iterations"]) == 1
+                assert max(ib["residual"], inf["residual"]) <= 2 * eps
+            assert rel(ub, us) < 1e-11
+            assert ib["initial_residual"] == pytest.approx(inf["initial_residual"], rel=1e-12)
+        # a segment table that splits a mesh (an element neighbouring
+        # another segment) is refused
+        bad = np.array([0, 10, big.nel], dtype=np.int32)
+        with pytest.raises(S.SsgError):
+            ctx.solve_helmholtz_segments(S.X_VELOCITY, bad, [1.0, 2.0], f, np.zeros_like(f),
+                                         [1e-10, 1e-10])
+    finally:
+        ctx.close()
+
+
+def test_shared_launch_batches_match_solo():
+    """ssg_server_set_batching: a burst of small Helmholtz requests of one
+    order (different boxes and lambdas) behind a one-slot server runs in
+    shared-launch batches; every request against the same request solved
+    alone by a server without batching: status OK, solution within 1e-11
+    relative (the batch groups each segment's sums differently)."""
+    n = 6
+    shapes = [(3, 3, 3), (4, 3, 3), (3, 4, 3), (3, 3, 4)]
+    reqs = [(shapes[k % 4], 0.5 + 9.5 * k) for k in range(10)]
+    fs = [periodic_box_fourier_rhs(sh, n, 500 + k) for k, (sh, _) in enumerate(reqs)]
+
+    def run(batching):
+        srv = S.Server(0, hbm_budget=20e9, max_active=1)
+        try:
+            if batching:
+                srv.set_batching(8, 1 << 20)
+            ids = [srv.submit(box_mesh(sh), n, fs[k], lam=lam, eps=1e-10, precision="fp64")
+                   for k, (sh, lam) in enumerate(reqs)]
+            out = [srv.wait(r) for r in ids]
+            return out, srv.stats()
+        finally:
+            srv.close()
+
+    solo, st0 = run(False)
+    batched, st1 = run(True)
+    assert st0["batches"] == 0
+    print(f"shared launches: {st1['batches']} batches holding {st1['batched_requests']} of "
+          f"{len(reqs)} requests")
+    assert st1["batches"] >= 1 and st1["batched_requests"] >= 2
+    assert st1["completed"] == len(reqs)
+    for k in range(len(reqs)):
+        (ua, sa, ia), (ub, sb, ib) = solo[k], batched[k]
+        assert sa == "SSG_OK" and sb == "SSG_OK", (k, sa, sb)
+        assert ib["residual"] <= 1e-10
+        assert rel(ub, ua) < 1e-11, k
