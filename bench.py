@@ -420,7 +420,9 @@ def run_serving(args, device):
                 "mesh_misses": st["mesh_misses"], "evictions": st["evictions"],
                 "max_in_flight": st["max_active_seen"]}
 
+    burst = None if args.serve_open_only else run_burst(device)
     return {
+        "shared_launch_burst": burst,
         "workload": (f"{len(stream)} requests ({npois} Poisson FCG+p-MG, "
                      f"{len(stream) - npois} Helmholtz CG-Jacobi), periodic boxes E "
                      f"log-uniform in [8, 4096] rounded to near-cubes a*b*c from 2*2*2 "
@@ -434,6 +436,53 @@ def run_serving(args, device):
         "max_rel_diff_mixed_vs_fp64": diff,
         "slots": args.serve_slots,
     }
+
+
+def run_burst(device, nreq=64, n=8):
+    """A burst of small Helmholtz requests of one order (periodic boxes of 8 to
+    64 elements, n = 8, lambda in (0, 100]) submitted at once: one slot
+    without batching, eight slots without batching (overlap on streams), and
+    one slot with shared-launch batches of up to 16 requests
+    (ssg_server_set_batching).  The burst runs once to warm the resident
+    contexts, then timed; batches build their context every time."""
+    import numpy as np
+    import ssenss_b200 as S
+    from ssenss_b200.mesh import box_mesh, periodic_box_fourier_rhs
+    rng = np.random.default_rng(17)
+    shapes = [(2, 2, 2), (2, 2, 3), (3, 3, 3), (2, 4, 4), (4, 4, 4), (3, 3, 2)]
+    reqs = []
+    for k in range(nreq):
+        sh = shapes[int(rng.integers(len(shapes)))]
+        reqs.append((sh, float(rng.uniform(0.5, 100.0)), periodic_box_fourier_rhs(sh, n, 900 + k)))
+    meshes = {sh: box_mesh(sh) for sh in shapes}
+
+    def once(slots, batch):
+        srv = S.Server(device, hbm_budget=40e9, max_active=slots)
+        if batch:
+            srv.set_batching(16, 1 << 16)
+        out = None
+        for _ in range(2):
+            t0 = time.perf_counter()
+            ids = [srv.submit(meshes[sh], n, f, lam=lam, eps=EPS, precision="fp64")
+                   for sh, lam, f in reqs]
+            out = [srv.wait(r) for r in ids]
+            wall = time.perf_counter() - t0
+        st = srv.stats()
+        srv.close()
+        return out, {"solves_per_s": nreq / wall, "wall_ms": 1e3 * wall,
+                     "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
+                     "batches": st["batches"], "batched_requests": st["batched_requests"],
+                     "failed": sum(1 for o in out if o[1] != "SSG_OK")}
+
+    ref, one = once(1, False)
+    _, eight = once(8, False)
+    bat, batched = once(1, True)
+    diff = max(float(np.abs(a[0] - b[0]).max() / max(np.abs(a[0]).max(), 1e-300))
+               for a, b in zip(bat, ref))
+    return {"workload": f"{nreq} Helmholtz requests at once, n = {n}, periodic boxes of 8 to "
+                        f"64 elements, lambda in (0, 100], stop {EPS} absolute, FP64",
+            "one_slot": one, "eight_slots": eight, "one_slot_shared_launches": batched,
+            "max_rel_diff_batched_vs_one_slot": diff}
 
 
 # ---------------------------------------------------------------------------
