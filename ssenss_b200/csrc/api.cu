@@ -72,6 +72,11 @@ static void free_mesh(ssg_context* c) {
     free_workspace(c->ws);
     c->ws = nullptr;
   }
+  if (c->seg) {
+    seg_scratch_free(*c->seg);
+    delete c->seg;
+    c->seg = nullptr;
+  }
   for (auto& l : c->lev) free_level(l);
   dfree(c->d_pairs); c->d_pairs = nullptr;
   dfree(c->inv_mass); c->inv_mass = nullptr;

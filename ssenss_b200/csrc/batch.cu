@@ -228,6 +228,26 @@ __global__ void __launch_bounds__(kSegThreads) k_seg_p(SegArgs a, double* __rest
   }
 }
 
+// one context's DSS map (dss_map_table layout: gather words, then per
+// element records) into a concatenation's map at point offset P and element
+// offset E: every point index (>= 0) moves by P, record codes and -1 stay
+__global__ void k_dss_map_shift(const int* __restrict__ src, size_t npts, size_t head,
+                                size_t rec_ints, int* __restrict__ dst, size_t P,
+                                size_t head_dst, size_t rec_dst) {
+  const size_t n = npts + rec_ints;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    if (i < npts) {
+      const int w = src[i];
+      dst[P + i] = w >= 0 ? w + (int)P : w;
+    } else {
+      const size_t k = i - npts;
+      const int v = src[head + k];
+      dst[head_dst + rec_dst + k] = v >= 0 ? v + (int)P : v;
+    }
+  }
+}
+
 // bj_s = lambda_s bj over one segment's points
 __global__ void k_seg_scale(size_t lo, size_t n, double lam, const double* __restrict__ bj,
                             double* __restrict__ out) {
@@ -239,32 +259,219 @@ __global__ void k_seg_scale(size_t lo, size_t n, double lam, const double* __res
 }  // namespace dev
 }  // namespace ssg
 
-using namespace ssg;
+namespace ssg {
 
 namespace {
 
-struct SegBuffers {
-  ssg_context* c;
-  std::vector<void*> ptrs;
-  explicit SegBuffers(ssg_context* cc) : c(cc) {}
-  template <typename T>
-  ssg_status get(T** p, size_t count) {
-    void* q = nullptr;
-    if (cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T)) != cudaSuccess) {
-      cudaGetLastError();
-      return fail(c, SSG_ERR_NOMEM, "segmented solve buffers");
-    }
-    ptrs.push_back(q);
-    *p = static_cast<T*>(q);
-    return SSG_OK;
+template <typename T>
+ssg_status seg_alloc(ssg_context* c, T** p, size_t count) {
+  void* q = nullptr;
+  if (cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T)) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(c, SSG_ERR_NOMEM, "segmented solve scratch");
   }
-  ~SegBuffers() {
-    cudaStreamSynchronize(c->stream);
-    for (void* q : ptrs) cudaFree(q);
+  *p = static_cast<T*>(q);
+  return SSG_OK;
+}
+
+template <typename T>
+void seg_release(T*& p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+
+// capacity for nch chunks, nseg segments and np points (grown, never shrunk;
+// a grown group is reallocated whole, contents not kept)
+ssg_status seg_reserve(ssg_context* c, SegScratch& W, size_t nch, size_t nseg, size_t np) {
+  if (nch > W.cap_chunks) {
+    seg_release(W.chunk_seg);
+    seg_release(W.chunk_n);
+    seg_release(W.chunk_lo);
+    seg_release(W.part);
+    W.cap_chunks = 0;
+    SSG_TRY(seg_alloc(c, &W.chunk_seg, nch));
+    SSG_TRY(seg_alloc(c, &W.chunk_n, nch));
+    SSG_TRY(seg_alloc(c, &W.chunk_lo, nch));
+    SSG_TRY(seg_alloc(c, &W.part, 4 * nch));
+    W.cap_chunks = nch;
   }
-};
+  if (nseg > W.cap_segs) {
+    seg_release(W.seg_chunk0);
+    seg_release(W.sc);
+    W.cap_segs = 0;
+    SSG_TRY(seg_alloc(c, &W.seg_chunk0, nseg + 1));
+    SSG_TRY(seg_alloc(c, &W.sc, (size_t)dev::SG_SIZE * nseg));
+    W.cap_segs = nseg;
+  }
+  if (!W.active) SSG_TRY(seg_alloc(c, &W.active, 1));
+  if (np > W.cap_points) {
+    double** vecs[] = {&W.bj_s, &W.dinv_s, &W.x, &W.r, &W.z, &W.p, &W.ap, &W.aploc, &W.f};
+    for (double** v : vecs) seg_release(*v);
+    W.cap_points = 0;
+    for (double** v : vecs) SSG_TRY(seg_alloc(c, v, np));
+    W.cap_points = np;
+  }
+  return SSG_OK;
+}
 
 }  // namespace
+
+void seg_scratch_free(SegScratch& W) {
+  seg_release(W.chunk_seg);
+  seg_release(W.chunk_n);
+  seg_release(W.chunk_lo);
+  seg_release(W.part);
+  seg_release(W.seg_chunk0);
+  seg_release(W.sc);
+  seg_release(W.active);
+  double** vecs[] = {&W.bj_s, &W.dinv_s, &W.x, &W.r, &W.z, &W.p, &W.ap, &W.aploc, &W.f};
+  for (double** v : vecs) seg_release(*v);
+  W = SegScratch();
+}
+
+ssg_status seg_solve(ssg_context* c, const SegLevel& L, SegScratch& W, int nseg,
+                     const int* seg_first, const double* lambda, const double* f, double* u,
+                     const double* eps, int max_iter, ssg_solve_info* info) {
+  const size_t np = L.npts, nt = L.nt;
+  cudaStream_t s = c->stream;
+  // chunk tables: fixed chunks of points inside each segment
+  std::vector<int> chunk_seg, chunk_n, seg_chunk0(nseg + 1);
+  std::vector<size_t> chunk_lo;
+  for (int sg = 0; sg < nseg; ++sg) {
+    seg_chunk0[sg] = (int)chunk_seg.size();
+    const size_t lo = (size_t)seg_first[sg] * nt, hi = (size_t)seg_first[sg + 1] * nt;
+    for (size_t q = lo; q < hi; q += dev::kSegChunk) {
+      chunk_seg.push_back(sg);
+      chunk_lo.push_back(q);
+      chunk_n.push_back((int)std::min<size_t>(dev::kSegChunk, hi - q));
+    }
+  }
+  seg_chunk0[nseg] = (int)chunk_seg.size();
+  const int nch = (int)chunk_seg.size();
+  SSG_TRY(seg_reserve(c, W, nch, nseg, np));
+
+  SSG_CUDA(c, cudaMemcpyAsync(W.chunk_seg, chunk_seg.data(), nch * sizeof(int),
+                              cudaMemcpyHostToDevice, s));
+  SSG_CUDA(c, cudaMemcpyAsync(W.chunk_n, chunk_n.data(), nch * sizeof(int),
+                              cudaMemcpyHostToDevice, s));
+  SSG_CUDA(c, cudaMemcpyAsync(W.chunk_lo, chunk_lo.data(), nch * sizeof(size_t),
+                              cudaMemcpyHostToDevice, s));
+  SSG_CUDA(c, cudaMemcpyAsync(W.seg_chunk0, seg_chunk0.data(), (nseg + 1) * sizeof(int),
+                              cudaMemcpyHostToDevice, s));
+  std::vector<double> sc((size_t)dev::SG_SIZE * nseg, 0.0);
+  for (int sg = 0; sg < nseg; ++sg) sc[(size_t)dev::SG_SIZE * sg + dev::SG_EPS] = eps[sg];
+  SSG_CUDA(c, cudaMemcpyAsync(W.sc, sc.data(), sc.size() * sizeof(double),
+                              cudaMemcpyHostToDevice, s));
+  SSG_CUDA(c, cudaMemcpyAsync(W.f, f, np * sizeof(double), cudaMemcpyDefault, s));
+  SSG_CUDA(c, cudaMemcpyAsync(W.x, u, np * sizeof(double), cudaMemcpyDefault, s));
+  dev::SegArgs a;
+  a.chunk_seg = W.chunk_seg;
+  a.chunk_lo = W.chunk_lo;
+  a.chunk_n = W.chunk_n;
+  a.seg_chunk0 = W.seg_chunk0;
+  a.part = W.part;
+  a.sc = W.sc;
+  a.active = W.active;
+  a.nseg = nseg;
+  a.max_iter = max_iter;
+
+  // per segment: lambda_s bj for the operator (lambda 1 in the kernel) and
+  // the Jacobi inverse 1 / DSS(kdiag + (lambda_s rho) J) (src/helmholtz.c:
+  // 51-68, src/precon.c:336-359)
+  for (int sg = 0; sg < nseg; ++sg) {
+    const size_t lo = (size_t)seg_first[sg] * nt;
+    const size_t n = (size_t)(seg_first[sg + 1] - seg_first[sg]) * nt;
+    count_launch();
+    dev::k_seg_scale<<<vec_blocks(n), 256, 0, s>>>(lo, n, lambda[sg], L.bj, W.bj_s);
+    SSG_CUDA(c, cudaGetLastError());
+    SSG_CUDA(c, run_helm_diag(s, n, nt, L.kdiag + lo, L.rho, L.det + lo, lambda[sg],
+                              W.aploc + lo));
+  }
+  SSG_CUDA(c, run_dss(s, DSS_PLAIN, false, L.n, L.nel, W.aploc, W.dinv_s, nullptr, L.dss,
+                      nullptr, nullptr, nullptr, nullptr));
+  SSG_CUDA(c, run_recip(s, np, W.dinv_s));
+
+  // mask f; r = f - DSS(mask A x); z = dinv r; p = z; rdz
+  if (L.mask) SSG_CUDA(c, run_mul(s, false, np, W.f, L.mask));
+  auto op = [&](const double* in) -> ssg_status {
+    SSG_CUDA(c, run_ax(s, L.n, L.nel, 0, true, false, in, W.aploc, L.gf, np, W.bj_s, L.D, L.S,
+                       1.0, nullptr));
+    SSG_CUDA(c, run_dss(s, DSS_PLAIN, false, L.n, L.nel, W.aploc, W.ap, nullptr, L.dss, L.mask,
+                        nullptr, nullptr, nullptr));
+    return SSG_OK;
+  };
+  SSG_TRY(op(W.x));
+  count_launch();
+  dev::k_seg_init<<<nch, dev::kSegThreads, 0, s>>>(a, W.f, W.ap, W.dinv_s, L.mult, W.r, W.z,
+                                                   W.p);
+  SSG_CUDA(c, cudaGetLastError());
+  count_launch();
+  dev::k_seg_init_finish<<<(nseg + 255) / 256, 256, 0, s>>>(a);
+  SSG_CUDA(c, cudaGetLastError());
+
+  // iterations, enqueued in chunks of 8 with a host check of the active
+  // count between chunks
+  for (int it = 0; it < max_iter; ++it) {
+    SSG_TRY(op(W.p));
+    count_launch();
+    dev::k_seg_pap<<<nch, dev::kSegThreads, 0, s>>>(a, W.p, W.ap, L.mult);
+    count_launch();
+    dev::k_seg_update<<<nch, dev::kSegThreads, 0, s>>>(a, W.x, W.p, W.r, W.ap, W.dinv_s, L.mult,
+                                                       W.z);
+    count_launch();
+    dev::k_seg_finish<<<1, 1024, 0, s>>>(a);
+    count_launch();
+    dev::k_seg_p<<<nch, dev::kSegThreads, 0, s>>>(a, W.p, W.z, L.mask);
+    SSG_CUDA(c, cudaGetLastError());
+    if (it % 8 == 7 || it == max_iter - 1) {
+      SSG_CUDA(c, cudaMemcpyAsync(c->h_pin, W.active, sizeof(int), cudaMemcpyDeviceToHost, s));
+      SSG_CUDA(c, cudaStreamSynchronize(s));
+      int act = 0;
+      std::memcpy(&act, c->h_pin, sizeof(int));
+      if (c->cancel && *c->cancel) return fail(c, SSG_ERR_CANCELLED, "solve cancelled");
+      if (act == 0) break;
+    }
+  }
+  SSG_CUDA(c, cudaMemcpyAsync(u, W.x, np * sizeof(double), cudaMemcpyDefault, s));
+  SSG_CUDA(c, cudaMemcpyAsync(sc.data(), W.sc, sc.size() * sizeof(double),
+                              cudaMemcpyDeviceToHost, s));
+  SSG_CUDA(c, cudaStreamSynchronize(s));
+  ssg_status st = SSG_OK;
+  for (int sg = 0; sg < nseg; ++sg) {
+    const double* q = sc.data() + (size_t)dev::SG_SIZE * sg;
+    info[sg].iterations = (int)q[dev::SG_ITER];
+    info[sg].residual = q[dev::SG_ERR];
+    info[sg].initial_residual = q[dev::SG_R0];
+    info[sg].solve_ms = 0.0;
+    info[sg].history_len = 0;
+    if (!std::isfinite(q[dev::SG_ERR]))
+      st = SSG_NONFINITE;
+    else if (!(q[dev::SG_ERR] <= eps[sg]) && st == SSG_OK)
+      st = SSG_MAXITER;
+  }
+  return st;
+}
+
+size_t dss_record_ints(int n) {
+  const int I = n > 2 ? n - 2 : 0;
+  return (size_t)12 * I * 4 + 8 * 8;
+}
+
+cudaError_t run_dss_map_shift(cudaStream_t s, const int* src, int n, int nel, int* dst,
+                              size_t P, size_t npts_dst, int E) {
+  const size_t nt = (size_t)n * n * n, npts = nt * nel;
+  const size_t rec = dss_record_ints(n);
+  const size_t total = npts + rec * nel;
+  count_launch();
+  dev::k_dss_map_shift<<<vec_blocks(total), 256, 0, s>>>(
+      src, npts, dss_map_records_offset(npts), rec * nel, dst, P,
+      dss_map_records_offset(npts_dst), rec * (size_t)E);
+  return cudaGetLastError();
+}
+
+}  // namespace ssg
+
+using namespace ssg;
 
 extern "C" ssg_status ssg_solve_helmholtz_segments(ssg_context* c, int var, int nseg,
                                                    const int* seg_first, const double* lambda,
@@ -293,142 +500,22 @@ extern "C" ssg_status ssg_solve_helmholtz_segments(ssg_context* c, int var, int 
       }
   }
   SSG_CUDA(c, cudaSetDevice(c->device));
-  SSG_TRY(ensure_workspace(c));
-  const DevLevel& L = c->lev[0];
-  const size_t np = L.npts, nt = L.nt;
-  cudaStream_t s = c->stream;
-
-  // chunk tables: fixed chunks of points inside each segment
-  std::vector<int> chunk_seg, chunk_n, seg_chunk0(nseg + 1);
-  std::vector<size_t> chunk_lo;
-  for (int sg = 0; sg < nseg; ++sg) {
-    seg_chunk0[sg] = (int)chunk_seg.size();
-    const size_t lo = (size_t)seg_first[sg] * nt, hi = (size_t)seg_first[sg + 1] * nt;
-    for (size_t q = lo; q < hi; q += dev::kSegChunk) {
-      chunk_seg.push_back(sg);
-      chunk_lo.push_back(q);
-      chunk_n.push_back((int)std::min<size_t>(dev::kSegChunk, hi - q));
-    }
-  }
-  seg_chunk0[nseg] = (int)chunk_seg.size();
-  const int nch = (int)chunk_seg.size();
-
-  SegBuffers B(c);
-  dev::SegArgs a;
-  int *d_cs, *d_cn, *d_s0, *d_act;
-  size_t* d_lo;
-  double *d_part, *d_sc, *bj_s, *dinv_s, *x, *r, *z, *p, *ap, *aploc, *fd;
-  SSG_TRY(B.get(&d_cs, nch));
-  SSG_TRY(B.get(&d_cn, nch));
-  SSG_TRY(B.get(&d_lo, nch));
-  SSG_TRY(B.get(&d_s0, nseg + 1));
-  SSG_TRY(B.get(&d_act, 1));
-  SSG_TRY(B.get(&d_part, 4 * (size_t)nch));
-  SSG_TRY(B.get(&d_sc, dev::SG_SIZE * (size_t)nseg));
-  SSG_TRY(B.get(&bj_s, np));
-  SSG_TRY(B.get(&dinv_s, np));
-  SSG_TRY(B.get(&x, np));
-  SSG_TRY(B.get(&r, np));
-  SSG_TRY(B.get(&z, np));
-  SSG_TRY(B.get(&p, np));
-  SSG_TRY(B.get(&ap, np));
-  SSG_TRY(B.get(&aploc, np));
-  SSG_TRY(B.get(&fd, np));
-  SSG_CUDA(c, cudaMemcpyAsync(d_cs, chunk_seg.data(), nch * sizeof(int),
-                              cudaMemcpyHostToDevice, s));
-  SSG_CUDA(c, cudaMemcpyAsync(d_cn, chunk_n.data(), nch * sizeof(int), cudaMemcpyHostToDevice,
-                              s));
-  SSG_CUDA(c, cudaMemcpyAsync(d_lo, chunk_lo.data(), nch * sizeof(size_t),
-                              cudaMemcpyHostToDevice, s));
-  SSG_CUDA(c, cudaMemcpyAsync(d_s0, seg_chunk0.data(), (nseg + 1) * sizeof(int),
-                              cudaMemcpyHostToDevice, s));
-  {
-    std::vector<double> sc((size_t)dev::SG_SIZE * nseg, 0.0);
-    for (int sg = 0; sg < nseg; ++sg) sc[(size_t)dev::SG_SIZE * sg + dev::SG_EPS] = eps[sg];
-    SSG_CUDA(c, cudaMemcpyAsync(d_sc, sc.data(), sc.size() * sizeof(double),
-                                cudaMemcpyHostToDevice, s));
-  }
-  SSG_CUDA(c, cudaMemcpyAsync(fd, f, np * sizeof(double), cudaMemcpyDefault, s));
-  SSG_CUDA(c, cudaMemcpyAsync(x, u, np * sizeof(double), cudaMemcpyDefault, s));
-  a.chunk_seg = d_cs;
-  a.chunk_lo = d_lo;
-  a.chunk_n = d_cn;
-  a.seg_chunk0 = d_s0;
-  a.part = d_part;
-  a.sc = d_sc;
-  a.active = d_act;
-  a.nseg = nseg;
-  a.max_iter = max_iter;
-
-  // per segment: lambda_s bj for the operator (lambda 1 in the kernel) and
-  // the Jacobi inverse 1 / DSS(kdiag + (lambda_s rho) J) (src/helmholtz.c:
-  // 51-68, src/precon.c:336-359)
-  for (int sg = 0; sg < nseg; ++sg) {
-    const size_t lo = (size_t)seg_first[sg] * nt, n = (size_t)(seg_first[sg + 1] - seg_first[sg]) * nt;
-    count_launch();
-    dev::k_seg_scale<<<vec_blocks(n), 256, 0, s>>>(lo, n, lambda[sg], L.bj, bj_s);
-    SSG_CUDA(c, cudaGetLastError());
-    SSG_CUDA(c, run_helm_diag(s, n, nt, L.kdiag + lo, L.rho, L.det + lo, lambda[sg],
-                              aploc + lo));
-  }
-  SSG_CUDA(c, run_dss(s, DSS_PLAIN, false, L.n, c->nel, aploc, dinv_s, c->d_pairs, L.dss_ec,
-                      nullptr, nullptr, nullptr, nullptr));
-  SSG_CUDA(c, run_recip(s, np, dinv_s));
-
-  const double* mask = c->has_walls ? L.mask : nullptr;
-  // mask f; r = f - DSS(mask A x); z = dinv r; p = z; rdz
-  if (mask) SSG_CUDA(c, run_mul(s, false, np, fd, mask));
-  auto op = [&](const double* in) -> ssg_status {
-    SSG_CUDA(c, run_ax(s, L.n, c->nel, 0, true, false, in, aploc, L.gf, np, bj_s, L.D, L.S, 1.0,
-                       nullptr));
-    SSG_CUDA(c, run_dss(s, DSS_PLAIN, false, L.n, c->nel, aploc, ap, c->d_pairs, L.dss_ec, mask,
-                        nullptr, nullptr, nullptr));
-    return SSG_OK;
-  };
-  SSG_TRY(op(x));
-  count_launch();
-  dev::k_seg_init<<<nch, dev::kSegThreads, 0, s>>>(a, fd, ap, dinv_s, L.mult, r, z, p);
-  SSG_CUDA(c, cudaGetLastError());
-  count_launch();
-  dev::k_seg_init_finish<<<(nseg + 255) / 256, 256, 0, s>>>(a);
-  SSG_CUDA(c, cudaGetLastError());
-
-  // iterations, enqueued in chunks of 8 with a host check of the active
-  // count between chunks
-  for (int it = 0; it < max_iter; ++it) {
-    SSG_TRY(op(p));
-    count_launch();
-    dev::k_seg_pap<<<nch, dev::kSegThreads, 0, s>>>(a, p, ap, L.mult);
-    count_launch();
-    dev::k_seg_update<<<nch, dev::kSegThreads, 0, s>>>(a, x, p, r, ap, dinv_s, L.mult, z);
-    count_launch();
-    dev::k_seg_finish<<<1, 1024, 0, s>>>(a);
-    count_launch();
-    dev::k_seg_p<<<nch, dev::kSegThreads, 0, s>>>(a, p, z, mask);
-    SSG_CUDA(c, cudaGetLastError());
-    if (it % 8 == 7 || it == max_iter - 1) {
-      int act = 0;
-      SSG_CUDA(c, cudaMemcpyAsync(&act, d_act, sizeof(int), cudaMemcpyDeviceToHost, s));
-      SSG_CUDA(c, cudaStreamSynchronize(s));
-      if (c->cancel && *c->cancel) return fail(c, SSG_ERR_CANCELLED, "solve cancelled");
-      if (act == 0) break;
-    }
-  }
-  SSG_CUDA(c, cudaMemcpyAsync(u, x, np * sizeof(double), cudaMemcpyDefault, s));
-  std::vector<double> sc((size_t)dev::SG_SIZE * nseg);
-  SSG_CUDA(c, cudaMemcpyAsync(sc.data(), d_sc, sc.size() * sizeof(double),
-                              cudaMemcpyDeviceToHost, s));
-  SSG_CUDA(c, cudaStreamSynchronize(s));
-  ssg_status st = SSG_OK;
-  for (int sg = 0; sg < nseg; ++sg) {
-    const double* q = sc.data() + (size_t)dev::SG_SIZE * sg;
-    info[sg].iterations = (int)q[dev::SG_ITER];
-    info[sg].residual = q[dev::SG_ERR];
-    info[sg].initial_residual = q[dev::SG_R0];
-    info[sg].solve_ms = 0.0;
-    info[sg].history_len = 0;
-    if (!std::isfinite(q[dev::SG_ERR])) st = SSG_NONFINITE;
-    else if (!(q[dev::SG_ERR] <= eps[sg]) && st == SSG_OK) st = SSG_MAXITER;
-  }
-  return st;
+  const DevLevel& D = c->lev[0];
+  SegLevel L;
+  L.n = D.n;
+  L.nel = c->nel;
+  L.nt = D.nt;
+  L.npts = D.npts;
+  L.gf = D.gf;
+  L.bj = D.bj;
+  L.kdiag = D.kdiag;
+  L.rho = D.rho;
+  L.det = D.det;
+  L.mask = c->has_walls ? D.mask : nullptr;
+  L.D = D.D;
+  L.S = D.S;
+  L.mult = D.mult;
+  L.dss = D.dss_ec;
+  if (!c->seg) c->seg = new SegScratch();
+  return seg_solve(c, L, *c->seg, nseg, seg_first, lambda, f, u, eps, max_iter, info);
 }

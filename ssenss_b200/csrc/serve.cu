@@ -21,12 +21,13 @@
 //     its kernels interleave with theirs on the device.
 //   * Shared launches (ssg_server_set_batching): when the head of the queue
 //     is a small Helmholtz request and the requests right behind it are
-//     small Helmholtz requests of the same order, up to max_batch of them
-//     run as one segmented solve (ssg_solve_helmholtz_segments) on a
-//     context built for their concatenated meshes: every operator and DSS
-//     launch of an iteration serves all of them, each with its own lambda,
-//     CG scalars and stop.  Off by default: a batched result agrees with
-//     the request's solo result to rounding, not bitwise.
+//     small Helmholtz requests of the same order whose meshes have idle
+//     resident contexts, up to max_batch of them run as one segmented solve
+//     (seg_solve, batch.cu): their resident level-0 data is copied device to
+//     device into one concatenated level (a per-worker arena, reused), and
+//     every operator and DSS launch of an iteration serves all of them, each
+//     with its own lambda, CG scalars and stop.  Off by default: a batched
+//     result agrees with the request's solo result to rounding, not bitwise.
 //   * Cancellation and deadlines: queued requests end at once; running ones
 //     at their next host synchronisation point (once per outer iteration).
 #include <cuda_runtime.h>
@@ -62,6 +63,7 @@ struct Request {
   std::vector<int> neigh;
   std::vector<double> rhs;
   double* out = nullptr;
+  bool walls = false;          // a wall code in the neighbour table
   size_t bytes_est = 0;
   double t_submit = 0, t_start = 0, t_done = 0, deadline = 0;
   bool done = false;
@@ -152,7 +154,7 @@ void finish_request(ssg_server* S, Request* r, ssg_status st) {
 }
 
 bool batchable(const ssg_server* S, const Request* r) {
-  return S->max_batch > 1 && r->d.lambda > 0.0 && !r->d.relative && !r->cancel &&
+  return S->max_batch > 1 && r->d.lambda > 0.0 && !r->d.relative && !r->cancel && !r->walls &&
          (size_t)r->d.nel * r->d.n * r->d.n * r->d.n <= S->batch_points;
 }
 
@@ -175,9 +177,10 @@ bool make_room(ssg_server* S, size_t need, std::vector<ssg_context*>& evict) {
 // Decide for the head of the queue (lock held).  Returns the request to run
 // and the resident slot it uses (new ones already reserved), or nullptr.
 // A shared-launch batch: *batch receives its requests (the head first) and
-// *batch_bytes the bytes reserved for its context; *slot stays null.
+// *batch_slots the resident context each reads (marked busy); *slot stays
+// null.
 Request* admit(ssg_server* S, Resident** slot, std::vector<ssg_context*>& evict,
-               std::vector<Request*>* batch, size_t* batch_bytes) {
+               std::vector<Request*>* batch, std::vector<Resident*>* batch_slots) {
   while (!S->queue.empty()) {
     Request* r = S->queue.front();
     if (r->cancel) {
@@ -193,32 +196,40 @@ Request* admit(ssg_server* S, Resident** slot, std::vector<ssg_context*>& evict,
       continue;
     }
     if (S->active >= S->max_active) return nullptr;
-    // small Helmholtz requests of one order queued back to back: one
-    // shared-launch batch (arrival order kept: only the run at the head)
+    // small Helmholtz requests of one order queued back to back, each with
+    // an idle resident context of its mesh (or sharing one with an earlier
+    // member: the level data is only read): one shared-launch batch
+    // (arrival order kept: only the run at the head)
     if (batchable(S, r)) {
-      std::vector<Request*> b{r};
-      int nel = r->d.nel;
-      for (size_t i = 1; i < S->queue.size() && (int)b.size() < S->max_batch; ++i) {
+      std::vector<Request*> b;
+      std::vector<Resident*> sl;
+      for (size_t i = 0; i < S->queue.size() && (int)b.size() < S->max_batch; ++i) {
         Request* q = S->queue[i];
-        if (!batchable(S, q) || q->d.n != r->d.n) break;
+        if (!batchable(S, q) || q->d.n != r->d.n || q->d.mesh_key == 0) break;
+        Resident* x = nullptr;
+        for (size_t k = 0; k < b.size() && !x; ++k)
+          if (b[k]->d.mesh_key == q->d.mesh_key) x = sl[k];
+        if (!x)
+          for (auto& y : S->resident)
+            if (!y.busy && y.ctx && y.key == q->d.mesh_key) {
+              x = &y;
+              break;
+            }
+        if (!x) break;
+        x->busy = true;
         b.push_back(q);
-        nel += q->d.nel;
+        sl.push_back(x);
       }
       if (b.size() >= 2) {
-        const size_t need = estimate_bytes(r->d.n, nel, SSG_PRECISION_FP64) +
-                            (size_t)nel * r->d.n * r->d.n * r->d.n * 12 * sizeof(double);
-        if (need <= S->budget) {
-          if (!make_room(S, need, evict)) return nullptr;   // wait for a completion
-          S->in_use += need;
-          S->peak = std::max(S->peak, S->in_use);
-          for (size_t k = 0; k < b.size(); ++k) S->queue.pop_front();
-          *batch = std::move(b);
-          *batch_bytes = need;
-          ++S->batches;
-          S->batched += batch->size();
-          return r;
-        }
+        for (size_t k = 0; k < b.size(); ++k) S->queue.pop_front();
+        S->hits += b.size();
+        ++S->batches;
+        S->batched += b.size();
+        *batch = std::move(b);
+        *batch_slots = std::move(sl);
+        return r;
       }
+      for (Resident* x : sl) x->busy = false;
     }
     // an idle resident context of this mesh and precision
     if (r->d.mesh_key != 0)
@@ -295,39 +306,115 @@ ssg_status run_request(ssg_server* S, Request* r, Resident* slot) {
   return st;
 }
 
-// A shared-launch batch: the requests' meshes concatenated in one context
-// (built for the batch and dropped after it), solved as segments.
-ssg_status run_batch(ssg_server* S, std::vector<Request*>& b) {
+// Per-worker device arena of shared-launch batches: the concatenated
+// level-0 data and the segmented solve's scratch, grown to the largest batch
+// and reused; its own context gives the stream and error reporting.
+struct BatchArena {
+  ssg_context* c = nullptr;
+  ssg::SegScratch W;
+  double *gf = nullptr, *bj = nullptr, *kdiag = nullptr, *det = nullptr;
+  uint8_t* mult = nullptr;
+  int* dss = nullptr;
+  size_t cap_points = 0, cap_dss = 0;
+  void release() {
+    ssg::seg_scratch_free(W);
+    void* ps[] = {gf, bj, kdiag, det, mult, dss};
+    for (void* p : ps)
+      if (p) cudaFree(p);
+    gf = bj = kdiag = det = nullptr;
+    mult = nullptr;
+    dss = nullptr;
+    cap_points = cap_dss = 0;
+    if (c) ssg_destroy(c);
+    c = nullptr;
+  }
+};
+
+template <typename T>
+ssg_status arena_alloc(ssg_context* c, T** p, size_t count) {
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  void* q = nullptr;
+  if (cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T)) != cudaSuccess) {
+    cudaGetLastError();
+    return ssg::fail(c, SSG_ERR_NOMEM, "batch arena");
+  }
+  *p = static_cast<T*>(q);
+  return SSG_OK;
+}
+
+// The batch's level-0 data concatenated in the arena (device to device from
+// the resident contexts, DSS map indices shifted), then one segmented solve.
+ssg_status run_batch(ssg_server* S, BatchArena& A, std::vector<Request*>& b,
+                     std::vector<Resident*>& sl) {
+  if (!A.c) SSG_TRY(ssg_create(S->device, &A.c));
+  ssg_context* c = A.c;
   const int n = b[0]->d.n;
   const size_t nt = (size_t)n * n * n;
-  std::vector<double> vert, f, lam, eps;
-  std::vector<int> neigh, first{0};
+  std::vector<int> first{0};
+  std::vector<double> f, lam, eps;
   for (Request* r : b) {
-    const int off = first.back();
-    vert.insert(vert.end(), r->vert.begin(), r->vert.end());
-    for (int v : r->neigh) neigh.push_back(v >= 0 ? v + off : v);
+    first.push_back(first.back() + r->d.nel);
     f.insert(f.end(), r->rhs.begin(), r->rhs.end());
     lam.push_back(r->d.lambda);
     eps.push_back(r->d.eps);
-    first.push_back(off + r->d.nel);
   }
   const int nel = first.back();
-  ssg_context* c = nullptr;
-  SSG_TRY(ssg_create(S->device, &c));
-  ssg_set_setup_options(c, SSG_SETUP_NO_DEALIAS | SSG_SETUP_NO_PARTICLES |
-                               SSG_SETUP_OPPOSITE_PAIRING);
-  ssg_status st = ssg_setup_mesh(c, n, nel, vert.data(), neigh.data());
-  std::vector<double> u((size_t)nel * nt, 0.0);
+  const size_t np = (size_t)nel * nt;
+  const size_t ndss = ssg::dss_map_records_offset(np) + ssg::dss_record_ints(n) * nel;
+  if (np > A.cap_points) {
+    A.cap_points = 0;
+    SSG_TRY(arena_alloc(c, &A.gf, 6 * np));
+    SSG_TRY(arena_alloc(c, &A.bj, np));
+    SSG_TRY(arena_alloc(c, &A.kdiag, np));
+    SSG_TRY(arena_alloc(c, &A.det, np));
+    SSG_TRY(arena_alloc(c, &A.mult, np));
+    A.cap_points = np;
+  }
+  if (ndss > A.cap_dss) {
+    A.cap_dss = 0;
+    SSG_TRY(arena_alloc(c, &A.dss, ndss));
+    A.cap_dss = ndss;
+  }
+  cudaStream_t s = c->stream;
+  for (size_t k = 0; k < b.size(); ++k) {
+    const ssg::DevLevel& D = sl[k]->ctx->lev[0];
+    const size_t P = (size_t)first[k] * nt, m = D.npts;
+    for (int a = 0; a < 6; ++a)
+      SSG_CUDA(c, cudaMemcpyAsync(A.gf + a * np + P, D.gf + a * m, m * sizeof(double),
+                                  cudaMemcpyDeviceToDevice, s));
+    SSG_CUDA(c, cudaMemcpyAsync(A.bj + P, D.bj, m * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    SSG_CUDA(c, cudaMemcpyAsync(A.kdiag + P, D.kdiag, m * sizeof(double),
+                                cudaMemcpyDeviceToDevice, s));
+    SSG_CUDA(c, cudaMemcpyAsync(A.det + P, D.det, m * sizeof(double), cudaMemcpyDeviceToDevice,
+                                s));
+    SSG_CUDA(c, cudaMemcpyAsync(A.mult + P, D.mult, m, cudaMemcpyDeviceToDevice, s));
+    SSG_CUDA(c, ssg::run_dss_map_shift(s, D.dss_ec, n, b[k]->d.nel, A.dss, P, np, first[k]));
+  }
+  const ssg::DevLevel& D0 = sl[0]->ctx->lev[0];
+  ssg::SegLevel L;
+  L.n = n;
+  L.nel = nel;
+  L.nt = nt;
+  L.npts = np;
+  L.gf = A.gf;
+  L.bj = A.bj;
+  L.kdiag = A.kdiag;
+  L.rho = D0.rho;
+  L.det = A.det;
+  L.mask = nullptr;     // batched meshes have no walls
+  L.D = D0.D;
+  L.S = D0.S;
+  L.mult = A.mult;
+  L.dss = A.dss;
+  std::vector<double> u(np, 0.0);
   std::vector<ssg_solve_info> info(b.size());
   int max_iter = 0;
   for (Request* r : b) max_iter = std::max(max_iter, r->d.max_iter > 0 ? r->d.max_iter : 5000);
-  if (st == SSG_OK) {
-    c->cancel = &b[0]->cancel;
-    st = ssg_solve_helmholtz_segments(c, SSG_X_VELOCITY, (int)b.size(), first.data(), lam.data(),
-                                      f.data(), u.data(), eps.data(), max_iter, info.data());
-    c->cancel = nullptr;
-  }
-  ssg_destroy(c);
+  c->cancel = &b[0]->cancel;
+  const ssg_status st = ssg::seg_solve(c, L, A.W, (int)b.size(), first.data(), lam.data(),
+                                       f.data(), u.data(), eps.data(), max_iter, info.data());
+  c->cancel = nullptr;
   if (st != SSG_OK && st != SSG_MAXITER) return st;
   for (size_t k = 0; k < b.size(); ++k) {
     Request* r = b[k];
@@ -339,19 +426,24 @@ ssg_status run_batch(ssg_server* S, std::vector<Request*>& b) {
 
 void worker(ssg_server* S) {
   cudaSetDevice(S->device);
+  BatchArena arena;
   std::unique_lock<std::mutex> lk(S->mu);
   for (;;) {
     Resident* slot = nullptr;
     std::vector<ssg_context*> evict;
     std::vector<Request*> batch;
-    size_t batch_bytes = 0;
+    std::vector<Resident*> batch_slots;
     Request* r = nullptr;
     S->cv.wait(lk, [&] {
       if (S->stop && S->queue.empty()) return true;
-      r = admit(S, &slot, evict, &batch, &batch_bytes);
+      r = admit(S, &slot, evict, &batch, &batch_slots);
       return r != nullptr || !evict.empty();
     });
-    if (!r && evict.empty() && S->stop && S->queue.empty()) return;
+    if (!r && evict.empty() && S->stop && S->queue.empty()) {
+      lk.unlock();
+      arena.release();
+      return;
+    }
     if (!r) {
       lk.unlock();
       for (ssg_context* c : evict) ssg_destroy(c);
@@ -366,10 +458,14 @@ void worker(ssg_server* S) {
       for (Request* q : batch) q->t_start = r->t_start;
       lk.unlock();
       for (ssg_context* c : evict) ssg_destroy(c);
-      const ssg_status bst = run_batch(S, batch);
+      const ssg_status bst = run_batch(S, arena, batch, batch_slots);
       lk.lock();
       --S->active;
-      S->in_use -= batch_bytes;
+      const double now = now_s();
+      for (Resident* x : batch_slots) {
+        x->busy = false;
+        x->last_used = now;
+      }
       for (Request* q : batch) {
         // each request's own outcome: its segment's stop
         ssg_status qs = bst;
@@ -470,6 +566,7 @@ ssg_status ssg_server_submit(ssg_server* S, const ssg_request* d, const double* 
   const size_t np = (size_t)d->nel * d->n * d->n * d->n;
   r->vert.assign(d->vertices, d->vertices + 24 * (size_t)d->nel);
   r->neigh.assign(d->neigh, d->neigh + 26 * (size_t)d->nel);
+  for (int v : r->neigh) r->walls = r->walls || v < 0;
   r->d.vertices = nullptr;
   r->d.neigh = nullptr;
   r->rhs.assign(rhs, rhs + np);

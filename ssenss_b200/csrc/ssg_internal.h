@@ -131,6 +131,28 @@ struct Workspace;
 
 void free_workspace(Workspace* w);
 
+// The level-0 data a segmented Helmholtz solve reads (batch.cu): a context's
+// own level, or the serving loop's assembly of several contexts' levels.
+struct SegLevel {
+  int n = 0, nel = 0;
+  size_t nt = 0, npts = 0;
+  const double *gf = nullptr, *bj = nullptr, *kdiag = nullptr, *rho = nullptr, *det = nullptr;
+  const double *mask = nullptr, *D = nullptr, *S = nullptr;
+  const uint8_t* mult = nullptr;
+  const int* dss = nullptr;    // DSS map (dss_map_table layout)
+};
+
+// Device scratch of segmented solves, grown on demand and reused.
+struct SegScratch {
+  int *chunk_seg = nullptr, *chunk_n = nullptr, *seg_chunk0 = nullptr, *active = nullptr;
+  size_t* chunk_lo = nullptr;
+  double *part = nullptr, *sc = nullptr;
+  double *bj_s = nullptr, *dinv_s = nullptr, *x = nullptr, *r = nullptr, *z = nullptr;
+  double *p = nullptr, *ap = nullptr, *aploc = nullptr, *f = nullptr;
+  size_t cap_chunks = 0, cap_segs = 0, cap_points = 0;
+};
+void seg_scratch_free(SegScratch& W);
+
 }  // namespace ssg
 
 struct ssg_context {
@@ -186,6 +208,7 @@ struct ssg_context {
   double* d_stage[4] = {nullptr, nullptr, nullptr, nullptr};
   size_t stage_cap = 0;
   ssg::Workspace* ws = nullptr;
+  ssg::SegScratch* seg = nullptr;   // segmented Helmholtz solves (batch.cu)
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
 
@@ -207,6 +230,20 @@ ssg_status cuda_fail(ssg_context* c, cudaError_t e, const char* what);
 bool is_device_ptr(const void* p);
 
 enum Frame { FR_LEVEL0 = 0, FR_HELM = 8, FR_FCG = 9, FR_MISC = 10, FR_COUNT = 12 };
+
+// batch.cu: segments seg_first[s] .. seg_first[s+1]-1 of L, each its own
+// Jacobi-CG Helmholtz solve (lambda[s], eps[s]) sharing every operator and
+// DSS launch; f, u host or device; on c's stream
+ssg_status seg_solve(ssg_context* c, const SegLevel& L, SegScratch& W, int nseg,
+                     const int* seg_first, const double* lambda, const double* f, double* u,
+                     const double* eps, int max_iter, ssg_solve_info* info);
+
+// ints per element of the edge/corner records of a DSS map of order n, and
+// the copy of one context's map into a concatenation's (points shifted by P,
+// records placed at element offset E; npts_dst: the concatenation's points)
+size_t dss_record_ints(int n);
+cudaError_t run_dss_map_shift(cudaStream_t s, const int* src, int n, int nel, int* dst,
+                              size_t P, size_t npts_dst, int E);
 
 // solver.cu
 ssg_status ensure_workspace(ssg_context* c);
