@@ -362,19 +362,26 @@ ssg_status run_batch(ssg_server* S, BatchArena& A, std::vector<Request*>& b,
   const int nel = first.back();
   const size_t np = (size_t)nel * nt;
   const size_t ndss = ssg::dss_map_records_offset(np) + ssg::dss_record_ints(n) * nel;
+  // grown at most to the largest batch the settings allow (a cudaFree on
+  // growth synchronises the device), so sized for that the first time
+  const size_t full = std::min<size_t>((size_t)S->max_batch * S->batch_points, (size_t)1 << 24);
   if (np > A.cap_points) {
+    const size_t cap = std::max(np, full);
     A.cap_points = 0;
-    SSG_TRY(arena_alloc(c, &A.gf, 6 * np));
-    SSG_TRY(arena_alloc(c, &A.bj, np));
-    SSG_TRY(arena_alloc(c, &A.kdiag, np));
-    SSG_TRY(arena_alloc(c, &A.det, np));
-    SSG_TRY(arena_alloc(c, &A.mult, np));
-    A.cap_points = np;
+    SSG_TRY(arena_alloc(c, &A.gf, 6 * cap));
+    SSG_TRY(arena_alloc(c, &A.bj, cap));
+    SSG_TRY(arena_alloc(c, &A.kdiag, cap));
+    SSG_TRY(arena_alloc(c, &A.det, cap));
+    SSG_TRY(arena_alloc(c, &A.mult, cap));
+    A.cap_points = cap;
   }
   if (ndss > A.cap_dss) {
+    // records per point are largest at the smallest order (n = 2: 64 ints
+    // per 8 points)
+    const size_t cap = std::max(ndss, ssg::dss_map_records_offset(full) + 8 * full);
     A.cap_dss = 0;
-    SSG_TRY(arena_alloc(c, &A.dss, ndss));
-    A.cap_dss = ndss;
+    SSG_TRY(arena_alloc(c, &A.dss, cap));
+    A.cap_dss = cap;
   }
   cudaStream_t s = c->stream;
   for (size_t k = 0; k < b.size(); ++k) {
