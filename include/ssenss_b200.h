@@ -370,8 +370,12 @@ ssg_status ssg_server_create(int device, size_t hbm_budget, int max_active,
  * order queued directly behind it, up to max_batch in all, as one
  * ssg_solve_helmholtz_segments on their concatenated meshes -- one operator
  * and one DSS launch per iteration for all of them, each with its own
- * lambda, CG scalars and stop.  Results agree with the solo solve to
- * rounding (not bitwise); batched requests use no resident context. */
+ * lambda, CG scalars and stop.  The requests' resident contexts provide the
+ * data (copied device to device into one concatenated level); a request
+ * whose mesh has no idle resident context yet runs alone.  Results agree
+ * with the solo solve to rounding (not bitwise).  Each worker keeps a batch
+ * arena of up to max_batch * max_points points (about 170 bytes a point),
+ * outside the HBM budget. */
 ssg_status ssg_server_set_batching(ssg_server *srv, int max_batch,
 		size_t max_points);
 /* rhs (host, nel x n^3, an assembled weak right-hand side) is copied at
