@@ -45,40 +45,51 @@ struct CoarseArgs {
   double* frame = nullptr;
 };
 
-// A_e u for one n = 2 element (8 points), same contraction order as k_ax
-__device__ __forceinline__ void elem_op2(const CoarseArgs& a, const double* sD, const double* u8,
-                                         double* out8, size_t e) {
-  double w0[8], w1[8], w2[8];
+// A_e u at one point g of an n = 2 element (the contraction order of k_ax:
+// r-, s-, t-derivatives as two-term sums, the metric products
+// w_a = sum_b G_ab u_b, then (D^T w0 + D^T w1) + D^T w2).  The element's 8
+// points are held by 8 consecutive lanes (lane & 7 = point index in the
+// element) and the neighbours' values come by shuffles, so the operator
+// runs with one point per thread.  All 32 lanes of the warp call it (lanes
+// past the end pass valid = false).
+__device__ __forceinline__ double point_op2(const CoarseArgs& a, const double* sD, double uown,
+                                            size_t g, bool valid) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31, grp = lane & ~7, q = lane & 7;
+  const int i = q & 1, j = (q >> 1) & 1, k = q >> 2;
+  double ur = 0, us = 0, ut = 0;
 #pragma unroll
-  for (int q = 0; q < 8; ++q) {
-    const int i = q & 1, j = (q >> 1) & 1, k = q >> 2;
-    double ur = 0, us = 0, ut = 0;
-#pragma unroll
-    for (int m = 0; m < 2; ++m) {
-      ur += sD[i * 2 + m] * u8[(k * 2 + j) * 2 + m];
-      us += sD[j * 2 + m] * u8[(k * 2 + m) * 2 + i];
-      ut += sD[k * 2 + m] * u8[(m * 2 + j) * 2 + i];
-    }
-    const size_t o = e * 8 + q;
-    const double g0 = a.gf[o], g1 = a.gf[a.npts + o], g2 = a.gf[2 * a.npts + o],
-                 g3 = a.gf[3 * a.npts + o], g4 = a.gf[4 * a.npts + o],
-                 g5 = a.gf[5 * a.npts + o];
-    w0[q] = g0 * ur + g1 * us + g2 * ut;
-    w1[q] = g1 * ur + g3 * us + g4 * ut;
-    w2[q] = g2 * ur + g4 * us + g5 * ut;
+  for (int m = 0; m < 2; ++m) {
+    const double vr = __shfl_sync(full, uown, grp | ((k * 2 + j) * 2 + m));
+    const double vs = __shfl_sync(full, uown, grp | ((k * 2 + m) * 2 + i));
+    const double vt = __shfl_sync(full, uown, grp | ((m * 2 + j) * 2 + i));
+    ur += sD[i * 2 + m] * vr;
+    us += sD[j * 2 + m] * vs;
+    ut += sD[k * 2 + m] * vt;
   }
-#pragma unroll
-  for (int q = 0; q < 8; ++q) {
-    const int i = q & 1, j = (q >> 1) & 1, k = q >> 2;
-    double acc = 0, acs = 0, act = 0;
-#pragma unroll
-    for (int m = 0; m < 2; ++m) {
-      acc += sD[m * 2 + i] * w0[(k * 2 + j) * 2 + m];
-      acs += sD[m * 2 + j] * w1[(k * 2 + m) * 2 + i];
-      act += sD[m * 2 + k] * w2[(m * 2 + j) * 2 + i];
-    }
-    out8[q] = (acc + acs) + act;
+  double g0 = 0, g1 = 0, g2 = 0, g3 = 0, g4 = 0, g5 = 0;
+  if (valid) {
+    g0 = a.gf[g];
+    g1 = a.gf[a.npts + g];
+    g2 = a.gf[2 * a.npts + g];
+    g3 = a.gf[3 * a.npts + g];
+    g4 = a.gf[4 * a.npts + g];
+    g5 = a.gf[5 * a.npts + g];
   }
+  const double w0 = g0 * ur + g1 * us + g2 * ut;
+  const double w1 = g1 * ur + g3 * us + g4 * ut;
+  const double w2 = g2 * ur + g4 * us + g5 * ut;
+  double acc = 0, acs = 0, act = 0;
+#pragma unroll
+  for (int m = 0; m < 2; ++m) {
+    const double v0 = __shfl_sync(full, w0, grp | ((k * 2 + j) * 2 + m));
+    const double v1 = __shfl_sync(full, w1, grp | ((k * 2 + m) * 2 + i));
+    const double v2 = __shfl_sync(full, w2, grp | ((m * 2 + j) * 2 + i));
+    acc += sD[m * 2 + i] * v0;
+    acs += sD[m * 2 + j] * v1;
+    act += sD[m * 2 + k] * v2;
+  }
+  return (acc + acs) + act;
 }
 
 // sum over all blocks of NQ partial arrays, identical in every block
@@ -120,14 +131,16 @@ __global__ void __launch_bounds__(256) k_coarse_cg(CoarseArgs a) {
   const size_t nthr = (size_t)gridDim.x * blockDim.x;
   const int G = gridDim.x;
 
+  // one point per thread, an element's 8 points in 8 consecutive lanes; the
+  // loop runs warp-uniformly (point_op2 shuffles across the warp)
+  const size_t wbase = tid - (threadIdx.x & 31);
+
   // r = f - DSS(A x); nullspace of r (src/solver.c:49-53)
-  for (size_t e = tid; e < (size_t)a.nel; e += nthr) {
-    double u8[8], o8[8];
-#pragma unroll
-    for (int q = 0; q < 8; ++q) u8[q] = a.x[e * 8 + q];
-    elem_op2(a, sD, u8, o8, e);
-#pragma unroll
-    for (int q = 0; q < 8; ++q) a.aploc[e * 8 + q] = o8[q];
+  for (size_t b = wbase; b < a.npts; b += nthr) {
+    const size_t g = b + (threadIdx.x & 31);
+    const bool valid = g < a.npts;
+    const double o = point_op2(a, sD, valid ? a.x[g] : 0.0, g, valid);
+    if (valid) a.aploc[g] = o;
   }
   grid.sync();
   {
@@ -169,19 +182,17 @@ __global__ void __launch_bounds__(256) k_coarse_cg(CoarseArgs a) {
   for (; it < a.max_iter; ++it) {
     const bool first = it == 0;
     // p = beta p + (z - c) (first: p = z - c); aploc = A_e p
-    for (size_t e = tid; e < (size_t)a.nel; e += nthr) {
-      double u8[8], o8[8];
-#pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        const size_t g = e * 8 + q;
+    for (size_t b = wbase; b < a.npts; b += nthr) {
+      const size_t g = b + (threadIdx.x & 31);
+      const bool valid = g < a.npts;
+      double pv = 0.0;
+      if (valid) {
         const double zc = a.z[g] - cz;
-        const double pv = first ? zc : beta * a.p[g] + zc;
+        pv = first ? zc : beta * a.p[g] + zc;
         a.p[g] = pv;
-        u8[q] = pv;
       }
-      elem_op2(a, sD, u8, o8, e);
-#pragma unroll
-      for (int q = 0; q < 8; ++q) a.aploc[e * 8 + q] = o8[q];
+      const double o = point_op2(a, sD, pv, g, valid);
+      if (valid) a.aploc[g] = o;
     }
     grid.sync();
     // ap = DSS(aploc); (p w).ap; first: (r w).p and (r w).r
