@@ -453,8 +453,8 @@ cudaError_t run_convection(cudaStream_t s, int nel, int e0, int nel_fac, int n, 
                            const double* Dh, const double* Jh, const double* Dd,
                            const double* Jd, double* scratch) {
   if (nel <= 0) return cudaSuccess;
-  if (convection_dmma_applies(n, m, u, v))
-    return run_convection_dmma(s, nel, e0, nel_fac, u, udv, W, Dh, Jh);
+  if (convection_dmma_applies(n, m))
+    return run_convection_dmma(s, nel, e0, nel_fac, u, v, udv, W, Dh, Jh);
   // the compile-time-order kernel reads element lines with 16-byte loads:
   // fields at addresses that are not 16-byte aligned take the runtime-order
   // kernel

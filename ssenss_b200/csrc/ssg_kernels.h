@@ -204,12 +204,13 @@ cudaError_t run_convection(cudaStream_t s, int nel, int e0, int nel_fac, int n, 
                            const double* u, const double* v, double* udv, const double* W,
                            const double* Dh, const double* Jh, const double* Dd,
                            const double* Jd, double* scratch);
-// Self-convection (u advecting itself) at n = 8, m = 12 on the FP64 tensor
-// cores (conv_dmma.cu); run_convection takes it when u == v
-bool convection_dmma_applies(int n, int m, const double* u, const double* v);
+// Convection at n = 8, m = 12 on the FP64 tensor cores (conv_dmma.cu): the
+// self-convection kernel when u == v, else the general one; run_convection
+// takes them at that order
+bool convection_dmma_applies(int n, int m);
 cudaError_t run_convection_dmma(cudaStream_t s, int nel, int e0, int nel_fac, const double* u,
-                                double* udv, const double* W, const double* Dh,
-                                const double* Jh);
+                                const double* v, double* udv, const double* W,
+                                const double* Dh, const double* Jh);
 // Lagrangian particle advance to time t (particles.cu); passes: device int
 // that receives the largest per-particle pass count (atomicMax, caller zeroes).
 // order (np ints) and bucket (2 (nel + 1) ints): scratch of the element-order
