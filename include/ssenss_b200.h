@@ -280,11 +280,12 @@ ssg_status ssg_multigrid_preconditioner(ssg_context *ctx, const double *r,
 
 /* Dealiased skew-symmetric convection of the whole mesh --
  * convection_operator for every element (src/convection.c:31-69).
- * u (advecting), v (advected), udv: 3 x nel x n^3.  Passing the same
- * pointer as u and v (the time step's call, src/navier_stokes.c:59) takes
- * the self-convection kernel at n = 8 (FP64 tensor cores, three fields
- * interpolated instead of six); the result agrees with the general form to
- * rounding. */
+ * u (advecting), v (advected), udv: 3 x nel x n^3.  At n = 8 both forms
+ * the time step calls run on the FP64 tensor cores: a field advected by
+ * another (the RK4 stages, src/time.c:114-116) and, when u and v are the
+ * same pointer, the velocity advecting itself (the history term,
+ * src/navier_stokes.c:79-83: three fields interpolated instead of six);
+ * the two agree to rounding. */
 ssg_status ssg_convection_operator(ssg_context *ctx, const double *u,
 		const double *v, double *udv);
 /* convection_operator for the elements first .. first+count-1 only: the

@@ -439,8 +439,9 @@ void convection_operator(struct element *sel, struct trivec *u,
 	const int e = sel->geom->id;
 	if (sel->basis->n != G_n || e < 0 || e >= G_nel)
 		fatal_error("ssenss_b200: convection_operator on an unknown element");
-	/* the time step advects the velocity with itself (u == v): one staged
-	 * field, which the library runs on its self-convection kernel */
+	/* the velocity advecting itself (u == v, the step's history term,
+	 * src/navier_stokes.c:79-83): one staged field, which the library runs
+	 * on its self-convection kernel */
 	const double *gv = u == v ? G_conv : G_conv + 3 * G_nt;
 	for (int c = 0; c < 3; ++c) {
 		memcpy(G_conv + c * G_nt, ***u->ind[c], G_nt * sizeof(double));

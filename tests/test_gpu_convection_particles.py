@@ -62,9 +62,9 @@ SELF_CASES = {
 
 @pytest.mark.parametrize("name", list(SELF_CASES))
 def test_self_convection_matches_oracle(name, gpu_ctx_factory):
-    """convection_operator(u, u), the time step's call: at n = 8 the
-    tensor-core kernel, against the oracle and against the general kernel
-    (a copy of u as the advected field) run on the same inputs."""
+    """convection_operator(u, u), the time step's history term: at n = 8 the
+    self-convection kernel, against the oracle and against the general
+    kernel (a copy of u as the advected field) on the same inputs."""
     mesh, n, orc, ctx = case(name, gpu_ctx_factory, SELF_CASES)
     rng = np.random.default_rng(21)
     u = rng.standard_normal((3, mesh.nel, n, n, n))
