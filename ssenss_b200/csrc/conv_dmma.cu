@@ -430,19 +430,11 @@ cudaError_t run_convection_dmma(cudaStream_t s, int nel, int e0, int nel_fac, co
   int dev = 0, sms = 0;
   cudaError_t err = cudaGetDevice(&dev);
   if (err != cudaSuccess) return err;
-  static bool attr[2][64] = {};
-  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  static SmemAttr attr_self, attr_uv;
   const bool self = u == v;
-  if (!attr[self][dev]) {
-    err = self ? cudaFuncSetAttribute(dev::k_convection_dmma,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)SMEM_SELF)
-               : cudaFuncSetAttribute(dev::k_convection_dmma_uv,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)SMEM_GEN);
-    if (err != cudaSuccess) return err;
-    attr[self][dev] = true;
-  }
+  err = self ? attr_self.ensure((const void*)dev::k_convection_dmma, SMEM_SELF)
+             : attr_uv.ensure((const void*)dev::k_convection_dmma_uv, SMEM_GEN);
+  if (err != cudaSuccess) return err;
   err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   if (err != cudaSuccess) return err;
   count_launch();

@@ -433,14 +433,9 @@ static cudaError_t launch_fast(cudaStream_t s, int nel, int e0, int nel_fac, con
         mt.JT[p * M + o] = Jh[o * N + p];
       }
     constexpr size_t smem = dev::conv_smem_bytes<N, M>();
-    static bool attr = false;
-    if (!attr) {
-      cudaError_t e = cudaFuncSetAttribute(dev::k_convection<N, M>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)smem);
-      if (e != cudaSuccess) return e;
-      attr = true;
-    }
+    static SmemAttr attr;
+    cudaError_t e = attr.ensure((const void*)dev::k_convection<N, M>, smem);
+    if (e != cudaSuccess) return e;
     count_launch();
     dev::k_convection<N, M><<<grid, dev::kConvThreads, smem, s>>>(nel, e0, nel_fac, u, v, udv,
                                                                  W, mt);
@@ -476,13 +471,10 @@ cudaError_t run_convection(cudaStream_t s, int nel, int e0, int nel_fac, int n, 
   if (!in_smem && !scratch) return cudaErrorInvalidValue;
   const size_t smem = convection_rt_smem(n, m, in_smem);
   if (smem > kConvSmemMax) return cudaErrorInvalidValue;
-  static bool attr = false;
-  if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(dev::k_convection_rt,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)kConvSmemMax);
+  static SmemAttr attr;
+  {
+    cudaError_t e = attr.ensure((const void*)dev::k_convection_rt, kConvSmemMax);
     if (e != cudaSuccess) return e;
-    attr = true;
   }
   const int grid = in_smem ? nel : std::min(nel, kConvScratchBlocks);
   count_launch();

@@ -596,11 +596,10 @@ static cudaError_t launch_ax_t(cudaStream_t s, int nel, int epb, T* u, T* au, co
                                const ScalarOp& dop) {
   const size_t smem = (4 * N * AxLayout<N>::P + (size_t)epb * 3 * N * N * AxLayout<N>::Q) *
                       sizeof(double);
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaFuncSetAttribute(k_ax<N, T, HELM, FUSEP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         200 * 1024);
-    attr_set = true;
+  static SmemAttr attr;
+  {
+    cudaError_t e = attr.ensure((const void*)k_ax<N, T, HELM, FUSEP>, 200 * 1024);
+    if (e != cudaSuccess) return e;
   }
   dim3 blk(N, N, epb);
   dim3 grd((nel + epb - 1) / epb);
@@ -615,13 +614,10 @@ static cudaError_t launch_axl_t(cudaStream_t s, int nel, T* u, T* au, const T* g
                                 const ScalarOp& dop) {
   using L = AxLine<N>;
   constexpr size_t smem = (size_t)L::SMEM * sizeof(T);
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(k_axl<N, T, HELM, FUSEP>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
+  static SmemAttr attr;
+  {
+    cudaError_t e = attr.ensure((const void*)k_axl<N, T, HELM, FUSEP>, smem);
     if (e != cudaSuccess) return e;
-    attr_set = true;
   }
   const int grd = (nel + L::EPB - 1) / L::EPB;
   { SSG_COUNT(); k_axl<N, T, HELM, FUSEP><<<grd, L::THREADS, smem, s>>>(nel, u, au, gf, npts, bj, D, S, lambda, pu, dop); }

@@ -91,6 +91,29 @@ inline void count_launch() {
   ++t_launches;
 }
 
+// cudaFuncSetAttribute(MaxDynamicSharedMemorySize) for a kernel, once per
+// device (the attribute belongs to the device's context) and again only when
+// a larger size is asked; safe from several host threads (a race at worst
+// sets the same attribute twice).  One object per kernel, as a static.
+struct SmemAttr {
+  std::atomic<int> bytes[64] = {};
+  cudaError_t ensure(const void* func, size_t need) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (bytes[dev].load(std::memory_order_acquire) >= (int)need) return cudaSuccess;
+    e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need);
+    if (e == cudaSuccess) {
+      int cur = bytes[dev].load(std::memory_order_relaxed);
+      while (cur < (int)need &&
+             !bytes[dev].compare_exchange_weak(cur, (int)need, std::memory_order_release))
+        ;
+    }
+    return e;
+  }
+};
+
 int vec_blocks(size_t npts);
 // elements-per-block value of the operator launch that selects the line-form
 // kernel (k_axl, a fixed number of elements per block) for orders other
