@@ -562,10 +562,9 @@ thread_local unsigned long long t_launches = 0;
 
 // Launch shapes chosen by the autotuner (tune.cu); 0 = the default rule.
 // Process-wide: they depend on the order and the device, not on the mesh.
-int g_tune_ax_epb[SSG_MAXN + 1] = {0};
-int g_tune_dss_bps[SSG_MAXN + 1] = {0};
-int g_tune_vec_bps = 0;
-int g_tune_ax_kind[SSG_MAXN + 1] = {0};
+std::atomic<int> g_tune_ax_epb[SSG_MAXN + 1] = {};
+std::atomic<int> g_tune_dss_bps[SSG_MAXN + 1] = {};
+std::atomic<int> g_tune_vec_bps{0};
 
 int ax_epb_max(int n) {
   // elements per block: up to 256 threads, <= 96 KB of FP64 shared memory
@@ -580,12 +579,12 @@ int ax_epb_max(int n) {
 // kernels loop grid-stride with four points in flight per thread
 int vec_blocks(size_t npts) {
   size_t b = (npts + 255) / 256;
-  const size_t cap = (size_t)148 * (g_tune_vec_bps > 0 ? g_tune_vec_bps : kVecBpsDefault);
+  const size_t cap = (size_t)148 * (g_tune_vec_bps.load() > 0 ? g_tune_vec_bps.load() : kVecBpsDefault);
   return (int)(b < cap ? (b ? b : 1) : cap);
 }
 
 int ax_epb(int n) {
-  if (n >= 0 && n <= SSG_MAXN && g_tune_ax_epb[n] != 0) return g_tune_ax_epb[n];
+  if (n >= 0 && n <= SSG_MAXN && g_tune_ax_epb[n].load() != 0) return g_tune_ax_epb[n].load();
   return kAxLine;
 }
 
@@ -699,7 +698,7 @@ cudaError_t run_ax(cudaStream_t s, int n, int nel, int epb, bool helm, bool fp32
 int dss_grid(int n, int nel) {
   const size_t tasks = (size_t)nel * n * n * n;
   const size_t g = (tasks + 255) / 256;
-  const int bps = (n >= 0 && n <= SSG_MAXN && g_tune_dss_bps[n] > 0) ? g_tune_dss_bps[n] : 8;
+  const int bps = (n >= 0 && n <= SSG_MAXN && g_tune_dss_bps[n].load() > 0) ? g_tune_dss_bps[n].load() : 8;
   const size_t cap = (size_t)148 * bps;
   return (int)(g < cap ? (g ? g : 1) : cap);
 }

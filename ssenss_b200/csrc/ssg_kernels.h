@@ -123,18 +123,14 @@ constexpr int kAxLine = -1;
 int ax_epb(int n);
 int ax_epb_max(int n);
 int dss_grid(int n, int nel);
-// autotuned launch shapes (0 = default rule), indexed by order n
-extern int g_tune_ax_epb[];
-extern int g_tune_dss_bps[];
-extern int g_tune_vec_bps;
+// autotuned launch shapes (0 = default rule), indexed by order n; atomics:
+// the tuner may run while other host threads launch
+extern std::atomic<int> g_tune_ax_epb[];
+extern std::atomic<int> g_tune_dss_bps[];
+extern std::atomic<int> g_tune_vec_bps;
 // untuned vector-kernel blocks per SM: the CG update's residency (3 x 256
 // threads at <= 85 registers), so its grid is one full wave
 constexpr int kVecBpsDefault = 3;
-// operator kernel kind per order: default, the shared-memory kernel, or the
-// FP64 tensor-core kernel (n = 8 only); run_ax's epb = AX_DMMA forces the
-// latter
-enum { AX_KIND_DEFAULT = 0, AX_KIND_CLASSIC = 1, AX_KIND_DMMA = 2, AX_DMMA = -1 };
-extern int g_tune_ax_kind[];
 namespace dev { struct PUpdate; }
 cudaError_t run_ax8_dmma(cudaStream_t s, int nel, bool helm, bool fp32, void* u, void* au,
                          const void* gf, size_t npts, const double* bj, const double* D,

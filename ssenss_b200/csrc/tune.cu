@@ -244,8 +244,8 @@ ssg_status ssg_tuning(int n, int* ax_elements_per_block, int* dss_blocks_per_sm,
   // 0: the FP64 tensor-core operator (one warp per element)
   const bool dmma = n == 8;
   if (ax_elements_per_block) *ax_elements_per_block = dmma ? 0 : ax_epb(n);
-  if (dss_blocks_per_sm) *dss_blocks_per_sm = g_tune_dss_bps[n] > 0 ? g_tune_dss_bps[n] : 8;
-  if (vector_blocks_per_sm) *vector_blocks_per_sm = g_tune_vec_bps > 0 ? g_tune_vec_bps : kVecBpsDefault;
+  if (dss_blocks_per_sm) *dss_blocks_per_sm = g_tune_dss_bps[n].load() > 0 ? g_tune_dss_bps[n].load() : 8;
+  if (vector_blocks_per_sm) *vector_blocks_per_sm = g_tune_vec_bps.load() > 0 ? g_tune_vec_bps.load() : kVecBpsDefault;
   return SSG_OK;
 }
 
