@@ -295,6 +295,21 @@ ssg_status ssg_convection_operator(ssg_context *ctx, const double *u,
 ssg_status ssg_convection_elements(ssg_context *ctx, int first, int count,
 		const double *u, const double *v, double *udv);
 
+/* The velocity history the convection sub-steps interpolate in time
+ * (add_interpolated_velocity, src/time.c:132-152): sel->u, sel->old->u,
+ * sel->old->old->u (each 3 x nel x n^3, host or device, copied) at the
+ * solver time t (params->t) with step dt (params->dt). */
+ssg_status ssg_set_velocity_history(ssg_context *ctx, const double *u,
+		const double *u_old, const double *u_oldold, double t, double dt);
+/* integrate_convection_rk4 (src/time.c:84-130) on the device: u
+ * (3 x nel x n^3, host or device, in/out) += beta * the history
+ * interpolated at t0, then RK4 sub-steps of dt from t0 to t, each stage a
+ * dealiased convection of the stage field by the interpolated velocity,
+ * DSS and the inverse mass.  Needs the dealiasing grid and
+ * ssg_set_velocity_history. */
+ssg_status ssg_integrate_convection_rk4(ssg_context *ctx, double *u, double t0,
+		double t, double dt, double beta);
+
 /* ---- launch-shape autotuner (no reference counterpart) ---------------------- */
 
 /* Time every candidate launch shape of the operator (elements per block),

@@ -327,6 +327,8 @@ class Reference(_Common):
             L.ssgref_particles_advance.argtypes = [C.c_size_t, _dp, _ip]
             L.ssgref_set_level0_factor.argtypes = [C.c_int, _dp]
             L.ssgref_set_svv.argtypes = [C.c_int, C.c_double]
+            L.ssgref_integrate_convection_rk4.argtypes = [_dp, C.c_double, C.c_double,
+                                                          C.c_double, C.c_double]
             L.ssgref_particles_advance.restype = C.c_int
             cls._lib = L
         return cls._lib
@@ -440,6 +442,14 @@ class Reference(_Common):
     # -- time stepping / particles -------------------------------------------
     def init_tgv(self):
         self.lib().ssgref_init_tgv()
+
+    def integrate_convection_rk4(self, u, t0, t, dt, beta):
+        """integrate_convection_rk4 (src/time.c:84-130) on u (3, nel, n, n,
+        n), returned updated; the history from set_field, the solver time
+        from set_params."""
+        u = _f64(u).copy()
+        self.lib().ssgref_integrate_convection_rk4(_d(u), t0, t, dt, beta)
+        return u
 
     def init_ethier_steinman(self):
         """The reference's analytic test case (src/test.c:202-214):

@@ -613,6 +613,23 @@ void ssgref_convection(const double *u, const double *v, double *out)
 	free_trivec(to);
 }
 
+/* integrate_convection_rk4 (src/time.c:84-130) on u (3 x nel x n^3,
+ * in/out) with the velocity history set by ssgref_set_field and the time
+ * by ssgref_set_time; in the build linked with the binding the call is the
+ * binding's (the library's device sub-steps). */
+void ssgref_integrate_convection_rk4(double *u, double t0, double t, double dt,
+		double beta)
+{
+	struct trivec **tu = new_ptr_array(H_nel, H_n,
+			(void *(*) ()) new_trivec);
+	for (int e = 0; e < H_nel; ++e)
+		trivec_in(tu[e], u, e);
+	integrate_convection_rk4(H_sel, tu, t0, t, dt, beta);
+	for (int e = 0; e < H_nel; ++e)
+		trivec_out(tu[e], u, e);
+	free_ptr_array(tu, H_nel, free_trivec);
+}
+
 /* ---- Navier-Stokes step on the Taylor-Green vortex ---- */
 
 static double tgv_u(double x, double y, double z, double t)

@@ -332,6 +332,20 @@ class Context:
                     "convection_operator")
         return out
 
+    def set_velocity_history(self, u, u_old, u_oldold, t, dt):
+        """ssg_set_velocity_history: the three velocity levels (3, nel, n,
+        n, n each) at solver time t with step dt."""
+        self._check(self.lib.ssg_set_velocity_history(self.h, _ptr(u), _ptr(u_old),
+                                                      _ptr(u_oldold), float(t), float(dt)),
+                    "set_velocity_history")
+
+    def integrate_convection_rk4(self, u, t0, t, dt, beta):
+        """ssg_integrate_convection_rk4 on u (3, nel, n, n, n), in place."""
+        self._check(self.lib.ssg_integrate_convection_rk4(self.h, _ptr(u), float(t0), float(t),
+                                                          float(dt), float(beta)),
+                    "integrate_convection_rk4")
+        return u
+
     def convection_elements(self, first, u, v, out=None):
         """ssg_convection_elements: convection of the elements first ..
         first + count - 1, fields shaped (3, count, n, n, n)."""

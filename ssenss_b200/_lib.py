@@ -106,6 +106,10 @@ SIGNATURES = [
     ("ssg_autotune", C.c_int, [C.c_void_p, C.c_int]),
     ("ssg_set_setup_options", C.c_int, [C.c_void_p, C.c_uint]),
     ("ssg_set_svv", C.c_int, [C.c_void_p, C.c_int, C.c_double]),
+    ("ssg_set_velocity_history", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                           C.c_double, C.c_double]),
+    ("ssg_integrate_convection_rk4", C.c_int, [C.c_void_p, C.c_void_p, C.c_double, C.c_double,
+                                               C.c_double, C.c_double]),
     ("ssg_memory_info", C.c_int, [C.c_void_p, C.POINTER(C.c_size_t)]),
     ("ssg_request_bytes", C.c_size_t, [C.c_int, C.c_int, C.c_int]),
     ("ssg_gll", C.c_int, [C.c_int, _dp, _dp]),

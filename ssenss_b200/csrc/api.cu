@@ -77,6 +77,9 @@ static void free_mesh(ssg_context* c) {
     delete c->seg;
     c->seg = nullptr;
   }
+  if (c->vhist) cudaFree(c->vhist);
+  if (c->rk_scratch) cudaFree(c->rk_scratch);
+  c->vhist = c->rk_scratch = nullptr;
   for (auto& l : c->lev) free_level(l);
   dfree(c->d_pairs); c->d_pairs = nullptr;
   dfree(c->inv_mass); c->inv_mass = nullptr;

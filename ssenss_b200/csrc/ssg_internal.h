@@ -209,6 +209,11 @@ struct ssg_context {
   size_t stage_cap = 0;
   ssg::Workspace* ws = nullptr;
   ssg::SegScratch* seg = nullptr;   // segmented Helmholtz solves (batch.cu)
+  // convection sub-steps (timestep.cu): velocity history (oldest first,
+  // 3 levels x 3 components x npts) with its time and step, and scratch
+  double* vhist = nullptr;
+  double vhist_t = 0.0, vhist_dt = 0.0;
+  double* rk_scratch = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
 

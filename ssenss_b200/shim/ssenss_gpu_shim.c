@@ -12,6 +12,7 @@
  *   global_inverse_mass_matrix_operator              (src/poisson.h)
  *   jacobi_preconditioner, multigrid_preconditioner  (src/precon.h:47-50)
  *   convection_operator                              (src/convection.h:22-23)
+ *   integrate_convection_rk4                         (src/time.h)
  *   integrate_particle_equations                     (src/particles.h:71)
  *
  * The reference's definitions of those names are renamed at build time
@@ -50,6 +51,7 @@
 #include "global.h"
 #include "convection.h"
 #include "particles.h"
+#include "time.h"
 
 #include "ssenss_b200.h"
 #include "ssenss_gpu_shim.h"
@@ -62,6 +64,8 @@ static int G_n, G_nel, G_device;
 static size_t G_nt;                 /* n^3 */
 static double *G_u;                 /* nel n^3: gathered solution / guess */
 static double *G_conv;              /* 9 n^3: one element's convection operands */
+static double *G_rk;                /* 12 x npts: velocity history and the field of
+                                     * integrate_convection_rk4 */
 static double G_hist[SHIM_HISTORY_CAP];
 static struct ssenss_gpu_solve G_last;
 
@@ -216,6 +220,7 @@ int ssenss_gpu_attach(struct element **sel, int device)
 
 	G_u = alloc_doubles(9 * np > 9 * G_nt ? 9 * np : 9 * G_nt);
 	G_conv = alloc_doubles(9 * G_nt);
+	G_rk = alloc_doubles(12 * np);
 	memset(&G_last, 0, sizeof(G_last));
 	G_last.history = G_hist;
 	return 0;
@@ -228,7 +233,8 @@ void ssenss_gpu_detach(void)
 	G = NULL;
 	free(G_u);
 	free(G_conv);
-	G_u = G_conv = NULL;
+	free(G_rk);
+	G_u = G_conv = G_rk = NULL;
 }
 
 const struct ssenss_gpu_solve *ssenss_gpu_last_solve(void)
@@ -454,6 +460,55 @@ void convection_operator(struct element *sel, struct trivec *u,
 	for (int c = 0; c < 3; ++c)
 		memcpy(***udv->ind[c], G_conv + (6 + c) * G_nt,
 				G_nt * sizeof(double));
+}
+
+/* ---- convection sub-steps (src/time.c:84-130) --------------------------- */
+
+/* trivec fields of every element into / out of one contiguous buffer,
+ * component-major, elements by their global id */
+static void gather_trivec(double *dst, struct element **sel, struct trivec **v,
+		struct trivec *(*pick)(struct element *))
+{
+	const size_t np = G_nt * G_nel;
+	for (int i = 0; i < G_nel; ++i) {
+		const int e = sel[i]->geom->id;
+		struct trivec *t = v ? v[i] : pick(sel[i]);
+		for (int c = 0; c < 3; ++c)
+			memcpy(dst + c * np + e * G_nt, ***t->ind[c],
+					G_nt * sizeof(double));
+	}
+}
+
+static struct trivec *vel_now(struct element *s) { return s->u; }
+static struct trivec *vel_old(struct element *s) { return s->old->u; }
+static struct trivec *vel_oldold(struct element *s) { return s->old->old->u; }
+
+/* The whole mesh's convection sub-steps in one library call: the velocity
+ * history and u go to the device once, the 8 stages of the two RK4
+ * sub-steps run there, u comes back. */
+void integrate_convection_rk4(struct element **sel, struct trivec **u,
+		double t0, double t, double dt, double beta)
+{
+	need("integrate_convection_rk4");
+	if ((*sel)->nel != G_nel || (*sel)->basis->n != G_n)
+		fatal_error("ssenss_b200: integrate_convection_rk4 on another mesh");
+	const size_t np = G_nt * G_nel;
+	double *h = G_rk, *f = G_rk + 9 * np;
+	gather_trivec(h, sel, NULL, vel_now);
+	gather_trivec(h + 3 * np, sel, NULL, vel_old);
+	gather_trivec(h + 6 * np, sel, NULL, vel_oldold);
+	check(ssg_set_velocity_history(G, h, h + 3 * np, h + 6 * np,
+			(*sel)->params->t, (*sel)->params->dt),
+			"integrate_convection_rk4 (history)");
+	gather_trivec(f, sel, u, NULL);
+	check(ssg_integrate_convection_rk4(G, f, t0, t, dt, beta),
+			"integrate_convection_rk4");
+	for (int i = 0; i < G_nel; ++i) {
+		const int e = sel[i]->geom->id;
+		for (int c = 0; c < 3; ++c)
+			memcpy(***u[i]->ind[c], f + c * np + e * G_nt,
+					G_nt * sizeof(double));
+	}
 }
 
 /* ---- particles (src/particles.c:182-218) ------------------------------ */
