@@ -117,6 +117,7 @@ __global__ void __launch_bounds__(AxLine<N>::THREADS)
 //   DSS_DOT2:  store; partial sums (y w) out, (y w) y2            [2]
 //   DSS_RESID: out = y - DSS; partial sum w out                   [1]
 //   DSS_AVG:   out = DSS * w (direct_stiffness_averaging)
+//   DSS_SCALE: out = DSS * y (the DSS, then the inverse mass product)
 // w = 1 / multiplicity = 1 / (1 + number of contributions).
 // ---------------------------------------------------------------------------
 template <int N, typename T, int MODE>
@@ -197,7 +198,8 @@ __global__ void __launch_bounds__(256, (MODE == DSS_CGUPD || MODE == DSS_DOT2) ?
         er[u] = (double)cr[qq];
         ed[u] = (double)cd[qq];
       }
-      if (MODE == DSS_RESID || MODE == DSS_DOT || MODE == DSS_DOT2) ey[u] = (double)y[qq];
+      if (MODE == DSS_RESID || MODE == DSS_DOT || MODE == DSS_DOT2 || MODE == DSS_SCALE)
+        ey[u] = (double)y[qq];
       if (MODE == DSS_DOT2) ey2[u] = (double)y2[qq];
     }
 #pragma unroll
@@ -242,6 +244,8 @@ __global__ void __launch_bounds__(256, (MODE == DSS_CGUPD || MODE == DSS_DOT2) ?
         s0 += (double)rv * w;
       } else if (MODE == DSS_AVG) {
         out[g] = (T)(acc * w);
+      } else if (MODE == DSS_SCALE) {
+        out[g] = (T)(acc * ey[u]);
       } else {
         const T av = (T)acc;
         out[g] = av;
@@ -727,6 +731,14 @@ static cudaError_t run_dss_n(cudaStream_t s, int mode, int nel, const T* in, T* 
       break;
     case DSS_CGUPD:
       { SSG_COUNT(); k_dss<N, T, DSS_CGUPD><<<grd, 256, 0, s>>>(nel, in, out, ec_tab, mask, y, y2, part, stop, op, cg); }
+      break;
+    case DSS_SCALE:
+      if constexpr (sizeof(T) == sizeof(double)) {
+        SSG_COUNT();
+        k_dss<N, T, DSS_SCALE><<<grd, 256, 0, s>>>(nel, in, out, ec_tab, mask, y, y2, part, stop, op, cg);
+      } else {
+        return cudaErrorInvalidValue;
+      }
       break;
     default:
       return cudaErrorInvalidValue;

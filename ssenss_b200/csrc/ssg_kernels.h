@@ -55,8 +55,10 @@ struct PtrList {
 };
 
 // DSS epilogue modes (kernels.cu); DSS_CGUPD: the gathered ap feeds the CG
-// update x += alpha p, r -= alpha ap, z = dinv r with its four partial sums
-enum { DSS_PLAIN = 0, DSS_DOT = 1, DSS_RESID = 2, DSS_AVG = 3, DSS_DOT2 = 4, DSS_CGUPD = 5 };
+// update x += alpha p, r -= alpha ap, z = dinv r with its four partial sums;
+// DSS_SCALE: out = DSS * y pointwise (FP64 only: the inverse mass product)
+enum { DSS_PLAIN = 0, DSS_DOT = 1, DSS_RESID = 2, DSS_AVG = 3, DSS_DOT2 = 4, DSS_CGUPD = 5,
+       DSS_SCALE = 6 };
 
 // vectors of the DSS_CGUPD epilogue (storage type of the level)
 struct DssCg {

@@ -6,12 +6,15 @@
 // four stages, and each stage evaluates the dealiased convection of a stage
 // field advected by the velocity interpolated in time from the last three
 // steps -- 24 of the 25 convection evaluations of a step.  Here a stage is
-// one convection launch over all elements, one DSS and one inverse-mass
-// product per component, and a few vector kernels; the velocity history and
-// the stage fields stay on the device.
+// three kinds of launch: one pass that forms the stage field and the
+// interpolated velocity, the convection over all elements, and per component
+// one DSS whose epilogue multiplies by the inverse mass; a sub-step ends with
+// one pass of the four stage updates.  The velocity history and the stage
+// fields stay on the device.
 //
 // The vector updates keep the reference's operation order, each axpy
-// y += alpha x as one fused multiply-add (the BLAS daxpy form); the
+// y += alpha x as one fused multiply-add (the BLAS daxpy form), also where
+// one pass applies several in sequence; the
 // interpolation weights are computed on the host exactly as the reference
 // computes them.  The convection and the DSS agree with the reference's to
 // their own tolerances (1e-13 and bitwise), so the result agrees to
@@ -19,6 +22,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <utility>
 
 #include "ssg_internal.h"
 #include "ssg_kernels.h"
@@ -45,16 +49,37 @@ __global__ void k_interp_velocity(size_t n, double* __restrict__ out, bool init,
   }
 }
 
-// y = u (+ alpha f): the stage field
-__global__ void k_stage_field(size_t n, double* __restrict__ y, const double* __restrict__ u,
-                              const double* __restrict__ f, double alpha, bool add) {
-  SSG_TS_LOOP(q, n) y[q] = add ? fma(alpha, f[q], u[q]) : u[q];
+// one stage's inputs: the stage field y = u (+ alpha f) and the velocity
+// interpolated in time, ut = wa uoo + wb uo + wc u (each term only where its
+// flag is set, in that order)
+__global__ void k_stage_inputs(size_t n, double* __restrict__ y, const double* __restrict__ u,
+                               const double* __restrict__ f, double alpha, bool add,
+                               double* __restrict__ ut, const double* __restrict__ uoo,
+                               const double* __restrict__ uo, const double* __restrict__ uc,
+                               double wa, double wb, double wc, bool fa, bool fb, bool fc) {
+  SSG_TS_LOOP(q, n) {
+    y[q] = add ? fma(alpha, f[q], u[q]) : u[q];
+    double v = 0.0;
+    if (fa) v = fma(wa, uoo[q], v);
+    if (fb) v = fma(wb, uo[q], v);
+    if (fc) v = fma(wc, uc[q], v);
+    ut[q] = v;
+  }
 }
 
-// u += alpha f
-__global__ void k_axpy(size_t n, double* __restrict__ u, const double* __restrict__ f,
-                       double alpha) {
-  SSG_TS_LOOP(q, n) u[q] = fma(alpha, f[q], u[q]);
+// u += c0 f0; u += c1 f1; u += c2 f2; u += c3 f3 (four axpys in that order,
+// each rounded as its own fused multiply-add)
+__global__ void k_axpy4(size_t n, double* __restrict__ u, const double* __restrict__ f0,
+                        const double* __restrict__ f1, const double* __restrict__ f2,
+                        const double* __restrict__ f3, double c0, double c1, double c2,
+                        double c3) {
+  SSG_TS_LOOP(q, n) {
+    double v = u[q];
+    v = fma(c0, f0[q], v);
+    v = fma(c1, f1[q], v);
+    v = fma(c2, f2[q], v);
+    u[q] = fma(c3, f3[q], v);
+  }
 }
 
 }  // namespace dev
@@ -141,6 +166,9 @@ ssg_status ssg_integrate_convection_rk4(ssg_context* c, double* u, double t0, do
     }
     c->rk_scratch = static_cast<double*>(p);
   }
+  // f[i] holds the stage's raw convection, then the buffer y held is swapped
+  // in: the DSS with the inverse mass product reads f[i] and writes y, and
+  // the stage field's buffer is free again once the convection has run
   double* du = c->rk_scratch;
   double* y = du + np;
   double* ut = y + np;
@@ -151,43 +179,39 @@ ssg_status ssg_integrate_convection_rk4(ssg_context* c, double* u, double t0, do
   const int nb = vec_blocks(np);
   SSG_CUDA(c, cudaMemcpyAsync(du, u, np * sizeof(double), cudaMemcpyDefault, s));
 
-  auto interp = [&](double* out, bool init, double tt, double alpha) -> ssg_status {
-    const InterpWeights w = interp_weights(c, tt, alpha);
-    count_launch();
-    dev::k_interp_velocity<<<nb, 256, 0, s>>>(np, out, init, uoo, uo, uc, w.a, w.b, w.c, w.fa,
-                                               w.fb, w.fc);
-    SSG_CUDA(c, cudaGetLastError());
-    return SSG_OK;
-  };
   const double a[4] = {0.0, 0.5, 0.5, 1.0};
   const double b[4] = {1.0, 2.0, 2.0, 1.0};
-
-  SSG_TRY(interp(du, true, t0, beta));
+  {
+    const InterpWeights w = interp_weights(c, t0, beta);
+    count_launch();
+    dev::k_interp_velocity<<<nb, 256, 0, s>>>(np, du, true, uoo, uo, uc, w.a, w.b, w.c, w.fa,
+                                               w.fb, w.fc);
+    SSG_CUDA(c, cudaGetLastError());
+  }
   int k = 0;
   while (t0 + (double)k++ * dt < t - 0.5 * dt) {
     for (int i = 0; i < 4; ++i) {
+      const InterpWeights w = interp_weights(c, t0 + ((double)(k - 1) + a[i]) * dt, 1.0);
       count_launch();
-      dev::k_stage_field<<<nb, 256, 0, s>>>(np, y, du, i > 0 ? f[i - 1] : du, -dt * a[i], i > 0);
+      dev::k_stage_inputs<<<nb, 256, 0, s>>>(np, y, du, i > 0 ? f[i - 1] : du, -dt * a[i],
+                                             i > 0, ut, uoo, uo, uc, w.a, w.b, w.c, w.fa, w.fb,
+                                             w.fc);
       SSG_CUDA(c, cudaGetLastError());
-      SSG_TRY(interp(ut, false, t0 + ((double)(k - 1) + a[i]) * dt, 1.0));
       SSG_CUDA(c, run_convection(s, c->nel, 0, c->nel, c->n, c->m, ut, y, f[i], c->conv_w,
                                  c->host.conv.D.data(), c->host.jconv.data(), c->conv_D,
                                  c->conv_J, c->conv_scratch));
-      // trivec_inverse_mass_matrix: per component DSS, then 1 / DSS(mass)
-      for (int comp = 0; comp < 3; ++comp) {
-        double* fc = f[i] + comp * npc;
-        SSG_CUDA(c, run_dss(s, DSS_PLAIN, false, L.n, c->nel, fc, y + comp * npc, c->d_pairs,
-                            L.dss_ec, nullptr, nullptr, nullptr, nullptr));
-        SSG_CUDA(c, cudaMemcpyAsync(fc, y + comp * npc, npc * sizeof(double),
-                                    cudaMemcpyDeviceToDevice, s));
-        SSG_CUDA(c, run_mul(s, false, npc, fc, c->inv_mass));
-      }
+      // trivec_inverse_mass_matrix: per component the DSS, then the product
+      // with 1 / DSS(mass), in one pass
+      for (int comp = 0; comp < 3; ++comp)
+        SSG_CUDA(c, run_dss(s, DSS_SCALE, false, L.n, c->nel, f[i] + comp * npc,
+                            y + comp * npc, c->d_pairs, L.dss_ec, nullptr, c->inv_mass, nullptr,
+                            nullptr));
+      std::swap(f[i], y);
     }
-    for (int i = 0; i < 4; ++i) {
-      count_launch();
-      dev::k_axpy<<<nb, 256, 0, s>>>(np, du, f[i], -dt * b[i] / 6.0);
-      SSG_CUDA(c, cudaGetLastError());
-    }
+    count_launch();
+    dev::k_axpy4<<<nb, 256, 0, s>>>(np, du, f[0], f[1], f[2], f[3], -dt * b[0] / 6.0,
+                                    -dt * b[1] / 6.0, -dt * b[2] / 6.0, -dt * b[3] / 6.0);
+    SSG_CUDA(c, cudaGetLastError());
   }
   SSG_CUDA(c, cudaMemcpyAsync(u, du, np * sizeof(double), cudaMemcpyDefault, s));
   SSG_CUDA(c, cudaStreamSynchronize(s));

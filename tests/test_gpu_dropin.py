@@ -28,9 +28,10 @@ viscosity, 10 steps: the same bars, and both runs within ES_EXACT of the
 exact velocity.
 
 Bars (each stated where it is asserted):
-  * every solve of every step: the same number of iterations, or one apart
-    only where the residual at the deciding iteration lies within a factor 2
-    of eps (conftest.same_stop); Helmholtz (Jacobi CG) residual histories as
+  * every solve of every step: the same number of iterations, or else, from
+    the shorter run's last iteration on, every residual but each run's last
+    within a factor 2 of eps (the stop then falls where rounding puts it);
+    Helmholtz (Jacobi CG) residual histories as
     conftest.check_history (with eps itself as the floor), pressure (FCG +
     p-multigrid) histories: the first residual within POISSON_INPUT_EPS
     times eps, the rest within POISSON_HIST_REL of the first residual plus
@@ -272,12 +273,24 @@ def _check_steps(cpu, gpu, steps, label):
           f"deviation {worst[6]:.2e} absolute ({worst[6] / worst[4][0]:.2e} of h0, step "
           f"{worst[0]}, solve {worst[1]}), fields u v w p after {steps} steps "
           f"{', '.join(f'{d:.2e}' for d in devs)}")
+    for r in rows:
+        if r[2] != r[3]:
+            print(f"  step {r[0]} solve {tuple(int(v) for v in r[1])} stops apart: "
+                  f"{' '.join(f'{h:.3e}' for h in r[4])} / {' '.join(f'{h:.3e}' for h in r[5])}")
     for s, kv, lc, lg, hc, hg, dmax in rows:
         if lc != lg:
-            assert abs(lc - lg) == 1, (s, kv, lc, lg)
+            # the stop differs only where rounding decides it: from the
+            # shorter run's last iteration on, each run's residuals lie
+            # within a factor 2 of eps until its own last one (which may
+            # fall further).  Late in the run a pressure solve starts a few
+            # eps from the stop, and the V-cycle, whose inner solves stop on
+            # the same absolute eps, then lowers the residual only slowly:
+            # it can sit just above eps for an iteration or two in one
+            # arithmetic and just below in the other
             k = min(lc, lg) - 1
-            for h in (hc[k], hg[k]):
-                assert 0.5 * EPS <= h <= 2 * EPS, (s, kv, hc, hg)
+            for h in (hc, hg):
+                band = h[k:max(k + 1, len(h) - 1)]
+                assert all(0.5 * EPS <= v <= 2 * EPS for v in band), (s, kv, lc, lg, hc, hg)
         d = history_deviation(hg, hc)
         if kv[0] == 0:
             # FCG + p-multigrid: the first residual (the step's input)
