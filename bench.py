@@ -77,7 +77,7 @@ def parse():
                     help="conv section: the launches only, no timing loop")
     ap.add_argument("--sections", default="all",
                     choices=["all", "fp64", "mixed", "op", "conv", "serve", "extra", "channel",
-                             "particles"],
+                             "particles", "step"],
                     help="fp64: only the FP64 solves; op / conv: only the operator / "
                          "convection launches (for profiler captures)")
     return ap.parse_args()
@@ -682,6 +682,54 @@ def run_convection(args, ctx, mesh, n, device, calls=25):
             "substeps_ms_per_step": ms_sub / 5}
 
 
+def run_timestep(args, ctx, mesh, n, device, steps=5, warmup=2):
+    """The whole time step on the device (ssg_navier_stokes_step, the
+    reference's integrate_navier_stokes, src/navier_stokes.c:224-235) on the
+    TGV box from its analytic state: the velocity and pressure at three
+    levels, their convection and double-curl histories computed by the
+    library.  ms_per_step: device time of `steps` steps after `warmup`,
+    with each solve's iterations of the last step."""
+    import numpy as np
+    import torch
+    dev = torch.device("cuda", device)
+    X, Y, Z = (ctx.level_data(0, 12 + a) for a in range(3))
+    dt = 1e-3
+    t = 0.0
+    u, conv, rot, p = [], [], [], []
+    for lev in range(3):
+        g = np.exp(-2.0 * (t - lev * dt) / 1600.0)
+        ul = torch.from_numpy(np.stack([np.sin(X) * np.cos(Y) * np.cos(Z) * g,
+                                        -np.cos(X) * np.sin(Y) * np.cos(Z) * g,
+                                        0 * X])).to(dev)
+        u.append(ul)
+        conv.append(ctx.convection_operator(ul, ul, torch.empty_like(ul)))
+        rot.append(ctx.stokes_operator(0, ul, None, torch.empty_like(ul)))
+        p.append(torch.from_numpy((np.cos(2 * X) + np.cos(2 * Y)) * (np.cos(2 * Z) + 2.0)
+                                  / 16.0 * g * g).to(dev))
+    ctx.flow_set(u, conv, rot, p, None, t)
+    lib_stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    for _ in range(warmup):
+        ctx.navier_stokes_step(history=False)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(lib_stream)
+    last = None
+    for _ in range(steps):
+        last = ctx.navier_stokes_step(history=False)
+    e1.record(lib_stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    npts = mesh.nel * n ** 3
+    return {"workload": f"TGV {args.ne}^3 N={n-1}: integrate_navier_stokes on the device, "
+                        f"dt {dt}, Re 1600, from the analytic state",
+            "ms_per_step": ms, "steps_per_s": 1e3 / ms, "steps_timed": steps,
+            "points": npts,
+            "iterations_last_step": {"pressure": last[0]["iterations"],
+                                     "u": last[1]["iterations"], "v": last[2]["iterations"],
+                                     "w": last[3]["iterations"]}}
+
+
 # ---------------------------------------------------------------------------
 # GPU arm
 # ---------------------------------------------------------------------------
@@ -765,6 +813,14 @@ def run_ours(args):
                "channel": run_channel(args, local)}
         if rank == 0:
             print(json.dumps({"metric": METRIC, "sections": "extra", **res}))
+        ctx.close()
+        return 0
+
+    if args.sections == "step":
+        res = run_timestep(args, ctx, mesh, n, local, steps=max(1, args.steps),
+                           warmup=max(1, args.warmup))
+        if rank == 0 and not args.no_time:
+            print(json.dumps({"metric": METRIC, "sections": "step", "timestep": res}))
         ctx.close()
         return 0
 
@@ -906,6 +962,7 @@ def run_ours(args):
     extra = {}
     if not args.no_extra:
         extra["convection"] = run_convection(args, ctx, mesh, n, local)
+        extra["timestep"] = run_timestep(args, ctx, mesh, n, local)
         extra["particles"] = run_particles(args, ctx, mesh, n, local)
         extra["channel"] = run_channel(args, local)
 
@@ -972,6 +1029,7 @@ def run_ours(args):
         "channel_c3": extra.get("channel"),
         "particles_c4": extra.get("particles"),
         "convection": extra.get("convection"),
+        "timestep": extra.get("timestep"),
         "cpu_baseline": cpu,
         "gpu_launches": int(launches),
         "clocks": clocks,

@@ -310,6 +310,64 @@ ssg_status ssg_set_velocity_history(ssg_context *ctx, const double *u,
 ssg_status ssg_integrate_convection_rk4(ssg_context *ctx, double *u, double t0,
 		double t, double dt, double beta);
 
+/* ---- the whole time step on the device (src/navier_stokes.c) --------------- */
+
+/* The per-element state integrate_navier_stokes (src/navier_stokes.c:
+ * 224-235) reads and writes, gathered over the mesh: level 0 = the current
+ * time (sel->u, sel->conv, sel->rot, sel->p), 1 = sel->old->..., 2 =
+ * sel->old->old->...  u, conv, rot and f hold three components of
+ * nel x n^3 each (component-major); p one.  Host or device pointers. */
+typedef struct ssg_flow_fields {
+	double *u[3];     /* velocity */
+	double *conv[3];  /* convection history (the velocity's self-convection) */
+	double *rot[3];   /* double-curl history (curl curl u times the mass) */
+	double *p[3];     /* pressure */
+	double *f;        /* body force (sel->f); may be null: zero */
+} ssg_flow_fields;
+
+/* Copy the state in (every level of u, conv, rot and p is needed) at
+ * solver time t (params->t).  The fields then stay on the device; the
+ * parameters of ssg_set_parameters are the step's dt, visc and dens.
+ * Needs the dealiasing grid and the level-0 Jacobian
+ * (ssg_setup_particle_geometry, or ssg_setup_mesh with particles). */
+ssg_status ssg_flow_set(ssg_context *ctx, const ssg_flow_fields *in, double t);
+/* Copy the resident state out into the non-null pointers of out; *t (if
+ * not null) = the solver time. */
+ssg_status ssg_flow_get(ssg_context *ctx, ssg_flow_fields *out, double *t);
+/* One step of integrate_navier_stokes on the resident state: the convection
+ * history and sub-steps, the pressure right-hand side, extrapolation and
+ * solve, the velocity right-hand sides, extrapolation and solves; the time
+ * advances by dt.  f (3 x nel x n^3, may be null: the resident body force
+ * stays) is the step's source term (set_source_term at t + dt).  On a mesh
+ * with walls, bc_u and bc_dudt (3 x nel x n^3 each) hold the boundary
+ * functions sel->bc_func[c] and sel->bc_dfunc[c] at t + dt on every wall
+ * node (other entries are not read); without walls they may be null.
+ * info (may be null): 4 records, the pressure solve and the three velocity
+ * solves in order.  Returns SSG_MAXITER (after finishing the step) when a
+ * solve reached the reference's cap of 5000 iterations. */
+ssg_status ssg_navier_stokes_step(ssg_context *ctx, const double *f,
+		const double *bc_u, const double *bc_dudt, ssg_solve_info *info);
+
+/* The Stokes operators of the step, element by element without a DSS, on
+ * the same fields as the step (its scratch: not while a step runs):
+ *   SSG_STOKES_DOUBLE_CURL: out (3 fields) = double_curl_operator(in)
+ *     (src/stokes.c:94-105: the mass times curl curl of in, 3 fields);
+ *   SSG_STOKES_PRESSURE_RHS: out (1 field) = -dens/dt times
+ *     discrete_divergence_operator(in) (src/stokes.c:52-69) plus, on the
+ *     wall faces, add_surface_integral of the three fields g
+ *     (src/navier_stokes.c:132-141);
+ *   SSG_STOKES_VELOCITY_RHS: out (3 fields) = the mass times in / (dt visc)
+ *     minus (discrete_gradient_operator(g) plus, on the faces without a
+ *     wall, add_surface_integral of g, one field) / (visc dens)
+ *     (src/navier_stokes.c:180-196). */
+enum {
+	SSG_STOKES_DOUBLE_CURL = 0,
+	SSG_STOKES_PRESSURE_RHS = 1,
+	SSG_STOKES_VELOCITY_RHS = 2
+};
+ssg_status ssg_stokes_operator(ssg_context *ctx, int which, const double *in,
+		const double *g, double *out);
+
 /* ---- launch-shape autotuner (no reference counterpart) ---------------------- */
 
 /* Time every candidate launch shape of the operator (elements per block),

@@ -327,6 +327,7 @@ class Reference(_Common):
             L.ssgref_particles_advance.argtypes = [C.c_size_t, _dp, _ip]
             L.ssgref_set_level0_factor.argtypes = [C.c_int, _dp]
             L.ssgref_set_svv.argtypes = [C.c_int, C.c_double]
+            L.ssgref_stokes_operator.argtypes = [C.c_int, _dp, _dp, _dp]
             L.ssgref_integrate_convection_rk4.argtypes = [_dp, C.c_double, C.c_double,
                                                           C.c_double, C.c_double]
             L.ssgref_particles_advance.restype = C.c_int
@@ -459,6 +460,19 @@ class Reference(_Common):
     def ns_step(self):
         self.lib().ssgref_ns_step()
 
+    def stokes_operator(self, which, u, g=None):
+        """The Stokes operators of a step, element by element (no DSS):
+        which 0 = double_curl_operator(u); 1 = the pressure right-hand side
+        of u~ = u with the surface terms of g (3 fields) on the walls; 2 =
+        the velocity right-hand sides of u~ = u and the pressure g."""
+        u = _f64(u)
+        shape = self._shape()
+        out = np.zeros(shape if which == 1 else (3,) + shape)
+        if g is None:
+            g = np.zeros((3,) + shape)
+        self.lib().ssgref_stokes_operator(which, _d(u), _d(_f64(g)), _d(out))
+        return out
+
     def step_log(self, clear=True):
         """Every solve the Navier-Stokes steps ran since the last clear:
         list of (kind 0 Poisson / 1 Helmholtz, var, residual history)."""
@@ -519,3 +533,9 @@ class ReferenceGPU(Reference):
 
     _lib = None
     _path = REF_GPU_SO
+
+    def device_step(self, on):
+        """integrate_navier_stokes as one library step on the device (True,
+        the binding's default) or the reference's own step with its solves
+        bound to the library (False)."""
+        self.lib().ssgref_gpu_device_step(1 if on else 0)

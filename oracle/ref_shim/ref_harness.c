@@ -630,6 +630,60 @@ void ssgref_integrate_convection_rk4(double *u, double t0, double t, double dt,
 	free_ptr_array(tu, H_nel, free_trivec);
 }
 
+/* The Stokes operators of a time step on flat fields, element by element
+ * with the reference's functions (no DSS):
+ * which 0: out (3 fields) = double_curl_operator(in) (src/stokes.c:94-105);
+ * which 1: out (1 field) = discrete_divergence_operator(in) scaled by
+ *   -dens/dt, plus add_surface_integral of g (3 fields) on the wall faces,
+ *   the steps of compute_pressure_rhs (src/navier_stokes.c:132-141);
+ * which 2: out (3 fields) = the steps of compute_velocity_rhs
+ *   (src/navier_stokes.c:180-196) on in = u~ and g = p (1 field). */
+void ssgref_stokes_operator(int which, const double *in, const double *g,
+		double *out)
+{
+	static const int deriv[3] = { X_DERIV, Y_DERIV, Z_DERIV };
+	const size_t nt = (size_t) H_n * H_n * H_n;
+	struct trivec *ti = new_trivec(H_n);
+	struct trivec *tg = new_trivec(H_n);
+	struct trivec *to = new_trivec(H_n);
+	double ***p = new_3d_array(H_n, H_n, H_n);
+	for (int e = 0; e < H_nel; ++e) {
+		struct element *s = H_sel[e];
+		trivec_in(ti, in, e);
+		if (which == 0) {
+			double_curl_operator(s, ti, to);
+			trivec_out(to, out, e);
+		} else if (which == 1) {
+			trivec_in(tg, g, e);
+			discrete_divergence_operator(s, ti, p);
+			scale_array(**p, s->ntot, -s->params->dens / s->params->dt);
+			for (int j = 0; j < 3; ++j)
+				add_surface_integral(s, *tg->ind[j], p, deriv[j],
+						~s->bc);
+			memcpy(out + e * nt, **p, nt * sizeof(double));
+		} else {
+			memcpy(**p, g + e * nt, nt * sizeof(double));
+			scale_trivec(ti, s->ntot, 1.0 / (s->params->dt
+					* s->params->visc));
+			discrete_gradient_operator(s, p, tg);
+			for (int j = 0; j < 3; ++j) {
+				test_function_inner_product(s, *ti->ind[j],
+						*to->ind[j]);
+				add_surface_integral(s, p, *tg->ind[j], deriv[j],
+						s->bc);
+				add_array(***tg->ind[j], ***to->ind[j], s->ntot,
+						-1.0 / (s->params->visc
+						* s->params->dens));
+			}
+			trivec_out(to, out, e);
+		}
+	}
+	free_3d_array(p);
+	free_trivec(ti);
+	free_trivec(tg);
+	free_trivec(to);
+}
+
 /* ---- Navier-Stokes step on the Taylor-Green vortex ---- */
 
 static double tgv_u(double x, double y, double z, double t)
@@ -698,62 +752,71 @@ void ssgref_ns_step(void)
 	set_source_term(H_sel, Y_SOURCE, one_func, H_params->gy);
 	set_source_term(H_sel, Z_SOURCE, one_func, H_params->gz);
 	integrate_navier_stokes(H_sel);
+#ifdef SSGREF_GPU_SHIM
+	/* a step the binding ran on the device: its four solves */
+	const struct ssenss_gpu_solve *g;
+	const int k = ssenss_gpu_step_solves(&g);
+	for (int i = 0; i < k; ++i)
+		step_record(g[i].kind, g[i].var, g[i].history,
+				g[i].history_len < 5001 ? g[i].history_len : 5001);
+#endif
 }
+
+#ifdef SSGREF_GPU_SHIM
+/* integrate_navier_stokes on the device (1) or the reference's own step
+ * with its solves bound to the library (0) */
+void ssgref_gpu_device_step(int on)
+{
+	ssenss_gpu_device_step(on);
+}
+#endif
 
 double ssgref_time(void)
 {
 	return H_params->t;
 }
 
-/* which: 0..2 = u,v,w; 3 = p; 4..6 = reference-domain velocity ur. */
+/* The field `which` of history level hist_level of element s:
+ * 0..2 = u,v,w; 3 = p; 4..6 = reference-domain velocity ur; 7..9 = the
+ * convection history conv; 10..12 = the double-curl history rot. */
+static double ***state_field(struct element *s, int which, int hist_level)
+{
+	struct trivec *u = s->u, *ur = s->ur, *cv = s->conv, *rt = s->rot;
+	double ***p = s->p;
+	if (hist_level >= 1) {
+		u = s->old->u; ur = s->old->ur; p = s->old->p;
+		cv = s->old->conv; rt = s->old->rot;
+	}
+	if (hist_level >= 2) {
+		u = s->old->old->u; ur = s->old->old->ur;
+		p = s->old->old->p;
+		cv = s->old->old->conv; rt = s->old->old->rot;
+	}
+	if (which < 3)
+		return *u->ind[which];
+	if (which == 3)
+		return p;
+	if (which < 7)
+		return *ur->ind[which - 4];
+	if (which < 10)
+		return *cv->ind[which - 7];
+	return *rt->ind[which - 10];
+}
+
 void ssgref_get_field(int which, int hist_level, double *dst)
 {
 	const size_t nt = (size_t) H_n * H_n * H_n;
-	for (int e = 0; e < H_nel; ++e) {
-		struct element *s = H_sel[e];
-		double ***src;
-		struct trivec *u = s->u, *ur = s->ur;
-		double ***p = s->p;
-		if (hist_level >= 1) {
-			u = s->old->u; ur = s->old->ur; p = s->old->p;
-		}
-		if (hist_level >= 2) {
-			u = s->old->old->u; ur = s->old->old->ur;
-			p = s->old->old->p;
-		}
-		if (which < 3)
-			src = *u->ind[which];
-		else if (which == 3)
-			src = p;
-		else
-			src = *ur->ind[which - 4];
-		memcpy(dst + e * nt, **src, nt * sizeof(double));
-	}
+	for (int e = 0; e < H_nel; ++e)
+		memcpy(dst + e * nt, **state_field(H_sel[e], which, hist_level),
+				nt * sizeof(double));
 }
 
 void ssgref_set_field(int which, int hist_level, const double *src)
 {
 	const size_t nt = (size_t) H_n * H_n * H_n;
-	for (int e = 0; e < H_nel; ++e) {
-		struct element *s = H_sel[e];
-		double ***dst;
-		struct trivec *u = s->u, *ur = s->ur;
-		double ***p = s->p;
-		if (hist_level >= 1) {
-			u = s->old->u; ur = s->old->ur; p = s->old->p;
-		}
-		if (hist_level >= 2) {
-			u = s->old->old->u; ur = s->old->old->ur;
-			p = s->old->old->p;
-		}
-		if (which < 3)
-			dst = *u->ind[which];
-		else if (which == 3)
-			dst = p;
-		else
-			dst = *ur->ind[which - 4];
-		memcpy(**dst, src + e * nt, nt * sizeof(double));
-	}
+	for (int e = 0; e < H_nel; ++e)
+		memcpy(**state_field(H_sel[e], which, hist_level), src + e * nt,
+				nt * sizeof(double));
 }
 
 /* ---- particles (src/particles.c:182-218) ---- */

@@ -346,6 +346,77 @@ class Context:
                     "integrate_convection_rk4")
         return u
 
+    # -- the whole time step (src/navier_stokes.c:224-235) -------------------
+    def flow_set(self, u, conv, rot, p, f=None, t=0.0):
+        """ssg_flow_set: u, conv, rot: three levels (newest first) of (3,
+        nel, n, n, n); p: three levels of (nel, n, n, n); f: (3, nel, n, n,
+        n) or None (zero); t: solver time."""
+        ff = _lib.FlowFields()
+        for l in range(3):
+            ff.u[l] = _ptr(u[l])
+            ff.conv[l] = _ptr(conv[l])
+            ff.rot[l] = _ptr(rot[l])
+            ff.p[l] = _ptr(p[l])
+        ff.f = _ptr(f) if f is not None else None
+        self._check(self.lib.ssg_flow_set(self.h, C.byref(ff), float(t)), "flow_set")
+
+    def flow_get(self):
+        """ssg_flow_get: dict of u, conv, rot (3 levels each, newest first),
+        p (3 levels), f and t, as numpy arrays."""
+        sh = self.shape()
+        out = {k: [np.empty((3,) + sh) for _ in range(3)] for k in ("u", "conv", "rot")}
+        out["p"] = [np.empty(sh) for _ in range(3)]
+        out["f"] = np.empty((3,) + sh)
+        ff = _lib.FlowFields()
+        for l in range(3):
+            ff.u[l] = _ptr(out["u"][l])
+            ff.conv[l] = _ptr(out["conv"][l])
+            ff.rot[l] = _ptr(out["rot"][l])
+            ff.p[l] = _ptr(out["p"][l])
+        ff.f = _ptr(out["f"])
+        t = C.c_double()
+        self._check(self.lib.ssg_flow_get(self.h, C.byref(ff), C.byref(t)), "flow_get")
+        out["t"] = t.value
+        return out
+
+    def navier_stokes_step(self, f=None, bc_u=None, bc_dudt=None, history=True):
+        """ssg_navier_stokes_step: one step on the resident fields.  Returns
+        the four solves (pressure, then u, v, w) as dicts."""
+        infos = (SolveInfo * 4)()
+        hists = []
+        if history:
+            for k in range(4):
+                h = np.zeros(5001)
+                hists.append(h)
+                infos[k].history = h.ctypes.data_as(_lib._dp)
+                infos[k].history_cap = len(h)
+        st = self.lib.ssg_navier_stokes_step(
+            self.h, _ptr(f) if f is not None else None,
+            _ptr(bc_u) if bc_u is not None else None,
+            _ptr(bc_dudt) if bc_dudt is not None else None, infos)
+        self._check(st, "navier_stokes_step", ok=(0, 5))
+        res = []
+        for k in range(4):
+            i = infos[k]
+            d = {"iterations": i.iterations, "residual": i.residual,
+                 "initial_residual": i.initial_residual, "solve_ms": i.solve_ms}
+            if history:
+                d["history"] = hists[k][:i.history_len].copy()
+            res.append(d)
+        return res
+
+    def stokes_operator(self, which, u, g=None, out=None):
+        """ssg_stokes_operator: which 0 = double curl of u; 1 = pressure
+        right-hand side of u~ = u and g (3 fields); 2 = velocity right-hand
+        sides of u~ = u and the pressure g (no DSS)."""
+        if out is None:
+            sh = self.shape()
+            out = np.empty(sh if which == 1 else (3,) + sh)
+        self._check(self.lib.ssg_stokes_operator(self.h, int(which), _ptr(u),
+                                                 _ptr(g) if g is not None else None,
+                                                 _ptr(out)), "stokes_operator")
+        return out
+
     def convection_elements(self, first, u, v, out=None):
         """ssg_convection_elements: convection of the elements first ..
         first + count - 1, fields shaped (3, count, n, n, n)."""

@@ -43,6 +43,18 @@ class Request(C.Structure):
     ]
 
 
+class FlowFields(C.Structure):
+    """ssg_flow_fields: history levels newest first; u, conv, rot and f
+    three fields each, p one."""
+    _fields_ = [
+        ("u", C.c_void_p * 3),
+        ("conv", C.c_void_p * 3),
+        ("rot", C.c_void_p * 3),
+        ("p", C.c_void_p * 3),
+        ("f", C.c_void_p),
+    ]
+
+
 class ServerStats(C.Structure):
     _fields_ = [
         ("submitted", C.c_ulonglong), ("completed", C.c_ulonglong),
@@ -110,6 +122,12 @@ SIGNATURES = [
                                            C.c_double, C.c_double]),
     ("ssg_integrate_convection_rk4", C.c_int, [C.c_void_p, C.c_void_p, C.c_double, C.c_double,
                                                C.c_double, C.c_double]),
+    ("ssg_flow_set", C.c_int, [C.c_void_p, C.POINTER(FlowFields), C.c_double]),
+    ("ssg_flow_get", C.c_int, [C.c_void_p, C.POINTER(FlowFields), _dp]),
+    ("ssg_navier_stokes_step", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                         C.POINTER(SolveInfo)]),
+    ("ssg_stokes_operator", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+                                      C.c_void_p]),
     ("ssg_memory_info", C.c_int, [C.c_void_p, C.POINTER(C.c_size_t)]),
     ("ssg_request_bytes", C.c_size_t, [C.c_int, C.c_int, C.c_int]),
     ("ssg_gll", C.c_int, [C.c_int, _dp, _dp]),

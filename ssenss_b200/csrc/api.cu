@@ -80,6 +80,14 @@ static void free_mesh(ssg_context* c) {
   if (c->vhist) cudaFree(c->vhist);
   if (c->rk_scratch) cudaFree(c->rk_scratch);
   c->vhist = c->rk_scratch = nullptr;
+  dfree(c->flow_buf);
+  dfree(c->flow_sw);
+  dfree(c->flow_bc);
+  c->flow_buf = c->flow_sw = nullptr;
+  c->flow_bc = nullptr;
+  for (int l = 0; l < 3; ++l) c->fu[l] = c->fconv[l] = c->frot[l] = c->fp[l] = nullptr;
+  c->ff = c->fut = c->fa = c->fb = c->fbc = nullptr;
+  c->flow_ready = false;
   for (auto& l : c->lev) free_level(l);
   dfree(c->d_pairs); c->d_pairs = nullptr;
   dfree(c->inv_mass); c->inv_mass = nullptr;

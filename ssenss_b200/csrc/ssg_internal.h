@@ -214,6 +214,24 @@ struct ssg_context {
   double* vhist = nullptr;
   double vhist_t = 0.0, vhist_dt = 0.0;
   double* rk_scratch = nullptr;
+  // resident time step (flow.cu): one allocation holding the velocity,
+  // convection and double-curl histories (3 fields each), the pressure
+  // history, the body force, u~, two scratch triples and the wall values;
+  // history slots newest first, rotated by the time shifts
+  double* flow_buf = nullptr;
+  double* fu[3] = {nullptr, nullptr, nullptr};
+  double* fconv[3] = {nullptr, nullptr, nullptr};
+  double* frot[3] = {nullptr, nullptr, nullptr};
+  double* fp[3] = {nullptr, nullptr, nullptr};
+  double* ff = nullptr;
+  double* fut = nullptr;
+  double* fa = nullptr;
+  double* fb = nullptr;
+  double* fbc = nullptr;        // walls: u (3 fields), then du/dt (3 fields)
+  double* flow_sw = nullptr;    // surface weights (nel x 3 x 6 x n^2)
+  int* flow_bc = nullptr;       // wall face bits per element
+  double flow_t = 0.0;
+  bool flow_ready = false;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
 
@@ -262,6 +280,13 @@ ssg_status mg_apply(ssg_context* c, const double* r, double* z, double eps);
 ssg_status fcg_solve(ssg_context* c, const double* f, double* u, double eps, int max_iter,
                      ssg_solve_info* info);
 ssg_status helmholtz_diag_update(ssg_context* c);
+// timestep.cu: the convection sub-steps of integrate_convection_rk4 on
+// device fields (du, 3 fields, in/out; the velocity history oldest first,
+// at time th with step dth), and the scratch they use
+ssg_status ensure_rk_scratch(ssg_context* c);
+ssg_status convection_rk4(ssg_context* c, double* du, double t0, double t, double dt,
+                          double beta, const double* uoo, const double* uo, const double* uc,
+                          double th, double dth);
 // drop captured CUDA graphs (launch shapes or buffers changed)
 void invalidate_graphs(ssg_context* c);
 

@@ -232,6 +232,18 @@ bool convection_dmma_applies(int n, int m);
 cudaError_t run_convection_dmma(cudaStream_t s, int nel, int e0, int nel_fac, const double* u,
                                 const double* v, double* udv, const double* W,
                                 const double* Dh, const double* Jh);
+// Stokes operators of the time step, one element per block (stokes.cu):
+// which 0 = the double curl of in (3 fields) into out (3 fields); 1 = the
+// pressure right-hand side of in = u~ (3 fields) and g (3 fields, surface
+// terms on the wall faces) into out (1 field), x = -dens / dt; 2 = the
+// velocity right-hand sides of in = u~ and g = p (1 field, surface terms on
+// the other faces) into out (3 fields), x = 1 / (dt visc), y = -1 / (visc
+// dens).  tinv: 9 x npts; rho: n^3; det: npts; D: n x n; bc: wall face bits
+// per element; sw: surface weights (nel x 3 x 6 x n^2)
+cudaError_t run_stokes(cudaStream_t s, int which, int n, int nel, const double* tinv,
+                       const double* rho, const double* det, const double* D, const int* bc,
+                       const double* sw, size_t npts, const double* in, const double* g,
+                       double* out, double x, double y);
 // Lagrangian particle advance to time t (particles.cu); passes: device int
 // that receives the largest per-particle pass count (atomicMax, caller zeroes).
 // order (np ints) and bucket (2 (nel + 1) ints): scratch of the element-order

@@ -96,8 +96,7 @@ struct InterpWeights {
   bool fa, fb, fc;
 };
 
-InterpWeights interp_weights(const ssg_context* c, double t, double alpha) {
-  const double t0 = c->vhist_t, dt0 = c->vhist_dt;
+InterpWeights interp_weights(double t0, double dt0, double t, double alpha) {
   const double d[3] = {t - t0 + 2.0 * dt0, t - t0 + dt0, t - t0};
   const double a = 0.5 * d[1] * d[2] / std::pow(dt0, 2);
   const double b = -d[0] * d[2] / std::pow(dt0, 2);
@@ -114,6 +113,74 @@ InterpWeights interp_weights(const ssg_context* c, double t, double alpha) {
 }
 
 }  // namespace
+
+namespace ssg {
+
+ssg_status ensure_rk_scratch(ssg_context* c) {
+  if (c->rk_scratch) return SSG_OK;
+  // the stage field y, the interpolated velocity, f_0 .. f_3 and the field
+  // of the C entry point, 3 x npts each
+  void* p = nullptr;
+  if (cudaMalloc(&p, 7 * 3 * c->lev[0].npts * sizeof(double)) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(c, SSG_ERR_NOMEM, "convection sub-step scratch");
+  }
+  c->rk_scratch = static_cast<double*>(p);
+  return SSG_OK;
+}
+
+ssg_status convection_rk4(ssg_context* c, double* du, double t0, double t, double dt,
+                          double beta, const double* uoo, const double* uo, const double* uc,
+                          double th, double dth) {
+  const DevLevel& L = c->lev[0];
+  const size_t npc = L.npts, np = 3 * npc;
+  cudaStream_t s = c->stream;
+  SSG_TRY(ensure_rk_scratch(c));
+  // f[i] holds the stage's raw convection, then the buffer y held is swapped
+  // in: the DSS with the inverse mass product reads f[i] and writes y, and
+  // the stage field's buffer is free again once the convection has run
+  double* y = c->rk_scratch;
+  double* ut = y + np;
+  double* f[4] = {ut + np, ut + 2 * np, ut + 3 * np, ut + 4 * np};
+  const int nb = vec_blocks(np);
+  const double a[4] = {0.0, 0.5, 0.5, 1.0};
+  const double b[4] = {1.0, 2.0, 2.0, 1.0};
+  {
+    const InterpWeights w = interp_weights(th, dth, t0, beta);
+    count_launch();
+    dev::k_interp_velocity<<<nb, 256, 0, s>>>(np, du, true, uoo, uo, uc, w.a, w.b, w.c, w.fa,
+                                               w.fb, w.fc);
+    SSG_CUDA(c, cudaGetLastError());
+  }
+  int k = 0;
+  while (t0 + (double)k++ * dt < t - 0.5 * dt) {
+    for (int i = 0; i < 4; ++i) {
+      const InterpWeights w = interp_weights(th, dth, t0 + ((double)(k - 1) + a[i]) * dt, 1.0);
+      count_launch();
+      dev::k_stage_inputs<<<nb, 256, 0, s>>>(np, y, du, i > 0 ? f[i - 1] : du, -dt * a[i],
+                                             i > 0, ut, uoo, uo, uc, w.a, w.b, w.c, w.fa, w.fb,
+                                             w.fc);
+      SSG_CUDA(c, cudaGetLastError());
+      SSG_CUDA(c, run_convection(s, c->nel, 0, c->nel, c->n, c->m, ut, y, f[i], c->conv_w,
+                                 c->host.conv.D.data(), c->host.jconv.data(), c->conv_D,
+                                 c->conv_J, c->conv_scratch));
+      // trivec_inverse_mass_matrix: per component the DSS, then the product
+      // with 1 / DSS(mass), in one pass
+      for (int comp = 0; comp < 3; ++comp)
+        SSG_CUDA(c, run_dss(s, DSS_SCALE, false, L.n, c->nel, f[i] + comp * npc,
+                            y + comp * npc, c->d_pairs, L.dss_ec, nullptr, c->inv_mass, nullptr,
+                            nullptr));
+      std::swap(f[i], y);
+    }
+    count_launch();
+    dev::k_axpy4<<<nb, 256, 0, s>>>(np, du, f[0], f[1], f[2], f[3], -dt * b[0] / 6.0,
+                                    -dt * b[1] / 6.0, -dt * b[2] / 6.0, -dt * b[3] / 6.0);
+    SSG_CUDA(c, cudaGetLastError());
+  }
+  return SSG_OK;
+}
+
+}  // namespace ssg
 
 extern "C" {
 
@@ -154,67 +221,15 @@ ssg_status ssg_integrate_convection_rk4(ssg_context* c, double* u, double t0, do
   if (!(dt > 0.0) || !std::isfinite(t0) || !std::isfinite(t) || !std::isfinite(beta))
     return fail(c, SSG_ERR_ARG, "bad time arguments");
   SSG_CUDA(c, cudaSetDevice(c->device));
-  const DevLevel& L = c->lev[0];
-  const size_t npc = L.npts, np = 3 * npc;
-  cudaStream_t s = c->stream;
-  if (!c->rk_scratch) {
-    // staged u, the stage field y, the interpolated velocity, f_0 .. f_3
-    void* p = nullptr;
-    if (cudaMalloc(&p, 7 * np * sizeof(double)) != cudaSuccess) {
-      cudaGetLastError();
-      return fail(c, SSG_ERR_NOMEM, "convection sub-step scratch");
-    }
-    c->rk_scratch = static_cast<double*>(p);
-  }
-  // f[i] holds the stage's raw convection, then the buffer y held is swapped
-  // in: the DSS with the inverse mass product reads f[i] and writes y, and
-  // the stage field's buffer is free again once the convection has run
-  double* du = c->rk_scratch;
-  double* y = du + np;
-  double* ut = y + np;
-  double* f[4] = {ut + np, ut + 2 * np, ut + 3 * np, ut + 4 * np};
-  const double* uoo = c->vhist;
-  const double* uo = c->vhist + np;
-  const double* uc = c->vhist + 2 * np;
-  const int nb = vec_blocks(np);
-  SSG_CUDA(c, cudaMemcpyAsync(du, u, np * sizeof(double), cudaMemcpyDefault, s));
-
-  const double a[4] = {0.0, 0.5, 0.5, 1.0};
-  const double b[4] = {1.0, 2.0, 2.0, 1.0};
-  {
-    const InterpWeights w = interp_weights(c, t0, beta);
-    count_launch();
-    dev::k_interp_velocity<<<nb, 256, 0, s>>>(np, du, true, uoo, uo, uc, w.a, w.b, w.c, w.fa,
-                                               w.fb, w.fc);
-    SSG_CUDA(c, cudaGetLastError());
-  }
-  int k = 0;
-  while (t0 + (double)k++ * dt < t - 0.5 * dt) {
-    for (int i = 0; i < 4; ++i) {
-      const InterpWeights w = interp_weights(c, t0 + ((double)(k - 1) + a[i]) * dt, 1.0);
-      count_launch();
-      dev::k_stage_inputs<<<nb, 256, 0, s>>>(np, y, du, i > 0 ? f[i - 1] : du, -dt * a[i],
-                                             i > 0, ut, uoo, uo, uc, w.a, w.b, w.c, w.fa, w.fb,
-                                             w.fc);
-      SSG_CUDA(c, cudaGetLastError());
-      SSG_CUDA(c, run_convection(s, c->nel, 0, c->nel, c->n, c->m, ut, y, f[i], c->conv_w,
-                                 c->host.conv.D.data(), c->host.jconv.data(), c->conv_D,
-                                 c->conv_J, c->conv_scratch));
-      // trivec_inverse_mass_matrix: per component the DSS, then the product
-      // with 1 / DSS(mass), in one pass
-      for (int comp = 0; comp < 3; ++comp)
-        SSG_CUDA(c, run_dss(s, DSS_SCALE, false, L.n, c->nel, f[i] + comp * npc,
-                            y + comp * npc, c->d_pairs, L.dss_ec, nullptr, c->inv_mass, nullptr,
-                            nullptr));
-      std::swap(f[i], y);
-    }
-    count_launch();
-    dev::k_axpy4<<<nb, 256, 0, s>>>(np, du, f[0], f[1], f[2], f[3], -dt * b[0] / 6.0,
-                                    -dt * b[1] / 6.0, -dt * b[2] / 6.0, -dt * b[3] / 6.0);
-    SSG_CUDA(c, cudaGetLastError());
-  }
-  SSG_CUDA(c, cudaMemcpyAsync(u, du, np * sizeof(double), cudaMemcpyDefault, s));
-  SSG_CUDA(c, cudaStreamSynchronize(s));
+  SSG_TRY(ensure_rk_scratch(c));
+  const size_t np = 3 * c->lev[0].npts;
+  double* du = c->rk_scratch + 6 * np;
+  SSG_CUDA(c, cudaMemcpyAsync(du, u, np * sizeof(double), cudaMemcpyDefault, c->stream));
+  const double* h = c->vhist;
+  SSG_TRY(convection_rk4(c, du, t0, t, dt, beta, h, h + np, h + 2 * np, c->vhist_t,
+                         c->vhist_dt));
+  SSG_CUDA(c, cudaMemcpyAsync(u, du, np * sizeof(double), cudaMemcpyDefault, c->stream));
+  SSG_CUDA(c, cudaStreamSynchronize(c->stream));
   return SSG_OK;
 }
 

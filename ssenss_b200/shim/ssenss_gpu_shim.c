@@ -13,6 +13,7 @@
  *   jacobi_preconditioner, multigrid_preconditioner  (src/precon.h:47-50)
  *   convection_operator                              (src/convection.h:22-23)
  *   integrate_convection_rk4                         (src/time.h)
+ *   integrate_navier_stokes                          (src/navier_stokes.h)
  *   integrate_particle_equations                     (src/particles.h:71)
  *
  * The reference's definitions of those names are renamed at build time
@@ -52,6 +53,7 @@
 #include "convection.h"
 #include "particles.h"
 #include "time.h"
+#include "navier_stokes.h"
 
 #include "ssenss_b200.h"
 #include "ssenss_gpu_shim.h"
@@ -66,6 +68,7 @@ static double *G_u;                 /* nel n^3: gathered solution / guess */
 static double *G_conv;              /* 9 n^3: one element's convection operands */
 static double *G_rk;                /* 12 x npts: velocity history and the field of
                                      * integrate_convection_rk4 */
+static double *G_flow;              /* 39 x npts: the state of integrate_navier_stokes */
 static double G_hist[SHIM_HISTORY_CAP];
 static struct ssenss_gpu_solve G_last;
 
@@ -234,7 +237,8 @@ void ssenss_gpu_detach(void)
 	free(G_u);
 	free(G_conv);
 	free(G_rk);
-	G_u = G_conv = G_rk = NULL;
+	free(G_flow);
+	G_u = G_conv = G_rk = G_flow = NULL;
 }
 
 const struct ssenss_gpu_solve *ssenss_gpu_last_solve(void)
@@ -509,6 +513,180 @@ void integrate_convection_rk4(struct element **sel, struct trivec **u,
 			memcpy(***u[i]->ind[c], f + c * np + e * G_nt,
 					G_nt * sizeof(double));
 	}
+}
+
+/* ---- the whole time step (src/navier_stokes.c:224-235) ------------------ */
+
+static int G_device_step = 1;
+static struct ssenss_gpu_solve G_step[4];
+static double G_step_hist[4][SHIM_HISTORY_CAP];
+static int G_step_len;
+
+void ssenss_gpu_device_step(int on)
+{
+	G_device_step = on;
+}
+
+int ssenss_gpu_step_solves(const struct ssenss_gpu_solve **solves)
+{
+	*solves = G_step;
+	return G_step_len;
+}
+
+/* the state of history level l (0 = now, 1 = old, 2 = old->old) */
+struct level_state {
+	struct trivec *u, *conv, *rot;
+	double ***p;
+};
+
+static struct level_state level_state(struct element *s, int l)
+{
+	struct level_state r = { s->u, s->conv, s->rot, s->p };
+	struct old_element *o = s->old;
+	for (int k = 0; k < l; ++k) {
+		r.u = o->u;
+		r.conv = o->conv;
+		r.rot = o->rot;
+		r.p = o->p;
+		o = o->old;
+	}
+	return r;
+}
+
+/* one trivec per element into / out of dst, component-major */
+static void move_trivec(double *buf, struct trivec *t, int e, int out)
+{
+	const size_t np = G_nt * G_nel;
+	for (int c = 0; c < 3; ++c) {
+		double *d = buf + c * np + (size_t) e * G_nt;
+		if (out)
+			memcpy(***t->ind[c], d, G_nt * sizeof(double));
+		else
+			memcpy(d, ***t->ind[c], G_nt * sizeof(double));
+	}
+}
+
+/* staging layout: per level u, conv, rot (3 fields each), p (1 field);
+ * then f, the wall values of u and of du/dt (3 fields each) */
+static void flow_fields(ssg_flow_fields *ff)
+{
+	const size_t np = G_nt * G_nel;
+	for (int l = 0; l < 3; ++l) {
+		double *b = G_flow + (size_t) l * 10 * np;
+		ff->u[l] = b;
+		ff->conv[l] = b + 3 * np;
+		ff->rot[l] = b + 6 * np;
+		ff->p[l] = b + 9 * np;
+	}
+	ff->f = G_flow + 30 * np;
+}
+
+static void move_state(struct element **sel, int out)
+{
+	ssg_flow_fields ff;
+	flow_fields(&ff);
+	for (int i = 0; i < G_nel; ++i) {
+		const int e = sel[i]->geom->id;
+		for (int l = 0; l < 3; ++l) {
+			struct level_state st = level_state(sel[i], l);
+			move_trivec(ff.u[l], st.u, e, out);
+			move_trivec(ff.conv[l], st.conv, e, out);
+			move_trivec(ff.rot[l], st.rot, e, out);
+			double *d = ff.p[l] + (size_t) e * G_nt;
+			if (out)
+				memcpy(**st.p, d, G_nt * sizeof(double));
+			else
+				memcpy(d, **st.p, G_nt * sizeof(double));
+		}
+		if (!out)
+			move_trivec(ff.f, sel[i]->f, e, 0);
+	}
+}
+
+/* bc_func and bc_dfunc of every element at t + dt on its wall nodes, as
+ * set_dirichlet_boundaries evaluates them (src/poisson.c:101-143) */
+static void wall_values(struct element **sel, double *bu, double *bd)
+{
+	const size_t np = G_nt * G_nel;
+	const int n = G_n, m = n - 1;
+	memset(bu, 0, 3 * np * sizeof(double));
+	memset(bd, 0, 3 * np * sizeof(double));
+	for (int i = 0; i < G_nel; ++i) {
+		const struct element *s = sel[i];
+		const int bc = s->bc, e = s->geom->id;
+		if (!bc)
+			continue;
+		const double t = s->params->t + s->params->dt;
+		const double *x = **s->geom->grid->x;
+		const double *y = **s->geom->grid->y;
+		const double *z = **s->geom->grid->z;
+		for (size_t q = 0; q < G_nt; ++q) {
+			const int a = q % n, b = (q / n) % n, k = q / (n * n);
+			const int wall = ((bc & DIRICHLET_W) && a == 0)
+					|| ((bc & DIRICHLET_E) && a == m)
+					|| ((bc & DIRICHLET_S) && b == 0)
+					|| ((bc & DIRICHLET_N) && b == m)
+					|| ((bc & DIRICHLET_B) && k == 0)
+					|| ((bc & DIRICHLET_T) && k == m);
+			if (!wall)
+				continue;
+			for (int c = 0; c < 3; ++c) {
+				const size_t g = c * np + (size_t) e * G_nt + q;
+				bu[g] = s->bc_func[c](x[q], y[q], z[q], t);
+				bd[g] = s->bc_dfunc[c](x[q], y[q], z[q], t);
+			}
+		}
+	}
+}
+
+/* The whole step on the device: the state goes to the library, one
+ * ssg_navier_stokes_step runs the convection history and sub-steps, the
+ * pressure and velocity right-hand sides, extrapolations and the four
+ * solves there, and the state comes back.  With the device step switched
+ * off (ssenss_gpu_device_step(0)) the reference's own integrate_navier_
+ * stokes runs, its solves and convection calls through this binding. */
+void integrate_navier_stokes(struct element **sel)
+{
+	G_step_len = 0;
+	if (!G_device_step) {
+		host_integrate_navier_stokes(sel);
+		return;
+	}
+	need_level0(sel, "integrate_navier_stokes");
+	sync_parameters(sel);
+	const size_t np = G_nt * G_nel;
+	if (!G_flow)
+		G_flow = alloc_doubles(39 * np);
+	move_state(sel, 0);
+	ssg_flow_fields ff;
+	flow_fields(&ff);
+	check(ssg_flow_set(G, &ff, (*sel)->params->t), "integrate_navier_stokes (state)");
+	double *bu = G_flow + 33 * np, *bd = G_flow + 36 * np;
+	wall_values(sel, bu, bd);
+	ssg_solve_info info[4];
+	for (int k = 0; k < 4; ++k) {
+		info[k] = new_info();
+		info[k].history = G_step_hist[k];
+	}
+	ssg_status st = solve_status(ssg_navier_stokes_step(G, ff.f, bu, bd, info),
+			"integrate_navier_stokes");
+	ff.f = NULL;
+	check(ssg_flow_get(G, &ff, NULL), "integrate_navier_stokes (state)");
+	move_state(sel, 1);
+	for (int k = 0; k < 4; ++k) {
+		struct ssenss_gpu_solve *r = &G_step[k];
+		r->kind = k ? 1 : 0;
+		r->var = k ? X_VELOCITY + k - 1 : PRESSURE;
+		r->status = st;
+		r->iterations = info[k].iterations;
+		r->eps = 0.0;
+		r->residual = info[k].residual;
+		r->solve_ms = info[k].solve_ms;
+		r->history_len = info[k].history_len;
+		r->history = G_step_hist[k];
+	}
+	G_step_len = 4;
+	(*sel)->params->t += (*sel)->params->dt;
 }
 
 /* ---- particles (src/particles.c:182-218) ------------------------------ */

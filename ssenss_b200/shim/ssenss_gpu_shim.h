@@ -49,4 +49,19 @@ struct ssenss_gpu_solve {
 };
 const struct ssenss_gpu_solve *ssenss_gpu_last_solve(void);
 
+/* integrate_navier_stokes runs the whole step on the device (on, the
+ * default: ssg_navier_stokes_step on the state copied in and out) or the
+ * reference's own step with its solves and convection calls bound to the
+ * library (off). */
+void ssenss_gpu_device_step(int on);
+
+/* The solves of the last integrate_navier_stokes that ran on the device
+ * (the pressure solve, then the three velocity solves): *solves points at
+ * them; returns how many (0 after a step the reference's code ran). */
+int ssenss_gpu_step_solves(const struct ssenss_gpu_solve **solves);
+
+/* the reference's own step, renamed at build time (-Dintegrate_navier_
+ * stokes=host_integrate_navier_stokes on src/navier_stokes.c) */
+void host_integrate_navier_stokes(struct element **sel);
+
 #endif
