@@ -209,6 +209,23 @@ def reference_sample(mesh, n, f, max_iter):
     return dt, max_iter
 
 
+def reference_step_sample(steps=2):
+    """The reference's integrate_navier_stokes (src/navier_stokes.c:224-235)
+    on C1 (TGV 4^3, n = 8, dt 1e-3, Re 1600) from its initial state, 1 core:
+    seconds per step over `steps` steps after one untimed step."""
+    import oracle
+    from ssenss_b200.mesh import tgv_box
+    ref = oracle.Reference(tgv_box(4), 8, dt=1e-3, visc=1.0 / 1600.0, dens=1.0)
+    ref.init_tgv()
+    ref.ns_step()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        ref.ns_step()
+    dt = (time.perf_counter() - t0) / steps
+    ref.close()
+    return dt
+
+
 # resident memory of one reference process at the 16^3, n = 8 workload
 # (measured: 4.1 GB peak), used to bound how many run at once
 REF_PROC_BYTES = 4.6e9
@@ -682,7 +699,7 @@ def run_convection(args, ctx, mesh, n, device, calls=25):
             "substeps_ms_per_step": ms_sub / 5}
 
 
-def run_timestep(args, ctx, mesh, n, device, steps=5, warmup=2):
+def run_timestep(args, ctx, mesh, n, device, steps=5, warmup=2, c1=True):
     """The whole time step on the device (ssg_navier_stokes_step, the
     reference's integrate_navier_stokes, src/navier_stokes.c:224-235) on the
     TGV box from its analytic state: the velocity and pressure at three
@@ -721,13 +738,27 @@ def run_timestep(args, ctx, mesh, n, device, steps=5, warmup=2):
     e1.synchronize()
     ms = e0.elapsed_time(e1) / steps
     npts = mesh.nel * n ** 3
-    return {"workload": f"TGV {args.ne}^3 N={n-1}: integrate_navier_stokes on the device, "
-                        f"dt {dt}, Re 1600, from the analytic state",
-            "ms_per_step": ms, "steps_per_s": 1e3 / ms, "steps_timed": steps,
-            "points": npts,
-            "iterations_last_step": {"pressure": last[0]["iterations"],
-                                     "u": last[1]["iterations"], "v": last[2]["iterations"],
-                                     "w": last[3]["iterations"]}}
+    out = {"workload": f"TGV {args.ne}^3 N={n-1}: integrate_navier_stokes on the device, "
+                       f"dt {dt}, Re 1600, from the analytic state",
+           "ms_per_step": ms, "steps_per_s": 1e3 / ms, "steps_timed": steps,
+           "points": npts,
+           "iterations_last_step": {"pressure": last[0]["iterations"],
+                                    "u": last[1]["iterations"], "v": last[2]["iterations"],
+                                    "w": last[3]["iterations"]}}
+    if c1:
+        # the same at C1 (TGV 4^3, n = 8), the size the reference's own step
+        # is timed at in the CPU baseline
+        import ssenss_b200 as S
+        from ssenss_b200.mesh import tgv_box
+        small = S.Context(device)
+        try:
+            small.set_parameters(dt, 1.0 / 1600.0, 1.0)
+            small.setup_mesh(tgv_box(4), n)
+            sub = run_timestep(args, small, tgv_box(4), n, device, steps=10, warmup=2, c1=False)
+            out["c1"] = {"ms_per_step": sub["ms_per_step"], "points": sub["points"]}
+        finally:
+            small.close()
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -980,6 +1011,14 @@ def run_ours(args):
         except Exception as ex:  # reported, never fatal
             cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference",
                    "sample": f"failed: {ex}"}
+        if cpu is not None and not args.no_extra:
+            try:
+                cpu["timestep_c1"] = {
+                    "ms_per_step": 1e3 * reference_step_sample(),
+                    "sample": ("integrate_navier_stokes on C1 (TGV 4^3, n = 8), 2 steps after "
+                               "one untimed step, reference compiled in place, 1 thread")}
+            except Exception as ex:  # reported, never fatal
+                cpu["timestep_c1"] = {"ms_per_step": None, "sample": f"failed: {ex}"}
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
