@@ -22,13 +22,15 @@
 // residual_tolerance (src/navier_stokes.c:94-99) of its right-hand side.
 //
 // The history shifts (time_shift, src/time.c:30-42) rotate buffers instead
-// of copying them.  Wall values come from the caller, evaluated at t + dt
+// of copying them; the velocity and pressure keep their current level in one
+// buffer (the solves' CUDA graphs are captured per solution vector).  Wall values come from the caller, evaluated at t + dt
 // at every node: the reference evaluates its boundary functions on the host
 // (set_dirichlet_boundaries, src/poisson.c:101-143), and so does a caller.
 #include <cuda_runtime.h>
 
 #include <cmath>
 #include <cstring>
+#include <utility>
 #include <vector>
 
 #include "ssg_internal.h"
@@ -91,20 +93,24 @@ __global__ void k_pressure_gradient_estimate(DpdArgs A) {
   }
 }
 
-// x2 <- a1 x0 + a2 x1 + a3 x2 (three axpys onto zero, single_stiffly_stable,
-// src/time.c:51-75), then the wall values where given (set_dirichlet_
-// boundaries); x2 is read before it is written, point by point
-__global__ void k_extrapolate(size_t npts, int ncomp, const double* x0, const double* x1,
-                              double* x2, double a1, double a2, double a3, const double* wallv,
-                              const int* bc, int n, int nt) {
+// cur <- a1 cur + a2 old + a3 oldold (three axpys onto zero,
+// single_stiffly_stable, src/time.c:51-75), then the wall values where
+// given (set_dirichlet_boundaries), and oldold <- the previous cur: with the
+// old and oldold slots swapped afterwards this is the time shift, while the
+// current level stays in one buffer (the solves' graphs are keyed on it)
+__global__ void k_extrapolate(size_t npts, int ncomp, double* cur, const double* old,
+                              double* oldold, double a1, double a2, double a3,
+                              const double* wallv, const int* bc, int n, int nt) {
   SSG_FLOW_LOOP(g, npts) {
     const bool wall = wallv && on_wall(bc[g / nt], n, (int)(g % nt));
     for (int c = 0; c < ncomp; ++c) {
       const size_t x = c * npts + g;
-      double v = fma(a1, x0[x], 0.0);
-      v = fma(a2, x1[x], v);
-      v = fma(a3, x2[x], v);
-      x2[x] = wall ? wallv[x] : v;
+      const double u0 = cur[x];
+      double v = fma(a1, u0, 0.0);
+      v = fma(a2, old[x], v);
+      v = fma(a3, oldold[x], v);
+      oldold[x] = u0;
+      cur[x] = wall ? wallv[x] : v;
     }
   }
 }
@@ -403,7 +409,7 @@ ssg_status ssg_navier_stokes_step(ssg_context* c, const double* f, const double*
   dev::k_extrapolate<<<nb, 256, 0, s>>>(np, 1, c->fp[0], c->fp[1], c->fp[2], 3.0, -3.0, 1.0,
                                         nullptr, c->flow_bc, L.n, (int)L.nt);
   SSG_CUDA(c, cudaGetLastError());
-  rotate(c->fp);
+  std::swap(c->fp[1], c->fp[2]);
   ssg_status worst = SSG_OK;
   ssg_status st = ssg_solve_poisson_cg(c, c->fb, c->fp[0], eps_p, kMaxIter,
                                        info ? &info[0] : nullptr);
@@ -426,7 +432,7 @@ ssg_status ssg_navier_stokes_step(ssg_context* c, const double* f, const double*
   dev::k_extrapolate<<<nb, 256, 0, s>>>(np, 3, c->fu[0], c->fu[1], c->fu[2], 3.0, -3.0, 1.0,
                                         wall_u, c->flow_bc, L.n, (int)L.nt);
   SSG_CUDA(c, cudaGetLastError());
-  rotate(c->fu);
+  std::swap(c->fu[1], c->fu[2]);
   for (int d = 0; d < 3; ++d) {
     st = ssg_solve_helmholtz_cg(c, SSG_X_VELOCITY + d, c->fb + d * np, c->fu[0] + d * np,
                                 eps_u[d], kMaxIter, info ? &info[1 + d] : nullptr);

@@ -61,9 +61,14 @@ struct Workspace {
   const double* fcg_u = nullptr;   // the solution vector the graphs update
   bool fcg_failed = false;
   int fcg_warm = 0;          // solves run directly with this configuration
-  // the Jacobi CG loop (iterations after the first) as one WHILE graph
-  cudaGraphExec_t cgloop = nullptr;
-  unsigned long long cgloop_kernels = 0;
+  // the Jacobi CG loop (iterations after the first) as one WHILE graph per
+  // operand set, a few kept (the three velocity components of a time step
+  // each have their own), the least recently used replaced
+  static constexpr int kLoops = 4;
+  cudaGraphExec_t cgloop[kLoops] = {};
+  unsigned long long cgloop_kernels[kLoops] = {};
+  unsigned long long cgloop_used[kLoops] = {};
+  unsigned long long cgloop_clock = 0;
   struct LoopKey {
     const void* f = nullptr;
     const void* x = nullptr;
@@ -76,7 +81,7 @@ struct Workspace {
              max_iter == o.max_iter && hist_cap == o.hist_cap && var == o.var &&
              level == o.level && frame == o.frame && fp32 == o.fp32;
     }
-  } cgloop_key;
+  } cgloop_key[kLoops];
   bool cgloop_failed = false;
 };
 
@@ -90,10 +95,13 @@ static void drop_iteration_graphs(Workspace* w) {
   w->fcg_warm = 0;
   w->fcg_eps = -1.0;
   w->fcg_u = nullptr;
-  if (w->cgloop) cudaGraphExecDestroy(w->cgloop);
-  w->cgloop = nullptr;
+  for (int i = 0; i < Workspace::kLoops; ++i) {
+    if (w->cgloop[i]) cudaGraphExecDestroy(w->cgloop[i]);
+    w->cgloop[i] = nullptr;
+    w->cgloop_key[i] = Workspace::LoopKey();
+    w->cgloop_used[i] = 0;
+  }
   w->cgloop_failed = false;
-  w->cgloop_key = Workspace::LoopKey();
 }
 
 void free_workspace(Workspace* w) {
@@ -355,9 +363,18 @@ ssg_status cg_solve(ssg_context* c, int level, int var, bool fp32, void* f, void
   const bool loop_graph = sync_each && c->graphs && !wsp->cgloop_failed && max_iter > 1;
   for (int it = 0; it < max_iter; ++it) {
     if (loop_graph && it == 1) {
-      if (!(wsp->cgloop && wsp->cgloop_key == key)) {
-        if (wsp->cgloop) cudaGraphExecDestroy(wsp->cgloop);
-        wsp->cgloop = nullptr;
+      // the cached graph of these operands, else the slot to capture into
+      // (an empty one, or the least recently used)
+      int slot = -1;
+      for (int i = 0; i < Workspace::kLoops && slot < 0; ++i)
+        if (wsp->cgloop[i] && wsp->cgloop_key[i] == key) slot = i;
+      if (slot < 0) {
+        slot = 0;
+        for (int i = 1; i < Workspace::kLoops; ++i)
+          if (wsp->cgloop_used[i] < wsp->cgloop_used[slot]) slot = i;
+        if (wsp->cgloop[slot]) cudaGraphExecDestroy(wsp->cgloop[slot]);
+        wsp->cgloop[slot] = nullptr;
+        wsp->cgloop_used[slot] = 0;
         pu.first = 0;
         dop.code = OP_CG_ALPHA;
         const bool ok = build_conditional_graph(
@@ -379,21 +396,22 @@ ssg_status cg_solve(ssg_context* c, int level, int var, bool fp32, void* f, void
               }
               return SSG_OK;
             },
-            &wsp->cgloop, &wsp->cgloop_kernels);
+            &wsp->cgloop[slot], &wsp->cgloop_kernels[slot]);
         if (ok) {
-          wsp->cgloop_key = key;
+          wsp->cgloop_key[slot] = key;
         } else {
           wsp->cgloop_failed = true;
         }
       }
-      if (wsp->cgloop) {
-        SSG_CUDA(c, cudaGraphLaunch(wsp->cgloop, s));
+      if (wsp->cgloop[slot]) {
+        wsp->cgloop_used[slot] = ++wsp->cgloop_clock;
+        SSG_CUDA(c, cudaGraphLaunch(wsp->cgloop[slot], s));
         double iters;
         SSG_TRY(read_flag(c, fr + F_ITER, &iters));
         SSG_TRY(check_interrupt(c));
         // guard + one body (and its guard) per iteration that ran
         const unsigned long long k = 1 + (unsigned long long)std::max(0.0, iters - 1.0) *
-                                             (wsp->cgloop_kernels + 1);
+                                             (wsp->cgloop_kernels[slot] + 1);
         g_launches += k;
         t_launches += k;
         break;
