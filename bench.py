@@ -849,7 +849,7 @@ def run_ours(args):
 
     if args.sections == "step":
         res = run_timestep(args, ctx, mesh, n, local, steps=max(1, args.steps),
-                           warmup=max(1, args.warmup))
+                           warmup=max(1, args.warmup), c1=not args.no_time)
         if rank == 0 and not args.no_time:
             print(json.dumps({"metric": METRIC, "sections": "step", "timestep": res}))
         ctx.close()

@@ -273,6 +273,51 @@ __global__ void __launch_bounds__(256, (MODE == DSS_CGUPD || MODE == DSS_DOT2) ?
   }
 }
 
+// DSS of three fields `stride` apart that share one gather map (the
+// components of a vector field): out_c = DSS(in_c), with SCALE times y (the
+// inverse mass); each node's sources are decoded once for the three, and
+// each sum is the reference's order as in k_dss
+template <int N, bool SCALE>
+__global__ void __launch_bounds__(256) k_dss3(int nel, const double* __restrict__ in,
+                                              double* __restrict__ out, size_t stride,
+                                              const int* __restrict__ map,
+                                              const double* __restrict__ y) {
+  constexpr int NT = N * N * N;
+  constexpr int I = N > 2 ? N - 2 : 0, ECI = 12 * I;
+  const size_t ntask = (size_t)nel * NT;
+  const int4* __restrict__ ec =
+      reinterpret_cast<const int4*>(map + dss_map_records_offset(ntask));
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < ntask;
+       q += (size_t)gridDim.x * blockDim.x) {
+    const int e = (int)(q / NT);
+    const int gw = __ldg(map + q);
+    int4 a = make_int4(-1, -1, -1, -1), b = make_int4(-1, -1, -1, -1);
+    if (gw <= -2) {
+      const int code = -gw - 2;
+      const int4* rec = ec + (size_t)e * (ECI + 16) + (code >> 1);
+      a = __ldg(rec);
+      if (code & 1) b = __ldg(rec + 1);
+    }
+    const int src[7] = {gw >= 0 ? gw : a.x, a.y, a.z, a.w, b.x, b.y, b.z};
+    double own[3], v[3][7];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      own[c] = in[c * stride + q];
+#pragma unroll
+      for (int m = 0; m < 7; ++m) v[c][m] = src[m] >= 0 ? in[c * stride + src[m]] : 0.0;
+    }
+    const double w = SCALE ? y[q] : 1.0;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      double acc = own[c];
+#pragma unroll
+      for (int m = 0; m < 7; ++m)
+        if (src[m] >= 0) acc += v[c][m];
+      out[c * stride + q] = SCALE ? acc * w : acc;
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // tensor-product transfer between orders, stages in x, y, z order
 // (interpolate_to_grid / integrate_to_grid, src/interpolation.c:136-176):
@@ -774,6 +819,31 @@ cudaError_t run_dss(cudaStream_t s, int mode, bool fp32, int n, int nel, const v
                             mask, (const float*)y, (const float*)y2, part, stop, o, g);
   return run_dss_t<double>(s, mode, n, nel, (const double*)in, (double*)out, pairs, ec_tab,
                            mask, (const double*)y, (const double*)y2, part, stop, o, g);
+}
+
+template <int N>
+static cudaError_t run_dss3_n(cudaStream_t s, bool scale, int nel, const double* in,
+                              double* out, size_t stride, const int* ec_tab, const double* y) {
+  const int grd = dss_grid(N, nel);
+  SSG_COUNT();
+  if (scale)
+    k_dss3<N, true><<<grd, 256, 0, s>>>(nel, in, out, stride, ec_tab, y);
+  else
+    k_dss3<N, false><<<grd, 256, 0, s>>>(nel, in, out, stride, ec_tab, y);
+  return cudaGetLastError();
+}
+
+cudaError_t run_dss3(cudaStream_t s, bool scale, int n, int nel, const double* in, double* out,
+                     size_t stride, const int* ec_tab, const double* y) {
+  if (!ec_tab || (scale && !y)) return cudaErrorInvalidValue;
+  switch (n) {
+#define SSG_DSS3N(NV) \
+  case NV: return run_dss3_n<NV>(s, scale, nel, in, out, stride, ec_tab, y);
+    SSG_DSS3N(2) SSG_DSS3N(3) SSG_DSS3N(4) SSG_DSS3N(5) SSG_DSS3N(6) SSG_DSS3N(7)
+    SSG_DSS3N(8) SSG_DSS3N(9) SSG_DSS3N(10) SSG_DSS3N(11) SSG_DSS3N(12)
+#undef SSG_DSS3N
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 template <typename T, bool ADD>

@@ -153,6 +153,10 @@ cudaError_t run_dss(cudaStream_t s, int mode, bool fp32, int n, int nel, const v
                     void* out, const int* pairs, const int* ec_tab, const double* mask,
                     const void* y, const void* y2, double* part, const double* stop = nullptr,
                     const ScalarOp* op = nullptr, const DssCg* cg = nullptr);
+// DSS of three FP64 fields `stride` apart (a vector field's components) in
+// one launch, out-of-place; scale: then times y pointwise (the inverse mass)
+cudaError_t run_dss3(cudaStream_t s, bool scale, int n, int nel, const double* in, double* out,
+                     size_t stride, const int* ec_tab, const double* y);
 cudaError_t run_tensor3(cudaStream_t s, bool fp32, bool add, int nel, int ni, int no,
                         const double* A, const void* in, void* out);
 cudaError_t run_cg_update(cudaStream_t s, bool fp32, size_t npts, const double* alpha,

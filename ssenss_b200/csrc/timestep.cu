@@ -6,9 +6,9 @@
 // four stages, and each stage evaluates the dealiased convection of a stage
 // field advected by the velocity interpolated in time from the last three
 // steps -- 24 of the 25 convection evaluations of a step.  Here a stage is
-// three kinds of launch: one pass that forms the stage field and the
-// interpolated velocity, the convection over all elements, and per component
-// one DSS whose epilogue multiplies by the inverse mass; a sub-step ends with
+// three launches: one pass that forms the stage field and the interpolated
+// velocity, the convection over all elements, and one DSS of the three
+// components whose epilogue multiplies by the inverse mass; a sub-step ends with
 // one pass of the four stage updates.  The velocity history and the stage
 // fields stay on the device.
 //
@@ -165,11 +165,8 @@ ssg_status convection_rk4(ssg_context* c, double* du, double t0, double t, doubl
                                  c->host.conv.D.data(), c->host.jconv.data(), c->conv_D,
                                  c->conv_J, c->conv_scratch));
       // trivec_inverse_mass_matrix: per component the DSS, then the product
-      // with 1 / DSS(mass), in one pass
-      for (int comp = 0; comp < 3; ++comp)
-        SSG_CUDA(c, run_dss(s, DSS_SCALE, false, L.n, c->nel, f[i] + comp * npc,
-                            y + comp * npc, c->d_pairs, L.dss_ec, nullptr, c->inv_mass, nullptr,
-                            nullptr));
+      // with 1 / DSS(mass), the three components in one pass
+      SSG_CUDA(c, run_dss3(s, true, L.n, c->nel, f[i], y, npc, L.dss_ec, c->inv_mass));
       std::swap(f[i], y);
     }
     count_launch();
