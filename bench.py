@@ -699,52 +699,94 @@ def run_convection(args, ctx, mesh, n, device, calls=25):
             "substeps_ms_per_step": ms_sub / 5}
 
 
-def run_timestep(args, ctx, mesh, n, device, steps=5, warmup=2, c1=True):
-    """The whole time step on the device (ssg_navier_stokes_step, the
-    reference's integrate_navier_stokes, src/navier_stokes.c:224-235) on the
-    TGV box from its analytic state: the velocity and pressure at three
-    levels, their convection and double-curl histories computed by the
-    library.  ms_per_step: device time of `steps` steps after `warmup`,
-    with each solve's iterations of the last step."""
+def tgv_initial_state(ctx, device):
+    """The reference's Taylor-Green initial state (src/poisson.c:245-273 with
+    the TGV functions, pressure at three levels) built by the library on its
+    own grid: the velocity at three levels, the convection and double-curl
+    histories of the two older levels (zero at the oldest), the TGV
+    pressure."""
     import numpy as np
     import torch
     dev = torch.device("cuda", device)
     X, Y, Z = (ctx.level_data(0, 12 + a) for a in range(3))
+    u = torch.from_numpy(np.stack([np.sin(X) * np.cos(Y) * np.cos(Z),
+                                   -np.cos(X) * np.sin(Y) * np.cos(Z), 0 * X])).to(dev)
+    conv = ctx.convection_operator(u, u, torch.empty_like(u))
+    rot = ctx.stokes_operator(0, u, None, torch.empty_like(u))
+    p = torch.from_numpy((np.cos(2 * X) + np.cos(2 * Y)) * (np.cos(2 * Z) + 2.0) / 16.0).to(dev)
+    zero = torch.zeros_like(u)
+    return [u, u.clone(), u.clone()], [conv, conv.clone(), zero], [rot, rot.clone(), zero.clone()], \
+        [p, p.clone(), p.clone()]
+
+
+def run_timestep(args, ctx, mesh, n, device, steps=50, warmup=3, c1=True):
+    """C2's time integration: `steps` steps of the reference's
+    integrate_navier_stokes (src/navier_stokes.c:224-235) on the device
+    (ssg_navier_stokes_step) from the reference's Taylor-Green initial state,
+    FP64 and then mixed precision, device time per step; the velocity and
+    pressure after the last step against the reference's own run of the
+    same steps (tests/golden/c2_tgv16_n8_steps.npz, written by the reference
+    compiled in place: a seeded sample of 8192 points and the whole-field
+    rms), as L2 errors over the sample relative to its norm and as max
+    errors relative to the field's largest magnitude.  `warmup` untimed steps
+    from the same state first (graph captures of the solves), then the state
+    is set again."""
+    import numpy as np
+    import torch
+    dev = torch.device("cuda", device)
     dt = 1e-3
-    t = 0.0
-    u, conv, rot, p = [], [], [], []
-    for lev in range(3):
-        g = np.exp(-2.0 * (t - lev * dt) / 1600.0)
-        ul = torch.from_numpy(np.stack([np.sin(X) * np.cos(Y) * np.cos(Z) * g,
-                                        -np.cos(X) * np.sin(Y) * np.cos(Z) * g,
-                                        0 * X])).to(dev)
-        u.append(ul)
-        conv.append(ctx.convection_operator(ul, ul, torch.empty_like(ul)))
-        rot.append(ctx.stokes_operator(0, ul, None, torch.empty_like(ul)))
-        p.append(torch.from_numpy((np.cos(2 * X) + np.cos(2 * Y)) * (np.cos(2 * Z) + 2.0)
-                                  / 16.0 * g * g).to(dev))
-    ctx.flow_set(u, conv, rot, p, None, t)
+    rec = None
+    path = os.path.join(ROOT, "tests", "golden", "c2_tgv16_n8_steps.npz")
+    if steps == 50 and os.path.exists(path):
+        rec = np.load(path)
     lib_stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
-    for _ in range(warmup):
-        ctx.navier_stokes_step(history=False)
-    torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(lib_stream)
-    last = None
-    for _ in range(steps):
-        last = ctx.navier_stokes_step(history=False)
-    e1.record(lib_stream)
-    e1.synchronize()
-    ms = e0.elapsed_time(e1) / steps
+    state = tgv_initial_state(ctx, device)
     npts = mesh.nel * n ** 3
-    out = {"workload": f"TGV {args.ne}^3 N={n-1}: integrate_navier_stokes on the device, "
-                       f"dt {dt}, Re 1600, from the analytic state",
-           "ms_per_step": ms, "steps_per_s": 1e3 / ms, "steps_timed": steps,
-           "points": npts,
-           "iterations_last_step": {"pressure": last[0]["iterations"],
-                                    "u": last[1]["iterations"], "v": last[2]["iterations"],
-                                    "w": last[3]["iterations"]}}
+    out = {"workload": f"TGV {args.ne}^3 N={n-1}: {steps} steps of integrate_navier_stokes on "
+                       f"the device, dt {dt}, Re 1600, from the reference's initial state",
+           "points": npts, "steps_timed": steps}
+    for prec in ("fp64", "mixed"):
+        ctx.set_precision(prec)
+        if warmup > 0:
+            ctx.flow_set(*state, None, 0.0)
+            for _ in range(warmup):
+                ctx.navier_stokes_step(history=False)
+        ctx.flow_set(*state, None, 0.0)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(lib_stream)
+        iters = []
+        for _ in range(steps):
+            last = ctx.navier_stokes_step(history=False)
+            iters.append([g["iterations"] for g in last])
+        e1.record(lib_stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        r = {"ms_per_step": ms, "steps_per_s": 1e3 / ms,
+             "solve_iterations_total": [int(x) for x in np.sum(iters, axis=0)],
+             "iterations_last_step": {"pressure": iters[-1][0], "u": iters[-1][1],
+                                      "v": iters[-1][2], "w": iters[-1][3]}}
+        if rec is not None:
+            f = ctx.flow_get()
+            idx = rec["sample_index"]
+            ug = np.stack([f["u"][0][c].reshape(-1)[idx] for c in range(3)])
+            pg = f["p"][0].reshape(-1)[idx]
+            ur, pr = rec["snap_u"][-1], rec["snap_p"][-1]
+            umax = max(rec["snap_maxabs"][-1, 0], rec["snap_maxabs"][-1, 1])
+            r["vs_reference"] = {
+                "velocity_l2_rel": float(np.linalg.norm(ug - ur) / np.linalg.norm(ur)),
+                "pressure_l2_rel": float(np.linalg.norm(pg - pr) / np.linalg.norm(pr)),
+                "velocity_max_rel": float(np.max(np.abs(ug - ur)) / umax),
+                "pressure_max_rel": float(np.max(np.abs(pg - pr)) / rec["snap_maxabs"][-1, 3]),
+                "reference_iterations_total": [int(x) for x in rec["iterations"].sum(axis=0)],
+                "sample": f"{idx.size} seeded points of {npts}, after step {steps}"}
+        out[prec] = r
+    ctx.set_precision("fp64")
+    out["ms_per_step"] = out["fp64"]["ms_per_step"]
+    out["mixed_speedup_steps_vs_fp64"] = out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"]
+    if rec is not None:
+        out["reference_cpu_s_per_step"] = float(rec["cpu_s_per_step"])
     if c1:
         # the same at C1 (TGV 4^3, n = 8), the size the reference's own step
         # is timed at in the CPU baseline
@@ -754,8 +796,11 @@ def run_timestep(args, ctx, mesh, n, device, steps=5, warmup=2, c1=True):
         try:
             small.set_parameters(dt, 1.0 / 1600.0, 1.0)
             small.setup_mesh(tgv_box(4), n)
-            sub = run_timestep(args, small, tgv_box(4), n, device, steps=10, warmup=2, c1=False)
-            out["c1"] = {"ms_per_step": sub["ms_per_step"], "points": sub["points"]}
+            sub = run_timestep(args, small, tgv_box(4), n, device, steps=20, warmup=warmup,
+                               c1=False)
+            out["c1"] = {"ms_per_step": sub["fp64"]["ms_per_step"],
+                         "mixed_ms_per_step": sub["mixed"]["ms_per_step"],
+                         "points": sub["points"], "steps": 20}
         finally:
             small.close()
     return out
@@ -848,7 +893,8 @@ def run_ours(args):
         return 0
 
     if args.sections == "step":
-        res = run_timestep(args, ctx, mesh, n, local, steps=max(1, args.steps),
+        res = run_timestep(args, ctx, mesh, n, local,
+                           steps=max(1, args.steps) if args.no_time else 50,
                            warmup=max(1, args.warmup), c1=not args.no_time)
         if rank == 0 and not args.no_time:
             print(json.dumps({"metric": METRIC, "sections": "step", "timestep": res}))

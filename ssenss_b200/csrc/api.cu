@@ -90,6 +90,7 @@ static void free_mesh(ssg_context* c) {
   c->flow_ready = false;
   for (auto& l : c->lev) free_level(l);
   dfree(c->d_pairs); c->d_pairs = nullptr;
+  dfree(c->d_nbreg); c->d_nbreg = nullptr;
   dfree(c->inv_mass); c->inv_mass = nullptr;
   dfree(c->conv_w); dfree(c->conv_D); dfree(c->conv_J);
   dfree(c->conv_scratch);
@@ -197,6 +198,26 @@ static ssg_status upload_all(ssg_context* c) {
   if ((size_t)nel * H.lev[0].nt >= (size_t)INT32_MAX)
     return fail(c, SSG_ERR_ARG, "mesh exceeds 2^31 local points (32-bit node indices)");
   SSG_TRY(dupload(c, &c->d_pairs, H.pairs.data(), H.pairs.size()));
+  {
+    // the line-run DSS applies where every face, edge and corner is
+    // paired with the opposite one of its neighbour (faces w/e, s/n, b/t;
+    // edges and corners with every side flipped)
+    std::vector<int> nb((size_t)nel * 26, -1);
+    bool regular = true;
+    for (size_t e = 0; e < (size_t)nel && regular; ++e)
+      for (int sl = 0; sl < 26; ++sl) {
+        const int other = H.pairs[2 * (26 * e + sl)], found = H.pairs[2 * (26 * e + sl) + 1];
+        if (other < 0) continue;
+        const int j = sl < 6 ? sl : (sl < 18 ? sl - 6 : sl - 18);
+        const int opp = sl < 6 ? (j ^ 1) : (sl < 18 ? (j ^ 3) : (j ^ 7));
+        if (found != opp) {
+          regular = false;
+          break;
+        }
+        nb[26 * e + sl] = other;
+      }
+    if (regular) SSG_TRY(dupload(c, &c->d_nbreg, nb.data(), nb.size()));
+  }
   for (int l = 0; l < H.nlev; ++l) {
     const ssg::HostLevel& h = H.lev[l];
     ssg::DevLevel& d = c->lev[l];
@@ -330,7 +351,7 @@ ssg_status helmholtz_diag_update(ssg_context* c) {
   SSG_TRY(ensure_workspace(c));
   double* tmp = workspace_scratch(c);
   SSG_CUDA(c, run_helm_diag(c->stream, d.npts, d.nt, d.kdiag, d.rho, d.det, lam, tmp));
-  SSG_CUDA(c, run_dss(c->stream, DSS_PLAIN, false, d.n, c->nel, tmp, d.dinv_h, c->d_pairs,
+  SSG_CUDA(c, run_dss(c->stream, DSS_PLAIN, false, d.n, c->nel, tmp, d.dinv_h, c->d_nbreg,
                       d.dss_ec, nullptr, nullptr, nullptr, nullptr));
   SSG_CUDA(c, run_recip(c->stream, d.npts, d.dinv_h));
   d.lambda_h = lam;
@@ -690,7 +711,7 @@ ssg_status ssg_direct_stiffness_summation(ssg_context* c, double* u) {
                               c->stream));
   double* dout = (double*)du;
   if (!is_device_ptr(u)) dout = c->d_stage[0];
-  SSG_CUDA(c, run_dss(c->stream, DSS_PLAIN, false, c->n, c->nel, tmp, dout, c->d_pairs,
+  SSG_CUDA(c, run_dss(c->stream, DSS_PLAIN, false, c->n, c->nel, tmp, dout, c->d_nbreg,
                       c->lev[0].dss_ec,
                       nullptr, nullptr, nullptr, nullptr));
   return stage_back(c, u, dout, np);

@@ -395,9 +395,9 @@ ssg_status ssg_navier_stokes_step(ssg_context* c, const double* f, const double*
     dev::k_pressure_gradient_estimate<<<nb, 256, 0, s>>>(A);
     SSG_CUDA(c, cudaGetLastError());
   }
-  SSG_CUDA(c, run_dss3(s, true, L.n, c->nel, c->fa, c->fb, np, L.dss_ec, c->inv_mass));
+  SSG_CUDA(c, run_dss3(s, true, L.n, c->nel, c->fa, c->fb, np, c->d_nbreg, L.dss_ec, c->inv_mass));
   SSG_TRY(stokes(c, SSG_STOKES_PRESSURE_RHS, c->fut, c->fb, c->fa, -c->dens / dt, 0.0));
-  SSG_CUDA(c, run_dss(s, DSS_PLAIN, false, L.n, c->nel, c->fa, c->fb, c->d_pairs, L.dss_ec,
+  SSG_CUDA(c, run_dss(s, DSS_PLAIN, false, L.n, c->nel, c->fa, c->fb, c->d_nbreg, L.dss_ec,
                       nullptr, nullptr, nullptr, nullptr));
   double eps_p = 0.0;
   SSG_TRY(tolerance(c, c->fb, &eps_p));
@@ -419,7 +419,7 @@ ssg_status ssg_navier_stokes_step(ssg_context* c, const double* f, const double*
   // compute_velocity_rhs
   SSG_TRY(stokes(c, SSG_STOKES_VELOCITY_RHS, c->fut, c->fp[0], c->fa, 1.0 / (dt * c->visc),
                  -1.0 / (c->visc * c->dens)));
-  SSG_CUDA(c, run_dss3(s, false, L.n, c->nel, c->fa, c->fb, np, L.dss_ec, nullptr));
+  SSG_CUDA(c, run_dss3(s, false, L.n, c->nel, c->fa, c->fb, np, c->d_nbreg, L.dss_ec, nullptr));
   double eps_u[3];
   for (int d = 0; d < 3; ++d) SSG_TRY(tolerance(c, c->fb + d * np, &eps_u[d]));
 

@@ -21,8 +21,10 @@
 // (src/init.c:68-130), accumulating in FP64: for FP64 data the result is
 // bitwise equal to the reference's.
 #include <cuda/atomic>
+#include <atomic>
 #include <cuda_runtime.h>
 
+#include <initializer_list>
 #include <type_traits>
 
 #include <cstdint>
@@ -314,6 +316,302 @@ __global__ void __launch_bounds__(256) k_dss3(int nel, const double* __restrict_
       for (int m = 0; m < 7; ++m)
         if (src[m] >= 0) acc += v[c][m];
       out[c * stride + q] = SCALE ? acc * w : acc;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// DSS over runs of P consecutive nodes of an element x-line, for meshes
+// whose every face, edge and corner is paired with the opposite one of its
+// neighbour (checked on the host when the mesh is set up: every mesh with
+// three or more elements along each periodic direction, walls or not, and
+// the opposite pairing of small boxes).  There a neighbour's copy of node
+// (i, j, k) is the same node with the shared coordinates flipped
+// (0 <-> N-1), so the sources of every node follow from the element's 26
+// neighbour ids (nb26, -1 for none) without a per-node map:
+//   node i of line (j, k) adds, in the reference's order
+//   (src/global.c:241-257: faces w e s n b t, edges sw..tn, corners 0..7,
+//   pre-sum values):
+//     x-face  i = 0: w's (N-1, j, k)      i = N-1: e's (0, j, k)
+//     y-face  (j = 0: s, j = N-1: n)      the neighbour's node, j flipped
+//     z-face  (k = 0: b, k = N-1: t)      the neighbour's node, k flipped
+//     xy-edge i and j extreme             sw / se / nw / ne, i and j flipped
+//     xz-edge i and k extreme             bw / be / tw / te, i and k flipped
+//     yz-edge j and k extreme             bs / bn / ts / tn, j and k flipped
+//     corner  i, j and k extreme          the opposite corner
+// Same sums in the same order as k_dss, so the gathered values are bitwise
+// the same.  Each thread takes a run of P consecutive nodes of a line (half
+// or whole lines, DssRun), loaded and stored as 16- or 8-byte vectors where
+// the run allows; consecutive threads take consecutive runs, so a warp's
+// loads of its own nodes, of a face or edge neighbour's nodes and its
+// stores are contiguous, and only the line ends gather single values.  The
+// grid is one full wave of resident blocks walking the runs grid-stride.
+// ---------------------------------------------------------------------------
+template <int N, typename T>
+struct DssRun {
+  // nodes per thread, measured on the B200 at the periodic 16^3 box: FP64
+  // half lines from N = 6 (n = 8: 14.4 us per DSS + dot against 22.6 us
+  // for pairs and 16.4 us for whole lines; n = 12: 39.0 against 41.0 for
+  // whole lines), whole lines below and at odd orders (no vector split);
+  // FP32 whole lines (the mixed V-cycle's gather + update at n = 8: 19.5
+  // against 20.4 ms per solve with half lines)
+  static constexpr int P = sizeof(T) == 8 ? ((N % 2 == 0 && N >= 6) ? N / 2 : N) : N;
+  static constexpr int R = N / P;   // runs per line
+};
+
+template <int P, typename T>
+__device__ __forceinline__ void ld_run(const T* __restrict__ p, double (&v)[P]) {
+  if constexpr (sizeof(T) == 8 && P % 2 == 0) {
+#pragma unroll
+    for (int q = 0; q < P; q += 2) {
+      const double2 t = *reinterpret_cast<const double2*>(p + q);
+      v[q] = t.x;
+      v[q + 1] = t.y;
+    }
+  } else if constexpr (sizeof(T) == 4 && P % 4 == 0) {
+#pragma unroll
+    for (int q = 0; q < P; q += 4) {
+      const float4 t = *reinterpret_cast<const float4*>(p + q);
+      v[q] = t.x;
+      v[q + 1] = t.y;
+      v[q + 2] = t.z;
+      v[q + 3] = t.w;
+    }
+  } else if constexpr (sizeof(T) == 4 && P % 2 == 0) {
+#pragma unroll
+    for (int q = 0; q < P; q += 2) {
+      const float2 t = *reinterpret_cast<const float2*>(p + q);
+      v[q] = t.x;
+      v[q + 1] = t.y;
+    }
+  } else {
+#pragma unroll
+    for (int q = 0; q < P; ++q) v[q] = (double)p[q];
+  }
+}
+
+template <int P, typename T>
+__device__ __forceinline__ void st_run(T* __restrict__ p, const T (&v)[P]) {
+  if constexpr (sizeof(T) == 8 && P % 2 == 0) {
+#pragma unroll
+    for (int q = 0; q < P; q += 2)
+      *reinterpret_cast<double2*>(p + q) = make_double2(v[q], v[q + 1]);
+  } else if constexpr (sizeof(T) == 4 && P % 4 == 0) {
+#pragma unroll
+    for (int q = 0; q < P; q += 4)
+      *reinterpret_cast<float4*>(p + q) = make_float4(v[q], v[q + 1], v[q + 2], v[q + 3]);
+  } else if constexpr (sizeof(T) == 4 && P % 2 == 0) {
+#pragma unroll
+    for (int q = 0; q < P; q += 2)
+      *reinterpret_cast<float2*>(p + q) = make_float2(v[q], v[q + 1]);
+  } else {
+#pragma unroll
+    for (int q = 0; q < P; ++q) p[q] = v[q];
+  }
+}
+
+// The gathered run starting at global node g = run * P: own values plus
+// every contribution in the reference's order, and each node's contribution
+// count.  MASK: every value (own and neighbours') times the Dirichlet mask at
+// its own position.
+template <int N, int P, typename T, bool MASK>
+__device__ __forceinline__ void gather_run(const T* __restrict__ in,
+                                           const double* __restrict__ mask,
+                                           const int* __restrict__ nb26, size_t run,
+                                           double (&acc)[P], int (&cnt)[P]) {
+  constexpr int R = N / P;
+  constexpr int M = N - 1, NN = N * N;
+  constexpr size_t NT = (size_t)NN * N;
+  const size_t line = run / R;
+  const int i0 = (int)(run - line * R) * P;
+  const size_t e = line / NN;
+  const int jk = (int)(line - e * NN);
+  const int j = jk % N, k = jk / N;
+  const int lo = jk * N + i0;                // local index of the run's first node
+  const bool lo_end = i0 == 0, hi_end = i0 + P - 1 == M;
+  const bool jhi = j == M, khi = k == M;
+  const bool yf = j == 0 || jhi, zf = k == 0 || khi, yz = yf && zf;
+  const int dy = jhi ? -M * N : M * N;       // flip j
+  const int dz = khi ? -M * NN : M * NN;     // flip k
+  const int* __restrict__ nbe = nb26 + e * 26;
+  // neighbour element ids of the run's slots (an element's 26 ids are read
+  // by all its runs: L1 hits)
+  const int nw = lo_end ? __ldg(nbe + 0) : -1;
+  const int ne = hi_end ? __ldg(nbe + 1) : -1;
+  const int ny = yf ? __ldg(nbe + 2 + jhi) : -1;
+  const int nz = zf ? __ldg(nbe + 4 + khi) : -1;
+  const int nxy0 = (yf && lo_end) ? __ldg(nbe + 6 + 2 * jhi) : -1;
+  const int nxy1 = (yf && hi_end) ? __ldg(nbe + 7 + 2 * jhi) : -1;
+  const int nxz0 = (zf && lo_end) ? __ldg(nbe + 10 + 2 * khi) : -1;
+  const int nxz1 = (zf && hi_end) ? __ldg(nbe + 11 + 2 * khi) : -1;
+  const int nyz = yz ? __ldg(nbe + 14 + jhi + 2 * khi) : -1;
+  const int nc0 = (yz && lo_end) ? __ldg(nbe + 18 + 2 * jhi + 4 * khi) : -1;
+  const int nc1 = (yz && hi_end) ? __ldg(nbe + 19 + 2 * jhi + 4 * khi) : -1;
+  auto val = [&](size_t g) -> double {
+    double v = (double)in[g];
+    if (MASK) v = v * mask[g];
+    return v;
+  };
+  auto runv = [&](size_t g, double (&v)[P]) {
+    ld_run<P, T>(in + g, v);
+    if (MASK) {
+      double m[P];
+      ld_run<P, double>(mask + g, m);
+#pragma unroll
+      for (int q = 0; q < P; ++q) v[q] = v[q] * m[q];
+    }
+  };
+  double own[P], vy[P], vz[P], vyz[P];
+#pragma unroll
+  for (int q = 0; q < P; ++q) vy[q] = vz[q] = vyz[q] = 0.0;
+  runv(e * NT + lo, own);
+  if (ny >= 0) runv((size_t)ny * NT + (lo + dy), vy);
+  if (nz >= 0) runv((size_t)nz * NT + (lo + dz), vz);
+  if (nyz >= 0) runv((size_t)nyz * NT + (lo + dy + dz), vyz);
+  // line ends: node i = 0 reads its sources at i = N-1 (lo + M), node
+  // i = N-1 at i = 0 (lo - M)
+  const double vw = nw >= 0 ? val((size_t)nw * NT + (lo + M)) : 0.0;
+  const double ve = ne >= 0 ? val((size_t)ne * NT + (lo + P - 1 - M)) : 0.0;
+  const double vxy0 = nxy0 >= 0 ? val((size_t)nxy0 * NT + (lo + dy + M)) : 0.0;
+  const double vxy1 = nxy1 >= 0 ? val((size_t)nxy1 * NT + (lo + P - 1 + dy - M)) : 0.0;
+  const double vxz0 = nxz0 >= 0 ? val((size_t)nxz0 * NT + (lo + dz + M)) : 0.0;
+  const double vxz1 = nxz1 >= 0 ? val((size_t)nxz1 * NT + (lo + P - 1 + dz - M)) : 0.0;
+  const double vc0 = nc0 >= 0 ? val((size_t)nc0 * NT + (lo + dy + dz + M)) : 0.0;
+  const double vc1 = nc1 >= 0 ? val((size_t)nc1 * NT + (lo + P - 1 + dy + dz - M)) : 0.0;
+#pragma unroll
+  for (int q = 0; q < P; ++q) {
+    // q == 0 with lo_end is node i = 0, q == P-1 with hi_end node i = N-1
+    const bool first = q == 0, last = q == P - 1;
+    double a = own[q];
+    int c = 0;
+    if (first && nw >= 0) { a += vw; ++c; }
+    if (last && ne >= 0) { a += ve; ++c; }
+    if (ny >= 0) { a += vy[q]; ++c; }
+    if (nz >= 0) { a += vz[q]; ++c; }
+    if (first && nxy0 >= 0) { a += vxy0; ++c; }
+    if (last && nxy1 >= 0) { a += vxy1; ++c; }
+    if (first && nxz0 >= 0) { a += vxz0; ++c; }
+    if (last && nxz1 >= 0) { a += vxz1; ++c; }
+    if (nyz >= 0) { a += vyz[q]; ++c; }
+    if (first && nc0 >= 0) { a += vc0; ++c; }
+    if (last && nc1 >= 0) { a += vc1; ++c; }
+    acc[q] = a;
+    cnt[q] = c;
+  }
+}
+
+template <int N, int P, typename T, int MODE, bool MASK>
+__global__ void __launch_bounds__(256) k_dss_runs(int nel, const T* __restrict__ in,
+                                                  T* __restrict__ out,
+                                                  const int* __restrict__ nb26,
+                                                  const double* __restrict__ mask,
+                                                  const T* __restrict__ y,
+                                                  const T* __restrict__ y2,
+                                                  double* __restrict__ part,
+                                                  const double* __restrict__ stop, ScalarOp op,
+                                                  DssCg cg) {
+  if (stop && *stop != 0.0) return;   // uniform over the block
+  __shared__ double sred[2 * 32];
+  __shared__ double sred4[MODE == DSS_CGUPD ? 4 * 32 : 1];
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+  const double alpha = MODE == DSS_CGUPD ? *cg.alpha : 0.0;
+  const size_t nruns = (size_t)nel * N * N * (N / P);
+  for (size_t run = blockIdx.x * (size_t)blockDim.x + threadIdx.x; run < nruns;
+       run += (size_t)gridDim.x * blockDim.x) {
+    double acc[P];
+    int cnt[P];
+    gather_run<N, P, T, MASK>(in, mask, nb26, run, acc, cnt);
+    const size_t g = run * P;
+    if (MODE == DSS_CGUPD) {
+      // ap = acc: x += alpha p; r -= alpha ap; z = dinv r  (src/solver.c:66-71)
+      double ex[P], ep[P], er[P], ed[P];
+      ld_run<P, T>(reinterpret_cast<const T*>(cg.x) + g, ex);
+      ld_run<P, T>(reinterpret_cast<const T*>(cg.p) + g, ep);
+      ld_run<P, T>(reinterpret_cast<const T*>(cg.r) + g, er);
+      ld_run<P, T>(reinterpret_cast<const T*>(cg.dinv) + g, ed);
+      T xo[P], ro[P], zo[P];
+#pragma unroll
+      for (int q = 0; q < P; ++q) {
+        const double w = inv_count(1u + (unsigned)cnt[q]);
+        xo[q] = (T)(ex[q] + alpha * ep[q]);
+        ro[q] = (T)(er[q] + -alpha * acc[q]);
+        zo[q] = (T)((double)ro[q] * ed[q]);
+        const double rw = (double)ro[q] * w;
+        s0 += rw * (double)zo[q];
+        s1 += rw * (double)ro[q];
+        s2 += w * (double)zo[q];
+        s3 += rw;
+      }
+      st_run<P, T>(reinterpret_cast<T*>(cg.x) + g, xo);
+      st_run<P, T>(reinterpret_cast<T*>(cg.r) + g, ro);
+      st_run<P, T>(reinterpret_cast<T*>(cg.z) + g, zo);
+    } else {
+      double ey[P], ey2[P];
+      if (MODE == DSS_RESID || MODE == DSS_DOT || MODE == DSS_DOT2 || MODE == DSS_SCALE)
+        ld_run<P, T>(y + g, ey);
+      if (MODE == DSS_DOT2) ld_run<P, T>(y2 + g, ey2);
+      T o[P];
+#pragma unroll
+      for (int q = 0; q < P; ++q) {
+        const double w = inv_count(1u + (unsigned)cnt[q]);
+        if (MODE == DSS_RESID) {
+          o[q] = (T)(ey[q] + -acc[q]);
+          s0 += (double)o[q] * w;
+        } else if (MODE == DSS_AVG) {
+          o[q] = (T)(acc[q] * w);
+        } else if (MODE == DSS_SCALE) {
+          o[q] = (T)(acc[q] * ey[q]);
+        } else {
+          o[q] = (T)acc[q];
+          if (MODE == DSS_DOT || MODE == DSS_DOT2) {
+            const double yw = ey[q] * w;
+            s0 += yw * (double)o[q];
+            if (MODE == DSS_DOT2) s1 += yw * ey2[q];
+          }
+        }
+      }
+      st_run<P, T>(out + g, o);
+    }
+  }
+  if (MODE == DSS_DOT || MODE == DSS_RESID) {
+    double v[1] = {s0};
+    block_reduce<1>(v, sred);
+    finish<1>(v, part, op, sred);
+  } else if (MODE == DSS_DOT2) {
+    double v[2] = {s0, s1};
+    block_reduce<2>(v, sred);
+    finish<2>(v, part, op, sred);
+  } else if (MODE == DSS_CGUPD) {
+    double v[4] = {s0, s1, s2, s3};
+    block_reduce<4>(v, sred4);
+    finish<4>(v, part, op, sred4);
+  }
+}
+
+// k_dss3 over line runs (the opposite pairing, as k_dss_runs): the three
+// components' gathers of a run in flight together
+template <int N, int P, bool SCALE>
+__global__ void __launch_bounds__(256) k_dss3_runs(int nel, const double* __restrict__ in,
+                                                   double* __restrict__ out, size_t stride,
+                                                   const int* __restrict__ nb26,
+                                                   const double* __restrict__ y) {
+  const size_t nruns = (size_t)nel * N * N * (N / P);
+  for (size_t run = blockIdx.x * (size_t)blockDim.x + threadIdx.x; run < nruns;
+       run += (size_t)gridDim.x * blockDim.x) {
+    const size_t g = run * P;
+    double w[P];
+    if (SCALE) ld_run<P, double>(y + g, w);
+    double acc[3][P];
+    int cnt[3][P];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+      gather_run<N, P, double, false>(in + c * stride, nullptr, nb26, run, acc[c], cnt[c]);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      double o[P];
+#pragma unroll
+      for (int q = 0; q < P; ++q) o[q] = SCALE ? acc[c][q] * w[q] : acc[c][q];
+      st_run<P, double>(out + c * stride + g, o);
     }
   }
 }
@@ -752,35 +1050,62 @@ int dss_grid(int n, int nel) {
   return (int)(g < cap ? (g ? g : 1) : cap);
 }
 
+// one full wave: the kernel's resident blocks per SM (queried once per
+// kernel) on every SM, each thread walking its runs grid-stride
+template <typename K>
+static int full_wave(K kern, std::atomic<int>& occ, size_t runs) {
+  int v = occ.load(std::memory_order_relaxed);
+  if (v <= 0) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, kern, 256, 0) != cudaSuccess || v < 1)
+      v = 1;
+    occ.store(v, std::memory_order_relaxed);
+  }
+  const size_t need = (runs + 255) / 256, cap = (size_t)148 * v;
+  return (int)(need < cap ? (need ? need : 1) : cap);
+}
+
+template <int N, typename T, int MODE, bool MASK>
+static void launch_runs(cudaStream_t s, int nel, const T* in, T* out, const int* nb26,
+                        const double* mask, const T* y, const T* y2, double* part,
+                        const double* stop, const ScalarOp& op, const DssCg& cg) {
+  constexpr int P = DssRun<N, T>::P;
+  static std::atomic<int> occ{0};
+  auto kern = &k_dss_runs<N, P, T, MODE, MASK>;
+  const int grd = full_wave(kern, occ, (size_t)nel * N * N * (N / P));
+  kern<<<grd, 256, 0, s>>>(nel, in, out, nb26, mask, y, y2, part, stop, op, cg);
+}
+
+template <int N, typename T, int MODE>
+static void launch_dss(cudaStream_t s, int nel, const T* in, T* out, const int* nb26,
+                       const int* ec_tab, const double* mask, const T* y, const T* y2,
+                       double* part, const double* stop, const ScalarOp& op, const DssCg& cg) {
+  SSG_COUNT();
+  if (nb26) {
+    if (mask)
+      launch_runs<N, T, MODE, true>(s, nel, in, out, nb26, mask, y, y2, part, stop, op, cg);
+    else
+      launch_runs<N, T, MODE, false>(s, nel, in, out, nb26, nullptr, y, y2, part, stop, op, cg);
+  } else {
+    k_dss<N, T, MODE><<<dss_grid(N, nel), 256, 0, s>>>(nel, in, out, ec_tab, mask, y, y2, part,
+                                                      stop, op, cg);
+  }
+}
+
 template <int N, typename T>
 static cudaError_t run_dss_n(cudaStream_t s, int mode, int nel, const T* in, T* out,
-                             const int* ec_tab, const double* mask, const T* y,
+                             const int* nb26, const int* ec_tab, const double* mask, const T* y,
                              const T* y2, double* part, const double* stop,
                              const ScalarOp& op, const DssCg& cg) {
-  const int grd = dss_grid(N, nel);
   switch (mode) {
-    case DSS_PLAIN:
-      { SSG_COUNT(); k_dss<N, T, DSS_PLAIN><<<grd, 256, 0, s>>>(nel, in, out, ec_tab, mask, y, y2, part, stop, op, cg); }
-      break;
-    case DSS_DOT:
-      { SSG_COUNT(); k_dss<N, T, DSS_DOT><<<grd, 256, 0, s>>>(nel, in, out, ec_tab, mask, y, y2, part, stop, op, cg); }
-      break;
-    case DSS_DOT2:
-      { SSG_COUNT(); k_dss<N, T, DSS_DOT2><<<grd, 256, 0, s>>>(nel, in, out, ec_tab, mask, y, y2, part, stop, op, cg); }
-      break;
-    case DSS_RESID:
-      { SSG_COUNT(); k_dss<N, T, DSS_RESID><<<grd, 256, 0, s>>>(nel, in, out, ec_tab, mask, y, y2, part, stop, op, cg); }
-      break;
-    case DSS_AVG:
-      { SSG_COUNT(); k_dss<N, T, DSS_AVG><<<grd, 256, 0, s>>>(nel, in, out, ec_tab, mask, y, y2, part, stop, op, cg); }
-      break;
-    case DSS_CGUPD:
-      { SSG_COUNT(); k_dss<N, T, DSS_CGUPD><<<grd, 256, 0, s>>>(nel, in, out, ec_tab, mask, y, y2, part, stop, op, cg); }
-      break;
+#define SSG_DSSM(MV) \
+  case MV: launch_dss<N, T, MV>(s, nel, in, out, nb26, ec_tab, mask, y, y2, part, stop, op, cg); break;
+    SSG_DSSM(DSS_PLAIN) SSG_DSSM(DSS_DOT) SSG_DSSM(DSS_DOT2) SSG_DSSM(DSS_RESID)
+    SSG_DSSM(DSS_AVG) SSG_DSSM(DSS_CGUPD)
+#undef SSG_DSSM
     case DSS_SCALE:
       if constexpr (sizeof(T) == sizeof(double)) {
-        SSG_COUNT();
-        k_dss<N, T, DSS_SCALE><<<grd, 256, 0, s>>>(nel, in, out, ec_tab, mask, y, y2, part, stop, op, cg);
+        launch_dss<N, T, DSS_SCALE>(s, nel, in, out, nb26, ec_tab, mask, y, y2, part, stop, op,
+                                    cg);
       } else {
         return cudaErrorInvalidValue;
       }
@@ -793,13 +1118,12 @@ static cudaError_t run_dss_n(cudaStream_t s, int mode, int nel, const T* in, T* 
 
 template <typename T>
 static cudaError_t run_dss_t(cudaStream_t s, int mode, int n, int nel, const T* in, T* out,
-                             const int* pairs, const int* ec_tab, const double* mask,
+                             const int* nb26, const int* ec_tab, const double* mask,
                              const T* y, const T* y2, double* part, const double* stop,
                              const ScalarOp& op, const DssCg& cg) {
-  (void)pairs;   // folded into the level's gather words at set-up
   switch (n) {
 #define SSG_DSSN(NV) \
-  case NV: return run_dss_n<NV, T>(s, mode, nel, in, out, ec_tab, mask, y, y2, part, stop, op, cg);
+  case NV: return run_dss_n<NV, T>(s, mode, nel, in, out, nb26, ec_tab, mask, y, y2, part, stop, op, cg);
     SSG_DSSN(2) SSG_DSSN(3) SSG_DSSN(4) SSG_DSSN(5) SSG_DSSN(6) SSG_DSSN(7)
     SSG_DSSN(8) SSG_DSSN(9) SSG_DSSN(10) SSG_DSSN(11) SSG_DSSN(12)
 #undef SSG_DSSN
@@ -807,25 +1131,51 @@ static cudaError_t run_dss_t(cudaStream_t s, int mode, int n, int nel, const T* 
   }
 }
 
+// the line-run kernels load and store runs of a line as 8- or 16-byte
+// vectors when n is even: every array must then start on a 16-byte boundary
+// (the library's own vectors always do; a caller's pointer may not)
+static bool lines_aligned(int n, std::initializer_list<const void*> ptrs) {
+  if (n % 2) return true;
+  for (const void* p : ptrs)
+    if (reinterpret_cast<uintptr_t>(p) % 16u) return false;
+  return true;
+}
+
 cudaError_t run_dss(cudaStream_t s, int mode, bool fp32, int n, int nel, const void* in,
-                    void* out, const int* pairs, const int* ec_tab, const double* mask,
+                    void* out, const int* nb26, const int* ec_tab, const double* mask,
                     const void* y, const void* y2, double* part, const double* stop,
                     const ScalarOp* op, const DssCg* cg) {
   const ScalarOp o = op_or_none(op);
   const DssCg g = cg ? *cg : DssCg();
-  if (!ec_tab || (mode == DSS_CGUPD && !cg)) return cudaErrorInvalidValue;
+  if ((!ec_tab && !nb26) || (mode == DSS_CGUPD && !cg)) return cudaErrorInvalidValue;
+  if (nb26 && ec_tab && !lines_aligned(n, {in, out, mask, y, y2, g.x, g.p, g.r, g.dinv, g.z}))
+    nb26 = nullptr;
   if (fp32)
-    return run_dss_t<float>(s, mode, n, nel, (const float*)in, (float*)out, pairs, ec_tab,
+    return run_dss_t<float>(s, mode, n, nel, (const float*)in, (float*)out, nb26, ec_tab,
                             mask, (const float*)y, (const float*)y2, part, stop, o, g);
-  return run_dss_t<double>(s, mode, n, nel, (const double*)in, (double*)out, pairs, ec_tab,
+  return run_dss_t<double>(s, mode, n, nel, (const double*)in, (double*)out, nb26, ec_tab,
                            mask, (const double*)y, (const double*)y2, part, stop, o, g);
 }
 
 template <int N>
 static cudaError_t run_dss3_n(cudaStream_t s, bool scale, int nel, const double* in,
-                              double* out, size_t stride, const int* ec_tab, const double* y) {
-  const int grd = dss_grid(N, nel);
+                              double* out, size_t stride, const int* nb26, const int* ec_tab,
+                              const double* y) {
   SSG_COUNT();
+  if (nb26) {
+    constexpr int P = DssRun<N, double>::P;
+    static std::atomic<int> occ_s{0}, occ_p{0};
+    const size_t runs = (size_t)nel * N * N * (N / P);
+    if (scale) {
+      auto kern = &k_dss3_runs<N, P, true>;
+      kern<<<full_wave(kern, occ_s, runs), 256, 0, s>>>(nel, in, out, stride, nb26, y);
+    } else {
+      auto kern = &k_dss3_runs<N, P, false>;
+      kern<<<full_wave(kern, occ_p, runs), 256, 0, s>>>(nel, in, out, stride, nb26, y);
+    }
+    return cudaGetLastError();
+  }
+  const int grd = dss_grid(N, nel);
   if (scale)
     k_dss3<N, true><<<grd, 256, 0, s>>>(nel, in, out, stride, ec_tab, y);
   else
@@ -834,11 +1184,14 @@ static cudaError_t run_dss3_n(cudaStream_t s, bool scale, int nel, const double*
 }
 
 cudaError_t run_dss3(cudaStream_t s, bool scale, int n, int nel, const double* in, double* out,
-                     size_t stride, const int* ec_tab, const double* y) {
-  if (!ec_tab || (scale && !y)) return cudaErrorInvalidValue;
+                     size_t stride, const int* nb26, const int* ec_tab, const double* y) {
+  if ((!ec_tab && !nb26) || (scale && !y)) return cudaErrorInvalidValue;
+  if (nb26 && ec_tab &&
+      (!lines_aligned(n, {in, out, y}) || (n % 2 == 0 && (stride * sizeof(double)) % 16u)))
+    nb26 = nullptr;
   switch (n) {
 #define SSG_DSS3N(NV) \
-  case NV: return run_dss3_n<NV>(s, scale, nel, in, out, stride, ec_tab, y);
+  case NV: return run_dss3_n<NV>(s, scale, nel, in, out, stride, nb26, ec_tab, y);
     SSG_DSS3N(2) SSG_DSS3N(3) SSG_DSS3N(4) SSG_DSS3N(5) SSG_DSS3N(6) SSG_DSS3N(7)
     SSG_DSS3N(8) SSG_DSS3N(9) SSG_DSS3N(10) SSG_DSS3N(11) SSG_DSS3N(12)
 #undef SSG_DSS3N

@@ -125,7 +125,7 @@ size_t estimate_bytes(int n, int nel, int precision) {
     b += np * 9 * sizeof(double);                          // level work vectors
     if (precision == SSG_PRECISION_MIXED) b += np * 9 * sizeof(float);
   }
-  b += (size_t)nel * (52 + 26) * sizeof(int);   // pairing, neighbour table
+  b += (size_t)nel * (52 + 26 + 26) * sizeof(int);   // pairing, neighbour tables
   b += np0 * (8 + 8 + 8);                  // inverse mass, det J, workspace scratch
   b += np0 * 4 * 8;                        // staging (one field per slot)
   b += np0 * 24 * 8;                       // FCG: r, z, A p local, 11 + 10 directions

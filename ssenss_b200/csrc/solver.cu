@@ -242,7 +242,7 @@ ssg_status op_apply(ssg_context* c, int level, int var, bool fp32, const void* i
                      fp32 ? (const void*)L.gf32 : (const void*)L.gf, L.npts, L.bj, L.D, L.S,
                      lambda_of(c), nullptr));
   if (global)
-    SSG_CUDA(c, run_dss(c->stream, DSS_PLAIN, fp32, L.n, c->nel, loc, out, c->d_pairs, L.dss_ec,
+    SSG_CUDA(c, run_dss(c->stream, DSS_PLAIN, fp32, L.n, c->nel, loc, out, c->d_nbreg, L.dss_ec,
                         helm ? L.mask : nullptr, nullptr, nullptr, nullptr));
   return SSG_OK;
 }
@@ -304,7 +304,7 @@ ssg_status cg_solve(ssg_context* c, int level, int var, bool fp32, void* f, void
   SSG_CUDA(c, run_ax(s, L.n, c->nel, 0, helm, fp32, x, W.aploc, gf, np, L.bj, L.D, L.S, lam,
                      nullptr));
   op.code = OP_NULL_C;
-  SSG_CUDA(c, run_dss(s, DSS_RESID, fp32, L.n, c->nel, W.aploc, W.r, c->d_pairs, L.dss_ec, mask, f,
+  SSG_CUDA(c, run_dss(s, DSS_RESID, fp32, L.n, c->nel, W.aploc, W.r, c->d_nbreg, L.dss_ec, mask, f,
                       nullptr, c->d_part, nullptr, &op));
   if (pres) SSG_CUDA(c, run_add_const(s, fp32, np, W.r, fr + F_C, 1));
   // z = M^-1 r and its nullspace constant
@@ -384,11 +384,11 @@ ssg_status cg_solve(ssg_context* c, int level, int var, bool fp32, void* f, void
                                  L.S, lam, &pu));
               if (fused) {
                 op.code = OP_CG_BETA;
-                SSG_CUDA(c, run_dss(s, DSS_CGUPD, fp32, L.n, c->nel, W.aploc, nullptr, c->d_pairs,
+                SSG_CUDA(c, run_dss(s, DSS_CGUPD, fp32, L.n, c->nel, W.aploc, nullptr, c->d_nbreg,
                                     L.dss_ec, mask, nullptr, nullptr, c->d_part, stop, &op, &cg));
               } else {
                 op.code = OP_CG_ALPHA;
-                SSG_CUDA(c, run_dss(s, DSS_DOT, fp32, L.n, c->nel, W.aploc, W.ap, c->d_pairs,
+                SSG_CUDA(c, run_dss(s, DSS_DOT, fp32, L.n, c->nel, W.aploc, W.ap, c->d_nbreg,
                                     L.dss_ec, mask, W.p, nullptr, c->d_part, stop, &op));
                 op.code = OP_CG_BETA;
                 SSG_CUDA(c, run_cg_update(s, fp32, np, fr + F_ALPHA, x, W.p, W.r, W.ap, dinv,
@@ -434,12 +434,12 @@ ssg_status cg_solve(ssg_context* c, int level, int var, bool fp32, void* f, void
     if (fused) {
       // ap = DSS(mask aploc); x += alpha p; r -= alpha ap; z = M^-1 r; beta; err
       op.code = OP_CG_BETA;
-      SSG_CUDA(c, run_dss(s, DSS_CGUPD, fp32, L.n, c->nel, W.aploc, nullptr, c->d_pairs,
+      SSG_CUDA(c, run_dss(s, DSS_CGUPD, fp32, L.n, c->nel, W.aploc, nullptr, c->d_nbreg,
                           L.dss_ec, mask, nullptr, nullptr, c->d_part, stop, &op, &cg));
     } else {
       // ap = DSS(mask aploc); alpha = rdz / (p w).ap
       op.code = OP_CG_ALPHA;
-      SSG_CUDA(c, run_dss(s, DSS_DOT, fp32, L.n, c->nel, W.aploc, W.ap, c->d_pairs, L.dss_ec,
+      SSG_CUDA(c, run_dss(s, DSS_DOT, fp32, L.n, c->nel, W.aploc, W.ap, c->d_nbreg, L.dss_ec,
                           mask, W.p, nullptr, c->d_part, stop, &op));
       // x += alpha p; r -= alpha ap; z = M^-1 r; beta; err
       op.code = OP_CG_BETA;
@@ -507,14 +507,14 @@ static ssg_status mg_recurse(ssg_context* c, int L, void* f, void* x, double eps
     SSG_CUDA(c, run_ax(s, F.n, c->nel, 0, false, fp32, x, W.aploc,
                        fp32 ? (const void*)F.gf32 : (const void*)F.gf, F.npts, nullptr, F.D,
                        F.D, 0.0, nullptr));
-    SSG_CUDA(c, run_dss(s, DSS_RESID, fp32, F.n, c->nel, W.aploc, W.rr, c->d_pairs, F.dss_ec, nullptr,
+    SSG_CUDA(c, run_dss(s, DSS_RESID, fp32, F.n, c->nel, W.aploc, W.rr, c->d_nbreg, F.dss_ec, nullptr,
                         f, nullptr, c->d_part));
     rin = W.rr;
   }
   // restriction: (J^T)^3 then DSS-average at the coarse level
   SSG_CUDA(c, run_tensor3(s, fp32, false, c->nel, F.n, C.n,
                           C.Ar, rin, Wc.tc));
-  SSG_CUDA(c, run_dss(s, DSS_AVG, fp32, C.n, c->nel, Wc.tc, Wc.f, c->d_pairs, C.dss_ec, nullptr,
+  SSG_CUDA(c, run_dss(s, DSS_AVG, fp32, C.n, c->nel, Wc.tc, Wc.f, c->d_nbreg, C.dss_ec, nullptr,
                       nullptr, nullptr, nullptr));
   SSG_CUDA(c, cudaMemsetAsync(Wc.x, 0, C.npts * (fp32 ? sizeof(float) : sizeof(double)), s));
   SSG_TRY(mg_recurse(c, L + 1, Wc.f, Wc.x, eps, fp32));
@@ -657,7 +657,7 @@ ssg_status fcg_solve(ssg_context* c, const double* f, double* u, double eps, int
   SSG_CUDA(c, run_ax(s, L.n, c->nel, 0, false, false, u, w->aploc, L.gf, np, nullptr, L.D,
                      L.D, 0.0, nullptr));
   op.code = OP_NULL_C;
-  SSG_CUDA(c, run_dss(s, DSS_RESID, false, L.n, c->nel, w->aploc, w->r, c->d_pairs, L.dss_ec, nullptr,
+  SSG_CUDA(c, run_dss(s, DSS_RESID, false, L.n, c->nel, w->aploc, w->r, c->d_nbreg, L.dss_ec, nullptr,
                       f, nullptr, c->d_part, nullptr, &op));
   SSG_CUDA(c, run_add_const(s, false, np, w->r, fr + F_C, 1));
   PtrList ys;
@@ -723,7 +723,7 @@ ssg_status fcg_solve(ssg_context* c, const double* f, double* u, double eps, int
                        L.D, 0.0, nullptr));
     op.pap_idx[0] = aslot[0];
     op.code = OP_FCG_ALPHA;
-    SSG_CUDA(c, run_dss(s, DSS_DOT2, false, L.n, c->nel, w->aploc, ap0, c->d_pairs, L.dss_ec, nullptr,
+    SSG_CUDA(c, run_dss(s, DSS_DOT2, false, L.n, c->nel, w->aploc, ap0, c->d_nbreg, L.dss_ec, nullptr,
                         p0, w->r, c->d_part, nullptr, &op));
     // u += alpha p0; r -= alpha ap0; err
     op.code = OP_FCG_ERR;

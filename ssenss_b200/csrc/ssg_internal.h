@@ -174,6 +174,9 @@ struct ssg_context {
   int orders[SSG_MAXLEV] = {0};
   ssg::HostMesh host;
   int* d_pairs = nullptr;       // nel x 26 x int2
+  // nel x 26 neighbour ids when every pairing is the opposite face, edge
+  // or corner (the line-run DSS), else null (the gather-word DSS)
+  int* d_nbreg = nullptr;
   bool has_walls = false;
   ssg::DevLevel lev[SSG_MAXLEV];
   double* inv_mass = nullptr;   // level 0

@@ -148,15 +148,19 @@ cudaError_t run_ax(cudaStream_t s, int n, int nel, int epb, bool helm, bool fp32
 inline __host__ __device__ constexpr size_t dss_map_records_offset(size_t npts) {
   return (npts + 3) / 4 * 4;
 }
-// ec_tab: the DSS map of order n (dss_map_table)
+// ec_tab: the DSS map of order n (dss_map_table); nb26: the mesh's 26
+// neighbour ids per element when every face, edge and corner is paired with
+// the opposite one of its neighbour (the line-run kernel, no per-node
+// map read), else null (the gather-word kernel on ec_tab).  Both give the
+// same sums in the same order.
 cudaError_t run_dss(cudaStream_t s, int mode, bool fp32, int n, int nel, const void* in,
-                    void* out, const int* pairs, const int* ec_tab, const double* mask,
+                    void* out, const int* nb26, const int* ec_tab, const double* mask,
                     const void* y, const void* y2, double* part, const double* stop = nullptr,
                     const ScalarOp* op = nullptr, const DssCg* cg = nullptr);
 // DSS of three FP64 fields `stride` apart (a vector field's components) in
 // one launch, out-of-place; scale: then times y pointwise (the inverse mass)
 cudaError_t run_dss3(cudaStream_t s, bool scale, int n, int nel, const double* in, double* out,
-                     size_t stride, const int* ec_tab, const double* y);
+                     size_t stride, const int* nb26, const int* ec_tab, const double* y);
 cudaError_t run_tensor3(cudaStream_t s, bool fp32, bool add, int nel, int ni, int no,
                         const double* A, const void* in, void* out);
 cudaError_t run_cg_update(cudaStream_t s, bool fp32, size_t npts, const double* alpha,

@@ -166,7 +166,7 @@ ssg_status convection_rk4(ssg_context* c, double* du, double t0, double t, doubl
                                  c->conv_J, c->conv_scratch));
       // trivec_inverse_mass_matrix: per component the DSS, then the product
       // with 1 / DSS(mass), the three components in one pass
-      SSG_CUDA(c, run_dss3(s, true, L.n, c->nel, f[i], y, npc, L.dss_ec, c->inv_mass));
+      SSG_CUDA(c, run_dss3(s, true, L.n, c->nel, f[i], y, npc, c->d_nbreg, L.dss_ec, c->inv_mass));
       std::swap(f[i], y);
     }
     count_launch();

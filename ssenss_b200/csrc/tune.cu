@@ -79,7 +79,7 @@ static ssg_status tune_level(ssg_context* c, int level, double* a, double* b, do
       g_tune_dss_bps[n] = bps;
       float t = 0.f;
       SSG_TRY(time_launches(c, reps, [&] {
-        return run_dss(c->stream, DSS_DOT, false, n, c->nel, a, b, c->d_pairs, L.dss_ec,
+        return run_dss(c->stream, DSS_DOT, false, n, c->nel, a, b, c->d_nbreg, L.dss_ec,
                        nullptr, y, nullptr, c->d_part, nullptr, nullptr);
       }, &t));
       if (t < best) {
@@ -218,7 +218,7 @@ ssg_status ssg_time_smoother(ssg_context* c, int level, int reps, double* us) {
                   L.D, L.D, 0.0, nullptr);
   };
   auto dss = [&] {
-    return run_dss(c->stream, DSS_DOT, false, L.n, c->nel, buf[1], buf[2], c->d_pairs,
+    return run_dss(c->stream, DSS_DOT, false, L.n, c->nel, buf[1], buf[2], c->d_nbreg,
                    L.dss_ec, nullptr, buf[0], nullptr, c->d_part, nullptr, nullptr);
   };
   auto upd = [&] {
