@@ -361,6 +361,29 @@ __device__ __forceinline__ void direction_passes(const double* U, const double* 
   }
 }
 
+// the next element's fields and weights into L2 while this one computes:
+// lanes of warp 0 issue one bulk prefetch each (the three components of f0,
+// and of f1 when given, NT values each, `fstride` apart; the nine weight
+// arrays of MT values `wstride` apart); skipped for any address not on a
+// 16-byte boundary (a prefetch is only a hint)
+__device__ __forceinline__ void prefetch_element(int en, int nel, int e0, const double* f0,
+                                                 const double* f1, size_t fstride,
+                                                 const double* W, size_t wstride) {
+  if (threadIdx.x >= 32 || en >= nel) return;
+  const int lane = threadIdx.x;
+  const double* p = nullptr;
+  unsigned bytes = 0;
+  const int nf = f1 ? 6 : 3;
+  if (lane < nf) {
+    p = (lane < 3 ? f0 : f1) + (size_t)en * NT + (size_t)(lane % 3) * fstride;
+    bytes = NT * sizeof(double);
+  } else if (lane < nf + 9) {
+    p = W + (size_t)(e0 + en) * MT + (size_t)(lane - nf) * wstride;
+    bytes = MT * sizeof(double);
+  }
+  if (p && (reinterpret_cast<uintptr_t>(p) & 15u) == 0) bulk_prefetch_l2(p, bytes);
+}
+
 }  // namespace cdm
 
 // u advecting itself: U (3 fields), SK (3 fields)
@@ -378,6 +401,7 @@ __global__ void __launch_bounds__(cdm::THREADS, 2)
   const size_t nptsn = (size_t)nel * NT, wstride = (size_t)nel_fac * MT;
   for (int e = blockIdx.x; e < nel; e += gridDim.x) {
     const double* Wb = W + (size_t)(e0 + e) * MT;
+    prefetch_element(e + gridDim.x, nel, e0, u, nullptr, nptsn, W, wstride);
     // T1 in U, T2 in SK
     interpolate(3, u + (size_t)e * NT, nptsn, U, SK, U, FR);
     direction_passes<3>(U, U, SK, Wb, wstride, FR);
@@ -404,6 +428,7 @@ __global__ void __launch_bounds__(cdm::THREADS_UV, 1)
   const size_t nptsn = (size_t)nel * NT, wstride = (size_t)nel_fac * MT;
   for (int e = blockIdx.x; e < nel; e += gridDim.x) {
     const double* Wb = W + (size_t)(e0 + e) * MT;
+    prefetch_element(e + gridDim.x, nel, e0, u, v, nptsn, W, wstride);
     // u: T1 in U, T2 in V; v: T1 in V, T2 in SK
     interpolate(3, u + (size_t)e * NT, nptsn, U, V, U, FR);
     interpolate(3, v + (size_t)e * NT, nptsn, V, SK, V, FR);
