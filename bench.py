@@ -66,8 +66,9 @@ def parse():
                     help="launch the V-cycle kernels directly (no CUDA graph)")
     ap.add_argument("--serve-requests", type=int, default=300,
                     help="requests of the serving stream (the full stream is 2000)")
-    ap.add_argument("--serve-rate", type=float, default=20.0,
-                    help="Poisson arrival rate of the serving stream (requests/s)")
+    ap.add_argument("--serve-rate", type=float, default=15.0,
+                    help="Poisson arrival rate of the serving stream (requests/s; "
+                         "15/s is the rate the service target is stated at)")
     ap.add_argument("--serve-slots", type=int, default=8,
                     help="requests in flight at once in the serving loop")
     ap.add_argument("--serve-open-only", action="store_true",
