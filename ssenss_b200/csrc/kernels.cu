@@ -1148,8 +1148,10 @@ cudaError_t run_dss(cudaStream_t s, int mode, bool fp32, int n, int nel, const v
   const ScalarOp o = op_or_none(op);
   const DssCg g = cg ? *cg : DssCg();
   if ((!ec_tab && !nb26) || (mode == DSS_CGUPD && !cg)) return cudaErrorInvalidValue;
-  if (nb26 && ec_tab && !lines_aligned(n, {in, out, mask, y, y2, g.x, g.p, g.r, g.dinv, g.z}))
+  if (nb26 && !lines_aligned(n, {in, out, mask, y, y2, g.x, g.p, g.r, g.dinv, g.z})) {
+    if (!ec_tab) return cudaErrorMisalignedAddress;
     nb26 = nullptr;
+  }
   if (fp32)
     return run_dss_t<float>(s, mode, n, nel, (const float*)in, (float*)out, nb26, ec_tab,
                             mask, (const float*)y, (const float*)y2, part, stop, o, g);
@@ -1186,9 +1188,11 @@ static cudaError_t run_dss3_n(cudaStream_t s, bool scale, int nel, const double*
 cudaError_t run_dss3(cudaStream_t s, bool scale, int n, int nel, const double* in, double* out,
                      size_t stride, const int* nb26, const int* ec_tab, const double* y) {
   if ((!ec_tab && !nb26) || (scale && !y)) return cudaErrorInvalidValue;
-  if (nb26 && ec_tab &&
-      (!lines_aligned(n, {in, out, y}) || (n % 2 == 0 && (stride * sizeof(double)) % 16u)))
+  if (nb26 &&
+      (!lines_aligned(n, {in, out, y}) || (n % 2 == 0 && (stride * sizeof(double)) % 16u))) {
+    if (!ec_tab) return cudaErrorMisalignedAddress;
     nb26 = nullptr;
+  }
   switch (n) {
 #define SSG_DSS3N(NV) \
   case NV: return run_dss3_n<NV>(s, scale, nel, in, out, stride, nb26, ec_tab, y);
